@@ -1,0 +1,195 @@
+/*
+ * q2d_gpu.h — C ABI of the B200 (sm_100a) explicit finite-volume residual and
+ * time-update path of Q2D.
+ *
+ * Drop-in granularity: one call of q2d_gpu_step() replaces one (or N) executions of the
+ * body of Q2D's `Explicit_Step` for one grid level:
+ *   src/lib/numerics/time/explicit/Mod_Explicit.f90:10-174
+ * i.e. Compute_dt (Mod_dt.f90:10-106), Set_Global_dt (Mod_dt.f90:109-128), Copy_State
+ * (Mod_Explicit.f90:177-197), the n_RK stages of {Fill_Ghost_Cell (Lib_Ghost.f90:16-140),
+ * Fluxes (Mod_Fluxes.f90:97-234), BC_Fluxes (Mod_BC_Fluxes.f90:49-271), Compute_Sources
+ * (Mod_Sources.f90:79-91), RK_Newstate (Lib_Newstate.f90:14-161)}, Compute_Residual
+ * (Mod_Diagnostic.f90:438-469) and the TODO/stop logic (Mod_Explicit.f90:120-172).
+ *
+ * The per-face procedure pointers of the reference (Riemann, rlimiter, Fluxes, RK_Newstate,
+ * bound in Assign_Setup.f90:40-62) become the scheme fields of q2d_options: the library
+ * specialises its kernels on them once, at q2d_gpu_create().
+ *
+ * Conventions
+ *   - All arrays are host arrays owned by the caller, read or written only during the call
+ *     that receives them; no pointer is retained (ownership row of the boundary).
+ *   - Block and cell indices in q2d_bc_rec are 1-based like bc.txt (IO_BC.f90:209-402);
+ *     `b` is the 1-based index of the block inside its case, in q2d_gpu_add_block order.
+ *   - nodes_xy: the reference array node(0:ni,0:nj)%c(2) in Fortran order, i.e. x,y of
+ *     node (i,j) at nodes_xy[2*(i + (ni+1)*j) + {0,1}].
+ *   - cross_section: nodal A(0:ni,0:nj), i fastest (Lib_Source_Areavariation.f90:53-101);
+ *     NULL when the block has no area file.
+ *   - P: the reference array P(nprim=4, 1-gc:ni+gc, 1-gc:nj+gc), gc=2, Fortran order
+ *     (Mod_Allocate_Data.f90:122-123): variable v of cell (i,j) at
+ *     P[v + 4*((i+1) + (ni+4)*(j+1))], i in [-1, ni+2], j in [-1, nj+2]; only the
+ *     interior 1..ni x 1..nj is read or written. Variables: rho, u, v, p.
+ *   - Every function returns a Q2D_* status; nothing aborts the process (the reference's
+ *     `error stop`/`stop` sites map to Q2D_ERR_NONPHYSICAL / Q2D_ERR_NAN).
+ *   - Threading: one host thread per context; calls on one context are stream-ordered and
+ *     not re-entrant; separate contexts are independent.
+ */
+#ifndef Q2D_GPU_H
+#define Q2D_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define Q2D_OK               0
+#define Q2D_ERR_BADARG       1   /* invalid argument or call order */
+#define Q2D_ERR_OOM          2   /* device or host allocation failed */
+#define Q2D_ERR_CUDA         3   /* CUDA runtime error (message in q2d_gpu_last_error) */
+#define Q2D_ERR_NONPHYSICAL  4   /* non-physical interface state: Lib_Convective.f90:49-54 */
+#define Q2D_ERR_NAN          5   /* NaN or p<0 after the update: Lib_Newstate.f90:327-331 */
+#define Q2D_ERR_TIMEOUT      6   /* a bounded device wait ran out */
+#define Q2D_ERR_UNSUPPORTED  7   /* option or BC type outside the built path */
+#define Q2D_ERR_CAPACITY     8   /* request exceeds a fixed-size buffer or budget */
+
+/* ---- scheme selectors (keywords of Mod_Space.f90:43-76 and Mod_Riemann.f90:25-109) --- */
+#define Q2D_LIM_IORD       0   /* first order ('none' / unknown keyword)   Lib_Limiters.f90:26-33 */
+#define Q2D_LIM_MINMOD     1   /* 'minmod'                                  :36-46 */
+#define Q2D_LIM_VANLEER    2   /* 'vanleer'                                 :49-58 */
+#define Q2D_LIM_VANALBADA  3   /* 'vanalbada'                               :61-70 */
+#define Q2D_LIM_MC         4   /* 'mc'                                      :73-82 */
+#define Q2D_LIM_SUPERBEE   5   /* 'superbee'                                :85-94 */
+#define Q2D_LIM_LIMO3      6   /* 'LIMO3'                                   :98-110 */
+
+#define Q2D_RIEMANN_HLLC   0   /* 'HLLC' (default)    Lib_Riemann_HLL.f90:34-123 */
+#define Q2D_RIEMANN_HLLE   1   /* 'HLLE'              Lib_Riemann_HLL.f90:126-169 */
+#define Q2D_RIEMANN_LLF    2   /* 'LLF' / 'Rusanov'   Lib_Riemann_LF.f90:11-40 */
+
+#define Q2D_SRC_NONE       0
+#define Q2D_SRC_AXI        1   /* [Q2D-Sources] active = axisymmetric   Lib_Source_Axisymmetry.f90:40-78 */
+#define Q2D_SRC_AREA       2   /* [Q2D-Sources] active = area_variation Lib_Source_Areavariation.f90:104-144 */
+
+#define Q2D_PREC_FP64      0   /* plain FP64 everywhere */
+#define Q2D_PREC_FP32_FLUX 1   /* reconstruction, limiter, Riemann in FP32; state, flux sums,
+                                  RK combination, positivity checks and norms in FP64 */
+
+/* BC types served by the path (Mod_BC_Fluxes.f90:79-269 dispatch codes) */
+#define Q2D_BC_CONNECTION  101
+#define Q2D_BC_SYMMETRY    300
+#define Q2D_BC_EXTRAP      400
+#define Q2D_BC_STAGNATION  401
+#define Q2D_BC_SUPERSONIC  405
+#define Q2D_BC_OUTFLOW     406
+
+/* q2d_step_info.todo, the reference's obj_sim_param%TODO (Mod_Explicit.f90:161-169) */
+#define Q2D_TODO_CONTINUE  1
+#define Q2D_TODO_IO        2
+#define Q2D_TODO_END       3
+
+typedef struct q2d_ctx q2d_ctx;
+
+/* Numerics and run control. Mirrors the [Q2D-Numerics]/[Q2D-Parameters]/[Q2D-IO]/
+ * [Q2D-Sources] keys read in Register_Numerics.f90:31-76, Register_Sim_Param.f90:26-29,
+ * Register_IO.f90:26-35; defaults via q2d_options_default(). */
+typedef struct q2d_options {
+    int    limiter;         /* Q2D_LIM_*                       flux-limiter */
+    int    riemann;         /* Q2D_RIEMANN_*                   riemann-solver */
+    int    n_rk;            /* 1 ('euler'), 2 ('RK2'), 3 ('RK3') time-scheme */
+    int    time_accurate;   /* 0/1                             time-accurate */
+    int    source;          /* Q2D_SRC_*                       [Q2D-Sources] active */
+    int    precision;       /* Q2D_PREC_*                      (no reference counterpart) */
+    int    rampa_iter;      /* cfl-rise-threshold */
+    int    res_diter;       /* res-diter */
+    int    sol_diter;       /* sol-diter */
+    int    res_relative;    /* 0: stop on residual(1) <= res_threshold (reference);
+                               1: stop on residual(1) <= res_threshold * residual(1) of the
+                                  first step of the case (relative drop, used by serving) */
+    long long itermax;      /* iter-threshold */
+    double cfl;             /* cfl */
+    double res_threshold;   /* res-threshold */
+    double time_threshold;  /* time-threshold */
+    double sol_dtime;       /* sol-dtime */
+    double gas_R;           /* specific gas constant R = Runiv/W of the single species */
+    double gas_gamma;       /* ratio of specific heats of the calorically perfect closure */
+} q2d_options;
+
+/* One boundary-cell record: the 5-integer header line of bc.txt plus its property line
+ * (IO_BC.f90:209-402). Fields not used by a type are ignored. alpha >= 0.5*DBL_MAX means the
+ * 'normal' keyword (parse_dir_tok sentinel, Lib_BC_Fluxes_Inflow.f90:552-560). */
+typedef struct q2d_bc_rec {
+    int    b, i, j, f, type;
+    int    bs, is, js, fs, d11, d12, d21, d22;   /* 101: donor block/cell/face + orientation */
+    double T0;        /* 401: total T; 405: static T */
+    double p0;        /* 401: total p */
+    double pamb;      /* 405: static p; 406: back pressure (<=0: extrapolation) */
+    double mach;      /* 405: Mach */
+    double alpha;     /* 401/405: flow angle [rad] or the 'normal' sentinel */
+    double rel_fac;   /* 401/405/406: relaxation factor */
+} q2d_bc_rec;
+
+/* Per-case result of the last executed step (the reference's domain%dtglobal, %time,
+ * %iter, obj_sim_param%residuotot and TODO) plus the first error seen. */
+typedef struct q2d_step_info {
+    double    dtglobal;
+    double    time;
+    long long iter;
+    double    residual[4];   /* sqrt(sum over cells of |d rho|^2, |du|^2, |dv|^2, |dp|^2) */
+    double    residual0;     /* residual[0] of the first step of the case */
+    int       todo;          /* Q2D_TODO_* */
+    int       err;           /* Q2D_OK or Q2D_ERR_NONPHYSICAL / Q2D_ERR_NAN */
+    int       err_b, err_i, err_j, err_stage;   /* where err was first raised (1-based) */
+} q2d_step_info;
+
+/* Fills *opt with the reference defaults (HLLC, first order, euler, cfl 0.5, res-threshold
+ * 1e-10, time-threshold 1e30, iter-threshold 1e9, res-diter 1, R=287, gamma=1.4). */
+void q2d_options_default(q2d_options* opt);
+
+/* Creates a context on the current CUDA device. Replaces Assign_Setup (Assign_Setup.f90:11-117). */
+int  q2d_gpu_create(q2d_ctx** out, const q2d_options* opt);
+
+/* Adds an empty case (one Q2D domain: its blocks share dtglobal, time, iter, residual). */
+int  q2d_gpu_add_case(q2d_ctx* ctx, int* case_id);
+
+/* Adds a block to a case. Replaces Allocate_Block (Mod_Allocate_Data.f90:86-180) and the
+ * node/Cross_Section reads (IO_Solution.f90:38-129, Lib_Source_Areavariation.f90:53-101). */
+int  q2d_gpu_add_block(q2d_ctx* ctx, int case_id, int ni, int nj, const double* nodes_xy,
+                       const double* cross_section, int* block_id);
+
+/* Sets the boundary records of a case, sorted by block then face like bc.txt
+ * (Read_BCfile, IO_BC.f90:163-440; ordering consumed by Mod_BC_Fluxes.f90:79-84). */
+int  q2d_gpu_set_bcs(q2d_ctx* ctx, int case_id, const q2d_bc_rec* recs, int n);
+
+/* Copies the interior of a block's primitive state host->device (Read_IC result). */
+int  q2d_gpu_upload_prim(q2d_ctx* ctx, int block_id, const double* P);
+
+/* Builds metrics (Setup_Metrics, Mod_Metrics.f90:11-148) and the device work lists.
+ * Called implicitly by the first q2d_gpu_step(). */
+int  q2d_gpu_commit(q2d_ctx* ctx);
+
+/* Advances every running case by up to nsteps explicit steps (Explicit_Step). A case stops
+ * early when its TODO becomes END, when it raises IO (sol-diter / sol-dtime), or on error.
+ * out, when not NULL, receives q2d_gpu_num_cases() entries. Returns the first case error. */
+int  q2d_gpu_step(q2d_ctx* ctx, int nsteps, q2d_step_info* out);
+
+/* Reads the current step info of one case. */
+int  q2d_gpu_case_info(q2d_ctx* ctx, int case_id, q2d_step_info* out);
+
+/* Copies the interior of a block's primitive state device->host. */
+int  q2d_gpu_download_prim(q2d_ctx* ctx, int block_id, double* P);
+
+/* Number of cases and total interior cells of the context. */
+int       q2d_gpu_num_cases(const q2d_ctx* ctx);
+long long q2d_gpu_num_cells(const q2d_ctx* ctx);
+
+/* Number of kernel launches issued by this context since creation (instrumentation). */
+long long q2d_gpu_launch_count(const q2d_ctx* ctx);
+
+/* Text of a status code, and the last detailed error message of a context. */
+const char* q2d_gpu_errstr(int status);
+const char* q2d_gpu_last_error(const q2d_ctx* ctx);
+
+void q2d_gpu_destroy(q2d_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* Q2D_GPU_H */

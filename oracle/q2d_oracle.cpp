@@ -1,0 +1,1468 @@
+// q2d_oracle.cpp — CPU oracle: C++ restatement of Q2D's explicit residual + update path.
+//
+// TEST INFRASTRUCTURE ONLY (checker and timed CPU baseline). Each routine names the
+// reference Fortran file:line it restates (paths relative to the open-hydra/Q2D tree).
+// Loop nesting, accumulation order and operation order follow the Fortran so that the
+// oracle is the reference's arithmetic up to the thermodynamic closure (FLINT is absent;
+// the calorically perfect single-species closure implied by the constant-cp tables is
+// used, see the THERMO section). OpenMP parallelises the cell loops the way the
+// reference's `!$omp do` does; every reduction is summed in a fixed order.
+#include "q2d_oracle.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <cfloat>
+#include <vector>
+#include <algorithm>
+#include <new>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr int GC = 2;      // Global_m.f90:25
+constexpr int NPRIM = 4;   // rho, u, v, p (nsc = 1)
+
+// guide(f,:) for faces 1..4 (Parameters_m.f90:13-18)
+constexpr int GUIDE[5][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+
+// ---------------------------------------------------------------------------------------
+// THERMO: calorically perfect closure standing in for FLINT_Lib_Thermodynamic.
+//   co_rotot_Rtot -> rho = rho_1, R = gas_R ; f_ss -> sqrt(gamma p / rho) ; f_gamma -> gamma
+//   E0(p,rho,|V|) = p/((gamma-1) rho) + |V|^2/2 ; H0 = gamma p/((gamma-1) rho) + |V|^2/2
+//   h_tab/cp_tab lerp -> h = cp T, cp = gamma R/(gamma-1)
+//   prim2cons -> (rho, rho u, rho v, p/(gamma-1) + rho |V|^2/2)
+//   cons2prim -> p = (gamma-1)(rho E - rho |V|^2/2)
+// ---------------------------------------------------------------------------------------
+struct Gas {
+    double R, gamma, gm1, cp, cv;
+};
+
+inline double f_ss(const Gas& g, double p, double rho) { return std::sqrt(g.gamma * p / rho); }
+inline double E0(const Gas& g, double p, double rho, double modv) {
+    return p / (g.gm1 * rho) + 0.5 * modv * modv;
+}
+inline double H0(const Gas& g, double p, double rho, double modv) {
+    return g.gamma * p / (g.gm1 * rho) + 0.5 * modv * modv;
+}
+inline void prim2cons(const Gas& g, const double* P, double* U) {
+    U[0] = P[0];
+    U[1] = P[0] * P[1];
+    U[2] = P[0] * P[2];
+    U[3] = P[3] / g.gm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
+}
+inline void cons2prim(const Gas& g, const double* U, double* P) {
+    const double rho = U[0];
+    const double u = U[1] / rho;
+    const double v = U[2] / rho;
+    P[0] = rho;
+    P[1] = u;
+    P[2] = v;
+    P[3] = g.gm1 * (U[3] - 0.5 * rho * (u * u + v * v));
+}
+// check_gas_state (Lib_Convective.f90:49-54): non-physical when rho<=0, p<=0 or NaN.
+inline bool gas_state_bad(double rho, double p) { return !(rho > 0.0) || !(p > 0.0); }
+
+// ---------------------------------------------------------------------------------------
+// Limiters (Lib_Limiters.f90:26-110)
+// ---------------------------------------------------------------------------------------
+inline double lim_minmod(double x, double y) {          // :36-46
+    double r = 0.0;
+    if (x * y < 0.0) return r;
+    r = x;
+    if (std::fabs(x) > std::fabs(y)) r = y;
+    return r;
+}
+inline double lim_vanleer(double x, double y) {         // :49-58
+    double ru = y / (x + 1e-30);
+    double phi = (ru + std::fabs(ru)) / (1.0 + std::fabs(ru));
+    return phi * x;
+}
+inline double lim_vanalbada(double x, double y) {       // :61-70
+    double ru = y / (x + 1e-30);
+    double phi = (ru * ru + ru) / (1.0 + ru * ru);
+    return phi * x;
+}
+inline double fmax_(double a, double b) { return a > b ? a : b; }   // Fortran max on non-NaN
+inline double fmin_(double a, double b) { return a < b ? a : b; }
+inline double lim_mc(double x, double y) {              // :73-82
+    double ru = y / (x + 1e-30);
+    double phi = fmax_(0.0, fmin_(fmin_(2.0 * ru, 0.5 * (1.0 + ru)), 2.0));
+    return phi * x;
+}
+inline double lim_superbee(double x, double y) {        // :85-94
+    double ru = y / (x + 1e-30);
+    double phi = fmax_(fmax_(0.0, fmin_(2.0 * ru, 1.0)), fmin_(ru, 2.0));
+    return phi * x;
+}
+inline double lim_limo3(double x, double y) {           // :98-110
+    double ru = y / (x + 1e-30);
+    double a = (2.0 + ru) / 3.0;
+    double inner = fmin_(fmin_(2.0 * ru, (2.0 + ru) / 3.0), 1.6);
+    double mid = fmax_(fmax_(-0.5 * ru, 0.0), inner);
+    double phi = fmax_(0.0, fmin_(a, mid));
+    return phi * x;
+}
+inline double rlimiter(int lim, double x, double y) {
+    switch (lim) {
+        case Q2D_LIM_MINMOD: return lim_minmod(x, y);
+        case Q2D_LIM_VANLEER: return lim_vanleer(x, y);
+        case Q2D_LIM_VANALBADA: return lim_vanalbada(x, y);
+        case Q2D_LIM_MC: return lim_mc(x, y);
+        case Q2D_LIM_SUPERBEE: return lim_superbee(x, y);
+        case Q2D_LIM_LIMO3: return lim_limo3(x, y);
+        default: return 0.0;                             // rlimiter_IORD :26-33
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Riemann solvers. Arguments follow riemann_if (Mod_Riemann.f90:11-20) for nsc = 1:
+// (rho_s, u, v, p, a, rho_tot) for L and R, then nx, ny.
+// ---------------------------------------------------------------------------------------
+struct Flux4 { double r, u, v, e; };
+
+// roe_averages (Lib_Riemann_HLL.f90:229-317), constant-cp identities for the table lerps.
+inline void roe_averages(const Gas& g, double dl, double dr, double dltot, double drtot,
+                         double ul, double vl, double ur, double vr, double pl, double pr,
+                         double& h0l, double& h0r, double& rho_roe, double& u_roe,
+                         double& v_roe, double& a_roe, double& h0_roe) {
+    const double Rl = g.R, Rr = g.R;                        // f_Rtot
+    const double inv_dltot = 1.0 / dltot;
+    const double inv_drtot = 1.0 / drtot;
+    const double Tl = pl * inv_dltot / Rl;
+    const double Tr = pr * inv_drtot / Rr;
+    const double srL = std::sqrt(dltot);
+    const double srR = std::sqrt(drtot);
+    const double inv_sr = 1.0 / (srL + srR);
+    rho_roe = srL * srR;
+    u_roe = (srR * ur + srL * ul) * inv_sr;
+    v_roe = (srR * vr + srL * vl) * inv_sr;
+    const double R_roe = (srR * Rr + srL * Rl) * inv_sr;
+    const double T_roe = (srR * Tr + srL * Tl) * inv_sr;
+    const double invW = g.R;                                // Runiv / Wm_tab
+    const double hl = g.cp * Tl;                            // h_tab lerp at Tl
+    const double hr = g.cp * Tr;
+    const double el = hl - invW * Tl;
+    const double er = hr - invW * Tr;
+    h0l = 0.0 + hl * dl * inv_dltot;
+    h0r = 0.0 + hr * dr * inv_drtot;
+    const double d_roe = (srR * dr * inv_drtot + srL * dl * inv_dltot) * inv_sr;
+    const double cv_roe = 0.0 + d_roe * (0.5 * (g.cp + g.cp) - invW);
+    const double sum_ei = 0.0 + d_roe * (srR * er + srL * el) * inv_sr;
+    h0l = h0l + 0.5 * (ul * ul + vl * vl);
+    h0r = h0r + 0.5 * (ur * ur + vr * vr);
+    h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+    const double gam_roe = 1.0 + R_roe / cv_roe;
+    const double vel2 = u_roe * u_roe + v_roe * v_roe;
+    a_roe = std::sqrt((gam_roe - 1.0) * (h0_roe - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
+}
+
+// riemann_HLLC (Lib_Riemann_HLL.f90:34-123)
+inline Flux4 riemann_hllc(const Gas& g, double dl, double ul, double vl, double pl, double al,
+                          double dltot, double dr, double ur, double vr, double pr, double ar,
+                          double drtot, double nx, double ny) {
+    Flux4 F;
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    double h0l, h0r, rho_roe, u_roe, v_roe, a_roe, h0_roe;
+    roe_averages(g, dl, dr, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, rho_roe, u_roe,
+                 v_roe, a_roe, h0_roe);
+    const double un_roe = u_roe * nx + v_roe * ny;
+    const double e0l = h0l - pl / dltot;
+    const double e0r = h0r - pr / drtot;
+    const double S1 = fmin_(fmin_(0.0, unl - al), un_roe - a_roe);
+    const double S4 = fmax_(fmax_(0.0, unr + ar), un_roe + a_roe);
+    double inv_denom = 1.0 / (dltot * (S1 - unl) - drtot * (S4 - unr));
+    const double Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) * inv_denom;
+    const double pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
+    if (S1 >= 0.0) {
+        F.r = dltot * unl;
+        F.u = F.r * ul + pl * nx;
+        F.v = F.r * vl + pl * ny;
+        F.e = F.r * h0l;
+    } else if (Sstar >= 0.0) {
+        F.r = dltot * unl;
+        F.u = F.r * ul + pl * nx;
+        F.v = F.r * vl + pl * ny;
+        F.e = F.r * h0l;
+        inv_denom = 1.0 / (S1 - Sstar);
+        const double U1S = dltot * (S1 - unl) * inv_denom;
+        const double U2S = ((S1 - unl) * dltot * ul + (pstar - pl) * nx) * inv_denom;
+        const double U3S = ((S1 - unl) * dltot * vl + (pstar - pl) * ny) * inv_denom;
+        const double U5S = ((S1 - unl) * dltot * e0l - pl * unl + pstar * Sstar) * inv_denom;
+        F.r = F.r + S1 * (U1S - dltot);
+        F.u = F.u + S1 * (U2S - dltot * ul);
+        F.v = F.v + S1 * (U3S - dltot * vl);
+        F.e = F.e + S1 * (U5S - dltot * e0l);
+    } else if (S4 > 0.0) {
+        F.r = drtot * unr;
+        F.u = F.r * ur + pr * nx;
+        F.v = F.r * vr + pr * ny;
+        F.e = F.r * h0r;
+        inv_denom = 1.0 / (S4 - Sstar);
+        const double U1S = drtot * (S4 - unr) * inv_denom;
+        const double U2S = ((S4 - unr) * drtot * ur + (pstar - pr) * nx) * inv_denom;
+        const double U3S = ((S4 - unr) * drtot * vr + (pstar - pr) * ny) * inv_denom;
+        const double U5S = ((S4 - unr) * drtot * e0r - pr * unr + pstar * Sstar) * inv_denom;
+        F.r = F.r + S4 * (U1S - drtot);
+        F.u = F.u + S4 * (U2S - drtot * ur);
+        F.v = F.v + S4 * (U3S - drtot * vr);
+        F.e = F.e + S4 * (U5S - drtot * e0r);
+    } else {
+        F.r = drtot * unr;
+        F.u = F.r * ur + pr * nx;
+        F.v = F.r * vr + pr * ny;
+        F.e = F.r * h0r;
+    }
+    return F;
+}
+
+// riemann_HLLE (Lib_Riemann_HLL.f90:126-169)
+inline Flux4 riemann_hlle(const Gas& g, double dl, double ul, double vl, double pl, double al,
+                          double dltot, double dr, double ur, double vr, double pr, double ar,
+                          double drtot, double nx, double ny) {
+    Flux4 F;
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    double h0l, h0r, rho_roe, u_roe, v_roe, a_roe, h0_roe;
+    roe_averages(g, dl, dr, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, rho_roe, u_roe,
+                 v_roe, a_roe, h0_roe);
+    const double un_roe = u_roe * nx + v_roe * ny;
+    const double S1 = fmin_(fmin_(0.0, unl - al), un_roe - a_roe);
+    const double S4 = fmax_(fmax_(0.0, unr + ar), un_roe + a_roe);
+    const double inv_denom = 1.0 / (S4 - S1);
+    const double FrL = dltot * unl;
+    const double FrR = drtot * unr;
+    F.r = (S4 * FrL - S1 * FrR + S1 * S4 * (drtot - dltot)) * inv_denom;
+    F.u = (S4 * (FrL * ul + pl * nx) - S1 * (FrR * ur + pr * nx) +
+           S1 * S4 * (drtot * ur - dltot * ul)) * inv_denom;
+    F.v = (S4 * (FrL * vl + pl * ny) - S1 * (FrR * vr + pr * ny) +
+           S1 * S4 * (drtot * vr - dltot * vl)) * inv_denom;
+    F.e = (S4 * (FrL * h0l) - S1 * (FrR * h0r) +
+           S1 * S4 * (drtot * (h0r - pr / drtot) - dltot * (h0l - pl / dltot))) * inv_denom;
+    return F;
+}
+
+// fluxes (Lib_Riemann_LF.f90:101-118)
+inline Flux4 physical_flux(const Gas& g, double p, double r, double u, double v, double nx,
+                           double ny) {
+    Flux4 F;
+    F.r = r * (u * nx + v * ny);
+    F.u = F.r * u + p * nx;
+    F.v = F.r * v + p * ny;
+    F.e = F.r * H0(g, p, r, std::sqrt(u * u + v * v));
+    return F;
+}
+
+// riemann_LLF (Lib_Riemann_LF.f90:11-40)
+inline Flux4 riemann_llf(const Gas& g, double dl, double ul, double vl, double pl, double al,
+                         double dltot, double dr, double ur, double vr, double pr, double ar,
+                         double drtot, double nx, double ny) {
+    Flux4 F;
+    const double uln = ul * nx + vl * ny;
+    const double urn = ur * nx + vr * ny;
+    const double A = fmax_(fmax_(fmax_(std::fabs(uln - al), std::fabs(urn - ar)),
+                                 std::fabs(uln + al)), std::fabs(urn + ar));
+    const Flux4 Fr = physical_flux(g, pr, dr, ur, vr, nx, ny);
+    const Flux4 Fl = physical_flux(g, pl, dl, ul, vl, nx, ny);
+    F.r = 0.5 * (Fl.r + Fr.r - A * (drtot - dltot));
+    F.u = 0.5 * (Fr.u + Fl.u - A * (drtot * ur - dltot * ul));
+    F.v = 0.5 * (Fr.v + Fl.v - A * (drtot * vr - dltot * vl));
+    F.e = 0.5 * (Fl.e + Fr.e - A * (drtot * E0(g, pr, dr, std::sqrt(ur * ur + vr * vr)) -
+                                    dltot * E0(g, pl, dl, std::sqrt(ul * ul + vl * vl))));
+    return F;
+}
+
+inline Flux4 riemann(int kind, const Gas& g, const double* L, double aL, const double* R,
+                     double aR, double nx, double ny) {
+    switch (kind) {
+        case Q2D_RIEMANN_HLLE:
+            return riemann_hlle(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR,
+                                R[0], nx, ny);
+        case Q2D_RIEMANN_LLF:
+            return riemann_llf(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR,
+                               R[0], nx, ny);
+        default:
+            return riemann_hllc(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR,
+                                R[0], nx, ny);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Data structures (Advanced_Types_m.f90:17-89)
+// ---------------------------------------------------------------------------------------
+struct Block {
+    int ni = 0, nj = 0, case_id = 0, local_b = 0;
+    std::vector<double> node;     // (0:ni,0:nj) x,y
+    std::vector<double> area;     // (0:ni,0:nj) or empty
+    std::vector<double> P, PO, R; // (4, -1:ni+2, -1:nj+2)
+    std::vector<double> M;        // (4) per ghost-frame cell: M11 M12 M21 M22
+    std::vector<double> dl;       // (2) per ghost-frame cell
+    std::vector<double> sur;      // per ghost-frame cell
+    std::vector<double> f1;       // i-faces (0:ni,1:nj): nx ny len
+    std::vector<double> f2;       // j-faces (1:ni,0:nj): nx ny len
+    std::vector<double> dtlocal;  // (1:ni,1:nj)
+    std::vector<double> inv_r, Gx, Gy;   // (1:ni,1:nj)
+
+    int c(int i, int j) const { return (i + 1) + (ni + 4) * (j + 1); }
+    double nx_(int i, int j) const { return node[2 * (i + (ni + 1) * j)]; }
+    double ny_(int i, int j) const { return node[2 * (i + (ni + 1) * j) + 1]; }
+    double* p(int i, int j) { return &P[4 * c(i, j)]; }
+    const double* pc(int i, int j) const { return &P[4 * c(i, j)]; }
+    double* r(int i, int j) { return &R[4 * c(i, j)]; }
+    const double* face1(int i, int j) const { return &f1[3 * (i + (ni + 1) * (j - 1))]; }
+    const double* face2(int i, int j) const { return &f2[3 * ((i - 1) + ni * j)]; }
+    const double* face(int dir, int i, int j) const { return dir == 1 ? face1(i, j) : face2(i, j); }
+    double dlc(int i, int j, int d) const { return dl[2 * c(i, j) + (d - 1)]; }
+};
+
+struct Case {
+    std::vector<int> blocks;      // global ids, local order
+    std::vector<q2d_bc_rec> bc;
+    double time = 0.0, dtglobal = 0.0, time_from_call = 0.0;
+    long long iter = 0, iter_from_call = 0;
+    double res[4] = {0, 0, 0, 0};
+    double res0 = -1.0;
+    int todo = Q2D_TODO_CONTINUE;
+    int err = Q2D_OK, err_b = 0, err_i = 0, err_j = 0, err_stage = 0;
+    bool done = false;
+};
+
+}  // namespace
+
+struct q2d_oracle {
+    q2d_options opt;
+    Gas gas;
+    std::vector<Block> blk;
+    std::vector<Case> cases;
+    bool committed = false;
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------------------
+// Metrics (Lib_Metrics.f90)
+// ---------------------------------------------------------------------------------------
+struct V2 { double x, y; };
+
+// Compute_Metric_Tensor (Lib_Metrics.f90:125-189)
+int metric_tensor(V2 N1, V2 N2, V2 N3, V2 N4, double* M, double* dl, double* sur) {
+    double A[2][2];
+    A[0][0] = N4.x - N2.x + N3.x - N1.x;
+    A[0][1] = N4.y - N2.y + N3.y - N1.y;
+    A[1][0] = N4.x - N3.x + N2.x - N1.x;
+    A[1][1] = N4.y - N3.y + N2.y - N1.y;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) A[a][b] = 0.5 * A[a][b];
+    const double det = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+    if (std::fabs(det) == 0.0) return Q2D_ERR_BADARG;
+    M[0] = A[1][1] / det;     // cofactor(1,1)/det
+    M[1] = -A[1][0] / det;    // cofactor(1,2)/det
+    M[2] = -A[0][1] / det;    // cofactor(2,1)/det
+    M[3] = A[0][0] / det;     // cofactor(2,2)/det
+    for (int h = 0; h < 2; ++h) dl[h] = std::sqrt(A[h][0] * A[h][0] + A[h][1] * A[h][1]);
+    // tsurface(vx,vy,1,2,3,4): d1 = N4-N1, d2 = N3-N2
+    const double d1x = N4.x - N1.x, d1y = N4.y - N1.y;
+    const double d2x = N3.x - N2.x, d2y = N3.y - N2.y;
+    const double cross = d1x * d2y - d1y * d2x;
+    *sur = 0.5 * std::fabs(cross);
+    if (*sur <= 0.0) return Q2D_ERR_BADARG;
+    return Q2D_OK;
+}
+
+int metric_into(Block& B, int i, int j, V2 N1, V2 N2, V2 N3, V2 N4) {
+    const int k = B.c(i, j);
+    return metric_tensor(N1, N2, N3, N4, &B.M[4 * k], &B.dl[2 * k], &B.sur[k]);
+}
+
+V2 nodev(const Block& B, int i, int j) { return V2{B.nx_(i, j), B.ny_(i, j)}; }
+V2 quad_ex(V2 a, V2 b, V2 c) {   // 3a - 3b + c
+    return V2{3.0 * a.x - 3.0 * b.x + c.x, 3.0 * a.y - 3.0 * b.y + c.y};
+}
+V2 lin_ex(V2 a, V2 b) { return V2{2.0 * a.x - b.x, 2.0 * a.y - b.y}; }
+
+// Compute_Norm_Area (Lib_Metrics.f90:41-122)
+void norm_area(Block& B) {
+    const int im = B.ni, jm = B.nj;
+    auto sgn = [](double a) { return std::copysign(1.0, a); };
+    double d1x = B.nx_(1, 1) - B.nx_(1, 0), d1y = B.ny_(1, 1) - B.ny_(1, 0);
+    double snixx = d1y, sniyy = -d1x;
+    double ax = 0.5 * (B.nx_(1, 1) + B.nx_(1, 0)), ay = 0.5 * (B.ny_(1, 1) + B.ny_(1, 0));
+    double bx = 0.5 * (B.nx_(0, 1) + B.nx_(0, 0)), by = 0.5 * (B.ny_(0, 1) + B.ny_(0, 0));
+    double scal = (ax - bx) * snixx + (ay - by) * sniyy;
+    const double signi = sgn(scal);
+    d1x = B.nx_(0, 1) - B.nx_(1, 1);
+    d1y = B.ny_(0, 1) - B.ny_(1, 1);
+    double snjxx = d1y, snjyy = -d1x;
+    ax = 0.5 * (B.nx_(1, 1) + B.nx_(0, 1));
+    ay = 0.5 * (B.ny_(1, 1) + B.ny_(0, 1));
+    bx = 0.5 * (B.nx_(1, 0) + B.nx_(0, 0));
+    by = 0.5 * (B.ny_(1, 0) + B.ny_(0, 0));
+    scal = (ax - bx) * snjxx + (ay - by) * snjyy;
+    const double signj = sgn(scal);
+    B.f1.assign(3 * (im + 1) * jm, 0.0);
+    B.f2.assign(3 * im * (jm + 1), 0.0);
+    for (int j = 1; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+            const double dx = B.nx_(i, j) - B.nx_(i, j - 1), dy = B.ny_(i, j) - B.ny_(i, j - 1);
+            const double d3x = dy, d3y = -dx;
+            const double Ai = std::sqrt(d3x * d3x + d3y * d3y);
+            double* f = &B.f1[3 * (i + (im + 1) * (j - 1))];
+            f[0] = Ai == 0.0 ? 0.0 : d3x / Ai * signi;
+            f[1] = Ai == 0.0 ? 0.0 : d3y / Ai * signi;
+            f[2] = Ai;
+        }
+    for (int j = 0; j <= jm; ++j)
+        for (int i = 1; i <= im; ++i) {
+            const double dx = B.nx_(i - 1, j) - B.nx_(i, j), dy = B.ny_(i - 1, j) - B.ny_(i, j);
+            const double d3x = dy, d3y = -dx;
+            const double Aj = std::sqrt(d3x * d3x + d3y * d3y);
+            double* f = &B.f2[3 * ((i - 1) + im * j)];
+            f[0] = Aj == 0.0 ? 0.0 : d3x / Aj * signj;
+            f[1] = Aj == 0.0 ? 0.0 : d3y / Aj * signj;
+            f[2] = Aj;
+        }
+}
+
+// BC_Extrapolate_Metrics (Lib_Metrics.f90:285-395)
+int extrapolate_metrics(Block& B, int Im, int Jm, int Fm) {
+    V2 N1[2 * GC + 1], N2[2 * GC + 1], N3[2 * GC + 1], N4[2 * GC + 1];
+    auto at = [](V2* a, int g) -> V2& { return a[g + GC]; };
+    int e = Q2D_OK;
+    switch (Fm) {
+        case 1:
+            for (int g = 0; g <= GC; ++g) {
+                at(N1, g) = nodev(B, Im + g - 1, Jm - 1);
+                at(N2, g) = nodev(B, Im + g - 1, Jm);
+            }
+            for (int g = -1; g >= -GC; --g) {
+                at(N1, g) = quad_ex(at(N1, g + 1), at(N1, g + 2), at(N1, g + 3));
+                at(N2, g) = quad_ex(at(N2, g + 1), at(N2, g + 2), at(N2, g + 3));
+                e |= metric_into(B, Im + g, Jm, at(N1, g), at(N2, g), at(N1, g + 1), at(N2, g + 1));
+            }
+            break;
+        case 2:
+            for (int g = 0; g >= -GC; --g) {
+                at(N3, g) = nodev(B, Im + g, Jm - 1);
+                at(N4, g) = nodev(B, Im + g, Jm);
+            }
+            for (int g = 1; g <= GC; ++g) {
+                at(N3, g) = quad_ex(at(N3, g - 1), at(N3, g - 2), at(N3, g - 3));
+                at(N4, g) = quad_ex(at(N4, g - 1), at(N4, g - 2), at(N4, g - 3));
+                e |= metric_into(B, Im + g, Jm, at(N3, g - 1), at(N4, g - 1), at(N3, g), at(N4, g));
+            }
+            break;
+        case 3:
+            if (B.nj > 2) {
+                for (int g = 0; g <= GC; ++g) {
+                    at(N1, g) = nodev(B, Im - 1, Jm + g - 1);
+                    at(N3, g) = nodev(B, Im, Jm + g - 1);
+                }
+                for (int g = -1; g >= -GC; --g) {
+                    at(N1, g) = quad_ex(at(N1, g + 1), at(N1, g + 2), at(N1, g + 3));
+                    at(N3, g) = quad_ex(at(N3, g + 1), at(N3, g + 2), at(N3, g + 3));
+                    e |= metric_into(B, Im, Jm + g, at(N1, g), at(N1, g + 1), at(N3, g), at(N3, g + 1));
+                }
+            } else {
+                for (int g = 0; g <= 1; ++g) {
+                    at(N1, g) = nodev(B, Im - 1, Jm + g - 1);
+                    at(N3, g) = nodev(B, Im, Jm + g - 1);
+                }
+                for (int g = -1; g >= -GC; --g) {
+                    at(N1, g) = lin_ex(at(N1, g + 1), at(N1, g + 2));
+                    at(N3, g) = lin_ex(at(N3, g + 1), at(N3, g + 2));
+                    e |= metric_into(B, Im, Jm + g, at(N1, g), at(N1, g + 1), at(N3, g), at(N3, g + 1));
+                }
+            }
+            break;
+        case 4:
+            if (B.nj > 2) {
+                for (int g = 0; g >= -GC; --g) {
+                    at(N2, g) = nodev(B, Im - 1, Jm + g);
+                    at(N4, g) = nodev(B, Im, Jm + g);
+                }
+                for (int g = 1; g <= GC; ++g) {
+                    at(N2, g) = quad_ex(at(N2, g - 1), at(N2, g - 2), at(N2, g - 3));
+                    at(N4, g) = quad_ex(at(N4, g - 1), at(N4, g - 2), at(N4, g - 3));
+                    e |= metric_into(B, Im, Jm + g, at(N2, g - 1), at(N2, g), at(N4, g - 1), at(N4, g));
+                }
+            } else {
+                for (int g = 0; g >= -1; --g) {
+                    at(N2, g) = nodev(B, Im - 1, Jm + g);
+                    at(N4, g) = nodev(B, Im, Jm + g);
+                }
+                for (int g = 1; g <= GC; ++g) {
+                    at(N2, g) = lin_ex(at(N2, g - 1), at(N2, g - 2));
+                    at(N4, g) = lin_ex(at(N4, g - 1), at(N4, g - 2));
+                    e |= metric_into(B, Im, Jm + g, at(N2, g - 1), at(N2, g), at(N4, g - 1), at(N4, g));
+                }
+            }
+            break;
+    }
+    return e;
+}
+
+// BC_Symmetry_Metrics (Lib_Metrics.f90:398-441)
+void symmetry_metrics(Block& B, int Im, int Jm, int Fm) {
+    for (int g = 1; g <= GC; ++g) {
+        int di = 0, dj = 0, si = 0, sj = 0;
+        switch (Fm) {
+            case 1: di = Im - g; dj = Jm; si = Im + g - 1; sj = Jm; break;
+            case 2: di = Im + g; dj = Jm; si = Im - g + 1; sj = Jm; break;
+            case 3: di = Im; dj = Jm - g; si = Im; sj = Jm + g - 1; break;
+            case 4: di = Im; dj = Jm + g; si = Im; sj = Jm - g + 1; break;
+        }
+        const int kd = B.c(di, dj), ks = B.c(si, sj);
+        for (int q = 0; q < 4; ++q) B.M[4 * kd + q] = B.M[4 * ks + q];
+        for (int q = 0; q < 2; ++q) B.dl[2 * kd + q] = B.dl[2 * ks + q];
+        B.sur[kd] = B.sur[ks];
+    }
+}
+
+// BC_Connect_Metrics (Lib_Metrics.f90:444-553)
+int connect_metrics(Block& Bm, int Im, int Jm, int Fm, const Block& Bs, int Is, int Js, int Fs,
+                    int d11s, int d21s) {
+    static const int guides[5][2] = {{0, 0}, {0, 0}, {-1, 0}, {0, 0}, {0, -1}};
+    static const int guides2[5][2] = {{0, 0}, {1, 0}, {-2, 0}, {0, 1}, {0, -2}};
+    V2 N1[GC + 1], N2[GC + 1], N3[GC + 1], N4[GC + 1];
+    switch (Fm) {
+        case 1: N1[0] = nodev(Bm, Im - 1, Jm - 1); N2[0] = nodev(Bm, Im - 1, Jm); break;
+        case 2: N3[0] = nodev(Bm, Im, Jm - 1); N4[0] = nodev(Bm, Im, Jm); break;
+        case 3: N1[0] = nodev(Bm, Im - 1, Jm - 1); N3[0] = nodev(Bm, Im, Jm - 1); break;
+        case 4: N2[0] = nodev(Bm, Im - 1, Jm); N4[0] = nodev(Bm, Im, Jm); break;
+    }
+    int e = Q2D_OK;
+    for (int g = 1; g <= GC; ++g) {
+        const int Is1 = Is + (GC - g) * guides[Fs][0] + (g - 1) * guides2[Fs][0];
+        const int Js1 = Js + (GC - g) * guides[Fs][1] + (g - 1) * guides2[Fs][1];
+        int II, JJ, III, JJJ;
+        if (Fs <= 2) { II = Is1; JJ = (2 * Js1 + d11s + d21s) / 2; }
+        else { II = (2 * Is1 + d11s + d21s) / 2; JJ = Js1; }
+        if (II < 0 || II > Bs.ni || JJ < 0 || JJ > Bs.nj) return Q2D_ERR_BADARG;
+        const V2 a = nodev(Bs, II, JJ);
+        switch (Fm) { case 1: N2[g] = a; break; case 2: N4[g] = a; break;
+                      case 3: N3[g] = a; break; case 4: N4[g] = a; break; }
+        if (Fs <= 2) { III = II; JJJ = JJ - d11s; } else { III = II - d11s; JJJ = JJ; }
+        if (III < 0 || III > Bs.ni || JJJ < 0 || JJJ > Bs.nj) return Q2D_ERR_BADARG;
+        const V2 b = nodev(Bs, III, JJJ);
+        switch (Fm) { case 1: N1[g] = b; break; case 2: N3[g] = b; break;
+                      case 3: N1[g] = b; break; case 4: N2[g] = b; break; }
+        switch (Fm) {
+            case 1: e |= metric_into(Bm, Im - g, Jm, N1[g], N2[g], N1[g - 1], N2[g - 1]); break;
+            case 2: e |= metric_into(Bm, Im + g, Jm, N3[g - 1], N4[g - 1], N3[g], N4[g]); break;
+            case 3: e |= metric_into(Bm, Im, Jm - g, N1[g], N1[g - 1], N3[g], N3[g - 1]); break;
+            case 4: e |= metric_into(Bm, Im, Jm + g, N2[g - 1], N2[g], N4[g - 1], N4[g]); break;
+        }
+    }
+    return e;
+}
+
+// ---------------------------------------------------------------------------------------
+// Ghost cells (Lib_Ghost.f90:16-299)
+// ---------------------------------------------------------------------------------------
+void ghost_fill(q2d_oracle* o, Case& cs) {
+    for (const q2d_bc_rec& rec : cs.bc) {
+        Block& B = o->blk[cs.blocks[rec.b - 1]];
+        const int Im = rec.i, Jm = rec.j, Fm = rec.f;
+        switch (rec.type) {
+            case 101: {   // Ghost_Connection :143-160
+                const Block& S = o->blk[cs.blocks[rec.bs - 1]];
+                for (int g = 1; g <= GC; ++g) {
+                    const int Ig = Im - GUIDE[Fm][0] * g, Jg = Jm - GUIDE[Fm][1] * g;
+                    const double* src = S.pc(rec.is + GUIDE[rec.fs][0] * (g - 1),
+                                             rec.js + GUIDE[rec.fs][1] * (g - 1));
+                    std::memcpy(B.p(Ig, Jg), src, sizeof(double) * NPRIM);
+                }
+                break;
+            }
+            case 300: {   // Ghost_Symmetry :163-196
+                const int Ig = Im - GUIDE[Fm][0], Jg = Jm - GUIDE[Fm][1];
+                const double* n;
+                if (Fm <= 2) n = B.face1(Im - (Fm % 2), Jm);
+                else n = B.face2(Im, Jm - (Fm % 2));
+                const double* Pm = B.pc(Im, Jm);
+                double vx = Pm[1], vy = Pm[2];
+                const double udotn = vx * n[0] + vy * n[1];
+                vx = vx - 2.0 * udotn * n[0];
+                vy = vy - 2.0 * udotn * n[1];
+                double* Pg = B.p(Ig, Jg);
+                Pg[1] = vx;
+                Pg[2] = vy;
+                Pg[0] = Pm[0];
+                Pg[3] = Pm[3];
+                break;
+            }
+            case 0: case 401: case 405: case 406: {   // Ghost_ZG_Extrapolate :199-219
+                for (int g = 1; g <= GC; ++g) {
+                    const int Ig = Im - GUIDE[Fm][0] * g, Jg = Jm - GUIDE[Fm][1] * g;
+                    std::memcpy(B.p(Ig, Jg), B.pc(Im, Jm), sizeof(double) * NPRIM);
+                }
+                break;
+            }
+            default: {    // Ghost_Extrapolate :270-299 (400 and every other code)
+                const int si = -GUIDE[Fm][0], sj = -GUIDE[Fm][1];   // outward step
+                for (int g = 1; g <= GC; ++g) {
+                    double* dst = B.p(Im + si * g, Jm + sj * g);
+                    const double* a = B.pc(Im + si * (g - 1), Jm + sj * (g - 1));
+                    const double* b = B.pc(Im + si * (g - 2), Jm + sj * (g - 2));
+                    const double* c = B.pc(Im + si * (g - 3), Jm + sj * (g - 3));
+                    for (int v = 0; v < NPRIM; ++v) dst[v] = 3.0 * a[v] - 3.0 * b[v] + c[v];
+                }
+                break;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Face fluxes
+// ---------------------------------------------------------------------------------------
+struct FaceErr { bool bad = false; };
+
+// Reconstruction (Lib_Reconstruction.f90:10-29), elemental over the 4 primitives.
+inline void reconstruct(int lim, const double* prev, const double* loc, const double* next,
+                        const double* next2, double dl0, double dl1, double dl2, double dll,
+                        double dlr, double beta, double* pl, double* pr) {
+    for (int v = 0; v < NPRIM; ++v) {
+        const double s0 = (loc[v] - prev[v]) / dl0;
+        const double s1 = (next[v] - loc[v]) / dl1;
+        const double s2 = (next2[v] - next[v]) / dl2;
+        const double sl = rlimiter(lim, s1, s0);
+        const double sr = rlimiter(lim, s2, s1);
+        pl[v] = loc[v] + beta * sl * dll;
+        pr[v] = next[v] - beta * sr * dlr;
+    }
+}
+
+// Flux from two reconstructed states: Lib_Convective.f90:56-80 (also used by the connection
+// BC, Lib_BC_Fluxes_Connection.f90:97-130, which has the same body).
+inline bool face_flux_from_states(const q2d_oracle* o, const double* P1, const double* P4,
+                                  double nx, double ny, double int_l, double* flux) {
+    if (gas_state_bad(P1[0], P1[3]) || gas_state_bad(P4[0], P4[3])) return false;
+    const Gas& g = o->gas;
+    const double rotot1 = P1[0], rotot4 = P4[0];
+    const double a1 = f_ss(g, P1[3], rotot1);
+    const double a4 = f_ss(g, P4[3], rotot4);
+    const Flux4 F = riemann(o->opt.riemann, g, P1, a1, P4, a4, nx, ny);
+    const double su = std::copysign(0.5, F.r);
+    const double sp = 0.5 + su, sm = su - 0.5;
+    flux[0] = F.r * int_l * (sp * (P1[0] / rotot1) - sm * (P4[0] / rotot4));
+    flux[1] = F.u * int_l;
+    flux[2] = F.v * int_l;
+    flux[3] = F.e * int_l;
+    return true;
+}
+
+// Convective_Flux (Lib_Convective.f90:15-82): dl[-1..2], Prim[-1..2] along the direction.
+inline bool convective_flux(const q2d_oracle* o, const double* dlm1, const double* const* pr,
+                            double nx, double ny, double int_l, double* flux) {
+    const double l0 = 0.5 * (dlm1[0] + dlm1[1]);
+    const double l1 = 0.5 * (dlm1[1] + dlm1[2]);
+    const double l2 = 0.5 * (dlm1[2] + dlm1[3]);
+    const double lm = 0.5 * dlm1[1];
+    const double lp = 0.5 * dlm1[2];
+    double P1[4], P4[4];
+    reconstruct(o->opt.limiter, pr[0], pr[1], pr[2], pr[3], l0, l1, l2, lm, lp, 1.0, P1, P4);
+    return face_flux_from_states(o, P1, P4, nx, ny, int_l, flux);
+}
+
+// Fluxes_blk_omp_do (Mod_Fluxes.f90:97-234), Euler part. Returns false on a bad state.
+bool block_fluxes(const q2d_oracle* o, Block& B, int& eb_i, int& eb_j) {
+    const int n1 = B.ni, n2 = B.nj;
+    bool ok = true;
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= n2; ++j)
+        for (int i = 1; i <= n1; ++i) {
+            double* r = B.r(i, j);
+            r[0] = r[1] = r[2] = r[3] = 0.0;
+        }
+    int bi = 0, bj = 0;
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= n2; ++j) {
+        for (int i = 1; i <= n1 - 1; ++i) {
+            const double dl4[4] = {B.dlc(i - 1, j, 1), B.dlc(i, j, 1), B.dlc(i + 1, j, 1),
+                                   B.dlc(i + 2, j, 1)};
+            const double* pr[4] = {B.pc(i - 1, j), B.pc(i, j), B.pc(i + 1, j), B.pc(i + 2, j)};
+            const double* f = B.face1(i, j);
+            double fl[4];
+            if (!convective_flux(o, dl4, pr, f[0], f[1], f[2], fl)) {
+#pragma omp critical
+                { if (ok) { ok = false; bi = i; bj = j; } }
+                continue;
+            }
+            double* r0 = B.r(i, j);
+            double* r1 = B.r(i + 1, j);
+            for (int v = 0; v < 4; ++v) { r0[v] = r0[v] + fl[v]; r1[v] = r1[v] - fl[v]; }
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i <= n1; ++i) {
+        for (int j = 1; j <= n2 - 1; ++j) {
+            const double dl4[4] = {B.dlc(i, j - 1, 2), B.dlc(i, j, 2), B.dlc(i, j + 1, 2),
+                                   B.dlc(i, j + 2, 2)};
+            const double* pr[4] = {B.pc(i, j - 1), B.pc(i, j), B.pc(i, j + 1), B.pc(i, j + 2)};
+            const double* f = B.face2(i, j);
+            double fl[4];
+            if (!convective_flux(o, dl4, pr, f[0], f[1], f[2], fl)) {
+#pragma omp critical
+                { if (ok) { ok = false; bi = i; bj = j; } }
+                continue;
+            }
+            double* r0 = B.r(i, j);
+            double* r1 = B.r(i, j + 1);
+            for (int v = 0; v < 4; ++v) { r0[v] = r0[v] + fl[v]; r1[v] = r1[v] - fl[v]; }
+        }
+    }
+    if (!ok) { eb_i = bi; eb_j = bj; }
+    return ok;
+}
+
+// Face_Index (Lib_BC_Fluxes.f90:34-50)
+inline void face_index(int f, int ci, int cj, int& dir, int& fi, int& fj) {
+    if (f <= 2) { dir = 1; fi = ci - (f % 2); fj = cj; }
+    else { dir = 2; fi = ci; fj = cj - (f % 2); }
+}
+
+// BC_Symmetry_Eul (Lib_BC_Fluxes_Symmetry.f90:28-124), Un_wall = 0.
+void bc_symmetry(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm) {
+    const int modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm;
+    const int Int_i = Im + GUIDE[Fm][0], Int_j = Jm + GUIDE[Fm][1];
+    int dir, Fi, Fj;
+    face_index(Fm, Im, Jm, dir, Fi, Fj);
+    const double* fc = B.face(dir, Fi, Fj);
+    const double n0 = fc[0], n1 = fc[1], int_l = fc[2];
+    const double Bound_Dl = 0.5 * B.dlc(Im, Jm, dir);
+    const double Int_Dl = 0.5 * B.dlc(Int_i, Int_j, dir);
+    const double* Bp = B.pc(Im, Jm);
+    const double* Ip = B.pc(Int_i, Int_j);
+    double Un = Bp[1] * n0 + Bp[2] * n1;
+    double G[4] = {Bp[0], Bp[1], Bp[2], Bp[3]};
+    G[1] = G[1] - 2.0 * Un * n0;
+    G[2] = G[2] - 2.0 * Un * n1;
+    double P1[4], P3[4];
+    for (int v = 0; v < 4; ++v) {
+        P1[v] = modfm * G[v] + modfm1 * Ip[v];
+        P3[v] = modfm * Ip[v] + modfm1 * G[v];
+    }
+    const double Dist12 = 2.0 * Bound_Dl * modfm + (Bound_Dl + Int_Dl) * modfm1;
+    const double Dist23 = (Bound_Dl + Int_Dl) * modfm + 2.0 * Bound_Dl * modfm1;
+    double Face[4];
+    const double Dist = Bound_Dl * modfm2;
+    for (int v = 0; v < 4; ++v) {
+        const double s32 = (P3[v] - Bp[v]) / Dist23;
+        const double s21 = (Bp[v] - P1[v]) / Dist12;
+        const double s = rlimiter(o->opt.limiter, s32, s21);
+        Face[v] = Bp[v] + s * Dist;
+    }
+    const Gas& g = o->gas;
+    const double rotot = Face[0];
+    const double Sound = f_ss(g, Face[3], rotot);
+    Un = Face[1] * n0 + Face[2] * n1;
+    const double vtx = Face[1] - Un * n0, vty = Face[2] - Un * n1;
+    const double Un1 = Un * modfm2;
+    const double U1[2] = {Un1 * n0 + vtx, Un1 * n1 + vty};
+    const double U4[2] = {-Un1 * n0 + vtx, -Un1 * n1 + vty};
+    const double L[4] = {Face[0], U1[0], U1[1], Face[3]};
+    const double R[4] = {Face[0], U4[0], U4[1], Face[3]};
+    const Flux4 F = riemann(o->opt.riemann, g, L, Sound, R, Sound, n0, n1);
+    double* r = B.r(Im, Jm);
+    r[1] = r[1] + modfm2 * (F.u * int_l);
+    r[2] = r[2] + modfm2 * (F.v * int_l);
+}
+
+// BC_Extrapolation (Lib_BC_Fluxes_Extrapolation.f90:18-49)
+void bc_extrapolation(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm) {
+    int dir, Fi, Fj;
+    face_index(Fm, Im, Jm, dir, Fi, Fj);
+    const double* fc = B.face(dir, Fi, Fj);
+    const double n0 = fc[0], n1 = fc[1], int_l = fc[2];
+    const double* P = B.pc(Im, Jm);
+    const double Un = P[1] * n0 + P[2] * n1;
+    double F[4];
+    F[0] = P[0] * Un * int_l;
+    const double Fmass = F[0];
+    F[1] = Fmass * P[1] + P[3] * int_l * n0;
+    F[2] = Fmass * P[2] + P[3] * int_l * n1;
+    F[3] = Fmass * H0(o->gas, P[3], P[0], std::sqrt(P[1] * P[1] + P[2] * P[2]));
+    const double sgn = 1 - 2 * (Fm % 2);
+    double* r = B.r(Im, Jm);
+    for (int v = 0; v < 4; ++v) r[v] = r[v] + sgn * F[v];
+}
+
+struct InflowGeom {
+    int modfm, modfm1, modfm2;
+    double n0, n1, int_l, t0, t1, BC_Sign, Un, rho, Sound, Gamma, Riem;
+    const double* Bp;
+    const double* Ip;
+};
+
+// Setup_Inflow_Geometry (Lib_BC_Fluxes_Inflow.f90:489-541)
+InflowGeom inflow_geometry(const q2d_oracle* o, const Block& B, int Im, int Jm, int Fm) {
+    InflowGeom G;
+    G.modfm = Fm % 2; G.modfm1 = 1 - G.modfm; G.modfm2 = 1 - 2 * G.modfm;
+    const int Int_i = Im + GUIDE[Fm][0], Int_j = Jm + GUIDE[Fm][1];
+    int dir, Fi, Fj;
+    face_index(Fm, Im, Jm, dir, Fi, Fj);
+    G.Bp = B.pc(Im, Jm);
+    G.Ip = B.pc(Int_i, Int_j);
+    const double* fc = B.face(dir, Fi, Fj);
+    G.n0 = fc[0]; G.n1 = fc[1]; G.int_l = fc[2];
+    double tx, ty;
+    if (Fm <= 2) { tx = B.nx_(Fi, Fj) - B.nx_(Fi, Fj - 1); ty = B.ny_(Fi, Fj) - B.ny_(Fi, Fj - 1); }
+    else { tx = B.nx_(Fi, Fj) - B.nx_(Fi - 1, Fj); ty = B.ny_(Fi, Fj) - B.ny_(Fi - 1, Fj); }
+    const double tmod = std::sqrt(tx * tx + ty * ty);
+    G.t0 = tx / tmod; G.t1 = ty / tmod;
+    G.BC_Sign = (double)G.modfm2;
+    G.Un = G.Bp[1] * G.n0 + G.Bp[2] * G.n1;
+    G.rho = G.Bp[0];
+    G.Sound = f_ss(o->gas, G.Bp[3], G.rho);
+    G.Gamma = o->gas.gamma;
+    G.Riem = G.Sound + G.BC_Sign * 0.5 * (G.Gamma - 1.0) * G.Un;
+    return G;
+}
+
+// Compute_Inflow_Direction (Lib_BC_Fluxes_Inflow.f90:548-563)
+inline double inflow_direction(double n0, double n1, double alpha_in) {
+    if (alpha_in >= 0.5 * DBL_MAX) return std::atan(n1 / (n0 + 1e-20));
+    return alpha_in;
+}
+
+// BC_Inlet_StagnCond + Stagn_Inflow (Lib_BC_Fluxes_Inflow.f90:64-120, 412-483).
+// Returns false when the flow leaves the domain (caller falls back to symmetry).
+bool bc_stagnation(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm, const q2d_bc_rec& rec) {
+    const InflowGeom G = inflow_geometry(o, B, Im, Jm, Fm);
+    if (G.BC_Sign * G.Un >= 0.0) return false;
+    const double alpha = inflow_direction(G.n0, G.n1, rec.alpha);
+    const double Gamma = G.Gamma, Rg = o->gas.R;
+    const double XA = G.n1 - G.n0 * std::tan(alpha);
+    const double XB = G.t1 - G.t0 * std::tan(alpha);
+    const double E1 = -XA / XB;
+    double Discr = -1.0, p0try = rec.p0;
+    int iter = 0;
+    double Sound0 = 0, Coef_D = 0, YA = 0, YB = 0;
+    const double p = G.Bp[3];
+    while (Discr < 0.0) {
+        ++iter;
+        Sound0 = std::sqrt(Gamma * Rg * rec.T0);
+        Coef_D = (1.0 + E1 * E1) * (Gamma - 1.0) / 2.0;
+        double Coef_C = std::pow(p0try / p, (Gamma - 1.0) / Gamma);
+        const double ss = G.Sound / Sound0;
+        Coef_C = Coef_C * (ss * ss);
+        const double gh = (Gamma - 1.0) / 2.0;
+        YA = gh * gh + Coef_C * Coef_D;
+        YB = G.BC_Sign * G.Riem * ((Gamma - 1.0) / 2.0);
+        const double YC = G.Riem * G.Riem - Coef_C * (Sound0 * Sound0);
+        Discr = YB * YB - YA * YC;
+        if (Discr < 0.0 && std::fabs(Discr) < 1e-2) Discr = 0.0;
+        if (Discr < 0.0 && std::fabs(Discr) > 1e-2) p0try = rec.rel_fac * p0try + (1 - rec.rel_fac) * p;
+        if (iter > 1000) { Discr = 0.0; break; }
+    }
+    const double Un_Sign = std::copysign(1.0, G.Un);
+    const double Un3 = (YB + Un_Sign * std::sqrt(Discr)) / YA;
+    const double Sound3 = std::sqrt(Sound0 * Sound0 - Coef_D * (Un3 * Un3));
+    const double p3 = p0try * std::pow(Sound3 / Sound0, 2.0 * Gamma / (Gamma - 1.0));
+    const double Ut3 = Un3 * E1;
+    const double Face_rho = Gamma * p3 / (Sound3 * Sound3);
+    const double Face_r1 = 1.0 * Face_rho;
+    const double fu = Un3 * G.n0 + Ut3 * G.t0;
+    const double fv = Un3 * G.n1 + Ut3 * G.t1;
+    const double Face_T = p3 / (Rg * Face_rho);
+    const double Face_H = 0.0 + Face_r1 / Face_rho * (o->gas.cp * Face_T);
+    double F[4];
+    F[0] = Face_r1 * Un3 * G.int_l;
+    const double Fmass = Face_rho * Un3 * G.int_l;
+    F[1] = Fmass * fu + p3 * G.int_l * G.n0;
+    F[2] = Fmass * fv + p3 * G.int_l * G.n1;
+    F[3] = Fmass * (0.5 * (fu * fu + fv * fv) + Face_H);
+    double* r = B.r(Im, Jm);
+    for (int v = 0; v < 4; ++v) r[v] = r[v] + G.modfm2 * F[v];
+    return true;
+}
+
+// BC_Inlet_Supersonic_Static + Supersonic_Inflow (Lib_BC_Fluxes_Inflow.f90:272-311, 321-403)
+bool bc_supersonic(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm, const q2d_bc_rec& rec) {
+    const InflowGeom G = inflow_geometry(o, B, Im, Jm, Fm);
+    if (G.BC_Sign * G.Un >= 0.0) return false;
+    const Gas& g = o->gas;
+    const double* P2 = G.Bp;
+    const double flow_Sound = f_ss(g, P2[3], P2[0]);
+    const double flow_Mach = std::sqrt(P2[1] * P2[1] + P2[2] * P2[2]) / flow_Sound;
+    const double Mloc = rec.rel_fac * rec.mach + (1 - rec.rel_fac) * flow_Mach;
+    const double ploc = rec.rel_fac * rec.pamb + (1 - rec.rel_fac) * P2[3];
+    const double alpha = inflow_direction(G.n0, G.n1, rec.alpha);
+    double Sup[4];
+    Sup[3] = ploc;
+    const double Sup_rho = Sup[3] / (g.R * rec.T0);
+    Sup[0] = Sup_rho * 1.0;
+    const double Sup_Sound = f_ss(g, Sup[3], Sup_rho);
+    Sup[1] = Mloc * Sup_Sound * std::cos(alpha);
+    Sup[2] = Mloc * Sup_Sound * std::sin(alpha);
+    double P1[4], P3[4], Face[4];
+    for (int v = 0; v < 4; ++v) {
+        P1[v] = G.modfm * Sup[v] + G.modfm1 * G.Ip[v];
+        P3[v] = G.modfm * G.Ip[v] + G.modfm1 * Sup[v];
+    }
+    for (int v = 0; v < 4; ++v) {
+        const double d32 = P3[v] - P2[v], d21 = P2[v] - P1[v];
+        const double s = rlimiter(o->opt.limiter, d32, d21);
+        Face[v] = P2[v] + 0.5 * s * G.modfm2;
+    }
+    double PL[4], PR[4];
+    for (int v = 0; v < 4; ++v) {
+        PL[v] = G.modfm * Sup[v] + G.modfm1 * Face[v];
+        PR[v] = G.modfm * Face[v] + G.modfm1 * Sup[v];
+    }
+    const double aL = f_ss(g, PL[3], PL[0]);
+    const double aR = f_ss(g, PR[3], PR[0]);
+    const Flux4 F = riemann(o->opt.riemann, g, PL, aL, PR, aR, G.n0, G.n1);
+    const double su = std::copysign(1.0, F.r);
+    const double SelL = (1.0 + su) / 2.0, SelR = (su - 1.0) / 2.0;
+    const double Fmass = F.r * G.int_l;
+    double Fl[4];
+    Fl[0] = Fmass * (SelL * PL[0] / PL[0] - SelR * PR[0] / PR[0]);
+    Fl[1] = F.u * G.int_l;
+    Fl[2] = F.v * G.int_l;
+    Fl[3] = F.e * G.int_l;
+    double* r = B.r(Im, Jm);
+    for (int v = 0; v < 4; ++v) r[v] = r[v] + G.modfm2 * Fl[v];
+    return true;
+}
+
+// BC_Outflow + Outflow (Lib_BC_Fluxes_Outflow.f90:36-165)
+bool bc_outflow(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm, const q2d_bc_rec& rec) {
+    const int modfm = Fm % 2, modfm2 = 1 - 2 * modfm;
+    int dir, Fi, Fj;
+    face_index(Fm, Im, Jm, dir, Fi, Fj);
+    const double* Bp = B.pc(Im, Jm);
+    const double* fc = B.face(dir, Fi, Fj);
+    const double n0 = fc[0], n1 = fc[1], int_l = fc[2];
+    const double BC_Sign = (double)modfm2;
+    const double Un = Bp[1] * n0 + Bp[2] * n1;
+    if (BC_Sign * Un < 0.0) return false;
+    const Gas& g = o->gas;
+    const double rho = Bp[0];
+    const double Sound = f_ss(g, Bp[3], rho);
+    const double Gamma = g.gamma;
+    const double Riem = Sound + BC_Sign * 0.5 * (Gamma - 1.0) * Un;
+    const double vtx = Bp[1] - Un * n0, vty = Bp[2] - Un * n1;
+    const double Mach_N = std::fabs(Un / Sound);
+    double Face[4], Face_Un, Face_rho;
+    if (Mach_N < 1.0 && rec.pamb > 0.0) {
+        double p_exit = rec.pamb;
+        const double delta = 0.5 * (Gamma - 1.0);
+        const double den = 1.0 / std::pow(1 + delta, Gamma / (Gamma - 1.0));
+        const double pstar = Bp[3] * den * std::pow(1 + delta * (Mach_N * Mach_N), Gamma / (Gamma - 1.0));
+        if (pstar >= p_exit) p_exit = pstar;
+        const double Isen = (Gamma - 1.0) / (2.0 * Gamma);
+        Face[3] = p_exit * rec.rel_fac + Bp[3] * (1.0 - rec.rel_fac);
+        const double Face_Sound = Sound * std::pow(Face[3] / Bp[3], Isen);
+        Face_Un = (Riem - Face_Sound) / (BC_Sign * 0.5 * (Gamma - 1.0));
+        Face_rho = Gamma * Face[3] / (Face_Sound * Face_Sound);
+        Face[0] = Bp[0] / rho * Face_rho;
+        Face[1] = vtx + Face_Un * n0;
+        Face[2] = vty + Face_Un * n1;
+    } else {
+        for (int v = 0; v < 4; ++v) Face[v] = Bp[v];
+        Face_Un = Un;
+        Face_rho = rho;
+    }
+    const double Face_T = Face[3] / (g.R * Face_rho);
+    const double Face_H = 0.0 + Face[0] / Face_rho * (g.cp * Face_T);
+    double F[4];
+    F[0] = Face[0] * int_l * Face_Un;
+    const double mdot = Face_rho * int_l * Face_Un;
+    F[1] = Face[1] * mdot + Face[3] * int_l * n0;
+    F[2] = Face[2] * mdot + Face[3] * int_l * n1;
+    F[3] = mdot * (0.5 * (Face[1] * Face[1] + Face[2] * Face[2]) + Face_H);
+    double* r = B.r(Im, Jm);
+    for (int v = 0; v < 4; ++v) r[v] = r[v] + modfm2 * F[v];
+    return true;
+}
+
+// BC_Connection_Eul (Lib_BC_Fluxes_Connection.f90:24-133)
+bool bc_connection(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm) {
+    const int modfm = Fm % 2, modfm1 = 1 - modfm, modfm2 = 1 - 2 * modfm;
+    int dir, Fi, Fj;
+    face_index(Fm, Im, Jm, dir, Fi, Fj);
+    const int gx = GUIDE[Fm][0], gy = GUIDE[Fm][1];
+    const int I1 = modfm * (Im - gx * GC) + modfm1 * (Im + gx);
+    const int J1 = modfm * (Jm - gy * GC) + modfm1 * (Jm + gy);
+    const int I2 = modfm1 * Im + modfm * (Im - gx);
+    const int J2 = modfm1 * Jm + modfm * (Jm - gy);
+    const int I3 = modfm1 * (Im - gx) + modfm * Im;
+    const int J3 = modfm1 * (Jm - gy) + modfm * Jm;
+    const int I4 = modfm1 * (Im - gx * GC) + modfm * (Im + gx);
+    const int J4 = modfm1 * (Jm - gy * GC) + modfm * (Jm + gy);
+    const double* fc = B.face(dir, Fi, Fj);
+    const double Dl1 = B.dlc(I1, J1, dir) * 0.5;
+    const double Dl2 = B.dlc(I2, J2, dir) * 0.5;
+    const double Dl3 = B.dlc(I3, J3, dir) * 0.5;
+    const double Dl4 = B.dlc(I4, J4, dir) * 0.5;
+    const double Dist23 = Dl2 + Dl3, Dist12 = Dl1 + Dl2, Dist34 = Dl3 + Dl4;
+    double PL[4], PR[4];
+    reconstruct(o->opt.limiter, B.pc(I1, J1), B.pc(I2, J2), B.pc(I3, J3), B.pc(I4, J4), Dist12,
+                Dist23, Dist34, Dl2, Dl3, 1.0, PL, PR);
+    double F[4];
+    if (!face_flux_from_states(o, PL, PR, fc[0], fc[1], fc[2], F)) return false;
+    double* r = B.r(Im, Jm);
+    for (int v = 0; v < 4; ++v) r[v] = r[v] + F[v] * modfm2;
+    return true;
+}
+
+// BC_Fluxes (Mod_BC_Fluxes.f90:49-271), record order.
+bool bc_fluxes(q2d_oracle* o, Case& cs, int& eb, int& ei, int& ej) {
+    for (const q2d_bc_rec& rec : cs.bc) {
+        Block& B = o->blk[cs.blocks[rec.b - 1]];
+        const int Im = rec.i, Jm = rec.j, Fm = rec.f;
+        switch (rec.type) {
+            case 101:
+                if (!bc_connection(o, B, Im, Jm, Fm)) { eb = rec.b; ei = Im; ej = Jm; return false; }
+                break;
+            case 300: bc_symmetry(o, B, Im, Jm, Fm); break;
+            case 400: bc_extrapolation(o, B, Im, Jm, Fm); break;
+            case 401: if (!bc_stagnation(o, B, Im, Jm, Fm, rec)) bc_symmetry(o, B, Im, Jm, Fm); break;
+            case 405: if (!bc_supersonic(o, B, Im, Jm, Fm, rec)) bc_symmetry(o, B, Im, Jm, Fm); break;
+            case 406: if (!bc_outflow(o, B, Im, Jm, Fm, rec)) bc_symmetry(o, B, Im, Jm, Fm); break;
+            default: break;   // type 0: no flux
+        }
+    }
+    return true;
+}
+
+// Source_Axi_Eul_Blk (Lib_Source_Axisymmetry.f90:40-78) and
+// Source_Area_Eul_Blk (Lib_Source_Areavariation.f90:104-144)
+void sources(const q2d_oracle* o, Block& B) {
+    const Gas& g = o->gas;
+    const int src = o->opt.source;
+    if (src == Q2D_SRC_NONE) return;
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= B.nj; ++j)
+        for (int i = 1; i <= B.ni; ++i) {
+            const double* P = B.pc(i, j);
+            const double rho = P[0];
+            const double mod_v = std::sqrt(P[1] * P[1] + P[2] * P[2]);
+            const int k = (i - 1) + B.ni * (j - 1);
+            double S[4];
+            if (src == Q2D_SRC_AXI) {
+                const double invr = B.inv_r[k];
+                S[0] = -P[0] * P[2] * invr;
+                S[1] = -rho * P[1] * P[2] * invr;
+                S[2] = -rho * P[2] * P[2] * invr;
+                S[3] = -(rho * E0(g, P[3], P[0], mod_v) + P[3]) * P[2] * invr;
+            } else {
+                const double Gx = B.Gx[k], Gy = B.Gy[k];
+                const double VG = P[1] * Gx + P[2] * Gy;
+                S[0] = P[0] * VG;
+                S[1] = rho * P[1] * VG;
+                S[2] = rho * P[2] * VG;
+                S[3] = (rho * E0(g, P[3], P[0], mod_v) + P[3]) * VG;
+            }
+            double* r = B.r(i, j);
+            const double s = B.sur[B.c(i, j)];
+            for (int v = 0; v < 4; ++v) r[v] = r[v] - S[v] * s;
+        }
+}
+
+// RKcoeff (Lib_RK.f90:8-11)
+inline double rk_coeff(int n_rk, int irk) {
+    static const double C[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.5, 0.0}, {1.0, 0.25, 2.0 / 3.0}};
+    return C[n_rk - 1][irk - 1];
+}
+
+// Newstate_Conservative / Compute_Cons_NoIRS + Check_And_Fix_State
+// (Lib_Newstate.f90:14-161, 316-350)
+bool newstate(const q2d_oracle* o, Block& B, int irk, int& ei, int& ej) {
+    const Gas& g = o->gas;
+    const double c = rk_coeff(o->opt.n_rk, irk);
+    const double strangcoeff = 1.0;
+    bool ok = true;
+    int bi = 0, bj = 0;
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= B.nj; ++j)
+        for (int i = 1; i <= B.ni; ++i) {
+            double* prim = B.p(i, j);
+            const double* primold = &B.PO[4 * B.c(i, j)];
+            double* res = B.r(i, j);
+            const double surface = B.sur[B.c(i, j)];
+            const double dt = B.dtlocal[(i - 1) + B.ni * (j - 1)];
+            for (int v = 0; v < 4; ++v) res[v] = -res[v] / surface * dt * strangcoeff;
+            double consold[4], cons[4];
+            prim2cons(g, primold, consold);
+            prim2cons(g, prim, cons);
+            for (int v = 0; v < 4; ++v) cons[v] = consold[v] + (cons[v] - consold[v] + res[v]) * c;
+            cons2prim(g, cons, prim);
+            bool bad = false;
+            for (int v = 0; v < 4; ++v) bad = bad || std::isnan(prim[v]);
+            if (bad || prim[3] < 0.0) {
+#pragma omp critical
+                { if (ok) { ok = false; bi = i; bj = j; } }
+            }
+            if (prim[0] < 1e-20) prim[0] = 1e-20;
+        }
+    if (!ok) { ei = bi; ej = bj; }
+    return ok;
+}
+
+// Compute_dt (Mod_dt.f90:10-106), Euler model (model == 0).
+void compute_dt(q2d_oracle* o, Case& cs, int ndir) {
+    const Gas& g = o->gas;
+    double dtglobal = cs.dtglobal;
+    for (int bid : cs.blocks) {
+        Block& B = o->blk[bid];
+        double dmin = dtglobal;
+#pragma omp parallel for schedule(static) reduction(min : dmin)
+        for (int j = 1; j <= B.nj; ++j)
+            for (int i = 1; i <= B.ni; ++i) {
+                const double* P = B.pc(i, j);
+                const double* M = &B.M[4 * B.c(i, j)];
+                const double Sound = f_ss(g, P[3], P[0]);
+                double dtmin = 1e8;
+                for (int d = 1; d <= ndir; ++d) {
+                    const double m0 = M[2 * (d - 1)], m1 = M[2 * (d - 1) + 1];   // M(d,:)
+                    const double nrm = std::sqrt(m0 * m0 + m1 * m1);
+                    const double v0 = m0 / nrm, v1 = m1 / nrm;
+                    const double vel_ = std::fabs(P[1] * v0 + P[2] * v1);
+                    const double lambda = vel_ + Sound;
+                    const double dt = B.dlc(i, j, d) / lambda * o->opt.cfl;
+                    dtmin = fmin_(dt, dtmin);
+                }
+                double dtcell = dtmin;
+                if (cs.iter < o->opt.rampa_iter) dtcell = dtcell * (double)cs.iter / (double)o->opt.rampa_iter;
+                B.dtlocal[(i - 1) + B.ni * (j - 1)] = dtcell;
+                dmin = fmin_(dtcell, dmin);
+            }
+        dtglobal = dmin;
+    }
+    cs.dtglobal = dtglobal;
+}
+
+// Compute_Residual (Mod_Diagnostic.f90:438-469): sum of squares in (j, i) order.
+void compute_residual(q2d_oracle* o, Case& cs, double* total) {
+    for (int bid : cs.blocks) {
+        Block& B = o->blk[bid];
+        std::vector<double> rows(4 * (size_t)B.nj, 0.0);
+#pragma omp parallel for schedule(static)
+        for (int j = 1; j <= B.nj; ++j) {
+            double acc[4] = {0, 0, 0, 0};
+            for (int i = 1; i <= B.ni; ++i) {
+                const double* nw = B.pc(i, j);
+                const double* od = &B.PO[4 * B.c(i, j)];
+                for (int v = 0; v < 4; ++v) {
+                    const double rn = std::fabs(nw[v] - od[v]);
+                    acc[v] = acc[v] + rn * rn;
+                }
+            }
+            for (int v = 0; v < 4; ++v) rows[4 * (j - 1) + v] = acc[v];
+        }
+        for (int j = 0; j < B.nj; ++j)
+            for (int v = 0; v < 4; ++v) total[v] = total[v] + rows[4 * j + v];
+    }
+}
+
+// Explicit_Step (Mod_Explicit.f90:10-174) for one case.
+void explicit_step(q2d_oracle* o, Case& cs) {
+    const q2d_options& op = o->opt;
+    cs.iter += 1;
+    cs.iter_from_call += 1;
+    const int ndir = (o->blk[cs.blocks[0]].nj == 1) ? 1 : 2;   // Check_Mesh_Type
+    cs.dtglobal = 1e5;
+    compute_dt(o, cs, ndir);
+    if (op.time_accurate) {
+        for (int bid : cs.blocks) {   // Set_Global_dt
+            Block& B = o->blk[bid];
+            std::fill(B.dtlocal.begin(), B.dtlocal.end(), cs.dtglobal);
+        }
+        cs.time = cs.time + cs.dtglobal;
+    }
+    for (int bid : cs.blocks) {   // Copy_State
+        Block& B = o->blk[bid];
+        for (int j = 1; j <= B.nj; ++j)
+            for (int i = 1; i <= B.ni; ++i)
+                std::memcpy(&B.PO[4 * B.c(i, j)], B.pc(i, j), sizeof(double) * 4);
+    }
+    for (int irk = 1; irk <= op.n_rk; ++irk) {
+        ghost_fill(o, cs);
+        for (size_t lb = 0; lb < cs.blocks.size(); ++lb) {
+            int ei = 0, ej = 0;
+            if (!block_fluxes(o, o->blk[cs.blocks[lb]], ei, ej)) {
+                cs.err = Q2D_ERR_NONPHYSICAL; cs.err_b = (int)lb + 1; cs.err_i = ei; cs.err_j = ej;
+                cs.err_stage = irk; cs.done = true; return;
+            }
+        }
+        int eb = 0, ei = 0, ej = 0;
+        if (!bc_fluxes(o, cs, eb, ei, ej)) {
+            cs.err = Q2D_ERR_NONPHYSICAL; cs.err_b = eb; cs.err_i = ei; cs.err_j = ej;
+            cs.err_stage = irk; cs.done = true; return;
+        }
+        for (int bid : cs.blocks) sources(o, o->blk[bid]);
+        for (size_t lb = 0; lb < cs.blocks.size(); ++lb) {
+            if (!newstate(o, o->blk[cs.blocks[lb]], irk, ei, ej)) {
+                cs.err = Q2D_ERR_NAN; cs.err_b = (int)lb + 1; cs.err_i = ei; cs.err_j = ej;
+                cs.err_stage = irk; cs.done = true; return;
+            }
+        }
+    }
+    if (cs.iter_from_call == 1 || (cs.iter % op.res_diter) == 0) {
+        double tot[4] = {0, 0, 0, 0};
+        compute_residual(o, cs, tot);
+        for (int v = 0; v < 4; ++v) cs.res[v] = std::sqrt(tot[v]);
+        if (cs.res0 < 0.0) cs.res0 = cs.res[0];
+    }
+    const double thr = op.res_relative ? op.res_threshold * cs.res0 : op.res_threshold;
+    const bool endsim = (cs.iter_from_call >= op.itermax) || (cs.res[0] <= thr) ||
+                        (cs.time >= op.time_threshold);
+    const bool iosim = ((cs.iter % op.sol_diter) == 0) || (cs.time >= cs.time_from_call + op.sol_dtime);
+    if (endsim) { cs.todo = Q2D_TODO_END; cs.done = true; }
+    else if (iosim) cs.todo = Q2D_TODO_IO;
+    else cs.todo = Q2D_TODO_CONTINUE;
+}
+
+void fill_info(const Case& cs, q2d_step_info* out) {
+    out->dtglobal = cs.dtglobal;
+    out->time = cs.time;
+    out->iter = cs.iter;
+    for (int v = 0; v < 4; ++v) out->residual[v] = cs.res[v];
+    out->residual0 = cs.res0;
+    out->todo = cs.todo;
+    out->err = cs.err;
+    out->err_b = cs.err_b; out->err_i = cs.err_i; out->err_j = cs.err_j; out->err_stage = cs.err_stage;
+}
+
+int commit(q2d_oracle* o) {
+    if (o->committed) return Q2D_OK;
+    for (Block& B : o->blk) {
+        const size_t ng = (size_t)(B.ni + 4) * (B.nj + 4);
+        B.M.assign(4 * ng, 0.0);
+        B.dl.assign(2 * ng, 0.0);
+        B.sur.assign(ng, 0.0);
+        B.R.assign(4 * ng, 0.0);
+        B.PO.assign(4 * ng, 0.0);
+        B.dtlocal.assign((size_t)B.ni * B.nj, 0.0);
+        for (int j = 1; j <= B.nj; ++j)          // Setup_Metrics interior (Mod_Metrics.f90:41-56)
+            for (int i = 1; i <= B.ni; ++i) {
+                const int e = metric_into(B, i, j, nodev(B, i - 1, j - 1), nodev(B, i - 1, j),
+                                          nodev(B, i, j - 1), nodev(B, i, j));
+                if (e) return e;
+            }
+        norm_area(B);
+        const size_t n = (size_t)B.ni * B.nj;
+        if (o->opt.source == Q2D_SRC_AXI) {      // Precompute_Axisymmetric_Geometry :19-37
+            B.inv_r.assign(n, 0.0);
+            for (int j = 1; j <= B.nj; ++j)
+                for (int i = 1; i <= B.ni; ++i) {
+                    const double r_ave = 0.25 * (B.ny_(i, j) + B.ny_(i - 1, j) + B.ny_(i, j - 1) +
+                                                 B.ny_(i - 1, j - 1));
+                    B.inv_r[(i - 1) + B.ni * (j - 1)] = 1.0 / fmax_(r_ave, 1e-12);
+                }
+        }
+        if (o->opt.source == Q2D_SRC_AREA) {     // Precompute_Area_Geometry :26-50
+            B.Gx.assign(n, 0.0);
+            B.Gy.assign(n, 0.0);
+            if (!B.area.empty()) {
+                auto A = [&](int i, int j) { return B.area[i + (B.ni + 1) * j]; };
+                for (int j = 1; j <= B.nj; ++j)
+                    for (int i = 1; i <= B.ni; ++i) {
+                        const double dAij0 = 0.5 * ((A(i, j) - A(i - 1, j)) + (A(i, j - 1) - A(i - 1, j - 1)));
+                        const double dAij1 = 0.5 * ((A(i, j) - A(i, j - 1)) + (A(i - 1, j) - A(i - 1, j - 1)));
+                        const double* M = &B.M[4 * B.c(i, j)];
+                        const double dA0 = dAij0 * M[0] + dAij1 * M[2];
+                        const double dA1 = dAij0 * M[1] + dAij1 * M[3];
+                        const double Ac = 0.25 * (A(i, j) + A(i - 1, j) + A(i, j - 1) + A(i - 1, j - 1));
+                        B.Gx[(i - 1) + B.ni * (j - 1)] = -dA0 / fmax_(Ac, 1e-12);
+                        B.Gy[(i - 1) + B.ni * (j - 1)] = -dA1 / fmax_(Ac, 1e-12);
+                    }
+            }
+        }
+    }
+    for (Case& cs : o->cases) {                   // ghost metrics (Mod_Metrics.f90:97-146)
+        for (const q2d_bc_rec& rec : cs.bc) {
+            Block& B = o->blk[cs.blocks[rec.b - 1]];
+            int e = Q2D_OK;
+            if (rec.type == 101) {
+                const Block& S = o->blk[cs.blocks[rec.bs - 1]];
+                e = connect_metrics(B, rec.i, rec.j, rec.f, S, rec.is, rec.js, rec.fs, rec.d11, rec.d21);
+            } else if (rec.type == 300) {
+                symmetry_metrics(B, rec.i, rec.j, rec.f);
+            } else {
+                e = extrapolate_metrics(B, rec.i, rec.j, rec.f);
+            }
+            if (e) return e;
+        }
+        cs.time_from_call = cs.time;
+    }
+    o->committed = true;
+    return Q2D_OK;
+}
+
+bool rec_less(const q2d_bc_rec& a, const q2d_bc_rec& b) {
+    if (a.b != b.b) return a.b < b.b;
+    return a.f < b.f;
+}
+
+}  // namespace
+
+extern "C" {
+
+int q2d_oracle_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
+int q2d_oracle_create(q2d_oracle** out, const q2d_options* opt) {
+    if (!out || !opt) return Q2D_ERR_BADARG;
+    if (opt->n_rk < 1 || opt->n_rk > 3 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) ||
+        opt->res_diter < 1 || opt->sol_diter < 1)
+        return Q2D_ERR_BADARG;
+    q2d_oracle* o = new (std::nothrow) q2d_oracle();
+    if (!o) return Q2D_ERR_OOM;
+    o->opt = *opt;
+    o->gas.R = opt->gas_R;
+    o->gas.gamma = opt->gas_gamma;
+    o->gas.gm1 = opt->gas_gamma - 1.0;
+    o->gas.cp = opt->gas_gamma * opt->gas_R / (opt->gas_gamma - 1.0);
+    o->gas.cv = opt->gas_R / (opt->gas_gamma - 1.0);
+    *out = o;
+    return Q2D_OK;
+}
+
+int q2d_oracle_add_case(q2d_oracle* o, int* case_id) {
+    if (!o || o->committed) return Q2D_ERR_BADARG;
+    o->cases.emplace_back();
+    if (case_id) *case_id = (int)o->cases.size() - 1;
+    return Q2D_OK;
+}
+
+int q2d_oracle_add_block(q2d_oracle* o, int case_id, int ni, int nj, const double* nodes_xy,
+                         const double* cross_section, int* block_id) {
+    if (!o || o->committed || case_id < 0 || case_id >= (int)o->cases.size() || ni < 1 || nj < 1 ||
+        !nodes_xy)
+        return Q2D_ERR_BADARG;
+    Block B;
+    B.ni = ni; B.nj = nj; B.case_id = case_id;
+    B.local_b = (int)o->cases[case_id].blocks.size() + 1;
+    B.node.assign(nodes_xy, nodes_xy + 2 * (size_t)(ni + 1) * (nj + 1));
+    if (cross_section) B.area.assign(cross_section, cross_section + (size_t)(ni + 1) * (nj + 1));
+    B.P.assign(4 * (size_t)(ni + 4) * (nj + 4), 0.0);
+    o->blk.push_back(std::move(B));
+    o->cases[case_id].blocks.push_back((int)o->blk.size() - 1);
+    if (block_id) *block_id = (int)o->blk.size() - 1;
+    return Q2D_OK;
+}
+
+int q2d_oracle_set_bcs(q2d_oracle* o, int case_id, const q2d_bc_rec* recs, int n) {
+    if (!o || o->committed || case_id < 0 || case_id >= (int)o->cases.size() || n < 0 || (n && !recs))
+        return Q2D_ERR_BADARG;
+    Case& cs = o->cases[case_id];
+    std::vector<q2d_bc_rec> v(recs, recs + n);
+    for (const q2d_bc_rec& r : v) {
+        if (r.b < 1 || r.b > (int)cs.blocks.size() || r.f < 1 || r.f > 4) return Q2D_ERR_BADARG;
+        const Block& B = o->blk[cs.blocks[r.b - 1]];
+        if (r.i < 1 || r.i > B.ni || r.j < 1 || r.j > B.nj) return Q2D_ERR_BADARG;
+        switch (r.type) {
+            case 400:
+                if ((r.f <= 2 && B.ni < 3) || (r.f >= 3 && B.nj < 3)) return Q2D_ERR_BADARG;
+                break;
+            case 0: case 300: case 401: case 405: case 406:
+                if (r.f <= 2 && B.ni < 2) return Q2D_ERR_BADARG;
+                break;
+            case 101:
+                if (r.bs < 1 || r.bs > (int)cs.blocks.size() || r.fs < 1 || r.fs > 4) return Q2D_ERR_BADARG;
+                break;
+            default: return Q2D_ERR_UNSUPPORTED;
+        }
+    }
+    std::stable_sort(v.begin(), v.end(), rec_less);
+    cs.bc = std::move(v);
+    return Q2D_OK;
+}
+
+int q2d_oracle_upload_prim(q2d_oracle* o, int block_id, const double* P) {
+    if (!o || block_id < 0 || block_id >= (int)o->blk.size() || !P) return Q2D_ERR_BADARG;
+    Block& B = o->blk[block_id];
+    for (int j = 1; j <= B.nj; ++j)
+        for (int i = 1; i <= B.ni; ++i)
+            std::memcpy(B.p(i, j), &P[4 * B.c(i, j)], sizeof(double) * 4);
+    return Q2D_OK;
+}
+
+int q2d_oracle_download_prim(q2d_oracle* o, int block_id, double* P) {
+    if (!o || block_id < 0 || block_id >= (int)o->blk.size() || !P) return Q2D_ERR_BADARG;
+    Block& B = o->blk[block_id];
+    for (int j = 1; j <= B.nj; ++j)
+        for (int i = 1; i <= B.ni; ++i)
+            std::memcpy(&P[4 * B.c(i, j)], B.pc(i, j), sizeof(double) * 4);
+    return Q2D_OK;
+}
+
+int q2d_oracle_commit(q2d_oracle* o) {
+    if (!o) return Q2D_ERR_BADARG;
+    return commit(o);
+}
+
+int q2d_oracle_step(q2d_oracle* o, int nsteps, q2d_step_info* out) {
+    if (!o || nsteps < 0) return Q2D_ERR_BADARG;
+    int e = commit(o);
+    if (e) return e;
+    std::vector<char> paused(o->cases.size(), 0);
+    for (int s = 0; s < nsteps; ++s) {
+        bool any = false;
+        for (size_t c = 0; c < o->cases.size(); ++c) {
+            Case& cs = o->cases[c];
+            if (cs.done || paused[c]) continue;
+            explicit_step(o, cs);
+            if (cs.todo == Q2D_TODO_IO) paused[c] = 1;
+            any = true;
+        }
+        if (!any) break;
+    }
+    int first = Q2D_OK;
+    for (size_t c = 0; c < o->cases.size(); ++c) {
+        if (out) fill_info(o->cases[c], &out[c]);
+        if (!first && o->cases[c].err) first = o->cases[c].err;
+    }
+    return first;
+}
+
+int q2d_oracle_case_info(q2d_oracle* o, int case_id, q2d_step_info* out) {
+    if (!o || !out || case_id < 0 || case_id >= (int)o->cases.size()) return Q2D_ERR_BADARG;
+    fill_info(o->cases[case_id], out);
+    return Q2D_OK;
+}
+
+int q2d_oracle_get_geometry(q2d_oracle* o, int block_id, double* dl, double* sur, double* fi,
+                            double* fj) {
+    if (!o || block_id < 0 || block_id >= (int)o->blk.size()) return Q2D_ERR_BADARG;
+    int e = commit(o);
+    if (e) return e;
+    const Block& B = o->blk[block_id];
+    if (dl) std::memcpy(dl, B.dl.data(), sizeof(double) * B.dl.size());
+    if (sur)
+        for (int j = 1; j <= B.nj; ++j)
+            for (int i = 1; i <= B.ni; ++i) sur[(i - 1) + B.ni * (j - 1)] = B.sur[B.c(i, j)];
+    if (fi) std::memcpy(fi, B.f1.data(), sizeof(double) * B.f1.size());
+    if (fj) std::memcpy(fj, B.f2.data(), sizeof(double) * B.f2.size());
+    return Q2D_OK;
+}
+
+void q2d_oracle_destroy(q2d_oracle* o) { delete o; }
+
+double q2d_oracle_limiter(int limiter, double x, double y) { return rlimiter(limiter, x, y); }
+
+void q2d_oracle_riemann(int kind, const q2d_options* opt, const double* L, const double* R,
+                        double nx, double ny, double* flux4) {
+    Gas g;
+    g.R = opt->gas_R; g.gamma = opt->gas_gamma; g.gm1 = g.gamma - 1.0;
+    g.cp = g.gamma * g.R / g.gm1; g.cv = g.R / g.gm1;
+    const double aL = f_ss(g, L[3], L[0]), aR = f_ss(g, R[3], R[0]);
+    const Flux4 F = riemann(kind, g, L, aL, R, aR, nx, ny);
+    flux4[0] = F.r; flux4[1] = F.u; flux4[2] = F.v; flux4[3] = F.e;
+}
+
+}  // extern "C"

@@ -1,0 +1,56 @@
+/*
+ * q2d_oracle.h — CPU oracle for the Q2D explicit residual/update path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is a C++ restatement of the reference Fortran
+ * (open-hydra/Q2D) routines listed in each function's comment in q2d_oracle.cpp. It is the
+ * checker for the CUDA path and the timed CPU baseline; the product library never links,
+ * loads or calls it. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
+ * use it.
+ *
+ * Parity pinning: the reference cannot be built here (no Fortran compiler; the FLINT
+ * thermodynamics submodule is absent). The restatement is pinned end-to-end against the
+ * reference's committed outputs (tests/golden/: ShuOsher limiter baselines written by the
+ * reference binary, exact Riemann solutions) — see tests/test_oracle_golden.py.
+ * Thermodynamics uses the calorically perfect single-species closure that the reference's
+ * constant-cp gas tables imply (h = cp T, e = cv T, a = sqrt(gamma p / rho)).
+ *
+ * The exported API mirrors include/q2d_gpu.h one to one (q2d_oracle_* <-> q2d_gpu_*), so a
+ * test drives both through the same sequence of calls.
+ */
+#ifndef Q2D_ORACLE_H
+#define Q2D_ORACLE_H
+#include "../include/q2d_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct q2d_oracle q2d_oracle;
+
+int  q2d_oracle_create(q2d_oracle** out, const q2d_options* opt);
+int  q2d_oracle_add_case(q2d_oracle* o, int* case_id);
+int  q2d_oracle_add_block(q2d_oracle* o, int case_id, int ni, int nj, const double* nodes_xy,
+                          const double* cross_section, int* block_id);
+int  q2d_oracle_set_bcs(q2d_oracle* o, int case_id, const q2d_bc_rec* recs, int n);
+int  q2d_oracle_upload_prim(q2d_oracle* o, int block_id, const double* P);
+int  q2d_oracle_commit(q2d_oracle* o);
+int  q2d_oracle_step(q2d_oracle* o, int nsteps, q2d_step_info* out);
+int  q2d_oracle_case_info(q2d_oracle* o, int case_id, q2d_step_info* out);
+int  q2d_oracle_download_prim(q2d_oracle* o, int block_id, double* P);
+void q2d_oracle_destroy(q2d_oracle* o);
+int  q2d_oracle_set_threads(int n);   /* OpenMP threads used by the cell loops; returns the count */
+
+/* Geometry produced by Setup_Metrics, for tests: dl (2 per cell incl. ghosts, layout
+ * [(i+1)+(ni+4)*(j+1)]*2+d), sur (interior, i fastest), i-face and j-face (nx, ny, len). */
+int  q2d_oracle_get_geometry(q2d_oracle* o, int block_id, double* dl, double* sur,
+                             double* fi, double* fj);
+
+/* Scalar kernels for known-answer tests. */
+double q2d_oracle_limiter(int limiter, double x, double y);
+void   q2d_oracle_riemann(int riemann, const q2d_options* opt, const double* primL,
+                          const double* primR, double nx, double ny, double* flux4);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,503 @@
+// q2d_dev.cuh — device data layout and the per-face / per-cell physics of the Q2D explicit
+// path for sm_100a.
+//
+// Layout in HBM (all pools are structure-of-arrays planes, padded to 32 elements):
+//   state pools A, B, C    4 cell planes per block (rho, u, v, p), cell (i,j) at j*ni + i
+//   scalar pool            8 cell planes per block: sur, dtlocal, versor1 (x,y), versor2 (x,y),
+//                          source 0/1 (1/r for axisymmetric; Gx, Gy for area variation)
+//   dl pool                2 ghost-frame planes per block ((ni+4) x (nj+4), gc = 2)
+//   i-face / j-face pools  3 planes (nx, ny, int_l) on (ni+1) x nj and ni x (nj+1) faces
+//   node pool              2 planes (x, y) on (ni+1) x (nj+1) nodes
+// Index conventions follow the reference: face F of a row (0..ni) separates 1-based cells F
+// and F+1 (dir(1)%f(F,j), Lib_Metrics.f90:88-100); guide/face codes 1..4 as in
+// Parameters_m.f90:13-18.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace q2d {
+
+constexpr int kStatus_Running = 0;
+constexpr int kStatus_Paused = 1;   // TODO = IO inside a multi-step call
+constexpr int kStatus_Done = 2;     // TODO = END
+constexpr int kStatus_Error = 3;
+
+struct DBlock {
+    int ni, nj;
+    int case_id, local_b;
+    long long oc;     // offset of the block in 4-plane cell pools (elements); plane stride pc
+    long long pc;
+    long long og;     // offset in 2-plane ghost-frame pools; plane stride pg
+    long long pg;
+    long long ofi, pfi;   // i-face pool offset / plane stride
+    long long ofj, pfj;   // j-face pool offset / plane stride
+    long long on, pn;     // node pool offset / plane stride
+    int eo[4];            // offset of the edge records of faces 1..4
+};
+
+// One boundary-cell record as the kernels consume it.
+struct EdgeRec {
+    int type;        // BC code, or -1 when the face has no record
+    int bs;          // 101: global id of the donor block
+    int is, js, fs;  // 101: donor cell (1-based) and face
+    int param;       // index into BCParam (401/405/406), -1 otherwise
+};
+
+struct BCParam {
+    double T0, p0, pamb, mach, alpha, rel_fac;
+    double t0, t1;   // unit tangent of the boundary face (Setup_Inflow_Geometry)
+};
+
+struct DCase {
+    int item_begin, item_end;   // work items of the case (contiguous)
+    int ndir;                   // 1 when block 1 of the case has nj == 1 (Check_Mesh_Type)
+    int pad;
+};
+
+// Per-case run state, updated on the device by the last CTA that finishes a case's work in
+// each stage (no host round trip per step).
+struct CaseState {
+    double dt_step;        // dt of the step being run / about to run (min over cells, <= 1e5)
+    double dtglobal;       // reported dtglobal of the last started step
+    double time;
+    double time_from_call;
+    double res[4];
+    double res0;
+    long long iter;
+    long long iter_from_call;
+    int todo;
+    int status;
+    int err, err_b, err_i, err_j, err_stage;
+    unsigned int counter;  // items of the current stage finished (reset by the last CTA)
+    int pad;
+};
+
+struct WorkItem {
+    int block;   // global block id
+    int i0, j0;  // 0-based origin of the tile
+    int case_id;
+};
+
+struct Gas {
+    double R, gamma, gm1, cp, cv;
+    double gfac;   // gamma / (gamma - 1)
+};
+
+struct StageArgs {
+    const DBlock* blocks;
+    const DCase* cases;
+    CaseState* cstate;
+    const WorkItem* items;
+    int n_items;
+    const double* Pin;     // stencil state
+    const double* PO;      // state at the start of the step
+    double* Pout;
+    double* sc;            // scalar pool
+    const double* dl;
+    const float* dl32;
+    const double* fi;
+    const double* fj;
+    const EdgeRec* edges;
+    const BCParam* bcp;
+    double* part;          // per-item partials: 4 residual sums + dt min
+    Gas gas;
+    double rk_c;           // RKcoeff(n_rk, irk)
+    double cfl;
+    int irk, n_rk;
+    int first, last;       // stage is the first / last of the step
+    int limiter, source, time_accurate, rampa;
+    int res_diter, sol_diter, res_relative;
+    long long itermax;
+    double res_threshold, time_threshold, sol_dtime;
+    int* launch_flag;      // set to 1 by every kernel launch (instrumentation, unused by math)
+};
+
+// ---------------------------------------------------------------------------------------
+// Calorically perfect closure (the oracle's THERMO section): a = sqrt(gamma p / rho),
+// E0 = p/((gamma-1) rho) + |V|^2/2, H0 = gamma p/((gamma-1) rho) + |V|^2/2, h = cp T.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double f_ss(const Gas& g, double p, double rho) {
+    return sqrt(g.gamma * p / rho);
+}
+__device__ __forceinline__ double E0(const Gas& g, double p, double rho, double modv) {
+    return p / (g.gm1 * rho) + 0.5 * modv * modv;
+}
+__device__ __forceinline__ double H0(const Gas& g, double p, double rho, double modv) {
+    return g.gamma * p / (g.gm1 * rho) + 0.5 * modv * modv;
+}
+__device__ __forceinline__ bool gas_state_bad(double rho, double p) {
+    return !(rho > 0.0) || !(p > 0.0);
+}
+
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+
+// Limiters, FP64, operation order of Lib_Limiters.f90:26-110.
+__device__ __forceinline__ double rlimiter(int lim, double x, double y) {
+    if (lim == 1) {                                   // minmod :36-46
+        double r = 0.0;
+        if (x * y < 0.0) return r;
+        r = x;
+        if (fabs(x) > fabs(y)) r = y;
+        return r;
+    }
+    if (lim == 0) return 0.0;                         // IORD
+    const double ru = y / (x + 1e-30);
+    double phi;
+    switch (lim) {
+        case 2: phi = (ru + fabs(ru)) / (1.0 + fabs(ru)); break;                       // vanleer
+        case 3: phi = (ru * ru + ru) / (1.0 + ru * ru); break;                          // vanalbada
+        case 4: phi = dmax(0.0, dmin(dmin(2.0 * ru, 0.5 * (1.0 + ru)), 2.0)); break;   // MC
+        case 5: phi = dmax(dmax(0.0, dmin(2.0 * ru, 1.0)), dmin(ru, 2.0)); break;       // superbee
+        default: {                                                                      // LIMO3
+            const double a = (2.0 + ru) / 3.0;
+            const double inner = dmin(dmin(2.0 * ru, (2.0 + ru) / 3.0), 1.6);
+            const double mid = dmax(dmax(-0.5 * ru, 0.0), inner);
+            phi = dmax(0.0, dmin(a, mid));
+        }
+    }
+    return phi * x;
+}
+
+// Limiters, FP32, division-free algebraic equivalents of phi(y/x)*x (x = 0 gives 0 like the
+// reference's epsilon form).
+__device__ __forceinline__ float rlimiter32(int lim, float x, float y) {
+    switch (lim) {
+        case 0: return 0.0f;
+        case 1: {
+            if (x * y < 0.0f) return 0.0f;
+            return fabsf(x) > fabsf(y) ? y : x;
+        }
+        case 2: {   // 2xy/(x+y) when xy > 0
+            const float xy = x * y;
+            return xy > 0.0f ? __fdividef(2.0f * xy, x + y) : 0.0f;
+        }
+        case 3: {   // xy(x+y)/(x^2+y^2)
+            const float d = x * x + y * y;
+            return d > 0.0f ? __fdividef(x * y * (x + y), d) : 0.0f;
+        }
+        case 4: {   // MC
+            const float a = fminf(fminf(2.0f * y, 0.5f * (x + y)), 2.0f * x);
+            const float b = fmaxf(fmaxf(2.0f * y, 0.5f * (x + y)), 2.0f * x);
+            return x > 0.0f ? fmaxf(0.0f, a) : (x < 0.0f ? fminf(0.0f, b) : 0.0f);
+        }
+        case 5: {   // superbee
+            if (x > 0.0f) return fmaxf(fmaxf(0.0f, fminf(2.0f * y, x)), fminf(y, 2.0f * x));
+            if (x < 0.0f) return fminf(fminf(0.0f, fmaxf(2.0f * y, x)), fmaxf(y, 2.0f * x));
+            return 0.0f;
+        }
+        default: {  // LIMO3
+            const float t = (2.0f * x + y) * (1.0f / 3.0f);
+            if (x > 0.0f) {
+                const float inner = fminf(fminf(2.0f * y, t), 1.6f * x);
+                const float mid = fmaxf(fmaxf(-0.5f * y, 0.0f), inner);
+                return fmaxf(0.0f, fminf(t, mid));
+            }
+            if (x < 0.0f) {
+                const float inner = fmaxf(fmaxf(2.0f * y, t), 1.6f * x);
+                const float mid = fminf(fminf(-0.5f * y, 0.0f), inner);
+                return fminf(0.0f, fmaxf(t, mid));
+            }
+            return 0.0f;
+        }
+    }
+}
+
+struct F4 { double r, u, v, e; };
+
+// roe_averages (Lib_Riemann_HLL.f90:229-317), constant-cp identities, same operation order
+// as the oracle.
+__device__ __forceinline__ void roe_averages(const Gas& g, double dltot, double drtot, double ul,
+                                             double vl, double ur, double vr, double pl,
+                                             double pr, double& h0l, double& h0r,
+                                             double& u_roe, double& v_roe, double& a_roe) {
+    const double inv_dltot = 1.0 / dltot;
+    const double inv_drtot = 1.0 / drtot;
+    const double Tl = pl * inv_dltot / g.R;
+    const double Tr = pr * inv_drtot / g.R;
+    const double srL = sqrt(dltot);
+    const double srR = sqrt(drtot);
+    const double inv_sr = 1.0 / (srL + srR);
+    u_roe = (srR * ur + srL * ul) * inv_sr;
+    v_roe = (srR * vr + srL * vl) * inv_sr;
+    const double R_roe = (srR * g.R + srL * g.R) * inv_sr;
+    const double T_roe = (srR * Tr + srL * Tl) * inv_sr;
+    const double hl = g.cp * Tl;
+    const double hr = g.cp * Tr;
+    const double el = hl - g.R * Tl;
+    const double er = hr - g.R * Tr;
+    h0l = 0.0 + hl * dltot * inv_dltot;
+    h0r = 0.0 + hr * drtot * inv_drtot;
+    const double d_roe = (srR * drtot * inv_drtot + srL * dltot * inv_dltot) * inv_sr;
+    const double cv_roe = 0.0 + d_roe * (0.5 * (g.cp + g.cp) - g.R);
+    const double sum_ei = 0.0 + d_roe * (srR * er + srL * el) * inv_sr;
+    h0l = h0l + 0.5 * (ul * ul + vl * vl);
+    h0r = h0r + 0.5 * (ur * ur + vr * vr);
+    const double h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+    const double gam_roe = 1.0 + R_roe / cv_roe;
+    const double vel2 = u_roe * u_roe + v_roe * v_roe;
+    a_roe = sqrt((gam_roe - 1.0) * (h0_roe - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
+}
+
+// riemann_HLLC (Lib_Riemann_HLL.f90:34-123), FP64.
+__device__ __forceinline__ F4 riemann_hllc(const Gas& g, const double* L, double al,
+                                           const double* R, double ar, double nx, double ny) {
+    const double dltot = L[0], ul = L[1], vl = L[2], pl = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], pr = R[3];
+    F4 F;
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    double h0l, h0r, u_roe, v_roe, a_roe;
+    roe_averages(g, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, u_roe, v_roe, a_roe);
+    const double un_roe = u_roe * nx + v_roe * ny;
+    const double e0l = h0l - pl / dltot;
+    const double e0r = h0r - pr / drtot;
+    const double S1 = dmin(dmin(0.0, unl - al), un_roe - a_roe);
+    const double S4 = dmax(dmax(0.0, unr + ar), un_roe + a_roe);
+    double inv_denom = 1.0 / (dltot * (S1 - unl) - drtot * (S4 - unr));
+    const double Sstar = (pr - pl + dltot * unl * (S1 - unl) - drtot * unr * (S4 - unr)) * inv_denom;
+    const double pstar = dltot * (unl - S1) * (unl - Sstar) + pl;
+    if (S1 >= 0.0) {
+        F.r = dltot * unl;
+        F.u = F.r * ul + pl * nx;
+        F.v = F.r * vl + pl * ny;
+        F.e = F.r * h0l;
+    } else if (Sstar >= 0.0) {
+        F.r = dltot * unl;
+        F.u = F.r * ul + pl * nx;
+        F.v = F.r * vl + pl * ny;
+        F.e = F.r * h0l;
+        inv_denom = 1.0 / (S1 - Sstar);
+        const double U1S = dltot * (S1 - unl) * inv_denom;
+        const double U2S = ((S1 - unl) * dltot * ul + (pstar - pl) * nx) * inv_denom;
+        const double U3S = ((S1 - unl) * dltot * vl + (pstar - pl) * ny) * inv_denom;
+        const double U5S = ((S1 - unl) * dltot * e0l - pl * unl + pstar * Sstar) * inv_denom;
+        F.r = F.r + S1 * (U1S - dltot);
+        F.u = F.u + S1 * (U2S - dltot * ul);
+        F.v = F.v + S1 * (U3S - dltot * vl);
+        F.e = F.e + S1 * (U5S - dltot * e0l);
+    } else if (S4 > 0.0) {
+        F.r = drtot * unr;
+        F.u = F.r * ur + pr * nx;
+        F.v = F.r * vr + pr * ny;
+        F.e = F.r * h0r;
+        inv_denom = 1.0 / (S4 - Sstar);
+        const double U1S = drtot * (S4 - unr) * inv_denom;
+        const double U2S = ((S4 - unr) * drtot * ur + (pstar - pr) * nx) * inv_denom;
+        const double U3S = ((S4 - unr) * drtot * vr + (pstar - pr) * ny) * inv_denom;
+        const double U5S = ((S4 - unr) * drtot * e0r - pr * unr + pstar * Sstar) * inv_denom;
+        F.r = F.r + S4 * (U1S - drtot);
+        F.u = F.u + S4 * (U2S - drtot * ur);
+        F.v = F.v + S4 * (U3S - drtot * vr);
+        F.e = F.e + S4 * (U5S - drtot * e0r);
+    } else {
+        F.r = drtot * unr;
+        F.u = F.r * ur + pr * nx;
+        F.v = F.r * vr + pr * ny;
+        F.e = F.r * h0r;
+    }
+    return F;
+}
+
+// riemann_HLLE (Lib_Riemann_HLL.f90:126-169), FP64.
+__device__ __forceinline__ F4 riemann_hlle(const Gas& g, const double* L, double al,
+                                           const double* R, double ar, double nx, double ny) {
+    const double dltot = L[0], ul = L[1], vl = L[2], pl = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], pr = R[3];
+    F4 F;
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    double h0l, h0r, u_roe, v_roe, a_roe;
+    roe_averages(g, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, u_roe, v_roe, a_roe);
+    const double un_roe = u_roe * nx + v_roe * ny;
+    const double S1 = dmin(dmin(0.0, unl - al), un_roe - a_roe);
+    const double S4 = dmax(dmax(0.0, unr + ar), un_roe + a_roe);
+    const double inv_denom = 1.0 / (S4 - S1);
+    const double FrL = dltot * unl;
+    const double FrR = drtot * unr;
+    F.r = (S4 * FrL - S1 * FrR + S1 * S4 * (drtot - dltot)) * inv_denom;
+    F.u = (S4 * (FrL * ul + pl * nx) - S1 * (FrR * ur + pr * nx) +
+           S1 * S4 * (drtot * ur - dltot * ul)) * inv_denom;
+    F.v = (S4 * (FrL * vl + pl * ny) - S1 * (FrR * vr + pr * ny) +
+           S1 * S4 * (drtot * vr - dltot * vl)) * inv_denom;
+    F.e = (S4 * (FrL * h0l) - S1 * (FrR * h0r) +
+           S1 * S4 * (drtot * (h0r - pr / drtot) - dltot * (h0l - pl / dltot))) * inv_denom;
+    return F;
+}
+
+// riemann_LLF (Lib_Riemann_LF.f90:11-40) with fluxes (:101-118), FP64.
+__device__ __forceinline__ F4 phys_flux(const Gas& g, double p, double r, double u, double v,
+                                        double nx, double ny) {
+    F4 F;
+    F.r = r * (u * nx + v * ny);
+    F.u = F.r * u + p * nx;
+    F.v = F.r * v + p * ny;
+    F.e = F.r * H0(g, p, r, sqrt(u * u + v * v));
+    return F;
+}
+__device__ __forceinline__ F4 riemann_llf(const Gas& g, const double* L, double al,
+                                          const double* R, double ar, double nx, double ny) {
+    const double dltot = L[0], ul = L[1], vl = L[2], pl = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], pr = R[3];
+    F4 F;
+    const double uln = ul * nx + vl * ny;
+    const double urn = ur * nx + vr * ny;
+    const double A = dmax(dmax(dmax(fabs(uln - al), fabs(urn - ar)), fabs(uln + al)), fabs(urn + ar));
+    const F4 Fr = phys_flux(g, pr, drtot, ur, vr, nx, ny);
+    const F4 Fl = phys_flux(g, pl, dltot, ul, vl, nx, ny);
+    F.r = 0.5 * (Fl.r + Fr.r - A * (drtot - dltot));
+    F.u = 0.5 * (Fr.u + Fl.u - A * (drtot * ur - dltot * ul));
+    F.v = 0.5 * (Fr.v + Fl.v - A * (drtot * vr - dltot * vl));
+    F.e = 0.5 * (Fl.e + Fr.e - A * (drtot * E0(g, pr, drtot, sqrt(ur * ur + vr * vr)) -
+                                    dltot * E0(g, pl, dltot, sqrt(ul * ul + vl * vl))));
+    return F;
+}
+
+template <int RIEM>
+__device__ __forceinline__ F4 riemann64(const Gas& g, const double* L, double al, const double* R,
+                                        double ar, double nx, double ny) {
+    if (RIEM == 1) return riemann_hlle(g, L, al, R, ar, nx, ny);
+    if (RIEM == 2) return riemann_llf(g, L, al, R, ar, nx, ny);
+    return riemann_hllc(g, L, al, R, ar, nx, ny);
+}
+
+// Face flux from two reconstructed states (Lib_Convective.f90:56-80), FP64. Returns false on
+// a non-physical state (check_gas_state).
+template <int RIEM>
+__device__ __forceinline__ bool flux_from_states64(const Gas& g, const double* P1, const double* P4,
+                                                   double nx, double ny, double int_l, double* fl) {
+    const bool bad = gas_state_bad(P1[0], P1[3]) || gas_state_bad(P4[0], P4[3]);
+    const double a1 = f_ss(g, P1[3], P1[0]);
+    const double a4 = f_ss(g, P4[3], P4[0]);
+    const F4 F = riemann64<RIEM>(g, P1, a1, P4, a4, nx, ny);
+    // single species: sp*(rho1/rho1) - sm*(rho4/rho4) == 1 exactly
+    fl[0] = F.r * int_l;
+    fl[1] = F.u * int_l;
+    fl[2] = F.v * int_l;
+    fl[3] = F.e * int_l;
+    return !bad;
+}
+
+// ---------------------------------------------------------------------------------------
+// FP32-flux form. Reconstruction, limiter and the Riemann wave structure run in FP32; the
+// physical fluxes of the two face states, the state jumps and the sum F = F_K + S_K (U*_K -
+// U_K) stay FP64. (U*_K - U_K) is rewritten so that every FP32 product multiplies a state
+// jump (S* - un_K, p* - p_K): FP32 rounding then scales with the jump, not with |F|.
+// ---------------------------------------------------------------------------------------
+struct FluxState {   // FP64 face state plus its physical flux (per unit normal)
+    double r, u, v, p, un;
+    F4 F;
+};
+
+__device__ __forceinline__ void phys64(const Gas& g, const double* q, double nx, double ny,
+                                       FluxState& s) {
+    s.r = q[0]; s.u = q[1]; s.v = q[2]; s.p = q[3];
+    s.un = s.u * nx + s.v * ny;
+    const double m = s.r * s.un;
+    s.F.r = m;
+    s.F.u = m * s.u + s.p * nx;
+    s.F.v = m * s.v + s.p * ny;
+    // un * (rho E + p) = un * (gamma/(gamma-1) p + rho |V|^2 / 2): no division
+    s.F.e = s.un * (g.gfac * s.p + 0.5 * s.r * (s.u * s.u + s.v * s.v));
+}
+
+template <int RIEM>
+__device__ __forceinline__ F4 riemann32(const Gas& g, const FluxState& L, const FluxState& R,
+                                        float nx, float ny) {
+    // FP32 wave structure
+    const float rl = (float)L.r, rr = (float)R.r;
+    const float ul = (float)L.u, vl = (float)L.v, ur = (float)R.u, vr = (float)R.v;
+    const float pl = (float)L.p, pr = (float)R.p;
+    const float gam = (float)g.gamma;
+    const float irl = __frcp_rn(rl), irr = __frcp_rn(rr);
+    const float al = sqrtf(gam * pl * irl), ar = sqrtf(gam * pr * irr);
+    const float unl = (float)L.un, unr = (float)R.un;
+    // jumps, formed in FP64
+    const float dp = (float)(R.p - L.p);
+    const float dun = (float)(R.un - L.un);
+    if (RIEM == 2) {   // LLF: F = (F_L + F_R)/2 - A/2 (U_R - U_L)
+        const float A = fmaxf(fmaxf(fabsf(unl - al), fabsf(unr - ar)), fmaxf(fabsf(unl + al), fabsf(unr + ar)));
+        const double dU0 = R.r - L.r;
+        const double dU1 = R.r * R.u - L.r * L.u;
+        const double dU2 = R.r * R.v - L.r * L.v;
+        const double dU3 = (R.p / g.gm1 + 0.5 * R.r * (R.u * R.u + R.v * R.v)) -
+                           (L.p / g.gm1 + 0.5 * L.r * (L.u * L.u + L.v * L.v));
+        const double hA = 0.5 * (double)A;
+        F4 F;
+        F.r = 0.5 * (L.F.r + R.F.r) - hA * (double)(float)dU0;
+        F.u = 0.5 * (L.F.u + R.F.u) - hA * (double)(float)dU1;
+        F.v = 0.5 * (L.F.v + R.F.v) - hA * (double)(float)dU2;
+        F.e = 0.5 * (L.F.e + R.F.e) - hA * (double)(float)dU3;
+        return F;
+    }
+    // Roe averages (constant cp: gamma_roe = gamma, a^2 = (gamma-1)(h0 - |V|^2/2))
+    const float srL = sqrtf(rl), srR = sqrtf(rr);
+    const float isr = __frcp_rn(srL + srR);
+    const float u_roe = (srR * ur + srL * ul) * isr;
+    const float v_roe = (srR * vr + srL * vl) * isr;
+    const float gf = (float)g.gfac;
+    const float h0l = gf * pl * irl + 0.5f * (ul * ul + vl * vl);
+    const float h0r = gf * pr * irr + 0.5f * (ur * ur + vr * vr);
+    const float h0_roe = (srR * h0r + srL * h0l) * isr;
+    const float a_roe = sqrtf(fmaxf((gam - 1.0f) * (h0_roe - 0.5f * (u_roe * u_roe + v_roe * v_roe)), 0.0f));
+    const float un_roe = u_roe * nx + v_roe * ny;
+    const float S1 = fminf(fminf(0.0f, unl - al), un_roe - a_roe);
+    const float S4 = fmaxf(fmaxf(0.0f, unr + ar), un_roe + a_roe);
+    if (RIEM == 1) {   // HLLE: F = Fbar - (S4+S1)/(2(S4-S1)) dF + S1 S4/(S4-S1) dU
+        const float inv = __frcp_rn(S4 - S1);
+        const float c1 = 0.5f * (S4 + S1) * inv;
+        const float c2 = S1 * S4 * inv;
+        const double dU0 = R.r - L.r;
+        const double dU1 = R.r * R.u - L.r * L.u;
+        const double dU2 = R.r * R.v - L.r * L.v;
+        const double dU3 = (R.p / g.gm1 + 0.5 * R.r * (R.u * R.u + R.v * R.v)) -
+                           (L.p / g.gm1 + 0.5 * L.r * (L.u * L.u + L.v * L.v));
+        F4 F;
+        F.r = 0.5 * (L.F.r + R.F.r) + (double)(c2 * (float)dU0 - c1 * (float)(R.F.r - L.F.r));
+        F.u = 0.5 * (L.F.u + R.F.u) + (double)(c2 * (float)dU1 - c1 * (float)(R.F.u - L.F.u));
+        F.v = 0.5 * (L.F.v + R.F.v) + (double)(c2 * (float)dU2 - c1 * (float)(R.F.v - L.F.v));
+        F.e = 0.5 * (L.F.e + R.F.e) + (double)(c2 * (float)dU3 - c1 * (float)(R.F.e - L.F.e));
+        return F;
+    }
+    // HLLC (Batten), jump form
+    if (S1 >= 0.0f) return L.F;
+    const float D = rl * (S1 - unl) - rr * (S4 - unr);
+    const float sm_unl = (dp - rr * (S4 - unr) * dun) * __frcp_rn(D);   // S* - un_L
+    const float Sstar = unl + sm_unl;
+    if (Sstar >= 0.0f) {
+        const float inv = __frcp_rn(S1 - Sstar);
+        const float q = sm_unl * inv;
+        const float dps = rl * (S1 - unl) * sm_unl;                      // p* - p_L
+        const float e0l = pl * irl / (gam - 1.0f) + 0.5f * (ul * ul + vl * vl);
+        const float d0 = rl * q;
+        const float d1 = rl * ul * q + dps * nx * inv;
+        const float d2 = rl * vl * q + dps * ny * inv;
+        const float d3 = rl * e0l * q + (dps * Sstar + pl * sm_unl) * inv;
+        F4 F;
+        F.r = L.F.r + (double)(S1 * d0);
+        F.u = L.F.u + (double)(S1 * d1);
+        F.v = L.F.v + (double)(S1 * d2);
+        F.e = L.F.e + (double)(S1 * d3);
+        return F;
+    }
+    if (S4 > 0.0f) {
+        const float inv = __frcp_rn(S4 - Sstar);
+        const float sm_unr = sm_unl - dun;                               // S* - un_R
+        const float q = sm_unr * inv;
+        const float dps = rr * (S4 - unr) * sm_unr;                      // p* - p_R
+        const float e0r = pr * irr / (gam - 1.0f) + 0.5f * (ur * ur + vr * vr);
+        const float d0 = rr * q;
+        const float d1 = rr * ur * q + dps * nx * inv;
+        const float d2 = rr * vr * q + dps * ny * inv;
+        const float d3 = rr * e0r * q + (dps * Sstar + pr * sm_unr) * inv;
+        F4 F;
+        F.r = R.F.r + (double)(S4 * d0);
+        F.u = R.F.u + (double)(S4 * d1);
+        F.v = R.F.v + (double)(S4 * d2);
+        F.e = R.F.e + (double)(S4 * d3);
+        return F;
+    }
+    return R.F;
+}
+
+}  // namespace q2d

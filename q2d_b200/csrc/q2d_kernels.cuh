@@ -1,0 +1,19 @@
+// q2d_kernels.cuh — launch interface of the device code (q2d_kernels.cu) for the host
+// runtime (q2d_api.cu).
+#pragma once
+#include "q2d_dev.cuh"
+
+namespace q2d {
+
+// Tile configurations of the stage kernel (tile id -> TX x TY cells, NT threads):
+//   0: 32 x 7, 256 threads   1: 32 x 15, 512 threads   2: 64 x 7, 512 threads
+constexpr int kNumTiles = 3;
+void tile_dims(int tile, int* tx, int* ty, int* nt);
+
+cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int grid, cudaStream_t s);
+int stage_occupancy(int prec, int riem, int tile);
+cudaError_t launch_dt(const StageArgs& a, int tile, int grid, cudaStream_t s);
+cudaError_t launch_copy(const double* src, double* dst, long long n, int* flag, cudaStream_t s);
+cudaError_t launch_resume(CaseState* cs, int n, int* flag, cudaStream_t s);
+
+}  // namespace q2d

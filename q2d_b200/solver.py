@@ -1,0 +1,125 @@
+"""Host-side driver over the C ABI: the Python mirror of Q2D's Wrap_Setup / Wrap_Solve.
+
+`Q2DSolver` performs the setup sequence of Q2D_setup (src/lib/driver/Wrap_Setup.f90:10-167:
+options -> blocks + nodes + Cross_Section -> initial state -> bc records -> metrics) through
+the q2d_gpu_* entry points, and `solve()` repeats Q2D_solve (Wrap_Solve.f90:10-34) while the
+TODO flag asks for more steps, like the main loop of src/app/main.f90:47-50.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Iterable, Optional
+
+import numpy as np
+
+from . import _abi
+from .cases import CaseSpec
+
+
+class Q2DError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{where}: status {status} {detail}".strip())
+
+
+def make_options(case_or_opts, **overrides) -> _abi.Options:
+    base = dict(case_or_opts.options) if isinstance(case_or_opts, CaseSpec) else dict(case_or_opts)
+    base.update(overrides)
+    return _abi.default_options(**base)
+
+
+class Q2DSolver:
+    """A set of cases advanced together through one library context.
+
+    lib/prefix select the implementation behind the C ABI: the CUDA library
+    (`q2d_gpu`, default) or another library exporting the same entry points."""
+
+    def __init__(self, options: _abi.Options, cases: Iterable[CaseSpec], lib=None,
+                 prefix: str = "q2d_gpu"):
+        self.lib = lib if lib is not None else _abi.load_library()
+        self.prefix = prefix
+        self.options = options
+        self.cases = list(cases)
+        self.ctx = C.c_void_p()
+        self._call("create", C.byref(self.ctx), C.byref(options))
+        self.block_ids = []
+        try:
+            for cs in self.cases:
+                cid = C.c_int()
+                self._call("add_case", self.ctx, C.byref(cid))
+                ids = []
+                for b in cs.blocks:
+                    nodes = np.ascontiguousarray(b.nodes, dtype=np.float64)
+                    area = None if b.area is None else np.ascontiguousarray(b.area, dtype=np.float64)
+                    bid = C.c_int()
+                    self._call("add_block", self.ctx, cid.value, b.ni, b.nj, _abi.dptr(nodes),
+                               None if area is None else _abi.dptr(area), C.byref(bid))
+                    P = b.prim_ghost()
+                    self._call("upload_prim", self.ctx, bid.value, _abi.dptr(P))
+                    ids.append(bid.value)
+                self.block_ids.append(ids)
+                recs = _abi.bc_array(cs.bcs)
+                self._call("set_bcs", self.ctx, cid.value, recs, len(cs.bcs))
+            self._call("commit", self.ctx)
+        except Exception:
+            self.close()
+            raise
+
+    # -- plumbing -------------------------------------------------------------------------
+    def _fn(self, name):
+        return getattr(self.lib, f"{self.prefix}_{name}")
+
+    def _call(self, name, *args):
+        st = self._fn(name)(*args)
+        if st != _abi.OK:
+            detail = ""
+            if self.prefix == "q2d_gpu" and self.ctx:
+                msg = self.lib.q2d_gpu_last_error(self.ctx)
+                detail = msg.decode() if msg else ""
+            raise Q2DError(st, f"{self.prefix}_{name}", detail)
+        return st
+
+    # -- API ------------------------------------------------------------------------------
+    def step(self, nsteps: int = 1, check: bool = True) -> list:
+        infos = (_abi.StepInfo * max(len(self.cases), 1))()
+        st = self._fn("step")(self.ctx, nsteps, infos)
+        out = [infos[c].as_dict() for c in range(len(self.cases))]
+        if check and st != _abi.OK:
+            raise Q2DError(st, f"{self.prefix}_step", str([o["err_at"] for o in out if o["err"]]))
+        return out
+
+    def info(self, case: int = 0) -> dict:
+        s = _abi.StepInfo()
+        self._call("case_info", self.ctx, case, C.byref(s))
+        return s.as_dict()
+
+    def prim(self, case: int = 0, block: int = 0) -> np.ndarray:
+        b = self.cases[case].blocks[block]
+        P = np.zeros((b.nj + 4, b.ni + 4, 4))
+        self._call("download_prim", self.ctx, self.block_ids[case][block], _abi.dptr(P))
+        return P[2:b.nj + 2, 2:b.ni + 2, :].copy()
+
+    def solve(self, max_calls: int = 10 ** 9, steps_per_call: int = 1) -> dict:
+        """Runs until every case reports TODO = END (or an error)."""
+        for _ in range(max_calls):
+            infos = self.step(steps_per_call)
+            if all(i["todo"] == _abi.TODO_END or i["err"] for i in infos):
+                break
+        return self.info(0)
+
+    def close(self):
+        if self.ctx:
+            self._fn("destroy")(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

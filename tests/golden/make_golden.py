@@ -1,0 +1,56 @@
+"""Generates the committed golden fixtures of tests/golden from the reference tree.
+
+Run in a container that has the reference checkout (it is not needed afterwards):
+    python tests/golden/make_golden.py /path/to/open-hydra-Q2D
+
+Fixtures written (all small text/npz files):
+  shuosher_<lim>.txt  outputs of the reference binary for the Shu-Osher problem at N=400,
+                      t=1.8, HLLC, RK3, CFL 0.5, one per limiter (copied verbatim from
+                      test/1D/ShuOsher-LIMO3/reference/baseline_{iord,minmod,vanleer,mc}.dat)
+  sod79_exact.txt     exact Sod solution at t=0.2 (test/1D/Sod79/reference/exact.txt)
+  riemann_exact.npz   exact Riemann solutions sampled at cell centres for the seeded 1-D
+                      Riemann workloads, from the reference's own exact solver
+                      (test/common/pycheck/q2d_exact1d.py:riemann_exact, imported, not copied)
+"""
+import importlib.util
+import shutil
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+
+
+def main(ref_root: str) -> None:
+    ref = Path(ref_root)
+    for lim in ("iord", "minmod", "vanleer", "mc"):
+        shutil.copyfile(ref / f"test/1D/ShuOsher-LIMO3/reference/baseline_{lim}.dat",
+                        HERE / f"shuosher_{lim}.txt")
+    shutil.copyfile(ref / "test/1D/Sod79/reference/exact.txt", HERE / "sod79_exact.txt")
+
+    spec = importlib.util.spec_from_file_location(
+        "q2d_exact1d", ref / "test/common/pycheck/q2d_exact1d.py")
+    ex = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(ex)
+    from q2d_b200 import cases
+
+    out = {}
+    for tag, seed, ni in (("cfg1", cases.BASE_SEED, 1024), ("s1", 11, 256), ("s2", 12, 256)):
+        cs = cases.riemann_1d(ni=ni, seed=seed)
+        rl, ul, pl, rr, ur, pr = cs.meta["states"]
+        xc = 0.5 * (np.linspace(0, 1, ni + 1)[:-1] + np.linspace(0, 1, ni + 1)[1:])
+        sol = ex.riemann_exact(xc, cs.meta["t_end"], 0.5, rl, ul, pl, rr, ur, pr, 1.4)
+        rho, u, p = sol["rho"], sol["u"], sol["p"]
+        out[f"{tag}_states"] = np.array([rl, ul, pl, rr, ur, pr, ni, seed, cs.meta["t_end"]])
+        out[f"{tag}_rho"], out[f"{tag}_u"], out[f"{tag}_p"] = rho, u, p
+    # Toro test 1 (Sod) known answer of the exact solver: p* = 0.30313, u* = 0.92745
+    sol = ex.riemann_exact(np.array([0.5]), 0.2, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1, 1.4)
+    out["toro1_pstar_ustar"] = np.array([sol["pstar"], sol["ustar"]])
+    np.savez(HERE / "riemann_exact.npz", **out)
+    print("written:", sorted(p.name for p in HERE.iterdir() if p.suffix in (".txt", ".npz")))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
