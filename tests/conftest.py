@@ -28,18 +28,30 @@ def oracle_lib():
     return oracle.load()
 
 
+def var_scale(b: np.ndarray, gamma: float = 1.4) -> np.ndarray:
+    """Per-variable scale of a primitive state (rho, u, v, p): max|rho|, max|p|, and for both
+    velocity components the flow's velocity scale max(|u|, |v|, a) (a component that is
+    identically zero, like v in a 1-D problem, is measured against that scale)."""
+    b = b.reshape(-1, b.shape[-1])
+    a = np.sqrt(gamma * np.abs(b[:, 3]) / np.abs(b[:, 0]))
+    vs = max(np.abs(b[:, 1]).max(), np.abs(b[:, 2]).max(), a.max())
+    return np.array([np.abs(b[:, 0]).max(), vs, vs, np.abs(b[:, 3]).max()])
+
+
 def rel_linf(a: np.ndarray, b: np.ndarray) -> np.ndarray:
-    """max |a-b| / max |b| per primitive variable (last axis)."""
+    """max |a-b| / scale per primitive variable (last axis); scale from var_scale(b)."""
+    s = var_scale(b)
     a = a.reshape(-1, a.shape[-1])
     b = b.reshape(-1, b.shape[-1])
-    scale = np.maximum(np.abs(b).max(axis=0), 1e-300)
-    return np.abs(a - b).max(axis=0) / scale
+    return np.abs(a - b).max(axis=0) / s
 
 
 def rel_l1(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """sum |a-b| / (n * scale) per primitive variable; scale from var_scale(b)."""
+    s = var_scale(b)
     a = a.reshape(-1, a.shape[-1])
     b = b.reshape(-1, b.shape[-1])
-    return np.abs(a - b).sum(axis=0) / np.maximum(np.abs(b).sum(axis=0), 1e-300)
+    return np.abs(a - b).sum(axis=0) / (a.shape[0] * s)
 
 
 def cons(prim: np.ndarray, gamma: float = 1.4) -> np.ndarray:
