@@ -23,6 +23,7 @@
 #include "q2d_kernels.cuh"
 
 #include <cfloat>
+#include <type_traits>
 
 namespace q2d {
 
@@ -234,62 +235,63 @@ __device__ bool bc_outflow(const Gas& g, int Fm, const double* Bp, double n0, do
     return true;
 }
 
+// Boundary face flux by record type, states passed by value so that the common interior path
+// keeps its arrays in registers (BC_Fluxes dispatch, Mod_BC_Fluxes.f90:79-269; 401/405/406
+// fall back to BC_Symmetry_Eul when the flow direction does not match, :176-227).
+struct Q4 { double v[4]; };
+template <int RIEM>
+__device__ __noinline__ Q4 bc_face(const Gas g, int lim, int etype, int Fm, const Q4 Bp, const Q4 Ip,
+                                   double dlb, double dli, double nx, double ny, double ln,
+                                   const BCParam* bp) {
+    Q4 X = {{0.0, 0.0, 0.0, 0.0}};
+    bool done = true;
+    if (etype == 400) bc_extrapolation(g, Bp.v, nx, ny, ln, X.v);
+    else if (etype == 401) done = bc_stagnation(g, Fm, Bp.v, nx, ny, ln, *bp, X.v);
+    else if (etype == 405) done = bc_supersonic<RIEM>(g, lim, Fm, Bp.v, Ip.v, nx, ny, ln, *bp, X.v);
+    else if (etype == 406) done = bc_outflow(g, Fm, Bp.v, nx, ny, ln, *bp, X.v);
+    else if (etype == 300) done = false;
+    else if (etype != 0) return X;
+    if (etype == 0) return X;
+    if (!done) bc_symmetry<RIEM>(g, lim, Fm, Bp.v, Ip.v, 0.5 * dlb, 0.5 * dli, nx, ny, ln, X.v);
+    return X;
+}
+
 // ------------------------------------------------------------------------------------------
-// Interior face flux from a 4-cell stencil (prev, loc, next, next2) with mean cell lengths
-// dl[-1..2], FP64 or FP32-flux form.
+// Interior face flux from two reconstructed face states, FP64 or FP32-flux form.
 // ------------------------------------------------------------------------------------------
 template <int PREC, int RIEM>
-__device__ __forceinline__ bool interior_flux(const Gas& g, int lim, const double* q0, const double* q1,
-                                              const double* q2, const double* q3, double dlm1,
-                                              double dl0, double dl1, double dl2, double nx,
-                                              double ny, double int_l, double* fl) {
-    if (PREC == 0) {
-        // Convective_Flux (Lib_Convective.f90:34-46) + Reconstruction (Lib_Reconstruction.f90:21-27)
-        const double l0 = 0.5 * (dlm1 + dl0);
-        const double l1 = 0.5 * (dl0 + dl1);
-        const double l2 = 0.5 * (dl1 + dl2);
-        const double lm = 0.5 * dl0;
-        const double lp = 0.5 * dl1;
-        double PL[4], PR[4];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const double s0 = (q1[v] - q0[v]) / l0;
-            const double s1 = (q2[v] - q1[v]) / l1;
-            const double s2 = (q3[v] - q2[v]) / l2;
-            const double sl = rlimiter(lim, s1, s0);
-            const double sr = rlimiter(lim, s2, s1);
-            PL[v] = q1[v] + 1.0 * sl * lm;
-            PR[v] = q2[v] - 1.0 * sr * lp;
-        }
-        return flux_from_states64<RIEM>(g, PL, PR, nx, ny, int_l, fl);
-    } else {
-        // FP32 slopes of FP64 differences; face states = FP64 cell value + FP32 increment
-        const float il0 = __frcp_rn(0.5f * (float)(dlm1 + dl0));
-        const float il1 = __frcp_rn(0.5f * (float)(dl0 + dl1));
-        const float il2 = __frcp_rn(0.5f * (float)(dl1 + dl2));
-        const float lm = 0.5f * (float)dl0;
-        const float lp = 0.5f * (float)dl1;
-        double PL[4], PR[4];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const float s0 = (float)(q1[v] - q0[v]) * il0;
-            const float s1 = (float)(q2[v] - q1[v]) * il1;
-            const float s2 = (float)(q3[v] - q2[v]) * il2;
-            PL[v] = q1[v] + (double)(rlimiter32(lim, s1, s0) * lm);
-            PR[v] = q2[v] - (double)(rlimiter32(lim, s2, s1) * lp);
-        }
-        const bool bad = gas_state_bad(PL[0], PL[3]) || gas_state_bad(PR[0], PR[3]);
-        FluxState L, R;
-        phys64(g, PL, nx, ny, L);
-        phys64(g, PR, nx, ny, R);
-        const F4 F = riemann32<RIEM>(g, L, R, (float)nx, (float)ny);
-        fl[0] = F.r * int_l;
-        fl[1] = F.u * int_l;
-        fl[2] = F.v * int_l;
-        fl[3] = F.e * int_l;
-        return !bad;
-    }
+__device__ __forceinline__ bool face_flux(const Gas& g, const double* PL, const double* PR, double nx,
+                                          double ny, double int_l, double* X) {
+    if (PREC == 0) return flux_from_states64<RIEM>(g, PL, PR, nx, ny, int_l, X);
+    const bool bad = gas_state_bad(PL[0], PL[3]) || gas_state_bad(PR[0], PR[3]);
+    FluxState L, R;
+    phys64(g, PL, nx, ny, L);
+    phys64(g, PR, nx, ny, R);
+    const F4 F = riemann32<RIEM>(g, L, R, (float)nx, (float)ny);
+    X[0] = F.r * int_l;
+    X[1] = F.u * int_l;
+    X[2] = F.v * int_l;
+    X[3] = F.e * int_l;
+    return !bad;
 }
+
+// MUSCL pieces shared between faces (Lib_Reconstruction.f90:21-27): the slope of an
+// interface between cells a and b, (q_b - q_a) / (0.5 (dl_a + dl_b)), and the limited slope
+// of a cell, rlimiter(forward slope, backward slope). Every face of the reference recomputes
+// both for its two cells; here each is computed once per interface / cell, with the same
+// operations, so the face states are bitwise those of Convective_Flux.
+template <typename ST>
+__device__ __forceinline__ ST iface_slope(double qa, double qb, double dla, double dlb);
+template <>
+__device__ __forceinline__ double iface_slope<double>(double qa, double qb, double dla, double dlb) {
+    return (qb - qa) / (0.5 * (dla + dlb));
+}
+template <>
+__device__ __forceinline__ float iface_slope<float>(double qa, double qb, double dla, double dlb) {
+    return (float)(qb - qa) * __frcp_rn(0.5f * (float)(dla + dlb));
+}
+__device__ __forceinline__ double cell_sigma(int lim, double fwd, double bwd) { return rlimiter(lim, fwd, bwd); }
+__device__ __forceinline__ float cell_sigma(int lim, float fwd, float bwd) { return rlimiter32(lim, fwd, bwd); }
 
 // ------------------------------------------------------------------------------------------
 // Per-case finalisation by the last CTA of a case (called by all threads of the CTA).
@@ -418,21 +420,60 @@ __device__ __forceinline__ double cell_dt(const StageArgs& a, const double* P, c
 // ------------------------------------------------------------------------------------------
 // The stage kernel
 // ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
+}
+
+// Shared-memory layout of one tile (offsets in doubles).
+template <int PREC, int TX, int TY>
+struct Tile {
+    using ST = typename std::conditional<PREC == 0, double, float>::type;
+    static constexpr int W = TX + 4, H = TY + 4, AREA = W * H;
+    static constexpr int NSI = (TX + 3) * TY, NSJ = TX * (TY + 3);   // interfaces
+    static constexpr int NGI = (TX + 2) * TY, NGJ = TX * (TY + 2);   // limited cell slopes
+    static constexpr int NFI = (TX + 1) * TY, NFJ = TX * (TY + 1);   // faces
+    static constexpr int NC = TX * TY;                               // cells
+    static constexpr int oP = 0;                        // [4][H][W] primitive state + ghosts
+    static constexpr int oD = oP + 4 * AREA;            // [2][H][W] mean lengths dl(1), dl(2)
+    static constexpr int oC = oD + 2 * AREA;            // [6][NC]   U^n (4), sur, dt
+    static constexpr int oG = oC + 6 * NC;              // [3][NFI] + [3][NFJ] face nx, ny, len
+    static constexpr int nS = (int)((4 * (NSI + NSJ) * sizeof(ST) + 7) / 8);
+    static constexpr int nF = 4 * (NFI + NFJ);
+    static constexpr int oS = oG + 3 * (NFI + NFJ);     // interface slopes (ST), then face fluxes
+    static constexpr int oSG = oS + (nS > nF ? nS : nF);
+    static constexpr int nSG = (int)((4 * (NGI + NGJ) * sizeof(ST) + 7) / 8);
+    static constexpr int total = oSG + nSG;
+    static constexpr size_t bytes = sizeof(double) * (size_t)total;
+};
+
 template <int PREC, int RIEM, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
-    constexpr int W = TX + 4, H = TY + 4, AREA = W * H;
-    constexpr int NFI = (TX + 1) * TY, NFJ = TX * (TY + 1);
+__global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
+    using L = Tile<PREC, TX, TY>;
+    using ST = typename L::ST;
+    constexpr int W = L::W, AREA = L::AREA, NFI = L::NFI, NFJ = L::NFJ, NSI = L::NSI, NSJ = L::NSJ,
+                  NGI = L::NGI, NGJ = L::NGJ, NC = L::NC;
     extern __shared__ double smem[];
-    double* sP = smem;                  // [4][H][W]
-    double* sD = sP + 4 * AREA;         // [2][H][W]  mean lengths dl(1), dl(2)
-    double* sFi = sD + 2 * AREA;        // [4][TY][TX+1]
-    double* sFj = sFi + 4 * NFI;        // [4][TY+1][TX]
+    double* sP = smem + L::oP;
+    double* sD = smem + L::oD;
+    double* sC = smem + L::oC;
+    double* sGi = smem + L::oG;            // i-face geometry [3][NFI]
+    double* sGj = sGi + 3 * NFI;           // j-face geometry [3][NFJ]
+    ST* sSi = reinterpret_cast<ST*>(smem + L::oS);   // [4][NSI]
+    ST* sSj = sSi + 4 * NSI;                          // [4][NSJ]
+    double* sFi = smem + L::oS;            // [4][NFI] (aliases the slopes once they are consumed)
+    double* sFj = sFi + 4 * NFI;           // [4][NFJ]
+    ST* sGI = reinterpret_cast<ST*>(smem + L::oSG);  // [4][NGI]
+    ST* sGJ = sGI + 4 * NGI;                          // [4][NGJ]
     __shared__ double red[(NT / 32) * 5];
     __shared__ double tile_part[5];
     __shared__ int s_flag;
     const int tid = threadIdx.x;
     const Gas& g = a.gas;
-    if (tid == 0 && blockIdx.x == 0 && a.launch_flag) *a.launch_flag = 1;
+    const int lim = a.limiter;
 
     for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
         const WorkItem w = a.items[it];
@@ -442,77 +483,113 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
         const int ni = B.ni, nj = B.nj, i0 = w.i0, j0 = w.j0;
         const double* Pin = a.Pin + B.oc;
         const long long pc = B.pc;
+        const double* scb = a.sc + 2 * B.oc;   // 8-plane scalar pool of the block
 
-        // ---- 1. stage P (interior + donor ghosts) and dl into shared memory ----------------
+        // ---- 1. asynchronous loads of everything the tile reads --------------------------
         for (int idx = tid; idx < AREA; idx += NT) {
             const int r = idx / W, c = idx - r * W;
-            const bool hr = (r < 2 || r >= TY + 2), hc = (c < 2 || c >= TX + 2);
-            if (hr && hc) continue;   // corners of the cross are never read
+            if ((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2)) continue;
             const int ii = i0 - 2 + c, jj = j0 - 2 + r;
             const bool inI = (ii >= 0 && ii < ni), inJ = (jj >= 0 && jj < nj);
             if (ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1) {
-                const long long gidx = B.og + (long long)(jj + 2) * (ni + 4) + (ii + 2);
-                sD[idx] = a.dl[gidx];
-                sD[AREA + idx] = a.dl[gidx + B.pg];
+                const double* src = a.dl + B.og + (long long)(jj + 2) * (ni + 4) + (ii + 2);
+                cp_async8(sD + idx, src);
+                cp_async8(sD + AREA + idx, src + B.pg);
             }
             if (inI && inJ) {
-                const long long ci = (long long)jj * ni + ii;
+                const double* src = Pin + (long long)jj * ni + ii;
 #pragma unroll
-                for (int v = 0; v < 4; ++v) sP[v * AREA + idx] = Pin[v * pc + ci];
+                for (int v = 0; v < 4; ++v) cp_async8(sP + v * AREA + idx, src + v * pc);
             } else if (inI != inJ) {
                 int f, gd, k;
                 if (!inI) { f = ii < 0 ? 1 : 2; gd = ii < 0 ? -ii : ii - ni + 1; k = jj; }
                 else      { f = jj < 0 ? 3 : 4; gd = jj < 0 ? -jj : jj - nj + 1; k = ii; }
                 if (gd > 2) continue;
                 const EdgeRec e = a.edges[B.eo[f - 1] + k];
-                if (e.type == 101) {   // Ghost_Connection (Lib_Ghost.f90:143-160)
+                if (e.type == 101) {   // Ghost_Connection (Lib_Ghost.f90:143-160): donor cells
                     const DBlock S = a.blocks[e.bs];
                     const int si = e.is + guide_i(e.fs) * (gd - 1) - 1;
                     const int sj = e.js + guide_j(e.fs) * (gd - 1) - 1;
-                    const long long ci = (long long)sj * S.ni + si;
+                    const double* src = a.Pin + S.oc + (long long)sj * S.ni + si;
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) sP[v * AREA + idx] = a.Pin[S.oc + v * S.pc + ci];
+                    for (int v = 0; v < 4; ++v) cp_async8(sP + v * AREA + idx, src + v * S.pc);
                 }
             }
         }
+        for (int k = tid; k < NC; k += NT) {
+            const int row = k / TX, col = k - row * TX;
+            const int ii = i0 + col, jj = j0 + row;
+            if (ii >= ni || jj >= nj) continue;
+            const long long cg = (long long)jj * ni + ii;
+            cp_async8(sC + 4 * NC + k, scb + cg);                                  // sur
+            if (!a.time_accurate) cp_async8(sC + 5 * NC + k, scb + pc + cg);       // dt
+            if (!a.first) {
+                const double* po = a.PO + B.oc + cg;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) cp_async8(sC + v * NC + k, po + v * pc);
+            }
+        }
+        for (int f = tid; f < NFI + NFJ; f += NT) {
+            if (f < NFI) {
+                const int row = f / (TX + 1), col = f - row * (TX + 1);
+                const int jj = j0 + row, F = i0 + col;
+                if (jj >= nj || F > ni) continue;
+                const double* src = a.fi + B.ofi + (long long)jj * (ni + 1) + F;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) cp_async8(sGi + q * NFI + f, src + q * B.pfi);
+            } else {
+                const int ff = f - NFI;
+                const int row = ff / TX, col = ff - row * TX;
+                const int ii = i0 + col, G = j0 + row;
+                if (ii >= ni || G > nj) continue;
+                const double* src = a.fj + B.ofj + (long long)G * ni + ii;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) cp_async8(sGj + q * NFJ + ff, src + q * B.pfj);
+            }
+        }
+        cp_async_wait_all();
         __syncthreads();
 
-        // ---- 1b. non-connection ghost cells from the tile's own cells ----------------------
+        // ---- 2. ghost cells that follow from the tile's own cells --------------------------
         {
-            // edges touched by the tile: left (f=1), right (f=2), bottom (f=3), top (f=4)
             const int nrow = min(TY, nj - j0), ncol = min(TX, ni - i0);
             const int nl = (i0 == 0) ? nrow : 0;
             const int nr = (i0 + TX >= ni) ? nrow : 0;
             const int nb = (j0 == 0) ? ncol : 0;
             const int nt = (j0 + TY >= nj) ? ncol : 0;
             for (int t = tid; t < nl + nr + nb + nt; t += NT) {
-                int f, k, cb, rb, sc_, sr_;   // boundary cell position, outward step
-                if (t < nl) { f = 1; rb = 2 + t; cb = 2; k = j0 + t; sc_ = -1; sr_ = 0; }
-                else if (t < nl + nr) { f = 2; rb = 2 + (t - nl); cb = (ni - 1 - i0) + 2; k = j0 + (t - nl); sc_ = 1; sr_ = 0; }
-                else if (t < nl + nr + nb) { f = 3; cb = 2 + (t - nl - nr); rb = 2; k = i0 + (t - nl - nr); sc_ = 0; sr_ = -1; }
-                else { f = 4; cb = 2 + (t - nl - nr - nb); rb = (nj - 1 - j0) + 2; k = i0 + (t - nl - nr - nb); sc_ = 0; sr_ = 1; }
-                const EdgeRec e = a.edges[B.eo[f - 1] + k];
-                if (e.type == 101) continue;
+                int f, k, cb, rb, dc, dr, gidx;   // boundary cell, outward step, face geometry index
+                const double* gn;
+                int gstride;
+                if (t < nl) {
+                    f = 1; rb = 2 + t; cb = 2; k = j0 + t; dc = -1; dr = 0;
+                    gn = sGi; gstride = NFI; gidx = t * (TX + 1);
+                } else if (t < nl + nr) {
+                    const int u = t - nl;
+                    f = 2; rb = 2 + u; cb = (ni - 1 - i0) + 2; k = j0 + u; dc = 1; dr = 0;
+                    gn = sGi; gstride = NFI; gidx = u * (TX + 1) + (ni - i0);
+                } else if (t < nl + nr + nb) {
+                    const int u = t - nl - nr;
+                    f = 3; cb = 2 + u; rb = 2; k = i0 + u; dc = 0; dr = -1;
+                    gn = sGj; gstride = NFJ; gidx = u;
+                } else {
+                    const int u = t - nl - nr - nb;
+                    f = 4; cb = 2 + u; rb = (nj - 1 - j0) + 2; k = i0 + u; dc = 0; dr = 1;
+                    gn = sGj; gstride = NFJ; gidx = (nj - j0) * TX + u;
+                }
+                const int type = a.edges[B.eo[f - 1] + k].type;
+                if (type == 101) continue;
                 const int b0 = rb * W + cb;
-                const int s1 = b0 + sr_ * W + sc_;       // ghost layer 1
-                const int s2 = s1 + sr_ * W + sc_;       // ghost layer 2
-                const int in1 = b0 - sr_ * W - sc_;      // interior neighbours
-                const int in2 = in1 - sr_ * W - sc_;
-                if (e.type == 300) {   // Ghost_Symmetry (Lib_Ghost.f90:163-196)
-                    double nx, ny;
-                    if (f <= 2) {
-                        const long long fidx = B.ofi + (long long)k * (ni + 1) + (f == 1 ? 0 : ni);
-                        nx = a.fi[fidx]; ny = a.fi[fidx + B.pfi];
-                    } else {
-                        const long long fidx = B.ofj + (long long)(f == 3 ? 0 : nj) * ni + k;
-                        nx = a.fj[fidx]; ny = a.fj[fidx + B.pfj];
-                    }
+                const int s1 = b0 + dr * W + dc, s2 = s1 + dr * W + dc;
+                const int in1 = b0 - dr * W - dc, in2 = in1 - dr * W - dc;
+                if (type == 300) {   // Ghost_Symmetry (Lib_Ghost.f90:163-196)
+                    const double nx = gn[gidx], ny = gn[gstride + gidx];
                     const double vx = sP[AREA + b0], vy = sP[2 * AREA + b0];
                     const double udotn = vx * nx + vy * ny;
                     const double gx = vx - 2.0 * udotn * nx, gy = vy - 2.0 * udotn * ny;
                     sP[s1] = sP[b0]; sP[AREA + s1] = gx; sP[2 * AREA + s1] = gy; sP[3 * AREA + s1] = sP[3 * AREA + b0];
                     sP[s2] = sP[b0]; sP[AREA + s2] = gx; sP[2 * AREA + s2] = gy; sP[3 * AREA + s2] = sP[3 * AREA + b0];
-                } else if (e.type == 0 || e.type == 401 || e.type == 405 || e.type == 406 || e.type < 0) {
+                } else if (type == 0 || type == 401 || type == 405 || type == 406 || type < 0) {
 #pragma unroll
                     for (int v = 0; v < 4; ++v) {   // Ghost_ZG_Extrapolate (:199-219)
                         sP[v * AREA + s1] = sP[v * AREA + b0];
@@ -531,106 +608,110 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
         }
         __syncthreads();
 
-        // ---- 2. face fluxes ----------------------------------------------------------------
-        for (int f = tid; f < NFI + NFJ; f += NT) {
-            double X[4] = {0.0, 0.0, 0.0, 0.0};
-            bool ok = true;
-            int bad_i = 0, bad_j = 0;
-            if (f < NFI) {
-                const int row = f / (TX + 1), col = f - row * (TX + 1);
-                const int jj = j0 + row, F = i0 + col;   // face F between 1-based cells F, F+1
-                if (jj >= nj || F > ni) continue;
-                const long long fidx = B.ofi + (long long)jj * (ni + 1) + F;
-                const double nx = a.fi[fidx], ny = a.fi[fidx + B.pfi], ln = a.fi[fidx + 2 * B.pfi];
-                const int r = row + 2;
-                const int base = r * W + col;   // smem column of cell F-2 (0-based)
-                const EdgeRec* e = nullptr;
-                if (F == 0) e = &a.edges[B.eo[0] + jj];
-                else if (F == ni) e = &a.edges[B.eo[1] + jj];
-                const int etype = e ? e->type : 101;
-                if (etype == 101) {
-                    double q[4][4];
+        // ---- 3. interface slopes ---------------------------------------------------------
+        for (int k = tid; k < NSI + NSJ; k += NT) {
+            if (k < NSI) {
+                const int r = k / (TX + 3), c = k - r * (TX + 3);
+                const int p0 = (r + 2) * W + c;
+                const double da = sD[p0], db = sD[p0 + 1];
 #pragma unroll
-                    for (int s = 0; s < 4; ++s)
-#pragma unroll
-                        for (int v = 0; v < 4; ++v) q[s][v] = sP[v * AREA + base + s];
-                    ok = interior_flux<PREC, RIEM>(g, a.limiter, q[0], q[1], q[2], q[3], sD[base],
-                                                   sD[base + 1], sD[base + 2], sD[base + 3], nx, ny, ln, X);
-                    bad_i = F; bad_j = jj + 1;
-                } else if (etype >= 0) {
-                    const int Fm = (F == 0) ? 1 : 2;
-                    const int cb = base + ((F == 0) ? 2 : 1);   // boundary cell
-                    const int ci = cb + ((F == 0) ? 1 : -1);    // interior neighbour
-                    double Bp[4], Ip[4];
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) { Bp[v] = sP[v * AREA + cb]; Ip[v] = sP[v * AREA + ci]; }
-                    const BCParam bp = (e->param >= 0) ? a.bcp[e->param] : BCParam{};
-                    bool done = true;
-                    if (etype == 400) bc_extrapolation(g, Bp, nx, ny, ln, X);
-                    else if (etype == 401) done = bc_stagnation(g, Fm, Bp, nx, ny, ln, bp, X);
-                    else if (etype == 405) done = bc_supersonic<RIEM>(g, a.limiter, Fm, Bp, Ip, nx, ny, ln, bp, X);
-                    else if (etype == 406) done = bc_outflow(g, Fm, Bp, nx, ny, ln, bp, X);
-                    else if (etype == 300) done = false;
-                    if (!done)
-                        bc_symmetry<RIEM>(g, a.limiter, Fm, Bp, Ip, 0.5 * sD[cb], 0.5 * sD[ci], nx, ny, ln, X);
-                }
-                if (!ok) record_error(cs, 4, B.local_b, bad_i, bad_j, a.irk);
-#pragma unroll
-                for (int v = 0; v < 4; ++v) sFi[v * NFI + row * (TX + 1) + col] = X[v];
+                for (int v = 0; v < 4; ++v)
+                    sSi[v * NSI + k] = iface_slope<ST>(sP[v * AREA + p0], sP[v * AREA + p0 + 1], da, db);
             } else {
-                const int ff = f - NFI;
-                const int row = ff / TX, col = ff - row * TX;
-                const int ii = i0 + col, G = j0 + row;   // face G between 1-based rows G, G+1
-                if (ii >= ni || G > nj) continue;
-                const long long fidx = B.ofj + (long long)G * ni + ii;
-                const double nx = a.fj[fidx], ny = a.fj[fidx + B.pfj], ln = a.fj[fidx + 2 * B.pfj];
-                const int c = col + 2;
-                const int base = row * W + c;   // smem row of cell G-2 (0-based)
-                const EdgeRec* e = nullptr;
-                if (G == 0) e = &a.edges[B.eo[2] + ii];
-                else if (G == nj) e = &a.edges[B.eo[3] + ii];
-                const int etype = e ? e->type : 101;
-                if (etype == 101) {
-                    double q[4][4];
+                const int kk = k - NSI;
+                const int r = kk / TX, c = kk - r * TX;
+                const int p0 = r * W + c + 2;
+                const double da = sD[AREA + p0], db = sD[AREA + p0 + W];
 #pragma unroll
-                    for (int s = 0; s < 4; ++s)
-#pragma unroll
-                        for (int v = 0; v < 4; ++v) q[s][v] = sP[v * AREA + base + s * W];
-                    ok = interior_flux<PREC, RIEM>(g, a.limiter, q[0], q[1], q[2], q[3], sD[AREA + base],
-                                                   sD[AREA + base + W], sD[AREA + base + 2 * W],
-                                                   sD[AREA + base + 3 * W], nx, ny, ln, X);
-                    bad_i = ii + 1; bad_j = G;
-                } else if (etype >= 0) {
-                    const int Fm = (G == 0) ? 3 : 4;
-                    const int cb = base + ((G == 0) ? 2 : 1) * W;
-                    const int ci = cb + ((G == 0) ? W : -W);
-                    double Bp[4], Ip[4];
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) { Bp[v] = sP[v * AREA + cb]; Ip[v] = sP[v * AREA + ci]; }
-                    const BCParam bp = (e->param >= 0) ? a.bcp[e->param] : BCParam{};
-                    bool done = true;
-                    if (etype == 400) bc_extrapolation(g, Bp, nx, ny, ln, X);
-                    else if (etype == 401) done = bc_stagnation(g, Fm, Bp, nx, ny, ln, bp, X);
-                    else if (etype == 405) done = bc_supersonic<RIEM>(g, a.limiter, Fm, Bp, Ip, nx, ny, ln, bp, X);
-                    else if (etype == 406) done = bc_outflow(g, Fm, Bp, nx, ny, ln, bp, X);
-                    else if (etype == 300) done = false;
-                    if (!done)
-                        bc_symmetry<RIEM>(g, a.limiter, Fm, Bp, Ip, 0.5 * sD[AREA + cb], 0.5 * sD[AREA + ci], nx, ny, ln, X);
-                }
-                if (!ok) record_error(cs, 4, B.local_b, bad_i, bad_j, a.irk);
-#pragma unroll
-                for (int v = 0; v < 4; ++v) sFj[v * NFJ + row * TX + col] = X[v];
+                for (int v = 0; v < 4; ++v)
+                    sSj[v * NSJ + kk] = iface_slope<ST>(sP[v * AREA + p0], sP[v * AREA + p0 + W], da, db);
             }
         }
         __syncthreads();
 
-        // ---- 3. residual, sources, RK update (+ next dt and residual norm) ------------------
+        // ---- 4. limited slope of every cell next to a face of the tile -------------------
+        for (int k = tid; k < NGI + NGJ; k += NT) {
+            if (k < NGI) {
+                const int r = k / (TX + 2), c = k - r * (TX + 2);   // cell at smem column c+1
+                const int sfw = r * (TX + 3) + c + 1, sbw = sfw - 1;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) sGI[v * NGI + k] = cell_sigma(lim, sSi[v * NSI + sfw], sSi[v * NSI + sbw]);
+            } else {
+                const int kk = k - NGI;
+                const int r = kk / TX, c = kk - r * TX;               // cell at smem row r+1
+                const int sfw = (r + 1) * TX + c, sbw = r * TX + c;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) sGJ[v * NGJ + kk] = cell_sigma(lim, sSj[v * NSJ + sfw], sSj[v * NSJ + sbw]);
+            }
+        }
+        __syncthreads();
+
+        // ---- 5. face fluxes (interior: Riemann on MUSCL states; boundary: BC_Fluxes) -----
+        for (int f = tid; f < NFI + NFJ; f += NT) {
+            double X[4] = {0.0, 0.0, 0.0, 0.0};
+            bool isI = f < NFI;
+            int row, col, F, G, ii, jj, edge_k = -1, Fm = 0;
+            if (isI) {
+                row = f / (TX + 1); col = f - row * (TX + 1);
+                jj = j0 + row; F = i0 + col; ii = F; G = 0;
+                if (jj >= nj || F > ni) continue;
+                if (F == 0) { Fm = 1; edge_k = jj; } else if (F == ni) { Fm = 2; edge_k = jj; }
+            } else {
+                const int ff = f - NFI;
+                row = ff / TX; col = ff - row * TX;
+                ii = i0 + col; G = j0 + row; jj = G; F = 0;
+                if (ii >= ni || G > nj) continue;
+                if (G == 0) { Fm = 3; edge_k = ii; } else if (G == nj) { Fm = 4; edge_k = ii; }
+            }
+            const int fl = isI ? f : f - NFI;
+            const double* gq = isI ? sGi : sGj;
+            const int gs = isI ? NFI : NFJ;
+            const double nx = gq[fl], ny = gq[gs + fl], ln = gq[2 * gs + fl];
+            const int etype = Fm ? a.edges[B.eo[Fm - 1] + edge_k].type : 101;
+            const int dstep = isI ? 1 : W;                       // smem step along the direction
+            const int pL = isI ? (row + 2) * W + col + 1 : (row + 1) * W + col + 2;   // left cell
+            const double* dlp = sD + (isI ? 0 : AREA);
+            if (etype == 101) {
+                const ST* sg = isI ? sGI : sGJ;
+                const int ng = isI ? NGI : NGJ;
+                const int gL = isI ? row * (TX + 2) + col : row * TX + col;
+                const int gR = gL + (isI ? 1 : TX);
+                const double lm = 0.5 * dlp[pL], lp = 0.5 * dlp[pL + dstep];
+                double QL[4], QR[4];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    QL[v] = sP[v * AREA + pL] + (double)(1.0 * sg[v * ng + gL] * lm);
+                    QR[v] = sP[v * AREA + pL + dstep] - (double)(1.0 * sg[v * ng + gR] * lp);
+                }
+                if (!face_flux<PREC, RIEM>(g, QL, QR, nx, ny, ln, X))
+                    record_error(cs, 4, B.local_b, isI ? F : ii + 1, isI ? jj + 1 : G, a.irk);
+            } else if (etype >= 0) {
+                const bool minside = (Fm == 1 || Fm == 3);
+                const int cb = minside ? pL + dstep : pL;        // boundary cell
+                const int ci = minside ? cb + dstep : cb - dstep; // interior neighbour
+                Q4 Bp, Ip;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) { Bp.v[v] = sP[v * AREA + cb]; Ip.v[v] = sP[v * AREA + ci]; }
+                const int prm = a.edges[B.eo[Fm - 1] + edge_k].param;
+                const Q4 q = bc_face<RIEM>(g, lim, etype, Fm, Bp, Ip, dlp[cb], dlp[ci], nx, ny, ln,
+                                           prm >= 0 ? a.bcp + prm : nullptr);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) X[v] = q.v[v];
+            }
+            double* dst = isI ? sFi + fl : sFj + fl;
+            const int fs = isI ? NFI : NFJ;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) dst[v * fs] = X[v];
+        }
+        __syncthreads();
+
+        // ---- 6. residual, sources, RK update (+ next dt and residual norm) ----------------
         double acc[5] = {0.0, 0.0, 0.0, 0.0, 1e300};
         const double dt_case = __ldcg(&cs->dt_step);
         const long long iter_next = __ldcg(&cs->iter) + (a.first ? 1 : 0) + 1;
         const int ndir = a.cases[w.case_id].ndir;
-        for (int cidx = tid; cidx < TX * TY; cidx += NT) {
-            const int row = cidx / TX, col = cidx - row * TX;
+        for (int k = tid; k < NC; k += NT) {
+            const int row = k / TX, col = k - row * TX;
             const int ii = i0 + col, jj = j0 + row;
             if (ii >= ni || jj >= nj) continue;
             const int i1 = ii + 1, j1 = jj + 1;
@@ -653,8 +734,7 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
                 r[v] = x;
             }
             const long long cg = (long long)jj * ni + ii;
-            const double* scb = a.sc + 2 * B.oc;   // 8-plane scalar pool
-            const double sur = scb[cg];
+            const double sur = sC[4 * NC + k];
             double P[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) P[v] = sP[v * AREA + sidx];
@@ -681,16 +761,10 @@ __global__ void __launch_bounds__(NT) stage_kernel(const StageArgs a) {
                 for (int v = 0; v < 4; ++v) r[v] = r[v] - S[v] * sur;
             }
             // Compute_Cons_NoIRS (Lib_Newstate.f90:131-159)
-            const double dt = a.time_accurate ? dt_case : scb[pc + cg];
+            const double dt = a.time_accurate ? dt_case : sC[5 * NC + k];
             double PO[4];
-            if (a.first) {
 #pragma unroll
-                for (int v = 0; v < 4; ++v) PO[v] = P[v];
-            } else {
-                const double* po = a.PO + B.oc;
-#pragma unroll
-                for (int v = 0; v < 4; ++v) PO[v] = po[v * pc + cg];
-            }
+            for (int v = 0; v < 4; ++v) PO[v] = a.first ? P[v] : sC[v * NC + k];
             double res[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) res[v] = -r[v] / sur * dt * 1.0;
@@ -789,7 +863,7 @@ __global__ void resume_kernel(CaseState* cs, int n, int* launch_flag) {
 // ------------------------------------------------------------------------------------------
 template <int PREC, int RIEM, int TX, int TY, int NT>
 static cudaError_t launch_stage_t(const StageArgs& a, int grid, cudaStream_t s) {
-    constexpr size_t smem = sizeof(double) * (6 * (TX + 4) * (TY + 4) + 4 * (TX + 1) * TY + 4 * TX * (TY + 1));
+    constexpr size_t smem = Tile<PREC, TX, TY>::bytes;
     auto k = stage_kernel<PREC, RIEM, TX, TY, NT>;
     static bool attr_set = false;
     if (!attr_set) {
@@ -803,7 +877,7 @@ static cudaError_t launch_stage_t(const StageArgs& a, int grid, cudaStream_t s) 
 
 template <int PREC, int RIEM, int TX, int TY, int NT>
 static int occupancy_t() {
-    constexpr size_t smem = sizeof(double) * (6 * (TX + 4) * (TY + 4) + 4 * (TX + 1) * TY + 4 * TX * (TY + 1));
+    constexpr size_t smem = Tile<PREC, TX, TY>::bytes;
     auto k = stage_kernel<PREC, RIEM, TX, TY, NT>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int n = 0;
@@ -813,9 +887,9 @@ static int occupancy_t() {
 
 #define Q2D_TILE_SWITCH(TILE, CALL)                                          \
     switch (TILE) {                                                          \
-        case 1: CALL(32, 15, 512); break;                                    \
-        case 2: CALL(64, 7, 512); break;                                     \
-        default: CALL(32, 7, 256); break;                                    \
+        case 1: CALL(32, 8, 256); break;                                     \
+        case 2: CALL(64, 4, 256); break;                                     \
+        default: CALL(32, 10, 256); break;                                   \
     }
 
 cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int grid, cudaStream_t s) {

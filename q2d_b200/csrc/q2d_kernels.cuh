@@ -6,7 +6,7 @@
 namespace q2d {
 
 // Tile configurations of the stage kernel (tile id -> TX x TY cells, NT threads):
-//   0: 32 x 7, 256 threads   1: 32 x 15, 512 threads   2: 64 x 7, 512 threads
+//   0: 32 x 10, 256 threads   1: 32 x 8, 256 threads   2: 64 x 4, 256 threads
 constexpr int kNumTiles = 3;
 void tile_dims(int tile, int* tx, int* ty, int* nt);
 
