@@ -452,6 +452,7 @@ int q2d_gpu_create(q2d_ctx** out, const q2d_options* opt) {
     ctx->gas.cp = opt->gas_gamma * opt->gas_R / (opt->gas_gamma - 1.0);
     ctx->gas.cv = opt->gas_R / (opt->gas_gamma - 1.0);
     ctx->gas.gfac = opt->gas_gamma / (opt->gas_gamma - 1.0);
+    ctx->gas.igm1 = 1.0 / (opt->gas_gamma - 1.0);
     cudaGetDevice(&ctx->device);
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {

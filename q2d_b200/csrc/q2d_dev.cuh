@@ -81,6 +81,7 @@ struct WorkItem {
 struct Gas {
     double R, gamma, gm1, cp, cv;
     double gfac;   // gamma / (gamma - 1)
+    double igm1;   // 1 / (gamma - 1)
 };
 
 struct StageArgs {
@@ -202,6 +203,35 @@ __device__ __forceinline__ float rlimiter32(int lim, float x, float y) {
         }
     }
 }
+
+
+// Compile-time limiter selection for the hot loops (same arithmetic as rlimiter/rlimiter32).
+template <int LIM>
+__device__ __forceinline__ double lim64(double x, double y) {
+    if (LIM == 1) {
+        double r = 0.0;
+        if (x * y < 0.0) return r;
+        r = x;
+        if (fabs(x) > fabs(y)) r = y;
+        return r;
+    }
+    if (LIM == 0) return 0.0;
+    const double ru = y / (x + 1e-30);
+    double phi;
+    if (LIM == 2) phi = (ru + fabs(ru)) / (1.0 + fabs(ru));
+    else if (LIM == 3) phi = (ru * ru + ru) / (1.0 + ru * ru);
+    else if (LIM == 4) phi = dmax(0.0, dmin(dmin(2.0 * ru, 0.5 * (1.0 + ru)), 2.0));
+    else if (LIM == 5) phi = dmax(dmax(0.0, dmin(2.0 * ru, 1.0)), dmin(ru, 2.0));
+    else {
+        const double a = (2.0 + ru) / 3.0;
+        const double inner = dmin(dmin(2.0 * ru, (2.0 + ru) / 3.0), 1.6);
+        const double mid = dmax(dmax(-0.5 * ru, 0.0), inner);
+        phi = dmax(0.0, dmin(a, mid));
+    }
+    return phi * x;
+}
+template <int LIM>
+__device__ __forceinline__ float lim32(float x, float y) { return rlimiter32(LIM, x, y); }
 
 struct F4 { double r, u, v, e; };
 
@@ -401,6 +431,8 @@ __device__ __forceinline__ void phys64(const Gas& g, const double* q, double nx,
     s.F.e = s.un * (g.gfac * s.p + 0.5 * s.r * (s.u * s.u + s.v * s.v));
 }
 
+__device__ __forceinline__ float frcp(float x) { return __fdividef(1.0f, x); }
+
 template <int RIEM>
 __device__ __forceinline__ F4 riemann32(const Gas& g, const FluxState& L, const FluxState& R,
                                         float nx, float ny) {
@@ -409,7 +441,8 @@ __device__ __forceinline__ F4 riemann32(const Gas& g, const FluxState& L, const 
     const float ul = (float)L.u, vl = (float)L.v, ur = (float)R.u, vr = (float)R.v;
     const float pl = (float)L.p, pr = (float)R.p;
     const float gam = (float)g.gamma;
-    const float irl = __frcp_rn(rl), irr = __frcp_rn(rr);
+    const float igm1 = (float)(1.0 / g.gm1);
+    const float irl = frcp(rl), irr = frcp(rr);
     const float al = sqrtf(gam * pl * irl), ar = sqrtf(gam * pr * irr);
     const float unl = (float)L.un, unr = (float)R.un;
     // jumps, formed in FP64
@@ -420,8 +453,8 @@ __device__ __forceinline__ F4 riemann32(const Gas& g, const FluxState& L, const 
         const double dU0 = R.r - L.r;
         const double dU1 = R.r * R.u - L.r * L.u;
         const double dU2 = R.r * R.v - L.r * L.v;
-        const double dU3 = (R.p / g.gm1 + 0.5 * R.r * (R.u * R.u + R.v * R.v)) -
-                           (L.p / g.gm1 + 0.5 * L.r * (L.u * L.u + L.v * L.v));
+        const double dU3 = (R.p * g.igm1 + 0.5 * R.r * (R.u * R.u + R.v * R.v)) -
+                           (L.p * g.igm1 + 0.5 * L.r * (L.u * L.u + L.v * L.v));
         const double hA = 0.5 * (double)A;
         F4 F;
         F.r = 0.5 * (L.F.r + R.F.r) - hA * (double)(float)dU0;
@@ -432,7 +465,7 @@ __device__ __forceinline__ F4 riemann32(const Gas& g, const FluxState& L, const 
     }
     // Roe averages (constant cp: gamma_roe = gamma, a^2 = (gamma-1)(h0 - |V|^2/2))
     const float srL = sqrtf(rl), srR = sqrtf(rr);
-    const float isr = __frcp_rn(srL + srR);
+    const float isr = frcp(srL + srR);
     const float u_roe = (srR * ur + srL * ul) * isr;
     const float v_roe = (srR * vr + srL * vl) * isr;
     const float gf = (float)g.gfac;
@@ -444,14 +477,14 @@ __device__ __forceinline__ F4 riemann32(const Gas& g, const FluxState& L, const 
     const float S1 = fminf(fminf(0.0f, unl - al), un_roe - a_roe);
     const float S4 = fmaxf(fmaxf(0.0f, unr + ar), un_roe + a_roe);
     if (RIEM == 1) {   // HLLE: F = Fbar - (S4+S1)/(2(S4-S1)) dF + S1 S4/(S4-S1) dU
-        const float inv = __frcp_rn(S4 - S1);
+        const float inv = frcp(S4 - S1);
         const float c1 = 0.5f * (S4 + S1) * inv;
         const float c2 = S1 * S4 * inv;
         const double dU0 = R.r - L.r;
         const double dU1 = R.r * R.u - L.r * L.u;
         const double dU2 = R.r * R.v - L.r * L.v;
-        const double dU3 = (R.p / g.gm1 + 0.5 * R.r * (R.u * R.u + R.v * R.v)) -
-                           (L.p / g.gm1 + 0.5 * L.r * (L.u * L.u + L.v * L.v));
+        const double dU3 = (R.p * g.igm1 + 0.5 * R.r * (R.u * R.u + R.v * R.v)) -
+                           (L.p * g.igm1 + 0.5 * L.r * (L.u * L.u + L.v * L.v));
         F4 F;
         F.r = 0.5 * (L.F.r + R.F.r) + (double)(c2 * (float)dU0 - c1 * (float)(R.F.r - L.F.r));
         F.u = 0.5 * (L.F.u + R.F.u) + (double)(c2 * (float)dU1 - c1 * (float)(R.F.u - L.F.u));
@@ -462,13 +495,13 @@ __device__ __forceinline__ F4 riemann32(const Gas& g, const FluxState& L, const 
     // HLLC (Batten), jump form
     if (S1 >= 0.0f) return L.F;
     const float D = rl * (S1 - unl) - rr * (S4 - unr);
-    const float sm_unl = (dp - rr * (S4 - unr) * dun) * __frcp_rn(D);   // S* - un_L
+    const float sm_unl = (dp - rr * (S4 - unr) * dun) * frcp(D);   // S* - un_L
     const float Sstar = unl + sm_unl;
     if (Sstar >= 0.0f) {
-        const float inv = __frcp_rn(S1 - Sstar);
+        const float inv = frcp(S1 - Sstar);
         const float q = sm_unl * inv;
         const float dps = rl * (S1 - unl) * sm_unl;                      // p* - p_L
-        const float e0l = pl * irl / (gam - 1.0f) + 0.5f * (ul * ul + vl * vl);
+        const float e0l = pl * irl * igm1 + 0.5f * (ul * ul + vl * vl);
         const float d0 = rl * q;
         const float d1 = rl * ul * q + dps * nx * inv;
         const float d2 = rl * vl * q + dps * ny * inv;
@@ -481,11 +514,11 @@ __device__ __forceinline__ F4 riemann32(const Gas& g, const FluxState& L, const 
         return F;
     }
     if (S4 > 0.0f) {
-        const float inv = __frcp_rn(S4 - Sstar);
+        const float inv = frcp(S4 - Sstar);
         const float sm_unr = sm_unl - dun;                               // S* - un_R
         const float q = sm_unr * inv;
         const float dps = rr * (S4 - unr) * sm_unr;                      // p* - p_R
-        const float e0r = pr * irr / (gam - 1.0f) + 0.5f * (ur * ur + vr * vr);
+        const float e0r = pr * irr * igm1 + 0.5f * (ur * ur + vr * vr);
         const float d0 = rr * q;
         const float d1 = rr * ur * q + dps * nx * inv;
         const float d2 = rr * vr * q + dps * ny * inv;

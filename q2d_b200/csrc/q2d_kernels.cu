@@ -450,6 +450,90 @@ struct Tile {
     static constexpr size_t bytes = sizeof(double) * (size_t)total;
 };
 
+// Limited cell slopes of a tile (step 4 of the stage kernel), one limiter per instantiation.
+template <int LIM, int NT, int TX, int TY, typename ST>
+__device__ __forceinline__ void sigma_phase(const ST* sSi, const ST* sSj, ST* sGI, ST* sGJ) {
+    constexpr int NSI = (TX + 3) * TY, NSJ = TX * (TY + 3);
+    constexpr int NGI = (TX + 2) * TY, NGJ = TX * (TY + 2);
+    for (int k = threadIdx.x; k < NGI; k += NT) {
+        const int r = k / (TX + 2), c = k - r * (TX + 2);   // cell at smem column c+1
+        const int sfw = r * (TX + 3) + c + 1;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            if constexpr (sizeof(ST) == 8) sGI[v * NGI + k] = lim64<LIM>(sSi[v * NSI + sfw], sSi[v * NSI + sfw - 1]);
+            else sGI[v * NGI + k] = lim32<LIM>(sSi[v * NSI + sfw], sSi[v * NSI + sfw - 1]);
+        }
+    }
+    for (int k = threadIdx.x; k < NGJ; k += NT) {
+        const int r = k / TX, c = k - r * TX;               // cell at smem row r+1
+        const int sfw = (r + 1) * TX + c, sbw = r * TX + c;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            if constexpr (sizeof(ST) == 8) sGJ[v * NGJ + k] = lim64<LIM>(sSj[v * NSJ + sfw], sSj[v * NSJ + sbw]);
+            else sGJ[v * NGJ + k] = lim32<LIM>(sSj[v * NSJ + sfw], sSj[v * NSJ + sbw]);
+        }
+    }
+}
+
+// Face fluxes of one direction of a tile (step 5 of the stage kernel). IDIR: i-faces
+// (F = i0..i0+TX on TY rows) or j-faces (G = j0..j0+TY on TX columns).
+template <int PREC, int RIEM, bool IDIR, int NT, int TX, int TY, typename ST>
+__device__ __forceinline__ void face_phase(const StageArgs& a, const DBlock& B, CaseState* cs, int i0,
+                                           int j0, const double* sP, const double* sD,
+                                           const double* sG, const ST* sg, double* sF) {
+    constexpr int W = TX + 4, AREA = W * (TY + 4);
+    constexpr int NF = IDIR ? (TX + 1) * TY : TX * (TY + 1);
+    constexpr int NG = IDIR ? (TX + 2) * TY : TX * (TY + 2);
+    constexpr int ROWLEN = IDIR ? TX + 1 : TX;
+    constexpr int DSTEP = IDIR ? 1 : W;
+    const int ni = B.ni, nj = B.nj;
+    const double* dlp = sD + (IDIR ? 0 : AREA);
+    for (int f = threadIdx.x; f < NF; f += NT) {
+        const int row = f / ROWLEN, col = f - row * ROWLEN;
+        int pos, lenn, k;        // face index along the direction, its limit, edge position
+        if (IDIR) { pos = i0 + col; lenn = ni; k = j0 + row; if (k >= nj || pos > ni) continue; }
+        else      { pos = j0 + row; lenn = nj; k = i0 + col; if (k >= ni || pos > nj) continue; }
+        const double nx = sG[f], ny = sG[NF + f], ln = sG[2 * NF + f];
+        const int pL = IDIR ? (row + 2) * W + col + 1 : (row + 1) * W + col + 2;   // left cell
+        double X[4];
+        int etype = 101, Fm = 0;
+        if (pos == 0 || pos == lenn) {
+            Fm = IDIR ? (pos == 0 ? 1 : 2) : (pos == 0 ? 3 : 4);
+            etype = a.edges[B.eo[Fm - 1] + k].type;
+        }
+        if (etype == 101) {
+            const int gL = IDIR ? row * (TX + 2) + col : row * TX + col;
+            const int gR = gL + (IDIR ? 1 : TX);
+            const double lm = 0.5 * dlp[pL], lp = 0.5 * dlp[pL + DSTEP];
+            double QL[4], QR[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                QL[v] = sP[v * AREA + pL] + (double)(1.0 * sg[v * NG + gL] * lm);
+                QR[v] = sP[v * AREA + pL + DSTEP] - (double)(1.0 * sg[v * NG + gR] * lp);
+            }
+            if (!face_flux<PREC, RIEM>(a.gas, QL, QR, nx, ny, ln, X))
+                record_error(cs, 4, B.local_b, IDIR ? pos : k + 1, IDIR ? k + 1 : pos, a.irk);
+        } else if (etype >= 0) {
+            const bool minside = (Fm == 1 || Fm == 3);
+            const int cb = minside ? pL + DSTEP : pL;         // boundary cell
+            const int ci = minside ? cb + DSTEP : cb - DSTEP; // interior neighbour
+            Q4 Bp, Ip;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) { Bp.v[v] = sP[v * AREA + cb]; Ip.v[v] = sP[v * AREA + ci]; }
+            const int prm = a.edges[B.eo[Fm - 1] + k].param;
+            const Q4 q = bc_face<RIEM>(a.gas, a.limiter, etype, Fm, Bp, Ip, dlp[cb], dlp[ci], nx, ny, ln,
+                                       prm >= 0 ? a.bcp + prm : nullptr);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) X[v] = q.v[v];
+        } else {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) X[v] = 0.0;
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) sF[v * NF + f] = X[v];
+    }
+}
+
 template <int PREC, int RIEM, int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
     using L = Tile<PREC, TX, TY>;
@@ -630,79 +714,20 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
         __syncthreads();
 
         // ---- 4. limited slope of every cell next to a face of the tile -------------------
-        for (int k = tid; k < NGI + NGJ; k += NT) {
-            if (k < NGI) {
-                const int r = k / (TX + 2), c = k - r * (TX + 2);   // cell at smem column c+1
-                const int sfw = r * (TX + 3) + c + 1, sbw = sfw - 1;
-#pragma unroll
-                for (int v = 0; v < 4; ++v) sGI[v * NGI + k] = cell_sigma(lim, sSi[v * NSI + sfw], sSi[v * NSI + sbw]);
-            } else {
-                const int kk = k - NGI;
-                const int r = kk / TX, c = kk - r * TX;               // cell at smem row r+1
-                const int sfw = (r + 1) * TX + c, sbw = r * TX + c;
-#pragma unroll
-                for (int v = 0; v < 4; ++v) sGJ[v * NGJ + kk] = cell_sigma(lim, sSj[v * NSJ + sfw], sSj[v * NSJ + sbw]);
-            }
+        switch (lim) {
+            case 0: sigma_phase<0, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+            case 1: sigma_phase<1, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+            case 2: sigma_phase<2, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+            case 3: sigma_phase<3, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+            case 4: sigma_phase<4, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+            case 5: sigma_phase<5, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+            default: sigma_phase<6, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
         }
         __syncthreads();
 
         // ---- 5. face fluxes (interior: Riemann on MUSCL states; boundary: BC_Fluxes) -----
-        for (int f = tid; f < NFI + NFJ; f += NT) {
-            double X[4] = {0.0, 0.0, 0.0, 0.0};
-            bool isI = f < NFI;
-            int row, col, F, G, ii, jj, edge_k = -1, Fm = 0;
-            if (isI) {
-                row = f / (TX + 1); col = f - row * (TX + 1);
-                jj = j0 + row; F = i0 + col; ii = F; G = 0;
-                if (jj >= nj || F > ni) continue;
-                if (F == 0) { Fm = 1; edge_k = jj; } else if (F == ni) { Fm = 2; edge_k = jj; }
-            } else {
-                const int ff = f - NFI;
-                row = ff / TX; col = ff - row * TX;
-                ii = i0 + col; G = j0 + row; jj = G; F = 0;
-                if (ii >= ni || G > nj) continue;
-                if (G == 0) { Fm = 3; edge_k = ii; } else if (G == nj) { Fm = 4; edge_k = ii; }
-            }
-            const int fl = isI ? f : f - NFI;
-            const double* gq = isI ? sGi : sGj;
-            const int gs = isI ? NFI : NFJ;
-            const double nx = gq[fl], ny = gq[gs + fl], ln = gq[2 * gs + fl];
-            const int etype = Fm ? a.edges[B.eo[Fm - 1] + edge_k].type : 101;
-            const int dstep = isI ? 1 : W;                       // smem step along the direction
-            const int pL = isI ? (row + 2) * W + col + 1 : (row + 1) * W + col + 2;   // left cell
-            const double* dlp = sD + (isI ? 0 : AREA);
-            if (etype == 101) {
-                const ST* sg = isI ? sGI : sGJ;
-                const int ng = isI ? NGI : NGJ;
-                const int gL = isI ? row * (TX + 2) + col : row * TX + col;
-                const int gR = gL + (isI ? 1 : TX);
-                const double lm = 0.5 * dlp[pL], lp = 0.5 * dlp[pL + dstep];
-                double QL[4], QR[4];
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    QL[v] = sP[v * AREA + pL] + (double)(1.0 * sg[v * ng + gL] * lm);
-                    QR[v] = sP[v * AREA + pL + dstep] - (double)(1.0 * sg[v * ng + gR] * lp);
-                }
-                if (!face_flux<PREC, RIEM>(g, QL, QR, nx, ny, ln, X))
-                    record_error(cs, 4, B.local_b, isI ? F : ii + 1, isI ? jj + 1 : G, a.irk);
-            } else if (etype >= 0) {
-                const bool minside = (Fm == 1 || Fm == 3);
-                const int cb = minside ? pL + dstep : pL;        // boundary cell
-                const int ci = minside ? cb + dstep : cb - dstep; // interior neighbour
-                Q4 Bp, Ip;
-#pragma unroll
-                for (int v = 0; v < 4; ++v) { Bp.v[v] = sP[v * AREA + cb]; Ip.v[v] = sP[v * AREA + ci]; }
-                const int prm = a.edges[B.eo[Fm - 1] + edge_k].param;
-                const Q4 q = bc_face<RIEM>(g, lim, etype, Fm, Bp, Ip, dlp[cb], dlp[ci], nx, ny, ln,
-                                           prm >= 0 ? a.bcp + prm : nullptr);
-#pragma unroll
-                for (int v = 0; v < 4; ++v) X[v] = q.v[v];
-            }
-            double* dst = isI ? sFi + fl : sFj + fl;
-            const int fs = isI ? NFI : NFJ;
-#pragma unroll
-            for (int v = 0; v < 4; ++v) dst[v * fs] = X[v];
-        }
+        face_phase<PREC, RIEM, true, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sGi, sGI, sFi);
+        face_phase<PREC, RIEM, false, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sGj, sGJ, sFj);
         __syncthreads();
 
         // ---- 6. residual, sources, RK update (+ next dt and residual norm) ----------------
@@ -766,19 +791,36 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
 #pragma unroll
             for (int v = 0; v < 4; ++v) PO[v] = a.first ? P[v] : sC[v * NC + k];
             double res[4];
+            if (PREC == 0) {
 #pragma unroll
-            for (int v = 0; v < 4; ++v) res[v] = -r[v] / sur * dt * 1.0;
+                for (int v = 0; v < 4; ++v) res[v] = -r[v] / sur * dt * 1.0;
+            } else {
+                const double f = -dt / sur;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) res[v] = r[v] * f;
+            }
             double U0[4], U[4];
             U0[0] = PO[0]; U0[1] = PO[0] * PO[1]; U0[2] = PO[0] * PO[2];
-            U0[3] = PO[3] / g.gm1 + 0.5 * PO[0] * (PO[1] * PO[1] + PO[2] * PO[2]);
+            if (PREC == 0) {
+                U0[3] = PO[3] / g.gm1 + 0.5 * PO[0] * (PO[1] * PO[1] + PO[2] * PO[2]);
+                U[3] = P[3] / g.gm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
+            } else {
+                U0[3] = PO[3] * g.igm1 + 0.5 * PO[0] * (PO[1] * PO[1] + PO[2] * PO[2]);
+                U[3] = P[3] * g.igm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
+            }
             U[0] = P[0]; U[1] = P[0] * P[1]; U[2] = P[0] * P[2];
-            U[3] = P[3] / g.gm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
 #pragma unroll
             for (int v = 0; v < 4; ++v) U[v] = U0[v] + (U[v] - U0[v] + res[v]) * a.rk_c;
             double N[4];
             N[0] = U[0];
-            N[1] = U[1] / U[0];
-            N[2] = U[2] / U[0];
+            if (PREC == 0) {
+                N[1] = U[1] / U[0];
+                N[2] = U[2] / U[0];
+            } else {
+                const double ir = 1.0 / U[0];
+                N[1] = U[1] * ir;
+                N[2] = U[2] * ir;
+            }
             N[3] = g.gm1 * (U[3] - 0.5 * U[0] * (N[1] * N[1] + N[2] * N[2]));
             // Check_And_Fix_State (Lib_Newstate.f90:316-350)
             if (isnan(N[0]) || isnan(N[1]) || isnan(N[2]) || isnan(N[3]) || N[3] < 0.0)
