@@ -66,6 +66,8 @@ struct q2d_ctx {
     bool committed = false;
     bool dt_valid = false;
     int tile = 0;
+    int kernel = 1;       // 0: CTA-tile stage kernel, 1: warp-marching stage kernel
+    int march_h = 16;     // rows per warp-marching item
     int grid = 0;
     // device pools
     DevBuf<double> PA, PB, PC, SC, DL, FI, FJ, PART;
@@ -163,7 +165,10 @@ int enqueue_step(q2d_ctx* ctx, cudaStream_t s, int* nk) {
             else if (irk == 2) { a.Pin = ctx->PB.p; a.Pout = ctx->PC.p; }
             else { a.Pin = ctx->PC.p; a.Pout = ctx->PA.p; }
         }
-        CK(launch_stage(a, ctx->opt.precision, ctx->opt.riemann, ctx->tile, ctx->grid, s));
+        if (ctx->kernel == 1)
+            CK(launch_march(a, ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter, ctx->grid, s));
+        else
+            CK(launch_stage(a, ctx->opt.precision, ctx->opt.riemann, ctx->tile, ctx->grid, s));
         ++*nk;
     }
     if (n_rk == 1) {
@@ -177,7 +182,8 @@ int ensure_dt(q2d_ctx* ctx) {
     if (ctx->dt_valid) return Q2D_OK;
     StageArgs a = base_args(ctx);
     a.Pin = ctx->PA.p;
-    CK(launch_dt(a, ctx->tile, ctx->grid, ctx->stream));
+    if (ctx->kernel == 1) CK(launch_dt_march(a, ctx->grid, ctx->stream));
+    else CK(launch_dt(a, ctx->tile, ctx->grid, ctx->stream));
     ctx->launches += 1;
     ctx->dt_valid = true;
     return Q2D_OK;
@@ -323,8 +329,14 @@ int commit(q2d_ctx* ctx) {
         dcases[c].item_begin = (int)items.size();
         for (int gb : ctx->cases[c].blocks) {
             const HBlock& B = ctx->blocks[gb];
-            for (int j0 = 0; j0 < B.nj; j0 += TY)
-                for (int i0 = 0; i0 < B.ni; i0 += TX) items.push_back(WorkItem{gb, i0, j0, (int)c});
+            if (ctx->kernel == 1) {
+                for (int i0 = 0; i0 < B.ni; i0 += kMarchCols)
+                    for (int j0 = 0; j0 < B.nj; j0 += ctx->march_h)
+                        items.push_back(WorkItem{gb, i0, j0, (int)c, std::min(B.nj, j0 + ctx->march_h), 0});
+            } else {
+                for (int j0 = 0; j0 < B.nj; j0 += TY)
+                    for (int i0 = 0; i0 < B.ni; i0 += TX) items.push_back(WorkItem{gb, i0, j0, (int)c, 0, 0});
+            }
         }
         dcases[c].item_end = (int)items.size();
         dcases[c].ndir = ctx->blocks[ctx->cases[c].blocks[0]].nj == 1 ? 1 : 2;
@@ -394,8 +406,13 @@ int commit(q2d_ctx* ctx) {
     if (!edges.empty()) CK(cudaMemcpy(ctx->edges.p, edges.data(), sizeof(EdgeRec) * edges.size(), cudaMemcpyHostToDevice));
     if (!params.empty()) CK(cudaMemcpy(ctx->bcp.p, params.data(), sizeof(BCParam) * params.size(), cudaMemcpyHostToDevice));
     CK(cudaMemset(ctx->PART.p, 0, sizeof(double) * 5 * items.size()));
-    const int occ = std::max(1, stage_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->tile));
-    ctx->grid = (int)std::min<long long>((long long)items.size(), (long long)occ * ctx->num_sms);
+    if (ctx->kernel == 1) {
+        const int occ = std::max(1, march_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter));
+        ctx->grid = (int)std::min<long long>(((long long)items.size() + 3) / 4, (long long)occ * ctx->num_sms);
+    } else {
+        const int occ = std::max(1, stage_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->tile));
+        ctx->grid = (int)std::min<long long>((long long)items.size(), (long long)occ * ctx->num_sms);
+    }
     if (ctx->grid < 1) ctx->grid = 1;
     // release host copies of the big arrays
     for (HBlock& b : ctx->blocks) {
@@ -461,6 +478,10 @@ int q2d_gpu_create(q2d_ctx** out, const q2d_options* opt) {
     }
     const char* t = getenv("Q2D_TILE");
     if (t) ctx->tile = std::max(0, std::min(kNumTiles - 1, atoi(t)));
+    const char* kk = getenv("Q2D_KERNEL");
+    if (kk) ctx->kernel = atoi(kk) == 0 ? 0 : 1;
+    const char* mh = getenv("Q2D_MARCH_H");
+    if (mh) ctx->march_h = std::max(1, std::min(4096, atoi(mh)));
     *out = ctx;
     return Q2D_OK;
 }

@@ -74,8 +74,10 @@ struct CaseState {
 
 struct WorkItem {
     int block;   // global block id
-    int i0, j0;  // 0-based origin of the tile
+    int i0, j0;  // 0-based origin of the tile (tile kernel) or strip / first row (march kernel)
     int case_id;
+    int j1;      // march kernel: one past the last row of the item
+    int pad;
 };
 
 struct Gas {

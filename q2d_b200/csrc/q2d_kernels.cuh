@@ -12,6 +12,11 @@ void tile_dims(int tile, int* tx, int* ty, int* nt);
 
 cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int grid, cudaStream_t s);
 int stage_occupancy(int prec, int riem, int tile);
+// Warp-marching stage kernel (q2d_march.cuh): strips of 28 columns, item rows [j0, j1).
+constexpr int kMarchCols = 28;
+cudaError_t launch_march(const StageArgs& a, int prec, int riem, int lim, int grid, cudaStream_t s);
+int march_occupancy(int prec, int riem, int lim);
+cudaError_t launch_dt_march(const StageArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_dt(const StageArgs& a, int tile, int grid, cudaStream_t s);
 cudaError_t launch_copy(const double* src, double* dst, long long n, int* flag, cudaStream_t s);
 cudaError_t launch_resume(CaseState* cs, int n, int* flag, cudaStream_t s);

@@ -1,0 +1,10 @@
+// Instantiations of the warp-marching stage kernel: precision form 1, Riemann solver 1,
+// all seven limiters (compiled in separate units so they build in parallel).
+#include "q2d_march.cuh"
+
+namespace q2d {
+cudaError_t launch_march_p1_r1(const StageArgs& a, int lim, int grid, cudaStream_t s) {
+    return launch_march_t<1, 1>(a, lim, grid, s);
+}
+int march_occupancy_p1_r1(int lim) { return march_occupancy_t<1, 1>(lim); }
+}  // namespace q2d
