@@ -1,0 +1,197 @@
+"""The CPU oracle against the reference's own golden data and known answers.
+
+Pins (tests/golden, generated by tests/golden/make_golden.py from the reference tree):
+  - ShuOsher-LIMO3 limiter baselines: density written by the reference binary at N=400,
+    t=1.8, HLLC, RK3, CFL 0.5 (test/1D/ShuOsher-LIMO3/reference/baseline_*.dat);
+  - Sod79 exact solution table (test/1D/Sod79/reference/exact.txt) with the gates of
+    test/1D/Sod79/check.py (discretisation-error gates, shock position);
+  - exact Riemann solutions of the seeded 1-D workloads from the reference's exact solver
+    (test/common/pycheck/q2d_exact1d.py), and its Toro test-1 known answer.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from q2d_b200 import cases, make_options
+from oracle import oracle
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def run_oracle(cs, **kw):
+    s = oracle.solver(make_options(cs, **kw), [cs])
+    try:
+        info = s.solve(steps_per_call=200)
+        return s.prim(), info
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("lim", ["iord", "minmod", "vanleer", "mc"])
+def test_shuosher_matches_reference_binary(lim):
+    """The oracle reproduces the reference binary's Shu-Osher density to <= 1e-8 relative L1
+    (the baselines are printed with 10 significant digits) and <= 2e-7 max abs."""
+    ref = np.loadtxt(GOLD / f"shuosher_{lim}.txt")
+    cs = cases.shuosher()
+    P, info = run_oracle(cs, limiter=lim)
+    rho = P[0, :, 0]
+    assert np.allclose(cs.meta["xc"], ref[:, 0], atol=1e-9)
+    rel_l1 = np.abs(rho - ref[:, 1]).sum() / np.abs(ref[:, 1]).sum()
+    assert rel_l1 <= 1e-8, rel_l1
+    assert np.abs(rho - ref[:, 1]).max() <= 2e-7
+    assert info["todo"] == 3 and info["time"] >= 1.8
+
+
+def test_shuosher_negative_control():
+    """A perturbed closure (the table's gamma = cp/(cp-R) = 1.399996 instead of 1.4) must FAIL
+    the 1e-8 gate: the pin discriminates at the 1e-6 level."""
+    ref = np.loadtxt(GOLD / "shuosher_mc.txt")
+    R = 8314.46 / 28.970418
+    P, _ = run_oracle(cases.shuosher(gamma=1004.5 / (1004.5 - R)), limiter="mc")
+    rel_l1 = np.abs(P[0, :, 0] - ref[:, 1]).sum() / np.abs(ref[:, 1]).sum()
+    assert rel_l1 > 1e-7
+
+
+def test_sod79_exact_gates():
+    """Sod (rho 1/0.125, p 1/0.1) at 400 cells to t=0.2 with MC + HLLC, RK3, CFL 0.9:
+    relative L1 of rho and p against the reference's exact.txt within the check.py gates
+    (5e-3 / 3.5e-3) and the shock within 3 cells of x = 0.85043."""
+    ex = np.loadtxt(GOLD / "sod79_exact.txt")
+    cs = cases.riemann_1d(ni=400, nj=1, states=(1.0, 1.0, 0.125, 0.1), limiter="mc", t_end=0.2)
+    # the Sod79 case has BC 300 on every face (closed tube)
+    for r in cs.bcs:
+        r["type"] = 300
+    P, info = run_oracle(cs, cfl=0.9)
+    xc = 0.5 * (np.linspace(0, 1, 401)[:-1] + np.linspace(0, 1, 401)[1:])
+    rho, p = P[0, :, 0], P[0, :, 3]
+    re = np.interp(xc, ex[:, 0], ex[:, 1])
+    pe = np.interp(xc, ex[:, 0], ex[:, 3])
+    l1r = np.abs(rho - re).sum() / np.abs(re).sum()
+    l1p = np.abs(p - pe).sum() / np.abs(pe).sum()
+    assert l1r <= 5e-3 and l1p <= 3.5e-3, (l1r, l1p)
+    k = int(np.argmax(np.abs(np.diff(p[300:])))) + 300   # steepest pressure face right of the contact
+    assert abs(0.5 * (xc[k] + xc[k + 1]) - 0.85043) <= 3 * 0.0025
+
+
+def test_exact_riemann_seeded_workload():
+    """The seeded 1-D workload (1024 x 4, minmod + HLLC) against the reference's exact solver:
+    density L1 error of a first/second-order scheme at 1024 cells is a few 1e-3."""
+    d = np.load(GOLD / "riemann_exact.npz")
+    st = d["cfg1_states"]
+    rl, _, pl, rr, _, pr = st[:6]
+    cs = cases.riemann_1d(ni=int(st[6]), nj=4, states=(rl, pl, rr, pr), t_end=float(st[8]))
+    P, info = run_oracle(cs)
+    rho = P[:, :, 0].mean(axis=0)
+    l1 = np.abs(rho - d["cfg1_rho"]).mean() / np.abs(d["cfg1_rho"]).mean()
+    assert l1 <= 6e-3, l1
+    # the four rows of the quasi-1D block stay identical (symmetry walls)
+    assert np.abs(P[:, :, 0] - P[0:1, :, 0]).max() <= 1e-12
+
+
+def test_exact_solver_known_answer():
+    pstar, ustar = np.load(GOLD / "riemann_exact.npz")["toro1_pstar_ustar"]
+    assert abs(pstar - 0.30313) < 1e-5 and abs(ustar - 0.92745) < 1e-5
+
+
+# ------------------------------------------------------------------------------------------
+# known answers for the scalar kernels
+# ------------------------------------------------------------------------------------------
+LIM = {"iord": 0, "minmod": 1, "vanleer": 2, "vanalbada": 3, "mc": 4, "superbee": 5, "LIMO3": 6}
+
+
+def lim(name, x, y):
+    return oracle.load().q2d_oracle_limiter(LIM[name], x, y)
+
+
+def test_limiter_known_answers():
+    assert lim("iord", 1.0, 2.0) == 0.0
+    assert lim("minmod", 1.0, 2.0) == 1.0 and lim("minmod", 2.0, 1.0) == 1.0
+    assert lim("minmod", 1.0, -1.0) == 0.0 and lim("minmod", -3.0, -2.0) == -2.0
+    assert lim("minmod", 1.0, 1.0) == 1.0   # ties keep x (Lib_Limiters.f90:43-44)
+    assert abs(lim("vanleer", 1.0, 1.0) - 1.0) < 1e-15
+    assert abs(lim("vanleer", 1.0, 3.0) - 1.5) < 1e-15      # 2xy/(x+y)
+    assert lim("vanleer", 1.0, -1.0) == 0.0
+    assert abs(lim("vanalbada", 1.0, 1.0) - 1.0) < 1e-15
+    assert abs(lim("mc", 1.0, 3.0) - 2.0) < 1e-15           # min(2r, (1+r)/2, 2) * x
+    assert abs(lim("mc", 1.0, 0.5) - 0.75) < 1e-15
+    assert abs(lim("superbee", 1.0, 0.5) - 1.0) < 1e-15
+    assert abs(lim("superbee", 1.0, 3.0) - 2.0) < 1e-15
+    assert abs(lim("LIMO3", 1.0, 1.0) - 1.0) < 1e-15
+    assert lim("LIMO3", 1.0, -0.5) > 0.0                     # third order: no clip at extrema
+
+
+def riemann(kind, L, R, nx=1.0, ny=0.0):
+    import ctypes as C
+    lib = oracle.load()
+    opt = make_options({})
+    a = (C.c_double * 4)(*L)
+    b = (C.c_double * 4)(*R)
+    out = (C.c_double * 4)()
+    lib.q2d_oracle_riemann(kind, C.byref(opt), a, b, nx, ny, out)
+    return np.array(out[:])
+
+
+def phys_flux(P, nx, ny, g=1.4):
+    r, u, v, p = P
+    un = u * nx + v * ny
+    H = g / (g - 1) * p / r + 0.5 * (u * u + v * v)
+    return np.array([r * un, r * un * u + p * nx, r * un * v + p * ny, r * un * H])
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_riemann_consistency(kind):
+    """F(U, U) equals the physical flux for HLLC, HLLE and Rusanov, in any direction."""
+    rng = np.random.default_rng(5)
+    for _ in range(20):
+        P = [rng.uniform(0.2, 3), rng.uniform(-2, 2), rng.uniform(-2, 2), rng.uniform(0.2, 5)]
+        th = rng.uniform(0, 2 * np.pi)
+        n = (np.cos(th), np.sin(th))
+        F = riemann(kind, P, P, *n)
+        assert np.allclose(F, phys_flux(P, *n), rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_riemann_supersonic_upwinding(kind):
+    """Supersonic flow along the normal: HLLC/HLLE return the left physical flux exactly."""
+    L = [1.0, 5.0, 0.3, 1.0]
+    R = [0.5, 4.0, -0.2, 0.7]
+    F = riemann(kind, L, R)
+    if kind in (0, 1):
+        assert np.allclose(F, phys_flux(L, 1.0, 0.0), rtol=1e-13)
+
+
+def test_conservation_closed_domain():
+    """All-wall (BC 300) curvilinear box, random smooth state: the oracle conserves mass and
+    energy to round-off per step (sum of U * sur)."""
+    ni = nj = 24
+    rng = np.random.default_rng(3)
+    x, y = np.meshgrid(np.linspace(0, 1, ni + 1), np.linspace(0, 1, nj + 1))
+    x = x + 0.02 * np.sin(2 * np.pi * y)
+    nodes = np.stack([x, y], axis=-1)
+    prim = np.zeros((nj, ni, 4))
+    prim[..., 0] = 1 + 0.1 * rng.random((nj, ni))
+    prim[..., 1] = 0.1 * rng.standard_normal((nj, ni))
+    prim[..., 2] = 0.1 * rng.standard_normal((nj, ni))
+    prim[..., 3] = 1 + 0.1 * rng.random((nj, ni))
+    blk = cases.BlockSpec(ni, nj, nodes, prim)
+    bcs = cases.edge_records(1, ni, nj, {f: (300, {}) for f in (1, 2, 3, 4)})
+    cs = cases.CaseSpec("box", [blk], bcs, dict(limiter="vanleer", n_rk=3, cfl=0.4, time_accurate=1))
+    s = oracle.solver(make_options(cs), [cs])
+    try:
+        # cell areas from the nodes (shoelace on the quads)
+        X, Y = nodes[..., 0], nodes[..., 1]
+        d1x, d1y = X[1:, 1:] - X[:-1, :-1], Y[1:, 1:] - Y[:-1, :-1]
+        d2x, d2y = X[:-1, 1:] - X[1:, :-1], Y[:-1, 1:] - Y[1:, :-1]
+        sur = 0.5 * np.abs(d1x * d2y - d1y * d2x)
+
+        def totals(P):
+            from tests.conftest import cons
+            U = cons(P)
+            return np.array([(U[..., k] * sur).sum() for k in (0, 3)])
+        t0 = totals(s.prim())
+        s.step(20)
+        t1 = totals(s.prim())
+        assert np.all(np.abs(t1 - t0) <= 1e-12 * np.abs(t0)), (t0, t1)
+    finally:
+        s.close()
