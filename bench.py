@@ -1,0 +1,292 @@
+#!/usr/bin/env python
+"""Benchmark of the Q2D explicit residual/update path on B200.
+
+Workload (one "step" = one explicit SSP-RK3 time step — 3 fused stage kernels including the
+ghost fill, MUSCL + HLLC fluxes, boundary fluxes, area-variation sources, the RK update, the
+local time step and the residual norm — over every case of the batch):
+  the batched quasi-2D area-variation nozzles: 4096 independent cases, Nx ~ lognormal clipped
+  to [64, 1024], Ny ~ U{8..64}, A(x) = A_t (1 + k (x - x_t)^2), p0 ~ U[2, 10] bar,
+  T0 ~ U[300, 800] K, van Leer + HLLC, local time stepping; synthetic seeded inputs with the
+  layout of the reference's planar-nozzle case. Computed in the FP32-flux / FP64-state form;
+  the plain FP64 form of the same batch is timed beside it.
+
+Output: one JSON line (rank 0). `--impl reference` times the CPU oracle (the C++ restatement
+of the reference's OpenMP loops, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "cell-updates/s batched+served vs plain FP64 on 1 B200; p50/p99 solve latency"
+UNIT = "cell-updates/s"
+# Algorithmic bytes per cell-update (one SSP-RK3 step): per stage read state 32 + U^n 32 +
+# write 32 + dt 8 + node geometry 16 = 120, plus the dt pass 56, plus 16 per stage for the
+# area-variation geometry (Gx, Gy): 3 * (120 + 16) + 56 = 464.
+B_ALG = 464.0
+STAGES = 3
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cases", type=int, default=4096)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in Path(self.out.name).read_text().strip().splitlines()]
+        except Exception:
+            rows = []
+        rows = [[x.strip() for x in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def batch_cases(n, rank):
+    from q2d_b200 import cases
+    return cases.area_nozzle_batch(n=n, seed=cases.BASE_SEED + 3 + 7919 * rank)
+
+
+def time_device(lib, solver, K):
+    """K steps in one captured graph, CUDA events on the library's stream."""
+    import torch
+    stream = torch.cuda.ExternalStream(lib.q2d_gpu_stream(solver.ctx))
+    assert lib.q2d_gpu_prepare(solver.ctx, K) == 0
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    n0 = lib.q2d_gpu_launch_count(solver.ctx)
+    ev0.record(stream)
+    st = lib.q2d_gpu_step_async(solver.ctx, K)
+    ev1.record(stream)
+    lib.q2d_gpu_wait(solver.ctx, None)
+    torch.cuda.synchronize()
+    assert st == 0, st
+    return ev0.elapsed_time(ev1), lib.q2d_gpu_launch_count(solver.ctx) - n0
+
+
+def cpu_baseline(batch, budget_s=12.0):
+    """The CPU oracle (all host threads) on a bounded sample of the workload."""
+    from oracle import oracle
+    from q2d_b200 import make_options
+    threads = oracle.set_threads(os.cpu_count() or 1)
+    sample = batch[:256]
+    cells = sum(c.cells for c in sample)
+    s = oracle.solver(make_options(sample[0]), sample)
+    try:
+        s.step(1)   # first step (setup, dt)
+        t0 = time.perf_counter()
+        n = 0
+        while time.perf_counter() - t0 < budget_s and n < 200:
+            s.step(1)
+            n += 1
+        dt = time.perf_counter() - t0
+    finally:
+        s.close()
+    return {"value": cells * n / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(sample)} of the batch's cases ({cells} cells) x {n} steps, "
+                      f"{dt:.1f} s, C++ oracle -O3 OpenMP"}
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    batch = batch_cases(args.cases, 0)
+    cb = cpu_baseline(batch, budget_s=max(5.0, min(60.0, 0.5 * (args.steps + args.warmup))))
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batched area-variation nozzles (CPU oracle sample)", "cases": len(batch)},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    from q2d_b200 import make_options, _abi
+    from q2d_b200.solver import Q2DSolver
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lib = _abi.load_library()
+    K, W = args.steps, max(3, args.warmup)
+    batch = batch_cases(args.cases, rank)
+    cells = sum(c.cells for c in batch)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- FP32-flux / FP64-state batched form (the headline) ----------------------------
+    s = Q2DSolver(make_options(batch[0], precision=1), batch)
+    s.step(W)
+    barrier()
+    with ClockSampler(local) as clk:
+        ms, launches = time_device(lib, s, K)
+    ms = max_over_ranks(ms)
+    value = world * cells * K / (ms / 1e3)
+    infos = s.step(0)
+    errs = sum(1 for i in infos if i["err"])
+    t_launch = ms / 1e3 / (K * STAGES)
+    achieved = (B_ALG / STAGES) * cells / t_launch / 1e9
+    peaks = {}
+    try:
+        peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    try:
+        prof = json.loads((REPO / "profiles" / "traffic.json").read_text())
+        traffic = prof.get("dram_bytes_per_launch_full")
+    except Exception:
+        pass
+    # ---- e2e through the C ABI with host buffers ----------------------------------------
+    e2e = None
+    if not args.no_e2e:
+        P_host = []
+        for cs in batch:
+            a = torch.empty((cs.blocks[0].nj + 4, cs.blocks[0].ni + 4, 4), dtype=torch.float64,
+                            pin_memory=True).numpy()
+            a[...] = cs.blocks[0].prim_ghost()
+            P_host.append(a)
+        outs = [np.empty_like(a) for a in P_host]
+        infos_t = (_abi.StepInfo * len(batch))()
+        Ke = max(3, K // 2)
+        assert lib.q2d_gpu_prepare(s.ctx, 1) == 0
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for b, a in enumerate(P_host):
+            lib.q2d_gpu_upload_prim(s.ctx, s.block_ids[b][0], _abi.dptr(a))
+        for _ in range(Ke):
+            lib.q2d_gpu_step(s.ctx, 1, infos_t)
+        for b, o in enumerate(outs):
+            lib.q2d_gpu_download_prim(s.ctx, s.block_ids[b][0], _abi.dptr(o))
+        te = max_over_ranks(time.perf_counter() - t0)
+        bytes_state = sum(a.nbytes for a in P_host)
+        e2e = {"value": world * cells * Ke / te, "unit": UNIT,
+               "h2d_bytes_per_step": int(bytes_state / Ke),
+               "d2h_bytes_per_step": int(bytes_state / Ke + C.sizeof(_abi.StepInfo) * len(batch)),
+               "steps": Ke, "seconds": te,
+               "path": "q2d_gpu_upload_prim (every block) + q2d_gpu_step(1) x steps (per-step case info "
+                       "to host) + q2d_gpu_download_prim (every block)"}
+    s.close()
+    # ---- plain FP64 form of the same batch -------------------------------------------------
+    fp64 = None
+    if not args.no_fp64:
+        s64 = Q2DSolver(make_options(batch[0], precision=0), batch)
+        s64.step(W)
+        K64 = max(5, K // 4)
+        ms64, _ = time_device(lib, s64, K64)
+        ms64 = max_over_ranks(ms64)
+        v64 = world * cells * K64 / (ms64 / 1e3)
+        fp64 = {"value": v64, "unit": UNIT, "steps": K64, "ms_per_step": ms64 / K64,
+                "ratio_fp32flux_over_fp64": value / v64}
+        s64.close()
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(batch)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32-flux/fp64-state", "data": "synthetic",
+        "config": {"workload": "batched area-variation nozzles (4096 independent cases per GPU, "
+                               "Nx~lognormal[64,1024], Ny~U{8..64}), van Leer + HLLC, SSP-RK3, local dt",
+                   "cases_per_gpu": len(batch), "cells_per_gpu": cells,
+                   "parallelism": f"replicas x{world} (independent cases per GPU)",
+                   "l2": "inputs larger than L2 (state %.2f GB per buffer)" % (cells * 32 / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650",
+                     "bytes_per_cell_update": B_ALG, "launch_ms": t_launch * 1e3},
+        "gpu_launches": launches, "errors": errs,
+        "clocks": clk.summary(),
+        "e2e": e2e, "plain_fp64": fp64, "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

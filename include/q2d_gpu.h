@@ -170,6 +170,18 @@ int  q2d_gpu_commit(q2d_ctx* ctx);
  * out, when not NULL, receives q2d_gpu_num_cases() entries. Returns the first case error. */
 int  q2d_gpu_step(q2d_ctx* ctx, int nsteps, q2d_step_info* out);
 
+/* Asynchronous form of q2d_gpu_step: enqueues the steps on the context's stream and returns;
+ * q2d_gpu_wait() synchronises and fills out (q2d_gpu_num_cases() entries, or NULL). */
+int  q2d_gpu_step_async(q2d_ctx* ctx, int nsteps);
+int  q2d_gpu_wait(q2d_ctx* ctx, q2d_step_info* out);
+
+/* Builds (captures and instantiates) the CUDA graph of an nsteps call ahead of time, so that a
+ * later q2d_gpu_step(ctx, nsteps, ...) only launches it. */
+int  q2d_gpu_prepare(q2d_ctx* ctx, int nsteps);
+
+/* The CUDA stream (cudaStream_t) the context enqueues on, for event timing by callers. */
+void* q2d_gpu_stream(const q2d_ctx* ctx);
+
 /* Reads the current step info of one case. */
 int  q2d_gpu_case_info(q2d_ctx* ctx, int case_id, q2d_step_info* out);
 

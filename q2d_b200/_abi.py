@@ -171,6 +171,14 @@ def load_library() -> C.CDLL:
     lib.q2d_gpu_num_cells.argtypes = [C.c_void_p]
     lib.q2d_gpu_launch_count.restype = C.c_longlong
     lib.q2d_gpu_launch_count.argtypes = [C.c_void_p]
+    lib.q2d_gpu_step_async.restype = C.c_int
+    lib.q2d_gpu_step_async.argtypes = [C.c_void_p, C.c_int]
+    lib.q2d_gpu_wait.restype = C.c_int
+    lib.q2d_gpu_wait.argtypes = [C.c_void_p, C.POINTER(StepInfo)]
+    lib.q2d_gpu_prepare.restype = C.c_int
+    lib.q2d_gpu_prepare.argtypes = [C.c_void_p, C.c_int]
+    lib.q2d_gpu_stream.restype = C.c_void_p
+    lib.q2d_gpu_stream.argtypes = [C.c_void_p]
     lib.q2d_options_default.restype = None
     lib.q2d_options_default.argtypes = [C.POINTER(Options)]
     _LIB = lib

@@ -240,24 +240,12 @@ int choose_tile(q2d_ctx* ctx) {
 int commit(q2d_ctx* ctx) {
     if (ctx->committed) return Q2D_OK;
     if (ctx->cases.empty()) return fail(ctx, Q2D_ERR_BADARG, "no case");
-    // ---- host geometry -------------------------------------------------------------------
-    for (HBlock& b : ctx->blocks) {
-        int e = setup_block(b.ni, b.nj, b.nodes.data(), b.area.empty() ? nullptr : b.area.data(),
-                            ctx->opt.source, b.geom);
-        if (e) return fail(ctx, e, "degenerate cell in block " + std::to_string(b.local_b));
-    }
+    // ---- boundary records -> edge arrays (geometry of ghost cells is added per block below) --
     std::vector<EdgeRec> edges;
     std::vector<BCParam> params;
     for (size_t c = 0; c < ctx->cases.size(); ++c) {
         HCase& cs = ctx->cases[c];
         if (cs.blocks.empty()) return fail(ctx, Q2D_ERR_BADARG, "case without blocks");
-        for (const q2d_bc_rec& r : cs.bc) {
-            HBlock& B = ctx->blocks[cs.blocks[r.b - 1]];
-            const HBlock* D = r.type == 101 ? &ctx->blocks[cs.blocks[r.bs - 1]] : nullptr;
-            int e = ghost_metrics(r, B.ni, B.nj, B.nodes.data(), B.geom, D ? D->ni : 0, D ? D->nj : 0,
-                                  D ? D->nodes.data() : nullptr);
-            if (e) return fail(ctx, e, "ghost metrics failed for a boundary record");
-        }
         for (int gb : cs.blocks) {
             HBlock& B = ctx->blocks[gb];
             const int len[4] = {B.nj, B.nj, B.ni, B.ni};
@@ -341,37 +329,62 @@ int commit(q2d_ctx* ctx) {
         dcases[c].item_end = (int)items.size();
         dcases[c].ndir = ctx->blocks[ctx->cases[c].blocks[0]].nj == 1 ? 1 : 2;
     }
-    // ---- host planes -> device -----------------------------------------------------------
-    std::vector<double> sc(2 * oc, 0.0), dl(og, 0.0), fi(ofi, 0.0), fj(ofj, 0.0), pa(oc, 0.0);
-    for (HBlock& b : ctx->blocks) {
-        const DBlock& d = b.d;
-        const HostGeom& G = b.geom;
-        const long long n = (long long)b.ni * b.nj;
-        for (int j = 0; j < b.nj; ++j)
-            for (int i = 0; i < b.ni; ++i) {
-                const long long k = (long long)j * b.ni + i;
-                double v[4];
-                versors(G, i, j, v);
-                double* s = &sc[2 * d.oc];
-                s[k] = G.sur[G.g(i, j)];
-                s[2 * d.pc + k] = v[0];
-                s[3 * d.pc + k] = v[1];
-                s[4 * d.pc + k] = v[2];
-                s[5 * d.pc + k] = v[3];
-                s[6 * d.pc + k] = G.src0[k];
-                s[7 * d.pc + k] = G.src1[k];
-            }
-        for (long long k = 0; k < (long long)(b.ni + 4) * (b.nj + 4); ++k) {
-            dl[d.og + k] = G.dl[2 * k];
-            dl[d.og + d.pg + k] = G.dl[2 * k + 1];
+    // ---- device pools, filled block by block (host memory stays at one block) -------------
+    CK(cudaMemset(ctx->PB.p, 0, sizeof(double) * oc));
+    CK(cudaMemset(ctx->PC.p, 0, sizeof(double) * oc));
+    for (size_t c = 0; c < ctx->cases.size(); ++c) {
+        HCase& cs = ctx->cases[c];
+        for (int gb : cs.blocks) {
+            HBlock& b = ctx->blocks[gb];
+            int e = setup_block(b.ni, b.nj, b.nodes.data(), b.area.empty() ? nullptr : b.area.data(),
+                                ctx->opt.source, b.geom);
+            if (e) return fail(ctx, e, "degenerate cell in block " + std::to_string(b.local_b));
         }
-        for (long long k = 0; k < (long long)(b.ni + 1) * b.nj; ++k)
-            for (int q = 0; q < 3; ++q) fi[d.ofi + q * d.pfi + k] = G.fi[3 * k + q];
-        for (long long k = 0; k < (long long)b.ni * (b.nj + 1); ++k)
-            for (int q = 0; q < 3; ++q) fj[d.ofj + q * d.pfj + k] = G.fj[3 * k + q];
-        for (int v = 0; v < 4; ++v)
-            std::memcpy(&pa[d.oc + v * d.pc], &b.prim[(size_t)v * n], sizeof(double) * n);
-        ctx->total_cells += n;
+        for (const q2d_bc_rec& r : cs.bc) {
+            HBlock& B = ctx->blocks[cs.blocks[r.b - 1]];
+            const HBlock* D = r.type == 101 ? &ctx->blocks[cs.blocks[r.bs - 1]] : nullptr;
+            int e = ghost_metrics(r, B.ni, B.nj, B.nodes.data(), B.geom, D ? D->ni : 0, D ? D->nj : 0,
+                                  D ? D->nodes.data() : nullptr);
+            if (e) return fail(ctx, e, "ghost metrics failed for a boundary record");
+        }
+        for (int gb : cs.blocks) {
+            HBlock& b = ctx->blocks[gb];
+            const DBlock& d = b.d;
+            const HostGeom& G = b.geom;
+            const long long n = (long long)b.ni * b.nj;
+            std::vector<double> sc(8 * (size_t)d.pc, 0.0), dl(2 * (size_t)d.pg, 0.0), fi(3 * (size_t)d.pfi, 0.0),
+                fj(3 * (size_t)d.pfj, 0.0), pa(4 * (size_t)d.pc, 0.0);
+            for (int j = 0; j < b.nj; ++j)
+                for (int i = 0; i < b.ni; ++i) {
+                    const long long k = (long long)j * b.ni + i;
+                    double v[4];
+                    versors(G, i, j, v);
+                    sc[k] = G.sur[G.g(i, j)];
+                    sc[2 * d.pc + k] = v[0];
+                    sc[3 * d.pc + k] = v[1];
+                    sc[4 * d.pc + k] = v[2];
+                    sc[5 * d.pc + k] = v[3];
+                    sc[6 * d.pc + k] = G.src0[k];
+                    sc[7 * d.pc + k] = G.src1[k];
+                }
+            for (long long k = 0; k < (long long)(b.ni + 4) * (b.nj + 4); ++k) {
+                dl[k] = G.dl[2 * k];
+                dl[d.pg + k] = G.dl[2 * k + 1];
+            }
+            for (long long k = 0; k < (long long)(b.ni + 1) * b.nj; ++k)
+                for (int q = 0; q < 3; ++q) fi[q * d.pfi + k] = G.fi[3 * k + q];
+            for (long long k = 0; k < (long long)b.ni * (b.nj + 1); ++k)
+                for (int q = 0; q < 3; ++q) fj[q * d.pfj + k] = G.fj[3 * k + q];
+            for (int v = 0; v < 4; ++v) std::memcpy(&pa[v * d.pc], &b.prim[(size_t)v * n], sizeof(double) * n);
+            CK(cudaMemcpy(ctx->PA.p + d.oc, pa.data(), sizeof(double) * pa.size(), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ctx->SC.p + 2 * d.oc, sc.data(), sizeof(double) * sc.size(), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ctx->DL.p + d.og, dl.data(), sizeof(double) * dl.size(), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ctx->FI.p + d.ofi, fi.data(), sizeof(double) * fi.size(), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ctx->FJ.p + d.ofj, fj.data(), sizeof(double) * fj.size(), cudaMemcpyHostToDevice));
+            ctx->total_cells += n;
+            b.prim.clear(); b.prim.shrink_to_fit();
+            b.geom = HostGeom{};
+        }
     }
     std::vector<DBlock> db(ctx->blocks.size());
     for (size_t k = 0; k < ctx->blocks.size(); ++k) db[k] = ctx->blocks[k].d;
@@ -385,20 +398,11 @@ int commit(q2d_ctx* ctx) {
         s.time = ctx->cases[c].time0;
         s.time_from_call = s.time;
     }
-    CK(ctx->PA.alloc(oc)); CK(ctx->PB.alloc(oc)); CK(ctx->PC.alloc(oc));
-    CK(ctx->SC.alloc(2 * oc)); CK(ctx->DL.alloc(og)); CK(ctx->FI.alloc(ofi)); CK(ctx->FJ.alloc(ofj));
     CK(ctx->PART.alloc(5 * items.size()));
     CK(ctx->dblocks.alloc(db.size())); CK(ctx->dcases.alloc(dcases.size()));
     CK(ctx->cstate.alloc(st.size())); CK(ctx->items.alloc(items.size()));
     CK(ctx->edges.alloc(edges.size())); CK(ctx->bcp.alloc(params.size())); CK(ctx->flag.alloc(1));
     CK(cudaMallocHost(&ctx->h_state, sizeof(CaseState) * st.size()));
-    CK(cudaMemcpy(ctx->PA.p, pa.data(), sizeof(double) * oc, cudaMemcpyHostToDevice));
-    CK(cudaMemset(ctx->PB.p, 0, sizeof(double) * oc));
-    CK(cudaMemset(ctx->PC.p, 0, sizeof(double) * oc));
-    CK(cudaMemcpy(ctx->SC.p, sc.data(), sizeof(double) * 2 * oc, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->DL.p, dl.data(), sizeof(double) * og, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->FI.p, fi.data(), sizeof(double) * ofi, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->FJ.p, fj.data(), sizeof(double) * ofj, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->dblocks.p, db.data(), sizeof(DBlock) * db.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->dcases.p, dcases.data(), sizeof(DCase) * dcases.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->cstate.p, st.data(), sizeof(CaseState) * st.size(), cudaMemcpyHostToDevice));
@@ -414,11 +418,6 @@ int commit(q2d_ctx* ctx) {
         ctx->grid = (int)std::min<long long>((long long)items.size(), (long long)occ * ctx->num_sms);
     }
     if (ctx->grid < 1) ctx->grid = 1;
-    // release host copies of the big arrays
-    for (HBlock& b : ctx->blocks) {
-        b.prim.clear(); b.prim.shrink_to_fit();
-        b.geom = HostGeom{};
-    }
     ctx->committed = true;
     ctx->dt_valid = false;
     return Q2D_OK;
@@ -559,10 +558,9 @@ int q2d_gpu_upload_prim(q2d_ctx* ctx, int block_id, const double* P) {
         b.prim = std::move(planes);
         return Q2D_OK;
     }
-    for (int v = 0; v < 4; ++v)
-        CK(cudaMemcpyAsync(ctx->PA.p + b.d.oc + v * b.d.pc, &planes[v * n], sizeof(double) * n,
-                           cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<double> staged(4 * (size_t)b.d.pc, 0.0);
+    for (int v = 0; v < 4; ++v) std::memcpy(&staged[v * b.d.pc], &planes[v * n], sizeof(double) * n);
+    CK(cudaMemcpy(ctx->PA.p + b.d.oc, staged.data(), sizeof(double) * staged.size(), cudaMemcpyHostToDevice));
     ctx->dt_valid = false;
     return Q2D_OK;
 }
@@ -573,16 +571,16 @@ int q2d_gpu_download_prim(q2d_ctx* ctx, int block_id, double* P) {
     int e = commit(ctx);
     if (e) return e;
     HBlock& b = ctx->blocks[block_id];
-    const long long n = (long long)b.ni * b.nj;
-    std::vector<double> planes(4 * n);
-    for (int v = 0; v < 4; ++v)
-        CK(cudaMemcpyAsync(&planes[v * n], ctx->PA.p + b.d.oc + v * b.d.pc, sizeof(double) * n,
-                           cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<double> staged(4 * (size_t)b.d.pc);
+    CK(cudaMemcpyAsync(staged.data(), ctx->PA.p + b.d.oc, sizeof(double) * staged.size(),
+                       cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    const double* planes = staged.data();
+    const long long pcs = b.d.pc;
     for (int j = 0; j < b.nj; ++j)
         for (int i = 0; i < b.ni; ++i) {
             double* dst = &P[4 * ((size_t)(i + 2) + (size_t)(b.ni + 4) * (j + 2))];
-            for (int v = 0; v < 4; ++v) dst[v] = planes[v * n + (size_t)j * b.ni + i];
+            for (int v = 0; v < 4; ++v) dst[v] = planes[v * pcs + (size_t)j * b.ni + i];
         }
     return Q2D_OK;
 }
@@ -592,7 +590,7 @@ int q2d_gpu_commit(q2d_ctx* ctx) {
     return commit(ctx);
 }
 
-int q2d_gpu_step(q2d_ctx* ctx, int nsteps, q2d_step_info* out) {
+int q2d_gpu_step_async(q2d_ctx* ctx, int nsteps) {
     if (!ctx || nsteps < 0) return fail(ctx, Q2D_ERR_BADARG, "step: bad argument");
     int e = commit(ctx);
     if (e) return e;
@@ -608,6 +606,11 @@ int q2d_gpu_step(q2d_ctx* ctx, int nsteps, q2d_step_info* out) {
         CK(cudaMemcpyAsync(ctx->h_state, ctx->cstate.p, sizeof(CaseState) * ctx->cases.size(),
                            cudaMemcpyDeviceToHost, ctx->stream));
     }
+    return Q2D_OK;
+}
+
+int q2d_gpu_wait(q2d_ctx* ctx, q2d_step_info* out) {
+    if (!ctx) return Q2D_ERR_BADARG;
     CK(cudaStreamSynchronize(ctx->stream));
     int first = Q2D_OK;
     for (size_t c = 0; c < ctx->cases.size(); ++c) {
@@ -617,6 +620,22 @@ int q2d_gpu_step(q2d_ctx* ctx, int nsteps, q2d_step_info* out) {
         if (!first && info.err) first = info.err;
     }
     return first;
+}
+
+int q2d_gpu_step(q2d_ctx* ctx, int nsteps, q2d_step_info* out) {
+    int e = q2d_gpu_step_async(ctx, nsteps);
+    if (e) return e;
+    return q2d_gpu_wait(ctx, out);
+}
+
+void* q2d_gpu_stream(const q2d_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int q2d_gpu_prepare(q2d_ctx* ctx, int nsteps) {
+    if (!ctx || nsteps < 1) return fail(ctx, Q2D_ERR_BADARG, "prepare: bad argument");
+    int e = commit(ctx);
+    if (e) return e;
+    cudaGraphExec_t ge;
+    return get_graph(ctx, nsteps, &ge);
 }
 
 int q2d_gpu_case_info(q2d_ctx* ctx, int case_id, q2d_step_info* out) {
