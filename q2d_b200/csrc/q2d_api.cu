@@ -330,6 +330,8 @@ int commit(q2d_ctx* ctx) {
         dcases[c].ndir = ctx->blocks[ctx->cases[c].blocks[0]].nj == 1 ? 1 : 2;
     }
     // ---- device pools, filled block by block (host memory stays at one block) -------------
+    CK(ctx->PA.alloc(oc)); CK(ctx->PB.alloc(oc)); CK(ctx->PC.alloc(oc));
+    CK(ctx->SC.alloc(2 * oc)); CK(ctx->DL.alloc(og)); CK(ctx->FI.alloc(ofi)); CK(ctx->FJ.alloc(ofj));
     CK(cudaMemset(ctx->PB.p, 0, sizeof(double) * oc));
     CK(cudaMemset(ctx->PC.p, 0, sizeof(double) * oc));
     for (size_t c = 0; c < ctx->cases.size(); ++c) {
