@@ -179,6 +179,12 @@ int  q2d_gpu_wait(q2d_ctx* ctx, q2d_step_info* out);
  * later q2d_gpu_step(ctx, nsteps, ...) only launches it. */
 int  q2d_gpu_prepare(q2d_ctx* ctx, int nsteps);
 
+/* Autotuner (no reference counterpart): times each candidate schedule of the stage kernels
+ * (tile shape of the CTA-tile kernel, rows per item of the warp-marching kernel) for `steps`
+ * steps on this context's workload, keeps the fastest and restores the state. *schedule gets
+ * the chosen candidate index, *ms_per_step its time (either may be NULL). */
+int  q2d_gpu_autotune(q2d_ctx* ctx, int steps, int* schedule, float* ms_per_step);
+
 /* The CUDA stream (cudaStream_t) the context enqueues on, for event timing by callers. */
 void* q2d_gpu_stream(const q2d_ctx* ctx);
 

@@ -175,6 +175,8 @@ def load_library() -> C.CDLL:
     lib.q2d_gpu_step_async.argtypes = [C.c_void_p, C.c_int]
     lib.q2d_gpu_wait.restype = C.c_int
     lib.q2d_gpu_wait.argtypes = [C.c_void_p, C.POINTER(StepInfo)]
+    lib.q2d_gpu_autotune.restype = C.c_int
+    lib.q2d_gpu_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
     lib.q2d_gpu_prepare.restype = C.c_int
     lib.q2d_gpu_prepare.argtypes = [C.c_void_p, C.c_int]
     lib.q2d_gpu_stream.restype = C.c_void_p

@@ -66,7 +66,7 @@ struct q2d_ctx {
     bool committed = false;
     bool dt_valid = false;
     int tile = 0;
-    int kernel = 1;       // 0: CTA-tile stage kernel, 1: warp-marching stage kernel
+    int kernel = 0;       // 0: CTA-tile stage kernel, 1: warp-marching stage kernel
     int march_h = 16;     // rows per warp-marching item
     int grid = 0;
     // device pools
@@ -229,12 +229,51 @@ bool rec_less(const q2d_bc_rec& a, const q2d_bc_rec& b) {
     return a.b != b.b ? a.b < b.b : a.f < b.f;
 }
 
-int choose_tile(q2d_ctx* ctx) {
-    // Default tile: 32 x 15 when most blocks are tall, else 32 x 7 (the autotuner may replace it).
-    long long tall = 0, all = 0;
-    for (const HBlock& b : ctx->blocks) { all += (long long)b.ni * b.nj; if (b.nj >= 48) tall += (long long)b.ni * b.nj; }
-    (void)tall; (void)all;
-    return ctx->tile;
+
+// Work items of the current schedule (kernel / tile / rows per item), grouped by case, and
+// the persistent grid size. Re-run by the autotuner for every candidate schedule.
+int build_items(q2d_ctx* ctx) {
+    int TX, TY, NT;
+    tile_dims(ctx->tile, &TX, &TY, &NT);
+    std::vector<WorkItem> items;
+    std::vector<DCase> dcases(ctx->cases.size());
+    for (size_t c = 0; c < ctx->cases.size(); ++c) {
+        dcases[c].item_begin = (int)items.size();
+        for (int gb : ctx->cases[c].blocks) {
+            const HBlock& B = ctx->blocks[gb];
+            if (ctx->kernel == 1) {
+                for (int i0 = 0; i0 < B.ni; i0 += kMarchCols)
+                    for (int j0 = 0; j0 < B.nj; j0 += ctx->march_h)
+                        items.push_back(WorkItem{gb, i0, j0, (int)c, std::min(B.nj, j0 + ctx->march_h), 0});
+            } else {
+                for (int j0 = 0; j0 < B.nj; j0 += TY)
+                    for (int i0 = 0; i0 < B.ni; i0 += TX) items.push_back(WorkItem{gb, i0, j0, (int)c, 0, 0});
+            }
+        }
+        dcases[c].item_end = (int)items.size();
+        dcases[c].ndir = ctx->blocks[ctx->cases[c].blocks[0]].nj == 1 ? 1 : 2;
+    }
+    ctx->items.release();
+    ctx->PART.release();
+    ctx->dcases.release();
+    CK(ctx->items.alloc(items.size()));
+    CK(ctx->PART.alloc(5 * items.size()));
+    CK(ctx->dcases.alloc(dcases.size()));
+    CK(cudaMemcpy(ctx->items.p, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->dcases.p, dcases.data(), sizeof(DCase) * dcases.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemset(ctx->PART.p, 0, sizeof(double) * 5 * items.size()));
+    if (ctx->kernel == 1) {
+        const int occ = std::max(1, march_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter));
+        ctx->grid = (int)std::min<long long>(((long long)items.size() + 3) / 4, (long long)occ * ctx->num_sms);
+    } else {
+        const int occ = std::max(1, stage_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->tile));
+        ctx->grid = (int)std::min<long long>((long long)items.size(), (long long)occ * ctx->num_sms);
+    }
+    if (ctx->grid < 1) ctx->grid = 1;
+    for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+    ctx->graphs.clear();
+    ctx->graph_kernels.clear();
+    return Q2D_OK;
 }
 
 int commit(q2d_ctx* ctx) {
@@ -307,28 +346,6 @@ int commit(q2d_ctx* ctx) {
         oc += 4 * d.pc; og += 2 * d.pg; ofi += 3 * d.pfi; ofj += 3 * d.pfj;
     }
     ctx->pool4 = oc;
-    // ---- work items ----------------------------------------------------------------------
-    int TX, TY, NT;
-    ctx->tile = choose_tile(ctx);
-    tile_dims(ctx->tile, &TX, &TY, &NT);
-    std::vector<WorkItem> items;
-    std::vector<DCase> dcases(ctx->cases.size());
-    for (size_t c = 0; c < ctx->cases.size(); ++c) {
-        dcases[c].item_begin = (int)items.size();
-        for (int gb : ctx->cases[c].blocks) {
-            const HBlock& B = ctx->blocks[gb];
-            if (ctx->kernel == 1) {
-                for (int i0 = 0; i0 < B.ni; i0 += kMarchCols)
-                    for (int j0 = 0; j0 < B.nj; j0 += ctx->march_h)
-                        items.push_back(WorkItem{gb, i0, j0, (int)c, std::min(B.nj, j0 + ctx->march_h), 0});
-            } else {
-                for (int j0 = 0; j0 < B.nj; j0 += TY)
-                    for (int i0 = 0; i0 < B.ni; i0 += TX) items.push_back(WorkItem{gb, i0, j0, (int)c, 0, 0});
-            }
-        }
-        dcases[c].item_end = (int)items.size();
-        dcases[c].ndir = ctx->blocks[ctx->cases[c].blocks[0]].nj == 1 ? 1 : 2;
-    }
     // ---- device pools, filled block by block (host memory stays at one block) -------------
     CK(ctx->PA.alloc(oc)); CK(ctx->PB.alloc(oc)); CK(ctx->PC.alloc(oc));
     CK(ctx->SC.alloc(2 * oc)); CK(ctx->DL.alloc(og)); CK(ctx->FI.alloc(ofi)); CK(ctx->FJ.alloc(ofj));
@@ -400,28 +417,80 @@ int commit(q2d_ctx* ctx) {
         s.time = ctx->cases[c].time0;
         s.time_from_call = s.time;
     }
-    CK(ctx->PART.alloc(5 * items.size()));
-    CK(ctx->dblocks.alloc(db.size())); CK(ctx->dcases.alloc(dcases.size()));
-    CK(ctx->cstate.alloc(st.size())); CK(ctx->items.alloc(items.size()));
+    CK(ctx->dblocks.alloc(db.size()));
+    CK(ctx->cstate.alloc(st.size()));
     CK(ctx->edges.alloc(edges.size())); CK(ctx->bcp.alloc(params.size())); CK(ctx->flag.alloc(1));
     CK(cudaMallocHost(&ctx->h_state, sizeof(CaseState) * st.size()));
     CK(cudaMemcpy(ctx->dblocks.p, db.data(), sizeof(DBlock) * db.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->dcases.p, dcases.data(), sizeof(DCase) * dcases.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->cstate.p, st.data(), sizeof(CaseState) * st.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->items.p, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice));
     if (!edges.empty()) CK(cudaMemcpy(ctx->edges.p, edges.data(), sizeof(EdgeRec) * edges.size(), cudaMemcpyHostToDevice));
     if (!params.empty()) CK(cudaMemcpy(ctx->bcp.p, params.data(), sizeof(BCParam) * params.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemset(ctx->PART.p, 0, sizeof(double) * 5 * items.size()));
-    if (ctx->kernel == 1) {
-        const int occ = std::max(1, march_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter));
-        ctx->grid = (int)std::min<long long>(((long long)items.size() + 3) / 4, (long long)occ * ctx->num_sms);
-    } else {
-        const int occ = std::max(1, stage_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->tile));
-        ctx->grid = (int)std::min<long long>((long long)items.size(), (long long)occ * ctx->num_sms);
+    {
+        int e = build_items(ctx);
+        if (e) return e;
     }
-    if (ctx->grid < 1) ctx->grid = 1;
     ctx->committed = true;
     ctx->dt_valid = false;
+    return Q2D_OK;
+}
+
+// ---- autotuner ------------------------------------------------------------------------------
+// Times every schedule (stage-kernel tile shape or warp-marching rows per item) for `steps`
+// explicit steps on the context's own workload and keeps the fastest. The state, the case
+// states and the time steps are saved before and restored after, so tuning has no effect on
+// the results.
+struct Schedule { int kernel, tile, march_h; };
+
+int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
+    static const Schedule cands[] = {{0, 0, 16}, {0, 1, 16}, {0, 2, 16}, {1, 0, 8}, {1, 0, 16}};
+    const int ncand = (int)(sizeof(cands) / sizeof(cands[0]));
+    const size_t nst = ctx->cases.size();
+    DevBuf<double> saveP, saveSC;
+    DevBuf<CaseState> saveCS;
+    CK(saveP.alloc(ctx->pool4));
+    CK(saveSC.alloc(2 * ctx->pool4));
+    CK(saveCS.alloc(nst));
+    if (int e = ensure_dt(ctx)) return e;
+    CK(cudaMemcpyAsync(saveP.p, ctx->PA.p, sizeof(double) * ctx->pool4, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(saveSC.p, ctx->SC.p, sizeof(double) * 2 * ctx->pool4, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(saveCS.p, ctx->cstate.p, sizeof(CaseState) * nst, cudaMemcpyDeviceToDevice, ctx->stream));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int besti = 0;
+    for (int k = 0; k < ncand; ++k) {
+        ctx->kernel = cands[k].kernel;
+        ctx->tile = cands[k].tile;
+        ctx->march_h = cands[k].march_h;
+        if (int e = build_items(ctx)) return e;
+        int nk = 0;
+        for (int w = 0; w < 1 && nk >= 0; ++w)
+            if (int e = enqueue_step(ctx, ctx->stream, &nk)) return e;   // warm-up step
+        CK(cudaEventRecord(e0, ctx->stream));
+        for (int sidx = 0; sidx < steps; ++sidx)
+            if (int e = enqueue_step(ctx, ctx->stream, &nk)) return e;
+        CK(cudaEventRecord(e1, ctx->stream));
+        CK(cudaEventSynchronize(e1));
+        ctx->launches += nk;
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) { best = ms; besti = k; }
+        // restore before the next candidate
+        CK(cudaMemcpyAsync(ctx->PA.p, saveP.p, sizeof(double) * ctx->pool4, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->SC.p, saveSC.p, sizeof(double) * 2 * ctx->pool4, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->cstate.p, saveCS.p, sizeof(CaseState) * nst, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    ctx->kernel = cands[besti].kernel;
+    ctx->tile = cands[besti].tile;
+    ctx->march_h = cands[besti].march_h;
+    if (int e = build_items(ctx)) return e;
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    saveP.release(); saveSC.release(); saveCS.release();
+    if (best_out) *best_out = besti;
+    if (ms_out) *ms_out = best / (float)steps;
     return Q2D_OK;
 }
 
@@ -631,6 +700,13 @@ int q2d_gpu_step(q2d_ctx* ctx, int nsteps, q2d_step_info* out) {
 }
 
 void* q2d_gpu_stream(const q2d_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int q2d_gpu_autotune(q2d_ctx* ctx, int steps, int* schedule, float* ms_per_step) {
+    if (!ctx || steps < 1) return fail(ctx, Q2D_ERR_BADARG, "autotune: bad argument");
+    int e = commit(ctx);
+    if (e) return e;
+    return autotune(ctx, steps, schedule, ms_per_step);
+}
 
 int q2d_gpu_prepare(q2d_ctx* ctx, int nsteps) {
     if (!ctx || nsteps < 1) return fail(ctx, Q2D_ERR_BADARG, "prepare: bad argument");

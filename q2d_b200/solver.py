@@ -88,6 +88,16 @@ class Q2DSolver:
             raise Q2DError(st, f"{self.prefix}_step", str([o["err_at"] for o in out if o["err"]]))
         return out
 
+    SCHEDULES = ["tile 32x10", "tile 32x8", "tile 64x4", "march 28 cols x 8 rows", "march 28 cols x 16 rows"]
+
+    def autotune(self, steps: int = 2) -> dict:
+        """Times every stage-kernel schedule on this workload and keeps the fastest
+        (q2d_gpu_autotune); the state is left unchanged."""
+        idx = C.c_int()
+        ms = C.c_float()
+        self._call("autotune", self.ctx, steps, C.byref(idx), C.byref(ms))
+        return {"schedule": self.SCHEDULES[idx.value], "ms_per_step": ms.value}
+
     def info(self, case: int = 0) -> dict:
         s = _abi.StepInfo()
         self._call("case_info", self.ctx, case, C.byref(s))
