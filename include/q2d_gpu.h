@@ -185,6 +185,27 @@ int  q2d_gpu_prepare(q2d_ctx* ctx, int nsteps);
  * the chosen candidate index, *ms_per_step its time (either may be NULL). */
 int  q2d_gpu_autotune(q2d_ctx* ctx, int steps, int* schedule, float* ms_per_step);
 
+/* Allocation-free residual norm. No counterpart in the reference: it serves callers that
+ * cannot call cudaMalloc when they need the residual — a host whose device memory is owned
+ * by its own pool allocator (for instance a Fortran driver that pre-allocates every array),
+ * or a latency-critical path that cannot take the implicit synchronisation of an allocation.
+ * It computes sqrt(sum over cells of |new - old|^2) for rho, u, v and p (Compute_Residual,
+ * Mod_Diagnostic.f90:438-469, and the sqrt of Mod_Explicit.f90:132) from two caller-owned
+ * device states stored as 4 planes (rho, u, v, p) of plane_stride doubles, cells
+ * 0..ncells-1 of each plane, and writes the 4 norms to device memory at norms_out. The work
+ * is enqueued on `stream` (a cudaStream_t; NULL is the legacy default stream) and the call
+ * returns without synchronising. It allocates nothing: its scratch is a fixed device array of
+ * Q2D_NOALLOC_MAX_PARTIALS x 4 doubles (256 KiB) that every GPU loading the library holds
+ * until the process exits; ncells above Q2D_NOALLOC_MAX_PARTIALS *
+ * Q2D_NOALLOC_CELLS_PER_PARTIAL (16,777,216) returns Q2D_ERR_CAPACITY. The first call on a
+ * device looks up that array's device address on the current device, so make it before any
+ * stream capture. All calls on one device share the array and each call overwrites the part
+ * it uses: calls that overlap on the GPU (concurrent streams) race. */
+#define Q2D_NOALLOC_MAX_PARTIALS      8192
+#define Q2D_NOALLOC_CELLS_PER_PARTIAL 2048
+int  q2d_gpu_residual_norm_noalloc(const double* p_new, const double* p_old, long long ncells,
+                                   long long plane_stride, double* norms_out, void* stream);
+
 /* The CUDA stream (cudaStream_t) the context enqueues on, for event timing by callers. */
 void* q2d_gpu_stream(const q2d_ctx* ctx);
 

@@ -177,6 +177,9 @@ def load_library() -> C.CDLL:
     lib.q2d_gpu_wait.argtypes = [C.c_void_p, C.POINTER(StepInfo)]
     lib.q2d_gpu_autotune.restype = C.c_int
     lib.q2d_gpu_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
+    lib.q2d_gpu_residual_norm_noalloc.restype = C.c_int
+    lib.q2d_gpu_residual_norm_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong,
+                                                  C.c_void_p, C.c_void_p]
     lib.q2d_gpu_prepare.restype = C.c_int
     lib.q2d_gpu_prepare.argtypes = [C.c_void_p, C.c_int]
     lib.q2d_gpu_stream.restype = C.c_void_p
