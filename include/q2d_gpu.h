@@ -215,9 +215,36 @@ int  q2d_gpu_case_info(q2d_ctx* ctx, int case_id, q2d_step_info* out);
 /* Copies the interior of a block's primitive state device->host. */
 int  q2d_gpu_download_prim(q2d_ctx* ctx, int block_id, double* P);
 
-/* Number of cases and total interior cells of the context. */
+/* Number of cases (case slots of a serving context) and total interior cells of the cases
+ * the context holds. */
 int       q2d_gpu_num_cases(const q2d_ctx* ctx);
 long long q2d_gpu_num_cells(const q2d_ctx* ctx);
+
+/* ---- serving: continuous batching of independent cases (no reference counterpart) --------
+ * The reference runs one domain per process from input files (main.f90:20-50). A serving
+ * context holds up to max_cases independent cases in device pools sized from device_bytes
+ * (state, metrics and face geometry: about 240 bytes per interior cell; the work lists and
+ * per-case records are extra), all advanced together by q2d_gpu_step / step_async / wait, each
+ * with its own time step, iteration count, residual, TODO state and error status.
+ *
+ * q2d_serve_admit adds a case between steps: nblocks blocks with the arguments of
+ * q2d_gpu_add_block and q2d_gpu_upload_prim (P[b] in the ghosted Fortran layout) and the
+ * boundary records of q2d_gpu_set_bcs. It validates the input, computes the metrics and
+ * reserves device memory on the host at once, and its device writes are applied by the next
+ * step call after the work in flight, so it may overlap a running step. It returns
+ * Q2D_ERR_CAPACITY when no slot is free or the pools cannot hold the case (nothing is kept).
+ * The case starts at iteration 0 with a fresh residual reference; the other cases' results do
+ * not depend on when it arrives.
+ * q2d_serve_retire frees a case's slot and memory (its results are no longer readable).
+ * q2d_serve_block_id maps (case, 1-based block) to the block id of download_prim / upload_prim.
+ * q2d_serve_free_cells estimates how many more interior cells the pools can take. */
+int  q2d_serve_create(q2d_ctx** out, const q2d_options* opt, unsigned long long device_bytes, int max_cases);
+int  q2d_serve_admit(q2d_ctx* ctx, int nblocks, const int* ni, const int* nj, const double* const* nodes_xy,
+                     const double* const* cross_sections, const double* const* P, const q2d_bc_rec* recs,
+                     int nrecs, int* case_id);
+int  q2d_serve_retire(q2d_ctx* ctx, int case_id);
+int  q2d_serve_block_id(const q2d_ctx* ctx, int case_id, int b, int* block_id);
+long long q2d_serve_free_cells(const q2d_ctx* ctx);
 
 /* Number of kernel launches issued by this context since creation (instrumentation). */
 long long q2d_gpu_launch_count(const q2d_ctx* ctx);

@@ -186,6 +186,18 @@ def load_library() -> C.CDLL:
     lib.q2d_gpu_stream.argtypes = [C.c_void_p]
     lib.q2d_options_default.restype = None
     lib.q2d_options_default.argtypes = [C.POINTER(Options)]
+    PD = C.POINTER(C.POINTER(C.c_double))
+    lib.q2d_serve_create.restype = C.c_int
+    lib.q2d_serve_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Options), C.c_ulonglong, C.c_int]
+    lib.q2d_serve_admit.restype = C.c_int
+    lib.q2d_serve_admit.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), PD, PD, PD,
+                                    C.POINTER(BCRec), C.c_int, C.POINTER(C.c_int)]
+    lib.q2d_serve_retire.restype = C.c_int
+    lib.q2d_serve_retire.argtypes = [C.c_void_p, C.c_int]
+    lib.q2d_serve_block_id.restype = C.c_int
+    lib.q2d_serve_block_id.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]
+    lib.q2d_serve_free_cells.restype = C.c_longlong
+    lib.q2d_serve_free_cells.argtypes = [C.c_void_p]
     _LIB = lib
     return lib
 

@@ -1,9 +1,17 @@
-// q2d_api.cu — host runtime behind include/q2d_gpu.h: contexts, device memory, work lists,
-// CUDA-graph execution of N explicit steps, state transfer.
+// q2d_api.cu — host runtime behind include/q2d_gpu.h: contexts, device pools and their
+// allocators, work lists, CUDA-graph execution of N explicit steps, state transfer, the
+// schedule autotuner and the serving (continuous batching) entry points.
 //
 // Replaces, for one grid level: Assign_Setup (procedure-pointer binding -> kernel selection),
-// Allocate_Block / Setup_Metrics (device pools built at commit), and the Explicit_Step loop
-// (a captured graph of n_rk fused stage kernels per step; Mod_Explicit.f90:10-174).
+// Allocate_Block / Setup_Metrics (per-case device regions filled when the case is
+// materialised), and the Explicit_Step loop (a captured graph of n_rk fused stage kernels per
+// step; Mod_Explicit.f90:10-174). The reference's single domain becomes a "case"; a context
+// holds many cases, each with its own dtglobal, time, iteration count, residual and TODO state.
+//
+// Batch contexts (q2d_gpu_create ... commit) size their pools exactly for the cases added
+// before commit. Serving contexts (q2d_serve_create) size the pools from a byte budget and
+// admit / retire cases between steps; admission does its host work (validation, metrics)
+// at once and defers every device write to the next step call, after the work in flight.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,18 +30,30 @@ using namespace q2d;
 
 namespace {
 
+// Device images of one block, built on the host when its case is prepared and copied to the
+// block's regions when the case is uploaded.
+struct Staged {
+    std::vector<double> pa, sc, dl, fi, fj;
+};
+
 struct HBlock {
-    int ni, nj, case_id, local_b;
+    int ni = 0, nj = 0, case_id = -1, local_b = 0;
     std::vector<double> nodes, area;
-    std::vector<double> prim;   // 4 planes, interior
-    HostGeom geom;
+    std::vector<double> prim;      // 4 planes, interior (until the case is prepared)
+    std::vector<EdgeRec> edge[4];  // records of faces 1..4 (param: index into the case's params)
+    Staged staged;
     DBlock d{};
+    bool alive = false;            // holds device regions
 };
 
 struct HCase {
-    std::vector<int> blocks;
+    std::vector<int> blocks;       // global block ids
     std::vector<q2d_bc_rec> bc;
+    std::vector<BCParam> params;
     double time0 = 0.0;
+    bool used = false;             // slot holds a case
+    bool prepared = false;         // regions reserved, device images staged
+    bool resident = false;         // device images and run state uploaded
 };
 
 template <typename T>
@@ -51,7 +71,60 @@ struct DevBuf {
     }
 };
 
+// First-fit allocator over an index space [0, cap) of a pool (offsets in elements).
+struct Arena {
+    long long cap = 0;
+    std::map<long long, long long> free;   // offset -> length, coalesced
+    void init(long long c) {
+        cap = c;
+        free.clear();
+        if (c > 0) free[0] = c;
+    }
+    bool alloc(long long n, long long* off) {
+        for (auto it = free.begin(); it != free.end(); ++it)
+            if (it->second >= n) {
+                *off = it->first;
+                const long long rest = it->second - n, o = it->first + n;
+                free.erase(it);
+                if (rest > 0) free[o] = rest;
+                return true;
+            }
+        return false;
+    }
+    void release(long long off, long long n) {
+        if (n <= 0) return;
+        auto it = free.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != free.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free.erase(nx);
+        }
+        if (it != free.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free.erase(it);
+            }
+        }
+    }
+    long long free_total() const {
+        long long t = 0;
+        for (auto& kv : free) t += kv.second;
+        return t;
+    }
+};
+
 long long round32(long long n) { return (n + 31) / 32 * 32; }
+
+// Element counts of one block's regions: 4-plane cell space, 2-plane ghost frame, 3-plane
+// i-face and j-face spaces. Planes are padded to 32 elements (256 B).
+struct Extents {
+    long long pc, pg, pfi, pfj;
+};
+Extents block_extents(int ni, int nj) {
+    return {round32((long long)ni * nj), round32((long long)(ni + 4) * (nj + 4)),
+            round32((long long)(ni + 1) * nj), round32((long long)ni * (nj + 1))};
+}
 
 }  // namespace
 
@@ -62,15 +135,20 @@ struct q2d_ctx {
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     std::vector<HBlock> blocks;
-    std::vector<HCase> cases;
+    std::vector<HCase> cases;     // slots
+    bool serving = false;
     bool committed = false;
-    bool dt_valid = false;
+    bool dt_valid = false;        // every running case has its time step
+    bool dt_new = false;          // some case was uploaded after the last time-step pass
+    bool dirty = false;           // uploads, slot resets or list rebuild pending
+    std::vector<int> reset_slots; // retired slots whose device run state still has to be reset
     int tile = 0;
     int kernel = 0;       // 0: CTA-tile stage kernel, 1: warp-marching stage kernel
     int march_h = 16;     // rows per warp-marching item
     int grid = 0;
-    // device pools
+    // device pools and their allocators
     DevBuf<double> PA, PB, PC, SC, DL, FI, FJ, PART;
+    Arena ac, ag, afi, afj;
     DevBuf<DBlock> dblocks;
     DevBuf<DCase> dcases;
     DevBuf<CaseState> cstate;
@@ -79,8 +157,7 @@ struct q2d_ctx {
     DevBuf<BCParam> bcp;
     DevBuf<int> flag;
     CaseState* h_state = nullptr;   // pinned mirror
-    long long total_cells = 0;
-    long long pool4 = 0;            // elements of a 4-plane cell pool
+    int n_items = 0;
     std::map<int, cudaGraphExec_t> graphs;
     std::map<int, int> graph_kernels;
     long long launches = 0;
@@ -99,9 +176,9 @@ int cuda_fail(q2d_ctx* c, cudaError_t e, const char* where) {
     return Q2D_ERR_CUDA;
 }
 
-#define CK(call)                                              \
-    do {                                                      \
-        cudaError_t e_ = (call);                              \
+#define CK(call)                                                 \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
     } while (0)
 
@@ -111,7 +188,7 @@ StageArgs base_args(q2d_ctx* ctx) {
     a.cases = ctx->dcases.p;
     a.cstate = ctx->cstate.p;
     a.items = ctx->items.p;
-    a.n_items = (int)ctx->items.n;
+    a.n_items = ctx->n_items;
     a.sc = ctx->SC.p;
     a.dl = ctx->DL.p;
     a.dl32 = nullptr;
@@ -149,6 +226,7 @@ double rk_coeff(int n_rk, int irk) {
 // stage of RK3 reads C and updates A in place (each cell reads only its own U^n from A).
 int enqueue_step(q2d_ctx* ctx, cudaStream_t s, int* nk) {
     const int n_rk = ctx->opt.n_rk;
+    if (ctx->n_items == 0) return Q2D_OK;
     for (int irk = 1; irk <= n_rk; ++irk) {
         StageArgs a = base_args(ctx);
         a.irk = irk;
@@ -172,21 +250,34 @@ int enqueue_step(q2d_ctx* ctx, cudaStream_t s, int* nk) {
         ++*nk;
     }
     if (n_rk == 1) {
-        CK(launch_copy(ctx->PB.p, ctx->PA.p, ctx->pool4, ctx->flag.p, s));
+        CK(launch_copy(ctx->PB.p, ctx->PA.p, ctx->ac.cap, ctx->flag.p, s));
         ++*nk;
     }
     return Q2D_OK;
 }
 
+// Compute_dt for the cases that need it: every running case after a state upload, only the
+// newly uploaded ones after an admission (the others keep the time step their last stage
+// computed, so a case's trajectory does not depend on when other cases arrive).
 int ensure_dt(q2d_ctx* ctx) {
-    if (ctx->dt_valid) return Q2D_OK;
-    StageArgs a = base_args(ctx);
-    a.Pin = ctx->PA.p;
-    if (ctx->kernel == 1) CK(launch_dt_march(a, ctx->grid, ctx->stream));
-    else CK(launch_dt(a, ctx->tile, ctx->grid, ctx->stream));
-    ctx->launches += 1;
+    if (ctx->dt_valid && !ctx->dt_new) return Q2D_OK;
+    if (ctx->n_items > 0) {
+        StageArgs a = base_args(ctx);
+        a.Pin = ctx->PA.p;
+        a.first = ctx->dt_valid ? 1 : 0;   // pending-only pass
+        if (ctx->kernel == 1) CK(launch_dt_march(a, ctx->grid, ctx->stream));
+        else CK(launch_dt(a, ctx->tile, ctx->grid, ctx->stream));
+        ctx->launches += 1;
+    }
     ctx->dt_valid = true;
+    ctx->dt_new = false;
     return Q2D_OK;
+}
+
+void drop_graphs(q2d_ctx* ctx) {
+    for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+    ctx->graphs.clear();
+    ctx->graph_kernels.clear();
 }
 
 int get_graph(q2d_ctx* ctx, int nsteps, cudaGraphExec_t* out) {
@@ -229,39 +320,263 @@ bool rec_less(const q2d_bc_rec& a, const q2d_bc_rec& b) {
     return a.b != b.b ? a.b < b.b : a.f < b.f;
 }
 
+CaseState fresh_state(double time0) {
+    CaseState s;
+    std::memset(&s, 0, sizeof(s));
+    s.res0 = -1.0;
+    s.todo = Q2D_TODO_CONTINUE;
+    s.status = kStatus_Running;
+    s.time = time0;
+    s.time_from_call = time0;
+    s.dt_pending = 1;
+    return s;
+}
 
-// Work items of the current schedule (kernel / tile / rows per item), grouped by case, and
-// the persistent grid size. Re-run by the autotuner for every candidate schedule.
-int build_items(q2d_ctx* ctx) {
+CaseState empty_state() {
+    CaseState s;
+    std::memset(&s, 0, sizeof(s));
+    s.res0 = -1.0;
+    s.todo = Q2D_TODO_END;
+    s.status = kStatus_Done;
+    return s;
+}
+
+// Grows a device buffer to at least n elements (contents are not kept).
+template <typename T>
+cudaError_t ensure_cap(DevBuf<T>& b, size_t n) {
+    if (b.p && b.n >= n) return cudaSuccess;
+    b.release();
+    return b.alloc(std::max<size_t>(n, 1) + n / 4);
+}
+
+// Validates the boundary records of a case and derives per-block edge records and the
+// parameters of its inflow / outflow faces.
+int build_case_edges(q2d_ctx* ctx, int c) {
+    HCase& cs = ctx->cases[c];
+    cs.params.clear();
+    for (int gb : cs.blocks) {
+        HBlock& B = ctx->blocks[gb];
+        const int len[4] = {B.nj, B.nj, B.ni, B.ni};
+        for (int f = 0; f < 4; ++f) B.edge[f].assign(len[f], EdgeRec{-1, 0, 0, 0, 0, -1});
+    }
+    for (const q2d_bc_rec& r : cs.bc) {
+        HBlock& B = ctx->blocks[cs.blocks[r.b - 1]];
+        const bool pos_ok = (r.f == 1 && r.i == 1) || (r.f == 2 && r.i == B.ni) ||
+                            (r.f == 3 && r.j == 1) || (r.f == 4 && r.j == B.nj);
+        if (!pos_ok) return fail(ctx, Q2D_ERR_BADARG, "boundary record not on its face");
+        const int k = (r.f <= 2) ? r.j - 1 : r.i - 1;
+        EdgeRec& er = B.edge[r.f - 1][k];
+        if (er.type != -1) return fail(ctx, Q2D_ERR_BADARG, "duplicate boundary record");
+        er.type = r.type;
+        if (r.type == 101) {
+            const HBlock& D = ctx->blocks[cs.blocks[r.bs - 1]];
+            const int gi = r.fs == 1 ? 1 : (r.fs == 2 ? -1 : 0);
+            const int gj = r.fs == 3 ? 1 : (r.fs == 4 ? -1 : 0);
+            for (int g = 0; g < 2; ++g) {
+                const int si = r.is + gi * g, sj = r.js + gj * g;
+                if (si < 1 || si > D.ni || sj < 1 || sj > D.nj)
+                    return fail(ctx, Q2D_ERR_BADARG, "connection donor cell outside its block");
+            }
+            er.bs = cs.blocks[r.bs - 1];
+            er.is = r.is; er.js = r.js; er.fs = r.fs;
+        }
+        if (r.type == 401 || r.type == 405 || r.type == 406) {
+            BCParam p{};
+            p.T0 = r.T0; p.p0 = r.p0; p.pamb = r.pamb; p.mach = r.mach;
+            p.alpha = r.alpha; p.rel_fac = r.rel_fac;
+            face_tangent(r, B.ni, B.nodes.data(), &p.t0, &p.t1);
+            er.param = (int)cs.params.size();
+            cs.params.push_back(p);
+        }
+    }
+    for (int gb : cs.blocks) {
+        const HBlock& B = ctx->blocks[gb];
+        for (int f = 0; f < 4; ++f)
+            for (const EdgeRec& e : B.edge[f])
+                if (e.type == -1)
+                    return fail(ctx, Q2D_ERR_BADARG, "boundary cell without a record (block " +
+                                std::to_string(B.local_b) + ", face " + std::to_string(f + 1) + ")");
+    }
+    return Q2D_OK;
+}
+
+void release_regions(q2d_ctx* ctx, HBlock& b) {
+    if (!b.alive) return;
+    ctx->ac.release(b.d.oc, 4 * b.d.pc);
+    ctx->ag.release(b.d.og, 2 * b.d.pg);
+    ctx->afi.release(b.d.ofi, 3 * b.d.pfi);
+    ctx->afj.release(b.d.ofj, 3 * b.d.pfj);
+    b.alive = false;
+}
+
+// Reserves the device regions of every block of a case (all or nothing).
+bool reserve_regions(q2d_ctx* ctx, int c) {
+    HCase& cs = ctx->cases[c];
+    for (size_t k = 0; k < cs.blocks.size(); ++k) {
+        HBlock& b = ctx->blocks[cs.blocks[k]];
+        DBlock& d = b.d;
+        const Extents x = block_extents(b.ni, b.nj);
+        d = DBlock{};
+        d.ni = b.ni; d.nj = b.nj; d.case_id = c; d.local_b = b.local_b;
+        d.pc = x.pc; d.pg = x.pg; d.pfi = x.pfi; d.pfj = x.pfj;
+        long long oc, og, ofi, ofj;
+        bool okc = ctx->ac.alloc(4 * x.pc, &oc);
+        bool okg = okc && ctx->ag.alloc(2 * x.pg, &og);
+        bool oki = okg && ctx->afi.alloc(3 * x.pfi, &ofi);
+        bool okj = oki && ctx->afj.alloc(3 * x.pfj, &ofj);
+        if (!okj) {
+            if (oki) ctx->afi.release(ofi, 3 * x.pfi);
+            if (okg) ctx->ag.release(og, 2 * x.pg);
+            if (okc) ctx->ac.release(oc, 4 * x.pc);
+            for (size_t q = 0; q < k; ++q) release_regions(ctx, ctx->blocks[cs.blocks[q]]);
+            return false;
+        }
+        d.oc = oc; d.og = og; d.ofi = ofi; d.ofj = ofj;
+        b.alive = true;
+    }
+    return true;
+}
+
+// Host half of materialising a case: edge records, device regions, metrics (Setup_Metrics
+// restated on the host) and the device images of every block, staged for upload.
+int prepare_case(q2d_ctx* ctx, int c) {
+    HCase& cs = ctx->cases[c];
+    if (int e = build_case_edges(ctx, c)) return e;
+    std::vector<HostGeom> geo(cs.blocks.size());
+    for (size_t lb = 0; lb < cs.blocks.size(); ++lb) {
+        HBlock& b = ctx->blocks[cs.blocks[lb]];
+        int e = setup_block(b.ni, b.nj, b.nodes.data(), b.area.empty() ? nullptr : b.area.data(),
+                            ctx->opt.source, geo[lb]);
+        if (e) return fail(ctx, e, "degenerate cell in block " + std::to_string(b.local_b));
+    }
+    for (const q2d_bc_rec& r : cs.bc) {
+        HBlock& B = ctx->blocks[cs.blocks[r.b - 1]];
+        const HBlock* D = r.type == 101 ? &ctx->blocks[cs.blocks[r.bs - 1]] : nullptr;
+        int e = ghost_metrics(r, B.ni, B.nj, B.nodes.data(), geo[r.b - 1], D ? D->ni : 0, D ? D->nj : 0,
+                              D ? D->nodes.data() : nullptr);
+        if (e) return fail(ctx, e, "ghost metrics failed for a boundary record");
+    }
+    if (!reserve_regions(ctx, c)) return fail(ctx, Q2D_ERR_CAPACITY, "device memory budget exhausted");
+    for (size_t lb = 0; lb < cs.blocks.size(); ++lb) {
+        HBlock& b = ctx->blocks[cs.blocks[lb]];
+        const DBlock& d = b.d;
+        const HostGeom& G = geo[lb];
+        const long long n = (long long)b.ni * b.nj;
+        Staged& S = b.staged;
+        S.sc.assign(8 * (size_t)d.pc, 0.0);
+        S.dl.assign(2 * (size_t)d.pg, 0.0);
+        S.fi.assign(3 * (size_t)d.pfi, 0.0);
+        S.fj.assign(3 * (size_t)d.pfj, 0.0);
+        S.pa.assign(4 * (size_t)d.pc, 0.0);
+        for (int j = 0; j < b.nj; ++j)
+            for (int i = 0; i < b.ni; ++i) {
+                const long long k = (long long)j * b.ni + i;
+                double v[4];
+                versors(G, i, j, v);
+                S.sc[k] = G.sur[G.g(i, j)];
+                S.sc[2 * d.pc + k] = v[0];
+                S.sc[3 * d.pc + k] = v[1];
+                S.sc[4 * d.pc + k] = v[2];
+                S.sc[5 * d.pc + k] = v[3];
+                S.sc[6 * d.pc + k] = G.src0[k];
+                S.sc[7 * d.pc + k] = G.src1[k];
+            }
+        for (long long k = 0; k < (long long)(b.ni + 4) * (b.nj + 4); ++k) {
+            S.dl[k] = G.dl[2 * k];
+            S.dl[d.pg + k] = G.dl[2 * k + 1];
+        }
+        for (long long k = 0; k < (long long)(b.ni + 1) * b.nj; ++k)
+            for (int q = 0; q < 3; ++q) S.fi[q * d.pfi + k] = G.fi[3 * k + q];
+        for (long long k = 0; k < (long long)b.ni * (b.nj + 1); ++k)
+            for (int q = 0; q < 3; ++q) S.fj[q * d.pfj + k] = G.fj[3 * k + q];
+        for (int v = 0; v < 4; ++v) std::memcpy(&S.pa[v * d.pc], &b.prim[(size_t)v * n], sizeof(double) * n);
+        b.prim.clear();
+        b.prim.shrink_to_fit();
+        geo[lb] = HostGeom{};
+    }
+    cs.prepared = true;
+    return Q2D_OK;
+}
+
+// Device half: copies the staged images into the case's regions and starts its run state.
+// Called only while no work is in flight on the context's stream.
+int upload_case(q2d_ctx* ctx, int c) {
+    HCase& cs = ctx->cases[c];
+    for (int gb : cs.blocks) {
+        HBlock& b = ctx->blocks[gb];
+        const DBlock& d = b.d;
+        Staged& S = b.staged;
+        CK(cudaMemcpy(ctx->PA.p + d.oc, S.pa.data(), sizeof(double) * S.pa.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->SC.p + 2 * d.oc, S.sc.data(), sizeof(double) * S.sc.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->DL.p + d.og, S.dl.data(), sizeof(double) * S.dl.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->FI.p + d.ofi, S.fi.data(), sizeof(double) * S.fi.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->FJ.p + d.ofj, S.fj.data(), sizeof(double) * S.fj.size(), cudaMemcpyHostToDevice));
+        S = Staged{};
+    }
+    const CaseState s = fresh_state(cs.time0);
+    CK(cudaMemcpy(ctx->cstate.p + c, &s, sizeof(CaseState), cudaMemcpyHostToDevice));
+    cs.resident = true;
+    ctx->dt_new = true;
+    return Q2D_OK;
+}
+
+// Device descriptor arrays (blocks, edge records, BC parameters, work items, per-case item
+// ranges) of the resident cases, and the persistent grid size. Called only while no work is
+// in flight on the context's stream.
+int rebuild_device_lists(q2d_ctx* ctx) {
     int TX, TY, NT;
     tile_dims(ctx->tile, &TX, &TY, &NT);
+    std::vector<DBlock> db(ctx->blocks.size());
+    std::vector<EdgeRec> edges;
+    std::vector<BCParam> params;
     std::vector<WorkItem> items;
-    std::vector<DCase> dcases(ctx->cases.size());
+    std::vector<DCase> dcases(ctx->cases.size(), DCase{0, 0, 2, 0});
     for (size_t c = 0; c < ctx->cases.size(); ++c) {
+        HCase& cs = ctx->cases[c];
         dcases[c].item_begin = (int)items.size();
-        for (int gb : ctx->cases[c].blocks) {
-            const HBlock& B = ctx->blocks[gb];
-            if (ctx->kernel == 1) {
-                for (int i0 = 0; i0 < B.ni; i0 += kMarchCols)
-                    for (int j0 = 0; j0 < B.nj; j0 += ctx->march_h)
-                        items.push_back(WorkItem{gb, i0, j0, (int)c, std::min(B.nj, j0 + ctx->march_h), 0});
-            } else {
-                for (int j0 = 0; j0 < B.nj; j0 += TY)
-                    for (int i0 = 0; i0 < B.ni; i0 += TX) items.push_back(WorkItem{gb, i0, j0, (int)c, 0, 0});
+        if (cs.used && cs.resident) {
+            const int pbase = (int)params.size();
+            params.insert(params.end(), cs.params.begin(), cs.params.end());
+            for (int gb : cs.blocks) {
+                HBlock& B = ctx->blocks[gb];
+                for (int f = 0; f < 4; ++f) {
+                    B.d.eo[f] = (int)edges.size();
+                    for (EdgeRec e : B.edge[f]) {
+                        if (e.param >= 0) e.param += pbase;
+                        edges.push_back(e);
+                    }
+                }
+                if (ctx->kernel == 1) {
+                    for (int i0 = 0; i0 < B.ni; i0 += kMarchCols)
+                        for (int j0 = 0; j0 < B.nj; j0 += ctx->march_h)
+                            items.push_back(WorkItem{gb, i0, j0, (int)c, std::min(B.nj, j0 + ctx->march_h), 0});
+                } else {
+                    for (int j0 = 0; j0 < B.nj; j0 += TY)
+                        for (int i0 = 0; i0 < B.ni; i0 += TX) items.push_back(WorkItem{gb, i0, j0, (int)c, 0, 0});
+                }
             }
+            dcases[c].ndir = ctx->blocks[cs.blocks[0]].nj == 1 ? 1 : 2;
         }
         dcases[c].item_end = (int)items.size();
-        dcases[c].ndir = ctx->blocks[ctx->cases[c].blocks[0]].nj == 1 ? 1 : 2;
     }
-    ctx->items.release();
-    ctx->PART.release();
-    ctx->dcases.release();
-    CK(ctx->items.alloc(items.size()));
-    CK(ctx->PART.alloc(5 * items.size()));
-    CK(ctx->dcases.alloc(dcases.size()));
-    CK(cudaMemcpy(ctx->items.p, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice));
+    for (size_t k = 0; k < ctx->blocks.size(); ++k) db[k] = ctx->blocks[k].d;
+    CK(ensure_cap(ctx->dblocks, db.size()));
+    CK(ensure_cap(ctx->edges, edges.size()));
+    CK(ensure_cap(ctx->bcp, params.size()));
+    CK(ensure_cap(ctx->items, items.size()));
+    if (!ctx->PART.p || ctx->PART.n < 5 * items.size()) {
+        CK(ensure_cap(ctx->PART, 5 * items.size()));
+        CK(cudaMemset(ctx->PART.p, 0, sizeof(double) * ctx->PART.n));
+    }
+    if (!db.empty()) CK(cudaMemcpy(ctx->dblocks.p, db.data(), sizeof(DBlock) * db.size(), cudaMemcpyHostToDevice));
+    if (!edges.empty())
+        CK(cudaMemcpy(ctx->edges.p, edges.data(), sizeof(EdgeRec) * edges.size(), cudaMemcpyHostToDevice));
+    if (!params.empty())
+        CK(cudaMemcpy(ctx->bcp.p, params.data(), sizeof(BCParam) * params.size(), cudaMemcpyHostToDevice));
+    if (!items.empty())
+        CK(cudaMemcpy(ctx->items.p, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->dcases.p, dcases.data(), sizeof(DCase) * dcases.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemset(ctx->PART.p, 0, sizeof(double) * 5 * items.size()));
+    ctx->n_items = (int)items.size();
     if (ctx->kernel == 1) {
         const int occ = std::max(1, march_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter));
         ctx->grid = (int)std::min<long long>(((long long)items.size() + 3) / 4, (long long)occ * ctx->num_sms);
@@ -270,189 +585,94 @@ int build_items(q2d_ctx* ctx) {
         ctx->grid = (int)std::min<long long>((long long)items.size(), (long long)occ * ctx->num_sms);
     }
     if (ctx->grid < 1) ctx->grid = 1;
-    for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
-    ctx->graphs.clear();
-    ctx->graph_kernels.clear();
+    drop_graphs(ctx);
+    return Q2D_OK;
+}
+
+// Applies what admissions and retirements left for the device, after the work in flight.
+int apply_pending(q2d_ctx* ctx) {
+    if (!ctx->dirty) return Q2D_OK;
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int c : ctx->reset_slots) {
+        if (ctx->cases[c].used) continue;   // slot taken again: the upload below starts it
+        const CaseState s = empty_state();
+        CK(cudaMemcpy(ctx->cstate.p + c, &s, sizeof(CaseState), cudaMemcpyHostToDevice));
+    }
+    ctx->reset_slots.clear();
+    for (size_t c = 0; c < ctx->cases.size(); ++c) {
+        HCase& cs = ctx->cases[c];
+        if (cs.used && cs.prepared && !cs.resident)
+            if (int e = upload_case(ctx, (int)c)) return e;
+    }
+    if (int e = rebuild_device_lists(ctx)) return e;
+    ctx->dirty = false;
+    return Q2D_OK;
+}
+
+int allocate_pools(q2d_ctx* ctx, long long ec, long long eg, long long efi, long long efj, int ncases) {
+    CK(ctx->PA.alloc(ec)); CK(ctx->PB.alloc(ec)); CK(ctx->PC.alloc(ec));
+    CK(ctx->SC.alloc(2 * ec)); CK(ctx->DL.alloc(eg)); CK(ctx->FI.alloc(efi)); CK(ctx->FJ.alloc(efj));
+    CK(cudaMemset(ctx->PB.p, 0, sizeof(double) * (ec ? ec : 1)));
+    CK(cudaMemset(ctx->PC.p, 0, sizeof(double) * (ec ? ec : 1)));
+    ctx->ac.init(ec); ctx->ag.init(eg); ctx->afi.init(efi); ctx->afj.init(efj);
+    CK(ctx->dcases.alloc(ncases));
+    CK(ctx->cstate.alloc(ncases));
+    CK(ctx->flag.alloc(1));
+    CK(cudaMallocHost(&ctx->h_state, sizeof(CaseState) * ncases));
+    std::vector<CaseState> st(ncases, empty_state());   // empty slots read as finished
+    CK(cudaMemcpy(ctx->cstate.p, st.data(), sizeof(CaseState) * ncases, cudaMemcpyHostToDevice));
     return Q2D_OK;
 }
 
 int commit(q2d_ctx* ctx) {
     if (ctx->committed) return Q2D_OK;
     if (ctx->cases.empty()) return fail(ctx, Q2D_ERR_BADARG, "no case");
-    // ---- boundary records -> edge arrays (geometry of ghost cells is added per block below) --
-    std::vector<EdgeRec> edges;
-    std::vector<BCParam> params;
+    long long ec = 0, eg = 0, efi = 0, efj = 0;
+    for (const HBlock& b : ctx->blocks) {
+        const Extents x = block_extents(b.ni, b.nj);
+        ec += 4 * x.pc; eg += 2 * x.pg; efi += 3 * x.pfi; efj += 3 * x.pfj;
+    }
+    for (size_t c = 0; c < ctx->cases.size(); ++c)
+        if (ctx->cases[c].blocks.empty()) return fail(ctx, Q2D_ERR_BADARG, "case without blocks");
+    if (int e = allocate_pools(ctx, ec, eg, efi, efj, (int)ctx->cases.size())) return e;
+    // prepared and uploaded case by case: host memory stays at one case's images
     for (size_t c = 0; c < ctx->cases.size(); ++c) {
-        HCase& cs = ctx->cases[c];
-        if (cs.blocks.empty()) return fail(ctx, Q2D_ERR_BADARG, "case without blocks");
-        for (int gb : cs.blocks) {
-            HBlock& B = ctx->blocks[gb];
-            const int len[4] = {B.nj, B.nj, B.ni, B.ni};
-            for (int f = 0; f < 4; ++f) {
-                B.d.eo[f] = (int)edges.size();
-                edges.resize(edges.size() + len[f], EdgeRec{-1, 0, 0, 0, 0, -1});
-            }
-        }
-        for (const q2d_bc_rec& r : cs.bc) {
-            HBlock& B = ctx->blocks[cs.blocks[r.b - 1]];
-            const bool pos_ok = (r.f == 1 && r.i == 1) || (r.f == 2 && r.i == B.ni) ||
-                                (r.f == 3 && r.j == 1) || (r.f == 4 && r.j == B.nj);
-            if (!pos_ok) return fail(ctx, Q2D_ERR_BADARG, "boundary record not on its face");
-            const int k = (r.f <= 2) ? r.j - 1 : r.i - 1;
-            EdgeRec& er = edges[B.d.eo[r.f - 1] + k];
-            if (er.type != -1) return fail(ctx, Q2D_ERR_BADARG, "duplicate boundary record");
-            er.type = r.type;
-            if (r.type == 101) {
-                const HBlock& D = ctx->blocks[cs.blocks[r.bs - 1]];
-                const int gi = r.fs == 1 ? 1 : (r.fs == 2 ? -1 : 0);
-                const int gj = r.fs == 3 ? 1 : (r.fs == 4 ? -1 : 0);
-                for (int g = 0; g < 2; ++g) {
-                    const int si = r.is + gi * g, sj = r.js + gj * g;
-                    if (si < 1 || si > D.ni || sj < 1 || sj > D.nj)
-                        return fail(ctx, Q2D_ERR_BADARG, "connection donor cell outside its block");
-                }
-                er.bs = cs.blocks[r.bs - 1];
-                er.is = r.is; er.js = r.js; er.fs = r.fs;
-            }
-            if (r.type == 401 || r.type == 405 || r.type == 406) {
-                BCParam p{};
-                p.T0 = r.T0; p.p0 = r.p0; p.pamb = r.pamb; p.mach = r.mach;
-                p.alpha = r.alpha; p.rel_fac = r.rel_fac;
-                face_tangent(r, B.ni, B.nodes.data(), &p.t0, &p.t1);
-                er.param = (int)params.size();
-                params.push_back(p);
-            }
-        }
-        for (int gb : cs.blocks) {
-            const HBlock& B = ctx->blocks[gb];
-            const int len[4] = {B.nj, B.nj, B.ni, B.ni};
-            for (int f = 0; f < 4; ++f)
-                for (int k = 0; k < len[f]; ++k)
-                    if (edges[B.d.eo[f] + k].type == -1)
-                        return fail(ctx, Q2D_ERR_BADARG, "boundary cell without a record (block " +
-                                    std::to_string(B.local_b) + ", face " + std::to_string(f + 1) + ")");
-        }
+        ctx->cases[c].used = true;
+        if (int e = prepare_case(ctx, (int)c)) return e;
+        if (int e = upload_case(ctx, (int)c)) return e;
     }
-    // ---- pool layout ---------------------------------------------------------------------
-    long long oc = 0, og = 0, ofi = 0, ofj = 0;
-    for (HBlock& b : ctx->blocks) {
-        DBlock& d = b.d;
-        d.ni = b.ni; d.nj = b.nj; d.case_id = b.case_id; d.local_b = b.local_b;
-        d.pc = round32((long long)b.ni * b.nj);
-        d.pg = round32((long long)(b.ni + 4) * (b.nj + 4));
-        d.pfi = round32((long long)(b.ni + 1) * b.nj);
-        d.pfj = round32((long long)b.ni * (b.nj + 1));
-        d.oc = oc; d.og = og; d.ofi = ofi; d.ofj = ofj; d.on = 0; d.pn = 0;
-        oc += 4 * d.pc; og += 2 * d.pg; ofi += 3 * d.pfi; ofj += 3 * d.pfj;
-    }
-    ctx->pool4 = oc;
-    // ---- device pools, filled block by block (host memory stays at one block) -------------
-    CK(ctx->PA.alloc(oc)); CK(ctx->PB.alloc(oc)); CK(ctx->PC.alloc(oc));
-    CK(ctx->SC.alloc(2 * oc)); CK(ctx->DL.alloc(og)); CK(ctx->FI.alloc(ofi)); CK(ctx->FJ.alloc(ofj));
-    CK(cudaMemset(ctx->PB.p, 0, sizeof(double) * oc));
-    CK(cudaMemset(ctx->PC.p, 0, sizeof(double) * oc));
-    for (size_t c = 0; c < ctx->cases.size(); ++c) {
-        HCase& cs = ctx->cases[c];
-        for (int gb : cs.blocks) {
-            HBlock& b = ctx->blocks[gb];
-            int e = setup_block(b.ni, b.nj, b.nodes.data(), b.area.empty() ? nullptr : b.area.data(),
-                                ctx->opt.source, b.geom);
-            if (e) return fail(ctx, e, "degenerate cell in block " + std::to_string(b.local_b));
-        }
-        for (const q2d_bc_rec& r : cs.bc) {
-            HBlock& B = ctx->blocks[cs.blocks[r.b - 1]];
-            const HBlock* D = r.type == 101 ? &ctx->blocks[cs.blocks[r.bs - 1]] : nullptr;
-            int e = ghost_metrics(r, B.ni, B.nj, B.nodes.data(), B.geom, D ? D->ni : 0, D ? D->nj : 0,
-                                  D ? D->nodes.data() : nullptr);
-            if (e) return fail(ctx, e, "ghost metrics failed for a boundary record");
-        }
-        for (int gb : cs.blocks) {
-            HBlock& b = ctx->blocks[gb];
-            const DBlock& d = b.d;
-            const HostGeom& G = b.geom;
-            const long long n = (long long)b.ni * b.nj;
-            std::vector<double> sc(8 * (size_t)d.pc, 0.0), dl(2 * (size_t)d.pg, 0.0), fi(3 * (size_t)d.pfi, 0.0),
-                fj(3 * (size_t)d.pfj, 0.0), pa(4 * (size_t)d.pc, 0.0);
-            for (int j = 0; j < b.nj; ++j)
-                for (int i = 0; i < b.ni; ++i) {
-                    const long long k = (long long)j * b.ni + i;
-                    double v[4];
-                    versors(G, i, j, v);
-                    sc[k] = G.sur[G.g(i, j)];
-                    sc[2 * d.pc + k] = v[0];
-                    sc[3 * d.pc + k] = v[1];
-                    sc[4 * d.pc + k] = v[2];
-                    sc[5 * d.pc + k] = v[3];
-                    sc[6 * d.pc + k] = G.src0[k];
-                    sc[7 * d.pc + k] = G.src1[k];
-                }
-            for (long long k = 0; k < (long long)(b.ni + 4) * (b.nj + 4); ++k) {
-                dl[k] = G.dl[2 * k];
-                dl[d.pg + k] = G.dl[2 * k + 1];
-            }
-            for (long long k = 0; k < (long long)(b.ni + 1) * b.nj; ++k)
-                for (int q = 0; q < 3; ++q) fi[q * d.pfi + k] = G.fi[3 * k + q];
-            for (long long k = 0; k < (long long)b.ni * (b.nj + 1); ++k)
-                for (int q = 0; q < 3; ++q) fj[q * d.pfj + k] = G.fj[3 * k + q];
-            for (int v = 0; v < 4; ++v) std::memcpy(&pa[v * d.pc], &b.prim[(size_t)v * n], sizeof(double) * n);
-            CK(cudaMemcpy(ctx->PA.p + d.oc, pa.data(), sizeof(double) * pa.size(), cudaMemcpyHostToDevice));
-            CK(cudaMemcpy(ctx->SC.p + 2 * d.oc, sc.data(), sizeof(double) * sc.size(), cudaMemcpyHostToDevice));
-            CK(cudaMemcpy(ctx->DL.p + d.og, dl.data(), sizeof(double) * dl.size(), cudaMemcpyHostToDevice));
-            CK(cudaMemcpy(ctx->FI.p + d.ofi, fi.data(), sizeof(double) * fi.size(), cudaMemcpyHostToDevice));
-            CK(cudaMemcpy(ctx->FJ.p + d.ofj, fj.data(), sizeof(double) * fj.size(), cudaMemcpyHostToDevice));
-            ctx->total_cells += n;
-            b.prim.clear(); b.prim.shrink_to_fit();
-            b.geom = HostGeom{};
-        }
-    }
-    std::vector<DBlock> db(ctx->blocks.size());
-    for (size_t k = 0; k < ctx->blocks.size(); ++k) db[k] = ctx->blocks[k].d;
-    std::vector<CaseState> st(ctx->cases.size());
-    for (size_t c = 0; c < ctx->cases.size(); ++c) {
-        CaseState& s = st[c];
-        std::memset(&s, 0, sizeof(s));
-        s.res0 = -1.0;
-        s.todo = Q2D_TODO_CONTINUE;
-        s.status = kStatus_Running;
-        s.time = ctx->cases[c].time0;
-        s.time_from_call = s.time;
-    }
-    CK(ctx->dblocks.alloc(db.size()));
-    CK(ctx->cstate.alloc(st.size()));
-    CK(ctx->edges.alloc(edges.size())); CK(ctx->bcp.alloc(params.size())); CK(ctx->flag.alloc(1));
-    CK(cudaMallocHost(&ctx->h_state, sizeof(CaseState) * st.size()));
-    CK(cudaMemcpy(ctx->dblocks.p, db.data(), sizeof(DBlock) * db.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->cstate.p, st.data(), sizeof(CaseState) * st.size(), cudaMemcpyHostToDevice));
-    if (!edges.empty()) CK(cudaMemcpy(ctx->edges.p, edges.data(), sizeof(EdgeRec) * edges.size(), cudaMemcpyHostToDevice));
-    if (!params.empty()) CK(cudaMemcpy(ctx->bcp.p, params.data(), sizeof(BCParam) * params.size(), cudaMemcpyHostToDevice));
-    {
-        int e = build_items(ctx);
-        if (e) return e;
-    }
+    if (int e = rebuild_device_lists(ctx)) return e;
     ctx->committed = true;
     ctx->dt_valid = false;
     return Q2D_OK;
 }
 
+// Committed / pending state brought up to date before device work.
+int ready(q2d_ctx* ctx) {
+    if (!ctx->serving) return commit(ctx);
+    return apply_pending(ctx);
+}
+
 // ---- autotuner ------------------------------------------------------------------------------
 // Times every schedule (stage-kernel tile shape or warp-marching rows per item) for `steps`
-// explicit steps on the context's own workload and keeps the fastest. The state, the case
-// states and the time steps are saved before and restored after, so tuning has no effect on
-// the results.
+// explicit steps on the context's own workload and keeps the fastest. The state, the scalar
+// planes (time steps) and the case states are saved before and restored after each candidate,
+// so tuning leaves the results unchanged.
 struct Schedule { int kernel, tile, march_h; };
 
 int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
     static const Schedule cands[] = {{0, 0, 16}, {0, 1, 16}, {0, 2, 16}, {1, 0, 8}, {1, 0, 16}};
     const int ncand = (int)(sizeof(cands) / sizeof(cands[0]));
     const size_t nst = ctx->cases.size();
+    const long long ec = ctx->ac.cap;
     DevBuf<double> saveP, saveSC;
     DevBuf<CaseState> saveCS;
-    CK(saveP.alloc(ctx->pool4));
-    CK(saveSC.alloc(2 * ctx->pool4));
+    CK(saveP.alloc(ec));
+    CK(saveSC.alloc(2 * ec));
     CK(saveCS.alloc(nst));
     if (int e = ensure_dt(ctx)) return e;
-    CK(cudaMemcpyAsync(saveP.p, ctx->PA.p, sizeof(double) * ctx->pool4, cudaMemcpyDeviceToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(saveSC.p, ctx->SC.p, sizeof(double) * 2 * ctx->pool4, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(saveP.p, ctx->PA.p, sizeof(double) * ec, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(saveSC.p, ctx->SC.p, sizeof(double) * 2 * ec, cudaMemcpyDeviceToDevice, ctx->stream));
     CK(cudaMemcpyAsync(saveCS.p, ctx->cstate.p, sizeof(CaseState) * nst, cudaMemcpyDeviceToDevice, ctx->stream));
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
@@ -460,13 +680,13 @@ int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
     float best = 1e30f;
     int besti = 0;
     for (int k = 0; k < ncand; ++k) {
+        CK(cudaStreamSynchronize(ctx->stream));
         ctx->kernel = cands[k].kernel;
         ctx->tile = cands[k].tile;
         ctx->march_h = cands[k].march_h;
-        if (int e = build_items(ctx)) return e;
+        if (int e = rebuild_device_lists(ctx)) return e;
         int nk = 0;
-        for (int w = 0; w < 1 && nk >= 0; ++w)
-            if (int e = enqueue_step(ctx, ctx->stream, &nk)) return e;   // warm-up step
+        if (int e = enqueue_step(ctx, ctx->stream, &nk)) return e;   // warm-up step
         CK(cudaEventRecord(e0, ctx->stream));
         for (int sidx = 0; sidx < steps; ++sidx)
             if (int e = enqueue_step(ctx, ctx->stream, &nk)) return e;
@@ -476,22 +696,103 @@ int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
         float ms = 0.0f;
         CK(cudaEventElapsedTime(&ms, e0, e1));
         if (ms < best) { best = ms; besti = k; }
-        // restore before the next candidate
-        CK(cudaMemcpyAsync(ctx->PA.p, saveP.p, sizeof(double) * ctx->pool4, cudaMemcpyDeviceToDevice, ctx->stream));
-        CK(cudaMemcpyAsync(ctx->SC.p, saveSC.p, sizeof(double) * 2 * ctx->pool4, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->PA.p, saveP.p, sizeof(double) * ec, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->SC.p, saveSC.p, sizeof(double) * 2 * ec, cudaMemcpyDeviceToDevice, ctx->stream));
         CK(cudaMemcpyAsync(ctx->cstate.p, saveCS.p, sizeof(CaseState) * nst, cudaMemcpyDeviceToDevice, ctx->stream));
     }
+    CK(cudaStreamSynchronize(ctx->stream));
     ctx->kernel = cands[besti].kernel;
     ctx->tile = cands[besti].tile;
     ctx->march_h = cands[besti].march_h;
-    if (int e = build_items(ctx)) return e;
-    CK(cudaStreamSynchronize(ctx->stream));
+    if (int e = rebuild_device_lists(ctx)) return e;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     saveP.release(); saveSC.release(); saveCS.release();
     if (best_out) *best_out = besti;
     if (ms_out) *ms_out = best / (float)steps;
     return Q2D_OK;
+}
+
+int check_options(const q2d_options* opt) {
+    if (opt->n_rk < 1 || opt->n_rk > 3 || opt->limiter < 0 || opt->limiter > 6 || opt->riemann < 0 ||
+        opt->riemann > 2 || opt->source < 0 || opt->source > 2 || opt->precision < 0 ||
+        opt->precision > 1 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) || opt->res_diter < 1 ||
+        opt->sol_diter < 1 || !(opt->cfl > 0.0))
+        return Q2D_ERR_BADARG;
+    return Q2D_OK;
+}
+
+// Input checks of Read_BC (Lib_IO.f90) and of the boundary kinds on this path.
+int check_recs(q2d_ctx* ctx, const HCase& cs, const std::vector<q2d_bc_rec>& v) {
+    for (const q2d_bc_rec& r : v) {
+        if (r.b < 1 || r.b > (int)cs.blocks.size() || r.f < 1 || r.f > 4)
+            return fail(ctx, Q2D_ERR_BADARG, "set_bcs: block or face out of range");
+        const HBlock& B = ctx->blocks[cs.blocks[r.b - 1]];
+        if (r.i < 1 || r.i > B.ni || r.j < 1 || r.j > B.nj)
+            return fail(ctx, Q2D_ERR_BADARG, "set_bcs: cell out of range");
+        switch (r.type) {
+            case 400:
+                if ((r.f <= 2 && B.ni < 3) || (r.f >= 3 && B.nj < 3))
+                    return fail(ctx, Q2D_ERR_BADARG, "set_bcs: extrapolation needs 3 cells");
+                break;
+            case 0: case 300: case 401: case 405: case 406:
+                if (r.f <= 2 && B.ni < 2) return fail(ctx, Q2D_ERR_BADARG, "set_bcs: block too thin");
+                break;
+            case 101:
+                if (r.bs < 1 || r.bs > (int)cs.blocks.size() || r.fs < 1 || r.fs > 4)
+                    return fail(ctx, Q2D_ERR_BADARG, "set_bcs: bad connection donor");
+                break;
+            default:
+                return fail(ctx, Q2D_ERR_UNSUPPORTED, "set_bcs: BC type " + std::to_string(r.type) +
+                                                          " is not on the built path");
+        }
+    }
+    return Q2D_OK;
+}
+
+// Fortran P(1:4, -1:ni+2, -1:nj+2) (ghost frame of 2) -> 4 interior planes
+void fortran_to_planes(int ni, int nj, const double* P, std::vector<double>& planes) {
+    const long long n = (long long)ni * nj;
+    planes.assign(4 * n, 0.0);
+    for (int j = 0; j < nj; ++j)
+        for (int i = 0; i < ni; ++i) {
+            const double* src = &P[4 * ((size_t)(i + 2) + (size_t)(ni + 4) * (j + 2))];
+            for (int v = 0; v < 4; ++v) planes[v * n + (size_t)j * ni + i] = src[v];
+        }
+}
+
+q2d_ctx* new_ctx(const q2d_options* opt) {
+    q2d_ctx* ctx = new (std::nothrow) q2d_ctx();
+    if (!ctx) return nullptr;
+    ctx->opt = *opt;
+    ctx->gas.R = opt->gas_R;
+    ctx->gas.gamma = opt->gas_gamma;
+    ctx->gas.gm1 = opt->gas_gamma - 1.0;
+    ctx->gas.cp = opt->gas_gamma * opt->gas_R / (opt->gas_gamma - 1.0);
+    ctx->gas.cv = opt->gas_R / (opt->gas_gamma - 1.0);
+    ctx->gas.gfac = opt->gas_gamma / (opt->gas_gamma - 1.0);
+    ctx->gas.igm1 = 1.0 / (opt->gas_gamma - 1.0);
+    cudaGetDevice(&ctx->device);
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return nullptr;
+    }
+    const char* t = getenv("Q2D_TILE");
+    if (t) ctx->tile = std::max(0, std::min(kNumTiles - 1, atoi(t)));
+    const char* kk = getenv("Q2D_KERNEL");
+    if (kk) ctx->kernel = atoi(kk) == 0 ? 0 : 1;
+    const char* mh = getenv("Q2D_MARCH_H");
+    if (mh) ctx->march_h = std::max(1, std::min(4096, atoi(mh)));
+    return ctx;
+}
+
+void free_case_blocks(q2d_ctx* ctx, HCase& cs) {
+    for (int gb : cs.blocks) {
+        release_regions(ctx, ctx->blocks[gb]);
+        ctx->blocks[gb] = HBlock{};
+    }
+    cs = HCase{};
 }
 
 }  // namespace
@@ -523,41 +824,17 @@ void q2d_options_default(q2d_options* o) {
 int q2d_gpu_create(q2d_ctx** out, const q2d_options* opt) {
     if (!out || !opt) return Q2D_ERR_BADARG;
     *out = nullptr;
-    if (opt->n_rk < 1 || opt->n_rk > 3 || opt->limiter < 0 || opt->limiter > 6 || opt->riemann < 0 ||
-        opt->riemann > 2 || opt->source < 0 || opt->source > 2 || opt->precision < 0 ||
-        opt->precision > 1 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) || opt->res_diter < 1 ||
-        opt->sol_diter < 1 || !(opt->cfl > 0.0))
-        return Q2D_ERR_BADARG;
+    if (check_options(opt)) return Q2D_ERR_BADARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return Q2D_ERR_CUDA;
-    q2d_ctx* ctx = new (std::nothrow) q2d_ctx();
+    q2d_ctx* ctx = new_ctx(opt);
     if (!ctx) return Q2D_ERR_OOM;
-    ctx->opt = *opt;
-    ctx->gas.R = opt->gas_R;
-    ctx->gas.gamma = opt->gas_gamma;
-    ctx->gas.gm1 = opt->gas_gamma - 1.0;
-    ctx->gas.cp = opt->gas_gamma * opt->gas_R / (opt->gas_gamma - 1.0);
-    ctx->gas.cv = opt->gas_R / (opt->gas_gamma - 1.0);
-    ctx->gas.gfac = opt->gas_gamma / (opt->gas_gamma - 1.0);
-    ctx->gas.igm1 = 1.0 / (opt->gas_gamma - 1.0);
-    cudaGetDevice(&ctx->device);
-    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        delete ctx;
-        return Q2D_ERR_CUDA;
-    }
-    const char* t = getenv("Q2D_TILE");
-    if (t) ctx->tile = std::max(0, std::min(kNumTiles - 1, atoi(t)));
-    const char* kk = getenv("Q2D_KERNEL");
-    if (kk) ctx->kernel = atoi(kk) == 0 ? 0 : 1;
-    const char* mh = getenv("Q2D_MARCH_H");
-    if (mh) ctx->march_h = std::max(1, std::min(4096, atoi(mh)));
     *out = ctx;
     return Q2D_OK;
 }
 
 int q2d_gpu_add_case(q2d_ctx* ctx, int* case_id) {
-    if (!ctx || ctx->committed) return fail(ctx, Q2D_ERR_BADARG, "add_case after commit");
+    if (!ctx || ctx->committed || ctx->serving) return fail(ctx, Q2D_ERR_BADARG, "add_case after commit");
     ctx->cases.emplace_back();
     if (case_id) *case_id = (int)ctx->cases.size() - 1;
     return Q2D_OK;
@@ -565,8 +842,8 @@ int q2d_gpu_add_case(q2d_ctx* ctx, int* case_id) {
 
 int q2d_gpu_add_block(q2d_ctx* ctx, int case_id, int ni, int nj, const double* nodes_xy,
                       const double* cross_section, int* block_id) {
-    if (!ctx || ctx->committed || case_id < 0 || case_id >= (int)ctx->cases.size() || ni < 1 ||
-        nj < 1 || !nodes_xy)
+    if (!ctx || ctx->committed || ctx->serving || case_id < 0 || case_id >= (int)ctx->cases.size() ||
+        ni < 1 || nj < 1 || !nodes_xy)
         return fail(ctx, Q2D_ERR_BADARG, "add_block: bad argument");
     HBlock b;
     b.ni = ni; b.nj = nj; b.case_id = case_id;
@@ -581,56 +858,37 @@ int q2d_gpu_add_block(q2d_ctx* ctx, int case_id, int ni, int nj, const double* n
 }
 
 int q2d_gpu_set_bcs(q2d_ctx* ctx, int case_id, const q2d_bc_rec* recs, int n) {
-    if (!ctx || ctx->committed || case_id < 0 || case_id >= (int)ctx->cases.size() || n < 0 ||
-        (n && !recs))
+    if (!ctx || ctx->committed || ctx->serving || case_id < 0 || case_id >= (int)ctx->cases.size() ||
+        n < 0 || (n && !recs))
         return fail(ctx, Q2D_ERR_BADARG, "set_bcs: bad argument");
     HCase& cs = ctx->cases[case_id];
     std::vector<q2d_bc_rec> v(recs, recs + n);
-    for (const q2d_bc_rec& r : v) {
-        if (r.b < 1 || r.b > (int)cs.blocks.size() || r.f < 1 || r.f > 4)
-            return fail(ctx, Q2D_ERR_BADARG, "set_bcs: block or face out of range");
-        const HBlock& B = ctx->blocks[cs.blocks[r.b - 1]];
-        if (r.i < 1 || r.i > B.ni || r.j < 1 || r.j > B.nj)
-            return fail(ctx, Q2D_ERR_BADARG, "set_bcs: cell out of range");
-        switch (r.type) {
-            case 400:
-                if ((r.f <= 2 && B.ni < 3) || (r.f >= 3 && B.nj < 3))
-                    return fail(ctx, Q2D_ERR_BADARG, "set_bcs: extrapolation needs 3 cells");
-                break;
-            case 0: case 300: case 401: case 405: case 406:
-                if (r.f <= 2 && B.ni < 2) return fail(ctx, Q2D_ERR_BADARG, "set_bcs: block too thin");
-                break;
-            case 101:
-                if (r.bs < 1 || r.bs > (int)cs.blocks.size() || r.fs < 1 || r.fs > 4)
-                    return fail(ctx, Q2D_ERR_BADARG, "set_bcs: bad connection donor");
-                break;
-            default:
-                return fail(ctx, Q2D_ERR_UNSUPPORTED, "set_bcs: BC type " + std::to_string(r.type) +
-                                                          " is not on the built path");
-        }
-    }
+    if (int e = check_recs(ctx, cs, v)) return e;
     std::stable_sort(v.begin(), v.end(), rec_less);
     cs.bc = std::move(v);
     return Q2D_OK;
 }
 
 int q2d_gpu_upload_prim(q2d_ctx* ctx, int block_id, const double* P) {
-    if (!ctx || block_id < 0 || block_id >= (int)ctx->blocks.size() || !P)
+    if (!ctx || block_id < 0 || block_id >= (int)ctx->blocks.size() || !P || ctx->blocks[block_id].case_id < 0)
         return fail(ctx, Q2D_ERR_BADARG, "upload_prim: bad argument");
     HBlock& b = ctx->blocks[block_id];
-    const long long n = (long long)b.ni * b.nj;
-    std::vector<double> planes(4 * n);
-    for (int j = 0; j < b.nj; ++j)
-        for (int i = 0; i < b.ni; ++i) {
-            const double* src = &P[4 * ((size_t)(i + 2) + (size_t)(b.ni + 4) * (j + 2))];
-            for (int v = 0; v < 4; ++v) planes[v * n + (size_t)j * b.ni + i] = src[v];
+    std::vector<double> planes;
+    fortran_to_planes(b.ni, b.nj, P, planes);
+    if (!ctx->cases[b.case_id].resident) {
+        if (ctx->cases[b.case_id].prepared) {
+            for (int v = 0; v < 4; ++v)
+                std::memcpy(&b.staged.pa[v * b.d.pc], &planes[v * (size_t)b.ni * b.nj],
+                            sizeof(double) * b.ni * b.nj);
+        } else {
+            b.prim = std::move(planes);
         }
-    if (!ctx->committed) {
-        b.prim = std::move(planes);
         return Q2D_OK;
     }
+    const long long n = (long long)b.ni * b.nj;
     std::vector<double> staged(4 * (size_t)b.d.pc, 0.0);
     for (int v = 0; v < 4; ++v) std::memcpy(&staged[v * b.d.pc], &planes[v * n], sizeof(double) * n);
+    CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaMemcpy(ctx->PA.p + b.d.oc, staged.data(), sizeof(double) * staged.size(), cudaMemcpyHostToDevice));
     ctx->dt_valid = false;
     return Q2D_OK;
@@ -639,38 +897,37 @@ int q2d_gpu_upload_prim(q2d_ctx* ctx, int block_id, const double* P) {
 int q2d_gpu_download_prim(q2d_ctx* ctx, int block_id, double* P) {
     if (!ctx || block_id < 0 || block_id >= (int)ctx->blocks.size() || !P)
         return fail(ctx, Q2D_ERR_BADARG, "download_prim: bad argument");
-    int e = commit(ctx);
-    if (e) return e;
+    if (int e = ready(ctx)) return e;
     HBlock& b = ctx->blocks[block_id];
+    if (!b.alive || b.case_id < 0 || !ctx->cases[b.case_id].resident)
+        return fail(ctx, Q2D_ERR_BADARG, "download_prim: block not resident");
     std::vector<double> staged(4 * (size_t)b.d.pc);
     CK(cudaMemcpyAsync(staged.data(), ctx->PA.p + b.d.oc, sizeof(double) * staged.size(),
                        cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    const double* planes = staged.data();
     const long long pcs = b.d.pc;
     for (int j = 0; j < b.nj; ++j)
         for (int i = 0; i < b.ni; ++i) {
             double* dst = &P[4 * ((size_t)(i + 2) + (size_t)(b.ni + 4) * (j + 2))];
-            for (int v = 0; v < 4; ++v) dst[v] = planes[v * pcs + (size_t)j * b.ni + i];
+            for (int v = 0; v < 4; ++v) dst[v] = staged[v * pcs + (size_t)j * b.ni + i];
         }
     return Q2D_OK;
 }
 
 int q2d_gpu_commit(q2d_ctx* ctx) {
     if (!ctx) return Q2D_ERR_BADARG;
-    return commit(ctx);
+    return ready(ctx);
 }
 
 int q2d_gpu_step_async(q2d_ctx* ctx, int nsteps) {
     if (!ctx || nsteps < 0) return fail(ctx, Q2D_ERR_BADARG, "step: bad argument");
-    int e = commit(ctx);
-    if (e) return e;
+    if (int e = ready(ctx)) return e;
     CK(launch_resume(ctx->cstate.p, (int)ctx->cases.size(), ctx->flag.p, ctx->stream));
     ctx->launches += 1;
-    if ((e = ensure_dt(ctx))) return e;
-    if (nsteps > 0) {
+    if (int e = ensure_dt(ctx)) return e;
+    if (nsteps > 0 && ctx->n_items > 0) {
         cudaGraphExec_t ge;
-        if ((e = get_graph(ctx, nsteps, &ge))) return e;
+        if (int e = get_graph(ctx, nsteps, &ge)) return e;
         CK(cudaGraphLaunch(ge, ctx->stream));
         ctx->launches += ctx->graph_kernels[nsteps];
     } else {
@@ -688,7 +945,7 @@ int q2d_gpu_wait(q2d_ctx* ctx, q2d_step_info* out) {
         q2d_step_info info;
         fill_info(ctx->h_state[c], &info);
         if (out) out[c] = info;
-        if (!first && info.err) first = info.err;
+        if (!first && info.err && ctx->cases[c].used) first = info.err;
     }
     return first;
 }
@@ -703,15 +960,14 @@ void* q2d_gpu_stream(const q2d_ctx* ctx) { return ctx ? (void*)ctx->stream : nul
 
 int q2d_gpu_autotune(q2d_ctx* ctx, int steps, int* schedule, float* ms_per_step) {
     if (!ctx || steps < 1) return fail(ctx, Q2D_ERR_BADARG, "autotune: bad argument");
-    int e = commit(ctx);
-    if (e) return e;
+    if (int e = ready(ctx)) return e;
     return autotune(ctx, steps, schedule, ms_per_step);
 }
 
 int q2d_gpu_prepare(q2d_ctx* ctx, int nsteps) {
     if (!ctx || nsteps < 1) return fail(ctx, Q2D_ERR_BADARG, "prepare: bad argument");
-    int e = commit(ctx);
-    if (e) return e;
+    if (int e = ready(ctx)) return e;
+    if (ctx->n_items == 0) return Q2D_OK;
     cudaGraphExec_t ge;
     return get_graph(ctx, nsteps, &ge);
 }
@@ -719,8 +975,7 @@ int q2d_gpu_prepare(q2d_ctx* ctx, int nsteps) {
 int q2d_gpu_case_info(q2d_ctx* ctx, int case_id, q2d_step_info* out) {
     if (!ctx || !out || case_id < 0 || case_id >= (int)ctx->cases.size())
         return fail(ctx, Q2D_ERR_BADARG, "case_info: bad argument");
-    int e = commit(ctx);
-    if (e) return e;
+    if (int e = ready(ctx)) return e;
     CK(cudaMemcpyAsync(ctx->h_state, ctx->cstate.p, sizeof(CaseState) * ctx->cases.size(),
                        cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -729,13 +984,115 @@ int q2d_gpu_case_info(q2d_ctx* ctx, int case_id, q2d_step_info* out) {
 }
 
 int q2d_gpu_num_cases(const q2d_ctx* ctx) { return ctx ? (int)ctx->cases.size() : 0; }
+
 long long q2d_gpu_num_cells(const q2d_ctx* ctx) {
     if (!ctx) return 0;
     long long n = 0;
-    for (const HBlock& b : ctx->blocks) n += (long long)b.ni * b.nj;
+    for (const HCase& cs : ctx->cases)
+        if (!ctx->serving || cs.used)
+            for (int gb : cs.blocks) n += (long long)ctx->blocks[gb].ni * ctx->blocks[gb].nj;
     return n;
 }
+
 long long q2d_gpu_launch_count(const q2d_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+// ---- serving ---------------------------------------------------------------------------------
+int q2d_serve_create(q2d_ctx** out, const q2d_options* opt, unsigned long long device_bytes, int max_cases) {
+    if (!out || !opt || max_cases < 1 || device_bytes < (1ull << 20)) return Q2D_ERR_BADARG;
+    *out = nullptr;
+    if (check_options(opt)) return Q2D_ERR_BADARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return Q2D_ERR_CUDA;
+    q2d_ctx* ctx = new_ctx(opt);
+    if (!ctx) return Q2D_ERR_OOM;
+    ctx->serving = true;
+    ctx->cases.resize(max_cases);
+    // Bytes per interior cell: states 3 x 4 planes + scalars 8 planes (160 B), ghost frame
+    // 2 planes with up to 50 % halo (24 B), i- and j-faces 3 planes each with up to 15 %
+    // extra faces (55 B).
+    const long long cells = (long long)((double)device_bytes / 239.2);
+    const long long ec = 4 * cells, eg = 3 * cells + 4096, efi = (long long)(3.45 * (double)cells) + 4096,
+                    efj = efi;
+    int e = allocate_pools(ctx, ec, eg, efi, efj, max_cases);
+    if (!e) e = rebuild_device_lists(ctx);
+    if (e) {
+        q2d_gpu_destroy(ctx);
+        return e;
+    }
+    ctx->committed = true;
+    ctx->dt_valid = true;
+    *out = ctx;
+    return Q2D_OK;
+}
+
+int q2d_serve_admit(q2d_ctx* ctx, int nblocks, const int* ni, const int* nj, const double* const* nodes_xy,
+                    const double* const* cross_sections, const double* const* P, const q2d_bc_rec* recs,
+                    int nrecs, int* case_id) {
+    if (!ctx || !ctx->serving || nblocks < 1 || !ni || !nj || !nodes_xy || !P || nrecs < 0 || (nrecs && !recs))
+        return fail(ctx, Q2D_ERR_BADARG, "serve_admit: bad argument");
+    for (int b = 0; b < nblocks; ++b)
+        if (ni[b] < 1 || nj[b] < 1 || !nodes_xy[b] || !P[b])
+            return fail(ctx, Q2D_ERR_BADARG, "serve_admit: bad block");
+    int slot = -1;
+    for (size_t c = 0; c < ctx->cases.size(); ++c)
+        if (!ctx->cases[c].used) { slot = (int)c; break; }
+    if (slot < 0) return fail(ctx, Q2D_ERR_CAPACITY, "serve_admit: no free case slot");
+    HCase& cs = ctx->cases[slot];
+    cs = HCase{};
+    cs.used = true;
+    for (int b = 0; b < nblocks; ++b) {
+        int gid = -1;
+        for (size_t k = 0; k < ctx->blocks.size(); ++k)
+            if (ctx->blocks[k].case_id < 0 && !ctx->blocks[k].alive) { gid = (int)k; break; }
+        if (gid < 0) { ctx->blocks.emplace_back(); gid = (int)ctx->blocks.size() - 1; }
+        HBlock& hb = ctx->blocks[gid];
+        hb = HBlock{};
+        hb.ni = ni[b]; hb.nj = nj[b]; hb.case_id = slot; hb.local_b = b + 1;
+        hb.nodes.assign(nodes_xy[b], nodes_xy[b] + 2 * (size_t)(ni[b] + 1) * (nj[b] + 1));
+        if (cross_sections && cross_sections[b])
+            hb.area.assign(cross_sections[b], cross_sections[b] + (size_t)(ni[b] + 1) * (nj[b] + 1));
+        fortran_to_planes(ni[b], nj[b], P[b], hb.prim);
+        cs.blocks.push_back(gid);
+    }
+    std::vector<q2d_bc_rec> v(recs, recs + nrecs);
+    int e = check_recs(ctx, cs, v);
+    if (!e) {
+        std::stable_sort(v.begin(), v.end(), rec_less);
+        cs.bc = std::move(v);
+        e = prepare_case(ctx, slot);
+    }
+    if (e) {
+        free_case_blocks(ctx, cs);
+        return e;
+    }
+    ctx->dirty = true;
+    if (case_id) *case_id = slot;
+    return Q2D_OK;
+}
+
+int q2d_serve_retire(q2d_ctx* ctx, int case_id) {
+    if (!ctx || !ctx->serving || case_id < 0 || case_id >= (int)ctx->cases.size() || !ctx->cases[case_id].used)
+        return fail(ctx, Q2D_ERR_BADARG, "serve_retire: bad argument");
+    free_case_blocks(ctx, ctx->cases[case_id]);
+    ctx->reset_slots.push_back(case_id);
+    ctx->dirty = true;
+    return Q2D_OK;
+}
+
+int q2d_serve_block_id(const q2d_ctx* ctx, int case_id, int b, int* block_id) {
+    if (!ctx || case_id < 0 || case_id >= (int)ctx->cases.size() || !ctx->cases[case_id].used || b < 1 ||
+        b > (int)ctx->cases[case_id].blocks.size() || !block_id)
+        return Q2D_ERR_BADARG;
+    *block_id = ctx->cases[case_id].blocks[b - 1];
+    return Q2D_OK;
+}
+
+long long q2d_serve_free_cells(const q2d_ctx* ctx) {
+    if (!ctx) return 0;
+    const long long c = ctx->ac.free_total() / 4, g = ctx->ag.free_total() / 3,
+                    f = std::min(ctx->afi.free_total(), ctx->afj.free_total()) * 100 / 345;
+    return std::min(c, std::min(g, f));
+}
 
 const char* q2d_gpu_errstr(int status) {
     switch (status) {
@@ -757,7 +1114,7 @@ const char* q2d_gpu_last_error(const q2d_ctx* ctx) { return ctx ? ctx->last_erro
 void q2d_gpu_destroy(q2d_ctx* ctx) {
     if (!ctx) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+    drop_graphs(ctx);
     ctx->PA.release(); ctx->PB.release(); ctx->PC.release(); ctx->SC.release(); ctx->DL.release();
     ctx->FI.release(); ctx->FJ.release(); ctx->PART.release(); ctx->dblocks.release();
     ctx->dcases.release(); ctx->cstate.release(); ctx->items.release(); ctx->edges.release();

@@ -69,7 +69,7 @@ struct CaseState {
     int status;
     int err, err_b, err_i, err_j, err_stage;
     unsigned int counter;  // items of the current stage finished (reset by the last CTA)
-    int pad;
+    int dt_pending;        // the case has no time step yet (admitted after the last dt pass)
 };
 
 struct WorkItem {

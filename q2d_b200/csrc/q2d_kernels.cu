@@ -474,7 +474,8 @@ __global__ void __launch_bounds__(NT) dt_kernel(const StageArgs a) {
         const WorkItem w = a.items[it];
         const DBlock B = a.blocks[w.block];
         CaseState* cs = &a.cstate[w.case_id];
-        if (__ldcg(&cs->status) != kStatus_Running) continue;
+        // a.first != 0: only cases admitted since the last pass (others keep their time step)
+        if (__ldcg(&cs->status) != kStatus_Running || (a.first && !__ldcg(&cs->dt_pending))) continue;
         const long long iter_next = __ldcg(&cs->iter) + 1;
         const int ndir = a.cases[w.case_id].ndir;
         double acc[5] = {0.0, 0.0, 0.0, 0.0, 1e300};
@@ -507,7 +508,8 @@ __global__ void __launch_bounds__(128) dt_march_kernel(const StageArgs a) {
         const WorkItem w = a.items[it];
         const DBlock B = a.blocks[w.block];
         CaseState* cs = &a.cstate[w.case_id];
-        if (__ldcg(&cs->status) != kStatus_Running) continue;
+        // a.first != 0: only cases admitted since the last pass (others keep their time step)
+        if (__ldcg(&cs->status) != kStatus_Running || (a.first && !__ldcg(&cs->dt_pending))) continue;
         const long long iter_next = __ldcg(&cs->iter) + 1;
         const int ndir = a.cases[w.case_id].ndir;
         double acc[5] = {0.0, 0.0, 0.0, 0.0, 1e300};

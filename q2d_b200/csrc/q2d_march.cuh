@@ -71,7 +71,10 @@ __device__ __forceinline__ void warp_item_done(const StageArgs& a, int case_id, 
             cs->iter_from_call += 1;
             if (a.time_accurate) cs->time = cs->time + cs->dt_step;
         }
-        if (with_dt) cs->dt_step = fmin(acc[4], 1e5);
+        if (with_dt) {
+            cs->dt_step = fmin(acc[4], 1e5);
+            cs->dt_pending = 0;
+        }
         if (with_res) {   // Mod_Explicit.f90:120-170
             if (cs->iter_from_call == 1 || (cs->iter % a.res_diter) == 0) {
                 for (int k = 0; k < 4; ++k) cs->res[k] = sqrt(acc[k]);

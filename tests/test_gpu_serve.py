@@ -1,0 +1,138 @@
+"""Serving context (q2d_serve_*): continuous batching on the GPU.
+
+* Each result is the same alone and in the mix: cases admitted at different times into a
+  running context, next to other cases, end bit-for-bit where they end when served alone
+  (tolerance 0: every cell update, time step and residual of a case reads only that case's
+  data, and admissions compute time steps only for the new cases).
+* Served results equal the batch path's (q2d_gpu_* context with the same options and steps).
+* Memory-budget admission: a full context refuses with Q2D_ERR_CAPACITY and keeps running;
+  retirement frees the slot and the memory for the next request.
+* The request loop serves a small stream to completion and retires every case on its residual
+  drop or its iteration cap.
+"""
+import numpy as np
+import pytest
+
+from q2d_b200 import _abi, cases
+from q2d_b200.serve import Request, ServeContext, serve, serve_options
+from q2d_b200.solver import Q2DSolver
+
+pytestmark = pytest.mark.gpu
+
+BUDGET = 256 << 20
+
+
+def small_requests():
+    rng = np.random.default_rng(123)
+    return [cases.request_case("ramp", 800, rng), cases.request_case("nozzle", 640, rng),
+            cases.request_case("ramp", 1500, rng), cases.request_case("nozzle", 2000, rng)]
+
+
+def run_alone(case, opts, steps):
+    with ServeContext(opts, BUDGET, 4) as sc:
+        cid = sc.admit(case)
+        assert cid is not None
+        sc.step_async(steps)
+        infos = sc.wait()
+        return [sc.prim(cid, b) for b in range(len(case.blocks))], infos[cid]
+
+
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64, _abi.PREC_FP32_FLUX])
+def test_alone_equals_in_mix(precision):
+    reqs = small_requests()
+    steps = 24
+    opts = serve_options(precision=precision, itermax=steps, drop=1e-30)
+    alone = [run_alone(c, opts, steps + 10) for c in reqs]
+    # mix: admissions staggered over the run; every case stops at its own itermax
+    with ServeContext(opts, BUDGET, 8) as sc:
+        ids = [sc.admit(reqs[0])]
+        sc.step_async(5); sc.wait()
+        ids.append(sc.admit(reqs[1]))
+        ids.append(sc.admit(reqs[2]))
+        sc.step_async(7); sc.wait()
+        ids.append(sc.admit(reqs[3]))
+        for _ in range(6):
+            sc.step_async(6)
+            infos = sc.wait()
+        for k, (cid, c) in enumerate(zip(ids, reqs)):
+            inf = infos[cid]
+            assert inf.iter == steps and inf.todo == _abi.TODO_END and inf.err == 0
+            a_state, a_inf = alone[k]
+            for b in range(len(c.blocks)):
+                m = sc.prim(cid, b)
+                assert np.array_equal(m, a_state[b]), f"case {k} block {b}: in-mix result differs from alone"
+            assert inf.residual[0] == a_inf.residual[0] and inf.dtglobal == a_inf.dtglobal
+
+
+def test_multiblock_axisymmetric_alone_equals_in_mix():
+    a = cases.nozzle_axi(ni=40, nj=12, nblocks=2, seed=21)
+    b = cases.nozzle_axi(ni=32, nj=10, nblocks=3, seed=22)
+    opts = _abi.default_options(**dict(a.options, itermax=15, res_threshold=0.0, sol_diter=10 ** 9))
+    alone_b = run_alone(b, opts, 20)
+    with ServeContext(opts, BUDGET, 4) as sc:
+        ia = sc.admit(a)
+        sc.step_async(4); sc.wait()
+        ib = sc.admit(b)
+        for _ in range(4):
+            sc.step_async(5)
+            infos = sc.wait()
+        assert infos[ia].iter == 15 and infos[ib].iter == 15
+        for k in range(3):
+            assert np.array_equal(sc.prim(ib, k), alone_b[0][k])
+
+
+def test_served_equals_batch_path():
+    reqs = small_requests()[:2]
+    opts = serve_options(precision=_abi.PREC_FP32_FLUX, itermax=12, drop=1e-30)
+    g = Q2DSolver(opts, reqs)
+    try:
+        g.step(12)
+        batch = [g.prim(c, 0) for c in range(len(reqs))]
+    finally:
+        g.close()
+    with ServeContext(opts, BUDGET, 4) as sc:
+        ids = [sc.admit(c) for c in reqs]
+        sc.step_async(12)
+        sc.wait()
+        for k, cid in enumerate(ids):
+            assert np.array_equal(sc.prim(cid, 0), batch[k])
+
+
+def test_capacity_admission_and_retire():
+    rng = np.random.default_rng(5)
+    big = cases.request_case("nozzle", 60000, rng)
+    opts = serve_options(itermax=5)
+    # a budget for about 1.5 of these cases
+    budget = int(1.5 * big.cells * 240)
+    with ServeContext(opts, budget, 4) as sc:
+        c0 = sc.admit(big)
+        assert c0 is not None
+        assert sc.admit(big) is None            # memory exhausted: refused, nothing kept
+        sc.step_async(5)
+        infos = sc.wait()
+        assert infos[c0].iter == 5 and infos[c0].todo == _abi.TODO_END
+        sc.retire(c0)
+        c1 = sc.admit(big)
+        assert c1 is not None
+        sc.step_async(5)
+        infos = sc.wait()
+        assert infos[c1].iter == 5 and infos[c1].err == 0
+    # slots exhausted
+    small = cases.request_case("ramp", 500, rng)
+    with ServeContext(opts, BUDGET, 2) as sc:
+        assert sc.admit(small) is not None and sc.admit(small) is not None
+        assert sc.admit(small) is None
+
+
+def test_request_loop_small_stream():
+    rng = np.random.default_rng(9)
+    reqs = [Request(k, 0.002 * k, kind, cells, int(rng.integers(1 << 31)))
+            for k, (kind, cells) in enumerate([("ramp", 900), ("nozzle", 1200), ("ramp", 3000),
+                                               ("nozzle", 700), ("ramp", 2000), ("nozzle", 5000)])]
+    opts = serve_options(itermax=300, drop=1e-3)
+    st = serve(reqs, opts, device_bytes=int(2 * 5000 * 240 + (1 << 20)), max_cases=3, steps_per_call=10,
+               realtime=False)
+    assert st["served"] == len(reqs) and st["errors"] == 0 and st["rejected"] == 0
+    for r in reqs:
+        assert r.iters <= 300 and (r.iters == 300 or r.residual_drop <= 1e-3)
+    assert st["cell_updates"] > 0 and st["p99_latency_s"] >= st["p50_latency_s"] > 0
