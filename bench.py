@@ -51,6 +51,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrivals per second")
+    ap.add_argument("--serve-seconds", type=float, default=1.0, help="length of the arrival window")
+    ap.add_argument("--serve-iters", type=int, default=200, help="iteration cap (fixed end) per request")
+    ap.add_argument("--serve-gb", type=float, default=6.0, help="device-memory budget of the pools")
     return ap.parse_args()
 
 
@@ -104,6 +109,24 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def read_traffic(schedule):
+    """DRAM bytes (read + write) per stage launch of the full batch, from the ncu summary of
+    the stage kernel under profiles/ (a smaller batch captured and scaled by cells), when that
+    summary was taken with the same schedule; otherwise None."""
+    f = REPO / "profiles" / "stage_kernel_batched_nozzles.md"
+    try:
+        kv = {}
+        for line in f.read_text().splitlines():
+            if line.startswith("- ") and ":" in line:
+                k, v = line[2:].split(":", 1)
+                kv[k.strip()] = v.strip()
+        if kv.get("schedule") != schedule:
+            return None
+        return float(kv["dram_bytes_per_launch_full_batch"])
+    except Exception:
+        return None
+
+
 def batch_cases(n, rank):
     from q2d_b200 import cases
     return cases.area_nozzle_batch(n=n, seed=cases.BASE_SEED + 3 + 7919 * rank)
@@ -148,6 +171,71 @@ def cpu_baseline(batch, budget_s=12.0):
     return {"value": cells * n / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{len(sample)} of the batch's cases ({cells} cells) x {n} steps, "
                       f"{dt:.1f} s, C++ oracle -O3 OpenMP"}
+
+
+def serving_leg(args, lib):
+    """The served request stream: Poisson arrivals of planar ramps and quasi-2D nozzles with
+    log-normal sizes in [4e3, 2e6] cells, admitted by memory budget into one serving context
+    (FP32-flux / FP64-state), retired on a 1e-8 relative residual drop or at the iteration cap.
+    Beside it, a sample of the same requests solved one after another through the plain FP64
+    path (one context per request, wall clock including setup and read-back, as for serving)."""
+    from q2d_b200 import _abi, make_options
+    from q2d_b200.serve import request_stream, serve, serve_options
+    from q2d_b200.solver import Q2DSolver
+    reqs = request_stream(args.serve_rate, args.serve_seconds)
+    opts = serve_options(itermax=args.serve_iters, drop=1e-8)
+    st = serve(reqs, opts, device_bytes=int(args.serve_gb * (1 << 30)), max_cases=4096, steps_per_call=10)
+    # sequential plain FP64 on the first requests of the same stream
+    seq = request_stream(args.serve_rate, args.serve_seconds)[:8]
+    opts64 = serve_options(precision=_abi.PREC_FP64, itermax=args.serve_iters, drop=1e-8)
+    t0 = time.perf_counter()
+    cu = 0
+    for r in seq:
+        case = r.build()
+        s = Q2DSolver(opts64, [case])
+        try:
+            info = s.solve(steps_per_call=args.serve_iters)
+            _ = [s.prim(0, b) for b in range(len(case.blocks))]
+            cu += case.cells * info["iter"]
+        finally:
+            s.close()
+    tseq = time.perf_counter() - t0
+    seq_v = cu / tseq
+    st.update({"arrival_rate_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,
+               "iteration_cap": args.serve_iters, "residual_drop": 1e-8, "budget_gb": args.serve_gb,
+               "dtype": "fp32-flux/fp64-state",
+               "sequential_plain_fp64": {"value": seq_v, "unit": UNIT, "requests": len(seq),
+                                         "cell_updates": cu, "seconds": tseq},
+               "ratio_served_over_sequential_fp64": st["cell_updates_per_s"] / seq_v})
+    return st
+
+
+def accuracy_leg(batch):
+    """FP32-flux vs plain FP64 on the same cases after the same steps: relative L1 and L-inf
+    of the primitive variables (each variable over its own scale), worst case of the sample."""
+    from q2d_b200 import make_options
+    from q2d_b200.solver import Q2DSolver
+    sample = batch[:64]
+    steps = 200
+    out = []
+    for prec in (1, 0):
+        s = Q2DSolver(make_options(sample[0], precision=prec), sample)
+        try:
+            s.step(steps)
+            out.append([s.prim(c, 0) for c in range(len(sample))])
+        finally:
+            s.close()
+    l1 = linf = 0.0
+    for a, b in zip(out[0], out[1]):
+        bb = b.reshape(-1, 4)
+        snd = np.sqrt(1.4 * np.abs(bb[:, 3]) / np.abs(bb[:, 0]))
+        vs = max(np.abs(bb[:, 1]).max(), np.abs(bb[:, 2]).max(), snd.max())
+        sc = np.array([np.abs(bb[:, 0]).max(), vs, vs, np.abs(bb[:, 3]).max()])
+        d = np.abs(a.reshape(-1, 4) - bb) / sc
+        l1 = max(l1, float(d.mean(axis=0).max()))
+        linf = max(linf, float(d.max()))
+    return {"vs": "plain FP64 GPU path", "cases": len(sample), "steps": steps,
+            "rel_l1_max": l1, "rel_linf_max": linf}
 
 
 def reference_arm(args):
@@ -213,12 +301,7 @@ def main():
     except Exception:
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
-    traffic = None
-    try:
-        prof = json.loads((REPO / "profiles" / "traffic.json").read_text())
-        traffic = prof.get("dram_bytes_per_launch_full")
-    except Exception:
-        pass
+    traffic = read_traffic(tuned["schedule"])
     # ---- e2e through the C ABI with host buffers ----------------------------------------
     e2e = None
     if not args.no_e2e:
@@ -264,6 +347,10 @@ def main():
                 "schedule": tuned64["schedule"] + " (autotuned)",
                 "ratio_fp32flux_over_fp64": value / v64}
         s64.close()
+    served = None
+    if not args.no_serve:
+        served = serving_leg(args, lib)
+    accuracy = accuracy_leg(batch) if not args.no_fp64 else None
     cpu = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline(batch)
@@ -287,7 +374,8 @@ def main():
                      "bytes_per_cell_update": B_ALG, "launch_ms": t_launch * 1e3},
         "gpu_launches": launches, "errors": errs,
         "clocks": clk.summary(),
-        "e2e": e2e, "plain_fp64": fp64, "cpu_baseline": cpu,
+        "e2e": e2e, "plain_fp64": fp64, "served": served, "accuracy_fp32flux": accuracy,
+        "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
 
