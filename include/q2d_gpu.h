@@ -185,6 +185,13 @@ int  q2d_gpu_prepare(q2d_ctx* ctx, int nsteps);
  * the chosen candidate index, *ms_per_step its time (either may be NULL). */
 int  q2d_gpu_autotune(q2d_ctx* ctx, int steps, int* schedule, float* ms_per_step);
 
+/* Pins the schedule of the stage kernels (the index the autotuner reports) without tuning:
+ * 0-2 CTA-tile kernel on 32x10, 32x8, 64x4 tiles; 3-4 warp-marching kernel with 8 / 16 rows
+ * per item; 5-7 FP32-flux tile kernel on 32x10, 32x8, 64x4 tiles (FP32-flux form only, and its
+ * default). q2d_gpu_get_schedule returns the current one. */
+int  q2d_gpu_set_schedule(q2d_ctx* ctx, int schedule);
+int  q2d_gpu_get_schedule(const q2d_ctx* ctx);
+
 /* Allocation-free residual norm. No counterpart in the reference: it serves callers that
  * cannot call cudaMalloc when they need the residual — a host whose device memory is owned
  * by its own pool allocator (for instance a Fortran driver that pre-allocates every array),

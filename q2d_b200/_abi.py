@@ -184,6 +184,10 @@ def load_library() -> C.CDLL:
     lib.q2d_gpu_prepare.argtypes = [C.c_void_p, C.c_int]
     lib.q2d_gpu_stream.restype = C.c_void_p
     lib.q2d_gpu_stream.argtypes = [C.c_void_p]
+    lib.q2d_gpu_set_schedule.restype = C.c_int
+    lib.q2d_gpu_set_schedule.argtypes = [C.c_void_p, C.c_int]
+    lib.q2d_gpu_get_schedule.restype = C.c_int
+    lib.q2d_gpu_get_schedule.argtypes = [C.c_void_p]
     lib.q2d_options_default.restype = None
     lib.q2d_options_default.argtypes = [C.POINTER(Options)]
     PD = C.POINTER(C.POINTER(C.c_double))

@@ -295,6 +295,34 @@ def area_nozzle_batch(n: int = 4096, seed: int = BASE_SEED + 3, nx_range=(64, 10
                         float(T0[c])) for c in range(n)]
 
 
+def closed_box(ni: int = 24, nj: int = 24, seed: int = 3, **options) -> CaseSpec:
+    """A closed curvilinear box (slip walls, BC 300, on all four faces) holding a random state:
+    mass and energy can only change by round-off. Options default to van Leer, RK3,
+    CFL 0.4, time-accurate."""
+    rng = np.random.default_rng(seed)
+    x, y = np.meshgrid(np.linspace(0, 1, ni + 1), np.linspace(0, 1, nj + 1))
+    x = x + 0.02 * np.sin(2 * np.pi * y)
+    nodes = np.stack([x, y], axis=-1)
+    prim = np.zeros((nj, ni, 4))
+    prim[..., 0] = 1 + 0.1 * rng.random((nj, ni))
+    prim[..., 1] = 0.1 * rng.standard_normal((nj, ni))
+    prim[..., 2] = 0.1 * rng.standard_normal((nj, ni))
+    prim[..., 3] = 1 + 0.1 * rng.random((nj, ni))
+    blk = BlockSpec(ni, nj, nodes, prim)
+    bcs = edge_records(1, ni, nj, {f: (300, {}) for f in (1, 2, 3, 4)})
+    opts = dict(limiter="vanleer", n_rk=3, cfl=0.4, time_accurate=1)
+    opts.update(options)
+    return CaseSpec("box", [blk], bcs, opts)
+
+
+def cell_areas(block: BlockSpec) -> np.ndarray:
+    """Quadrilateral cell areas from the nodes (half the cross product of the diagonals)."""
+    X, Y = block.nodes[..., 0], block.nodes[..., 1]
+    d1x, d1y = X[1:, 1:] - X[:-1, :-1], Y[1:, 1:] - Y[:-1, :-1]
+    d2x, d2y = X[:-1, 1:] - X[1:, :-1], Y[:-1, 1:] - Y[1:, :-1]
+    return 0.5 * np.abs(d1x * d2y - d1y * d2x)
+
+
 def request_case(kind: str, cells: int, rng: np.random.Generator) -> CaseSpec:
     """One served request: a planar ramp or a quasi-2D nozzle with about `cells` cells."""
     if kind == "ramp":

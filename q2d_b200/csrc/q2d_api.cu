@@ -143,7 +143,7 @@ struct q2d_ctx {
     bool dirty = false;           // uploads, slot resets or list rebuild pending
     std::vector<int> reset_slots; // retired slots whose device run state still has to be reset
     int tile = 0;
-    int kernel = 0;       // 0: CTA-tile stage kernel, 1: warp-marching stage kernel
+    int kernel = 0;       // 0: CTA-tile stage kernel, 1: warp-marching, 2: FP32-flux tile kernel
     int march_h = 16;     // rows per warp-marching item
     int grid = 0;
     // device pools and their allocators
@@ -245,6 +245,8 @@ int enqueue_step(q2d_ctx* ctx, cudaStream_t s, int* nk) {
         }
         if (ctx->kernel == 1)
             CK(launch_march(a, ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter, ctx->grid, s));
+        else if (ctx->kernel == 2)
+            CK(launch_stage32(a, ctx->opt.riemann, ctx->tile, ctx->grid, s));
         else
             CK(launch_stage(a, ctx->opt.precision, ctx->opt.riemann, ctx->tile, ctx->grid, s));
         ++*nk;
@@ -581,7 +583,8 @@ int rebuild_device_lists(q2d_ctx* ctx) {
         const int occ = std::max(1, march_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter));
         ctx->grid = (int)std::min<long long>(((long long)items.size() + 3) / 4, (long long)occ * ctx->num_sms);
     } else {
-        const int occ = std::max(1, stage_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->tile));
+        const int occ = std::max(1, ctx->kernel == 2 ? stage32_occupancy(ctx->opt.riemann, ctx->tile)
+                                                     : stage_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->tile));
         ctx->grid = (int)std::min<long long>((long long)items.size(), (long long)occ * ctx->num_sms);
     }
     if (ctx->grid < 1) ctx->grid = 1;
@@ -659,10 +662,20 @@ int ready(q2d_ctx* ctx) {
 // planes (time steps) and the case states are saved before and restored after each candidate,
 // so tuning leaves the results unchanged.
 struct Schedule { int kernel, tile, march_h; };
+// Candidate schedules, indexed like the autotuner's result: CTA-tile stage kernel on tiles
+// 32x10, 32x8, 64x4; warp-marching kernel with 8 or 16 rows per item; FP32-flux tile kernel
+// on tiles 32x10, 32x8, 64x4 (FP32-flux form only).
+const Schedule kSchedules[] = {{0, 0, 16}, {0, 1, 16}, {0, 2, 16}, {1, 0, 8}, {1, 0, 16},
+                               {2, 0, 16}, {2, 1, 16}, {2, 2, 16}};
+constexpr int kNumSchedules = (int)(sizeof(kSchedules) / sizeof(kSchedules[0]));
+
+bool schedule_allowed(const q2d_ctx* ctx, int k) {
+    return kSchedules[k].kernel != 2 || ctx->opt.precision == Q2D_PREC_FP32_FLUX;
+}
 
 int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
-    static const Schedule cands[] = {{0, 0, 16}, {0, 1, 16}, {0, 2, 16}, {1, 0, 8}, {1, 0, 16}};
-    const int ncand = (int)(sizeof(cands) / sizeof(cands[0]));
+    const Schedule* cands = kSchedules;
+    const int ncand = kNumSchedules;
     const size_t nst = ctx->cases.size();
     const long long ec = ctx->ac.cap;
     DevBuf<double> saveP, saveSC;
@@ -680,6 +693,7 @@ int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
     float best = 1e30f;
     int besti = 0;
     for (int k = 0; k < ncand; ++k) {
+        if (!schedule_allowed(ctx, k)) continue;
         CK(cudaStreamSynchronize(ctx->stream));
         ctx->kernel = cands[k].kernel;
         ctx->tile = cands[k].tile;
@@ -781,7 +795,9 @@ q2d_ctx* new_ctx(const q2d_options* opt) {
     const char* t = getenv("Q2D_TILE");
     if (t) ctx->tile = std::max(0, std::min(kNumTiles - 1, atoi(t)));
     const char* kk = getenv("Q2D_KERNEL");
-    if (kk) ctx->kernel = atoi(kk) == 0 ? 0 : 1;
+    if (kk) ctx->kernel = std::max(0, std::min(2, atoi(kk)));
+    if (!kk && opt->precision == Q2D_PREC_FP32_FLUX) ctx->kernel = 2;
+    if (ctx->kernel == 2 && opt->precision != Q2D_PREC_FP32_FLUX) ctx->kernel = 0;
     const char* mh = getenv("Q2D_MARCH_H");
     if (mh) ctx->march_h = std::max(1, std::min(4096, atoi(mh)));
     return ctx;
@@ -957,6 +973,26 @@ int q2d_gpu_step(q2d_ctx* ctx, int nsteps, q2d_step_info* out) {
 }
 
 void* q2d_gpu_stream(const q2d_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int q2d_gpu_set_schedule(q2d_ctx* ctx, int schedule) {
+    if (!ctx || schedule < 0 || schedule >= kNumSchedules || !schedule_allowed(ctx, schedule))
+        return fail(ctx, Q2D_ERR_BADARG, "set_schedule: unknown schedule or not valid for this precision");
+    if (int e = ready(ctx)) return e;
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->kernel = kSchedules[schedule].kernel;
+    ctx->tile = kSchedules[schedule].tile;
+    ctx->march_h = kSchedules[schedule].march_h;
+    return rebuild_device_lists(ctx);
+}
+
+int q2d_gpu_get_schedule(const q2d_ctx* ctx) {
+    if (!ctx) return -1;
+    for (int k = 0; k < kNumSchedules; ++k)
+        if (kSchedules[k].kernel == ctx->kernel && kSchedules[k].tile == ctx->tile &&
+            (ctx->kernel != 1 || kSchedules[k].march_h == ctx->march_h))
+            return k;
+    return -1;
+}
 
 int q2d_gpu_autotune(q2d_ctx* ctx, int steps, int* schedule, float* ms_per_step) {
     if (!ctx || steps < 1) return fail(ctx, Q2D_ERR_BADARG, "autotune: bad argument");

@@ -7,6 +7,15 @@
 
 namespace q2d {
 
+// 8-byte asynchronous global -> shared copies (cp.async), completed by cp_async_wait_all.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
+}
+
 __device__ __forceinline__ int guide_i(int f) { return f == 1 ? 1 : (f == 2 ? -1 : 0); }
 __device__ __forceinline__ int guide_j(int f) { return f == 3 ? 1 : (f == 4 ? -1 : 0); }
 

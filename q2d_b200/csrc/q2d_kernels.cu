@@ -33,13 +33,6 @@ namespace q2d {
 // ------------------------------------------------------------------------------------------
 // The stage kernel
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
-}
 
 // Shared-memory layout of one tile (offsets in doubles).
 template <int PREC, int TX, int TY>
@@ -641,6 +634,25 @@ cudaError_t launch_copy(const double* src, double* dst, long long n, int* flag, 
 cudaError_t launch_resume(CaseState* cs, int n, int* flag, cudaStream_t s) {
     resume_kernel<<<(n + 255) / 256 > 0 ? (n + 255) / 256 : 1, 256, 0, s>>>(cs, n, flag);
     return cudaGetLastError();
+}
+
+cudaError_t launch_stage32_r0(const StageArgs& a, int tile, int grid, cudaStream_t s);
+cudaError_t launch_stage32_r1(const StageArgs& a, int tile, int grid, cudaStream_t s);
+cudaError_t launch_stage32_r2(const StageArgs& a, int tile, int grid, cudaStream_t s);
+int stage32_occupancy_r0(int tile);
+int stage32_occupancy_r1(int tile);
+int stage32_occupancy_r2(int tile);
+
+cudaError_t launch_stage32(const StageArgs& a, int riem, int tile, int grid, cudaStream_t s) {
+    if (riem == 1) return launch_stage32_r1(a, tile, grid, s);
+    if (riem == 2) return launch_stage32_r2(a, tile, grid, s);
+    return launch_stage32_r0(a, tile, grid, s);
+}
+
+int stage32_occupancy(int riem, int tile) {
+    if (riem == 1) return stage32_occupancy_r1(tile);
+    if (riem == 2) return stage32_occupancy_r2(tile);
+    return stage32_occupancy_r0(tile);
 }
 
 #define Q2D_MARCH_DECL(P, R)                                                                  \

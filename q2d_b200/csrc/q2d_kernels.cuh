@@ -12,6 +12,9 @@ void tile_dims(int tile, int* tx, int* ty, int* nt);
 
 cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int grid, cudaStream_t s);
 int stage_occupancy(int prec, int riem, int tile);
+// FP32-flux stage kernel (q2d_stage32.cuh) on the same tiles and work items.
+cudaError_t launch_stage32(const StageArgs& a, int riem, int tile, int grid, cudaStream_t s);
+int stage32_occupancy(int riem, int tile);
 // Warp-marching stage kernel (q2d_march.cuh): strips of 28 columns, item rows [j0, j1).
 constexpr int kMarchCols = 28;
 cudaError_t launch_march(const StageArgs& a, int prec, int riem, int lim, int grid, cudaStream_t s);

@@ -1,0 +1,568 @@
+// q2d_stage32.cuh — the fused RK-stage kernel of the FP32-flux / FP64-state form (sm_100a).
+//
+// Same work per launch as the FP64 stage kernel (q2d_kernels.cu): one RK stage for every
+// running case, CTAs taking TX x TY tiles of blocks in a grid-stride loop. The precision split
+// follows the form's definition: MUSCL reconstruction, limiters and the interior Riemann fluxes
+// run in FP32 and the face fluxes are kept in FP32; the residual accumulation (flux
+// differences), sources, RK stage combination, positivity checks, the new state and the
+// residual norms are FP64. Boundary-face fluxes (Lib_BC_Fluxes_*.f90) are computed in FP64 from
+// the FP64 state and stored like the interior ones.
+//
+// Per tile there are two CTA barriers:
+//   1. loads: the FP64 cell data of the tile (state, U^n, sur, dt, source geometry) by cp.async;
+//      the stencil state of the tile and its cross-shaped 2-cell halo converted to FP32, with
+//      every ghost cell (Fill_Ghost_Cell, Lib_Ghost.f90:16-299) evaluated from HBM by the thread
+//      that stores it; mean cell lengths and face geometry converted to FP32;
+//   2. faces: each interior face reconstructs its two states from its 4-cell stencil
+//      (Lib_Reconstruction.f90:10-29: three slopes, two limited slopes) and solves the Riemann
+//      problem (Convective_Flux, Lib_Convective.f90:15-82); boundary faces follow BC_Fluxes;
+//   3. cells: residual in the reference's accumulation order, sources, Newstate_Conservative
+//      + RK_stage + Check_And_Fix_State in FP64 and, on the last stage, the cell's next time
+//      step (FP32 arithmetic) and its squared change for the residual norm.
+#pragma once
+#include "q2d_common.cuh"
+#include "q2d_kernels.cuh"
+
+namespace q2d {
+
+// Shared-memory layout of one tile: FP64 cell planes first, then FP32 arrays.
+template <int TX, int TY>
+struct Tile32 {
+    static constexpr int W = TX + 4, H = TY + 4, AREA = W * H;
+    static constexpr int NFI = (TX + 1) * TY, NFJ = TX * (TY + 1), NF = NFI + NFJ;
+    static constexpr int NC = TX * TY;
+    // FP64 cell planes: 0-3 state, 4-7 state at the start of the step, 8 sur, 9 dt, 10-11 source
+    static constexpr int NCD = 12;
+    static constexpr int oP = 2 * NCD * NC;   // FP32 offsets from here on
+    static constexpr int oD = oP + 4 * AREA;  // [2][AREA] mean cell lengths
+    static constexpr int oG = oD + 2 * AREA;  // [3][NF] face nx, ny, length (i faces, then j faces)
+    static constexpr int oF = oG + 3 * NF;    // [4][NF] face fluxes (times length)
+    static constexpr int nfloats = oF + 4 * NF;
+    static constexpr size_t bytes = sizeof(float) * (size_t)nfloats;
+};
+
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// 1/x in FP64 from the FP32 hardware reciprocal and two Newton-Raphson steps (each doubles the
+// number of correct bits: 2^-22 -> 2^-44 -> below the FP64 rounding). Valid for |x| in the
+// normal FP32 range, which holds for cell volumes and densities.
+__device__ __forceinline__ double rcp64(double x) {
+    double y = (double)rcp_approx((float)x);
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
+// FP32 face state with its physical flux per unit normal.
+struct FS32 {
+    float r, u, v, p, un;
+    float Fr, Fu, Fv, Fe;
+};
+
+__device__ __forceinline__ FS32 phys32(float r, float u, float v, float p, float nx, float ny, float gf) {
+    FS32 s;
+    s.r = r; s.u = u; s.v = v; s.p = p;
+    s.un = u * nx + v * ny;
+    const float m = r * s.un;
+    s.Fr = m;
+    s.Fu = m * u + p * nx;
+    s.Fv = m * v + p * ny;
+    s.Fe = s.un * (gf * p + 0.5f * r * (u * u + v * v));
+    return s;
+}
+
+// Riemann solvers in FP32 (riemann_HLLC / riemann_HLLE, Lib_Riemann_HLL.f90:34-169; riemann_LLF,
+// Lib_Riemann_LF.f90:11-40): clamped Einfeldt speeds from constant-cp Roe averages, HLLC star
+// states written through the jumps (S* - un_K, p* - p_K). Returns the flux per unit length.
+template <int RIEM>
+__device__ __forceinline__ void riemann_f32(const FS32& L, const FS32& R, float nx, float ny, float gam,
+                                            float gm1, float gf, float* F) {
+    const float irl = rcp_approx(L.r), irr = rcp_approx(R.r);
+    const float al = sqrtf(gam * L.p * irl), ar = sqrtf(gam * R.p * irr);
+    if (RIEM == 2) {
+        const float A = fmaxf(fmaxf(fabsf(L.un - al), fabsf(R.un - ar)), fmaxf(fabsf(L.un + al), fabsf(R.un + ar)));
+        const float igm1 = 1.0f / gm1;
+        const float eL = L.p * igm1 + 0.5f * L.r * (L.u * L.u + L.v * L.v);
+        const float eR = R.p * igm1 + 0.5f * R.r * (R.u * R.u + R.v * R.v);
+        F[0] = 0.5f * (L.Fr + R.Fr - A * (R.r - L.r));
+        F[1] = 0.5f * (L.Fu + R.Fu - A * (R.r * R.u - L.r * L.u));
+        F[2] = 0.5f * (L.Fv + R.Fv - A * (R.r * R.v - L.r * L.v));
+        F[3] = 0.5f * (L.Fe + R.Fe - A * (eR - eL));
+        return;
+    }
+    const float srL = sqrtf(L.r), srR = sqrtf(R.r);
+    const float isr = rcp_approx(srL + srR);
+    const float u_roe = (srR * R.u + srL * L.u) * isr;
+    const float v_roe = (srR * R.v + srL * L.v) * isr;
+    const float h0l = gf * L.p * irl + 0.5f * (L.u * L.u + L.v * L.v);
+    const float h0r = gf * R.p * irr + 0.5f * (R.u * R.u + R.v * R.v);
+    const float h0_roe = (srR * h0r + srL * h0l) * isr;
+    const float a_roe = sqrtf(fmaxf(gm1 * (h0_roe - 0.5f * (u_roe * u_roe + v_roe * v_roe)), 0.0f));
+    const float un_roe = u_roe * nx + v_roe * ny;
+    const float S1 = fminf(fminf(0.0f, L.un - al), un_roe - a_roe);
+    const float S4 = fmaxf(fmaxf(0.0f, R.un + ar), un_roe + a_roe);
+    if (RIEM == 1) {
+        const float inv = rcp_approx(S4 - S1);
+        const float c = S1 * S4;
+        const float eL = L.r * h0l - L.p, eR = R.r * h0r - R.p;
+        F[0] = (S4 * L.Fr - S1 * R.Fr + c * (R.r - L.r)) * inv;
+        F[1] = (S4 * L.Fu - S1 * R.Fu + c * (R.r * R.u - L.r * L.u)) * inv;
+        F[2] = (S4 * L.Fv - S1 * R.Fv + c * (R.r * R.v - L.r * L.v)) * inv;
+        F[3] = (S4 * L.Fe - S1 * R.Fe + c * (eR - eL)) * inv;
+        return;
+    }
+    if (S1 >= 0.0f) { F[0] = L.Fr; F[1] = L.Fu; F[2] = L.Fv; F[3] = L.Fe; return; }
+    const float D = L.r * (S1 - L.un) - R.r * (S4 - R.un);
+    const float sm_unl = ((R.p - L.p) - R.r * (S4 - R.un) * (R.un - L.un)) * rcp_approx(D);   // S* - un_L
+    const float Sstar = L.un + sm_unl;
+    if (Sstar >= 0.0f) {
+        const float inv = rcp_approx(S1 - Sstar);
+        const float q = sm_unl * inv;
+        const float dps = L.r * (S1 - L.un) * sm_unl;                               // p* - p_L
+        const float e0l = h0l - L.p * irl;
+        F[0] = L.Fr + S1 * (L.r * q);
+        F[1] = L.Fu + S1 * (L.r * L.u * q + dps * nx * inv);
+        F[2] = L.Fv + S1 * (L.r * L.v * q + dps * ny * inv);
+        F[3] = L.Fe + S1 * (L.r * e0l * q + (dps * Sstar + L.p * sm_unl) * inv);
+        return;
+    }
+    if (S4 > 0.0f) {
+        const float inv = rcp_approx(S4 - Sstar);
+        const float sm_unr = sm_unl - (R.un - L.un);                                // S* - un_R
+        const float q = sm_unr * inv;
+        const float dps = R.r * (S4 - R.un) * sm_unr;                               // p* - p_R
+        const float e0r = h0r - R.p * irr;
+        F[0] = R.Fr + S4 * (R.r * q);
+        F[1] = R.Fu + S4 * (R.r * R.u * q + dps * nx * inv);
+        F[2] = R.Fv + S4 * (R.r * R.v * q + dps * ny * inv);
+        F[3] = R.Fe + S4 * (R.r * e0r * q + (dps * Sstar + R.p * sm_unr) * inv);
+        return;
+    }
+    F[0] = R.Fr; F[1] = R.Fu; F[2] = R.Fv; F[3] = R.Fe;
+}
+
+// One interior face: stencil cells m (= L-1), L, R, p (= R+1) at shared offsets base + k*step.
+template <int RIEM, int LIM, int AREA>
+__device__ __forceinline__ bool face32(const float* sP, const float* dlp, int base, int step, float nx,
+                                      float ny, float len, float gam, float gm1, float gf, float* out) {
+    const float dm = dlp[base], d0 = dlp[base + step], d1 = dlp[base + 2 * step], d2 = dlp[base + 3 * step];
+    const float il0 = rcp_approx(0.5f * (dm + d0));
+    const float il1 = rcp_approx(0.5f * (d0 + d1));
+    const float il2 = rcp_approx(0.5f * (d1 + d2));
+    const float lm = 0.5f * d0, lp = 0.5f * d1;
+    float QL[4], QR[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const float* q = sP + v * AREA + base;
+        const float qm = q[0], q0 = q[step], q1 = q[2 * step], q2 = q[3 * step];
+        const float s0 = (q0 - qm) * il0, s1 = (q1 - q0) * il1, s2 = (q2 - q1) * il2;
+        QL[v] = q0 + lim32<LIM>(s1, s0) * lm;
+        QR[v] = q1 - lim32<LIM>(s2, s1) * lp;
+    }
+    const bool ok = QL[0] > 0.0f && QL[3] > 0.0f && QR[0] > 0.0f && QR[3] > 0.0f;
+    const FS32 L = phys32(QL[0], QL[1], QL[2], QL[3], nx, ny, gf);
+    const FS32 R = phys32(QR[0], QR[1], QR[2], QR[3], nx, ny, gf);
+    float F[4];
+    riemann_f32<RIEM>(L, R, nx, ny, gam, gm1, gf, F);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) out[v] = F[v] * len;
+    return ok;
+}
+
+// Interior faces of a tile (i faces, then j faces); boundary positions are left to the
+// boundary-face loop.
+template <int RIEM, int LIM, int NT, int TX, int TY>
+__device__ __forceinline__ void interior_faces32(const StageArgs& a, const DBlock& B, CaseState* cs, int i0,
+                                                 int j0, const float* sP, const float* sD, const float* sG,
+                                                 float* sF, float gam, float gm1, float gf) {
+    using L = Tile32<TX, TY>;
+    constexpr int W = L::W, AREA = L::AREA, NFI = L::NFI, NF = L::NF;
+    const int ni = B.ni, nj = B.nj;
+    for (int f = threadIdx.x; f < NF; f += NT) {
+        int base, step, pos, lenn, k, kmax, ii, jj;
+        const float* dlp;
+        if (f < NFI) {
+            const int row = f / (TX + 1), col = f - row * (TX + 1);
+            pos = i0 + col; lenn = ni; k = j0 + row; kmax = nj;
+            base = (row + 2) * W + col; step = 1; dlp = sD;
+            ii = pos; jj = k + 1;
+        } else {
+            const int ff = f - NFI;
+            const int row = ff / TX, col = ff - row * TX;
+            pos = j0 + row; lenn = nj; k = i0 + col; kmax = ni;
+            base = row * W + col + 2; step = W; dlp = sD + AREA;
+            ii = k + 1; jj = pos;
+        }
+        if (k >= kmax || pos <= 0 || pos >= lenn) continue;
+        float out[4];
+        const bool ok = face32<RIEM, LIM, AREA>(sP, dlp, base, step, sG[f], sG[NF + f], sG[2 * NF + f], gam,
+                                                gm1, gf, out);
+        if (!ok) record_error(cs, 4, B.local_b, ii, jj, a.irk);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) sF[v * NF + f] = out[v];
+    }
+}
+
+template <int RIEM, int AREA>
+__device__ __forceinline__ bool face32_lim(int lim, const float* sP, const float* dlp, int base, int step,
+                                          float nx, float ny, float len, float gam, float gm1, float gf,
+                                          float* out) {
+    switch (lim) {
+        case 0: return face32<RIEM, 0, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 1: return face32<RIEM, 1, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 2: return face32<RIEM, 2, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 3: return face32<RIEM, 3, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 4: return face32<RIEM, 4, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 5: return face32<RIEM, 5, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        default: return face32<RIEM, 6, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+    }
+}
+
+template <int RIEM, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT, 3) stage32_kernel(const StageArgs a) {
+    using L = Tile32<TX, TY>;
+    constexpr int W = L::W, AREA = L::AREA, NFI = L::NFI, NF = L::NF, NC = L::NC;
+    extern __shared__ double smem[];
+    double* sC = smem;
+    float* sf = reinterpret_cast<float*>(smem);
+    float* sP = sf + L::oP;
+    float* sD = sf + L::oD;
+    float* sG = sf + L::oG;
+    float* sF = sf + L::oF;
+    __shared__ double red[(NT / 32) * 5];
+    __shared__ double tile_part[5];
+    __shared__ int s_flag;
+    const int tid = threadIdx.x;
+    const Gas& g = a.gas;
+    const float gam = (float)g.gamma, gm1 = (float)g.gm1, gf = (float)g.gfac;
+
+    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+        const WorkItem w = a.items[it];
+        const DBlock B = a.blocks[w.block];
+        CaseState* cs = &a.cstate[w.case_id];
+        if (__ldcg(&cs->status) != kStatus_Running) continue;   // uniform over the CTA
+        const int ni = B.ni, nj = B.nj, i0 = w.i0, j0 = w.j0;
+        const double* Pin = a.Pin + B.oc;
+        const long long pc = B.pc;
+        const double* scb = a.sc + 2 * B.oc;
+
+        // ---- 1. loads ------------------------------------------------------------------------
+        for (int k = tid; k < NC; k += NT) {
+            const int row = k / TX, col = k - row * TX;
+            const int ii = i0 + col, jj = j0 + row;
+            if (ii >= ni || jj >= nj) continue;
+            const long long cg = (long long)jj * ni + ii;
+            cp_async8(sC + 8 * NC + k, scb + cg);                                 // sur
+            if (!a.time_accurate) cp_async8(sC + 9 * NC + k, scb + pc + cg);      // dt
+            if (!a.first) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) cp_async8(sC + (4 + v) * NC + k, a.PO + B.oc + v * pc + cg);
+            }
+            if (a.source) {
+                cp_async8(sC + 10 * NC + k, scb + 6 * pc + cg);
+                if (a.source == 2) cp_async8(sC + 11 * NC + k, scb + 7 * pc + cg);
+            }
+        }
+        for (int f = tid; f < NF; f += NT) {
+            const double* src;
+            long long ps;
+            if (f < NFI) {
+                const int row = f / (TX + 1), col = f - row * (TX + 1);
+                const int jj = j0 + row, F = i0 + col;
+                if (jj >= nj || F > ni) continue;
+                src = a.fi + B.ofi + (long long)jj * (ni + 1) + F;
+                ps = B.pfi;
+            } else {
+                const int ff = f - NFI;
+                const int row = ff / TX, col = ff - row * TX;
+                const int ii = i0 + col, G = j0 + row;
+                if (ii >= ni || G > nj) continue;
+                src = a.fj + B.ofj + (long long)G * ni + ii;
+                ps = B.pfj;
+            }
+            sG[f] = (float)__ldg(src);
+            sG[NF + f] = (float)__ldg(src + ps);
+            sG[2 * NF + f] = (float)__ldg(src + 2 * ps);
+        }
+        for (int idx = tid; idx < AREA; idx += NT) {
+            const int r = idx / W, c = idx - r * W;
+            if ((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2)) continue;
+            const int ii = i0 - 2 + c, jj = j0 - 2 + r;
+            if (ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1) {
+                const double* src = a.dl + B.og + (long long)(jj + 2) * (ni + 4) + (ii + 2);
+                sD[idx] = (float)__ldg(src);
+                sD[AREA + idx] = (float)__ldg(src + B.pg);
+            }
+            const bool inI = (ii >= 0 && ii < ni), inJ = (jj >= 0 && jj < nj);
+            double q[4];
+            if (inI && inJ) {
+                const double* src = Pin + (long long)jj * ni + ii;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) q[v] = __ldg(src + v * pc);
+                if (r >= 2 && r < TY + 2 && c >= 2 && c < TX + 2) {
+                    const int kk = (r - 2) * TX + (c - 2);
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) sC[v * NC + kk] = q[v];
+                }
+            } else if (inI != inJ) {
+                // ghost cell gd layers beyond face f at tangential index k (Fill_Ghost_Cell)
+                int f, gd, k, bi, bj, di, dj;
+                if (!inI) {
+                    f = ii < 0 ? 1 : 2; gd = ii < 0 ? -ii : ii - ni + 1; k = jj;
+                    bi = ii < 0 ? 0 : ni - 1; bj = jj; di = ii < 0 ? 1 : -1; dj = 0;
+                } else {
+                    f = jj < 0 ? 3 : 4; gd = jj < 0 ? -jj : jj - nj + 1; k = ii;
+                    bi = ii; bj = jj < 0 ? 0 : nj - 1; di = 0; dj = jj < 0 ? 1 : -1;
+                }
+                if (gd > 2) continue;
+                const EdgeRec e = a.edges[B.eo[f - 1] + k];
+                const double* pb = Pin + (long long)bj * ni + bi;     // boundary cell
+                if (e.type == 101) {   // Ghost_Connection (Lib_Ghost.f90:143-160)
+                    const DBlock S = a.blocks[e.bs];
+                    const int si = e.is + guide_i(e.fs) * (gd - 1) - 1;
+                    const int sj = e.js + guide_j(e.fs) * (gd - 1) - 1;
+                    const double* src = a.Pin + S.oc + (long long)sj * S.ni + si;
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) q[v] = __ldg(src + v * S.pc);
+                } else if (e.type == 300) {   // Ghost_Symmetry (Lib_Ghost.f90:163-196)
+                    const double* gn = f <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (f == 1 ? 0 : ni)
+                                              : a.fj + B.ofj + (long long)(f == 3 ? 0 : nj) * ni + bi;
+                    const long long gs = f <= 2 ? B.pfi : B.pfj;
+                    const double nx = __ldg(gn), ny = __ldg(gn + gs);
+                    const double vx = __ldg(pb + pc), vy = __ldg(pb + 2 * pc);
+                    const double udotn = vx * nx + vy * ny;
+                    q[0] = __ldg(pb);
+                    q[1] = vx - 2.0 * udotn * nx;
+                    q[2] = vy - 2.0 * udotn * ny;
+                    q[3] = __ldg(pb + 3 * pc);
+                } else if (e.type == 0 || e.type == 401 || e.type == 405 || e.type == 406 || e.type < 0) {
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) q[v] = __ldg(pb + v * pc);   // Ghost_ZG_Extrapolate
+                } else {   // Ghost_Extrapolate (Lib_Ghost.f90:270-299)
+                    const long long s1 = (long long)dj * ni + di;
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        const double b0 = __ldg(pb + v * pc), i1 = __ldg(pb + v * pc + s1),
+                                     i2 = __ldg(pb + v * pc + 2 * s1);
+                        const double g1 = 3.0 * b0 - 3.0 * i1 + i2;
+                        q[v] = gd == 1 ? g1 : 3.0 * g1 - 3.0 * b0 + i1;
+                    }
+                }
+            } else {
+                continue;
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) sP[v * AREA + idx] = (float)q[v];
+        }
+        cp_async_wait_all();
+        __syncthreads();
+
+        // ---- 2. face fluxes ------------------------------------------------------------------
+        switch (a.limiter) {
+            case 0: interior_faces32<RIEM, 0, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+            case 1: interior_faces32<RIEM, 1, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+            case 2: interior_faces32<RIEM, 2, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+            case 3: interior_faces32<RIEM, 3, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+            case 4: interior_faces32<RIEM, 4, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+            case 5: interior_faces32<RIEM, 5, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+            default: interior_faces32<RIEM, 6, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+        }
+        {   // boundary faces (BC_Fluxes, Mod_BC_Fluxes.f90:79-269), FP64 from the FP64 state
+            const int nrow = min(TY, nj - j0), ncol = min(TX, ni - i0);
+            const int nl = (i0 == 0) ? nrow : 0;
+            const int nr = (i0 + TX >= ni) ? nrow : 0;
+            const int nb = (j0 == 0) ? ncol : 0;
+            const int nt = (j0 + TY >= nj) ? ncol : 0;
+            for (int t = tid; t < nl + nr + nb + nt; t += NT) {
+                int Fm, k, bi, bj, di, dj, f;
+                if (t < nl) {
+                    Fm = 1; k = j0 + t; bi = 0; bj = k; di = 1; dj = 0; f = t * (TX + 1);
+                } else if (t < nl + nr) {
+                    const int u = t - nl;
+                    Fm = 2; k = j0 + u; bi = ni - 1; bj = k; di = -1; dj = 0; f = u * (TX + 1) + (ni - i0);
+                } else if (t < nl + nr + nb) {
+                    const int u = t - nl - nr;
+                    Fm = 3; k = i0 + u; bi = k; bj = 0; di = 0; dj = 1; f = NFI + u;
+                } else {
+                    const int u = t - nl - nr - nb;
+                    Fm = 4; k = i0 + u; bi = k; bj = nj - 1; di = 0; dj = -1; f = NFI + (nj - j0) * TX + u;
+                }
+                const EdgeRec e = a.edges[B.eo[Fm - 1] + k];
+                double X[4] = {0.0, 0.0, 0.0, 0.0};
+                if (e.type == 101) {   // BC_Connection_Eul: the interior scheme on the ghost stencil
+                    const int cb = (bj - j0 + 2) * W + (bi - i0 + 2);
+                    int base, step;
+                    const float* dlp;
+                    if (Fm <= 2) { step = 1; dlp = sD; base = Fm == 1 ? cb - 2 : cb - 1; }
+                    else { step = W; dlp = sD + AREA; base = Fm == 3 ? cb - 2 * W : cb - W; }
+                    float out[4];
+                    const bool ok = face32_lim<RIEM, AREA>(a.limiter, sP, dlp, base, step, sG[f], sG[NF + f],
+                                                           sG[2 * NF + f], gam, gm1, gf, out);
+                    if (!ok) record_error(cs, 4, B.local_b, bi + 1, bj + 1, a.irk);
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) X[v] = (double)out[v];
+                } else if (e.type >= 0) {
+                    const double* pb = Pin + (long long)bj * ni + bi;
+                    const int ni2 = bi + di, nj2 = bj + dj;   // inward neighbour
+                    Q4 Bp, Ip;
+                    if (ni2 >= 0 && ni2 < ni && nj2 >= 0 && nj2 < nj) {
+                        const double* pi = Pin + (long long)nj2 * ni + ni2;
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) Ip.v[v] = __ldg(pi + v * pc);
+                    } else {   // one-cell-thick block: the neighbour is the opposite ghost
+                        const int sidx = (nj2 - j0 + 2) * W + (ni2 - i0 + 2);
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) Ip.v[v] = (double)sP[v * AREA + sidx];
+                    }
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) Bp.v[v] = __ldg(pb + v * pc);
+                    const double* dlb = a.dl + B.og + (long long)(Fm <= 2 ? 0 : 1) * B.pg;
+                    const double dlbv = __ldg(dlb + (long long)(bj + 2) * (ni + 4) + (bi + 2));
+                    const double dli = __ldg(dlb + (long long)(nj2 + 2) * (ni + 4) + (ni2 + 2));
+                    const double* gsrc = Fm <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (Fm == 1 ? 0 : ni)
+                                                 : a.fj + B.ofj + (long long)(Fm == 3 ? 0 : nj) * ni + bi;
+                    const long long gs = Fm <= 2 ? B.pfi : B.pfj;
+                    const double nx = __ldg(gsrc), ny = __ldg(gsrc + gs), ln = __ldg(gsrc + 2 * gs);
+                    const Q4 q = bc_face<RIEM>(a.gas, a.limiter, e.type, Fm, Bp, Ip, dlbv, dli, nx, ny, ln,
+                                               e.param >= 0 ? a.bcp + e.param : nullptr);
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) X[v] = q.v[v];
+                }
+#pragma unroll
+                for (int v = 0; v < 4; ++v) sF[v * NF + f] = (float)X[v];
+            }
+        }
+        __syncthreads();
+
+        // ---- 3. residual, sources, RK update (+ next dt and residual norm) -----------------------
+        double acc[5] = {0.0, 0.0, 0.0, 0.0, 1e300};
+        const double dt_case = __ldcg(&cs->dt_step);
+        const long long iter_next = __ldcg(&cs->iter) + (a.first ? 1 : 0) + 1;
+        const int ndir = a.cases[w.case_id].ndir;
+        for (int k = tid; k < NC; k += NT) {
+            const int row = k / TX, col = k - row * TX;
+            const int ii = i0 + col, jj = j0 + row;
+            if (ii >= ni || jj >= nj) continue;
+            const int i1 = ii + 1, j1 = jj + 1;
+            const int fi0 = row * (TX + 1) + col, fj0 = NFI + row * TX + col;
+            double r[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {   // interior i, interior j, then boundary faces 1..4
+                const float* Fv = sF + v * NF;
+                double x = 0.0;
+                if (i1 > 1) x = x - (double)Fv[fi0];
+                if (i1 < ni) x = x + (double)Fv[fi0 + 1];
+                if (j1 > 1) x = x - (double)Fv[fj0];
+                if (j1 < nj) x = x + (double)Fv[fj0 + TX];
+                if (i1 == 1) x = x - (double)Fv[fi0];
+                if (i1 == ni) x = x + (double)Fv[fi0 + 1];
+                if (j1 == 1) x = x - (double)Fv[fj0];
+                if (j1 == nj) x = x + (double)Fv[fj0 + TX];
+                r[v] = x;
+            }
+            const long long cg = (long long)jj * ni + ii;
+            const double sur = sC[8 * NC + k];
+            double P[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) P[v] = sC[v * NC + k];
+            if (a.source) {
+                // S = [rho, rho u, rho v, rho E0 + p] * f0 with f0 = -v/r (Lib_Source_Axisymmetry.f90:
+                // 65-76) or V.G (Lib_Source_Areavariation.f90:120-142); Res -= S * sur
+                const double rE0 = P[3] * g.igm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
+                const double f0 = a.source == 1 ? -P[2] * sC[10 * NC + k]
+                                                : P[1] * sC[10 * NC + k] + P[2] * sC[11 * NC + k];
+                const double fs = f0 * sur;
+                r[0] = r[0] - P[0] * fs;
+                r[1] = r[1] - P[0] * P[1] * fs;
+                r[2] = r[2] - P[0] * P[2] * fs;
+                r[3] = r[3] - (rE0 + P[3]) * fs;
+            }
+            const double dt = a.time_accurate ? dt_case : sC[9 * NC + k];
+            double PO[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) PO[v] = a.first ? P[v] : sC[(4 + v) * NC + k];
+            const double fr = -dt * rcp64(sur);
+            double U0[4], U[4];
+            U0[0] = PO[0]; U0[1] = PO[0] * PO[1]; U0[2] = PO[0] * PO[2];
+            U0[3] = PO[3] * g.igm1 + 0.5 * PO[0] * (PO[1] * PO[1] + PO[2] * PO[2]);
+            U[0] = P[0]; U[1] = P[0] * P[1]; U[2] = P[0] * P[2];
+            U[3] = P[3] * g.igm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) U[v] = U0[v] + (U[v] - U0[v] + r[v] * fr) * a.rk_c;
+            double N[4];
+            N[0] = U[0];
+            const double ir = rcp64(U[0]);
+            N[1] = U[1] * ir;
+            N[2] = U[2] * ir;
+            N[3] = g.gm1 * (U[3] - 0.5 * U[0] * (N[1] * N[1] + N[2] * N[2]));
+            if (isnan(N[0]) || isnan(N[1]) || isnan(N[2]) || isnan(N[3]) || N[3] < 0.0)
+                record_error(cs, 5, B.local_b, i1, j1, a.irk);
+            if (N[0] < 1e-20) N[0] = 1e-20;
+            double* po = a.Pout + B.oc;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) po[v * pc + cg] = N[v];
+            if (a.last) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const double d = fabs(N[v] - PO[v]);
+                    acc[v] += d * d;
+                }
+                // Compute_dt (Mod_dt.f90:59-104) in FP32 arithmetic
+                const int sidx = (row + 2) * W + (col + 2);
+                const float rho = (float)N[0], u = (float)N[1], vv = (float)N[2], p = (float)N[3];
+                const float snd = sqrtf(gam * p * rcp_approx(rho));
+                const float cfl = (float)a.cfl;
+                float dtmin = 1e8f;
+                {
+                    const float e0 = (float)scb[2 * pc + cg], e1 = (float)scb[3 * pc + cg];
+                    dtmin = fminf(dtmin, sD[sidx] * rcp_approx(fabsf(u * e0 + vv * e1) + snd) * cfl);
+                }
+                if (ndir == 2) {
+                    const float e0 = (float)scb[4 * pc + cg], e1 = (float)scb[5 * pc + cg];
+                    dtmin = fminf(dtmin, sD[AREA + sidx] * rcp_approx(fabsf(u * e0 + vv * e1) + snd) * cfl);
+                }
+                double dtn = (double)dtmin;
+                if (iter_next < a.rampa) dtn = dtn * (double)iter_next / (double)a.rampa;
+                if (!a.time_accurate) a.sc[2 * B.oc + pc + cg] = dtn;
+                acc[4] = fmin(acc[4], dtn);
+            }
+        }
+        if (a.last) {
+            block_reduce_store<NT>(acc, red, tile_part);
+            if (tid == 0)
+                for (int k = 0; k < 5; ++k) a.part[5 * (size_t)it + k] = tile_part[k];
+        }
+        item_done<NT>(a, w.case_id, a.last != 0, a.last != 0, a.first != 0, red, &s_flag);
+    }
+}
+
+template <int RIEM, int TX, int TY, int NT>
+cudaError_t launch_stage32_t(const StageArgs& a, int grid, cudaStream_t s) {
+    constexpr size_t smem = Tile32<TX, TY>::bytes;
+    auto k = stage32_kernel<RIEM, TX, TY, NT>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    k<<<grid, NT, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int RIEM, int TX, int TY, int NT>
+int stage32_occupancy_t() {
+    constexpr size_t smem = Tile32<TX, TY>::bytes;
+    auto k = stage32_kernel<RIEM, TX, TY, NT>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, NT, smem);
+    return n;
+}
+
+}  // namespace q2d

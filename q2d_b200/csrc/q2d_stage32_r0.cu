@@ -1,0 +1,22 @@
+// Instantiations of the FP32-flux stage kernel for Riemann solver 0 (see q2d_stage32.cuh).
+#include "q2d_stage32.cuh"
+
+namespace q2d {
+
+cudaError_t launch_stage32_r0(const StageArgs& a, int tile, int grid, cudaStream_t s) {
+    switch (tile) {
+        case 1: return launch_stage32_t<0, 32, 8, 256>(a, grid, s);
+        case 2: return launch_stage32_t<0, 64, 4, 256>(a, grid, s);
+        default: return launch_stage32_t<0, 32, 10, 256>(a, grid, s);
+    }
+}
+
+int stage32_occupancy_r0(int tile) {
+    switch (tile) {
+        case 1: return stage32_occupancy_t<0, 32, 8, 256>();
+        case 2: return stage32_occupancy_t<0, 64, 4, 256>();
+        default: return stage32_occupancy_t<0, 32, 10, 256>();
+    }
+}
+
+}  // namespace q2d

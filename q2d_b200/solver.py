@@ -88,7 +88,18 @@ class Q2DSolver:
             raise Q2DError(st, f"{self.prefix}_step", str([o["err_at"] for o in out if o["err"]]))
         return out
 
-    SCHEDULES = ["tile 32x10", "tile 32x8", "tile 64x4", "march 28 cols x 8 rows", "march 28 cols x 16 rows"]
+    SCHEDULES = ["tile 32x10", "tile 32x8", "tile 64x4", "march 28 cols x 8 rows", "march 28 cols x 16 rows",
+                 "fp32-flux tile 32x10", "fp32-flux tile 32x8", "fp32-flux tile 64x4"]
+
+    def set_schedule(self, schedule) -> None:
+        """Pins a schedule (index or name from SCHEDULES) without tuning (q2d_gpu_set_schedule)."""
+        idx = self.SCHEDULES.index(schedule) if isinstance(schedule, str) else int(schedule)
+        self._call("set_schedule", self.ctx, idx)
+
+    @property
+    def schedule(self) -> str:
+        k = self.lib.q2d_gpu_get_schedule(self.ctx)
+        return self.SCHEDULES[k] if k >= 0 else "unknown"
 
     def autotune(self, steps: int = 2) -> dict:
         """Times every stage-kernel schedule on this workload and keeps the fastest

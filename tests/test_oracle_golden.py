@@ -164,27 +164,10 @@ def test_riemann_supersonic_upwinding(kind):
 def test_conservation_closed_domain():
     """All-wall (BC 300) curvilinear box, random smooth state: the oracle conserves mass and
     energy to round-off per step (sum of U * sur)."""
-    ni = nj = 24
-    rng = np.random.default_rng(3)
-    x, y = np.meshgrid(np.linspace(0, 1, ni + 1), np.linspace(0, 1, nj + 1))
-    x = x + 0.02 * np.sin(2 * np.pi * y)
-    nodes = np.stack([x, y], axis=-1)
-    prim = np.zeros((nj, ni, 4))
-    prim[..., 0] = 1 + 0.1 * rng.random((nj, ni))
-    prim[..., 1] = 0.1 * rng.standard_normal((nj, ni))
-    prim[..., 2] = 0.1 * rng.standard_normal((nj, ni))
-    prim[..., 3] = 1 + 0.1 * rng.random((nj, ni))
-    blk = cases.BlockSpec(ni, nj, nodes, prim)
-    bcs = cases.edge_records(1, ni, nj, {f: (300, {}) for f in (1, 2, 3, 4)})
-    cs = cases.CaseSpec("box", [blk], bcs, dict(limiter="vanleer", n_rk=3, cfl=0.4, time_accurate=1))
+    cs = cases.closed_box(24, 24, seed=3)
+    sur = cases.cell_areas(cs.blocks[0])
     s = oracle.solver(make_options(cs), [cs])
     try:
-        # cell areas from the nodes (shoelace on the quads)
-        X, Y = nodes[..., 0], nodes[..., 1]
-        d1x, d1y = X[1:, 1:] - X[:-1, :-1], Y[1:, 1:] - Y[:-1, :-1]
-        d2x, d2y = X[:-1, 1:] - X[1:, :-1], Y[:-1, 1:] - Y[1:, :-1]
-        sur = 0.5 * np.abs(d1x * d2y - d1y * d2x)
-
         def totals(P):
             from tests.conftest import cons
             U = cons(P)
