@@ -29,6 +29,59 @@ __device__ __forceinline__ void record_error(CaseState* cs, int code, int b, int
 }
 
 // ------------------------------------------------------------------------------------------
+// Ghost cell (ii, jj) of block B outside exactly one of its index ranges (Fill_Ghost_Cell,
+// Lib_Ghost.f90:16-299), evaluated from the stage's input state in HBM: gd = 1, 2 layers beyond
+// face f at tangential index k. Returns false beyond the second layer.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool ghost_value(const StageArgs& a, const DBlock& B, int ii, int jj, double* q) {
+    const int ni = B.ni, nj = B.nj;
+    const bool inI = (ii >= 0 && ii < ni);
+    int f, gd, k, bi, bj, di, dj;
+    if (!inI) {
+        f = ii < 0 ? 1 : 2; gd = ii < 0 ? -ii : ii - ni + 1; k = jj;
+        bi = ii < 0 ? 0 : ni - 1; bj = jj; di = ii < 0 ? 1 : -1; dj = 0;
+    } else {
+        f = jj < 0 ? 3 : 4; gd = jj < 0 ? -jj : jj - nj + 1; k = ii;
+        bi = ii; bj = jj < 0 ? 0 : nj - 1; di = 0; dj = jj < 0 ? 1 : -1;
+    }
+    if (gd > 2) return false;
+    const long long pc = B.pc;
+    const EdgeRec e = a.edges[B.eo[f - 1] + k];
+    const double* pb = a.Pin + B.oc + (long long)bj * ni + bi;    // boundary cell
+    if (e.type == 101) {   // Ghost_Connection (Lib_Ghost.f90:143-160): the donor block's cells
+        const DBlock S = a.blocks[e.bs];
+        const int si = e.is + guide_i(e.fs) * (gd - 1) - 1;
+        const int sj = e.js + guide_j(e.fs) * (gd - 1) - 1;
+        const double* src = a.Pin + S.oc + (long long)sj * S.ni + si;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) q[v] = __ldg(src + v * S.pc);
+    } else if (e.type == 300) {   // Ghost_Symmetry (Lib_Ghost.f90:163-196)
+        const double* gn = f <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (f == 1 ? 0 : ni)
+                                  : a.fj + B.ofj + (long long)(f == 3 ? 0 : nj) * ni + bi;
+        const long long gs = f <= 2 ? B.pfi : B.pfj;
+        const double nx = __ldg(gn), ny = __ldg(gn + gs);
+        const double vx = __ldg(pb + pc), vy = __ldg(pb + 2 * pc);
+        const double udotn = vx * nx + vy * ny;
+        q[0] = __ldg(pb);
+        q[1] = vx - 2.0 * udotn * nx;
+        q[2] = vy - 2.0 * udotn * ny;
+        q[3] = __ldg(pb + 3 * pc);
+    } else if (e.type == 0 || e.type == 401 || e.type == 405 || e.type == 406 || e.type < 0) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) q[v] = __ldg(pb + v * pc);   // Ghost_ZG_Extrapolate (:199-219)
+    } else {   // Ghost_Extrapolate (Lib_Ghost.f90:270-299)
+        const long long s1 = (long long)dj * ni + di;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const double b0 = __ldg(pb + v * pc), i1 = __ldg(pb + v * pc + s1), i2 = __ldg(pb + v * pc + 2 * s1);
+            const double g1 = 3.0 * b0 - 3.0 * i1 + i2;
+            q[v] = gd == 1 ? g1 : 3.0 * g1 - 3.0 * b0 + i1;
+        }
+    }
+    return true;
+}
+
+// ------------------------------------------------------------------------------------------
 // Boundary-face fluxes, FP64 (the oracle's restatement of Lib_BC_Fluxes_*.f90). Each returns
 // the reference's `Flux` vector; the cell adds it with the sign of its face like an interior
 // face (modfm2 = -1 on faces 1/3, +1 on faces 2/4).

@@ -190,19 +190,11 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
                 const double* src = Pin + (long long)jj * ni + ii;
 #pragma unroll
                 for (int v = 0; v < 4; ++v) cp_async8(sP + v * AREA + idx, src + v * pc);
-            } else if (inI != inJ) {
-                int f, gd, k;
-                if (!inI) { f = ii < 0 ? 1 : 2; gd = ii < 0 ? -ii : ii - ni + 1; k = jj; }
-                else      { f = jj < 0 ? 3 : 4; gd = jj < 0 ? -jj : jj - nj + 1; k = ii; }
-                if (gd > 2) continue;
-                const EdgeRec e = a.edges[B.eo[f - 1] + k];
-                if (e.type == 101) {   // Ghost_Connection (Lib_Ghost.f90:143-160): donor cells
-                    const DBlock S = a.blocks[e.bs];
-                    const int si = e.is + guide_i(e.fs) * (gd - 1) - 1;
-                    const int sj = e.js + guide_j(e.fs) * (gd - 1) - 1;
-                    const double* src = a.Pin + S.oc + (long long)sj * S.ni + si;
+            } else if (inI != inJ) {   // every ghost the tile's faces read, from HBM
+                double q[4];
+                if (ghost_value(a, B, ii, jj, q)) {
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) cp_async8(sP + v * AREA + idx, src + v * S.pc);
+                    for (int v = 0; v < 4; ++v) sP[v * AREA + idx] = q[v];
                 }
             }
         }
@@ -238,64 +230,6 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
             }
         }
         cp_async_wait_all();
-        __syncthreads();
-
-        // ---- 2. ghost cells that follow from the tile's own cells --------------------------
-        {
-            const int nrow = min(TY, nj - j0), ncol = min(TX, ni - i0);
-            const int nl = (i0 == 0) ? nrow : 0;
-            const int nr = (i0 + TX >= ni) ? nrow : 0;
-            const int nb = (j0 == 0) ? ncol : 0;
-            const int nt = (j0 + TY >= nj) ? ncol : 0;
-            for (int t = tid; t < nl + nr + nb + nt; t += NT) {
-                int f, k, cb, rb, dc, dr, gidx;   // boundary cell, outward step, face geometry index
-                const double* gn;
-                int gstride;
-                if (t < nl) {
-                    f = 1; rb = 2 + t; cb = 2; k = j0 + t; dc = -1; dr = 0;
-                    gn = sGi; gstride = NFI; gidx = t * (TX + 1);
-                } else if (t < nl + nr) {
-                    const int u = t - nl;
-                    f = 2; rb = 2 + u; cb = (ni - 1 - i0) + 2; k = j0 + u; dc = 1; dr = 0;
-                    gn = sGi; gstride = NFI; gidx = u * (TX + 1) + (ni - i0);
-                } else if (t < nl + nr + nb) {
-                    const int u = t - nl - nr;
-                    f = 3; cb = 2 + u; rb = 2; k = i0 + u; dc = 0; dr = -1;
-                    gn = sGj; gstride = NFJ; gidx = u;
-                } else {
-                    const int u = t - nl - nr - nb;
-                    f = 4; cb = 2 + u; rb = (nj - 1 - j0) + 2; k = i0 + u; dc = 0; dr = 1;
-                    gn = sGj; gstride = NFJ; gidx = (nj - j0) * TX + u;
-                }
-                const int type = a.edges[B.eo[f - 1] + k].type;
-                if (type == 101) continue;
-                const int b0 = rb * W + cb;
-                const int s1 = b0 + dr * W + dc, s2 = s1 + dr * W + dc;
-                const int in1 = b0 - dr * W - dc, in2 = in1 - dr * W - dc;
-                if (type == 300) {   // Ghost_Symmetry (Lib_Ghost.f90:163-196)
-                    const double nx = gn[gidx], ny = gn[gstride + gidx];
-                    const double vx = sP[AREA + b0], vy = sP[2 * AREA + b0];
-                    const double udotn = vx * nx + vy * ny;
-                    const double gx = vx - 2.0 * udotn * nx, gy = vy - 2.0 * udotn * ny;
-                    sP[s1] = sP[b0]; sP[AREA + s1] = gx; sP[2 * AREA + s1] = gy; sP[3 * AREA + s1] = sP[3 * AREA + b0];
-                    sP[s2] = sP[b0]; sP[AREA + s2] = gx; sP[2 * AREA + s2] = gy; sP[3 * AREA + s2] = sP[3 * AREA + b0];
-                } else if (type == 0 || type == 401 || type == 405 || type == 406 || type < 0) {
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) {   // Ghost_ZG_Extrapolate (:199-219)
-                        sP[v * AREA + s1] = sP[v * AREA + b0];
-                        sP[v * AREA + s2] = sP[v * AREA + b0];
-                    }
-                } else {
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) {   // Ghost_Extrapolate (:270-299)
-                        const double* q = sP + v * AREA;
-                        const double g1 = 3.0 * q[b0] - 3.0 * q[in1] + q[in2];
-                        sP[v * AREA + s1] = g1;
-                        sP[v * AREA + s2] = 3.0 * g1 - 3.0 * q[b0] + q[in1];
-                    }
-                }
-            }
-        }
         __syncthreads();
 
         // ---- 3. interface slopes ---------------------------------------------------------

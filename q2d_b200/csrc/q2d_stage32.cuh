@@ -309,50 +309,8 @@ __global__ void __launch_bounds__(NT, 3) stage32_kernel(const StageArgs a) {
 #pragma unroll
                     for (int v = 0; v < 4; ++v) sC[v * NC + kk] = q[v];
                 }
-            } else if (inI != inJ) {
-                // ghost cell gd layers beyond face f at tangential index k (Fill_Ghost_Cell)
-                int f, gd, k, bi, bj, di, dj;
-                if (!inI) {
-                    f = ii < 0 ? 1 : 2; gd = ii < 0 ? -ii : ii - ni + 1; k = jj;
-                    bi = ii < 0 ? 0 : ni - 1; bj = jj; di = ii < 0 ? 1 : -1; dj = 0;
-                } else {
-                    f = jj < 0 ? 3 : 4; gd = jj < 0 ? -jj : jj - nj + 1; k = ii;
-                    bi = ii; bj = jj < 0 ? 0 : nj - 1; di = 0; dj = jj < 0 ? 1 : -1;
-                }
-                if (gd > 2) continue;
-                const EdgeRec e = a.edges[B.eo[f - 1] + k];
-                const double* pb = Pin + (long long)bj * ni + bi;     // boundary cell
-                if (e.type == 101) {   // Ghost_Connection (Lib_Ghost.f90:143-160)
-                    const DBlock S = a.blocks[e.bs];
-                    const int si = e.is + guide_i(e.fs) * (gd - 1) - 1;
-                    const int sj = e.js + guide_j(e.fs) * (gd - 1) - 1;
-                    const double* src = a.Pin + S.oc + (long long)sj * S.ni + si;
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) q[v] = __ldg(src + v * S.pc);
-                } else if (e.type == 300) {   // Ghost_Symmetry (Lib_Ghost.f90:163-196)
-                    const double* gn = f <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (f == 1 ? 0 : ni)
-                                              : a.fj + B.ofj + (long long)(f == 3 ? 0 : nj) * ni + bi;
-                    const long long gs = f <= 2 ? B.pfi : B.pfj;
-                    const double nx = __ldg(gn), ny = __ldg(gn + gs);
-                    const double vx = __ldg(pb + pc), vy = __ldg(pb + 2 * pc);
-                    const double udotn = vx * nx + vy * ny;
-                    q[0] = __ldg(pb);
-                    q[1] = vx - 2.0 * udotn * nx;
-                    q[2] = vy - 2.0 * udotn * ny;
-                    q[3] = __ldg(pb + 3 * pc);
-                } else if (e.type == 0 || e.type == 401 || e.type == 405 || e.type == 406 || e.type < 0) {
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) q[v] = __ldg(pb + v * pc);   // Ghost_ZG_Extrapolate
-                } else {   // Ghost_Extrapolate (Lib_Ghost.f90:270-299)
-                    const long long s1 = (long long)dj * ni + di;
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) {
-                        const double b0 = __ldg(pb + v * pc), i1 = __ldg(pb + v * pc + s1),
-                                     i2 = __ldg(pb + v * pc + 2 * s1);
-                        const double g1 = 3.0 * b0 - 3.0 * i1 + i2;
-                        q[v] = gd == 1 ? g1 : 3.0 * g1 - 3.0 * b0 + i1;
-                    }
-                }
+            } else if (inI != inJ) {   // ghost cell (Fill_Ghost_Cell) from HBM
+                if (!ghost_value(a, B, ii, jj, q)) continue;
             } else {
                 continue;
             }

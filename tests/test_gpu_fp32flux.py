@@ -104,10 +104,13 @@ def test_conservation_closed_domain(precision):
 
 
 def test_fp32flux_state_independent_of_tile():
+    """Every face flux and cell update reads the same inputs whatever the tile shape; the
+    kernels of different tile shapes may still fuse FP64 multiply-adds differently, so states
+    agree to FP64 rounding (1e-13 relative), not necessarily bit for bit."""
     batch = cases.area_nozzle_batch(n=5, seed=17, nx_range=(40, 150), ny_range=(8, 20))
     ref, _ = run(batch, 30, schedule=SCHED[0], precision=1)
     for sch in SCHED[1:3]:
         got, _ = run(batch, 30, schedule=sch, precision=1)
         for ca, cb in zip(got, ref):
             for xa, xb in zip(ca, cb):
-                assert np.array_equal(xa, xb), sch
+                assert rel_linf(xa, xb).max() <= 1e-13, sch

@@ -72,3 +72,25 @@ def test_time_accurate_to_end_time():
     assert gi[0]["todo"] == oi[0]["todo"] == 3
     assert gi[0]["iter"] == oi[0]["iter"]
     assert abs(gi[0]["time"] - oi[0]["time"]) <= 1e-12
+
+
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 4])
+def test_halo_reaching_ghosts_of_untouched_edge(schedule):
+    """ni = 129 and nj = 41 leave a last tile one cell wide / one row high for every tile
+    shape, so the halo of the tile before it reaches the ghost layer of a block edge that
+    none of its own cells touch."""
+    from q2d_b200 import make_options
+    from q2d_b200.solver import Q2DSolver
+    from oracle import oracle
+    cs = cases.ramp(129, 41, seed=8)
+    opts = make_options(cs)
+    g = Q2DSolver(opts, [cs])
+    o = oracle.solver(opts, [cs])
+    try:
+        g.set_schedule(schedule)
+        g.step(3)
+        o.step(3)
+        check([[g.prim(0, 0)]], [[o.prim(0, 0)]], 1e-11, f"ramp 129x41 schedule {schedule}")
+    finally:
+        g.close()
+        o.close()
