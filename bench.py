@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--schedule", type=int, default=None,
+                    help="pin the stage-kernel schedule of the headline leg instead of autotuning")
+    ap.add_argument("--form", default="fp32-flux", choices=["fp32-flux", "fp64"],
+                    help="precision form of the headline leg (profiling of the plain FP64 kernel)")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="length of the arrival window")
     ap.add_argument("--serve-iters", type=int, default=200, help="iteration cap (fixed end) per request")
@@ -283,8 +287,14 @@ def main():
         return float(t.item())
 
     # ---- FP32-flux / FP64-state batched form (the headline) ----------------------------
-    s = Q2DSolver(make_options(batch[0], precision=1), batch)
-    tuned = s.autotune(2)
+    prec = 1 if args.form == "fp32-flux" else 0
+    s = Q2DSolver(make_options(batch[0], precision=prec), batch)
+    if args.schedule is None:
+        tuned = s.autotune(2)
+        tuned["schedule"] += " (autotuned)"
+    else:
+        s.set_schedule(args.schedule)
+        tuned = {"schedule": s.schedule + " (pinned)"}
     s.step(W)
     barrier()
     with ClockSampler(local) as clk:
@@ -301,7 +311,7 @@ def main():
     except Exception:
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
-    traffic = read_traffic(tuned["schedule"])
+    traffic = read_traffic(s.schedule)
     # ---- e2e through the C ABI with host buffers ----------------------------------------
     e2e = None
     if not args.no_e2e:
@@ -361,11 +371,11 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "fp32-flux/fp64-state", "data": "synthetic",
+        "dtype": "fp32-flux/fp64-state" if prec == 1 else "f64", "data": "synthetic",
         "config": {"workload": "batched area-variation nozzles (4096 independent cases per GPU, "
                                "Nx~lognormal[64,1024], Ny~U{8..64}), van Leer + HLLC, SSP-RK3, local dt",
                    "cases_per_gpu": len(batch), "cells_per_gpu": cells,
-                   "schedule": tuned["schedule"] + " (autotuned)",
+                   "schedule": tuned["schedule"],
                    "parallelism": f"replicas x{world} (independent cases per GPU)",
                    "l2": "inputs larger than L2 (state %.2f GB per buffer)" % (cells * 32 / 1e9)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

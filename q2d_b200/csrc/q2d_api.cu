@@ -664,9 +664,10 @@ int ready(q2d_ctx* ctx) {
 struct Schedule { int kernel, tile, march_h; };
 // Candidate schedules, indexed like the autotuner's result: CTA-tile stage kernel on tiles
 // 32x10, 32x8, 64x4; warp-marching kernel with 8 or 16 rows per item; FP32-flux tile kernel
-// on tiles 32x10, 32x8, 64x4 (FP32-flux form only).
+// on tiles 32x10, 32x8, 64x4 with registers for 4 CTAs per SM, and 32x10 with registers for 3
+// (FP32-flux form only).
 const Schedule kSchedules[] = {{0, 0, 16}, {0, 1, 16}, {0, 2, 16}, {1, 0, 8}, {1, 0, 16},
-                               {2, 0, 16}, {2, 1, 16}, {2, 2, 16}};
+                               {2, 0, 16}, {2, 1, 16}, {2, 2, 16}, {2, 3, 16}};
 constexpr int kNumSchedules = (int)(sizeof(kSchedules) / sizeof(kSchedules[0]));
 
 bool schedule_allowed(const q2d_ctx* ctx, int k) {

@@ -5,11 +5,12 @@
 // follows the form's definition: MUSCL reconstruction, limiters and the interior Riemann fluxes
 // run in FP32 and the face fluxes are kept in FP32; the residual accumulation (flux
 // differences), sources, RK stage combination, positivity checks, the new state and the
-// residual norms are FP64. Boundary-face fluxes (Lib_BC_Fluxes_*.f90) are computed in FP64 from
-// the FP64 state and stored like the interior ones.
+// residual norms are FP64. Wall (symmetry) and extrapolation boundary fluxes are FP32 like the
+// interior ones; inflow and outflow records (Lib_BC_Fluxes_Inflow/Outflow.f90) are evaluated in
+// FP64 from the FP64 state.
 //
 // Per tile there are two CTA barriers:
-//   1. loads: the FP64 cell data of the tile (state, U^n, sur, dt, source geometry) by cp.async;
+//   1. loads: the FP64 cell data of the tile (U^n, sur, dt, source geometry) by cp.async;
 //      the stencil state of the tile and its cross-shaped 2-cell halo converted to FP32, with
 //      every ghost cell (Fill_Ghost_Cell, Lib_Ghost.f90:16-299) evaluated from HBM by the thread
 //      that stores it; mean cell lengths and face geometry converted to FP32;
@@ -31,8 +32,8 @@ struct Tile32 {
     static constexpr int W = TX + 4, H = TY + 4, AREA = W * H;
     static constexpr int NFI = (TX + 1) * TY, NFJ = TX * (TY + 1), NF = NFI + NFJ;
     static constexpr int NC = TX * TY;
-    // FP64 cell planes: 0-3 state, 4-7 state at the start of the step, 8 sur, 9 dt, 10-11 source
-    static constexpr int NCD = 12;
+    // FP64 cell planes: 0-3 state at the start of the step, 4 sur, 5 dt, 6-7 source geometry
+    static constexpr int NCD = 8;
     static constexpr int oP = 2 * NCD * NC;   // FP32 offsets from here on
     static constexpr int oD = oP + 4 * AREA;  // [2][AREA] mean cell lengths
     static constexpr int oG = oD + 2 * AREA;  // [3][NF] face nx, ny, length (i faces, then j faces)
@@ -223,8 +224,66 @@ __device__ __forceinline__ bool face32_lim(int lim, const float* sP, const float
     }
 }
 
-template <int RIEM, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, 3) stage32_kernel(const StageArgs a) {
+// Boundary faces of the FP32-flux form in FP32 (the FP64 restatements are in q2d_common.cuh).
+// BC_Symmetry_Eul (Lib_BC_Fluxes_Symmetry.f90:28-124): mirrored ghost, limited slope of the
+// boundary cell, Riemann problem between the face state and its mirror; momentum flux only.
+template <int RIEM, int LIM>
+__device__ __forceinline__ void bc_symmetry32(int Fm, const float* B, const float* I, float dlb, float dli,
+                                              float nx, float ny, float len, float gam, float gm1, float gf,
+                                              float* out) {
+    const bool minside = (Fm & 1) != 0;   // faces 1 and 3
+    const float bd = 0.5f * dlb, id = 0.5f * dli;
+    const float un = B[1] * nx + B[2] * ny;
+    const float G[4] = {B[0], B[1] - 2.0f * un * nx, B[2] - 2.0f * un * ny, B[3]};
+    const float i12 = rcp_approx(minside ? 2.0f * bd : bd + id);
+    const float i23 = rcp_approx(minside ? bd + id : 2.0f * bd);
+    const float dist = minside ? -bd : bd;
+    float Fc[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const float P1 = minside ? G[v] : I[v], P3 = minside ? I[v] : G[v];
+        Fc[v] = B[v] + lim32<LIM>((P3 - B[v]) * i23, (B[v] - P1) * i12) * dist;
+    }
+    const float Un = Fc[1] * nx + Fc[2] * ny;
+    const float vtx = Fc[1] - Un * nx, vty = Fc[2] - Un * ny;
+    const float Un1 = minside ? -Un : Un;
+    const FS32 L = phys32(Fc[0], Un1 * nx + vtx, Un1 * ny + vty, Fc[3], nx, ny, gf);
+    const FS32 R = phys32(Fc[0], -Un1 * nx + vtx, -Un1 * ny + vty, Fc[3], nx, ny, gf);
+    float F[4];
+    riemann_f32<RIEM>(L, R, nx, ny, gam, gm1, gf, F);
+    out[0] = 0.0f;
+    out[1] = F[1] * len;
+    out[2] = F[2] * len;
+    out[3] = 0.0f;
+}
+
+// BC_Extrapolation (Lib_BC_Fluxes_Extrapolation.f90:18-49): exact flux of the boundary cell.
+__device__ __forceinline__ void bc_extrapolation32(const float* B, float nx, float ny, float len, float gf,
+                                                   float* out) {
+    const float m = B[0] * (B[1] * nx + B[2] * ny) * len;
+    out[0] = m;
+    out[1] = m * B[1] + B[3] * len * nx;
+    out[2] = m * B[2] + B[3] * len * ny;
+    out[3] = m * (gf * B[3] * rcp_approx(B[0]) + 0.5f * (B[1] * B[1] + B[2] * B[2]));
+}
+
+template <int RIEM>
+__device__ __forceinline__ void bc_symmetry32_lim(int lim, int Fm, const float* B, const float* I, float dlb,
+                                                  float dli, float nx, float ny, float len, float gam,
+                                                  float gm1, float gf, float* out) {
+    switch (lim) {
+        case 0: bc_symmetry32<RIEM, 0>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
+        case 1: bc_symmetry32<RIEM, 1>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
+        case 2: bc_symmetry32<RIEM, 2>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
+        case 3: bc_symmetry32<RIEM, 3>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
+        case 4: bc_symmetry32<RIEM, 4>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
+        case 5: bc_symmetry32<RIEM, 5>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
+        default: bc_symmetry32<RIEM, 6>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
+    }
+}
+
+template <int RIEM, int TX, int TY, int NT, int MB>
+__global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
     using L = Tile32<TX, TY>;
     constexpr int W = L::W, AREA = L::AREA, NFI = L::NFI, NF = L::NF, NC = L::NC;
     extern __shared__ double smem[];
@@ -252,70 +311,91 @@ __global__ void __launch_bounds__(NT, 3) stage32_kernel(const StageArgs a) {
         const double* scb = a.sc + 2 * B.oc;
 
         // ---- 1. loads ------------------------------------------------------------------------
-        for (int k = tid; k < NC; k += NT) {
+        for (int k = tid; k < NC; k += NT) {   // FP64 cell data, asynchronous
             const int row = k / TX, col = k - row * TX;
             const int ii = i0 + col, jj = j0 + row;
             if (ii >= ni || jj >= nj) continue;
             const long long cg = (long long)jj * ni + ii;
-            cp_async8(sC + 8 * NC + k, scb + cg);                                 // sur
-            if (!a.time_accurate) cp_async8(sC + 9 * NC + k, scb + pc + cg);      // dt
             if (!a.first) {
 #pragma unroll
-                for (int v = 0; v < 4; ++v) cp_async8(sC + (4 + v) * NC + k, a.PO + B.oc + v * pc + cg);
+                for (int v = 0; v < 4; ++v) cp_async8(sC + v * NC + k, a.PO + B.oc + v * pc + cg);
             }
+            cp_async8(sC + 4 * NC + k, scb + cg);                                 // sur
+            if (!a.time_accurate) cp_async8(sC + 5 * NC + k, scb + pc + cg);      // dt
             if (a.source) {
-                cp_async8(sC + 10 * NC + k, scb + 6 * pc + cg);
-                if (a.source == 2) cp_async8(sC + 11 * NC + k, scb + 7 * pc + cg);
+                cp_async8(sC + 6 * NC + k, scb + 6 * pc + cg);
+                if (a.source == 2) cp_async8(sC + 7 * NC + k, scb + 7 * pc + cg);
             }
         }
-        for (int f = tid; f < NF; f += NT) {
-            const double* src;
-            long long ps;
+        // face geometry and the state / lengths of the cross-shaped halo: branch-free address
+        // selection so that every load of a thread is in flight before the first use
+#pragma unroll
+        for (int u = 0; u < (NF + NT - 1) / NT; ++u) {
+            const int f = tid + u * NT;
+            bool ok;
+            long long off, ps;
+            const double* base;
             if (f < NFI) {
                 const int row = f / (TX + 1), col = f - row * (TX + 1);
                 const int jj = j0 + row, F = i0 + col;
-                if (jj >= nj || F > ni) continue;
-                src = a.fi + B.ofi + (long long)jj * (ni + 1) + F;
+                ok = jj < nj && F <= ni;
+                off = (long long)jj * (ni + 1) + F;
+                base = a.fi + B.ofi;
                 ps = B.pfi;
             } else {
                 const int ff = f - NFI;
                 const int row = ff / TX, col = ff - row * TX;
                 const int ii = i0 + col, G = j0 + row;
-                if (ii >= ni || G > nj) continue;
-                src = a.fj + B.ofj + (long long)G * ni + ii;
+                ok = f < NF && ii < ni && G <= nj;
+                off = (long long)G * ni + ii;
+                base = a.fj + B.ofj;
                 ps = B.pfj;
             }
-            sG[f] = (float)__ldg(src);
-            sG[NF + f] = (float)__ldg(src + ps);
-            sG[2 * NF + f] = (float)__ldg(src + 2 * ps);
+            const double* src = base + (ok ? off : 0);
+            const double x = __ldg(src), y = __ldg(src + ps), z = __ldg(src + 2 * ps);
+            if (ok) {
+                sG[f] = (float)x;
+                sG[NF + f] = (float)y;
+                sG[2 * NF + f] = (float)z;
+            }
         }
-        for (int idx = tid; idx < AREA; idx += NT) {
+        bool edge = false;
+#pragma unroll
+        for (int u = 0; u < (AREA + NT - 1) / NT; ++u) {
+            const int idx = tid + u * NT;
             const int r = idx / W, c = idx - r * W;
-            if ((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2)) continue;
             const int ii = i0 - 2 + c, jj = j0 - 2 + r;
-            if (ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1) {
-                const double* src = a.dl + B.og + (long long)(jj + 2) * (ni + 4) + (ii + 2);
-                sD[idx] = (float)__ldg(src);
-                sD[AREA + idx] = (float)__ldg(src + B.pg);
+            const bool cross = idx < AREA && !((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2));
+            const bool inI = ii >= 0 && ii < ni, inJ = jj >= 0 && jj < nj;
+            const bool inner = cross && inI && inJ;
+            const bool indl = cross && ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1;
+            edge = edge || (cross && inI != inJ);
+            const double* src = Pin + (inner ? (long long)jj * ni + ii : 0);
+            const double* dsrc = a.dl + B.og + (indl ? (long long)(jj + 2) * (ni + 4) + (ii + 2) : 0);
+            const double q0 = __ldg(src), q1 = __ldg(src + pc), q2 = __ldg(src + 2 * pc), q3 = __ldg(src + 3 * pc);
+            const double d0 = __ldg(dsrc), d1 = __ldg(dsrc + B.pg);
+            if (indl) {
+                sD[idx] = (float)d0;
+                sD[AREA + idx] = (float)d1;
             }
-            const bool inI = (ii >= 0 && ii < ni), inJ = (jj >= 0 && jj < nj);
-            double q[4];
-            if (inI && inJ) {
-                const double* src = Pin + (long long)jj * ni + ii;
-#pragma unroll
-                for (int v = 0; v < 4; ++v) q[v] = __ldg(src + v * pc);
-                if (r >= 2 && r < TY + 2 && c >= 2 && c < TX + 2) {
-                    const int kk = (r - 2) * TX + (c - 2);
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) sC[v * NC + kk] = q[v];
-                }
-            } else if (inI != inJ) {   // ghost cell (Fill_Ghost_Cell) from HBM
-                if (!ghost_value(a, B, ii, jj, q)) continue;
-            } else {
-                continue;
+            if (inner) {
+                sP[idx] = (float)q0;
+                sP[AREA + idx] = (float)q1;
+                sP[2 * AREA + idx] = (float)q2;
+                sP[3 * AREA + idx] = (float)q3;
             }
+        }
+        if (__syncthreads_or(edge)) {   // ghost cells (Fill_Ghost_Cell), only next to block edges
+            for (int idx = tid; idx < AREA; idx += NT) {
+                const int r = idx / W, c = idx - r * W;
+                if ((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2)) continue;
+                const int ii = i0 - 2 + c, jj = j0 - 2 + r;
+                const bool inI = ii >= 0 && ii < ni, inJ = jj >= 0 && jj < nj;
+                double q[4];
+                if (inI == inJ || !ghost_value(a, B, ii, jj, q)) continue;
 #pragma unroll
-            for (int v = 0; v < 4; ++v) sP[v * AREA + idx] = (float)q[v];
+                for (int v = 0; v < 4; ++v) sP[v * AREA + idx] = (float)q[v];
+            }
         }
         cp_async_wait_all();
         __syncthreads();
@@ -330,13 +410,14 @@ __global__ void __launch_bounds__(NT, 3) stage32_kernel(const StageArgs a) {
             case 5: interior_faces32<RIEM, 5, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
             default: interior_faces32<RIEM, 6, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
         }
-        {   // boundary faces (BC_Fluxes, Mod_BC_Fluxes.f90:79-269), FP64 from the FP64 state
+        {   // boundary faces (BC_Fluxes, Mod_BC_Fluxes.f90:79-269), on the threads with the fewest
+            // interior faces (the highest thread indices)
             const int nrow = min(TY, nj - j0), ncol = min(TX, ni - i0);
             const int nl = (i0 == 0) ? nrow : 0;
             const int nr = (i0 + TX >= ni) ? nrow : 0;
             const int nb = (j0 == 0) ? ncol : 0;
             const int nt = (j0 + TY >= nj) ? ncol : 0;
-            for (int t = tid; t < nl + nr + nb + nt; t += NT) {
+            for (int t = NT - 1 - tid; t < nl + nr + nb + nt; t += NT) {
                 int Fm, k, bi, bj, di, dj, f;
                 if (t < nl) {
                     Fm = 1; k = j0 + t; bi = 0; bj = k; di = 1; dj = 0; f = t * (TX + 1);
@@ -351,48 +432,53 @@ __global__ void __launch_bounds__(NT, 3) stage32_kernel(const StageArgs a) {
                     Fm = 4; k = i0 + u; bi = k; bj = nj - 1; di = 0; dj = -1; f = NFI + (nj - j0) * TX + u;
                 }
                 const EdgeRec e = a.edges[B.eo[Fm - 1] + k];
-                double X[4] = {0.0, 0.0, 0.0, 0.0};
+                const int cb = (bj - j0 + 2) * W + (bi - i0 + 2);     // boundary cell
+                const int ci = cb + dj * W + di;                       // its inward neighbour
+                const float* dlp = Fm <= 2 ? sD : sD + AREA;
+                const float nx = sG[f], ny = sG[NF + f], ln = sG[2 * NF + f];
+                float X[4] = {0.0f, 0.0f, 0.0f, 0.0f};
                 if (e.type == 101) {   // BC_Connection_Eul: the interior scheme on the ghost stencil
-                    const int cb = (bj - j0 + 2) * W + (bi - i0 + 2);
-                    int base, step;
-                    const float* dlp;
-                    if (Fm <= 2) { step = 1; dlp = sD; base = Fm == 1 ? cb - 2 : cb - 1; }
-                    else { step = W; dlp = sD + AREA; base = Fm == 3 ? cb - 2 * W : cb - W; }
-                    float out[4];
-                    const bool ok = face32_lim<RIEM, AREA>(a.limiter, sP, dlp, base, step, sG[f], sG[NF + f],
-                                                           sG[2 * NF + f], gam, gm1, gf, out);
+                    const int step = Fm <= 2 ? 1 : W;
+                    const int base = (Fm == 1 || Fm == 3) ? cb - 2 * step : cb - step;
+                    const bool ok = face32_lim<RIEM, AREA>(a.limiter, sP, dlp, base, step, nx, ny, ln, gam, gm1,
+                                                           gf, X);
                     if (!ok) record_error(cs, 4, B.local_b, bi + 1, bj + 1, a.irk);
+                } else if (e.type == 300 || e.type == 400) {
+                    float Bq[4], Iq[4];
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) X[v] = (double)out[v];
-                } else if (e.type >= 0) {
+                    for (int v = 0; v < 4; ++v) { Bq[v] = sP[v * AREA + cb]; Iq[v] = sP[v * AREA + ci]; }
+                    if (e.type == 300)
+                        bc_symmetry32_lim<RIEM>(a.limiter, Fm, Bq, Iq, dlp[cb], dlp[ci], nx, ny, ln, gam, gm1, gf, X);
+                    else
+                        bc_extrapolation32(Bq, nx, ny, ln, gf, X);
+                } else if (e.type > 0) {   // inflow / outflow records: FP64 from the FP64 state
                     const double* pb = Pin + (long long)bj * ni + bi;
-                    const int ni2 = bi + di, nj2 = bj + dj;   // inward neighbour
+                    const int ni2 = bi + di, nj2 = bj + dj;
                     Q4 Bp, Ip;
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) Bp.v[v] = __ldg(pb + v * pc);
                     if (ni2 >= 0 && ni2 < ni && nj2 >= 0 && nj2 < nj) {
                         const double* pi = Pin + (long long)nj2 * ni + ni2;
 #pragma unroll
                         for (int v = 0; v < 4; ++v) Ip.v[v] = __ldg(pi + v * pc);
                     } else {   // one-cell-thick block: the neighbour is the opposite ghost
-                        const int sidx = (nj2 - j0 + 2) * W + (ni2 - i0 + 2);
 #pragma unroll
-                        for (int v = 0; v < 4; ++v) Ip.v[v] = (double)sP[v * AREA + sidx];
+                        for (int v = 0; v < 4; ++v) Ip.v[v] = (double)sP[v * AREA + ci];
                     }
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) Bp.v[v] = __ldg(pb + v * pc);
                     const double* dlb = a.dl + B.og + (long long)(Fm <= 2 ? 0 : 1) * B.pg;
                     const double dlbv = __ldg(dlb + (long long)(bj + 2) * (ni + 4) + (bi + 2));
                     const double dli = __ldg(dlb + (long long)(nj2 + 2) * (ni + 4) + (ni2 + 2));
                     const double* gsrc = Fm <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (Fm == 1 ? 0 : ni)
                                                  : a.fj + B.ofj + (long long)(Fm == 3 ? 0 : nj) * ni + bi;
                     const long long gs = Fm <= 2 ? B.pfi : B.pfj;
-                    const double nx = __ldg(gsrc), ny = __ldg(gsrc + gs), ln = __ldg(gsrc + 2 * gs);
-                    const Q4 q = bc_face<RIEM>(a.gas, a.limiter, e.type, Fm, Bp, Ip, dlbv, dli, nx, ny, ln,
+                    const Q4 q = bc_face<RIEM>(a.gas, a.limiter, e.type, Fm, Bp, Ip, dlbv, dli, __ldg(gsrc),
+                                               __ldg(gsrc + gs), __ldg(gsrc + 2 * gs),
                                                e.param >= 0 ? a.bcp + e.param : nullptr);
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) X[v] = q.v[v];
+                    for (int v = 0; v < 4; ++v) X[v] = (float)q.v[v];
                 }
 #pragma unroll
-                for (int v = 0; v < 4; ++v) sF[v * NF + f] = (float)X[v];
+                for (int v = 0; v < 4; ++v) sF[v * NF + f] = X[v];
             }
         }
         __syncthreads();
@@ -406,6 +492,10 @@ __global__ void __launch_bounds__(NT, 3) stage32_kernel(const StageArgs a) {
             const int row = k / TX, col = k - row * TX;
             const int ii = i0 + col, jj = j0 + row;
             if (ii >= ni || jj >= nj) continue;
+            const long long cg = (long long)jj * ni + ii;
+            double P[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) P[v] = __ldg(Pin + v * pc + cg);
             const int i1 = ii + 1, j1 = jj + 1;
             const int fi0 = row * (TX + 1) + col, fj0 = NFI + row * TX + col;
             double r[4];
@@ -423,27 +513,23 @@ __global__ void __launch_bounds__(NT, 3) stage32_kernel(const StageArgs a) {
                 if (j1 == nj) x = x + (double)Fv[fj0 + TX];
                 r[v] = x;
             }
-            const long long cg = (long long)jj * ni + ii;
-            const double sur = sC[8 * NC + k];
-            double P[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) P[v] = sC[v * NC + k];
+            const double sur = sC[4 * NC + k];
             if (a.source) {
                 // S = [rho, rho u, rho v, rho E0 + p] * f0 with f0 = -v/r (Lib_Source_Axisymmetry.f90:
                 // 65-76) or V.G (Lib_Source_Areavariation.f90:120-142); Res -= S * sur
                 const double rE0 = P[3] * g.igm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
-                const double f0 = a.source == 1 ? -P[2] * sC[10 * NC + k]
-                                                : P[1] * sC[10 * NC + k] + P[2] * sC[11 * NC + k];
+                const double f0 = a.source == 1 ? -P[2] * sC[6 * NC + k]
+                                                : P[1] * sC[6 * NC + k] + P[2] * sC[7 * NC + k];
                 const double fs = f0 * sur;
                 r[0] = r[0] - P[0] * fs;
                 r[1] = r[1] - P[0] * P[1] * fs;
                 r[2] = r[2] - P[0] * P[2] * fs;
                 r[3] = r[3] - (rE0 + P[3]) * fs;
             }
-            const double dt = a.time_accurate ? dt_case : sC[9 * NC + k];
+            const double dt = a.time_accurate ? dt_case : sC[5 * NC + k];
             double PO[4];
 #pragma unroll
-            for (int v = 0; v < 4; ++v) PO[v] = a.first ? P[v] : sC[(4 + v) * NC + k];
+            for (int v = 0; v < 4; ++v) PO[v] = a.first ? P[v] : sC[v * NC + k];
             const double fr = -dt * rcp64(sur);
             double U0[4], U[4];
             U0[0] = PO[0]; U0[1] = PO[0] * PO[1]; U0[2] = PO[0] * PO[2];
@@ -499,10 +585,10 @@ __global__ void __launch_bounds__(NT, 3) stage32_kernel(const StageArgs a) {
     }
 }
 
-template <int RIEM, int TX, int TY, int NT>
+template <int RIEM, int TX, int TY, int NT, int MB>
 cudaError_t launch_stage32_t(const StageArgs& a, int grid, cudaStream_t s) {
     constexpr size_t smem = Tile32<TX, TY>::bytes;
-    auto k = stage32_kernel<RIEM, TX, TY, NT>;
+    auto k = stage32_kernel<RIEM, TX, TY, NT, MB>;
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -513,10 +599,10 @@ cudaError_t launch_stage32_t(const StageArgs& a, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template <int RIEM, int TX, int TY, int NT>
+template <int RIEM, int TX, int TY, int NT, int MB>
 int stage32_occupancy_t() {
     constexpr size_t smem = Tile32<TX, TY>::bytes;
-    auto k = stage32_kernel<RIEM, TX, TY, NT>;
+    auto k = stage32_kernel<RIEM, TX, TY, NT, MB>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, NT, smem);

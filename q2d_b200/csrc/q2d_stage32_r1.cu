@@ -1,21 +1,24 @@
-// Instantiations of the FP32-flux stage kernel for Riemann solver 1 (see q2d_stage32.cuh).
+// Instantiations of the FP32-flux stage kernel (tile 0-2: 32x10, 32x8, 64x4 at 4 CTAs per SM;
+// tile 3: 32x10 at 3 CTAs per SM) for Riemann solver 1 (see q2d_stage32.cuh).
 #include "q2d_stage32.cuh"
 
 namespace q2d {
 
 cudaError_t launch_stage32_r1(const StageArgs& a, int tile, int grid, cudaStream_t s) {
     switch (tile) {
-        case 1: return launch_stage32_t<1, 32, 8, 256>(a, grid, s);
-        case 2: return launch_stage32_t<1, 64, 4, 256>(a, grid, s);
-        default: return launch_stage32_t<1, 32, 10, 256>(a, grid, s);
+        case 1: return launch_stage32_t<1, 32, 8, 256, 4>(a, grid, s);
+        case 2: return launch_stage32_t<1, 64, 4, 256, 4>(a, grid, s);
+        case 3: return launch_stage32_t<1, 32, 10, 256, 3>(a, grid, s);
+        default: return launch_stage32_t<1, 32, 10, 256, 4>(a, grid, s);
     }
 }
 
 int stage32_occupancy_r1(int tile) {
     switch (tile) {
-        case 1: return stage32_occupancy_t<1, 32, 8, 256>();
-        case 2: return stage32_occupancy_t<1, 64, 4, 256>();
-        default: return stage32_occupancy_t<1, 32, 10, 256>();
+        case 1: return stage32_occupancy_t<1, 32, 8, 256, 4>();
+        case 2: return stage32_occupancy_t<1, 64, 4, 256, 4>();
+        case 3: return stage32_occupancy_t<1, 32, 10, 256, 3>();
+        default: return stage32_occupancy_t<1, 32, 10, 256, 4>();
     }
 }
 

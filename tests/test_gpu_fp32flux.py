@@ -104,13 +104,16 @@ def test_conservation_closed_domain(precision):
 
 
 def test_fp32flux_state_independent_of_tile():
-    """Every face flux and cell update reads the same inputs whatever the tile shape; the
-    kernels of different tile shapes may still fuse FP64 multiply-adds differently, so states
-    agree to FP64 rounding (1e-13 relative), not necessarily bit for bit."""
+    """Every face flux and cell update reads the same inputs whatever the tile shape, so the
+    32x10 and 32x8 schedules (and 32x10 at 3 or 4 CTAs per SM) give the same state bit for
+    bit. The compiler may fuse FP32 multiply-adds differently in other instantiations (64x4),
+    so that one agrees within the form's accuracy bound only."""
     batch = cases.area_nozzle_batch(n=5, seed=17, nx_range=(40, 150), ny_range=(8, 20))
     ref, _ = run(batch, 30, schedule=SCHED[0], precision=1)
-    for sch in SCHED[1:3]:
+    for sch in (SCHED[1], "fp32-flux tile 32x10 (3 CTAs/SM)"):
         got, _ = run(batch, 30, schedule=sch, precision=1)
         for ca, cb in zip(got, ref):
             for xa, xb in zip(ca, cb):
-                assert rel_linf(xa, xb).max() <= 1e-13, sch
+                assert np.array_equal(xa, xb), sch
+    got, _ = run(batch, 30, schedule=SCHED[2], precision=1)
+    compare(got, ref, SCHED[2])
