@@ -230,7 +230,8 @@ long long q2d_gpu_num_cells(const q2d_ctx* ctx);
 /* ---- serving: continuous batching of independent cases (no reference counterpart) --------
  * The reference runs one domain per process from input files (main.f90:20-50). A serving
  * context holds up to max_cases independent cases in device pools sized from device_bytes
- * (state, metrics and face geometry: about 240 bytes per interior cell; the work lists and
+ * (state, metrics and face geometry: about 240 bytes per interior cell, 306 in the FP32-flux
+ * form, which keeps FP32 copies of the geometry; the work lists and
  * per-case records are extra), all advanced together by q2d_gpu_step / step_async / wait, each
  * with its own time step, iteration count, residual, TODO state and error status.
  *

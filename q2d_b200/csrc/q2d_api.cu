@@ -34,6 +34,7 @@ namespace {
 // block's regions when the case is uploaded.
 struct Staged {
     std::vector<double> pa, sc, dl, fi, fj;
+    std::vector<float> dl32, fi4, fj4;   // FP32 geometry of the FP32-flux form
 };
 
 struct HBlock {
@@ -148,6 +149,7 @@ struct q2d_ctx {
     int grid = 0;
     // device pools and their allocators
     DevBuf<double> PA, PB, PC, SC, DL, FI, FJ, PART;
+    DevBuf<float> DL32, FI4, FJ4;   // FP32 geometry (FP32-flux form only): same regions as DL/FI/FJ
     Arena ac, ag, afi, afj;
     DevBuf<DBlock> dblocks;
     DevBuf<DCase> dcases;
@@ -191,7 +193,9 @@ StageArgs base_args(q2d_ctx* ctx) {
     a.n_items = ctx->n_items;
     a.sc = ctx->SC.p;
     a.dl = ctx->DL.p;
-    a.dl32 = nullptr;
+    a.dl32 = ctx->DL32.p;
+    a.fi4 = reinterpret_cast<const float4*>(ctx->FI4.p);
+    a.fj4 = reinterpret_cast<const float4*>(ctx->FJ4.p);
     a.fi = ctx->FI.p;
     a.fj = ctx->FJ.p;
     a.edges = ctx->edges.p;
@@ -492,6 +496,15 @@ int prepare_case(q2d_ctx* ctx, int c) {
         for (long long k = 0; k < (long long)b.ni * (b.nj + 1); ++k)
             for (int q = 0; q < 3; ++q) S.fj[q * d.pfj + k] = G.fj[3 * k + q];
         for (int v = 0; v < 4; ++v) std::memcpy(&S.pa[v * d.pc], &b.prim[(size_t)v * n], sizeof(double) * n);
+        if (ctx->opt.precision == Q2D_PREC_FP32_FLUX) {
+            S.dl32.assign(S.dl.begin(), S.dl.end());
+            S.fi4.assign(4 * (size_t)d.pfi, 0.0f);
+            S.fj4.assign(4 * (size_t)d.pfj, 0.0f);
+            for (long long k = 0; k < (long long)(b.ni + 1) * b.nj; ++k)
+                for (int q = 0; q < 3; ++q) S.fi4[4 * k + q] = (float)G.fi[3 * k + q];
+            for (long long k = 0; k < (long long)b.ni * (b.nj + 1); ++k)
+                for (int q = 0; q < 3; ++q) S.fj4[4 * k + q] = (float)G.fj[3 * k + q];
+        }
         b.prim.clear();
         b.prim.shrink_to_fit();
         geo[lb] = HostGeom{};
@@ -513,6 +526,11 @@ int upload_case(q2d_ctx* ctx, int c) {
         CK(cudaMemcpy(ctx->DL.p + d.og, S.dl.data(), sizeof(double) * S.dl.size(), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(ctx->FI.p + d.ofi, S.fi.data(), sizeof(double) * S.fi.size(), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(ctx->FJ.p + d.ofj, S.fj.data(), sizeof(double) * S.fj.size(), cudaMemcpyHostToDevice));
+        if (ctx->DL32.p) {   // face offsets are multiples of 32, so float index 2*off is 16-byte aligned
+            CK(cudaMemcpy(ctx->DL32.p + d.og, S.dl32.data(), sizeof(float) * S.dl32.size(), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ctx->FI4.p + 2 * d.ofi, S.fi4.data(), sizeof(float) * S.fi4.size(), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ctx->FJ4.p + 2 * d.ofj, S.fj4.data(), sizeof(float) * S.fj4.size(), cudaMemcpyHostToDevice));
+        }
         S = Staged{};
     }
     const CaseState s = fresh_state(cs.time0);
@@ -615,6 +633,9 @@ int apply_pending(q2d_ctx* ctx) {
 int allocate_pools(q2d_ctx* ctx, long long ec, long long eg, long long efi, long long efj, int ncases) {
     CK(ctx->PA.alloc(ec)); CK(ctx->PB.alloc(ec)); CK(ctx->PC.alloc(ec));
     CK(ctx->SC.alloc(2 * ec)); CK(ctx->DL.alloc(eg)); CK(ctx->FI.alloc(efi)); CK(ctx->FJ.alloc(efj));
+    if (ctx->opt.precision == Q2D_PREC_FP32_FLUX) {
+        CK(ctx->DL32.alloc(eg)); CK(ctx->FI4.alloc(2 * efi)); CK(ctx->FJ4.alloc(2 * efj));
+    }
     CK(cudaMemset(ctx->PB.p, 0, sizeof(double) * (ec ? ec : 1)));
     CK(cudaMemset(ctx->PC.p, 0, sizeof(double) * (ec ? ec : 1)));
     ctx->ac.init(ec); ctx->ag.init(eg); ctx->afi.init(efi); ctx->afj.init(efj);
@@ -1046,8 +1067,10 @@ int q2d_serve_create(q2d_ctx** out, const q2d_options* opt, unsigned long long d
     ctx->cases.resize(max_cases);
     // Bytes per interior cell: states 3 x 4 planes + scalars 8 planes (160 B), ghost frame
     // 2 planes with up to 50 % halo (24 B), i- and j-faces 3 planes each with up to 15 %
-    // extra faces (55 B).
-    const long long cells = (long long)((double)device_bytes / 239.2);
+    // extra faces (55 B); the FP32-flux form adds FP32 copies of the ghost-frame and face
+    // geometry (12 B + 55 B).
+    const double per_cell = opt->precision == Q2D_PREC_FP32_FLUX ? 306.4 : 239.2;
+    const long long cells = (long long)((double)device_bytes / per_cell);
     const long long ec = 4 * cells, eg = 3 * cells + 4096, efi = (long long)(3.45 * (double)cells) + 4096,
                     efj = efi;
     int e = allocate_pools(ctx, ec, eg, efi, efj, max_cases);
@@ -1154,6 +1177,7 @@ void q2d_gpu_destroy(q2d_ctx* ctx) {
     drop_graphs(ctx);
     ctx->PA.release(); ctx->PB.release(); ctx->PC.release(); ctx->SC.release(); ctx->DL.release();
     ctx->FI.release(); ctx->FJ.release(); ctx->PART.release(); ctx->dblocks.release();
+    ctx->DL32.release(); ctx->FI4.release(); ctx->FJ4.release();
     ctx->dcases.release(); ctx->cstate.release(); ctx->items.release(); ctx->edges.release();
     ctx->bcp.release(); ctx->flag.release();
     if (ctx->h_state) cudaFreeHost(ctx->h_state);

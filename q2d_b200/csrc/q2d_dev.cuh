@@ -97,9 +97,11 @@ struct StageArgs {
     double* Pout;
     double* sc;            // scalar pool
     const double* dl;
-    const float* dl32;
+    const float* dl32;     // FP32 copy of the dl pool (FP32-flux form)
     const double* fi;
     const double* fj;
+    const float4* fi4;     // FP32 copies of the face pools as (nx, ny, len, 0); a block's faces
+    const float4* fj4;     // start at float4 index ofi / 2 (ofj / 2)
     const EdgeRec* edges;
     const BCParam* bcp;
     double* part;          // per-item partials: 4 residual sums + dt min

@@ -26,7 +26,9 @@
 
 namespace q2d {
 
-// Shared-memory layout of one tile: FP64 cell planes first, then FP32 arrays.
+// Shared-memory layout of one tile (byte offsets): FP64 cell planes, then FP32 records of 16
+// bytes (one shared-memory access per cell state, face geometry or face flux) and the mean
+// cell lengths of both directions as pairs.
 template <int TX, int TY>
 struct Tile32 {
     static constexpr int W = TX + 4, H = TY + 4, AREA = W * H;
@@ -34,13 +36,16 @@ struct Tile32 {
     static constexpr int NC = TX * TY;
     // FP64 cell planes: 0-3 state at the start of the step, 4 sur, 5 dt, 6-7 source geometry
     static constexpr int NCD = 8;
-    static constexpr int oP = 2 * NCD * NC;   // FP32 offsets from here on
-    static constexpr int oD = oP + 4 * AREA;  // [2][AREA] mean cell lengths
-    static constexpr int oG = oD + 2 * AREA;  // [3][NF] face nx, ny, length (i faces, then j faces)
-    static constexpr int oF = oG + 3 * NF;    // [4][NF] face fluxes (times length)
-    static constexpr int nfloats = oF + 4 * NF;
-    static constexpr size_t bytes = sizeof(float) * (size_t)nfloats;
+    static constexpr size_t bP = sizeof(double) * NCD * NC;   // float4 [AREA]  rho, u, v, p
+    static constexpr size_t bG = bP + 16 * (size_t)AREA;      // float4 [NF]    nx, ny, length, -
+    static constexpr size_t bF = bG + 16 * (size_t)NF;        // float4 [NF]    flux times length
+    static constexpr size_t bD = bF + 16 * (size_t)NF;        // float2 [AREA]  dl(1), dl(2)
+    static constexpr size_t bytes = bD + 8 * (size_t)AREA;
 };
+
+__device__ __forceinline__ float comp(const float4& q, int v) {
+    return v == 0 ? q.x : (v == 1 ? q.y : (v == 2 ? q.z : q.w));
+}
 
 __device__ __forceinline__ float rcp_approx(float x) {
     float y;
@@ -147,20 +152,22 @@ __device__ __forceinline__ void riemann_f32(const FS32& L, const FS32& R, float 
     F[0] = R.Fr; F[1] = R.Fu; F[2] = R.Fv; F[3] = R.Fe;
 }
 
-// One interior face: stencil cells m (= L-1), L, R, p (= R+1) at shared offsets base + k*step.
-template <int RIEM, int LIM, int AREA>
-__device__ __forceinline__ bool face32(const float* sP, const float* dlp, int base, int step, float nx,
+// One interior face: stencil cells m (= L-1), L, R, p (= R+1) at shared positions base + k*step;
+// dlp is the cell-length pair array viewed as floats, offset to the face's direction.
+template <int RIEM, int LIM>
+__device__ __forceinline__ bool face32(const float4* sP, const float* dlp, int base, int step, float nx,
                                       float ny, float len, float gam, float gm1, float gf, float* out) {
-    const float dm = dlp[base], d0 = dlp[base + step], d1 = dlp[base + 2 * step], d2 = dlp[base + 3 * step];
+    const float dm = dlp[2 * base], d0 = dlp[2 * (base + step)], d1 = dlp[2 * (base + 2 * step)],
+                d2 = dlp[2 * (base + 3 * step)];
     const float il0 = rcp_approx(0.5f * (dm + d0));
     const float il1 = rcp_approx(0.5f * (d0 + d1));
     const float il2 = rcp_approx(0.5f * (d1 + d2));
     const float lm = 0.5f * d0, lp = 0.5f * d1;
     float QL[4], QR[4];
+    const float4 Cm = sP[base], C0 = sP[base + step], C1 = sP[base + 2 * step], C2 = sP[base + 3 * step];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        const float* q = sP + v * AREA + base;
-        const float qm = q[0], q0 = q[step], q1 = q[2 * step], q2 = q[3 * step];
+        const float qm = comp(Cm, v), q0 = comp(C0, v), q1 = comp(C1, v), q2 = comp(C2, v);
         const float s0 = (q0 - qm) * il0, s1 = (q1 - q0) * il1, s2 = (q2 - q1) * il2;
         QL[v] = q0 + lim32<LIM>(s1, s0) * lm;
         QR[v] = q1 - lim32<LIM>(s2, s1) * lp;
@@ -179,10 +186,10 @@ __device__ __forceinline__ bool face32(const float* sP, const float* dlp, int ba
 // boundary-face loop.
 template <int RIEM, int LIM, int NT, int TX, int TY>
 __device__ __forceinline__ void interior_faces32(const StageArgs& a, const DBlock& B, CaseState* cs, int i0,
-                                                 int j0, const float* sP, const float* sD, const float* sG,
-                                                 float* sF, float gam, float gm1, float gf) {
+                                                 int j0, const float4* sP, const float* sD, const float4* sG,
+                                                 float4* sF, float gam, float gm1, float gf) {
     using L = Tile32<TX, TY>;
-    constexpr int W = L::W, AREA = L::AREA, NFI = L::NFI, NF = L::NF;
+    constexpr int W = L::W, NFI = L::NFI, NF = L::NF;
     const int ni = B.ni, nj = B.nj;
     for (int f = threadIdx.x; f < NF; f += NT) {
         int base, step, pos, lenn, k, kmax, ii, jj;
@@ -196,31 +203,30 @@ __device__ __forceinline__ void interior_faces32(const StageArgs& a, const DBloc
             const int ff = f - NFI;
             const int row = ff / TX, col = ff - row * TX;
             pos = j0 + row; lenn = nj; k = i0 + col; kmax = ni;
-            base = row * W + col + 2; step = W; dlp = sD + AREA;
+            base = row * W + col + 2; step = W; dlp = sD + 1;
             ii = k + 1; jj = pos;
         }
         if (k >= kmax || pos <= 0 || pos >= lenn) continue;
         float out[4];
-        const bool ok = face32<RIEM, LIM, AREA>(sP, dlp, base, step, sG[f], sG[NF + f], sG[2 * NF + f], gam,
-                                                gm1, gf, out);
+        const float4 gq = sG[f];
+        const bool ok = face32<RIEM, LIM>(sP, dlp, base, step, gq.x, gq.y, gq.z, gam, gm1, gf, out);
         if (!ok) record_error(cs, 4, B.local_b, ii, jj, a.irk);
-#pragma unroll
-        for (int v = 0; v < 4; ++v) sF[v * NF + f] = out[v];
+        sF[f] = make_float4(out[0], out[1], out[2], out[3]);
     }
 }
 
-template <int RIEM, int AREA>
-__device__ __forceinline__ bool face32_lim(int lim, const float* sP, const float* dlp, int base, int step,
+template <int RIEM>
+__device__ __forceinline__ bool face32_lim(int lim, const float4* sP, const float* dlp, int base, int step,
                                           float nx, float ny, float len, float gam, float gm1, float gf,
                                           float* out) {
     switch (lim) {
-        case 0: return face32<RIEM, 0, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        case 1: return face32<RIEM, 1, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        case 2: return face32<RIEM, 2, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        case 3: return face32<RIEM, 3, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        case 4: return face32<RIEM, 4, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        case 5: return face32<RIEM, 5, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        default: return face32<RIEM, 6, AREA>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 0: return face32<RIEM, 0>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 1: return face32<RIEM, 1>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 2: return face32<RIEM, 2>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 3: return face32<RIEM, 3>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 4: return face32<RIEM, 4>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 5: return face32<RIEM, 5>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        default: return face32<RIEM, 6>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
     }
 }
 
@@ -286,13 +292,15 @@ template <int RIEM, int TX, int TY, int NT, int MB>
 __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
     using L = Tile32<TX, TY>;
     constexpr int W = L::W, AREA = L::AREA, NFI = L::NFI, NF = L::NF, NC = L::NC;
+    static_assert(L::bG % 16 == 0 && L::bF % 16 == 0 && L::bD % 8 == 0, "shared layout alignment");
     extern __shared__ double smem[];
     double* sC = smem;
-    float* sf = reinterpret_cast<float*>(smem);
-    float* sP = sf + L::oP;
-    float* sD = sf + L::oD;
-    float* sG = sf + L::oG;
-    float* sF = sf + L::oF;
+    unsigned char* sb = reinterpret_cast<unsigned char*>(smem);
+    float4* sP = reinterpret_cast<float4*>(sb + L::bP);
+    float4* sG = reinterpret_cast<float4*>(sb + L::bG);
+    float4* sF = reinterpret_cast<float4*>(sb + L::bF);
+    float2* sD2 = reinterpret_cast<float2*>(sb + L::bD);
+    const float* sD = reinterpret_cast<const float*>(sD2);
     __shared__ double red[(NT / 32) * 5];
     __shared__ double tile_part[5];
     __shared__ int s_flag;
@@ -329,35 +337,27 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
         }
         // face geometry and the state / lengths of the cross-shaped halo: branch-free address
         // selection so that every load of a thread is in flight before the first use
+        const float4* gi4 = a.fi4 + B.ofi / 2;
+        const float4* gj4 = a.fj4 + B.ofj / 2;
 #pragma unroll
         for (int u = 0; u < (NF + NT - 1) / NT; ++u) {
             const int f = tid + u * NT;
             bool ok;
-            long long off, ps;
-            const double* base;
+            const float4* src;
             if (f < NFI) {
                 const int row = f / (TX + 1), col = f - row * (TX + 1);
                 const int jj = j0 + row, F = i0 + col;
                 ok = jj < nj && F <= ni;
-                off = (long long)jj * (ni + 1) + F;
-                base = a.fi + B.ofi;
-                ps = B.pfi;
+                src = gi4 + (ok ? (long long)jj * (ni + 1) + F : 0);
             } else {
                 const int ff = f - NFI;
                 const int row = ff / TX, col = ff - row * TX;
                 const int ii = i0 + col, G = j0 + row;
                 ok = f < NF && ii < ni && G <= nj;
-                off = (long long)G * ni + ii;
-                base = a.fj + B.ofj;
-                ps = B.pfj;
+                src = gj4 + (ok ? (long long)G * ni + ii : 0);
             }
-            const double* src = base + (ok ? off : 0);
-            const double x = __ldg(src), y = __ldg(src + ps), z = __ldg(src + 2 * ps);
-            if (ok) {
-                sG[f] = (float)x;
-                sG[NF + f] = (float)y;
-                sG[2 * NF + f] = (float)z;
-            }
+            const float4 gq = __ldg(src);
+            if (ok) sG[f] = gq;
         }
         bool edge = false;
 #pragma unroll
@@ -371,19 +371,11 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             const bool indl = cross && ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1;
             edge = edge || (cross && inI != inJ);
             const double* src = Pin + (inner ? (long long)jj * ni + ii : 0);
-            const double* dsrc = a.dl + B.og + (indl ? (long long)(jj + 2) * (ni + 4) + (ii + 2) : 0);
+            const float* dsrc = a.dl32 + B.og + (indl ? (long long)(jj + 2) * (ni + 4) + (ii + 2) : 0);
             const double q0 = __ldg(src), q1 = __ldg(src + pc), q2 = __ldg(src + 2 * pc), q3 = __ldg(src + 3 * pc);
-            const double d0 = __ldg(dsrc), d1 = __ldg(dsrc + B.pg);
-            if (indl) {
-                sD[idx] = (float)d0;
-                sD[AREA + idx] = (float)d1;
-            }
-            if (inner) {
-                sP[idx] = (float)q0;
-                sP[AREA + idx] = (float)q1;
-                sP[2 * AREA + idx] = (float)q2;
-                sP[3 * AREA + idx] = (float)q3;
-            }
+            const float d0 = __ldg(dsrc), d1 = __ldg(dsrc + B.pg);
+            if (indl) sD2[idx] = make_float2(d0, d1);
+            if (inner) sP[idx] = make_float4((float)q0, (float)q1, (float)q2, (float)q3);
         }
         if (__syncthreads_or(edge)) {   // ghost cells (Fill_Ghost_Cell), only next to block edges
             for (int idx = tid; idx < AREA; idx += NT) {
@@ -393,8 +385,7 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                 const bool inI = ii >= 0 && ii < ni, inJ = jj >= 0 && jj < nj;
                 double q[4];
                 if (inI == inJ || !ghost_value(a, B, ii, jj, q)) continue;
-#pragma unroll
-                for (int v = 0; v < 4; ++v) sP[v * AREA + idx] = (float)q[v];
+                sP[idx] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
             }
         }
         cp_async_wait_all();
@@ -434,21 +425,21 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                 const EdgeRec e = a.edges[B.eo[Fm - 1] + k];
                 const int cb = (bj - j0 + 2) * W + (bi - i0 + 2);     // boundary cell
                 const int ci = cb + dj * W + di;                       // its inward neighbour
-                const float* dlp = Fm <= 2 ? sD : sD + AREA;
-                const float nx = sG[f], ny = sG[NF + f], ln = sG[2 * NF + f];
+                const float* dlp = Fm <= 2 ? sD : sD + 1;
+                const float4 gq = sG[f];
+                const float nx = gq.x, ny = gq.y, ln = gq.z;
                 float X[4] = {0.0f, 0.0f, 0.0f, 0.0f};
                 if (e.type == 101) {   // BC_Connection_Eul: the interior scheme on the ghost stencil
                     const int step = Fm <= 2 ? 1 : W;
                     const int base = (Fm == 1 || Fm == 3) ? cb - 2 * step : cb - step;
-                    const bool ok = face32_lim<RIEM, AREA>(a.limiter, sP, dlp, base, step, nx, ny, ln, gam, gm1,
-                                                           gf, X);
+                    const bool ok = face32_lim<RIEM>(a.limiter, sP, dlp, base, step, nx, ny, ln, gam, gm1, gf, X);
                     if (!ok) record_error(cs, 4, B.local_b, bi + 1, bj + 1, a.irk);
                 } else if (e.type == 300 || e.type == 400) {
-                    float Bq[4], Iq[4];
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) { Bq[v] = sP[v * AREA + cb]; Iq[v] = sP[v * AREA + ci]; }
+                    const float4 Bc = sP[cb], Ic = sP[ci];
+                    const float Bq[4] = {Bc.x, Bc.y, Bc.z, Bc.w}, Iq[4] = {Ic.x, Ic.y, Ic.z, Ic.w};
                     if (e.type == 300)
-                        bc_symmetry32_lim<RIEM>(a.limiter, Fm, Bq, Iq, dlp[cb], dlp[ci], nx, ny, ln, gam, gm1, gf, X);
+                        bc_symmetry32_lim<RIEM>(a.limiter, Fm, Bq, Iq, dlp[2 * cb], dlp[2 * ci], nx, ny, ln, gam, gm1,
+                                                gf, X);
                     else
                         bc_extrapolation32(Bq, nx, ny, ln, gf, X);
                 } else if (e.type > 0) {   // inflow / outflow records: FP64 from the FP64 state
@@ -462,8 +453,8 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
 #pragma unroll
                         for (int v = 0; v < 4; ++v) Ip.v[v] = __ldg(pi + v * pc);
                     } else {   // one-cell-thick block: the neighbour is the opposite ghost
-#pragma unroll
-                        for (int v = 0; v < 4; ++v) Ip.v[v] = (double)sP[v * AREA + ci];
+                        const float4 Ic = sP[ci];
+                        Ip.v[0] = Ic.x; Ip.v[1] = Ic.y; Ip.v[2] = Ic.z; Ip.v[3] = Ic.w;
                     }
                     const double* dlb = a.dl + B.og + (long long)(Fm <= 2 ? 0 : 1) * B.pg;
                     const double dlbv = __ldg(dlb + (long long)(bj + 2) * (ni + 4) + (bi + 2));
@@ -477,8 +468,7 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
 #pragma unroll
                     for (int v = 0; v < 4; ++v) X[v] = (float)q.v[v];
                 }
-#pragma unroll
-                for (int v = 0; v < 4; ++v) sF[v * NF + f] = X[v];
+                sF[f] = make_float4(X[0], X[1], X[2], X[3]);
             }
         }
         __syncthreads();
@@ -499,18 +489,19 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             const int i1 = ii + 1, j1 = jj + 1;
             const int fi0 = row * (TX + 1) + col, fj0 = NFI + row * TX + col;
             double r[4];
+            const float4 Fw = sF[fi0], Fe = sF[fi0 + 1], Fs = sF[fj0], Fn = sF[fj0 + TX];
 #pragma unroll
             for (int v = 0; v < 4; ++v) {   // interior i, interior j, then boundary faces 1..4
-                const float* Fv = sF + v * NF;
+                const double w = comp(Fw, v), e = comp(Fe, v), so = comp(Fs, v), no = comp(Fn, v);
                 double x = 0.0;
-                if (i1 > 1) x = x - (double)Fv[fi0];
-                if (i1 < ni) x = x + (double)Fv[fi0 + 1];
-                if (j1 > 1) x = x - (double)Fv[fj0];
-                if (j1 < nj) x = x + (double)Fv[fj0 + TX];
-                if (i1 == 1) x = x - (double)Fv[fi0];
-                if (i1 == ni) x = x + (double)Fv[fi0 + 1];
-                if (j1 == 1) x = x - (double)Fv[fj0];
-                if (j1 == nj) x = x + (double)Fv[fj0 + TX];
+                if (i1 > 1) x = x - w;
+                if (i1 < ni) x = x + e;
+                if (j1 > 1) x = x - so;
+                if (j1 < nj) x = x + no;
+                if (i1 == 1) x = x - w;
+                if (i1 == ni) x = x + e;
+                if (j1 == 1) x = x - so;
+                if (j1 == nj) x = x + no;
                 r[v] = x;
             }
             const double sur = sC[4 * NC + k];
@@ -564,11 +555,11 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                 float dtmin = 1e8f;
                 {
                     const float e0 = (float)scb[2 * pc + cg], e1 = (float)scb[3 * pc + cg];
-                    dtmin = fminf(dtmin, sD[sidx] * rcp_approx(fabsf(u * e0 + vv * e1) + snd) * cfl);
+                    dtmin = fminf(dtmin, sD[2 * sidx] * rcp_approx(fabsf(u * e0 + vv * e1) + snd) * cfl);
                 }
                 if (ndir == 2) {
                     const float e0 = (float)scb[4 * pc + cg], e1 = (float)scb[5 * pc + cg];
-                    dtmin = fminf(dtmin, sD[AREA + sidx] * rcp_approx(fabsf(u * e0 + vv * e1) + snd) * cfl);
+                    dtmin = fminf(dtmin, sD[2 * sidx + 1] * rcp_approx(fabsf(u * e0 + vv * e1) + snd) * cfl);
                 }
                 double dtn = (double)dtmin;
                 if (iter_next < a.rampa) dtn = dtn * (double)iter_next / (double)a.rampa;

@@ -103,7 +103,7 @@ def test_capacity_admission_and_retire():
     big = cases.request_case("nozzle", 60000, rng)
     opts = serve_options(itermax=5)
     # a budget for about 1.5 of these cases
-    budget = int(1.5 * big.cells * 240)
+    budget = int(1.5 * big.cells * 306)
     with ServeContext(opts, budget, 4) as sc:
         c0 = sc.admit(big)
         assert c0 is not None
@@ -130,7 +130,7 @@ def test_request_loop_small_stream():
             for k, (kind, cells) in enumerate([("ramp", 900), ("nozzle", 1200), ("ramp", 3000),
                                                ("nozzle", 700), ("ramp", 2000), ("nozzle", 5000)])]
     opts = serve_options(itermax=300, drop=1e-3)
-    st = serve(reqs, opts, device_bytes=int(2 * 5000 * 240 + (1 << 20)), max_cases=3, steps_per_call=10,
+    st = serve(reqs, opts, device_bytes=int(2 * 5000 * 306 + (1 << 20)), max_cases=3, steps_per_call=10,
                realtime=False)
     assert st["served"] == len(reqs) and st["errors"] == 0 and st["rejected"] == 0
     for r in reqs:
