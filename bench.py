@@ -63,11 +63,7 @@ def parse():
     return ap.parse_args()
 
 
-def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+from q2d_b200.replicas import dist_env  # noqa: E402  (one process per GPU, replicas)
 
 
 class ClockSampler:
@@ -117,7 +113,9 @@ def read_traffic(schedule):
     """DRAM bytes (read + write) per stage launch of the full batch, from the ncu summary of
     the stage kernel under profiles/ (a smaller batch captured and scaled by cells), when that
     summary was taken with the same schedule; otherwise None."""
-    f = REPO / "profiles" / "stage_kernel_batched_nozzles.md"
+    name = "stage32_kernel_batched_nozzles.md" if schedule.startswith("fp32-flux") else \
+        "stage_kernel_fp64_batched_nozzles.md"
+    f = REPO / "profiles" / name
     try:
         kv = {}
         for line in f.read_text().splitlines():
@@ -133,7 +131,8 @@ def read_traffic(schedule):
 
 def batch_cases(n, rank):
     from q2d_b200 import cases
-    return cases.area_nozzle_batch(n=n, seed=cases.BASE_SEED + 3 + 7919 * rank)
+    from q2d_b200.replicas import rank_seed
+    return cases.area_nozzle_batch(n=n, seed=rank_seed(cases.BASE_SEED + 3, rank))
 
 
 def time_device(lib, solver, K):
@@ -265,26 +264,20 @@ def main():
     import torch
     from q2d_b200 import make_options, _abi
     from q2d_b200.solver import Q2DSolver
+    from q2d_b200 import replicas
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        replicas.init("nccl", timeout_s=300)
     lib = _abi.load_library()
     K, W = args.steps, max(3, args.warmup)
     batch = batch_cases(args.cases, rank)
     cells = sum(c.cells for c in batch)
-
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
+    cells_all = replicas.sum_over_ranks(cells, "cuda")   # whole-job cells (replicas, weak scaling)
+    barrier = replicas.barrier
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, "cuda")
 
     # ---- FP32-flux / FP64-state batched form (the headline) ----------------------------
     prec = 1 if args.form == "fp32-flux" else 0
@@ -300,7 +293,7 @@ def main():
     with ClockSampler(local) as clk:
         ms, launches = time_device(lib, s, K)
     ms = max_over_ranks(ms)
-    value = world * cells * K / (ms / 1e3)
+    value = cells_all * K / (ms / 1e3)
     infos = s.step(0)
     errs = sum(1 for i in infos if i["err"])
     t_launch = ms / 1e3 / (K * STAGES)
@@ -336,7 +329,7 @@ def main():
             lib.q2d_gpu_download_prim(s.ctx, s.block_ids[b][0], _abi.dptr(o))
         te = max_over_ranks(time.perf_counter() - t0)
         bytes_state = sum(a.nbytes for a in P_host)
-        e2e = {"value": world * cells * Ke / te, "unit": UNIT,
+        e2e = {"value": cells_all * Ke / te, "unit": UNIT,
                "h2d_bytes_per_step": int(bytes_state / Ke),
                "d2h_bytes_per_step": int(bytes_state / Ke + C.sizeof(_abi.StepInfo) * len(batch)),
                "steps": Ke, "seconds": te,
@@ -352,7 +345,7 @@ def main():
         K64 = max(5, K // 4)
         ms64, _ = time_device(lib, s64, K64)
         ms64 = max_over_ranks(ms64)
-        v64 = world * cells * K64 / (ms64 / 1e3)
+        v64 = cells_all * K64 / (ms64 / 1e3)
         fp64 = {"value": v64, "unit": UNIT, "steps": K64, "ms_per_step": ms64 / K64,
                 "schedule": tuned64["schedule"] + " (autotuned)",
                 "ratio_fp32flux_over_fp64": value / v64}
