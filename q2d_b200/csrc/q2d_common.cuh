@@ -417,6 +417,31 @@ __device__ void item_done(const StageArgs& a, int case_id, bool with_res, bool w
     __syncthreads();
 }
 
+// Explicit_Step prologue of a case (Mod_Explicit.f90:38-55): done once per step, in the first
+// stage, by the CTA that takes the case's first item. Nothing in the other items of that stage
+// reads the fields it changes.
+__device__ __forceinline__ void step_prologue(const StageArgs& a, int case_id) {
+    CaseState* cs = &a.cstate[case_id];
+    cs->dtglobal = cs->dt_step;
+    cs->iter += 1;
+    cs->iter_from_call += 1;
+    if (a.time_accurate) cs->time = cs->time + cs->dt_step;
+}
+
+// End of one work item of a stage kernel. Only the last stage counts items to find the CTA that
+// finalises the case (residual, next dt, TODO; with a fence so that the item partials are
+// visible); the first stage of a multi-stage step runs the prologue from the case's first item;
+// middle stages only need the barrier that protects the shared tile.
+template <int NT>
+__device__ void stage_item_end(const StageArgs& a, int it, int case_id, double* red, int* s_flag) {
+    if (a.last) {
+        item_done<NT>(a, case_id, true, true, a.first != 0, red, s_flag);
+        return;
+    }
+    if (a.first && threadIdx.x == 0 && it == a.cases[case_id].item_begin) step_prologue(a, case_id);
+    __syncthreads();
+}
+
 template <int NT>
 __device__ void block_reduce_store(double* acc, double* red, double* out) {
     const int tid = threadIdx.x;

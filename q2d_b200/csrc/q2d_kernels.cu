@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
             if (tid == 0)
                 for (int k = 0; k < 5; ++k) a.part[5 * (size_t)it + k] = tile_part[k];
         }
-        item_done<NT>(a, w.case_id, a.last != 0, a.last != 0, a.first != 0, red, &s_flag);
+        stage_item_end<NT>(a, it, w.case_id, red, &s_flag);
     }
 }
 

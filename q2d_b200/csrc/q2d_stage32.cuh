@@ -34,8 +34,9 @@ struct Tile32 {
     static constexpr int W = TX + 4, H = TY + 4, AREA = W * H;
     static constexpr int NFI = (TX + 1) * TY, NFJ = TX * (TY + 1), NF = NFI + NFJ;
     static constexpr int NC = TX * TY;
-    // FP64 cell planes: 0-3 state at the start of the step, 4 sur, 5 dt, 6-7 source geometry
-    static constexpr int NCD = 8;
+    // FP64 cell planes: 0-3 state at the start of the step, 4 sur, 5 dt, 6-7 source geometry,
+    // 8-11 state
+    static constexpr int NCD = 12;
     static constexpr size_t bP = sizeof(double) * NCD * NC;   // float4 [AREA]  rho, u, v, p
     static constexpr size_t bG = bP + 16 * (size_t)AREA;      // float4 [NF]    nx, ny, length, -
     static constexpr size_t bF = bG + 16 * (size_t)NF;        // float4 [NF]    flux times length
@@ -376,6 +377,10 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             const float d0 = __ldg(dsrc), d1 = __ldg(dsrc + B.pg);
             if (indl) sD2[idx] = make_float2(d0, d1);
             if (inner) sP[idx] = make_float4((float)q0, (float)q1, (float)q2, (float)q3);
+            if (inner && r >= 2 && r < TY + 2 && c >= 2 && c < TX + 2) {   // the tile's own cells, FP64
+                const int kk = (r - 2) * TX + (c - 2);
+                sC[8 * NC + kk] = q0; sC[9 * NC + kk] = q1; sC[10 * NC + kk] = q2; sC[11 * NC + kk] = q3;
+            }
         }
         if (__syncthreads_or(edge)) {   // ghost cells (Fill_Ghost_Cell), only next to block edges
             for (int idx = tid; idx < AREA; idx += NT) {
@@ -485,7 +490,7 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             const long long cg = (long long)jj * ni + ii;
             double P[4];
 #pragma unroll
-            for (int v = 0; v < 4; ++v) P[v] = __ldg(Pin + v * pc + cg);
+            for (int v = 0; v < 4; ++v) P[v] = sC[(8 + v) * NC + k];
             const int i1 = ii + 1, j1 = jj + 1;
             const int fi0 = row * (TX + 1) + col, fj0 = NFI + row * TX + col;
             double r[4];
@@ -572,7 +577,7 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             if (tid == 0)
                 for (int k = 0; k < 5; ++k) a.part[5 * (size_t)it + k] = tile_part[k];
         }
-        item_done<NT>(a, w.case_id, a.last != 0, a.last != 0, a.first != 0, red, &s_flag);
+        stage_item_end<NT>(a, it, w.case_id, red, &s_flag);
     }
 }
 
