@@ -187,8 +187,8 @@ int  q2d_gpu_autotune(q2d_ctx* ctx, int steps, int* schedule, float* ms_per_step
 
 /* Pins the schedule of the stage kernels (the index the autotuner reports) without tuning:
  * 0-2 CTA-tile kernel on 32x10, 32x8, 64x4 tiles; 3-4 warp-marching kernel with 8 / 16 rows
- * per item; 5-7 FP32-flux tile kernel on 32x10, 32x8, 64x4 tiles, 8 the same on 32x10 tiles with
- * registers for 3 instead of 4 CTAs per SM (FP32-flux form only; 5 is its default). q2d_gpu_get_schedule returns the current one. */
+ * per item; 5-9 FP32-flux tile kernel on 32x10, 32x8, 64x4 (256 threads) and 32x16, 64x8 (512
+ * threads) tiles (FP32-flux form only; 5 is its default). q2d_gpu_get_schedule returns the current one. */
 int  q2d_gpu_set_schedule(q2d_ctx* ctx, int schedule);
 int  q2d_gpu_get_schedule(const q2d_ctx* ctx);
 

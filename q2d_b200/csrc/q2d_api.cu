@@ -685,10 +685,9 @@ int ready(q2d_ctx* ctx) {
 struct Schedule { int kernel, tile, march_h; };
 // Candidate schedules, indexed like the autotuner's result: CTA-tile stage kernel on tiles
 // 32x10, 32x8, 64x4; warp-marching kernel with 8 or 16 rows per item; FP32-flux tile kernel
-// on tiles 32x10, 32x8, 64x4 with registers for 4 CTAs per SM, and 32x10 with registers for 3
-// (FP32-flux form only).
+// on tiles 32x10, 32x8, 64x4 (256 threads) and 32x16, 64x8 (512 threads) (FP32-flux form only).
 const Schedule kSchedules[] = {{0, 0, 16}, {0, 1, 16}, {0, 2, 16}, {1, 0, 8}, {1, 0, 16},
-                               {2, 0, 16}, {2, 1, 16}, {2, 2, 16}, {2, 3, 16}};
+                               {2, 0, 16}, {2, 1, 16}, {2, 2, 16}, {2, 3, 16}, {2, 4, 16}};
 constexpr int kNumSchedules = (int)(sizeof(kSchedules) / sizeof(kSchedules[0]));
 
 bool schedule_allowed(const q2d_ctx* ctx, int k) {
@@ -814,14 +813,7 @@ q2d_ctx* new_ctx(const q2d_options* opt) {
         delete ctx;
         return nullptr;
     }
-    const char* t = getenv("Q2D_TILE");
-    if (t) ctx->tile = std::max(0, std::min(kNumTiles - 1, atoi(t)));
-    const char* kk = getenv("Q2D_KERNEL");
-    if (kk) ctx->kernel = std::max(0, std::min(2, atoi(kk)));
-    if (!kk && opt->precision == Q2D_PREC_FP32_FLUX) ctx->kernel = 2;
-    if (ctx->kernel == 2 && opt->precision != Q2D_PREC_FP32_FLUX) ctx->kernel = 0;
-    const char* mh = getenv("Q2D_MARCH_H");
-    if (mh) ctx->march_h = std::max(1, std::min(4096, atoi(mh)));
+    if (opt->precision == Q2D_PREC_FP32_FLUX) ctx->kernel = 2;   // default schedules 0 / 5
     return ctx;
 }
 

@@ -547,15 +547,23 @@ int stage_occupancy(int prec, int riem, int tile) {
 }
 
 void tile_dims(int tile, int* tx, int* ty, int* nt) {
-#define Q2D_CALL(TX, TY, NT) { *tx = TX; *ty = TY; *nt = NT; }
-    Q2D_TILE_SWITCH(tile, Q2D_CALL)
-#undef Q2D_CALL
+    switch (tile) {
+        case 1: *tx = 32; *ty = 8; *nt = 256; break;
+        case 2: *tx = 64; *ty = 4; *nt = 256; break;
+        case 3: *tx = 32; *ty = 16; *nt = 512; break;
+        case 4: *tx = 64; *ty = 8; *nt = 512; break;
+        default: *tx = 32; *ty = 10; *nt = 256; break;
+    }
 }
 
 cudaError_t launch_dt(const StageArgs& a, int tile, int grid, cudaStream_t s) {
-#define Q2D_CALL(TX, TY, NT) dt_kernel<TX, TY, NT><<<grid, NT, 0, s>>>(a);
-    Q2D_TILE_SWITCH(tile, Q2D_CALL)
-#undef Q2D_CALL
+    switch (tile) {
+        case 1: dt_kernel<32, 8, 256><<<grid, 256, 0, s>>>(a); break;
+        case 2: dt_kernel<64, 4, 256><<<grid, 256, 0, s>>>(a); break;
+        case 3: dt_kernel<32, 16, 512><<<grid, 512, 0, s>>>(a); break;
+        case 4: dt_kernel<64, 8, 512><<<grid, 512, 0, s>>>(a); break;
+        default: dt_kernel<32, 10, 256><<<grid, 256, 0, s>>>(a); break;
+    }
     return cudaGetLastError();
 }
 

@@ -5,9 +5,9 @@
 
 namespace q2d {
 
-// Tile configurations of the stage kernel (tile id -> TX x TY cells, NT threads):
-//   0: 32 x 10, 256 threads   1: 32 x 8, 256 threads   2: 64 x 4, 256 threads
-constexpr int kNumTiles = 3;
+// Tile configurations (tile id -> TX x TY cells, NT threads): 0: 32 x 10, 256; 1: 32 x 8, 256;
+// 2: 64 x 4, 256 (every stage kernel); 3: 32 x 16, 512; 4: 64 x 8, 512 (FP32-flux kernel only)
+constexpr int kNumTiles = 5;
 void tile_dims(int tile, int* tx, int* ty, int* nt);
 
 cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int grid, cudaStream_t s);

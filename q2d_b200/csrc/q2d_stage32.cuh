@@ -309,11 +309,44 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
     const Gas& g = a.gas;
     const float gam = (float)g.gamma, gm1 = (float)g.gm1, gf = (float)g.gfac;
 
-    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
-        const WorkItem w = a.items[it];
-        const DBlock B = a.blocks[w.block];
+    // Work-item descriptors (item, block, case status), double-buffered in shared memory: warp 0
+    // fetches the next item's while the CTA works on the current one.
+    __shared__ WorkItem sW[2];
+    __shared__ DBlock sBk[2];
+    __shared__ int sSt[2];
+    static_assert(sizeof(WorkItem) == 24 && sizeof(DBlock) % 4 == 0 && sizeof(DBlock) <= 128, "descriptor words");
+    constexpr int NWW = (int)(sizeof(WorkItem) / 4), NBW = (int)(sizeof(DBlock) / 4);
+    const int lane = tid & 31;
+    const bool w0 = tid < 32;
+    if (w0 && blockIdx.x < a.n_items) {
+        const int wv = lane < NWW ? __ldg(reinterpret_cast<const int*>(a.items + blockIdx.x) + lane) : 0;
+        const int blk = __shfl_sync(0xffffffffu, wv, 0), cid = __shfl_sync(0xffffffffu, wv, 3);
+        const int bv = lane < NBW ? __ldg(reinterpret_cast<const int*>(a.blocks + blk) + lane) : 0;
+        if (lane < NWW) reinterpret_cast<int*>(&sW[0])[lane] = wv;
+        if (lane < NBW) reinterpret_cast<int*>(&sBk[0])[lane] = bv;
+        if (lane == 0) sSt[0] = __ldcg(&a.cstate[cid].status);
+    }
+    __syncthreads();
+    int cur = 0;
+    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x, cur ^= 1) {
+        const int nit = it + gridDim.x;
+        const bool pre = w0 && nit < a.n_items;
+        int pw = 0, pb = 0, ps = 0;   // the next item's descriptor words held by warp 0
+        if (pre && lane < NWW) pw = __ldg(reinterpret_cast<const int*>(a.items + nit) + lane);
+        const WorkItem w = sW[cur];
+        const DBlock B = sBk[cur];
         CaseState* cs = &a.cstate[w.case_id];
-        if (__ldcg(&cs->status) != kStatus_Running) continue;   // uniform over the CTA
+        if (sSt[cur] != kStatus_Running) {   // uniform over the CTA: finish the prefetch, next item
+            if (pre) {
+                const int blk = __shfl_sync(0xffffffffu, pw, 0), cid = __shfl_sync(0xffffffffu, pw, 3);
+                pb = lane < NBW ? __ldg(reinterpret_cast<const int*>(a.blocks + blk) + lane) : 0;
+                if (lane < NWW) reinterpret_cast<int*>(&sW[cur ^ 1])[lane] = pw;
+                if (lane < NBW) reinterpret_cast<int*>(&sBk[cur ^ 1])[lane] = pb;
+                if (lane == 0) sSt[cur ^ 1] = __ldcg(&a.cstate[cid].status);
+            }
+            __syncthreads();
+            continue;
+        }
         const int ni = B.ni, nj = B.nj, i0 = w.i0, j0 = w.j0;
         const double* Pin = a.Pin + B.oc;
         const long long pc = B.pc;
@@ -360,7 +393,7 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             const float4 gq = __ldg(src);
             if (ok) sG[f] = gq;
         }
-        bool edge = false;
+        bool conn = false;   // a connection (101) ghost: evaluated in a second pass
 #pragma unroll
         for (int u = 0; u < (AREA + NT - 1) / NT; ++u) {
             const int idx = tid + u * NT;
@@ -370,7 +403,6 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             const bool inI = ii >= 0 && ii < ni, inJ = jj >= 0 && jj < nj;
             const bool inner = cross && inI && inJ;
             const bool indl = cross && ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1;
-            edge = edge || (cross && inI != inJ);
             const double* src = Pin + (inner ? (long long)jj * ni + ii : 0);
             const float* dsrc = a.dl32 + B.og + (indl ? (long long)(jj + 2) * (ni + 4) + (ii + 2) : 0);
             const double q0 = __ldg(src), q1 = __ldg(src + pc), q2 = __ldg(src + 2 * pc), q3 = __ldg(src + 3 * pc);
@@ -381,8 +413,54 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                 const int kk = (r - 2) * TX + (c - 2);
                 sC[8 * NC + kk] = q0; sC[9 * NC + kk] = q1; sC[10 * NC + kk] = q2; sC[11 * NC + kk] = q3;
             }
+            if (cross && inI != inJ) {
+                // ghost cell gd layers beyond face f (Fill_Ghost_Cell, Lib_Ghost.f90:16-299): the
+                // record type, the boundary cell, its two inward neighbours and the face normal are
+                // loaded together; the type picks the rule afterwards
+                int f, gd, k, bi, bj, di, dj, nn;
+                if (!inI) {
+                    f = ii < 0 ? 1 : 2; gd = ii < 0 ? -ii : ii - ni + 1; k = jj;
+                    bi = ii < 0 ? 0 : ni - 1; bj = jj; di = ii < 0 ? 1 : -1; dj = 0; nn = ni;
+                } else {
+                    f = jj < 0 ? 3 : 4; gd = jj < 0 ? -jj : jj - nj + 1; k = ii;
+                    bi = ii; bj = jj < 0 ? 0 : nj - 1; di = 0; dj = jj < 0 ? 1 : -1; nn = nj;
+                }
+                if (gd <= 2) {
+                    const int type = __ldg(&a.edges[B.eo[f - 1] + k].type);
+                    const long long s1 = nn >= 2 ? (long long)dj * ni + di : 0;
+                    const long long s2 = nn >= 3 ? 2 * s1 : s1;
+                    const double* pb = Pin + (long long)bj * ni + bi;
+                    const double* gn = f <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (f == 1 ? 0 : ni)
+                                              : a.fj + B.ofj + (long long)(f == 3 ? 0 : nj) * ni + bi;
+                    const long long gs = f <= 2 ? B.pfi : B.pfj;
+                    double b[4], c1[4], c2[4];
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        b[v] = __ldg(pb + v * pc);
+                        c1[v] = __ldg(pb + v * pc + s1);
+                        c2[v] = __ldg(pb + v * pc + s2);
+                    }
+                    const double nx = __ldg(gn), ny = __ldg(gn + gs);
+                    double q[4];
+                    if (type == 300) {   // Ghost_Symmetry (Lib_Ghost.f90:163-196)
+                        const double udotn = b[1] * nx + b[2] * ny;
+                        q[0] = b[0]; q[1] = b[1] - 2.0 * udotn * nx; q[2] = b[2] - 2.0 * udotn * ny; q[3] = b[3];
+                    } else if (type == 0 || type == 401 || type == 405 || type == 406 || type < 0) {
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) q[v] = b[v];   // Ghost_ZG_Extrapolate (:199-219)
+                    } else {   // Ghost_Extrapolate (:270-299); connection ghosts are redone below
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) {
+                            const double g1 = 3.0 * b[v] - 3.0 * c1[v] + c2[v];
+                            q[v] = gd == 1 ? g1 : 3.0 * g1 - 3.0 * b[v] + c1[v];
+                        }
+                    }
+                    conn = conn || type == 101;
+                    sP[idx] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+                }
+            }
         }
-        if (__syncthreads_or(edge)) {   // ghost cells (Fill_Ghost_Cell), only next to block edges
+        if (__syncthreads_or(conn)) {   // connection ghosts: the donor block's cells
             for (int idx = tid; idx < AREA; idx += NT) {
                 const int r = idx / W, c = idx - r * W;
                 if ((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2)) continue;
@@ -395,6 +473,11 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
         }
         cp_async_wait_all();
         __syncthreads();
+        if (pre) {   // next descriptor: block record and case status (the item arrived meanwhile)
+            const int blk = __shfl_sync(0xffffffffu, pw, 0), cid = __shfl_sync(0xffffffffu, pw, 3);
+            pb = lane < NBW ? __ldg(reinterpret_cast<const int*>(a.blocks + blk) + lane) : 0;
+            ps = lane == 0 ? __ldcg(&a.cstate[cid].status) : 0;
+        }
 
         // ---- 2. face fluxes ------------------------------------------------------------------
         switch (a.limiter) {
@@ -477,6 +560,11 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             }
         }
         __syncthreads();
+        if (pre) {   // store the next descriptor; the end-of-item barrier publishes it
+            if (lane < NWW) reinterpret_cast<int*>(&sW[cur ^ 1])[lane] = pw;
+            if (lane < NBW) reinterpret_cast<int*>(&sBk[cur ^ 1])[lane] = pb;
+            if (lane == 0) sSt[cur ^ 1] = ps;
+        }
 
         // ---- 3. residual, sources, RK update (+ next dt and residual norm) -----------------------
         double acc[5] = {0.0, 0.0, 0.0, 0.0, 1e300};

@@ -1,5 +1,5 @@
-// Instantiations of the FP32-flux stage kernel (tile 0-2: 32x10, 32x8, 64x4 at 4 CTAs per SM;
-// tile 3: 32x10 at 3 CTAs per SM) for Riemann solver 2 (see q2d_stage32.cuh).
+// Instantiations of the FP32-flux stage kernel (tiles 0-2: 32x10, 32x8, 64x4 with 256 threads;
+// tiles 3-4: 32x16, 64x8 with 512 threads) for Riemann solver 2 (see q2d_stage32.cuh).
 #include "q2d_stage32.cuh"
 
 namespace q2d {
@@ -8,7 +8,8 @@ cudaError_t launch_stage32_r2(const StageArgs& a, int tile, int grid, cudaStream
     switch (tile) {
         case 1: return launch_stage32_t<2, 32, 8, 256, 4>(a, grid, s);
         case 2: return launch_stage32_t<2, 64, 4, 256, 4>(a, grid, s);
-        case 3: return launch_stage32_t<2, 32, 10, 256, 3>(a, grid, s);
+        case 3: return launch_stage32_t<2, 32, 16, 512, 2>(a, grid, s);
+        case 4: return launch_stage32_t<2, 64, 8, 512, 2>(a, grid, s);
         default: return launch_stage32_t<2, 32, 10, 256, 4>(a, grid, s);
     }
 }
@@ -17,7 +18,8 @@ int stage32_occupancy_r2(int tile) {
     switch (tile) {
         case 1: return stage32_occupancy_t<2, 32, 8, 256, 4>();
         case 2: return stage32_occupancy_t<2, 64, 4, 256, 4>();
-        case 3: return stage32_occupancy_t<2, 32, 10, 256, 3>();
+        case 3: return stage32_occupancy_t<2, 32, 16, 512, 2>();
+        case 4: return stage32_occupancy_t<2, 64, 8, 512, 2>();
         default: return stage32_occupancy_t<2, 32, 10, 256, 4>();
     }
 }
