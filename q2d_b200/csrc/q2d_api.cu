@@ -149,6 +149,7 @@ struct q2d_ctx {
     int grid = 0;
     // device pools and their allocators
     DevBuf<double> PA, PB, PC, SC, DL, FI, FJ, PART;
+    DevBuf<double> XFER;            // staging rows of one block's state for upload / download
     DevBuf<float> DL32, FI4, FJ4;   // FP32 geometry (FP32-flux form only): same regions as DL/FI/FJ
     Arena ac, ag, afi, afj;
     DevBuf<DBlock> dblocks;
@@ -903,9 +904,23 @@ int q2d_gpu_upload_prim(q2d_ctx* ctx, int block_id, const double* P) {
     if (!ctx || block_id < 0 || block_id >= (int)ctx->blocks.size() || !P || ctx->blocks[block_id].case_id < 0)
         return fail(ctx, Q2D_ERR_BADARG, "upload_prim: bad argument");
     HBlock& b = ctx->blocks[block_id];
+    if (ctx->cases[b.case_id].resident) {
+        // the interior rows of P (4*ni doubles each, pitch 4*(ni+4)) by one strided copy into a
+        // staging buffer, then into the state planes on the device
+        const long long n = (long long)b.ni * b.nj;
+        CK(ensure_cap(ctx->XFER, 4 * (size_t)n));
+        const double* row0 = P + 4 * (2 + (size_t)(b.ni + 4) * 2);
+        CK(cudaMemcpy2DAsync(ctx->XFER.p, sizeof(double) * 4 * b.ni, row0, sizeof(double) * 4 * (b.ni + 4),
+                             sizeof(double) * 4 * b.ni, b.nj, cudaMemcpyHostToDevice, ctx->stream));
+        CK(launch_cells_to_planes(ctx->XFER.p, ctx->PA.p + b.d.oc, n, b.d.pc, ctx->stream));
+        ctx->launches += 1;
+        CK(cudaStreamSynchronize(ctx->stream));   // P is the caller's: done before returning
+        ctx->dt_valid = false;
+        return Q2D_OK;
+    }
     std::vector<double> planes;
     fortran_to_planes(b.ni, b.nj, P, planes);
-    if (!ctx->cases[b.case_id].resident) {
+    {
         if (ctx->cases[b.case_id].prepared) {
             for (int v = 0; v < 4; ++v)
                 std::memcpy(&b.staged.pa[v * b.d.pc], &planes[v * (size_t)b.ni * b.nj],
@@ -915,13 +930,6 @@ int q2d_gpu_upload_prim(q2d_ctx* ctx, int block_id, const double* P) {
         }
         return Q2D_OK;
     }
-    const long long n = (long long)b.ni * b.nj;
-    std::vector<double> staged(4 * (size_t)b.d.pc, 0.0);
-    for (int v = 0; v < 4; ++v) std::memcpy(&staged[v * b.d.pc], &planes[v * n], sizeof(double) * n);
-    CK(cudaStreamSynchronize(ctx->stream));
-    CK(cudaMemcpy(ctx->PA.p + b.d.oc, staged.data(), sizeof(double) * staged.size(), cudaMemcpyHostToDevice));
-    ctx->dt_valid = false;
-    return Q2D_OK;
 }
 
 int q2d_gpu_download_prim(q2d_ctx* ctx, int block_id, double* P) {
@@ -931,16 +939,16 @@ int q2d_gpu_download_prim(q2d_ctx* ctx, int block_id, double* P) {
     HBlock& b = ctx->blocks[block_id];
     if (!b.alive || b.case_id < 0 || !ctx->cases[b.case_id].resident)
         return fail(ctx, Q2D_ERR_BADARG, "download_prim: block not resident");
-    std::vector<double> staged(4 * (size_t)b.d.pc);
-    CK(cudaMemcpyAsync(staged.data(), ctx->PA.p + b.d.oc, sizeof(double) * staged.size(),
-                       cudaMemcpyDeviceToHost, ctx->stream));
+    // the state planes into interleaved rows on the device, then one strided copy into the
+    // interior rows of P (its ghost layers are left as they are)
+    const long long n = (long long)b.ni * b.nj;
+    CK(ensure_cap(ctx->XFER, 4 * (size_t)n));
+    CK(launch_planes_to_cells(ctx->PA.p + b.d.oc, b.d.pc, ctx->XFER.p, n, ctx->stream));
+    ctx->launches += 1;
+    double* row0 = P + 4 * (2 + (size_t)(b.ni + 4) * 2);
+    CK(cudaMemcpy2DAsync(row0, sizeof(double) * 4 * (b.ni + 4), ctx->XFER.p, sizeof(double) * 4 * b.ni,
+                         sizeof(double) * 4 * b.ni, b.nj, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    const long long pcs = b.d.pc;
-    for (int j = 0; j < b.nj; ++j)
-        for (int i = 0; i < b.ni; ++i) {
-            double* dst = &P[4 * ((size_t)(i + 2) + (size_t)(b.ni + 4) * (j + 2))];
-            for (int v = 0; v < 4; ++v) dst[v] = staged[v * pcs + (size_t)j * b.ni + i];
-        }
     return Q2D_OK;
 }
 
@@ -1168,7 +1176,7 @@ void q2d_gpu_destroy(q2d_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     drop_graphs(ctx);
     ctx->PA.release(); ctx->PB.release(); ctx->PC.release(); ctx->SC.release(); ctx->DL.release();
-    ctx->FI.release(); ctx->FJ.release(); ctx->PART.release(); ctx->dblocks.release();
+    ctx->FI.release(); ctx->FJ.release(); ctx->PART.release(); ctx->dblocks.release(); ctx->XFER.release();
     ctx->DL32.release(); ctx->FI4.release(); ctx->FJ4.release();
     ctx->dcases.release(); ctx->cstate.release(); ctx->items.release(); ctx->edges.release();
     ctx->bcp.release(); ctx->flag.release();

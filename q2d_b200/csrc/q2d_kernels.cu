@@ -567,6 +567,36 @@ cudaError_t launch_dt(const StageArgs& a, int tile, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// State transfer between the caller's cell-interleaved rows (rho, u, v, p per cell, the interior
+// rows of the reference's P array packed by a strided copy) and the block's 4 state planes.
+__global__ void cells_to_planes_kernel(const double2* __restrict__ in, double* __restrict__ out, long long n,
+                                       long long pc) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const double2 a = in[2 * c], b = in[2 * c + 1];
+        out[c] = a.x; out[pc + c] = a.y; out[2 * pc + c] = b.x; out[3 * pc + c] = b.y;
+    }
+}
+
+__global__ void planes_to_cells_kernel(const double* __restrict__ in, long long pc, double2* __restrict__ out,
+                                       long long n) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        out[2 * c] = make_double2(in[c], in[pc + c]);
+        out[2 * c + 1] = make_double2(in[2 * pc + c], in[3 * pc + c]);
+    }
+}
+
+cudaError_t launch_cells_to_planes(const double* in, double* out, long long n, long long pc, cudaStream_t s) {
+    const int grid = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 8));
+    cells_to_planes_kernel<<<grid, 256, 0, s>>>(reinterpret_cast<const double2*>(in), out, n, pc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_planes_to_cells(const double* in, long long pc, double* out, long long n, cudaStream_t s) {
+    const int grid = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 8));
+    planes_to_cells_kernel<<<grid, 256, 0, s>>>(in, pc, reinterpret_cast<double2*>(out), n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_copy(const double* src, double* dst, long long n, int* flag, cudaStream_t s) {
     const int grid = (int)std::min<long long>((n + 255) / 256, 148 * 8);
     copy_state_kernel<<<grid > 0 ? grid : 1, 256, 0, s>>>(src, dst, n, flag);

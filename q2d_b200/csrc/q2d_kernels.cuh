@@ -22,6 +22,9 @@ int march_occupancy(int prec, int riem, int lim);
 cudaError_t launch_dt_march(const StageArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_dt(const StageArgs& a, int tile, int grid, cudaStream_t s);
 cudaError_t launch_copy(const double* src, double* dst, long long n, int* flag, cudaStream_t s);
+// cell-interleaved (rho, u, v, p) <-> 4 planes of stride pc, n cells (state upload / download)
+cudaError_t launch_cells_to_planes(const double* in, double* out, long long n, long long pc, cudaStream_t s);
+cudaError_t launch_planes_to_cells(const double* in, long long pc, double* out, long long n, cudaStream_t s);
 cudaError_t launch_resume(CaseState* cs, int n, int* flag, cudaStream_t s);
 
 }  // namespace q2d
