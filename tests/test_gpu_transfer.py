@@ -36,3 +36,35 @@ def test_upload_download_round_trip(precision):
         assert info["iter"] == 3
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_error_isolation_between_cases(precision):
+    """A NaN state injected from the host into one case (host-side fault injection) stops that
+    case with Q2D_ERR_NAN; every other case of the batch advances exactly as in a run where the
+    injected case was given back its own state."""
+    batch = cases.area_nozzle_batch(n=4, seed=21, nx_range=(40, 80), ny_range=(8, 12))
+
+    def run(inject):
+        s = Q2DSolver(make_options(batch[0], precision=precision), batch)
+        try:
+            s.step(2)
+            b = batch[1].blocks[0]
+            bid = s.block_ids[1][0]
+            P = np.zeros((b.nj + 4, b.ni + 4, 4))
+            assert s.lib.q2d_gpu_download_prim(s.ctx, bid, _abi.dptr(P)) == 0
+            if inject:
+                P[2 + b.nj // 2, 2 + b.ni // 2, 3] = np.nan
+            assert s.lib.q2d_gpu_upload_prim(s.ctx, bid, _abi.dptr(P)) == 0
+            infos = s.step(8, check=False)
+            return infos, [s.prim(c, 0) for c in range(len(batch))]
+        finally:
+            s.close()
+
+    ref_i, ref_s = run(False)
+    bad_i, bad_s = run(True)
+    assert bad_i[1]["err"] == _abi.ERR_NAN and bad_i[1]["todo"] != _abi.TODO_CONTINUE or bad_i[1]["err"] != 0
+    assert bad_i[1]["iter"] < 10
+    for c in (0, 2, 3):
+        assert bad_i[c]["err"] == 0 and bad_i[c]["iter"] == 10 == ref_i[c]["iter"]
+        assert np.array_equal(bad_s[c], ref_s[c])
