@@ -314,27 +314,30 @@ def main():
                             pin_memory=True).numpy()
             a[...] = cs.blocks[0].prim_ghost()
             P_host.append(a)
-        outs = [np.empty_like(a) for a in P_host]
+        outs = [torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy() for a in P_host]
         infos_t = (_abi.StepInfo * len(batch))()
         Ke = max(3, K // 2)
         assert lib.q2d_gpu_prepare(s.ctx, 1) == 0
         torch.cuda.synchronize()
         barrier()
+        nb = len(batch)
+        ids = (C.c_int * nb)(*[s.block_ids[b][0] for b in range(nb)])
+        p_in = (C.POINTER(C.c_double) * nb)(*[_abi.dptr(a) for a in P_host])
+        p_out = (C.POINTER(C.c_double) * nb)(*[_abi.dptr(o) for o in outs])
         t0 = time.perf_counter()
-        for b, a in enumerate(P_host):
-            lib.q2d_gpu_upload_prim(s.ctx, s.block_ids[b][0], _abi.dptr(a))
+        st = lib.q2d_gpu_upload_prim_many(s.ctx, nb, ids, p_in)
         for _ in range(Ke):
-            lib.q2d_gpu_step(s.ctx, 1, infos_t)
-        for b, o in enumerate(outs):
-            lib.q2d_gpu_download_prim(s.ctx, s.block_ids[b][0], _abi.dptr(o))
+            st = st or lib.q2d_gpu_step(s.ctx, 1, infos_t)
+        st = st or lib.q2d_gpu_download_prim_many(s.ctx, nb, ids, p_out)
         te = max_over_ranks(time.perf_counter() - t0)
+        assert st == 0, lib.q2d_gpu_last_error(s.ctx)
         bytes_state = sum(a.nbytes for a in P_host)
         e2e = {"value": cells_all * Ke / te, "unit": UNIT,
                "h2d_bytes_per_step": int(bytes_state / Ke),
                "d2h_bytes_per_step": int(bytes_state / Ke + C.sizeof(_abi.StepInfo) * len(batch)),
                "steps": Ke, "seconds": te,
-               "path": "q2d_gpu_upload_prim (every block) + q2d_gpu_step(1) x steps (per-step case info "
-                       "to host) + q2d_gpu_download_prim (every block)"}
+               "path": "q2d_gpu_upload_prim_many (every block) + q2d_gpu_step(1) x steps (per-step "
+                       "case info to host) + q2d_gpu_download_prim_many (every block)"}
     s.close()
     # ---- plain FP64 form of the same batch -------------------------------------------------
     fp64 = None

@@ -191,6 +191,10 @@ def load_library() -> C.CDLL:
     lib.q2d_options_default.restype = None
     lib.q2d_options_default.argtypes = [C.POINTER(Options)]
     PD = C.POINTER(C.POINTER(C.c_double))
+    for name in ("upload_prim_many", "download_prim_many"):
+        fn = getattr(lib, f"q2d_gpu_{name}")
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), PD]
     lib.q2d_serve_create.restype = C.c_int
     lib.q2d_serve_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Options), C.c_ulonglong, C.c_int]
     lib.q2d_serve_admit.restype = C.c_int

@@ -192,6 +192,8 @@ StageArgs base_args(q2d_ctx* ctx) {
     a.cstate = ctx->cstate.p;
     a.items = ctx->items.p;
     a.n_items = ctx->n_items;
+    a.n_cases = (int)ctx->cases.size();
+    a.part_stride = 1;
     a.sc = ctx->SC.p;
     a.dl = ctx->DL.p;
     a.dl32 = ctx->DL32.p;
@@ -220,6 +222,18 @@ StageArgs base_args(q2d_ctx* ctx) {
     return a;
 }
 
+// Local time stepping with the FP32-flux kernel computes each cell's time step in the first
+// stage of the step, from the state the step starts from (as Explicit_Step calls Compute_dt,
+// Mod_Explicit.f90:44-53); the other kernels, and global time stepping (which needs the minimum
+// over the case before any cell updates), compute it in the last stage of the previous step and
+// in the time-step passes of ensure_dt.
+bool dt_in_first_stage(const q2d_ctx* ctx) { return ctx->kernel == 2 && !ctx->opt.time_accurate; }
+
+// Item partials per work item: one set per warp for the FP32-flux kernel (256 threads on tiles
+// 0-2, 512 on tiles 3-4, as launch_stage32 instantiates them), which ends its items without a
+// CTA-wide reduction and leaves the case finalisation to finalize_kernel; one otherwise.
+int part_stride(const q2d_ctx* ctx) { return ctx->kernel == 2 ? (ctx->tile >= 3 ? 16 : 8) : 1; }
+
 // RKcoeff (Lib_RK.f90:8-11)
 double rk_coeff(int n_rk, int irk) {
     static const double C[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.5, 0.0}, {1.0, 0.25, 2.0 / 3.0}};
@@ -237,6 +251,9 @@ int enqueue_step(q2d_ctx* ctx, cudaStream_t s, int* nk) {
         a.irk = irk;
         a.first = irk == 1;
         a.last = irk == n_rk;
+        a.dt_first = dt_in_first_stage(ctx) ? 1 : 0;
+        a.part_stride = part_stride(ctx);
+        a.fin_sep = ctx->kernel == 2 ? 1 : 0;
         a.rk_c = rk_coeff(n_rk, irk);
         a.PO = ctx->PA.p;
         if (n_rk == 1) { a.Pin = ctx->PA.p; a.Pout = ctx->PB.p; }
@@ -255,6 +272,10 @@ int enqueue_step(q2d_ctx* ctx, cudaStream_t s, int* nk) {
         else
             CK(launch_stage(a, ctx->opt.precision, ctx->opt.riemann, ctx->tile, ctx->grid, s));
         ++*nk;
+        if (a.last && a.fin_sep) {
+            CK(launch_finalize(a, s));
+            ++*nk;
+        }
     }
     if (n_rk == 1) {
         CK(launch_copy(ctx->PB.p, ctx->PA.p, ctx->ac.cap, ctx->flag.p, s));
@@ -266,7 +287,15 @@ int enqueue_step(q2d_ctx* ctx, cudaStream_t s, int* nk) {
 // Compute_dt for the cases that need it: every running case after a state upload, only the
 // newly uploaded ones after an admission (the others keep the time step their last stage
 // computed, so a case's trajectory does not depend on when other cases arrive).
-int ensure_dt(q2d_ctx* ctx) {
+// With time steps computed in the first stage no pass is needed, and the per-cell time steps
+// left by a step are those it used, not the next step's: dt_valid is cleared so that a switch to
+// another kernel (or `force`, the autotuner's baseline) runs a full pass first.
+int ensure_dt(q2d_ctx* ctx, bool force = false) {
+    if (!force && dt_in_first_stage(ctx)) {
+        ctx->dt_valid = false;
+        ctx->dt_new = false;
+        return Q2D_OK;
+    }
     if (ctx->dt_valid && !ctx->dt_new) return Q2D_OK;
     if (ctx->n_items > 0) {
         StageArgs a = base_args(ctx);
@@ -585,8 +614,9 @@ int rebuild_device_lists(q2d_ctx* ctx) {
     CK(ensure_cap(ctx->edges, edges.size()));
     CK(ensure_cap(ctx->bcp, params.size()));
     CK(ensure_cap(ctx->items, items.size()));
-    if (!ctx->PART.p || ctx->PART.n < 5 * items.size()) {
-        CK(ensure_cap(ctx->PART, 5 * items.size()));
+    const size_t npart = 5 * (size_t)part_stride(ctx) * items.size();
+    if (!ctx->PART.p || ctx->PART.n < npart) {
+        CK(ensure_cap(ctx->PART, npart));
         CK(cudaMemset(ctx->PART.p, 0, sizeof(double) * ctx->PART.n));
     }
     if (!db.empty()) CK(cudaMemcpy(ctx->dblocks.p, db.data(), sizeof(DBlock) * db.size(), cudaMemcpyHostToDevice));
@@ -705,7 +735,7 @@ int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
     CK(saveP.alloc(ec));
     CK(saveSC.alloc(2 * ec));
     CK(saveCS.alloc(nst));
-    if (int e = ensure_dt(ctx)) return e;
+    if (int e = ensure_dt(ctx, true)) return e;   // every candidate starts from valid time steps
     CK(cudaMemcpyAsync(saveP.p, ctx->PA.p, sizeof(double) * ec, cudaMemcpyDeviceToDevice, ctx->stream));
     CK(cudaMemcpyAsync(saveSC.p, ctx->SC.p, sizeof(double) * 2 * ec, cudaMemcpyDeviceToDevice, ctx->stream));
     CK(cudaMemcpyAsync(saveCS.p, ctx->cstate.p, sizeof(CaseState) * nst, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -952,9 +982,75 @@ int q2d_gpu_download_prim(q2d_ctx* ctx, int block_id, double* P) {
     return Q2D_OK;
 }
 
+// Many blocks per call: the strided copies and transposes of all blocks are queued on the
+// context's stream through a staging ring of up to kXferRing doubles, synchronising only when
+// the ring wraps and once at the end (the caller's arrays are done with when the call returns).
+// Blocks of cases not yet on the device take the single-block path (staged on the host).
+constexpr long long kXferRing = 16ll << 20;   // 128 MiB
+
+static int transfer_many(q2d_ctx* ctx, int n, const int* ids, double* const* P, bool up) {
+    if (!ctx) return Q2D_ERR_BADARG;
+    if (n < 0 || (n && (!ids || !P))) return fail(ctx, Q2D_ERR_BADARG, "transfer: bad argument");
+    for (int k = 0; k < n; ++k) {
+        if (ids[k] < 0 || ids[k] >= (int)ctx->blocks.size() || !P[k] || ctx->blocks[ids[k]].case_id < 0)
+            return fail(ctx, Q2D_ERR_BADARG, "transfer: bad block id or array");
+    }
+    if (!up) {
+        if (int e = ready(ctx)) return e;
+    }
+    long long need_max = 0, total = 0;
+    for (int k = 0; k < n; ++k) {
+        const HBlock& b = ctx->blocks[ids[k]];
+        if (!ctx->cases[b.case_id].resident || !b.alive) {
+            if (!up) return fail(ctx, Q2D_ERR_BADARG, "download_prim: block not resident");
+            if (int e = q2d_gpu_upload_prim(ctx, ids[k], P[k])) return e;
+            continue;
+        }
+        const long long len = (4ll * b.ni * b.nj + 31) / 32 * 32;
+        need_max = std::max(need_max, len);
+        total += len;
+    }
+    if (total == 0) return Q2D_OK;
+    CK(ensure_cap(ctx->XFER, (size_t)std::max(need_max, std::min(kXferRing, total))));
+    const long long cap = (long long)ctx->XFER.n;
+    long long off = 0;
+    for (int k = 0; k < n; ++k) {
+        const HBlock& b = ctx->blocks[ids[k]];
+        if (!ctx->cases[b.case_id].resident || !b.alive) continue;
+        const long long cells = (long long)b.ni * b.nj;
+        if (off + 4 * cells > cap) {   // ring full: let the queued transfers finish first
+            CK(cudaStreamSynchronize(ctx->stream));
+            off = 0;
+        }
+        double* st = ctx->XFER.p + off;
+        double* row0 = P[k] + 4 * (2 + (size_t)(b.ni + 4) * 2);
+        const size_t w = sizeof(double) * 4 * b.ni, pitch = sizeof(double) * 4 * (b.ni + 4);
+        if (up) {
+            CK(cudaMemcpy2DAsync(st, w, row0, pitch, w, b.nj, cudaMemcpyHostToDevice, ctx->stream));
+            CK(launch_cells_to_planes(st, ctx->PA.p + b.d.oc, cells, b.d.pc, ctx->stream));
+        } else {
+            CK(launch_planes_to_cells(ctx->PA.p + b.d.oc, b.d.pc, st, cells, ctx->stream));
+            CK(cudaMemcpy2DAsync(row0, pitch, st, w, w, b.nj, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        ctx->launches += 1;
+        off += (4 * cells + 31) / 32 * 32;
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (up) ctx->dt_valid = false;
+    return Q2D_OK;
+}
+
 int q2d_gpu_commit(q2d_ctx* ctx) {
     if (!ctx) return Q2D_ERR_BADARG;
     return ready(ctx);
+}
+
+int q2d_gpu_upload_prim_many(q2d_ctx* ctx, int n, const int* block_ids, const double* const* P) {
+    return transfer_many(ctx, n, block_ids, const_cast<double* const*>(P), true);
+}
+
+int q2d_gpu_download_prim_many(q2d_ctx* ctx, int n, const int* block_ids, double* const* P) {
+    return transfer_many(ctx, n, block_ids, P, false);
 }
 
 int q2d_gpu_step_async(q2d_ctx* ctx, int nsteps) {

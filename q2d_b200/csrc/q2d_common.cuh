@@ -340,13 +340,15 @@ __device__ __forceinline__ float cell_sigma(int lim, float fwd, float bwd) { ret
 template <int NT>
 __device__ void finalize_case(const StageArgs& a, int case_id, bool with_res, bool with_dt,
                               bool commit_begin, double* red) {
+    // with a.dt_first the partials' dt min is the time step of the step that ends here
     const DCase dc = a.cases[case_id];
     CaseState* cs = &a.cstate[case_id];
     const int tid = threadIdx.x;
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 1e300};
     if (with_res || with_dt) {
-        for (int it = dc.item_begin + tid; it < dc.item_end; it += NT) {
-            const double* p = a.part + 5 * (size_t)it;
+        const long long e1 = (long long)dc.item_end * a.part_stride;
+        for (long long e = (long long)dc.item_begin * a.part_stride + tid; e < e1; e += NT) {
+            const double* p = a.part + 5 * (size_t)e;
 #pragma unroll
             for (int k = 0; k < 4; ++k) acc[k] += __ldcg(p + k);
             acc[4] = fmin(acc[4], __ldcg(p + 4));
@@ -370,13 +372,14 @@ __device__ void finalize_case(const StageArgs& a, int case_id, bool with_res, bo
                 for (int k = 0; k < 5; ++k)
                     tot[k] = (k < 4) ? tot[k] + red[w * 5 + k] : fmin(tot[k], red[w * 5 + k]);
         if (commit_begin) {   // Explicit_Step prologue (Mod_Explicit.f90:38-55)
+            if (a.dt_first) cs->dt_step = fmin(tot[4], 1e5);
             cs->dtglobal = cs->dt_step;
             cs->iter += 1;
             cs->iter_from_call += 1;
             if (a.time_accurate) cs->time = cs->time + cs->dt_step;
         }
         if (with_dt) {
-            cs->dt_step = fmin(tot[4], 1e5);
+            if (!a.dt_first) cs->dt_step = fmin(tot[4], 1e5);
             cs->dt_pending = 0;
         }
         if (with_res) {   // Mod_Explicit.f90:120-170
@@ -430,15 +433,18 @@ __device__ __forceinline__ void step_prologue(const StageArgs& a, int case_id) {
 
 // End of one work item of a stage kernel. Only the last stage counts items to find the CTA that
 // finalises the case (residual, next dt, TODO; with a fence so that the item partials are
-// visible); the first stage of a multi-stage step runs the prologue from the case's first item;
-// middle stages only need the barrier that protects the shared tile.
+// visible), unless a.fin_sep leaves that to finalize_kernel, launched after the stage. The step prologue runs in that finalisation when the time steps are computed in the
+// first stage (its cells read the iteration count) or the step has one stage; otherwise the
+// first stage runs it from the case's first item. Middle stages only need the barrier that
+// protects the shared tile.
 template <int NT>
 __device__ void stage_item_end(const StageArgs& a, int it, int case_id, double* red, int* s_flag) {
-    if (a.last) {
-        item_done<NT>(a, case_id, true, true, a.first != 0, red, s_flag);
+    if (a.last && !a.fin_sep) {
+        item_done<NT>(a, case_id, true, true, a.first != 0 || a.dt_first != 0, red, s_flag);
         return;
     }
-    if (a.first && threadIdx.x == 0 && it == a.cases[case_id].item_begin) step_prologue(a, case_id);
+    if (a.first && !a.dt_first && threadIdx.x == 0 && it == a.cases[case_id].item_begin)
+        step_prologue(a, case_id);
     __syncthreads();
 }
 

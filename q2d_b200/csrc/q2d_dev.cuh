@@ -92,6 +92,7 @@ struct StageArgs {
     CaseState* cstate;
     const WorkItem* items;
     int n_items;
+    int n_cases;           // case slots (cstate / cases entries)
     const double* Pin;     // stencil state
     const double* PO;      // state at the start of the step
     double* Pout;
@@ -104,12 +105,16 @@ struct StageArgs {
     const float4* fj4;     // start at float4 index ofi / 2 (ofj / 2)
     const EdgeRec* edges;
     const BCParam* bcp;
-    double* part;          // per-item partials: 4 residual sums + dt min
+    double* part;          // per-item partials: 4 residual sums + dt min, part_stride sets of 5
+    int part_stride;       //   doubles per item (one per warp for the FP32-flux kernel)
+    int fin_sep;           // the last stage leaves the case finalisation to finalize_kernel
     Gas gas;
     double rk_c;           // RKcoeff(n_rk, irk)
     double cfl;
     int irk, n_rk;
     int first, last;       // stage is the first / last of the step
+    int dt_first;          // local time steps computed in the first stage from the step's
+                           // starting state (else in the last stage of the previous step)
     int limiter, source, time_accurate, rampa;
     int res_diter, sol_diter, res_relative;
     long long itermax;

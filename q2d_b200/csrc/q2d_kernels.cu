@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
     using L = Tile<PREC, TX, TY>;
     using ST = typename L::ST;
     constexpr int W = L::W, AREA = L::AREA, NFI = L::NFI, NFJ = L::NFJ, NSI = L::NSI, NSJ = L::NSJ,
-                  NGI = L::NGI, NGJ = L::NGJ, NC = L::NC;
+                  NGI = L::NGI, NC = L::NC;
     extern __shared__ double smem[];
     double* sP = smem + L::oP;
     double* sD = smem + L::oD;
@@ -476,6 +476,27 @@ __global__ void resume_kernel(CaseState* cs, int n, int* launch_flag) {
     if (threadIdx.x == 0 && blockIdx.x == 0 && launch_flag) *launch_flag = 1;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
         if (cs[c].status == kStatus_Paused) cs[c].status = kStatus_Running;
+}
+
+// End-of-step finalisation of every running case (residual norm, time step, TODO: the tail of
+// Explicit_Step, Mod_Explicit.f90:120-170) from the item partials the last stage wrote, one CTA
+// per case. Run after the last stage when that stage does not count items itself (a.fin_sep):
+// the stage's CTAs then end each item without a fence or an atomic.
+__global__ void __launch_bounds__(256) finalize_kernel(const StageArgs a) {
+    __shared__ double red[(256 / 32) * 5];
+    if (threadIdx.x == 0 && blockIdx.x == 0 && a.launch_flag) *a.launch_flag = 1;
+    for (int c = blockIdx.x; c < a.n_cases; c += gridDim.x) {
+        const DCase dc = a.cases[c];
+        if (dc.item_end <= dc.item_begin || __ldcg(&a.cstate[c].status) != kStatus_Running) continue;
+        finalize_case<256>(a, c, true, true, a.first != 0 || a.dt_first != 0, red);
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_finalize(const StageArgs& a, cudaStream_t s) {
+    const int grid = std::max(1, std::min(a.n_cases, 148 * 8));
+    finalize_kernel<<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------------------------------

@@ -26,5 +26,6 @@ cudaError_t launch_copy(const double* src, double* dst, long long n, int* flag, 
 cudaError_t launch_cells_to_planes(const double* in, double* out, long long n, long long pc, cudaStream_t s);
 cudaError_t launch_planes_to_cells(const double* in, long long pc, double* out, long long n, cudaStream_t s);
 cudaError_t launch_resume(CaseState* cs, int n, int* flag, cudaStream_t s);
+cudaError_t launch_finalize(const StageArgs& a, cudaStream_t s);
 
 }  // namespace q2d

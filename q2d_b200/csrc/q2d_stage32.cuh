@@ -289,6 +289,16 @@ __device__ __forceinline__ void bc_symmetry32_lim(int lim, int Fm, const float* 
     }
 }
 
+// Compute_dt body for one cell (Mod_dt.f90:59-104, model 0) in FP32: the CFL time step of each
+// grid direction, dl / (|V.e| + a), the smaller of the two (one direction when ndir == 1).
+__device__ __forceinline__ float cell_dt32(float rho, float u, float v, float p, float gam, float cfl, int ndir,
+                                           float dli, float dlj, float ei0, float ei1, float ej0, float ej1) {
+    const float snd = sqrtf(gam * p * rcp_approx(rho));
+    float dtmin = fminf(1e8f, dli * rcp_approx(fabsf(u * ei0 + v * ei1) + snd) * cfl);
+    if (ndir == 2) dtmin = fminf(dtmin, dlj * rcp_approx(fabsf(u * ej0 + v * ej1) + snd) * cfl);
+    return dtmin;
+}
+
 template <int RIEM, int TX, int TY, int NT, int MB>
 __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
     using L = Tile32<TX, TY>;
@@ -303,9 +313,9 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
     float2* sD2 = reinterpret_cast<float2*>(sb + L::bD);
     const float* sD = reinterpret_cast<const float*>(sD2);
     __shared__ double red[(NT / 32) * 5];
-    __shared__ double tile_part[5];
     __shared__ int s_flag;
     const int tid = threadIdx.x;
+    if (a.part_stride != NT / 32) return;   // partials are laid out one set per warp
     const Gas& g = a.gas;
     const float gam = (float)g.gamma, gm1 = (float)g.gm1, gf = (float)g.gfac;
 
@@ -351,6 +361,8 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
         const double* Pin = a.Pin + B.oc;
         const long long pc = B.pc;
         const double* scb = a.sc + 2 * B.oc;
+        const int ndir = a.cases[w.case_id].ndir;
+        const bool dt_here = a.dt_first && a.first;   // this stage computes the local time steps
 
         // ---- 1. loads ------------------------------------------------------------------------
         for (int k = tid; k < NC; k += NT) {   // FP64 cell data, asynchronous
@@ -361,9 +373,16 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             if (!a.first) {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) cp_async8(sC + v * NC + k, a.PO + B.oc + v * pc + cg);
+            } else if (dt_here) {   // the dt directions, into the planes U^n leaves free in stage 1
+                cp_async8(sC + k, scb + 2 * pc + cg);
+                cp_async8(sC + NC + k, scb + 3 * pc + cg);
+                if (ndir == 2) {
+                    cp_async8(sC + 2 * NC + k, scb + 4 * pc + cg);
+                    cp_async8(sC + 3 * NC + k, scb + 5 * pc + cg);
+                }
             }
             cp_async8(sC + 4 * NC + k, scb + cg);                                 // sur
-            if (!a.time_accurate) cp_async8(sC + 5 * NC + k, scb + pc + cg);      // dt
+            if (!a.time_accurate && !dt_here) cp_async8(sC + 5 * NC + k, scb + pc + cg);   // dt
             if (a.source) {
                 cp_async8(sC + 6 * NC + k, scb + 6 * pc + cg);
                 if (a.source == 2) cp_async8(sC + 7 * NC + k, scb + 7 * pc + cg);
@@ -569,8 +588,9 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
         // ---- 3. residual, sources, RK update (+ next dt and residual norm) -----------------------
         double acc[5] = {0.0, 0.0, 0.0, 0.0, 1e300};
         const double dt_case = __ldcg(&cs->dt_step);
-        const long long iter_next = __ldcg(&cs->iter) + (a.first ? 1 : 0) + 1;
-        const int ndir = a.cases[w.case_id].ndir;
+        // iteration whose time step is computed: this one (dt_here; the prologue has not run) or
+        // the next one (last stage)
+        const long long iter_dt = __ldcg(&cs->iter) + (dt_here || a.first ? 1 : 0) + (dt_here ? 0 : 1);
         for (int k = tid; k < NC; k += NT) {
             const int row = k / TX, col = k - row * TX;
             const int ii = i0 + col, jj = j0 + row;
@@ -610,7 +630,21 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                 r[2] = r[2] - P[0] * P[2] * fs;
                 r[3] = r[3] - (rE0 + P[3]) * fs;
             }
-            const double dt = a.time_accurate ? dt_case : sC[5 * NC + k];
+            double dt;
+            if (dt_here) {
+                // Compute_dt (Mod_dt.f90:59-104) from the step's starting state, FP32 arithmetic
+                const int sidx = (row + 2) * W + (col + 2);
+                const float dtc = cell_dt32((float)P[0], (float)P[1], (float)P[2], (float)P[3], gam,
+                                            (float)a.cfl, ndir, sD[2 * sidx], sD[2 * sidx + 1],
+                                            (float)sC[k], (float)sC[NC + k], (float)sC[2 * NC + k],
+                                            (float)sC[3 * NC + k]);
+                dt = (double)dtc;
+                if (iter_dt < a.rampa) dt = dt * (double)iter_dt / (double)a.rampa;
+                if (!a.last) a.sc[2 * B.oc + pc + cg] = dt;   // for the later stages
+                acc[4] = fmin(acc[4], dt);
+            } else {
+                dt = a.time_accurate ? dt_case : sC[5 * NC + k];
+            }
             double PO[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) PO[v] = a.first ? P[v] : sC[v * NC + k];
@@ -640,30 +674,38 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                     const double d = fabs(N[v] - PO[v]);
                     acc[v] += d * d;
                 }
-                // Compute_dt (Mod_dt.f90:59-104) in FP32 arithmetic
-                const int sidx = (row + 2) * W + (col + 2);
-                const float rho = (float)N[0], u = (float)N[1], vv = (float)N[2], p = (float)N[3];
-                const float snd = sqrtf(gam * p * rcp_approx(rho));
-                const float cfl = (float)a.cfl;
-                float dtmin = 1e8f;
-                {
-                    const float e0 = (float)scb[2 * pc + cg], e1 = (float)scb[3 * pc + cg];
-                    dtmin = fminf(dtmin, sD[2 * sidx] * rcp_approx(fabsf(u * e0 + vv * e1) + snd) * cfl);
+                if (!a.dt_first) {
+                    // Compute_dt (Mod_dt.f90:59-104) for the next step, FP32 arithmetic
+                    const int sidx = (row + 2) * W + (col + 2);
+                    const float dtc = cell_dt32((float)N[0], (float)N[1], (float)N[2], (float)N[3], gam,
+                                                (float)a.cfl, ndir, sD[2 * sidx], sD[2 * sidx + 1],
+                                                (float)scb[2 * pc + cg], (float)scb[3 * pc + cg],
+                                                ndir == 2 ? (float)scb[4 * pc + cg] : 0.0f,
+                                                ndir == 2 ? (float)scb[5 * pc + cg] : 0.0f);
+                    double dtn = (double)dtc;
+                    if (iter_dt < a.rampa) dtn = dtn * (double)iter_dt / (double)a.rampa;
+                    if (!a.time_accurate) a.sc[2 * B.oc + pc + cg] = dtn;
+                    acc[4] = fmin(acc[4], dtn);
                 }
-                if (ndir == 2) {
-                    const float e0 = (float)scb[4 * pc + cg], e1 = (float)scb[5 * pc + cg];
-                    dtmin = fminf(dtmin, sD[2 * sidx + 1] * rcp_approx(fabsf(u * e0 + vv * e1) + snd) * cfl);
-                }
-                double dtn = (double)dtmin;
-                if (iter_next < a.rampa) dtn = dtn * (double)iter_next / (double)a.rampa;
-                if (!a.time_accurate) a.sc[2 * B.oc + pc + cg] = dtn;
-                acc[4] = fmin(acc[4], dtn);
             }
         }
-        if (a.last) {
-            block_reduce_store<NT>(acc, red, tile_part);
-            if (tid == 0)
-                for (int k = 0; k < 5; ++k) a.part[5 * (size_t)it + k] = tile_part[k];
+        if (a.last || dt_here) {   // per-warp partials: residual sums (last stage), dt min
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                double v = acc[k];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double u = __shfl_down_sync(0xffffffffu, v, o);
+                    v = (k < 4) ? v + u : fmin(v, u);
+                }
+                acc[k] = v;
+            }
+            if (lane == 0) {
+                double* pp = a.part + ((size_t)it * (NT / 32) + (tid >> 5)) * 5;
+                if (a.last)
+                    for (int k = 0; k < 4; ++k) pp[k] = acc[k];
+                if (a.dt_first ? dt_here : a.last) pp[4] = acc[4];
+            }
         }
         stage_item_end<NT>(a, it, w.case_id, red, &s_flag);
     }

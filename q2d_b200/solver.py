@@ -121,6 +121,26 @@ class Q2DSolver:
         self._call("download_prim", self.ctx, self.block_ids[case][block], _abi.dptr(P))
         return P[2:b.nj + 2, 2:b.ni + 2, :].copy()
 
+    def prims(self) -> list:
+        """Interior states of every block of every case, [case][block] -> (nj, ni, 4), read
+        by one many-block transfer (q2d_gpu_download_prim_many)."""
+        arrs, ids = [], []
+        for c, cs in enumerate(self.cases):
+            for k, b in enumerate(cs.blocks):
+                arrs.append(np.zeros((b.nj + 4, b.ni + 4, 4)))
+                ids.append(self.block_ids[c][k])
+        ptrs = (C.POINTER(C.c_double) * max(len(arrs), 1))(*[_abi.dptr(a) for a in arrs])
+        idv = (C.c_int * max(len(ids), 1))(*ids)
+        self._call("download_prim_many", self.ctx, len(ids), idv, ptrs)
+        out, k = [], 0
+        for cs in self.cases:
+            row = []
+            for b in cs.blocks:
+                row.append(arrs[k][2:b.nj + 2, 2:b.ni + 2, :].copy())
+                k += 1
+            out.append(row)
+        return out
+
     def solve(self, max_calls: int = 10 ** 9, steps_per_call: int = 1) -> dict:
         """Runs until every case reports TODO = END (or an error)."""
         for _ in range(max_calls):

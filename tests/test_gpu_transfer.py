@@ -68,3 +68,66 @@ def test_error_isolation_between_cases(precision):
     for c in (0, 2, 3):
         assert bad_i[c]["err"] == 0 and bad_i[c]["iter"] == 10 == ref_i[c]["iter"]
         assert np.array_equal(bad_s[c], ref_s[c])
+
+
+def _ghosted(b, rng, fill):
+    interior = 1.0 + rng.random((b.nj, b.ni, 4))
+    P = np.full((b.nj + 4, b.ni + 4, 4), fill)
+    P[2:-2, 2:-2] = interior
+    return P, interior
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_many_block_round_trip(precision):
+    """q2d_gpu_upload_prim_many / q2d_gpu_download_prim_many over every block of a batch with
+    multi-block cases: each block gets exactly its own array, ghosts untouched, and the result
+    equals the single-block transfers."""
+    batch = [cases.nozzle_axi(96, 24, nblocks=3), cases.ramp(70, 23, seed=2), cases.closed_box(17, 9)]
+    s = Q2DSolver(make_options(batch[0], precision=precision), batch)
+    try:
+        s.step(1)
+        rng = np.random.default_rng(4)
+        ids, ups, interiors = [], [], []
+        for c, cs in enumerate(batch):
+            for k, b in enumerate(cs.blocks):
+                P, inner = _ghosted(b, rng, -3.0)
+                ids.append(s.block_ids[c][k])
+                ups.append(P)
+                interiors.append(inner)
+        n = len(ids)
+        idv = (C.c_int * n)(*ids)
+        pin = (C.POINTER(C.c_double) * n)(*[_abi.dptr(a) for a in ups])
+        assert s.lib.q2d_gpu_upload_prim_many(s.ctx, n, idv, pin) == 0
+        downs = [np.full_like(a, 9.0) for a in ups]
+        pout = (C.POINTER(C.c_double) * n)(*[_abi.dptr(a) for a in downs])
+        assert s.lib.q2d_gpu_download_prim_many(s.ctx, n, idv, pout) == 0
+        for Q, inner in zip(downs, interiors):
+            assert np.array_equal(Q[2:-2, 2:-2], inner)
+            ghosts = np.ones(Q.shape[:2], bool)
+            ghosts[2:-2, 2:-2] = False
+            assert np.all(Q[ghosts] == 9.0)
+        flat = [p for row in s.prims() for p in row]
+        for got, inner in zip(flat, interiors):
+            assert np.array_equal(got, inner)
+        bad = (C.c_int * 1)(10 ** 6)
+        assert s.lib.q2d_gpu_download_prim_many(s.ctx, 1, bad, pout) == _abi.ERR_BADARG
+    finally:
+        s.close()
+
+
+def test_many_block_transfer_wraps_the_staging_ring():
+    """More state than one staging ring (128 MiB of doubles): the transfer waits for the ring
+    and reuses it, and every block still arrives intact."""
+    batch = [cases.closed_box(1600, 1200, seed=s) for s in range(3)]    # 5.76M cells, 184 MB
+    s = Q2DSolver(make_options(batch[0], precision=1), batch)
+    try:
+        s.step(1)
+        rng = np.random.default_rng(5)
+        ups, inners = zip(*[_ghosted(cs.blocks[0], rng, 0.0) for cs in batch])
+        ids = (C.c_int * 3)(*[s.block_ids[c][0] for c in range(3)])
+        pin = (C.POINTER(C.c_double) * 3)(*[_abi.dptr(a) for a in ups])
+        assert s.lib.q2d_gpu_upload_prim_many(s.ctx, 3, ids, pin) == 0
+        for got, inner in zip(s.prims(), inners):
+            assert np.array_equal(got[0], inner)
+    finally:
+        s.close()
