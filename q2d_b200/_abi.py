@@ -144,7 +144,8 @@ def build_library(force: bool = False) -> Path:
 def _stale(target: Path, src_dir: Path) -> bool:
     t = target.stat().st_mtime
     files = list(src_dir.glob("*.cu")) + list(src_dir.glob("*.cuh")) + list(src_dir.glob("*.h")) \
-        + list(src_dir.glob("*.cpp")) + [REPO / "include" / "q2d_gpu.h", src_dir / "Makefile"]
+        + list(src_dir.glob("*.cpp")) + list((ROOT / "host").glob("*.cpp")) \
+        + [REPO / "include" / "q2d_gpu.h", src_dir / "Makefile"]
     return any(f.exists() and f.stat().st_mtime > t for f in files)
 
 

@@ -1,0 +1,170 @@
+"""The command-line host (q2d_b200/lib/q2d_host): reads a case directory in the reference's
+formats (input.ini, INPUT/bc.txt, INPUT/ic.tec, INPUT/block<b>_area.dat, INPUT/phase.txt) and
+runs it through the C ABI, as the Fortran host's Q2D_setup / Q2D_solve would.
+
+CPU tests run its --check mode (inputs parsed, no GPU); GPU tests run cases end to end and
+compare the written OUTPUT/field.tec with the same cases run through the Python binding, and
+the Shu-Osher run with the reference binary's own output."""
+import json
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from q2d_b200 import _abi, cases, make_options, refio
+from q2d_b200.solver import Q2DSolver
+
+GOLD = Path(__file__).resolve().parent / "golden"
+OPT_FIELDS = ["limiter", "riemann", "n_rk", "time_accurate", "source", "rampa_iter", "res_diter",
+              "sol_diter", "itermax", "cfl", "res_threshold", "time_threshold", "sol_dtime", "gas_R"]
+
+
+def host(*args, check=True):
+    r = subprocess.run([str(refio.host_binary()), *map(str, args)], capture_output=True, text=True, timeout=600)
+    if check and r.returncode != 0:
+        raise AssertionError(f"q2d_host {args}: rc={r.returncode}\n{r.stdout}\n{r.stderr}")
+    return r
+
+
+def small_cases():
+    return {
+        "ramp": cases.ramp(40, 12, seed=5),
+        "nozzle_axi": cases.nozzle_axi(48, 10, nblocks=3, seed=6),
+        "area_nozzle": cases.area_nozzle_batch(n=2, seed=7, nx_range=(40, 60), ny_range=(8, 10))[0],
+        "shuosher": cases.shuosher(ni=64),
+        "riemann1d": cases.riemann_1d(ni=50, nj=4, seed=8),
+    }
+
+
+def rec_tuple(r):
+    alpha = r.get("alpha", 0.0)
+    t = r["type"]
+    if t not in (401, 405):
+        alpha = 0.0
+    alpha = -1.0 if alpha >= 0.5 * _abi.NORMAL_DIR else alpha
+    keep = {401: ("T0", "p0", "rel_fac"), 405: ("mach", "T0", "pamb", "rel_fac"), 406: ("pamb", "rel_fac")}.get(t, ())
+    vals = [float(r[k]) if k in keep else (1.0 if k == "rel_fac" else 0.0)
+            for k in ("T0", "p0", "pamb", "mach")] + [alpha, float(r.get("rel_fac", 1.0)) if "rel_fac" in keep else 1.0]
+    ints = [r["b"], r["i"], r["j"], r["f"], t]
+    conn = [r.get("bs", 0), r.get("is_", r.get("is", 0)), r.get("js", 0), r.get("fs", 0),
+            r.get("d11", 0), r.get("d12", 0), r.get("d21", 0), r.get("d22", 0)] if t == 101 else [0] * 8
+    return ints + conn + vals
+
+
+@pytest.mark.parametrize("name", ["ramp", "nozzle_axi", "area_nozzle", "shuosher", "riemann1d"])
+def test_check_mode_reads_what_was_written(tmp_path, name):
+    cs = small_cases()[name]
+    refio.write_case(cs, tmp_path)
+    o = make_options(cs)
+    d = json.loads(host(tmp_path, "--check", "--gamma", repr(o.gas_gamma)).stdout)
+    for k in OPT_FIELDS:
+        assert d[k] == pytest.approx(getattr(o, k), rel=1e-15), k
+    assert d["gas_gamma"] == o.gas_gamma
+    assert d["unsupported"] == []
+    assert [(b["ni"], b["nj"]) for b in d["blocks"]] == [(b.ni, b.nj) for b in cs.blocks]
+    for got, B in zip(d["blocks"], cs.blocks):
+        assert got["prim_sum"] == pytest.approx(float(np.sum(B.prim[..., 0]) + np.sum(B.prim[..., 1]) +
+                                                      np.sum(B.prim[..., 2]) + np.sum(B.prim[..., 3])), rel=1e-12)
+        if B.area is not None:
+            assert got["area_sum"] == pytest.approx(float(np.sum(B.area)), rel=1e-12)
+    assert len(d["bcs"]) == len(cs.bcs)
+    for got, r in zip(d["bcs"], cs.bcs):
+        assert got[:13] == rec_tuple(r)[:13]
+        assert got[13:] == pytest.approx(rec_tuple(r)[13:], rel=1e-15)
+
+
+def test_check_mode_limiter_keywords(tmp_path):
+    """Setup_Space_Scheme / Assign_Limiter (Mod_Space.f90:18-78): MUSCL with 'none' is van Leer,
+    the keyword is case-sensitive (lower-case 'limo3' is first order), and the limiter applies
+    whatever the reconstruction keyword says."""
+    cs = cases.ramp(20, 8)
+    refio.write_case(cs, tmp_path)
+    ini = (tmp_path / "input.ini").read_text()
+    base = ini.replace("space-reconstruction = MUSCL\n", "").replace("flux-limiter = vanleer\n", "")
+    for recon, lim, want in [("MUSCL", "none", 2), ("MUSCL", "limo3", 0), ("MUSCL", "LIMO3", 6),
+                             ("first-order", "minmod", 1), ("MUSCL", "", 0), ("MUSCL", "superbee", 5)]:
+        extra = f"space-reconstruction = {recon}\n" + (f"flux-limiter = {lim}\n" if lim else "")
+        (tmp_path / "input.ini").write_text(base.replace("[Q2D-Numerics]\n", "[Q2D-Numerics]\n" + extra))
+        assert json.loads(host(tmp_path, "--check").stdout)["limiter"] == want, (recon, lim)
+
+
+def test_inputs_outside_the_path_fail_loudly(tmp_path):
+    cs = cases.ramp(20, 8)
+    refio.write_case(cs, tmp_path)
+    ini = (tmp_path / "input.ini").read_text()
+    (tmp_path / "input.ini").write_text(ini.replace("[Q2D-Numerics]\n", "[Q2D-Numerics]\nirs-beta = 0.5\n")
+                                        .replace("riemann-solver = HLLC", "riemann-solver = SLAU"))
+    d = json.loads(host(tmp_path, "--check").stdout)
+    assert "[Q2D-Numerics] irs-beta = 0.5" in d["unsupported"]
+    assert "[Q2D-Numerics] riemann-solver = SLAU" in d["unsupported"]
+    r = host(tmp_path, check=False)   # refused before any device call
+    assert r.returncode == 2 and "not on the built path" in r.stderr
+    (tmp_path / "input.ini").write_text(ini)
+    bc = (tmp_path / "INPUT" / "bc.txt").read_text().splitlines()
+    bc[0] = bc[0][:-8] + f"{410:8d}"
+    (tmp_path / "INPUT" / "bc.txt").write_text("\n".join(bc) + "\n")
+    r = host(tmp_path, "--check", check=False)
+    assert r.returncode == 1 and "410" in r.stderr
+
+
+def test_reads_list_directed_records_across_lines(tmp_path):
+    """Read_BCfile uses list-directed READs: a record may span lines, commas separate values and
+    anything after the needed values on a line is skipped."""
+    cs = cases.ramp(6, 4)
+    refio.write_case(cs, tmp_path)
+    txt = (tmp_path / "INPUT" / "bc.txt").read_text().splitlines()
+    out = []
+    for line in txt:
+        t = line.split()
+        if len(t) == 5 and t[4] == "405":
+            out += [f"{t[0]}, {t[1]}, {t[2]}", f"{t[3]} {t[4]}  ! trailing text"]
+        else:
+            out.append(line)
+    (tmp_path / "INPUT" / "bc.txt").write_text("\n".join(out) + "\n")
+    d = json.loads(host(tmp_path, "--check").stdout)
+    assert len(d["bcs"]) == len(cs.bcs)
+    assert [r[4] for r in d["bcs"]] == [r["type"] for r in cs.bcs]
+
+
+def _python_run(cs, steps, precision):
+    s = Q2DSolver(make_options(cs, precision=precision), [cs])
+    try:
+        s.step(steps, check=False)
+        return [s.prim(0, b) for b in range(len(cs.blocks))], s.info(0)
+    finally:
+        s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,precision", [("ramp", "fp64"), ("nozzle_axi", "fp64"), ("area_nozzle", "fp32-flux")])
+def test_host_run_equals_library_run(tmp_path, name, precision):
+    cs = small_cases()[name]
+    steps = 25
+    refio.write_case(cs, tmp_path, itermax=steps)
+    o = make_options(cs)
+    r = host(tmp_path, "--precision", precision, "--gamma", repr(o.gas_gamma), "--steps-per-call", 10)
+    assert "converged/ended after 25 steps" in r.stdout
+    got = refio.read_field(tmp_path / "OUTPUT" / "field.tec")
+    want, info = _python_run(cs, steps, 0 if precision == "fp64" else 1)
+    assert info["iter"] == steps
+    for g, w, B in zip(got, want, cs.blocks):
+        assert np.array_equal(g.nodes, np.asarray(B.nodes))
+        assert np.array_equal(g.prim, w)
+    hist = np.loadtxt(tmp_path / "OUTPUT" / "residuals.dat")
+    assert hist[-1, 0] == steps and hist[-1, 3] == pytest.approx(info["residual"][0], rel=1e-15)
+
+
+@pytest.mark.gpu
+def test_host_shuosher_matches_reference_binary(tmp_path):
+    """End to end from the reference's formats: the Shu-Osher case directory (N=400, MC, HLLC,
+    RK3, CFL 0.5, time-accurate to t=1.8) run by q2d_host on the GPU reproduces the density the
+    reference binary wrote (test/1D/ShuOsher-LIMO3/reference/baseline_mc.dat) to <= 1e-8
+    relative L1, the gate the oracle meets."""
+    cs = cases.shuosher()
+    refio.write_case(cs, tmp_path, limiter="mc")
+    host(tmp_path, "--steps-per-call", 200, "--quiet")
+    ref = np.loadtxt(GOLD / "shuosher_mc.txt")
+    rho = refio.read_field(tmp_path / "OUTPUT" / "field.tec")[0].prim[0, :, 0]
+    rel_l1 = np.abs(rho - ref[:, 1]).sum() / np.abs(ref[:, 1]).sum()
+    assert rel_l1 <= 1e-8, rel_l1
