@@ -181,11 +181,15 @@ def serving_leg(args, lib):
     log-normal sizes in [4e3, 2e6] cells, admitted by memory budget into one serving context
     (FP32-flux / FP64-state), retired on a 1e-8 relative residual drop or at the iteration cap.
     Beside it, a sample of the same requests solved one after another through the plain FP64
-    path (one context per request, wall clock including setup and read-back, as for serving)."""
+    path (one context per request, wall clock including setup and read-back, as for serving).
+    The payloads of both are generated before the timed region; admission (validation, metrics,
+    upload) is timed."""
     from q2d_b200 import _abi, make_options
     from q2d_b200.serve import request_stream, serve, serve_options
     from q2d_b200.solver import Q2DSolver
     reqs = request_stream(args.serve_rate, args.serve_seconds)
+    for r in reqs:   # the request payloads (grid, initial state, boundary records) come from clients
+        r.build()
     opts = serve_options(itermax=args.serve_iters, drop=1e-8)
     st = serve(reqs, opts, device_bytes=int(args.serve_gb * (1 << 30)), max_cases=4096, steps_per_call=10)
     # sequential plain FP64 on the first requests of the same stream

@@ -31,9 +31,11 @@ class BlockSpec:
     prim: np.ndarray
     area: Optional[np.ndarray] = None
 
-    def prim_ghost(self) -> np.ndarray:
-        """The interior state embedded in the reference layout P(4, -1:ni+2, -1:nj+2)."""
-        P = np.zeros((self.nj + 4, self.ni + 4, 4))
+    def prim_ghost(self, ghosts: Optional[float] = 0.0) -> np.ndarray:
+        """The interior state embedded in the reference layout P(4, -1:ni+2, -1:nj+2); the ghost
+        layers hold `ghosts` (None leaves them unset: the C ABI never reads them)."""
+        P = np.empty((self.nj + 4, self.ni + 4, 4)) if ghosts is None else \
+            np.full((self.nj + 4, self.ni + 4, 4), ghosts)
         P[2:self.nj + 2, 2:self.ni + 2, :] = self.prim
         return P
 

@@ -32,9 +32,13 @@ namespace {
 
 // Device images of one block, built on the host when its case is prepared and copied to the
 // block's regions when the case is uploaded.
+// Host images of a block's device planes, in one buffer: a slice of the context's pinned
+// staging area when it has room (serving), else a heap buffer of its own.
 struct Staged {
-    std::vector<double> pa, sc, dl, fi, fj;
-    std::vector<float> dl32, fi4, fj4;   // FP32 geometry of the FP32-flux form
+    double *pa = nullptr, *sc = nullptr, *dl = nullptr, *fi = nullptr, *fj = nullptr;
+    float *dl32 = nullptr, *fi4 = nullptr, *fj4 = nullptr;   // FP32 geometry of the FP32-flux form
+    size_t n_pa = 0, n_sc = 0, n_dl = 0, n_fi = 0, n_fj = 0, n_dl32 = 0, n_fi4 = 0, n_fj4 = 0;
+    std::unique_ptr<char[]> heap;
 };
 
 struct HBlock {
@@ -160,6 +164,8 @@ struct q2d_ctx {
     DevBuf<BCParam> bcp;
     DevBuf<int> flag;
     CaseState* h_state = nullptr;   // pinned mirror
+    char* pin = nullptr;            // pinned staging area of admissions (serving contexts)
+    size_t pin_cap = 0, pin_used = 0;
     int n_items = 0;
     std::map<int, cudaGraphExec_t> graphs;
     std::map<int, int> graph_kernels;
@@ -475,6 +481,37 @@ bool reserve_regions(q2d_ctx* ctx, int c) {
 
 // Host half of materialising a case: edge records, device regions, metrics (Setup_Metrics
 // restated on the host) and the device images of every block, staged for upload.
+// Carves the images of one block out of the pinned staging area (bump allocation, reset once
+// the uploads that read it have completed) or, when it is full, out of a heap buffer.
+void stage_alloc(q2d_ctx* ctx, Staged& S, const DBlock& d, bool fp32) {
+    auto al = [](size_t bytes) { return (bytes + 255) & ~size_t(255); };
+    S.n_pa = 4 * (size_t)d.pc; S.n_sc = 8 * (size_t)d.pc; S.n_dl = 2 * (size_t)d.pg;
+    S.n_fi = 3 * (size_t)d.pfi; S.n_fj = 3 * (size_t)d.pfj;
+    S.n_dl32 = fp32 ? 2 * (size_t)d.pg : 0; S.n_fi4 = fp32 ? 4 * (size_t)d.pfi : 0;
+    S.n_fj4 = fp32 ? 4 * (size_t)d.pfj : 0;
+    const size_t sizes[8] = {al(8 * S.n_pa), al(8 * S.n_sc), al(8 * S.n_dl), al(8 * S.n_fi), al(8 * S.n_fj),
+                             al(4 * S.n_dl32), al(4 * S.n_fi4), al(4 * S.n_fj4)};
+    size_t total = 0;
+    for (size_t s : sizes) total += s;
+    char* base;
+    if (ctx->pin && ctx->pin_used + total <= ctx->pin_cap) {
+        base = ctx->pin + ctx->pin_used;
+        ctx->pin_used += total;
+    } else {
+        S.heap.reset(new char[total]);
+        base = S.heap.get();
+    }
+    char* p = base;
+    S.pa = reinterpret_cast<double*>(p); p += sizes[0];
+    S.sc = reinterpret_cast<double*>(p); p += sizes[1];
+    S.dl = reinterpret_cast<double*>(p); p += sizes[2];
+    S.fi = reinterpret_cast<double*>(p); p += sizes[3];
+    S.fj = reinterpret_cast<double*>(p); p += sizes[4];
+    S.dl32 = fp32 ? reinterpret_cast<float*>(p) : nullptr; p += sizes[5];
+    S.fi4 = fp32 ? reinterpret_cast<float*>(p) : nullptr; p += sizes[6];
+    S.fj4 = fp32 ? reinterpret_cast<float*>(p) : nullptr;
+}
+
 int prepare_case(q2d_ctx* ctx, int c) {
     HCase& cs = ctx->cases[c];
     if (int e = build_case_edges(ctx, c)) return e;
@@ -498,43 +535,68 @@ int prepare_case(q2d_ctx* ctx, int c) {
         const DBlock& d = b.d;
         const HostGeom& G = geo[lb];
         const long long n = (long long)b.ni * b.nj;
+        const long long ngh = (long long)(b.ni + 4) * (b.nj + 4), nfi = (long long)(b.ni + 1) * b.nj,
+                        nfj = (long long)b.ni * (b.nj + 1);
+        const long long pc = d.pc, pg = d.pg, pfi = d.pfi, pfj = d.pfj;
+        const bool fp32 = ctx->opt.precision == Q2D_PREC_FP32_FLUX;
         Staged& S = b.staged;
-        S.sc.assign(8 * (size_t)d.pc, 0.0);
-        S.dl.assign(2 * (size_t)d.pg, 0.0);
-        S.fi.assign(3 * (size_t)d.pfi, 0.0);
-        S.fj.assign(3 * (size_t)d.pfj, 0.0);
-        S.pa.assign(4 * (size_t)d.pc, 0.0);
-        for (int j = 0; j < b.nj; ++j)
-            for (int i = 0; i < b.ni; ++i) {
-                const long long k = (long long)j * b.ni + i;
-                double v[4];
-                versors(G, i, j, v);
-                S.sc[k] = G.sur[G.g(i, j)];
-                S.sc[2 * d.pc + k] = v[0];
-                S.sc[3 * d.pc + k] = v[1];
-                S.sc[4 * d.pc + k] = v[2];
-                S.sc[5 * d.pc + k] = v[3];
-                S.sc[6 * d.pc + k] = G.src0[k];
-                S.sc[7 * d.pc + k] = G.src1[k];
+        // images of the device planes, filled in parallel; padding and the dt plane are zero
+        stage_alloc(ctx, S, d, fp32);
+        parallel_zero(S.sc, (size_t)pc, 2 * (size_t)pc);   // dt
+        for (int v = 0; v < 8; ++v) parallel_zero(S.sc, v * (size_t)pc + n, (v + 1) * (size_t)pc);
+        for (int v = 0; v < 4; ++v) parallel_zero(S.pa, v * (size_t)pc + n, (v + 1) * (size_t)pc);
+        for (int v = 0; v < 2; ++v) parallel_zero(S.dl, v * (size_t)pg + ngh, (v + 1) * (size_t)pg);
+        for (int q = 0; q < 3; ++q) parallel_zero(S.fi, q * (size_t)pfi + nfi, (q + 1) * (size_t)pfi);
+        for (int q = 0; q < 3; ++q) parallel_zero(S.fj, q * (size_t)pfj + nfj, (q + 1) * (size_t)pfj);
+        if (fp32) {
+            for (int v = 0; v < 2; ++v) parallel_zero(S.dl32, v * (size_t)pg + ngh, (v + 1) * (size_t)pg);
+            parallel_zero(S.fi4, 4 * (size_t)nfi, 4 * (size_t)pfi);
+            parallel_zero(S.fj4, 4 * (size_t)nfj, 4 * (size_t)pfj);
+        }
+        parallel_rows(b.nj, 160L * b.ni, [&](long long r0, long long r1) {
+            for (int j = (int)r0; j < (int)r1; ++j)
+                for (int i = 0; i < b.ni; ++i) {
+                    const long long k = (long long)j * b.ni + i;
+                    double v[4];
+                    versors(G, i, j, v);
+                    S.sc[k] = G.sur[G.g(i, j)];
+                    S.sc[2 * pc + k] = v[0];
+                    S.sc[3 * pc + k] = v[1];
+                    S.sc[4 * pc + k] = v[2];
+                    S.sc[5 * pc + k] = v[3];
+                    S.sc[6 * pc + k] = G.src0[k];
+                    S.sc[7 * pc + k] = G.src1[k];
+                    for (int q = 0; q < 4; ++q) S.pa[q * pc + k] = b.prim[(size_t)q * n + k];
+                }
+        });
+        parallel_rows(ngh, 32, [&](long long k0, long long k1) {
+            for (long long k = k0; k < k1; ++k) {
+                S.dl[k] = G.dl[2 * k];
+                S.dl[pg + k] = G.dl[2 * k + 1];
+                if (fp32) {
+                    S.dl32[k] = (float)G.dl[2 * k];
+                    S.dl32[pg + k] = (float)G.dl[2 * k + 1];
+                }
             }
-        for (long long k = 0; k < (long long)(b.ni + 4) * (b.nj + 4); ++k) {
-            S.dl[k] = G.dl[2 * k];
-            S.dl[d.pg + k] = G.dl[2 * k + 1];
-        }
-        for (long long k = 0; k < (long long)(b.ni + 1) * b.nj; ++k)
-            for (int q = 0; q < 3; ++q) S.fi[q * d.pfi + k] = G.fi[3 * k + q];
-        for (long long k = 0; k < (long long)b.ni * (b.nj + 1); ++k)
-            for (int q = 0; q < 3; ++q) S.fj[q * d.pfj + k] = G.fj[3 * k + q];
-        for (int v = 0; v < 4; ++v) std::memcpy(&S.pa[v * d.pc], &b.prim[(size_t)v * n], sizeof(double) * n);
-        if (ctx->opt.precision == Q2D_PREC_FP32_FLUX) {
-            S.dl32.assign(S.dl.begin(), S.dl.end());
-            S.fi4.assign(4 * (size_t)d.pfi, 0.0f);
-            S.fj4.assign(4 * (size_t)d.pfj, 0.0f);
-            for (long long k = 0; k < (long long)(b.ni + 1) * b.nj; ++k)
-                for (int q = 0; q < 3; ++q) S.fi4[4 * k + q] = (float)G.fi[3 * k + q];
-            for (long long k = 0; k < (long long)b.ni * (b.nj + 1); ++k)
-                for (int q = 0; q < 3; ++q) S.fj4[4 * k + q] = (float)G.fj[3 * k + q];
-        }
+        });
+        parallel_rows(nfi, 48, [&](long long k0, long long k1) {
+            for (long long k = k0; k < k1; ++k)
+                for (int q = 0; q < 3; ++q) {
+                    S.fi[q * pfi + k] = G.fi[3 * k + q];
+                    if (fp32) S.fi4[4 * k + q] = (float)G.fi[3 * k + q];
+                }
+            if (fp32)
+                for (long long k = k0; k < k1; ++k) S.fi4[4 * k + 3] = 0.0f;
+        });
+        parallel_rows(nfj, 48, [&](long long k0, long long k1) {
+            for (long long k = k0; k < k1; ++k)
+                for (int q = 0; q < 3; ++q) {
+                    S.fj[q * pfj + k] = G.fj[3 * k + q];
+                    if (fp32) S.fj4[4 * k + q] = (float)G.fj[3 * k + q];
+                }
+            if (fp32)
+                for (long long k = k0; k < k1; ++k) S.fj4[4 * k + 3] = 0.0f;
+        });
         b.prim.clear();
         b.prim.shrink_to_fit();
         geo[lb] = HostGeom{};
@@ -544,27 +606,32 @@ int prepare_case(q2d_ctx* ctx, int c) {
 }
 
 // Device half: copies the staged images into the case's regions and starts its run state.
-// Called only while no work is in flight on the context's stream.
+// Called only while no work is in flight on the context's stream. The copies are queued on the
+// stream; images in the pinned staging area stay allocated until finish_uploads().
 int upload_case(q2d_ctx* ctx, int c) {
     HCase& cs = ctx->cases[c];
+    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+    cudaStream_t s = ctx->stream;
     for (int gb : cs.blocks) {
         HBlock& b = ctx->blocks[gb];
         const DBlock& d = b.d;
         Staged& S = b.staged;
-        CK(cudaMemcpy(ctx->PA.p + d.oc, S.pa.data(), sizeof(double) * S.pa.size(), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ctx->SC.p + 2 * d.oc, S.sc.data(), sizeof(double) * S.sc.size(), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ctx->DL.p + d.og, S.dl.data(), sizeof(double) * S.dl.size(), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ctx->FI.p + d.ofi, S.fi.data(), sizeof(double) * S.fi.size(), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ctx->FJ.p + d.ofj, S.fj.data(), sizeof(double) * S.fj.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(ctx->PA.p + d.oc, S.pa, sizeof(double) * S.n_pa, h2d, s));
+        CK(cudaMemcpyAsync(ctx->SC.p + 2 * d.oc, S.sc, sizeof(double) * S.n_sc, h2d, s));
+        CK(cudaMemcpyAsync(ctx->DL.p + d.og, S.dl, sizeof(double) * S.n_dl, h2d, s));
+        CK(cudaMemcpyAsync(ctx->FI.p + d.ofi, S.fi, sizeof(double) * S.n_fi, h2d, s));
+        CK(cudaMemcpyAsync(ctx->FJ.p + d.ofj, S.fj, sizeof(double) * S.n_fj, h2d, s));
         if (ctx->DL32.p) {   // face offsets are multiples of 32, so float index 2*off is 16-byte aligned
-            CK(cudaMemcpy(ctx->DL32.p + d.og, S.dl32.data(), sizeof(float) * S.dl32.size(), cudaMemcpyHostToDevice));
-            CK(cudaMemcpy(ctx->FI4.p + 2 * d.ofi, S.fi4.data(), sizeof(float) * S.fi4.size(), cudaMemcpyHostToDevice));
-            CK(cudaMemcpy(ctx->FJ4.p + 2 * d.ofj, S.fj4.data(), sizeof(float) * S.fj4.size(), cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync(ctx->DL32.p + d.og, S.dl32, sizeof(float) * S.n_dl32, h2d, s));
+            CK(cudaMemcpyAsync(ctx->FI4.p + 2 * d.ofi, S.fi4, sizeof(float) * S.n_fi4, h2d, s));
+            CK(cudaMemcpyAsync(ctx->FJ4.p + 2 * d.ofj, S.fj4, sizeof(float) * S.n_fj4, h2d, s));
         }
+        if (S.heap) CK(cudaStreamSynchronize(s));   // a heap image is freed right away
         S = Staged{};
     }
-    const CaseState s = fresh_state(cs.time0);
-    CK(cudaMemcpy(ctx->cstate.p + c, &s, sizeof(CaseState), cudaMemcpyHostToDevice));
+    const CaseState st = fresh_state(cs.time0);
+    CK(cudaMemcpyAsync(ctx->cstate.p + c, &st, sizeof(CaseState), h2d, s));
+    CK(cudaStreamSynchronize(s));   // st is on this stack frame
     cs.resident = true;
     ctx->dt_new = true;
     return Q2D_OK;
@@ -656,6 +723,7 @@ int apply_pending(q2d_ctx* ctx) {
         if (cs.used && cs.prepared && !cs.resident)
             if (int e = upload_case(ctx, (int)c)) return e;
     }
+    ctx->pin_used = 0;   // every staged image has been uploaded (upload_case waits for its copies)
     if (int e = rebuild_device_lists(ctx)) return e;
     ctx->dirty = false;
     return Q2D_OK;
@@ -819,12 +887,15 @@ int check_recs(q2d_ctx* ctx, const HCase& cs, const std::vector<q2d_bc_rec>& v) 
 // Fortran P(1:4, -1:ni+2, -1:nj+2) (ghost frame of 2) -> 4 interior planes
 void fortran_to_planes(int ni, int nj, const double* P, std::vector<double>& planes) {
     const long long n = (long long)ni * nj;
-    planes.assign(4 * n, 0.0);
-    for (int j = 0; j < nj; ++j)
-        for (int i = 0; i < ni; ++i) {
-            const double* src = &P[4 * ((size_t)(i + 2) + (size_t)(ni + 4) * (j + 2))];
-            for (int v = 0; v < 4; ++v) planes[v * n + (size_t)j * ni + i] = src[v];
-        }
+    planes.resize(4 * n);
+    double* out = planes.data();
+    parallel_rows(nj, 64L * ni, [=](long long r0, long long r1) {
+        for (long long j = r0; j < r1; ++j)
+            for (int i = 0; i < ni; ++i) {
+                const double* src = &P[4 * ((size_t)(i + 2) + (size_t)(ni + 4) * (j + 2))];
+                for (int v = 0; v < 4; ++v) out[v * n + (size_t)j * ni + i] = src[v];
+            }
+    });
 }
 
 q2d_ctx* new_ctx(const q2d_options* opt) {
@@ -1171,6 +1242,11 @@ int q2d_serve_create(q2d_ctx** out, const q2d_options* opt, unsigned long long d
                     efj = efi;
     int e = allocate_pools(ctx, ec, eg, efi, efj, max_cases);
     if (!e) e = rebuild_device_lists(ctx);
+    if (!e) {   // pinned staging of admissions; without it they stage in pageable memory
+        const size_t cap = (size_t)std::min<unsigned long long>(2ull << 30, device_bytes / 2);
+        if (cudaHostAlloc(&ctx->pin, cap, cudaHostAllocDefault) == cudaSuccess) ctx->pin_cap = cap;
+        else { ctx->pin = nullptr; cudaGetLastError(); }
+    }
     if (e) {
         q2d_gpu_destroy(ctx);
         return e;
@@ -1277,6 +1353,7 @@ void q2d_gpu_destroy(q2d_ctx* ctx) {
     ctx->dcases.release(); ctx->cstate.release(); ctx->items.release(); ctx->edges.release();
     ctx->bcp.release(); ctx->flag.release();
     if (ctx->h_state) cudaFreeHost(ctx->h_state);
+    if (ctx->pin) cudaFreeHost(ctx->pin);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

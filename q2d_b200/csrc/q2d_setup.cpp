@@ -43,19 +43,95 @@ inline P2 l2(P2 a, P2 b) { return P2{2.0 * a.x - b.x, 2.0 * a.y - b.y}; }
 
 }  // namespace
 
+SetupPool& SetupPool::get() {
+    static SetupPool pool;
+    return pool;
+}
+
+SetupPool::SetupPool() {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int n = std::min(15, hw - 1);
+    for (int k = 0; k < n; ++k) th_.emplace_back([this] { loop(); });
+}
+
+SetupPool::~SetupPool() {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+}
+
+void SetupPool::loop() {
+    unsigned long long seen = 0;
+    for (;;) {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+        while (next_ < T_) {   // take chunks 1..T-1 of this generation
+            const int t = next_++;
+            const std::function<void(int)>* fn = fn_;
+            lk.unlock();
+            (*fn)(t);
+            lk.lock();
+            if (--pending_ == 0) done_cv_.notify_one();
+        }
+    }
+}
+
+void SetupPool::run(int T, const std::function<void(int)>& fn) {
+    std::lock_guard<std::mutex> serial(run_mu_);
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        fn_ = &fn;
+        T_ = T;
+        next_ = 1;
+        pending_ = T - 1;
+        ++gen_;
+    }
+    cv_.notify_all();
+    fn(0);
+    std::unique_lock<std::mutex> lk(mu_);
+    while (next_ < T_) {   // help with chunks no worker has taken yet
+        const int t = next_++;
+        lk.unlock();
+        fn(t);
+        lk.lock();
+        --pending_;
+    }
+    done_cv_.wait(lk, [&] { return pending_ == 0; });
+    fn_ = nullptr;
+    T_ = 0;
+}
+
 int setup_block(int ni, int nj, const double* nodes, const double* area, int source, HostGeom& G) {
     G.ni = ni;
     G.nj = nj;
     const size_t ng = (size_t)(ni + 4) * (nj + 4);
-    G.M.assign(4 * ng, 0.0);
-    G.dl.assign(2 * ng, 0.0);
-    G.sur.assign(ng, 0.0);
-    for (int j = 1; j <= nj; ++j)
-        for (int i = 1; i <= ni; ++i) {
-            const int e = metric_at(G, i, j, node(nodes, ni, i - 1, j - 1), node(nodes, ni, i - 1, j),
-                                    node(nodes, ni, i, j - 1), node(nodes, ni, i, j));
-            if (e) return e;
+    G.M.resize(4 * ng);
+    G.dl.resize(2 * ng);
+    G.sur.resize(ng);
+    // ghost-frame rows in parallel: zeroed, then the interior cells' metrics
+    std::vector<int> row_err((size_t)nj + 4, Q2D_OK);
+    parallel_rows(nj + 4, 8L * (ni + 4), [&](long long r0, long long r1) {
+        for (long long r = r0; r < r1; ++r) {
+            const size_t k0 = (size_t)r * (ni + 4), k1 = k0 + (ni + 4);
+            std::fill(G.M.begin() + 4 * k0, G.M.begin() + 4 * k1, 0.0);
+            std::fill(G.dl.begin() + 2 * k0, G.dl.begin() + 2 * k1, 0.0);
+            std::fill(G.sur.begin() + k0, G.sur.begin() + k1, 0.0);
+            const int j = (int)r - 1;   // 1-based interior row of frame row r
+            if (j < 1 || j > nj) continue;
+            for (int i = 1; i <= ni; ++i) {
+                const int e = metric_at(G, i, j, node(nodes, ni, i - 1, j - 1), node(nodes, ni, i - 1, j),
+                                        node(nodes, ni, i, j - 1), node(nodes, ni, i, j));
+                if (e) { row_err[(size_t)r] = e; break; }
+            }
         }
+    });
+    for (int e : row_err)
+        if (e) return e;
     // Compute_Norm_Area (Lib_Metrics.f90:41-122): one orientation sign per direction
     auto X = [&](int i, int j) { return node(nodes, ni, i, j); };
     double sgn_i, sgn_j;
@@ -73,53 +149,60 @@ int setup_block(int ni, int nj, const double* nodes, const double* area, int sou
         const double cy = 0.5 * (X(1, 1).y + X(0, 1).y) - 0.5 * (X(1, 0).y + X(0, 0).y);
         sgn_j = std::copysign(1.0, cx * sx + cy * sy);
     }
-    G.fi.assign(3 * (size_t)(ni + 1) * nj, 0.0);
-    G.fj.assign(3 * (size_t)ni * (nj + 1), 0.0);
-    for (int j = 1; j <= nj; ++j)
-        for (int F = 0; F <= ni; ++F) {
-            const double dx = X(F, j).x - X(F, j - 1).x, dy = X(F, j).y - X(F, j - 1).y;
-            const double sx = dy, sy = -dx;
-            const double A = std::sqrt(sx * sx + sy * sy);
-            double* f = &G.fi[3 * ((size_t)(j - 1) * (ni + 1) + F)];
-            f[0] = A == 0.0 ? 0.0 : sx / A * sgn_i;
-            f[1] = A == 0.0 ? 0.0 : sy / A * sgn_i;
-            f[2] = A;
-        }
-    for (int Gf = 0; Gf <= nj; ++Gf)
-        for (int i = 1; i <= ni; ++i) {
-            const double dx = X(i - 1, Gf).x - X(i, Gf).x, dy = X(i - 1, Gf).y - X(i, Gf).y;
-            const double sx = dy, sy = -dx;
-            const double A = std::sqrt(sx * sx + sy * sy);
-            double* f = &G.fj[3 * ((size_t)Gf * ni + (i - 1))];
-            f[0] = A == 0.0 ? 0.0 : sx / A * sgn_j;
-            f[1] = A == 0.0 ? 0.0 : sy / A * sgn_j;
-            f[2] = A;
-        }
+    G.fi.resize(3 * (size_t)(ni + 1) * nj);
+    G.fj.resize(3 * (size_t)ni * (nj + 1));
+    parallel_rows(nj, 24L * (ni + 1), [&](long long r0, long long r1) {
+        for (int j = (int)r0 + 1; j <= (int)r1; ++j)
+            for (int F = 0; F <= ni; ++F) {
+                const double dx = X(F, j).x - X(F, j - 1).x, dy = X(F, j).y - X(F, j - 1).y;
+                const double sx = dy, sy = -dx;
+                const double A = std::sqrt(sx * sx + sy * sy);
+                double* f = &G.fi[3 * ((size_t)(j - 1) * (ni + 1) + F)];
+                f[0] = A == 0.0 ? 0.0 : sx / A * sgn_i;
+                f[1] = A == 0.0 ? 0.0 : sy / A * sgn_i;
+                f[2] = A;
+            }
+    });
+    parallel_rows(nj + 1, 24L * ni, [&](long long r0, long long r1) {
+        for (int Gf = (int)r0; Gf < (int)r1; ++Gf)
+            for (int i = 1; i <= ni; ++i) {
+                const double dx = X(i - 1, Gf).x - X(i, Gf).x, dy = X(i - 1, Gf).y - X(i, Gf).y;
+                const double sx = dy, sy = -dx;
+                const double A = std::sqrt(sx * sx + sy * sy);
+                double* f = &G.fj[3 * ((size_t)Gf * ni + (i - 1))];
+                f[0] = A == 0.0 ? 0.0 : sx / A * sgn_j;
+                f[1] = A == 0.0 ? 0.0 : sy / A * sgn_j;
+                f[2] = A;
+            }
+    });
     // source geometry (Precompute_Axisymmetric_Geometry / Precompute_Area_Geometry)
     const size_t n = (size_t)ni * nj;
-    G.src0.assign(n, 0.0);
-    G.src1.assign(n, 0.0);
-    if (source == Q2D_SRC_AXI) {
-        for (int j = 1; j <= nj; ++j)
+    G.src0.resize(n);
+    G.src1.resize(n);
+    parallel_rows(nj, 16L * ni, [&](long long r0, long long r1) {
+        for (int j = (int)r0 + 1; j <= (int)r1; ++j)
             for (int i = 1; i <= ni; ++i) {
-                const double r = 0.25 * (X(i, j).y + X(i - 1, j).y + X(i, j - 1).y + X(i - 1, j - 1).y);
-                G.src0[(size_t)(j - 1) * ni + (i - 1)] = 1.0 / (r > 1e-12 ? r : 1e-12);
+                const size_t k = (size_t)(j - 1) * ni + (i - 1);
+                double s0 = 0.0, s1 = 0.0;
+                if (source == Q2D_SRC_AXI) {
+                    const double r = 0.25 * (X(i, j).y + X(i - 1, j).y + X(i, j - 1).y + X(i - 1, j - 1).y);
+                    s0 = 1.0 / (r > 1e-12 ? r : 1e-12);
+                } else if (source == Q2D_SRC_AREA && area) {
+                    auto A = [&](int a, int b) { return area[(size_t)a + (size_t)(ni + 1) * b]; };
+                    const double d0 = 0.5 * ((A(i, j) - A(i - 1, j)) + (A(i, j - 1) - A(i - 1, j - 1)));
+                    const double d1 = 0.5 * ((A(i, j) - A(i, j - 1)) + (A(i - 1, j) - A(i - 1, j - 1)));
+                    const double* M = &G.M[4 * G.g(i - 1, j - 1)];
+                    const double g0 = d0 * M[0] + d1 * M[2];
+                    const double g1 = d0 * M[1] + d1 * M[3];
+                    const double Ac = 0.25 * (A(i, j) + A(i - 1, j) + A(i, j - 1) + A(i - 1, j - 1));
+                    const double den = Ac > 1e-12 ? Ac : 1e-12;
+                    s0 = -g0 / den;
+                    s1 = -g1 / den;
+                }
+                G.src0[k] = s0;
+                G.src1[k] = s1;
             }
-    } else if (source == Q2D_SRC_AREA && area) {
-        auto A = [&](int i, int j) { return area[(size_t)i + (size_t)(ni + 1) * j]; };
-        for (int j = 1; j <= nj; ++j)
-            for (int i = 1; i <= ni; ++i) {
-                const double d0 = 0.5 * ((A(i, j) - A(i - 1, j)) + (A(i, j - 1) - A(i - 1, j - 1)));
-                const double d1 = 0.5 * ((A(i, j) - A(i, j - 1)) + (A(i - 1, j) - A(i - 1, j - 1)));
-                const double* M = &G.M[4 * G.g(i - 1, j - 1)];
-                const double g0 = d0 * M[0] + d1 * M[2];
-                const double g1 = d0 * M[1] + d1 * M[3];
-                const double Ac = 0.25 * (A(i, j) + A(i - 1, j) + A(i, j - 1) + A(i - 1, j - 1));
-                const double den = Ac > 1e-12 ? Ac : 1e-12;
-                G.src0[(size_t)(j - 1) * ni + (i - 1)] = -g0 / den;
-                G.src1[(size_t)(j - 1) * ni + (i - 1)] = -g1 / den;
-            }
-    }
+    });
     return Q2D_OK;
 }
 

@@ -57,7 +57,7 @@ class ServeContext:
         prims = (PD * nb)()
         for k, b in enumerate(case.blocks):
             nd = np.ascontiguousarray(b.nodes, dtype=np.float64)
-            P = b.prim_ghost()
+            P = b.prim_ghost(ghosts=None)
             keep += [nd, P]
             nodes[k] = _abi.dptr(nd)
             prims[k] = _abi.dptr(P)
