@@ -112,19 +112,19 @@ class ClockSampler:
 def read_traffic(schedule):
     """DRAM bytes (read + write) per stage launch of the full batch, from the ncu summary of
     the stage kernel under profiles/ (a smaller batch captured and scaled by cells), when that
-    summary was taken with the same schedule; otherwise None."""
+    summary holds a capture taken with the same schedule (lines "- schedule: S" followed by
+    "- dram_bytes_per_launch_full_batch: B"); otherwise None."""
     name = "stage32_kernel_batched_nozzles.md" if schedule.startswith("fp32-flux") else \
         "stage_kernel_fp64_batched_nozzles.md"
     f = REPO / "profiles" / name
     try:
-        kv = {}
+        cur = None
         for line in f.read_text().splitlines():
-            if line.startswith("- ") and ":" in line:
-                k, v = line[2:].split(":", 1)
-                kv[k.strip()] = v.strip()
-        if kv.get("schedule") != schedule:
-            return None
-        return float(kv["dram_bytes_per_launch_full_batch"])
+            if line.startswith("- schedule:"):
+                cur = line.split(":", 1)[1].strip()
+            elif line.startswith("- dram_bytes_per_launch_full_batch:") and cur == schedule:
+                return float(line.split(":", 1)[1])
+        return None
     except Exception:
         return None
 
