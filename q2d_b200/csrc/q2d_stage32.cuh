@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             const float4 gq = __ldg(src);
             if (ok) sG[f] = gq;
         }
-        bool conn = false;   // a connection (101) ghost: evaluated in a second pass
+        bool ghosts = false;   // the tile's halo reaches a ghost layer: second pass below
 #pragma unroll
         for (int u = 0; u < (AREA + NT - 1) / NT; ++u) {
             const int idx = tid + u * NT;
@@ -432,62 +432,72 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                 const int kk = (r - 2) * TX + (c - 2);
                 sC[8 * NC + kk] = q0; sC[9 * NC + kk] = q1; sC[10 * NC + kk] = q2; sC[11 * NC + kk] = q3;
             }
-            if (cross && inI != inJ) {
-                // ghost cell gd layers beyond face f (Fill_Ghost_Cell, Lib_Ghost.f90:16-299): the
-                // record type, the boundary cell, its two inward neighbours and the face normal are
-                // loaded together; the type picks the rule afterwards
-                int f, gd, k, bi, bj, di, dj, nn;
-                if (!inI) {
-                    f = ii < 0 ? 1 : 2; gd = ii < 0 ? -ii : ii - ni + 1; k = jj;
-                    bi = ii < 0 ? 0 : ni - 1; bj = jj; di = ii < 0 ? 1 : -1; dj = 0; nn = ni;
-                } else {
-                    f = jj < 0 ? 3 : 4; gd = jj < 0 ? -jj : jj - nj + 1; k = ii;
-                    bi = ii; bj = jj < 0 ? 0 : nj - 1; di = 0; dj = jj < 0 ? 1 : -1; nn = nj;
-                }
-                if (gd <= 2) {
-                    const int type = __ldg(&a.edges[B.eo[f - 1] + k].type);
-                    const long long s1 = nn >= 2 ? (long long)dj * ni + di : 0;
-                    const long long s2 = nn >= 3 ? 2 * s1 : s1;
-                    const double* pb = Pin + (long long)bj * ni + bi;
-                    const double* gn = f <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (f == 1 ? 0 : ni)
-                                              : a.fj + B.ofj + (long long)(f == 3 ? 0 : nj) * ni + bi;
-                    const long long gs = f <= 2 ? B.pfi : B.pfj;
-                    double b[4], c1[4], c2[4];
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) {
-                        b[v] = __ldg(pb + v * pc);
-                        c1[v] = __ldg(pb + v * pc + s1);
-                        c2[v] = __ldg(pb + v * pc + s2);
-                    }
-                    const double nx = __ldg(gn), ny = __ldg(gn + gs);
-                    double q[4];
-                    if (type == 300) {   // Ghost_Symmetry (Lib_Ghost.f90:163-196)
-                        const double udotn = b[1] * nx + b[2] * ny;
-                        q[0] = b[0]; q[1] = b[1] - 2.0 * udotn * nx; q[2] = b[2] - 2.0 * udotn * ny; q[3] = b[3];
-                    } else if (type == 0 || type == 401 || type == 405 || type == 406 || type < 0) {
-#pragma unroll
-                        for (int v = 0; v < 4; ++v) q[v] = b[v];   // Ghost_ZG_Extrapolate (:199-219)
-                    } else {   // Ghost_Extrapolate (:270-299); connection ghosts are redone below
-#pragma unroll
-                        for (int v = 0; v < 4; ++v) {
-                            const double g1 = 3.0 * b[v] - 3.0 * c1[v] + c2[v];
-                            q[v] = gd == 1 ? g1 : 3.0 * g1 - 3.0 * b[v] + c1[v];
-                        }
-                    }
-                    conn = conn || type == 101;
-                    sP[idx] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
-                }
+            // A ghost a face stencil of the tile reads: one of the two ghost layers, an i-ghost in
+            // a tile row or a j-ghost in a tile column (the boundary cell and its two inward
+            // neighbours are then in the same row or column of the tile and its halo). Its record type and boundary-face normal
+            // are parked in its own slot until the second pass computes it.
+            const bool ghost = cross && inI != inJ && (!inI ? (r >= 2 && r < TY + 2) : (c >= 2 && c < TX + 2)) &&
+                               ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1;
+            if (ghost) {
+                int f, k, bi, bj;
+                if (!inI) { f = ii < 0 ? 1 : 2; k = jj; bi = ii < 0 ? 0 : ni - 1; bj = jj; }
+                else { f = jj < 0 ? 3 : 4; k = ii; bi = ii; bj = jj < 0 ? 0 : nj - 1; }
+                const int type = __ldg(&a.edges[B.eo[f - 1] + k].type);
+                const float4 gq = f <= 2 ? __ldg(gi4 + (long long)bj * (ni + 1) + (f == 1 ? 0 : ni))
+                                         : __ldg(gj4 + (long long)(f == 3 ? 0 : nj) * ni + bi);
+                sP[idx] = make_float4(__int_as_float(type), gq.x, gq.y, 0.0f);
+                ghosts = true;
             }
         }
-        if (__syncthreads_or(conn)) {   // connection ghosts: the donor block's cells
-            for (int idx = tid; idx < AREA; idx += NT) {
+        if (__syncthreads_or(ghosts)) {
+            // ghost cells (Fill_Ghost_Cell, Lib_Ghost.f90:16-299) from the tile's FP32 state:
+            // symmetry mirrors the boundary cell's velocity about the face normal (:163-196),
+            // types 0 and 401-406 copy it (Ghost_ZG_Extrapolate, :199-219), the rest extrapolate
+            // quadratically (Ghost_Extrapolate, :270-299); connection ghosts copy the donor
+            // block's cells (Ghost_Connection, :143-160) from HBM
+#pragma unroll 1
+            for (int u = 0; u < (AREA + NT - 1) / NT; ++u) {
+                const int idx = tid + u * NT;
                 const int r = idx / W, c = idx - r * W;
-                if ((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2)) continue;
                 const int ii = i0 - 2 + c, jj = j0 - 2 + r;
                 const bool inI = ii >= 0 && ii < ni, inJ = jj >= 0 && jj < nj;
-                double q[4];
-                if (inI == inJ || !ghost_value(a, B, ii, jj, q)) continue;
-                sP[idx] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+                if (idx >= AREA || inI == inJ || !(!inI ? (r >= 2 && r < TY + 2) : (c >= 2 && c < TX + 2)) ||
+                    ii < -2 || ii > ni + 1 || jj < -2 || jj > nj + 1)
+                    continue;
+                int gd, bi, bj, s1, nn;
+                if (!inI) {
+                    gd = ii < 0 ? -ii : ii - ni + 1; bi = ii < 0 ? 0 : ni - 1; bj = jj;
+                    s1 = ii < 0 ? 1 : -1; nn = ni;
+                } else {
+                    gd = jj < 0 ? -jj : jj - nj + 1; bi = ii; bj = jj < 0 ? 0 : nj - 1;
+                    s1 = jj < 0 ? W : -W; nn = nj;
+                }
+                const float4 park = sP[idx];
+                const int type = __float_as_int(park.x);
+                float4 q;
+                if (type == 101) {
+                    double qd[4] = {0.0, 0.0, 0.0, 0.0};
+                    ghost_value(a, B, ii, jj, qd);
+                    q = make_float4((float)qd[0], (float)qd[1], (float)qd[2], (float)qd[3]);
+                } else {
+                    const int sb = (bj - j0 + 2) * W + (bi - i0 + 2);
+                    const int d1 = nn >= 2 ? s1 : 0, d2 = nn >= 3 ? 2 * s1 : d1;
+                    const float4 b = sP[sb], c1 = sP[sb + d1], c2 = sP[sb + d2];
+                    if (type == 300) {
+                        const float nx = park.y, ny = park.z;
+                        const float un = b.y * nx + b.z * ny;
+                        q = make_float4(b.x, b.y - 2.0f * un * nx, b.z - 2.0f * un * ny, b.w);
+                    } else if (type == 0 || type == 401 || type == 405 || type == 406 || type < 0) {
+                        q = b;
+                    } else {
+                        const float4 g1 = make_float4(3.0f * b.x - 3.0f * c1.x + c2.x, 3.0f * b.y - 3.0f * c1.y + c2.y,
+                                                      3.0f * b.z - 3.0f * c1.z + c2.z, 3.0f * b.w - 3.0f * c1.w + c2.w);
+                        q = gd == 1 ? g1
+                                    : make_float4(3.0f * g1.x - 3.0f * b.x + c1.x, 3.0f * g1.y - 3.0f * b.y + c1.y,
+                                                  3.0f * g1.z - 3.0f * b.z + c1.z, 3.0f * g1.w - 3.0f * b.w + c1.w);
+                    }
+                }
+                sP[idx] = q;
             }
         }
         cp_async_wait_all();
