@@ -434,8 +434,8 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             }
             // A ghost a face stencil of the tile reads: one of the two ghost layers, an i-ghost in
             // a tile row or a j-ghost in a tile column (the boundary cell and its two inward
-            // neighbours are then in the same row or column of the tile and its halo). Its record type and boundary-face normal
-            // are parked in its own slot until the second pass computes it.
+            // neighbours are then in the same row or column of the tile and its halo). Its record
+            // type and boundary-face normal are parked in its own slot until the second pass.
             const bool ghost = cross && inI != inJ && (!inI ? (r >= 2 && r < TY + 2) : (c >= 2 && c < TX + 2)) &&
                                ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1;
             if (ghost) {
