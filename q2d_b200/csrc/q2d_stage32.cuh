@@ -274,6 +274,53 @@ __device__ __forceinline__ void bc_extrapolation32(const float* B, float nx, flo
     out[3] = m * (gf * B[3] * rcp_approx(B[0]) + 0.5f * (B[1] * B[1] + B[2] * B[2]));
 }
 
+// BC_Inlet_StagnCond + Stagn_Inflow (Lib_BC_Fluxes_Inflow.f90:64-120, 412-483) in FP32 for the
+// common case: inflow through the face and a discriminant clearly above zero, where the
+// reference takes the first iterate (p0 itself). The face state is the isentropic state on the
+// outgoing Riemann invariant a + sign (gamma-1)/2 Un of the boundary cell, at the flow angle of
+// the record ('normal': the face normal, so that tan(alpha) = n1 / n0). Returns 0 with the
+// flux in out, 1 when the flow leaves through the inlet (the symmetry flux applies, :176-227),
+// 2 when the discriminant is negative or too close to zero for FP32 to decide (the FP64
+// routine then runs the reference's relaxation of p0).
+__device__ __forceinline__ int bc_stagnation32(int Fm, const float* B, float n0, float n1, float len,
+                                               float gam, float R, const BCParam& bp, float* out) {
+    const float sgn = (Fm & 1) ? -1.0f : 1.0f;
+    const float Un = B[1] * n0 + B[2] * n1;
+    if (sgn * Un >= 0.0f) return 1;
+    const float gh = 0.5f * (gam - 1.0f);
+    const float Sound = sqrtf(gam * B[3] * rcp_approx(B[0]));
+    const float Riem = Sound + sgn * gh * Un;
+    const float ta = bp.alpha >= 0.5 * DBL_MAX ? n1 * rcp_approx(n0 + 1e-20f) : tanf((float)bp.alpha);
+    const float t0 = (float)bp.t0, t1 = (float)bp.t1;
+    const float E1 = -(n1 - n0 * ta) * rcp_approx(t1 - t0 * ta);
+    const float Sound0 = sqrtf(gam * R * (float)bp.T0);
+    const float CoefD = (1.0f + E1 * E1) * gh;
+    const float p0 = (float)bp.p0;
+    const float ss = Sound * rcp_approx(Sound0);
+    const float CoefC = __powf(p0 * rcp_approx(B[3]), (gam - 1.0f) * rcp_approx(gam)) * (ss * ss);
+    const float YA = gh * gh + CoefC * CoefD;
+    const float YB = sgn * Riem * gh;
+    const float R2 = Riem * Riem, C2 = CoefC * (Sound0 * Sound0);
+    const float YC = R2 - C2;
+    const float Discr = YB * YB - YA * YC;
+    // FP32 error of Discr: a few ulps of its largest terms, plus the reference's 1e-2 band
+    const float tol = 1e-5f * (YB * YB + YA * (R2 + C2)) + 2e-2f;
+    if (!(Discr > tol)) return 2;
+    const float Un3 = (YB + copysignf(1.0f, Un) * sqrtf(Discr)) * rcp_approx(YA);
+    const float Sound3 = sqrtf(Sound0 * Sound0 - CoefD * (Un3 * Un3));
+    const float p3 = p0 * __powf(Sound3 * rcp_approx(Sound0), 2.0f * gam * rcp_approx(gam - 1.0f));
+    const float Ut3 = Un3 * E1;
+    const float rho = gam * p3 * rcp_approx(Sound3 * Sound3);
+    const float fu = Un3 * n0 + Ut3 * t0, fv = Un3 * n1 + Ut3 * t1;
+    const float H = gam * rcp_approx(gam - 1.0f) * p3 * rcp_approx(rho);   // cp T
+    const float m = rho * Un3 * len;
+    out[0] = m;
+    out[1] = m * fu + p3 * len * n0;
+    out[2] = m * fv + p3 * len * n1;
+    out[3] = m * (0.5f * (fu * fu + fv * fv) + H);
+    return 0;
+}
+
 template <int RIEM>
 __device__ __forceinline__ void bc_symmetry32_lim(int lim, int Fm, const float* B, const float* I, float dlb,
                                                   float dli, float nx, float ny, float len, float gam,
@@ -297,6 +344,25 @@ __device__ __forceinline__ float cell_dt32(float rho, float u, float v, float p,
     float dtmin = fminf(1e8f, dli * rcp_approx(fabsf(u * ei0 + v * ei1) + snd) * cfl);
     if (ndir == 2) dtmin = fminf(dtmin, dlj * rcp_approx(fabsf(u * ej0 + v * ej1) + snd) * cfl);
     return dtmin;
+}
+
+// Boundary face t of a tile (nl faces on block face 1, nr on face 2, nb on face 3, then face 4):
+// its block face Fm, its cell index k along that face and its slot f among the tile's faces.
+template <int TX>
+__device__ __forceinline__ void boundary_face_slot(int t, int nl, int nr, int nb, int i0, int j0, int ni,
+                                                   int nj, int NFI, int& Fm, int& k, int& f) {
+    if (t < nl) {
+        Fm = 1; k = j0 + t; f = t * (TX + 1);
+    } else if (t < nl + nr) {
+        const int u = t - nl;
+        Fm = 2; k = j0 + u; f = u * (TX + 1) + (ni - i0);
+    } else if (t < nl + nr + nb) {
+        const int u = t - nl - nr;
+        Fm = 3; k = i0 + u; f = NFI + u;
+    } else {
+        const int u = t - nl - nr - nb;
+        Fm = 4; k = i0 + u; f = NFI + (nj - j0) * TX + u;
+    }
 }
 
 template <int RIEM, int TX, int TY, int NT, int MB>
@@ -412,6 +478,18 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             const float4 gq = __ldg(src);
             if (ok) sG[f] = gq;
         }
+        {   // boundary-face records (type, BC parameter index), parked in the faces' flux slots
+            // until the face phase (Mod_BC_Fluxes.f90:79-84 order: faces 1..4 of the block)
+            const int nrow = min(TY, nj - j0), ncol = min(TX, ni - i0);
+            const int nl = (i0 == 0) ? nrow : 0, nr = (i0 + TX >= ni) ? nrow : 0;
+            const int nb = (j0 == 0) ? ncol : 0, nt = (j0 + TY >= nj) ? ncol : 0;
+            for (int t = tid; t < nl + nr + nb + nt; t += NT) {
+                int Fm, k, f;
+                boundary_face_slot<TX>(t, nl, nr, nb, i0, j0, ni, nj, NFI, Fm, k, f);
+                const EdgeRec* er = a.edges + B.eo[Fm - 1] + k;
+                sF[f] = make_float4(__int_as_float(__ldg(&er->type)), __int_as_float(__ldg(&er->param)), 0.0f, 0.0f);
+            }
+        }
         bool ghosts = false;   // the tile's halo reaches a ghost layer: second pass below
 #pragma unroll
         for (int u = 0; u < (AREA + NT - 1) / NT; ++u) {
@@ -526,20 +604,16 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             const int nb = (j0 == 0) ? ncol : 0;
             const int nt = (j0 + TY >= nj) ? ncol : 0;
             for (int t = NT - 1 - tid; t < nl + nr + nb + nt; t += NT) {
-                int Fm, k, bi, bj, di, dj, f;
-                if (t < nl) {
-                    Fm = 1; k = j0 + t; bi = 0; bj = k; di = 1; dj = 0; f = t * (TX + 1);
-                } else if (t < nl + nr) {
-                    const int u = t - nl;
-                    Fm = 2; k = j0 + u; bi = ni - 1; bj = k; di = -1; dj = 0; f = u * (TX + 1) + (ni - i0);
-                } else if (t < nl + nr + nb) {
-                    const int u = t - nl - nr;
-                    Fm = 3; k = i0 + u; bi = k; bj = 0; di = 0; dj = 1; f = NFI + u;
-                } else {
-                    const int u = t - nl - nr - nb;
-                    Fm = 4; k = i0 + u; bi = k; bj = nj - 1; di = 0; dj = -1; f = NFI + (nj - j0) * TX + u;
+                int Fm, k, f;
+                boundary_face_slot<TX>(t, nl, nr, nb, i0, j0, ni, nj, NFI, Fm, k, f);
+                const int bi = Fm == 1 ? 0 : (Fm == 2 ? ni - 1 : k), bj = Fm == 3 ? 0 : (Fm == 4 ? nj - 1 : k);
+                const int di = Fm == 1 ? 1 : (Fm == 2 ? -1 : 0), dj = Fm == 3 ? 1 : (Fm == 4 ? -1 : 0);
+                struct { int type, param; } e;   // the record parked by the load phase
+                {
+                    const float4 pk = sF[f];
+                    e.type = __float_as_int(pk.x);
+                    e.param = __float_as_int(pk.y);
                 }
-                const EdgeRec e = a.edges[B.eo[Fm - 1] + k];
                 const int cb = (bj - j0 + 2) * W + (bi - i0 + 2);     // boundary cell
                 const int ci = cb + dj * W + di;                       // its inward neighbour
                 const float* dlp = Fm <= 2 ? sD : sD + 1;
@@ -559,31 +633,44 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                                                 gf, X);
                     else
                         bc_extrapolation32(Bq, nx, ny, ln, gf, X);
-                } else if (e.type > 0) {   // inflow / outflow records: FP64 from the FP64 state
-                    const double* pb = Pin + (long long)bj * ni + bi;
-                    const int ni2 = bi + di, nj2 = bj + dj;
-                    Q4 Bp, Ip;
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) Bp.v[v] = __ldg(pb + v * pc);
-                    if (ni2 >= 0 && ni2 < ni && nj2 >= 0 && nj2 < nj) {
-                        const double* pi = Pin + (long long)nj2 * ni + ni2;
-#pragma unroll
-                        for (int v = 0; v < 4; ++v) Ip.v[v] = __ldg(pi + v * pc);
-                    } else {   // one-cell-thick block: the neighbour is the opposite ghost
-                        const float4 Ic = sP[ci];
-                        Ip.v[0] = Ic.x; Ip.v[1] = Ic.y; Ip.v[2] = Ic.z; Ip.v[3] = Ic.w;
+                } else if (e.type > 0) {   // inflow / outflow records
+                    int path = 2;
+                    if (e.type == 401 && e.param >= 0) {   // stagnation inflow: FP32 when it decides, else FP64
+                        const float4 Bc = sP[cb], Ic = sP[ci];
+                        const float Bq[4] = {Bc.x, Bc.y, Bc.z, Bc.w}, Iq[4] = {Ic.x, Ic.y, Ic.z, Ic.w};
+                        path = bc_stagnation32(Fm, Bq, nx, ny, ln, gam, (float)g.R, a.bcp[e.param], X);
+                        if (path == 1) {
+                            bc_symmetry32_lim<RIEM>(a.limiter, Fm, Bq, Iq, dlp[2 * cb], dlp[2 * ci], nx, ny, ln, gam,
+                                                    gm1, gf, X);
+                            path = 0;
+                        }
                     }
-                    const double* dlb = a.dl + B.og + (long long)(Fm <= 2 ? 0 : 1) * B.pg;
-                    const double dlbv = __ldg(dlb + (long long)(bj + 2) * (ni + 4) + (bi + 2));
-                    const double dli = __ldg(dlb + (long long)(nj2 + 2) * (ni + 4) + (ni2 + 2));
-                    const double* gsrc = Fm <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (Fm == 1 ? 0 : ni)
-                                                 : a.fj + B.ofj + (long long)(Fm == 3 ? 0 : nj) * ni + bi;
-                    const long long gs = Fm <= 2 ? B.pfi : B.pfj;
-                    const Q4 q = bc_face<RIEM>(a.gas, a.limiter, e.type, Fm, Bp, Ip, dlbv, dli, __ldg(gsrc),
-                                               __ldg(gsrc + gs), __ldg(gsrc + 2 * gs),
-                                               e.param >= 0 ? a.bcp + e.param : nullptr);
+                    if (path == 2) {   // FP64 from the FP64 state
+                        const double* pb = Pin + (long long)bj * ni + bi;
+                        const int ni2 = bi + di, nj2 = bj + dj;
+                        Q4 Bp, Ip;
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) X[v] = (float)q.v[v];
+                        for (int v = 0; v < 4; ++v) Bp.v[v] = __ldg(pb + v * pc);
+                        if (ni2 >= 0 && ni2 < ni && nj2 >= 0 && nj2 < nj) {
+                            const double* pi = Pin + (long long)nj2 * ni + ni2;
+#pragma unroll
+                            for (int v = 0; v < 4; ++v) Ip.v[v] = __ldg(pi + v * pc);
+                        } else {   // one-cell-thick block: the neighbour is the opposite ghost
+                            const float4 Ic = sP[ci];
+                            Ip.v[0] = Ic.x; Ip.v[1] = Ic.y; Ip.v[2] = Ic.z; Ip.v[3] = Ic.w;
+                        }
+                        const double* dlb = a.dl + B.og + (long long)(Fm <= 2 ? 0 : 1) * B.pg;
+                        const double dlbv = __ldg(dlb + (long long)(bj + 2) * (ni + 4) + (bi + 2));
+                        const double dli = __ldg(dlb + (long long)(nj2 + 2) * (ni + 4) + (ni2 + 2));
+                        const double* gsrc = Fm <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (Fm == 1 ? 0 : ni)
+                                                     : a.fj + B.ofj + (long long)(Fm == 3 ? 0 : nj) * ni + bi;
+                        const long long gs = Fm <= 2 ? B.pfi : B.pfj;
+                        const Q4 q = bc_face<RIEM>(a.gas, a.limiter, e.type, Fm, Bp, Ip, dlbv, dli, __ldg(gsrc),
+                                                   __ldg(gsrc + gs), __ldg(gsrc + 2 * gs),
+                                                   e.param >= 0 ? a.bcp + e.param : nullptr);
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) X[v] = (float)q.v[v];
+                    }
                 }
                 sF[f] = make_float4(X[0], X[1], X[2], X[3]);
             }

@@ -118,3 +118,25 @@ def test_fp32flux_state_independent_of_tile():
     for sch in (SCHED[2], "fp32-flux tile 32x16", "fp32-flux tile 64x8"):
         got, _ = run(batch, 30, schedule=sch, precision=1)
         compare(got, ref, sch)
+
+
+@pytest.mark.parametrize("variant", ["inflow", "reverse", "low_p0"])
+def test_stagnation_inflow_paths(variant):
+    """The FP32-flux kernel evaluates stagnation inflow faces (BC 401) in FP32 when the
+    discriminant of the face state is clearly positive, applies the symmetry flux when the flow
+    leaves through the inlet, and hands negative or marginal discriminants (the reference's p0
+    relaxation) to the FP64 routine. Each path stays within the form's tolerance of the plain
+    FP64 path: a normal inflow, a reversed initial velocity (outflow through the inlet), and a
+    total pressure below the interior pressure (negative discriminant)."""
+    import copy
+    cs = copy.deepcopy(cases.area_nozzle(96, 12, 1.5, 0.45, 5e5, 400.0))
+    if variant == "reverse":
+        cs.blocks[0].prim[..., 1] *= -1.0
+    elif variant == "low_p0":
+        for r in cs.bcs:
+            if r["type"] == 401:
+                r["p0"] = 0.5 * r["p0"]
+    s32, i32 = run([cs], 20, precision=1)
+    s64, i64 = run([cs], 20, precision=0)
+    assert i32[0]["err"] == 0 and i64[0]["err"] == 0
+    compare(s32, s64, f"stagnation inflow {variant}")
