@@ -224,10 +224,12 @@ int  q2d_gpu_download_prim(q2d_ctx* ctx, int block_id, double* P);
 
 /* Many-block forms of q2d_gpu_upload_prim / q2d_gpu_download_prim: block_ids[k] with the
  * ghosted array P[k], k < n. The host<->device copies of all blocks are queued back to back
- * and the call synchronises once (plus once per 128 MiB of staging), which is what a host that
- * reads or writes every block of a batch (the loops over blocks of Read_IC,
- * IO_Solution.f90:38-129, and of the solution writers set up at IO_Solution.f90:132-231) should call. Blocks of cases not on the device yet take the single-block
- * path; download requires every block to be on the device. */
+ * through a 128 MiB device staging ring and the call synchronises once: what a host that reads
+ * or writes every block of a batch (the loops over blocks of Read_IC, IO_Solution.f90:38-129,
+ * and of the solution writers set up at IO_Solution.f90:132-231) should call. Upload copies
+ * each whole array in one piece (its ghost values are read but not used); download writes the
+ * interior only. Blocks of cases not on the device yet take the single-block path; download
+ * requires every block to be on the device. Page-locked host arrays copy fastest. */
 int  q2d_gpu_upload_prim_many(q2d_ctx* ctx, int n, const int* block_ids, const double* const* P);
 int  q2d_gpu_download_prim_many(q2d_ctx* ctx, int n, const int* block_ids, double* const* P);
 

@@ -154,6 +154,7 @@ struct q2d_ctx {
     // device pools and their allocators
     DevBuf<double> PA, PB, PC, SC, DL, FI, FJ, PART;
     DevBuf<double> XFER;            // staging rows of one block's state for upload / download
+    DevBuf<XferDesc> XDESC;         // block descriptors of a many-block transfer segment
     DevBuf<float> DL32, FI4, FJ4;   // FP32 geometry (FP32-flux form only): same regions as DL/FI/FJ
     Arena ac, ag, afi, afj;
     DevBuf<DBlock> dblocks;
@@ -1077,35 +1078,64 @@ static int transfer_many(q2d_ctx* ctx, int n, const int* ids, double* const* P, 
             if (int e = q2d_gpu_upload_prim(ctx, ids[k], P[k])) return e;
             continue;
         }
-        const long long len = (4ll * b.ni * b.nj + 31) / 32 * 32;
+        const long long len = ((up ? 4ll * (b.ni + 4) * (b.nj + 4) : 4ll * b.ni * b.nj) + 31) / 32 * 32;
         need_max = std::max(need_max, len);
         total += len;
     }
     if (total == 0) return Q2D_OK;
     CK(ensure_cap(ctx->XFER, (size_t)std::max(need_max, std::min(kXferRing, total))));
     const long long cap = (long long)ctx->XFER.n;
-    long long off = 0;
+    // Segments of the staging ring: upload = one contiguous copy of each caller's whole array,
+    // then one transposing launch for the segment; download = one launch, then a strided copy
+    // of each block's interior rows (the caller's ghost layers are not written). Work on the
+    // one stream is ordered, so a segment reuses the ring without waiting on the host.
+    std::vector<XferDesc> seg;
+    std::vector<int> seg_k;
+    long long off = 0, seg_cells = 0;
+    auto flush = [&]() -> int {
+        if (seg.empty()) return Q2D_OK;
+        CK(ensure_cap(ctx->XDESC, seg.size()));
+        CK(cudaMemcpyAsync(ctx->XDESC.p, seg.data(), sizeof(XferDesc) * seg.size(), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        if (!up) CK(launch_transfer_many(ctx->XDESC.p, (int)seg.size(), seg_cells, false, ctx->XFER.p, ctx->PA.p,
+                                         ctx->stream));
+        for (size_t q = 0; q < seg.size(); ++q) {
+            const XferDesc& x = seg[q];
+            const HBlock& b = ctx->blocks[ids[seg_k[q]]];
+            if (!up) {
+                double* row0 = P[seg_k[q]] + 4 * (2 + (size_t)(b.ni + 4) * 2);
+                const size_t w = sizeof(double) * 4 * b.ni, pitch = sizeof(double) * 4 * (b.ni + 4);
+                CK(cudaMemcpy2DAsync(row0, pitch, ctx->XFER.p + x.stage, w, w, b.nj, cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+            }
+        }
+        if (up) CK(launch_transfer_many(ctx->XDESC.p, (int)seg.size(), seg_cells, true, ctx->XFER.p, ctx->PA.p,
+                                        ctx->stream));
+        ctx->launches += 1;
+        seg.clear();
+        seg_k.clear();
+        off = 0;
+        seg_cells = 0;
+        return Q2D_OK;
+    };
     for (int k = 0; k < n; ++k) {
         const HBlock& b = ctx->blocks[ids[k]];
         if (!ctx->cases[b.case_id].resident || !b.alive) continue;
         const long long cells = (long long)b.ni * b.nj;
-        if (off + 4 * cells > cap) {   // ring full: let the queued transfers finish first
-            CK(cudaStreamSynchronize(ctx->stream));
-            off = 0;
+        const long long len = up ? 4ll * (b.ni + 4) * (b.nj + 4) : 4 * cells;
+        if (off + len > cap || seg.size() >= 65535) {
+            if (int e = flush()) return e;
         }
-        double* st = ctx->XFER.p + off;
-        double* row0 = P[k] + 4 * (2 + (size_t)(b.ni + 4) * 2);
-        const size_t w = sizeof(double) * 4 * b.ni, pitch = sizeof(double) * 4 * (b.ni + 4);
-        if (up) {
-            CK(cudaMemcpy2DAsync(st, w, row0, pitch, w, b.nj, cudaMemcpyHostToDevice, ctx->stream));
-            CK(launch_cells_to_planes(st, ctx->PA.p + b.d.oc, cells, b.d.pc, ctx->stream));
-        } else {
-            CK(launch_planes_to_cells(ctx->PA.p + b.d.oc, b.d.pc, st, cells, ctx->stream));
-            CK(cudaMemcpy2DAsync(row0, pitch, st, w, w, b.nj, cudaMemcpyDeviceToHost, ctx->stream));
-        }
-        ctx->launches += 1;
-        off += (4 * cells + 31) / 32 * 32;
+        XferDesc x;
+        x.stage = off; x.plane = b.d.oc; x.pc = b.d.pc; x.ni = b.ni; x.nj = b.nj;
+        if (up)   // the whole array in one contiguous copy (its ghost values are not used)
+            CK(cudaMemcpyAsync(ctx->XFER.p + off, P[k], sizeof(double) * len, cudaMemcpyHostToDevice, ctx->stream));
+        seg.push_back(x);
+        seg_k.push_back(k);
+        seg_cells = std::max(seg_cells, cells);
+        off += (len + 31) / 32 * 32;
     }
+    if (int e = flush()) return e;
     CK(cudaStreamSynchronize(ctx->stream));
     if (up) ctx->dt_valid = false;
     return Q2D_OK;
@@ -1349,6 +1379,7 @@ void q2d_gpu_destroy(q2d_ctx* ctx) {
     drop_graphs(ctx);
     ctx->PA.release(); ctx->PB.release(); ctx->PC.release(); ctx->SC.release(); ctx->DL.release();
     ctx->FI.release(); ctx->FJ.release(); ctx->PART.release(); ctx->dblocks.release(); ctx->XFER.release();
+    ctx->XDESC.release();
     ctx->DL32.release(); ctx->FI4.release(); ctx->FJ4.release();
     ctx->dcases.release(); ctx->cstate.release(); ctx->items.release(); ctx->edges.release();
     ctx->bcp.release(); ctx->flag.release();

@@ -606,6 +606,51 @@ __global__ void planes_to_cells_kernel(const double* __restrict__ in, long long 
     }
 }
 
+// Many-block forms: one launch per staging segment, blockIdx.y over the segment's blocks.
+// Upload: the staging holds each caller's whole ghosted array P(4, -1:ni+2, -1:nj+2); only its
+// interior goes to the state planes. Download: the interior rows of each block, packed.
+__global__ void ghosted_to_planes_kernel(const XferDesc* __restrict__ d, int nd, const double* __restrict__ stage,
+                                         double* __restrict__ pool) {
+    for (int b = blockIdx.y; b < nd; b += gridDim.y) {
+        const XferDesc x = d[b];
+        const long long n = (long long)x.ni * x.nj;
+        const double2* in = reinterpret_cast<const double2*>(stage + x.stage);
+        double* out = pool + x.plane;
+        for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+             c += (long long)gridDim.x * blockDim.x) {
+            const long long j = c / x.ni, i = c - j * x.ni;
+            const long long g = (j + 2) * (x.ni + 4) + (i + 2);
+            const double2 a = in[2 * g], q = in[2 * g + 1];
+            out[c] = a.x; out[x.pc + c] = a.y; out[2 * x.pc + c] = q.x; out[3 * x.pc + c] = q.y;
+        }
+    }
+}
+
+__global__ void planes_to_rows_kernel(const XferDesc* __restrict__ d, int nd, const double* __restrict__ pool,
+                                      double* __restrict__ stage) {
+    for (int b = blockIdx.y; b < nd; b += gridDim.y) {
+        const XferDesc x = d[b];
+        const long long n = (long long)x.ni * x.nj;
+        const double* in = pool + x.plane;
+        double2* out = reinterpret_cast<double2*>(stage + x.stage);
+        for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+             c += (long long)gridDim.x * blockDim.x) {
+            out[2 * c] = make_double2(in[c], in[x.pc + c]);
+            out[2 * c + 1] = make_double2(in[2 * x.pc + c], in[3 * x.pc + c]);
+        }
+    }
+}
+
+cudaError_t launch_transfer_many(const XferDesc* d, int nd, long long max_cells, bool up, double* stage,
+                                 double* pool, cudaStream_t s) {
+    if (nd <= 0) return cudaSuccess;
+    const dim3 grid((unsigned)std::max<long long>(1, std::min<long long>((max_cells + 255) / 256, 64)),
+                    (unsigned)std::min(nd, 65535));
+    if (up) ghosted_to_planes_kernel<<<grid, 256, 0, s>>>(d, nd, stage, pool);
+    else planes_to_rows_kernel<<<grid, 256, 0, s>>>(d, nd, pool, stage);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_cells_to_planes(const double* in, double* out, long long n, long long pc, cudaStream_t s) {
     const int grid = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 8));
     cells_to_planes_kernel<<<grid, 256, 0, s>>>(reinterpret_cast<const double2*>(in), out, n, pc);

@@ -24,6 +24,13 @@ cudaError_t launch_dt(const StageArgs& a, int tile, int grid, cudaStream_t s);
 cudaError_t launch_copy(const double* src, double* dst, long long n, int* flag, cudaStream_t s);
 // cell-interleaved (rho, u, v, p) <-> 4 planes of stride pc, n cells (state upload / download)
 cudaError_t launch_cells_to_planes(const double* in, double* out, long long n, long long pc, cudaStream_t s);
+// One block of a many-block transfer: its staging offset and state-plane offset (doubles).
+struct XferDesc {
+    long long stage, plane, pc;
+    int ni, nj;
+};
+cudaError_t launch_transfer_many(const XferDesc* d, int nd, long long max_cells, bool up, double* stage,
+                                 double* pool, cudaStream_t s);
 cudaError_t launch_planes_to_cells(const double* in, long long pc, double* out, long long n, cudaStream_t s);
 cudaError_t launch_resume(CaseState* cs, int n, int* flag, cudaStream_t s);
 cudaError_t launch_finalize(const StageArgs& a, cudaStream_t s);
