@@ -38,8 +38,10 @@ struct Tile32 {
     // 8-11 state
     static constexpr int NCD = 12;
     static constexpr size_t bP = sizeof(double) * NCD * NC;   // float4 [AREA]  rho, u, v, p
-    static constexpr size_t bG = bP + 16 * (size_t)AREA;      // float4 [NF]    nx, ny, length, -
-    static constexpr size_t bF = bG + 16 * (size_t)NF;        // float4 [NF]    flux times length
+    // float4 [NF]: a face's geometry (nx, ny, length, packed boundary record) until its thread
+    // computes the face, then its flux times length in the same slot
+    static constexpr size_t bG = bP + 16 * (size_t)AREA;
+    static constexpr size_t bF = bG;
     static constexpr size_t bD = bF + 16 * (size_t)NF;        // float2 [AREA]  dl(1), dl(2)
     static constexpr size_t bytes = bD + 8 * (size_t)AREA;
 };
@@ -346,6 +348,21 @@ __device__ __forceinline__ float cell_dt32(float rho, float u, float v, float p,
     return dtmin;
 }
 
+// Boundary record of a face packed into one 32-bit word: the BC type as a 3-bit code and its
+// BC parameter index + 1 above it.
+__device__ __forceinline__ float pack_record(int type, int param) {
+    const unsigned code = type == 101 ? 1u : type == 300 ? 2u : type == 400 ? 3u : type == 401 ? 4u
+                        : type == 405 ? 5u : type == 406 ? 6u : type == 0 ? 7u : 0u;
+    return __uint_as_float(((unsigned)(param + 1) << 3) | code);
+}
+
+__device__ __forceinline__ void unpack_record(float w, int& type, int& param) {
+    const unsigned u = __float_as_uint(w);
+    static constexpr int kTypes[8] = {-1, 101, 300, 400, 401, 405, 406, 0};
+    type = kTypes[u & 7u];
+    param = (int)(u >> 3) - 1;
+}
+
 // Boundary face t of a tile (nl faces on block face 1, nr on face 2, nb on face 3, then face 4):
 // its block face Fm, its cell index k along that face and its slot f among the tile's faces.
 template <int TX>
@@ -370,6 +387,7 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
     using L = Tile32<TX, TY>;
     constexpr int W = L::W, AREA = L::AREA, NFI = L::NFI, NF = L::NF, NC = L::NC;
     static_assert(L::bG % 16 == 0 && L::bF % 16 == 0 && L::bD % 8 == 0, "shared layout alignment");
+    static_assert(L::bF == L::bG, "a face's flux replaces its geometry in the same slot");
     extern __shared__ double smem[];
     double* sC = smem;
     unsigned char* sb = reinterpret_cast<unsigned char*>(smem);
@@ -463,32 +481,27 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             const int f = tid + u * NT;
             bool ok;
             const float4* src;
+            const EdgeRec* er = a.edges;   // the face's boundary record, if it is on the block's edge
+            bool edge;
             if (f < NFI) {
                 const int row = f / (TX + 1), col = f - row * (TX + 1);
                 const int jj = j0 + row, F = i0 + col;
                 ok = jj < nj && F <= ni;
                 src = gi4 + (ok ? (long long)jj * (ni + 1) + F : 0);
+                edge = ok && (F == 0 || F == ni);
+                if (edge) er += B.eo[F == 0 ? 0 : 1] + jj;
             } else {
                 const int ff = f - NFI;
                 const int row = ff / TX, col = ff - row * TX;
                 const int ii = i0 + col, G = j0 + row;
                 ok = f < NF && ii < ni && G <= nj;
                 src = gj4 + (ok ? (long long)G * ni + ii : 0);
+                edge = ok && (G == 0 || G == nj);
+                if (edge) er += B.eo[G == 0 ? 2 : 3] + ii;
             }
-            const float4 gq = __ldg(src);
+            float4 gq = __ldg(src);
+            if (edge) gq.w = pack_record(__ldg(&er->type), __ldg(&er->param));
             if (ok) sG[f] = gq;
-        }
-        {   // boundary-face records (type, BC parameter index), parked in the faces' flux slots
-            // until the face phase (Mod_BC_Fluxes.f90:79-84 order: faces 1..4 of the block)
-            const int nrow = min(TY, nj - j0), ncol = min(TX, ni - i0);
-            const int nl = (i0 == 0) ? nrow : 0, nr = (i0 + TX >= ni) ? nrow : 0;
-            const int nb = (j0 == 0) ? ncol : 0, nt = (j0 + TY >= nj) ? ncol : 0;
-            for (int t = tid; t < nl + nr + nb + nt; t += NT) {
-                int Fm, k, f;
-                boundary_face_slot<TX>(t, nl, nr, nb, i0, j0, ni, nj, NFI, Fm, k, f);
-                const EdgeRec* er = a.edges + B.eo[Fm - 1] + k;
-                sF[f] = make_float4(__int_as_float(__ldg(&er->type)), __int_as_float(__ldg(&er->param)), 0.0f, 0.0f);
-            }
         }
         bool ghosts = false;   // the tile's halo reaches a ghost layer: second pass below
 #pragma unroll
@@ -608,16 +621,12 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                 boundary_face_slot<TX>(t, nl, nr, nb, i0, j0, ni, nj, NFI, Fm, k, f);
                 const int bi = Fm == 1 ? 0 : (Fm == 2 ? ni - 1 : k), bj = Fm == 3 ? 0 : (Fm == 4 ? nj - 1 : k);
                 const int di = Fm == 1 ? 1 : (Fm == 2 ? -1 : 0), dj = Fm == 3 ? 1 : (Fm == 4 ? -1 : 0);
-                struct { int type, param; } e;   // the record parked by the load phase
-                {
-                    const float4 pk = sF[f];
-                    e.type = __float_as_int(pk.x);
-                    e.param = __float_as_int(pk.y);
-                }
+                struct { int type, param; } e;   // the record packed with the face geometry
+                const float4 gq = sG[f];
+                unpack_record(gq.w, e.type, e.param);
                 const int cb = (bj - j0 + 2) * W + (bi - i0 + 2);     // boundary cell
                 const int ci = cb + dj * W + di;                       // its inward neighbour
                 const float* dlp = Fm <= 2 ? sD : sD + 1;
-                const float4 gq = sG[f];
                 const float nx = gq.x, ny = gq.y, ln = gq.z;
                 float X[4] = {0.0f, 0.0f, 0.0f, 0.0f};
                 if (e.type == 101) {   // BC_Connection_Eul: the interior scheme on the ghost stencil
