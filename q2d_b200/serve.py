@@ -27,6 +27,33 @@ from .cases import BASE_SEED, CaseSpec, request_case
 from .solver import Q2DError
 
 
+def wire(case: CaseSpec) -> dict:
+    """The request as the C ABI takes it (the layout a client would send: node coordinates,
+    the state in the reference's ghosted P array, the cross-sections and the bc.txt records as
+    q2d_bc_rec), built once per case and kept with it."""
+    w = getattr(case, "_wire", None)
+    if w is not None:
+        return w
+    nb = len(case.blocks)
+    PD = C.POINTER(C.c_double)
+    w = {"nb": nb, "ni": (C.c_int * nb)(*[b.ni for b in case.blocks]),
+         "nj": (C.c_int * nb)(*[b.nj for b in case.blocks]),
+         "nodes": (PD * nb)(), "areas": (PD * nb)(), "prims": (PD * nb)(), "keep": []}
+    for k, b in enumerate(case.blocks):
+        nd = np.ascontiguousarray(b.nodes, dtype=np.float64)
+        P = b.prim_ghost(ghosts=None)
+        w["keep"] += [nd, P]
+        w["nodes"][k] = _abi.dptr(nd)
+        w["prims"][k] = _abi.dptr(P)
+        if b.area is not None:
+            a = np.ascontiguousarray(b.area, dtype=np.float64)
+            w["keep"].append(a)
+            w["areas"][k] = _abi.dptr(a)
+    w["recs"] = _abi.bc_array(case.bcs)
+    case._wire = w
+    return w
+
+
 class ServeContext:
     """A serving context: case slots over device pools sized from a byte budget."""
 
@@ -47,28 +74,10 @@ class ServeContext:
 
     def admit(self, case: CaseSpec) -> Optional[int]:
         """Admits a case; returns its slot, or None when slots or memory are exhausted."""
-        nb = len(case.blocks)
-        ni = (C.c_int * nb)(*[b.ni for b in case.blocks])
-        nj = (C.c_int * nb)(*[b.nj for b in case.blocks])
-        keep = []
-        PD = C.POINTER(C.c_double)
-        nodes = (PD * nb)()
-        areas = (PD * nb)()
-        prims = (PD * nb)()
-        for k, b in enumerate(case.blocks):
-            nd = np.ascontiguousarray(b.nodes, dtype=np.float64)
-            P = b.prim_ghost(ghosts=None)
-            keep += [nd, P]
-            nodes[k] = _abi.dptr(nd)
-            prims[k] = _abi.dptr(P)
-            if b.area is not None:
-                a = np.ascontiguousarray(b.area, dtype=np.float64)
-                keep.append(a)
-                areas[k] = _abi.dptr(a)
-        recs = _abi.bc_array(case.bcs)
+        w = wire(case)
         cid = C.c_int(-1)
-        st = self.lib.q2d_serve_admit(self.ctx, nb, ni, nj, nodes, areas, prims, recs, len(case.bcs),
-                                      C.byref(cid))
+        st = self.lib.q2d_serve_admit(self.ctx, w["nb"], w["ni"], w["nj"], w["nodes"], w["areas"], w["prims"],
+                                      w["recs"], len(case.bcs), C.byref(cid))
         if st == _abi.ERR_CAPACITY:
             return None
         self._check(st, "q2d_serve_admit")
@@ -136,8 +145,10 @@ class Request:
     meta: dict = field(default_factory=dict)
 
     def build(self) -> CaseSpec:
+        """The request's payload: the case and its C-ABI layout (client side)."""
         if self.case is None:
             self.case = request_case(self.kind, self.cells, np.random.default_rng(self.seed))
+            wire(self.case)
         return self.case
 
     @property
