@@ -245,6 +245,10 @@ def accuracy_leg(batch):
             "rel_l1_max": l1, "rel_linf_max": linf}
 
 
+WORKLOAD = ("batched area-variation nozzles (4096 independent cases per GPU, Nx~lognormal[64,1024], "
+            "Ny~U{8..64}), van Leer + HLLC, SSP-RK3, local dt")
+
+
 def reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -254,7 +258,9 @@ def reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "batched area-variation nozzles (CPU oracle sample)", "cases": len(batch)},
+            "config": {"workload": WORKLOAD, "cases_per_gpu": len(batch),
+                       "cells_per_gpu": int(sum(cs.cells for cs in batch)), "parallelism": "host threads",
+                       "measured_on": "a bounded sample of the cases (cpu_baseline.sample)"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -373,9 +379,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32-flux/fp64-state" if prec == 1 else "f64", "data": "synthetic",
-        "config": {"workload": "batched area-variation nozzles (4096 independent cases per GPU, "
-                               "Nx~lognormal[64,1024], Ny~U{8..64}), van Leer + HLLC, SSP-RK3, local dt",
-                   "cases_per_gpu": len(batch), "cells_per_gpu": cells,
+        "config": {"workload": WORKLOAD, "cases_per_gpu": len(batch), "cells_per_gpu": cells,
                    "schedule": tuned["schedule"],
                    "parallelism": f"replicas x{world} (independent cases per GPU)",
                    "l2": "inputs larger than L2 (state %.2f GB per buffer)" % (cells * 32 / 1e9)},
