@@ -110,6 +110,8 @@ typedef struct q2d_options {
     double sol_dtime;       /* sol-dtime */
     double gas_R;           /* specific gas constant R = Runiv/W of the single species */
     double gas_gamma;       /* ratio of specific heats of the calorically perfect closure */
+    double irs_beta;        /* irs-beta: implicit residual smoothing when > 0 (Lib_IRS.f90:17-177,
+                               Assign_Setup.f90:61); 0 by default */
 } q2d_options;
 
 /* One boundary-cell record: the 5-integer header line of bc.txt plus its property line

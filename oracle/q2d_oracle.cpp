@@ -1073,7 +1073,7 @@ inline double rk_coeff(int n_rk, int irk) {
 
 // Newstate_Conservative / Compute_Cons_NoIRS + Check_And_Fix_State
 // (Lib_Newstate.f90:14-161, 316-350)
-bool newstate(const q2d_oracle* o, Block& B, int irk, int& ei, int& ej) {
+bool newstate(const q2d_oracle* o, Block& B, int irk, int& ei, int& ej, bool scaled) {
     const Gas& g = o->gas;
     const double c = rk_coeff(o->opt.n_rk, irk);
     const double strangcoeff = 1.0;
@@ -1087,7 +1087,8 @@ bool newstate(const q2d_oracle* o, Block& B, int irk, int& ei, int& ej) {
             double* res = B.r(i, j);
             const double surface = B.sur[B.c(i, j)];
             const double dt = B.dtlocal[(i - 1) + B.ni * (j - 1)];
-            for (int v = 0; v < 4; ++v) res[v] = -res[v] / surface * dt * strangcoeff;
+            if (!scaled)   // Compute_Cons_NoIRS; with IRS the residual was scaled before smoothing
+                for (int v = 0; v < 4; ++v) res[v] = -res[v] / surface * dt * strangcoeff;
             double consold[4], cons[4];
             prim2cons(g, primold, consold);
             prim2cons(g, prim, cons);
@@ -1103,6 +1104,46 @@ bool newstate(const q2d_oracle* o, Block& B, int irk, int& ei, int& ej) {
         }
     if (!ok) { ei = bi; ej = bj; }
     return ok;
+}
+
+// Residual_Smoothing (Lib_IRS.f90:17-177): per grid direction, the first ghost layer of the
+// (scaled) residual is filled by Ghost_Residual_Extrapolation (connections copy the donor cell,
+// every other record the boundary cell), then two Jacobi sweeps of
+// R*(i) = (R(i) + beta (R*(i-1) + R*(i+1))) / (1 + 2 beta) along that direction replace R.
+void residual_smoothing(q2d_oracle* o, Case& cs, double beta) {
+    const int ndir = (o->blk[cs.blocks[0]].nj == 1) ? 1 : 2;
+    for (int d = 1; d <= ndir; ++d) {
+        for (const q2d_bc_rec& r : cs.bc) {   // Ghost_Residual_Extrapolation (:125-177)
+            Block& B = o->blk[cs.blocks[r.b - 1]];
+            const int gi = r.i - (r.f == 1 ? 1 : r.f == 2 ? -1 : 0);
+            const int gj = r.j - (r.f == 3 ? 1 : r.f == 4 ? -1 : 0);
+            const double* src = r.type == 101 ? o->blk[cs.blocks[r.bs - 1]].r(r.is, r.js) : B.r(r.i, r.j);
+            double* g = B.r(gi, gj);
+            for (int v = 0; v < 4; ++v) g[v] = src[v];
+        }
+        for (int bid : cs.blocks) {   // Residual_Smoothing_Blk (:45-119)
+            Block& B = o->blk[bid];
+            std::vector<double> S(B.R), Sn(B.R);
+            for (int it = 0; it < 2; ++it) {
+#pragma omp parallel for schedule(static)
+                for (int j = 1; j <= B.nj; ++j)
+                    for (int i = 1; i <= B.ni; ++i) {
+                        const int i1 = d == 1 ? i - 1 : i, j1 = d == 1 ? j : j - 1;
+                        const int i2 = d == 1 ? i + 1 : i, j2 = d == 1 ? j : j + 1;
+                        const double* r0 = B.r(i, j);
+                        const double* rm = &S[4 * B.c(i1, j1)];
+                        const double* rp = &S[4 * B.c(i2, j2)];
+                        double* out = &Sn[4 * B.c(i, j)];
+                        for (int v = 0; v < 4; ++v) out[v] = (r0[v] + beta * (rm[v] + rp[v])) / (1.0 + 2.0 * beta);
+                    }
+                for (int j = 1; j <= B.nj; ++j)
+                    for (int i = 1; i <= B.ni; ++i)
+                        std::memcpy(&S[4 * B.c(i, j)], &Sn[4 * B.c(i, j)], sizeof(double) * 4);
+            }
+            for (int j = 1; j <= B.nj; ++j)
+                for (int i = 1; i <= B.ni; ++i) std::memcpy(B.r(i, j), &S[4 * B.c(i, j)], sizeof(double) * 4);
+        }
+    }
 }
 
 // Compute_dt (Mod_dt.f90:10-106), Euler model (model == 0).
@@ -1197,8 +1238,22 @@ void explicit_step(q2d_oracle* o, Case& cs) {
             cs.err_stage = irk; cs.done = true; return;
         }
         for (int bid : cs.blocks) sources(o, o->blk[bid]);
+        const bool irs = op.irs_beta > 0.0;
+        if (irs) {   // Newstate_Conservative IRS branch (Lib_Newstate.f90:36-66): scale, smooth, update
+            for (int bid : cs.blocks) {
+                Block& B = o->blk[bid];
+                for (int j = 1; j <= B.nj; ++j)
+                    for (int i = 1; i <= B.ni; ++i) {
+                        double* res = B.r(i, j);
+                        const double surface = B.sur[B.c(i, j)];
+                        const double dt = B.dtlocal[(i - 1) + B.ni * (j - 1)];
+                        for (int v = 0; v < 4; ++v) res[v] = -res[v] / surface * dt * 1.0;
+                    }
+            }
+            residual_smoothing(o, cs, op.irs_beta);
+        }
         for (size_t lb = 0; lb < cs.blocks.size(); ++lb) {
-            if (!newstate(o, o->blk[cs.blocks[lb]], irk, ei, ej)) {
+            if (!newstate(o, o->blk[cs.blocks[lb]], irk, ei, ej, irs)) {
                 cs.err = Q2D_ERR_NAN; cs.err_b = (int)lb + 1; cs.err_i = ei; cs.err_j = ej;
                 cs.err_stage = irk; cs.done = true; return;
             }
@@ -1317,7 +1372,7 @@ int q2d_oracle_set_threads(int n) {
 
 int q2d_oracle_create(q2d_oracle** out, const q2d_options* opt) {
     if (!out || !opt) return Q2D_ERR_BADARG;
-    if (opt->n_rk < 1 || opt->n_rk > 3 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) ||
+    if (opt->n_rk < 1 || opt->n_rk > 3 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) || !(opt->irs_beta >= 0.0) ||
         opt->res_diter < 1 || opt->sol_diter < 1)
         return Q2D_ERR_BADARG;
     q2d_oracle* o = new (std::nothrow) q2d_oracle();

@@ -153,6 +153,7 @@ struct q2d_ctx {
     int grid = 0;
     // device pools and their allocators
     DevBuf<double> PA, PB, PC, SC, DL, FI, FJ, PART;
+    DevBuf<double> RA, RB;          // scaled residuals for implicit residual smoothing (irs_beta > 0)
     DevBuf<double> XFER;            // staging rows of one block's state for upload / download
     DevBuf<XferDesc> XDESC;         // block descriptors of a many-block transfer segment
     DevBuf<float> DL32, FI4, FJ4;   // FP32 geometry (FP32-flux form only): same regions as DL/FI/FJ
@@ -272,13 +273,29 @@ int enqueue_step(q2d_ctx* ctx, cudaStream_t s, int* nk) {
             else if (irk == 2) { a.Pin = ctx->PB.p; a.Pout = ctx->PC.p; }
             else { a.Pin = ctx->PC.p; a.Pout = ctx->PA.p; }
         }
-        if (ctx->kernel == 1)
-            CK(launch_march(a, ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter, ctx->grid, s));
-        else if (ctx->kernel == 2)
-            CK(launch_stage32(a, ctx->opt.riemann, ctx->tile, ctx->grid, s));
-        else
-            CK(launch_stage(a, ctx->opt.precision, ctx->opt.riemann, ctx->tile, ctx->grid, s));
-        ++*nk;
+        auto stage = [&](const StageArgs& x) -> int {
+            if (ctx->kernel == 1)
+                CK(launch_march(x, ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter, ctx->grid, s));
+            else if (ctx->kernel == 2)
+                CK(launch_stage32(x, ctx->opt.riemann, ctx->tile, ctx->grid, s));
+            else
+                CK(launch_stage(x, ctx->opt.precision, ctx->opt.riemann, ctx->tile, ctx->grid, s));
+            ++*nk;
+            return Q2D_OK;
+        };
+        if (ctx->opt.irs_beta > 0.0) {
+            // Newstate_Conservative with IRS (Lib_Newstate.f90:36-66): the stage's scaled residual
+            // (stage prologue and time steps as usual), smoothing along i then j, then the update
+            // (item counting, residual partials and case finalisation as the stage's last pass)
+            StageArgs r1 = a;
+            r1.irs_mode = 1; r1.Rout = ctx->RA.p; r1.last = 0;
+            if (int e = stage(r1)) return e;
+            CK(launch_irs(a, ctx->tile, ctx->grid, 1, ctx->opt.irs_beta, ctx->RA.p, ctx->RB.p, s));
+            CK(launch_irs(a, ctx->tile, ctx->grid, 2, ctx->opt.irs_beta, ctx->RB.p, ctx->RA.p, s));
+            *nk += 2;
+            a.irs_mode = 2; a.Rin = ctx->RA.p; a.first = 0;
+        }
+        if (int e = stage(a)) return e;
         if (a.last && a.fin_sep) {
             CK(launch_finalize(a, s));
             ++*nk;
@@ -732,6 +749,7 @@ int apply_pending(q2d_ctx* ctx) {
 
 int allocate_pools(q2d_ctx* ctx, long long ec, long long eg, long long efi, long long efj, int ncases) {
     CK(ctx->PA.alloc(ec)); CK(ctx->PB.alloc(ec)); CK(ctx->PC.alloc(ec));
+    if (ctx->opt.irs_beta > 0.0) { CK(ctx->RA.alloc(ec)); CK(ctx->RB.alloc(ec)); }
     CK(ctx->SC.alloc(2 * ec)); CK(ctx->DL.alloc(eg)); CK(ctx->FI.alloc(efi)); CK(ctx->FJ.alloc(efj));
     if (ctx->opt.precision == Q2D_PREC_FP32_FLUX) {
         CK(ctx->DL32.alloc(eg)); CK(ctx->FI4.alloc(2 * efi)); CK(ctx->FJ4.alloc(2 * efj));
@@ -791,6 +809,7 @@ const Schedule kSchedules[] = {{0, 0, 16}, {0, 1, 16}, {0, 2, 16}, {1, 0, 8}, {1
 constexpr int kNumSchedules = (int)(sizeof(kSchedules) / sizeof(kSchedules[0]));
 
 bool schedule_allowed(const q2d_ctx* ctx, int k) {
+    if (kSchedules[k].kernel == 1 && ctx->opt.irs_beta > 0.0) return false;   // no IRS passes
     return kSchedules[k].kernel != 2 || ctx->opt.precision == Q2D_PREC_FP32_FLUX;
 }
 
@@ -852,7 +871,7 @@ int check_options(const q2d_options* opt) {
     if (opt->n_rk < 1 || opt->n_rk > 3 || opt->limiter < 0 || opt->limiter > 6 || opt->riemann < 0 ||
         opt->riemann > 2 || opt->source < 0 || opt->source > 2 || opt->precision < 0 ||
         opt->precision > 1 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) || opt->res_diter < 1 ||
-        opt->sol_diter < 1 || !(opt->cfl > 0.0))
+        opt->sol_diter < 1 || !(opt->cfl > 0.0) || !(opt->irs_beta >= 0.0) || !(opt->irs_beta < 1e300))
         return Q2D_ERR_BADARG;
     return Q2D_OK;
 }
@@ -1266,7 +1285,8 @@ int q2d_serve_create(q2d_ctx** out, const q2d_options* opt, unsigned long long d
     // 2 planes with up to 50 % halo (24 B), i- and j-faces 3 planes each with up to 15 %
     // extra faces (55 B); the FP32-flux form adds FP32 copies of the ghost-frame and face
     // geometry (12 B + 55 B).
-    const double per_cell = opt->precision == Q2D_PREC_FP32_FLUX ? 306.4 : 239.2;
+    const double per_cell = (opt->precision == Q2D_PREC_FP32_FLUX ? 306.4 : 239.2) +
+                            (opt->irs_beta > 0.0 ? 64.0 : 0.0);   // two residual pools with IRS
     const long long cells = (long long)((double)device_bytes / per_cell);
     const long long ec = 4 * cells, eg = 3 * cells + 4096, efi = (long long)(3.45 * (double)cells) + 4096,
                     efj = efi;
@@ -1380,6 +1400,7 @@ void q2d_gpu_destroy(q2d_ctx* ctx) {
     ctx->PA.release(); ctx->PB.release(); ctx->PC.release(); ctx->SC.release(); ctx->DL.release();
     ctx->FI.release(); ctx->FJ.release(); ctx->PART.release(); ctx->dblocks.release(); ctx->XFER.release();
     ctx->XDESC.release();
+    ctx->RA.release(); ctx->RB.release();
     ctx->DL32.release(); ctx->FI4.release(); ctx->FJ4.release();
     ctx->dcases.release(); ctx->cstate.release(); ctx->items.release(); ctx->edges.release();
     ctx->bcp.release(); ctx->flag.release();

@@ -113,6 +113,12 @@ struct StageArgs {
     double cfl;
     int irk, n_rk;
     int first, last;       // stage is the first / last of the step
+    // implicit residual smoothing (Lib_Newstate.f90:36-66): 0 off; 1 the stage writes its scaled
+    // residual -R dt / sur to Rout and stops there; 2 the stage updates the state from the
+    // smoothed residual in Rin (no fluxes)
+    int irs_mode;
+    double* Rout;
+    const double* Rin;
     int dt_first;          // local time steps computed in the first stage from the step's
                            // starting state (else in the last stage of the previous step)
     int limiter, source, time_accurate, rampa;

@@ -175,99 +175,124 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
         const long long pc = B.pc;
         const double* scb = a.sc + 2 * B.oc;   // 8-plane scalar pool of the block
 
-        // ---- 1. asynchronous loads of everything the tile reads --------------------------
-        for (int idx = tid; idx < AREA; idx += NT) {
-            const int r = idx / W, c = idx - r * W;
-            if ((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2)) continue;
-            const int ii = i0 - 2 + c, jj = j0 - 2 + r;
-            const bool inI = (ii >= 0 && ii < ni), inJ = (jj >= 0 && jj < nj);
-            if (ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1) {
-                const double* src = a.dl + B.og + (long long)(jj + 2) * (ni + 4) + (ii + 2);
-                cp_async8(sD + idx, src);
-                cp_async8(sD + AREA + idx, src + B.pg);
-            }
-            if (inI && inJ) {
-                const double* src = Pin + (long long)jj * ni + ii;
+        const int irs = a.irs_mode;
+        double* sR = sFi;   // mode 2: the smoothed residual [4][NC] (NFI >= NC), no faces computed
+        if (irs == 2) {
+            for (int k = tid; k < NC; k += NT) {
+                const int row = k / TX, col = k - row * TX;
+                const int ii = i0 + col, jj = j0 + row;
+                if (ii >= ni || jj >= nj) continue;
+                const long long cg = (long long)jj * ni + ii;
+                const int sidx = (row + 2) * W + (col + 2);
 #pragma unroll
-                for (int v = 0; v < 4; ++v) cp_async8(sP + v * AREA + idx, src + v * pc);
-            } else if (inI != inJ) {   // every ghost the tile's faces read, from HBM
-                double q[4];
-                if (ghost_value(a, B, ii, jj, q)) {
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) sP[v * AREA + idx] = q[v];
+                for (int v = 0; v < 4; ++v) {
+                    cp_async8(sP + v * AREA + sidx, Pin + v * pc + cg);
+                    cp_async8(sC + v * NC + k, a.PO + B.oc + v * pc + cg);
+                    cp_async8(sR + v * NFI + k, a.Rin + B.oc + v * pc + cg);
+                }
+                if (a.last) {   // cell lengths of the next step's time step
+                    const double* src = a.dl + B.og + (long long)(jj + 2) * (ni + 4) + (ii + 2);
+                    cp_async8(sD + sidx, src);
+                    cp_async8(sD + AREA + sidx, src + B.pg);
                 }
             }
-        }
-        for (int k = tid; k < NC; k += NT) {
-            const int row = k / TX, col = k - row * TX;
-            const int ii = i0 + col, jj = j0 + row;
-            if (ii >= ni || jj >= nj) continue;
-            const long long cg = (long long)jj * ni + ii;
-            cp_async8(sC + 4 * NC + k, scb + cg);                                  // sur
-            if (!a.time_accurate) cp_async8(sC + 5 * NC + k, scb + pc + cg);       // dt
-            if (!a.first) {
-                const double* po = a.PO + B.oc + cg;
+        } else {
+            // ---- 1. asynchronous loads of everything the tile reads --------------------------
+            for (int idx = tid; idx < AREA; idx += NT) {
+                const int r = idx / W, c = idx - r * W;
+                if ((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2)) continue;
+                const int ii = i0 - 2 + c, jj = j0 - 2 + r;
+                const bool inI = (ii >= 0 && ii < ni), inJ = (jj >= 0 && jj < nj);
+                if (ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1) {
+                    const double* src = a.dl + B.og + (long long)(jj + 2) * (ni + 4) + (ii + 2);
+                    cp_async8(sD + idx, src);
+                    cp_async8(sD + AREA + idx, src + B.pg);
+                }
+                if (inI && inJ) {
+                    const double* src = Pin + (long long)jj * ni + ii;
 #pragma unroll
-                for (int v = 0; v < 4; ++v) cp_async8(sC + v * NC + k, po + v * pc);
+                    for (int v = 0; v < 4; ++v) cp_async8(sP + v * AREA + idx, src + v * pc);
+                } else if (inI != inJ) {   // every ghost the tile's faces read, from HBM
+                    double q[4];
+                    if (ghost_value(a, B, ii, jj, q)) {
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) sP[v * AREA + idx] = q[v];
+                    }
+                }
             }
-        }
-        for (int f = tid; f < NFI + NFJ; f += NT) {
-            if (f < NFI) {
-                const int row = f / (TX + 1), col = f - row * (TX + 1);
-                const int jj = j0 + row, F = i0 + col;
-                if (jj >= nj || F > ni) continue;
-                const double* src = a.fi + B.ofi + (long long)jj * (ni + 1) + F;
+            for (int k = tid; k < NC; k += NT) {
+                const int row = k / TX, col = k - row * TX;
+                const int ii = i0 + col, jj = j0 + row;
+                if (ii >= ni || jj >= nj) continue;
+                const long long cg = (long long)jj * ni + ii;
+                cp_async8(sC + 4 * NC + k, scb + cg);                                  // sur
+                if (!a.time_accurate) cp_async8(sC + 5 * NC + k, scb + pc + cg);       // dt
+                if (!a.first) {
+                    const double* po = a.PO + B.oc + cg;
 #pragma unroll
-                for (int q = 0; q < 3; ++q) cp_async8(sGi + q * NFI + f, src + q * B.pfi);
-            } else {
-                const int ff = f - NFI;
-                const int row = ff / TX, col = ff - row * TX;
-                const int ii = i0 + col, G = j0 + row;
-                if (ii >= ni || G > nj) continue;
-                const double* src = a.fj + B.ofj + (long long)G * ni + ii;
+                    for (int v = 0; v < 4; ++v) cp_async8(sC + v * NC + k, po + v * pc);
+                }
+            }
+            for (int f = tid; f < NFI + NFJ; f += NT) {
+                if (f < NFI) {
+                    const int row = f / (TX + 1), col = f - row * (TX + 1);
+                    const int jj = j0 + row, F = i0 + col;
+                    if (jj >= nj || F > ni) continue;
+                    const double* src = a.fi + B.ofi + (long long)jj * (ni + 1) + F;
 #pragma unroll
-                for (int q = 0; q < 3; ++q) cp_async8(sGj + q * NFJ + ff, src + q * B.pfj);
+                    for (int q = 0; q < 3; ++q) cp_async8(sGi + q * NFI + f, src + q * B.pfi);
+                } else {
+                    const int ff = f - NFI;
+                    const int row = ff / TX, col = ff - row * TX;
+                    const int ii = i0 + col, G = j0 + row;
+                    if (ii >= ni || G > nj) continue;
+                    const double* src = a.fj + B.ofj + (long long)G * ni + ii;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) cp_async8(sGj + q * NFJ + ff, src + q * B.pfj);
+                }
             }
         }
         cp_async_wait_all();
         __syncthreads();
 
-        // ---- 3. interface slopes ---------------------------------------------------------
-        for (int k = tid; k < NSI + NSJ; k += NT) {
-            if (k < NSI) {
-                const int r = k / (TX + 3), c = k - r * (TX + 3);
-                const int p0 = (r + 2) * W + c;
-                const double da = sD[p0], db = sD[p0 + 1];
+        if (irs != 2) {
+            // ---- 3. interface slopes ---------------------------------------------------------
+            for (int k = tid; k < NSI + NSJ; k += NT) {
+                if (k < NSI) {
+                    const int r = k / (TX + 3), c = k - r * (TX + 3);
+                    const int p0 = (r + 2) * W + c;
+                    const double da = sD[p0], db = sD[p0 + 1];
 #pragma unroll
-                for (int v = 0; v < 4; ++v)
-                    sSi[v * NSI + k] = iface_slope<ST>(sP[v * AREA + p0], sP[v * AREA + p0 + 1], da, db);
-            } else {
-                const int kk = k - NSI;
-                const int r = kk / TX, c = kk - r * TX;
-                const int p0 = r * W + c + 2;
-                const double da = sD[AREA + p0], db = sD[AREA + p0 + W];
+                    for (int v = 0; v < 4; ++v)
+                        sSi[v * NSI + k] = iface_slope<ST>(sP[v * AREA + p0], sP[v * AREA + p0 + 1], da, db);
+                } else {
+                    const int kk = k - NSI;
+                    const int r = kk / TX, c = kk - r * TX;
+                    const int p0 = r * W + c + 2;
+                    const double da = sD[AREA + p0], db = sD[AREA + p0 + W];
 #pragma unroll
-                for (int v = 0; v < 4; ++v)
-                    sSj[v * NSJ + kk] = iface_slope<ST>(sP[v * AREA + p0], sP[v * AREA + p0 + W], da, db);
+                    for (int v = 0; v < 4; ++v)
+                        sSj[v * NSJ + kk] = iface_slope<ST>(sP[v * AREA + p0], sP[v * AREA + p0 + W], da, db);
+                }
             }
-        }
-        __syncthreads();
+            __syncthreads();
 
-        // ---- 4. limited slope of every cell next to a face of the tile -------------------
-        switch (lim) {
-            case 0: sigma_phase<0, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-            case 1: sigma_phase<1, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-            case 2: sigma_phase<2, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-            case 3: sigma_phase<3, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-            case 4: sigma_phase<4, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-            case 5: sigma_phase<5, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-            default: sigma_phase<6, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-        }
-        __syncthreads();
+            // ---- 4. limited slope of every cell next to a face of the tile -------------------
+            switch (lim) {
+                case 0: sigma_phase<0, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                case 1: sigma_phase<1, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                case 2: sigma_phase<2, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                case 3: sigma_phase<3, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                case 4: sigma_phase<4, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                case 5: sigma_phase<5, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                default: sigma_phase<6, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+            }
+            __syncthreads();
 
-        // ---- 5. face fluxes (interior: Riemann on MUSCL states; boundary: BC_Fluxes) -----
-        face_phase<PREC, RIEM, true, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sGi, sGI, sFi);
-        face_phase<PREC, RIEM, false, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sGj, sGJ, sFj);
+            // ---- 5. face fluxes (interior: Riemann on MUSCL states; boundary: BC_Fluxes) -----
+            face_phase<PREC, RIEM, true, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sGi, sGI, sFi);
+            face_phase<PREC, RIEM, false, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sGj, sGJ, sFj);
+        }
         __syncthreads();
 
         // ---- 6. residual, sources, RK update (+ next dt and residual norm) ----------------
@@ -282,6 +307,15 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
             const int i1 = ii + 1, j1 = jj + 1;
             const int sidx = (row + 2) * W + (col + 2);
             const int fi0 = row * (TX + 1) + col, fj0 = row * TX + col;
+            const long long cg = (long long)jj * ni + ii;
+            double P[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) P[v] = sP[v * AREA + sidx];
+            double res[4];   // the scaled residual -R / sur * dt of the update
+            if (irs == 2) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) res[v] = sR[v * NFI + k];
+            } else {
             double r[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
@@ -298,11 +332,7 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
                 if (j1 == nj) x = x + Fj[fj0 + TX];
                 r[v] = x;
             }
-            const long long cg = (long long)jj * ni + ii;
             const double sur = sC[4 * NC + k];
-            double P[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) P[v] = sP[v * AREA + sidx];
             if (a.source == 1) {   // Source_Axi_Eul_Blk (Lib_Source_Axisymmetry.f90:57-76)
                 const double invr = scb[6 * pc + cg];
                 const double mod_v = sqrt(P[1] * P[1] + P[2] * P[2]);
@@ -327,10 +357,6 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
             }
             // Compute_Cons_NoIRS (Lib_Newstate.f90:131-159)
             const double dt = a.time_accurate ? dt_case : sC[5 * NC + k];
-            double PO[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) PO[v] = a.first ? P[v] : sC[v * NC + k];
-            double res[4];
             if (PREC == 0) {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) res[v] = -r[v] / sur * dt * 1.0;
@@ -339,6 +365,16 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) res[v] = r[v] * f;
             }
+            if (irs == 1) {   // Scale_Residual_Cons (Lib_Newstate.f90:86-92): smoothed before the update
+                double* ro = a.Rout + B.oc;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) ro[v * pc + cg] = res[v];
+                continue;
+            }
+            }
+            double PO[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) PO[v] = a.first ? P[v] : sC[v * NC + k];
             double U0[4], U[4];
             U0[0] = PO[0]; U0[1] = PO[0] * PO[1]; U0[2] = PO[0] * PO[2];
             if (PREC == 0) {
@@ -476,6 +512,72 @@ __global__ void resume_kernel(CaseState* cs, int n, int* launch_flag) {
     if (threadIdx.x == 0 && blockIdx.x == 0 && launch_flag) *launch_flag = 1;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
         if (cs[c].status == kStatus_Paused) cs[c].status = kStatus_Running;
+}
+
+// Residual_Smoothing along one grid direction (Lib_IRS.f90:45-119) for every running case: two
+// Jacobi sweeps R*(p) = (R(p) + beta (R*(p-1) + R*(p+1))) / (1 + 2 beta) over the block's
+// interior, R* = R at the start, evaluated per cell from R at p-2 .. p+2 (each first-sweep
+// value with the same operations as the sweep). The first ghost layer is R of the donor cell
+// for a connection and of the boundary cell otherwise (Ghost_Residual_Extrapolation,
+// :125-177), taken from Rin, the residual before this direction. A 1-D case (ndir = 1) is
+// copied through in direction 2.
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) irs_kernel(const StageArgs a, int dir, double beta,
+                                                 const double* __restrict__ Rin, double* __restrict__ Rout) {
+    if (threadIdx.x == 0 && blockIdx.x == 0 && a.launch_flag) *a.launch_flag = 1;
+    const double den = 1.0 + 2.0 * beta;
+    for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+        const WorkItem w = a.items[it];
+        if (__ldcg(&a.cstate[w.case_id].status) != kStatus_Running) continue;
+        const DBlock B = a.blocks[w.block];
+        const int ni = B.ni, nj = B.nj;
+        const int ndir = a.cases[w.case_id].ndir;
+        for (int k = threadIdx.x; k < TX * TY; k += NT) {
+            const int row = k / TX, col = k - row * TX;
+            const int ii = w.i0 + col, jj = w.j0 + row;
+            if (ii >= ni || jj >= nj) continue;
+            const long long cg = (long long)jj * ni + ii;
+            if (dir == 2 && ndir == 1) {
+                for (int v = 0; v < 4; ++v) Rout[B.oc + v * B.pc + cg] = Rin[B.oc + v * B.pc + cg];
+                continue;
+            }
+            const int n = dir == 1 ? ni : nj, p = dir == 1 ? ii : jj;
+            const long long stride = dir == 1 ? 1 : ni;
+            // the records of the two ghost cells of this line
+            const EdgeRec elo = a.edges[B.eo[dir == 1 ? 0 : 2] + (dir == 1 ? jj : ii)];
+            const EdgeRec ehi = a.edges[B.eo[dir == 1 ? 1 : 3] + (dir == 1 ? jj : ii)];
+            for (int v = 0; v < 4; ++v) {
+                const double* line = Rin + B.oc + v * B.pc + cg - (long long)p * stride;   // position 0
+                auto ghost = [&](const EdgeRec& e, int bpos) -> double {
+                    if (e.type == 101) {
+                        const DBlock D = a.blocks[e.bs];
+                        return Rin[D.oc + v * D.pc + (long long)(e.js - 1) * D.ni + (e.is - 1)];
+                    }
+                    return line[(long long)bpos * stride];
+                };
+                auto R = [&](int q) -> double {
+                    if (q < 0) return ghost(elo, 0);
+                    if (q >= n) return ghost(ehi, n - 1);
+                    return line[(long long)q * stride];
+                };
+                const double sm = p - 1 >= 0 ? (R(p - 1) + beta * (R(p - 2) + R(p))) / den : R(p - 1);
+                const double sp = p + 1 < n ? (R(p + 1) + beta * (R(p) + R(p + 2))) / den : R(p + 1);
+                Rout[B.oc + v * B.pc + cg] = (R(p) + beta * (sm + sp)) / den;
+            }
+        }
+    }
+}
+
+cudaError_t launch_irs(const StageArgs& a, int tile, int grid, int dir, double beta, const double* Rin,
+                       double* Rout, cudaStream_t s) {
+    switch (tile) {
+        case 1: irs_kernel<32, 8, 256><<<grid, 256, 0, s>>>(a, dir, beta, Rin, Rout); break;
+        case 2: irs_kernel<64, 4, 256><<<grid, 256, 0, s>>>(a, dir, beta, Rin, Rout); break;
+        case 3: irs_kernel<32, 16, 512><<<grid, 512, 0, s>>>(a, dir, beta, Rin, Rout); break;
+        case 4: irs_kernel<64, 8, 512><<<grid, 512, 0, s>>>(a, dir, beta, Rin, Rout); break;
+        default: irs_kernel<32, 10, 256><<<grid, 256, 0, s>>>(a, dir, beta, Rin, Rout); break;
+    }
+    return cudaGetLastError();
 }
 
 // End-of-step finalisation of every running case (residual norm, time step, TODO: the tail of

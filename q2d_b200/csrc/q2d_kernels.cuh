@@ -34,5 +34,7 @@ cudaError_t launch_transfer_many(const XferDesc* d, int nd, long long max_cells,
 cudaError_t launch_planes_to_cells(const double* in, long long pc, double* out, long long n, cudaStream_t s);
 cudaError_t launch_resume(CaseState* cs, int n, int* flag, cudaStream_t s);
 cudaError_t launch_finalize(const StageArgs& a, cudaStream_t s);
+cudaError_t launch_irs(const StageArgs& a, int tile, int grid, int dir, double beta, const double* Rin,
+                       double* Rout, cudaStream_t s);
 
 }  // namespace q2d

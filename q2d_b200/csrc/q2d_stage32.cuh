@@ -448,147 +448,167 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
         const int ndir = a.cases[w.case_id].ndir;
         const bool dt_here = a.dt_first && a.first;   // this stage computes the local time steps
 
-        // ---- 1. loads ------------------------------------------------------------------------
-        for (int k = tid; k < NC; k += NT) {   // FP64 cell data, asynchronous
-            const int row = k / TX, col = k - row * TX;
-            const int ii = i0 + col, jj = j0 + row;
-            if (ii >= ni || jj >= nj) continue;
-            const long long cg = (long long)jj * ni + ii;
-            if (!a.first) {
+        const int irs = a.irs_mode;
+        if (irs == 2) {   // update from the smoothed residual: the tile's own cells only
+            for (int k = tid; k < NC; k += NT) {
+                const int row = k / TX, col = k - row * TX;
+                const int ii = i0 + col, jj = j0 + row;
+                if (ii >= ni || jj >= nj) continue;
+                const long long cg = (long long)jj * ni + ii;
 #pragma unroll
-                for (int v = 0; v < 4; ++v) cp_async8(sC + v * NC + k, a.PO + B.oc + v * pc + cg);
-            } else if (dt_here) {   // the dt directions, into the planes U^n leaves free in stage 1
-                cp_async8(sC + k, scb + 2 * pc + cg);
-                cp_async8(sC + NC + k, scb + 3 * pc + cg);
-                if (ndir == 2) {
-                    cp_async8(sC + 2 * NC + k, scb + 4 * pc + cg);
-                    cp_async8(sC + 3 * NC + k, scb + 5 * pc + cg);
+                for (int v = 0; v < 4; ++v) {
+                    cp_async8(sC + (8 + v) * NC + k, Pin + v * pc + cg);
+                    cp_async8(sC + v * NC + k, a.PO + B.oc + v * pc + cg);
+                    cp_async8(sC + (4 + v) * NC + k, a.Rin + B.oc + v * pc + cg);
+                }
+                if (a.last && !a.dt_first) {   // cell lengths of the next step's time step
+                    const float* dsrc = a.dl32 + B.og + (long long)(jj + 2) * (ni + 4) + (ii + 2);
+                    sD2[(row + 2) * W + (col + 2)] = make_float2(__ldg(dsrc), __ldg(dsrc + B.pg));
                 }
             }
-            cp_async8(sC + 4 * NC + k, scb + cg);                                 // sur
-            if (!a.time_accurate && !dt_here) cp_async8(sC + 5 * NC + k, scb + pc + cg);   // dt
-            if (a.source) {
-                cp_async8(sC + 6 * NC + k, scb + 6 * pc + cg);
-                if (a.source == 2) cp_async8(sC + 7 * NC + k, scb + 7 * pc + cg);
-            }
-        }
-        // face geometry and the state / lengths of the cross-shaped halo: branch-free address
-        // selection so that every load of a thread is in flight before the first use
-        const float4* gi4 = a.fi4 + B.ofi / 2;
-        const float4* gj4 = a.fj4 + B.ofj / 2;
+        } else {
+            // ---- 1. loads ------------------------------------------------------------------------
+            for (int k = tid; k < NC; k += NT) {   // FP64 cell data, asynchronous
+                const int row = k / TX, col = k - row * TX;
+                const int ii = i0 + col, jj = j0 + row;
+                if (ii >= ni || jj >= nj) continue;
+                const long long cg = (long long)jj * ni + ii;
+                if (!a.first) {
 #pragma unroll
-        for (int u = 0; u < (NF + NT - 1) / NT; ++u) {
-            const int f = tid + u * NT;
-            bool ok;
-            const float4* src;
-            const EdgeRec* er = a.edges;   // the face's boundary record, if it is on the block's edge
-            bool edge;
-            if (f < NFI) {
-                const int row = f / (TX + 1), col = f - row * (TX + 1);
-                const int jj = j0 + row, F = i0 + col;
-                ok = jj < nj && F <= ni;
-                src = gi4 + (ok ? (long long)jj * (ni + 1) + F : 0);
-                edge = ok && (F == 0 || F == ni);
-                if (edge) er += B.eo[F == 0 ? 0 : 1] + jj;
-            } else {
-                const int ff = f - NFI;
-                const int row = ff / TX, col = ff - row * TX;
-                const int ii = i0 + col, G = j0 + row;
-                ok = f < NF && ii < ni && G <= nj;
-                src = gj4 + (ok ? (long long)G * ni + ii : 0);
-                edge = ok && (G == 0 || G == nj);
-                if (edge) er += B.eo[G == 0 ? 2 : 3] + ii;
+                    for (int v = 0; v < 4; ++v) cp_async8(sC + v * NC + k, a.PO + B.oc + v * pc + cg);
+                } else if (dt_here) {   // the dt directions, into the planes U^n leaves free in stage 1
+                    cp_async8(sC + k, scb + 2 * pc + cg);
+                    cp_async8(sC + NC + k, scb + 3 * pc + cg);
+                    if (ndir == 2) {
+                        cp_async8(sC + 2 * NC + k, scb + 4 * pc + cg);
+                        cp_async8(sC + 3 * NC + k, scb + 5 * pc + cg);
+                    }
+                }
+                cp_async8(sC + 4 * NC + k, scb + cg);                                 // sur
+                if (!a.time_accurate && !dt_here) cp_async8(sC + 5 * NC + k, scb + pc + cg);   // dt
+                if (a.source) {
+                    cp_async8(sC + 6 * NC + k, scb + 6 * pc + cg);
+                    if (a.source == 2) cp_async8(sC + 7 * NC + k, scb + 7 * pc + cg);
+                }
             }
-            float4 gq = __ldg(src);
-            if (edge) gq.w = pack_record(__ldg(&er->type), __ldg(&er->param));
-            if (ok) sG[f] = gq;
-        }
-        bool ghosts = false;   // the tile's halo reaches a ghost layer: second pass below
+            // face geometry and the state / lengths of the cross-shaped halo: branch-free address
+            // selection so that every load of a thread is in flight before the first use
+            const float4* gi4 = a.fi4 + B.ofi / 2;
+            const float4* gj4 = a.fj4 + B.ofj / 2;
 #pragma unroll
-        for (int u = 0; u < (AREA + NT - 1) / NT; ++u) {
-            const int idx = tid + u * NT;
-            const int r = idx / W, c = idx - r * W;
-            const int ii = i0 - 2 + c, jj = j0 - 2 + r;
-            const bool cross = idx < AREA && !((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2));
-            const bool inI = ii >= 0 && ii < ni, inJ = jj >= 0 && jj < nj;
-            const bool inner = cross && inI && inJ;
-            const bool indl = cross && ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1;
-            const double* src = Pin + (inner ? (long long)jj * ni + ii : 0);
-            const float* dsrc = a.dl32 + B.og + (indl ? (long long)(jj + 2) * (ni + 4) + (ii + 2) : 0);
-            const double q0 = __ldg(src), q1 = __ldg(src + pc), q2 = __ldg(src + 2 * pc), q3 = __ldg(src + 3 * pc);
-            const float d0 = __ldg(dsrc), d1 = __ldg(dsrc + B.pg);
-            if (indl) sD2[idx] = make_float2(d0, d1);
-            if (inner) sP[idx] = make_float4((float)q0, (float)q1, (float)q2, (float)q3);
-            if (inner && r >= 2 && r < TY + 2 && c >= 2 && c < TX + 2) {   // the tile's own cells, FP64
-                const int kk = (r - 2) * TX + (c - 2);
-                sC[8 * NC + kk] = q0; sC[9 * NC + kk] = q1; sC[10 * NC + kk] = q2; sC[11 * NC + kk] = q3;
+            for (int u = 0; u < (NF + NT - 1) / NT; ++u) {
+                const int f = tid + u * NT;
+                bool ok;
+                const float4* src;
+                const EdgeRec* er = a.edges;   // the face's boundary record, if it is on the block's edge
+                bool edge;
+                if (f < NFI) {
+                    const int row = f / (TX + 1), col = f - row * (TX + 1);
+                    const int jj = j0 + row, F = i0 + col;
+                    ok = jj < nj && F <= ni;
+                    src = gi4 + (ok ? (long long)jj * (ni + 1) + F : 0);
+                    edge = ok && (F == 0 || F == ni);
+                    if (edge) er += B.eo[F == 0 ? 0 : 1] + jj;
+                } else {
+                    const int ff = f - NFI;
+                    const int row = ff / TX, col = ff - row * TX;
+                    const int ii = i0 + col, G = j0 + row;
+                    ok = f < NF && ii < ni && G <= nj;
+                    src = gj4 + (ok ? (long long)G * ni + ii : 0);
+                    edge = ok && (G == 0 || G == nj);
+                    if (edge) er += B.eo[G == 0 ? 2 : 3] + ii;
+                }
+                float4 gq = __ldg(src);
+                if (edge) gq.w = pack_record(__ldg(&er->type), __ldg(&er->param));
+                if (ok) sG[f] = gq;
             }
-            // A ghost a face stencil of the tile reads: one of the two ghost layers, an i-ghost in
-            // a tile row or a j-ghost in a tile column (the boundary cell and its two inward
-            // neighbours are then in the same row or column of the tile and its halo). Its record
-            // type and boundary-face normal are parked in its own slot until the second pass.
-            const bool ghost = cross && inI != inJ && (!inI ? (r >= 2 && r < TY + 2) : (c >= 2 && c < TX + 2)) &&
-                               ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1;
-            if (ghost) {
-                int f, k, bi, bj;
-                if (!inI) { f = ii < 0 ? 1 : 2; k = jj; bi = ii < 0 ? 0 : ni - 1; bj = jj; }
-                else { f = jj < 0 ? 3 : 4; k = ii; bi = ii; bj = jj < 0 ? 0 : nj - 1; }
-                const int type = __ldg(&a.edges[B.eo[f - 1] + k].type);
-                const float4 gq = f <= 2 ? __ldg(gi4 + (long long)bj * (ni + 1) + (f == 1 ? 0 : ni))
-                                         : __ldg(gj4 + (long long)(f == 3 ? 0 : nj) * ni + bi);
-                sP[idx] = make_float4(__int_as_float(type), gq.x, gq.y, 0.0f);
-                ghosts = true;
-            }
-        }
-        if (__syncthreads_or(ghosts)) {
-            // ghost cells (Fill_Ghost_Cell, Lib_Ghost.f90:16-299) from the tile's FP32 state:
-            // symmetry mirrors the boundary cell's velocity about the face normal (:163-196),
-            // types 0 and 401-406 copy it (Ghost_ZG_Extrapolate, :199-219), the rest extrapolate
-            // quadratically (Ghost_Extrapolate, :270-299); connection ghosts copy the donor
-            // block's cells (Ghost_Connection, :143-160) from HBM
-#pragma unroll 1
+            bool ghosts = false;   // the tile's halo reaches a ghost layer: second pass below
+#pragma unroll
             for (int u = 0; u < (AREA + NT - 1) / NT; ++u) {
                 const int idx = tid + u * NT;
                 const int r = idx / W, c = idx - r * W;
                 const int ii = i0 - 2 + c, jj = j0 - 2 + r;
+                const bool cross = idx < AREA && !((r < 2 || r >= TY + 2) && (c < 2 || c >= TX + 2));
                 const bool inI = ii >= 0 && ii < ni, inJ = jj >= 0 && jj < nj;
-                if (idx >= AREA || inI == inJ || !(!inI ? (r >= 2 && r < TY + 2) : (c >= 2 && c < TX + 2)) ||
-                    ii < -2 || ii > ni + 1 || jj < -2 || jj > nj + 1)
-                    continue;
-                int gd, bi, bj, s1, nn;
-                if (!inI) {
-                    gd = ii < 0 ? -ii : ii - ni + 1; bi = ii < 0 ? 0 : ni - 1; bj = jj;
-                    s1 = ii < 0 ? 1 : -1; nn = ni;
-                } else {
-                    gd = jj < 0 ? -jj : jj - nj + 1; bi = ii; bj = jj < 0 ? 0 : nj - 1;
-                    s1 = jj < 0 ? W : -W; nn = nj;
+                const bool inner = cross && inI && inJ;
+                const bool indl = cross && ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1;
+                const double* src = Pin + (inner ? (long long)jj * ni + ii : 0);
+                const float* dsrc = a.dl32 + B.og + (indl ? (long long)(jj + 2) * (ni + 4) + (ii + 2) : 0);
+                const double q0 = __ldg(src), q1 = __ldg(src + pc), q2 = __ldg(src + 2 * pc), q3 = __ldg(src + 3 * pc);
+                const float d0 = __ldg(dsrc), d1 = __ldg(dsrc + B.pg);
+                if (indl) sD2[idx] = make_float2(d0, d1);
+                if (inner) sP[idx] = make_float4((float)q0, (float)q1, (float)q2, (float)q3);
+                if (inner && r >= 2 && r < TY + 2 && c >= 2 && c < TX + 2) {   // the tile's own cells, FP64
+                    const int kk = (r - 2) * TX + (c - 2);
+                    sC[8 * NC + kk] = q0; sC[9 * NC + kk] = q1; sC[10 * NC + kk] = q2; sC[11 * NC + kk] = q3;
                 }
-                const float4 park = sP[idx];
-                const int type = __float_as_int(park.x);
-                float4 q;
-                if (type == 101) {
-                    double qd[4] = {0.0, 0.0, 0.0, 0.0};
-                    ghost_value(a, B, ii, jj, qd);
-                    q = make_float4((float)qd[0], (float)qd[1], (float)qd[2], (float)qd[3]);
-                } else {
-                    const int sb = (bj - j0 + 2) * W + (bi - i0 + 2);
-                    const int d1 = nn >= 2 ? s1 : 0, d2 = nn >= 3 ? 2 * s1 : d1;
-                    const float4 b = sP[sb], c1 = sP[sb + d1], c2 = sP[sb + d2];
-                    if (type == 300) {
-                        const float nx = park.y, ny = park.z;
-                        const float un = b.y * nx + b.z * ny;
-                        q = make_float4(b.x, b.y - 2.0f * un * nx, b.z - 2.0f * un * ny, b.w);
-                    } else if (type == 0 || type == 401 || type == 405 || type == 406 || type < 0) {
-                        q = b;
+                // A ghost a face stencil of the tile reads: one of the two ghost layers, an i-ghost in
+                // a tile row or a j-ghost in a tile column (the boundary cell and its two inward
+                // neighbours are then in the same row or column of the tile and its halo). Its record
+                // type and boundary-face normal are parked in its own slot until the second pass.
+                const bool ghost = cross && inI != inJ && (!inI ? (r >= 2 && r < TY + 2) : (c >= 2 && c < TX + 2)) &&
+                                   ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1;
+                if (ghost) {
+                    int f, k, bi, bj;
+                    if (!inI) { f = ii < 0 ? 1 : 2; k = jj; bi = ii < 0 ? 0 : ni - 1; bj = jj; }
+                    else { f = jj < 0 ? 3 : 4; k = ii; bi = ii; bj = jj < 0 ? 0 : nj - 1; }
+                    const int type = __ldg(&a.edges[B.eo[f - 1] + k].type);
+                    const float4 gq = f <= 2 ? __ldg(gi4 + (long long)bj * (ni + 1) + (f == 1 ? 0 : ni))
+                                             : __ldg(gj4 + (long long)(f == 3 ? 0 : nj) * ni + bi);
+                    sP[idx] = make_float4(__int_as_float(type), gq.x, gq.y, 0.0f);
+                    ghosts = true;
+                }
+            }
+            if (__syncthreads_or(ghosts)) {
+                // ghost cells (Fill_Ghost_Cell, Lib_Ghost.f90:16-299) from the tile's FP32 state:
+                // symmetry mirrors the boundary cell's velocity about the face normal (:163-196),
+                // types 0 and 401-406 copy it (Ghost_ZG_Extrapolate, :199-219), the rest extrapolate
+                // quadratically (Ghost_Extrapolate, :270-299); connection ghosts copy the donor
+                // block's cells (Ghost_Connection, :143-160) from HBM
+#pragma unroll 1
+                for (int u = 0; u < (AREA + NT - 1) / NT; ++u) {
+                    const int idx = tid + u * NT;
+                    const int r = idx / W, c = idx - r * W;
+                    const int ii = i0 - 2 + c, jj = j0 - 2 + r;
+                    const bool inI = ii >= 0 && ii < ni, inJ = jj >= 0 && jj < nj;
+                    if (idx >= AREA || inI == inJ || !(!inI ? (r >= 2 && r < TY + 2) : (c >= 2 && c < TX + 2)) ||
+                        ii < -2 || ii > ni + 1 || jj < -2 || jj > nj + 1)
+                        continue;
+                    int gd, bi, bj, s1, nn;
+                    if (!inI) {
+                        gd = ii < 0 ? -ii : ii - ni + 1; bi = ii < 0 ? 0 : ni - 1; bj = jj;
+                        s1 = ii < 0 ? 1 : -1; nn = ni;
                     } else {
-                        const float4 g1 = make_float4(3.0f * b.x - 3.0f * c1.x + c2.x, 3.0f * b.y - 3.0f * c1.y + c2.y,
-                                                      3.0f * b.z - 3.0f * c1.z + c2.z, 3.0f * b.w - 3.0f * c1.w + c2.w);
-                        q = gd == 1 ? g1
-                                    : make_float4(3.0f * g1.x - 3.0f * b.x + c1.x, 3.0f * g1.y - 3.0f * b.y + c1.y,
-                                                  3.0f * g1.z - 3.0f * b.z + c1.z, 3.0f * g1.w - 3.0f * b.w + c1.w);
+                        gd = jj < 0 ? -jj : jj - nj + 1; bi = ii; bj = jj < 0 ? 0 : nj - 1;
+                        s1 = jj < 0 ? W : -W; nn = nj;
                     }
+                    const float4 park = sP[idx];
+                    const int type = __float_as_int(park.x);
+                    float4 q;
+                    if (type == 101) {
+                        double qd[4] = {0.0, 0.0, 0.0, 0.0};
+                        ghost_value(a, B, ii, jj, qd);
+                        q = make_float4((float)qd[0], (float)qd[1], (float)qd[2], (float)qd[3]);
+                    } else {
+                        const int sb = (bj - j0 + 2) * W + (bi - i0 + 2);
+                        const int d1 = nn >= 2 ? s1 : 0, d2 = nn >= 3 ? 2 * s1 : d1;
+                        const float4 b = sP[sb], c1 = sP[sb + d1], c2 = sP[sb + d2];
+                        if (type == 300) {
+                            const float nx = park.y, ny = park.z;
+                            const float un = b.y * nx + b.z * ny;
+                            q = make_float4(b.x, b.y - 2.0f * un * nx, b.z - 2.0f * un * ny, b.w);
+                        } else if (type == 0 || type == 401 || type == 405 || type == 406 || type < 0) {
+                            q = b;
+                        } else {
+                            const float4 g1 = make_float4(3.0f * b.x - 3.0f * c1.x + c2.x, 3.0f * b.y - 3.0f * c1.y + c2.y,
+                                                          3.0f * b.z - 3.0f * c1.z + c2.z, 3.0f * b.w - 3.0f * c1.w + c2.w);
+                            q = gd == 1 ? g1
+                                        : make_float4(3.0f * g1.x - 3.0f * b.x + c1.x, 3.0f * g1.y - 3.0f * b.y + c1.y,
+                                                      3.0f * g1.z - 3.0f * b.z + c1.z, 3.0f * g1.w - 3.0f * b.w + c1.w);
+                        }
+                    }
+                    sP[idx] = q;
                 }
-                sP[idx] = q;
             }
         }
         cp_async_wait_all();
@@ -599,89 +619,91 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             ps = lane == 0 ? __ldcg(&a.cstate[cid].status) : 0;
         }
 
-        // ---- 2. face fluxes ------------------------------------------------------------------
-        switch (a.limiter) {
-            case 0: interior_faces32<RIEM, 0, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-            case 1: interior_faces32<RIEM, 1, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-            case 2: interior_faces32<RIEM, 2, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-            case 3: interior_faces32<RIEM, 3, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-            case 4: interior_faces32<RIEM, 4, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-            case 5: interior_faces32<RIEM, 5, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-            default: interior_faces32<RIEM, 6, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-        }
-        {   // boundary faces (BC_Fluxes, Mod_BC_Fluxes.f90:79-269), on the threads with the fewest
-            // interior faces (the highest thread indices)
-            const int nrow = min(TY, nj - j0), ncol = min(TX, ni - i0);
-            const int nl = (i0 == 0) ? nrow : 0;
-            const int nr = (i0 + TX >= ni) ? nrow : 0;
-            const int nb = (j0 == 0) ? ncol : 0;
-            const int nt = (j0 + TY >= nj) ? ncol : 0;
-            for (int t = NT - 1 - tid; t < nl + nr + nb + nt; t += NT) {
-                int Fm, k, f;
-                boundary_face_slot<TX>(t, nl, nr, nb, i0, j0, ni, nj, NFI, Fm, k, f);
-                const int bi = Fm == 1 ? 0 : (Fm == 2 ? ni - 1 : k), bj = Fm == 3 ? 0 : (Fm == 4 ? nj - 1 : k);
-                const int di = Fm == 1 ? 1 : (Fm == 2 ? -1 : 0), dj = Fm == 3 ? 1 : (Fm == 4 ? -1 : 0);
-                struct { int type, param; } e;   // the record packed with the face geometry
-                const float4 gq = sG[f];
-                unpack_record(gq.w, e.type, e.param);
-                const int cb = (bj - j0 + 2) * W + (bi - i0 + 2);     // boundary cell
-                const int ci = cb + dj * W + di;                       // its inward neighbour
-                const float* dlp = Fm <= 2 ? sD : sD + 1;
-                const float nx = gq.x, ny = gq.y, ln = gq.z;
-                float X[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                if (e.type == 101) {   // BC_Connection_Eul: the interior scheme on the ghost stencil
-                    const int step = Fm <= 2 ? 1 : W;
-                    const int base = (Fm == 1 || Fm == 3) ? cb - 2 * step : cb - step;
-                    const bool ok = face32_lim<RIEM>(a.limiter, sP, dlp, base, step, nx, ny, ln, gam, gm1, gf, X);
-                    if (!ok) record_error(cs, 4, B.local_b, bi + 1, bj + 1, a.irk);
-                } else if (e.type == 300 || e.type == 400) {
-                    const float4 Bc = sP[cb], Ic = sP[ci];
-                    const float Bq[4] = {Bc.x, Bc.y, Bc.z, Bc.w}, Iq[4] = {Ic.x, Ic.y, Ic.z, Ic.w};
-                    if (e.type == 300)
-                        bc_symmetry32_lim<RIEM>(a.limiter, Fm, Bq, Iq, dlp[2 * cb], dlp[2 * ci], nx, ny, ln, gam, gm1,
-                                                gf, X);
-                    else
-                        bc_extrapolation32(Bq, nx, ny, ln, gf, X);
-                } else if (e.type > 0) {   // inflow / outflow records
-                    int path = 2;
-                    if (e.type == 401 && e.param >= 0) {   // stagnation inflow: FP32 when it decides, else FP64
+        if (irs != 2) {
+            // ---- 2. face fluxes ------------------------------------------------------------------
+            switch (a.limiter) {
+                case 0: interior_faces32<RIEM, 0, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 1: interior_faces32<RIEM, 1, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 2: interior_faces32<RIEM, 2, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 3: interior_faces32<RIEM, 3, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 4: interior_faces32<RIEM, 4, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 5: interior_faces32<RIEM, 5, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                default: interior_faces32<RIEM, 6, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+            }
+            {   // boundary faces (BC_Fluxes, Mod_BC_Fluxes.f90:79-269), on the threads with the fewest
+                // interior faces (the highest thread indices)
+                const int nrow = min(TY, nj - j0), ncol = min(TX, ni - i0);
+                const int nl = (i0 == 0) ? nrow : 0;
+                const int nr = (i0 + TX >= ni) ? nrow : 0;
+                const int nb = (j0 == 0) ? ncol : 0;
+                const int nt = (j0 + TY >= nj) ? ncol : 0;
+                for (int t = NT - 1 - tid; t < nl + nr + nb + nt; t += NT) {
+                    int Fm, k, f;
+                    boundary_face_slot<TX>(t, nl, nr, nb, i0, j0, ni, nj, NFI, Fm, k, f);
+                    const int bi = Fm == 1 ? 0 : (Fm == 2 ? ni - 1 : k), bj = Fm == 3 ? 0 : (Fm == 4 ? nj - 1 : k);
+                    const int di = Fm == 1 ? 1 : (Fm == 2 ? -1 : 0), dj = Fm == 3 ? 1 : (Fm == 4 ? -1 : 0);
+                    struct { int type, param; } e;   // the record packed with the face geometry
+                    const float4 gq = sG[f];
+                    unpack_record(gq.w, e.type, e.param);
+                    const int cb = (bj - j0 + 2) * W + (bi - i0 + 2);     // boundary cell
+                    const int ci = cb + dj * W + di;                       // its inward neighbour
+                    const float* dlp = Fm <= 2 ? sD : sD + 1;
+                    const float nx = gq.x, ny = gq.y, ln = gq.z;
+                    float X[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                    if (e.type == 101) {   // BC_Connection_Eul: the interior scheme on the ghost stencil
+                        const int step = Fm <= 2 ? 1 : W;
+                        const int base = (Fm == 1 || Fm == 3) ? cb - 2 * step : cb - step;
+                        const bool ok = face32_lim<RIEM>(a.limiter, sP, dlp, base, step, nx, ny, ln, gam, gm1, gf, X);
+                        if (!ok) record_error(cs, 4, B.local_b, bi + 1, bj + 1, a.irk);
+                    } else if (e.type == 300 || e.type == 400) {
                         const float4 Bc = sP[cb], Ic = sP[ci];
                         const float Bq[4] = {Bc.x, Bc.y, Bc.z, Bc.w}, Iq[4] = {Ic.x, Ic.y, Ic.z, Ic.w};
-                        path = bc_stagnation32(Fm, Bq, nx, ny, ln, gam, (float)g.R, a.bcp[e.param], X);
-                        if (path == 1) {
-                            bc_symmetry32_lim<RIEM>(a.limiter, Fm, Bq, Iq, dlp[2 * cb], dlp[2 * ci], nx, ny, ln, gam,
-                                                    gm1, gf, X);
-                            path = 0;
+                        if (e.type == 300)
+                            bc_symmetry32_lim<RIEM>(a.limiter, Fm, Bq, Iq, dlp[2 * cb], dlp[2 * ci], nx, ny, ln, gam, gm1,
+                                                    gf, X);
+                        else
+                            bc_extrapolation32(Bq, nx, ny, ln, gf, X);
+                    } else if (e.type > 0) {   // inflow / outflow records
+                        int path = 2;
+                        if (e.type == 401 && e.param >= 0) {   // stagnation inflow: FP32 when it decides, else FP64
+                            const float4 Bc = sP[cb], Ic = sP[ci];
+                            const float Bq[4] = {Bc.x, Bc.y, Bc.z, Bc.w}, Iq[4] = {Ic.x, Ic.y, Ic.z, Ic.w};
+                            path = bc_stagnation32(Fm, Bq, nx, ny, ln, gam, (float)g.R, a.bcp[e.param], X);
+                            if (path == 1) {
+                                bc_symmetry32_lim<RIEM>(a.limiter, Fm, Bq, Iq, dlp[2 * cb], dlp[2 * ci], nx, ny, ln, gam,
+                                                        gm1, gf, X);
+                                path = 0;
+                            }
+                        }
+                        if (path == 2) {   // FP64 from the FP64 state
+                            const double* pb = Pin + (long long)bj * ni + bi;
+                            const int ni2 = bi + di, nj2 = bj + dj;
+                            Q4 Bp, Ip;
+#pragma unroll
+                            for (int v = 0; v < 4; ++v) Bp.v[v] = __ldg(pb + v * pc);
+                            if (ni2 >= 0 && ni2 < ni && nj2 >= 0 && nj2 < nj) {
+                                const double* pi = Pin + (long long)nj2 * ni + ni2;
+#pragma unroll
+                                for (int v = 0; v < 4; ++v) Ip.v[v] = __ldg(pi + v * pc);
+                            } else {   // one-cell-thick block: the neighbour is the opposite ghost
+                                const float4 Ic = sP[ci];
+                                Ip.v[0] = Ic.x; Ip.v[1] = Ic.y; Ip.v[2] = Ic.z; Ip.v[3] = Ic.w;
+                            }
+                            const double* dlb = a.dl + B.og + (long long)(Fm <= 2 ? 0 : 1) * B.pg;
+                            const double dlbv = __ldg(dlb + (long long)(bj + 2) * (ni + 4) + (bi + 2));
+                            const double dli = __ldg(dlb + (long long)(nj2 + 2) * (ni + 4) + (ni2 + 2));
+                            const double* gsrc = Fm <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (Fm == 1 ? 0 : ni)
+                                                         : a.fj + B.ofj + (long long)(Fm == 3 ? 0 : nj) * ni + bi;
+                            const long long gs = Fm <= 2 ? B.pfi : B.pfj;
+                            const Q4 q = bc_face<RIEM>(a.gas, a.limiter, e.type, Fm, Bp, Ip, dlbv, dli, __ldg(gsrc),
+                                                       __ldg(gsrc + gs), __ldg(gsrc + 2 * gs),
+                                                       e.param >= 0 ? a.bcp + e.param : nullptr);
+#pragma unroll
+                            for (int v = 0; v < 4; ++v) X[v] = (float)q.v[v];
                         }
                     }
-                    if (path == 2) {   // FP64 from the FP64 state
-                        const double* pb = Pin + (long long)bj * ni + bi;
-                        const int ni2 = bi + di, nj2 = bj + dj;
-                        Q4 Bp, Ip;
-#pragma unroll
-                        for (int v = 0; v < 4; ++v) Bp.v[v] = __ldg(pb + v * pc);
-                        if (ni2 >= 0 && ni2 < ni && nj2 >= 0 && nj2 < nj) {
-                            const double* pi = Pin + (long long)nj2 * ni + ni2;
-#pragma unroll
-                            for (int v = 0; v < 4; ++v) Ip.v[v] = __ldg(pi + v * pc);
-                        } else {   // one-cell-thick block: the neighbour is the opposite ghost
-                            const float4 Ic = sP[ci];
-                            Ip.v[0] = Ic.x; Ip.v[1] = Ic.y; Ip.v[2] = Ic.z; Ip.v[3] = Ic.w;
-                        }
-                        const double* dlb = a.dl + B.og + (long long)(Fm <= 2 ? 0 : 1) * B.pg;
-                        const double dlbv = __ldg(dlb + (long long)(bj + 2) * (ni + 4) + (bi + 2));
-                        const double dli = __ldg(dlb + (long long)(nj2 + 2) * (ni + 4) + (ni2 + 2));
-                        const double* gsrc = Fm <= 2 ? a.fi + B.ofi + (long long)bj * (ni + 1) + (Fm == 1 ? 0 : ni)
-                                                     : a.fj + B.ofj + (long long)(Fm == 3 ? 0 : nj) * ni + bi;
-                        const long long gs = Fm <= 2 ? B.pfi : B.pfj;
-                        const Q4 q = bc_face<RIEM>(a.gas, a.limiter, e.type, Fm, Bp, Ip, dlbv, dli, __ldg(gsrc),
-                                                   __ldg(gsrc + gs), __ldg(gsrc + 2 * gs),
-                                                   e.param >= 0 ? a.bcp + e.param : nullptr);
-#pragma unroll
-                        for (int v = 0; v < 4; ++v) X[v] = (float)q.v[v];
-                    }
+                    sF[f] = make_float4(X[0], X[1], X[2], X[3]);
                 }
-                sF[f] = make_float4(X[0], X[1], X[2], X[3]);
             }
         }
         __syncthreads();
@@ -707,6 +729,11 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             for (int v = 0; v < 4; ++v) P[v] = sC[(8 + v) * NC + k];
             const int i1 = ii + 1, j1 = jj + 1;
             const int fi0 = row * (TX + 1) + col, fj0 = NFI + row * TX + col;
+            double q[4];   // the scaled residual -R dt / sur of the update
+            if (irs == 2) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) q[v] = sC[(4 + v) * NC + k];
+            } else {
             double r[4];
             const float4 Fw = sF[fi0], Fe = sF[fi0 + 1], Fs = sF[fj0], Fn = sF[fj0 + TX];
 #pragma unroll
@@ -751,17 +778,26 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
             } else {
                 dt = a.time_accurate ? dt_case : sC[5 * NC + k];
             }
+            const double fr = -dt * rcp64(sur);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) q[v] = r[v] * fr;
+            if (irs == 1) {   // Scale_Residual_Cons (Lib_Newstate.f90:86-92): smoothed before the update
+                double* ro = a.Rout + B.oc;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) ro[v * pc + cg] = q[v];
+                continue;
+            }
+            }
             double PO[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) PO[v] = a.first ? P[v] : sC[v * NC + k];
-            const double fr = -dt * rcp64(sur);
             double U0[4], U[4];
             U0[0] = PO[0]; U0[1] = PO[0] * PO[1]; U0[2] = PO[0] * PO[2];
             U0[3] = PO[3] * g.igm1 + 0.5 * PO[0] * (PO[1] * PO[1] + PO[2] * PO[2]);
             U[0] = P[0]; U[1] = P[0] * P[1]; U[2] = P[0] * P[2];
             U[3] = P[3] * g.igm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
 #pragma unroll
-            for (int v = 0; v < 4; ++v) U[v] = U0[v] + (U[v] - U0[v] + r[v] * fr) * a.rk_c;
+            for (int v = 0; v < 4; ++v) U[v] = U0[v] + (U[v] - U0[v] + q[v]) * a.rk_c;
             double N[4];
             N[0] = U[0];
             const double ir = rcp64(U[0]);

@@ -144,10 +144,12 @@ Setup read_options(const Ini& ini) {
         o.rampa_iter = (int)to_int(*v, "cfl-rise-threshold");
     if (const std::string* v = ini_get(ini, "Numerics", "time-accurate"))
         o.time_accurate = to_bool(*v, "time-accurate") ? 1 : 0;
-    if (const std::string* v = ini_get(ini, "Numerics", "irs"))
-        if (to_bool(*v, "irs")) s.unsupported.push_back("[Q2D-Numerics] irs = " + *v);
-    if (const std::string* v = ini_get(ini, "Numerics", "irs-beta"))
-        if (to_double(*v, "irs-beta") > 0.0) s.unsupported.push_back("[Q2D-Numerics] irs-beta = " + *v);
+    // implicit residual smoothing: on when irs-beta > 0 (Assign_Setup.f90:61); 'irs = true' with
+    // beta 0 smooths by the identity
+    if (const std::string* v = ini_get(ini, "Numerics", "irs-beta")) {
+        o.irs_beta = to_double(*v, "irs-beta");
+        if (o.irs_beta < 0.0) die("irs-beta must be >= 0");
+    }
     if (const std::string* v = ini_get(ini, "Numerics", "integration-variables"))
         if (lower(*v) != "cons") s.unsupported.push_back("[Q2D-Numerics] integration-variables = " + *v);
     // Setup_Space_Scheme (Mod_Space.f90:18-41) then Assign_Limiter (:44-78): the limiter keyword
@@ -557,10 +559,11 @@ int run(int argc, char** argv) {
         std::fprintf(f, "{\"limiter\": %d, \"riemann\": %d, \"n_rk\": %d, \"time_accurate\": %d, \"source\": %d, "
                         "\"precision\": %d, \"rampa_iter\": %d, \"res_diter\": %d, \"sol_diter\": %d, "
                         "\"itermax\": %lld, \"cfl\": %.17g, \"res_threshold\": %.17g, \"time_threshold\": %.17g, "
-                        "\"sol_dtime\": %.17g, \"gas_R\": %.17g, \"gas_gamma\": %.17g, \"shell_diter\": %d,\n",
+                        "\"sol_dtime\": %.17g, \"gas_R\": %.17g, \"gas_gamma\": %.17g, \"shell_diter\": %d, "
+                        "\"irs_beta\": %.17g,\n",
                      o.limiter, o.riemann, o.n_rk, o.time_accurate, o.source, o.precision, o.rampa_iter, o.res_diter,
                      o.sol_diter, o.itermax, o.cfl, o.res_threshold, o.time_threshold, o.sol_dtime, o.gas_R,
-                     o.gas_gamma, S.shell_diter);
+                     o.gas_gamma, S.shell_diter, o.irs_beta);
         std::fprintf(f, " \"blocks\": [");
         for (size_t b = 0; b < blocks.size(); ++b) {
             double s = 0.0, sa = 0.0;

@@ -49,6 +49,7 @@ def _ini(o: _abi.Options) -> str:
              f"cfl-rise-threshold = {o.rampa_iter}",
              f"time-scheme = {_SCHEME_NAMES[o.n_rk]}",
              f"time-accurate = {'true' if o.time_accurate else 'false'}",
+             f"irs-beta = {o.irs_beta!r}",
              "integration-variables = cons"]
     if o.limiter == 0:
         lines.append("space-reconstruction = first-order")

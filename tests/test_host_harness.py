@@ -17,7 +17,7 @@ from q2d_b200.solver import Q2DSolver
 
 GOLD = Path(__file__).resolve().parent / "golden"
 OPT_FIELDS = ["limiter", "riemann", "n_rk", "time_accurate", "source", "rampa_iter", "res_diter",
-              "sol_diter", "itermax", "cfl", "res_threshold", "time_threshold", "sol_dtime", "gas_R"]
+              "sol_diter", "itermax", "cfl", "res_threshold", "time_threshold", "sol_dtime", "gas_R", "irs_beta"]
 
 
 def host(*args, check=True):
@@ -93,10 +93,10 @@ def test_inputs_outside_the_path_fail_loudly(tmp_path):
     cs = cases.ramp(20, 8)
     refio.write_case(cs, tmp_path)
     ini = (tmp_path / "input.ini").read_text()
-    (tmp_path / "input.ini").write_text(ini.replace("[Q2D-Numerics]\n", "[Q2D-Numerics]\nirs-beta = 0.5\n")
+    (tmp_path / "input.ini").write_text(ini.replace("space-reconstruction = MUSCL", "space-reconstruction = MUSCL-SD")
                                         .replace("riemann-solver = HLLC", "riemann-solver = SLAU"))
     d = json.loads(host(tmp_path, "--check").stdout)
-    assert "[Q2D-Numerics] irs-beta = 0.5" in d["unsupported"]
+    assert "[Q2D-Numerics] space-reconstruction = MUSCL-SD" in d["unsupported"]
     assert "[Q2D-Numerics] riemann-solver = SLAU" in d["unsupported"]
     r = host(tmp_path, check=False)   # refused before any device call
     assert r.returncode == 2 and "not on the built path" in r.stderr
@@ -127,8 +127,8 @@ def test_reads_list_directed_records_across_lines(tmp_path):
     assert [r[4] for r in d["bcs"]] == [r["type"] for r in cs.bcs]
 
 
-def _python_run(cs, steps, precision):
-    s = Q2DSolver(make_options(cs, precision=precision), [cs])
+def _python_run(cs, steps, precision, irs_beta=0.0):
+    s = Q2DSolver(make_options(cs, precision=precision, irs_beta=irs_beta), [cs])
     try:
         s.step(steps, check=False)
         return [s.prim(0, b) for b in range(len(cs.blocks))], s.info(0)
@@ -137,16 +137,17 @@ def _python_run(cs, steps, precision):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name,precision", [("ramp", "fp64"), ("nozzle_axi", "fp64"), ("area_nozzle", "fp32-flux")])
-def test_host_run_equals_library_run(tmp_path, name, precision):
+@pytest.mark.parametrize("name,precision,irs", [("ramp", "fp64", 0.0), ("nozzle_axi", "fp64", 0.0),
+                                               ("area_nozzle", "fp32-flux", 0.0), ("nozzle_axi", "fp64", 0.5)])
+def test_host_run_equals_library_run(tmp_path, name, precision, irs):
     cs = small_cases()[name]
     steps = 25
-    refio.write_case(cs, tmp_path, itermax=steps)
+    refio.write_case(cs, tmp_path, itermax=steps, irs_beta=irs)
     o = make_options(cs)
     r = host(tmp_path, "--precision", precision, "--gamma", repr(o.gas_gamma), "--steps-per-call", 10)
     assert "converged/ended after 25 steps" in r.stdout
     got = refio.read_field(tmp_path / "OUTPUT" / "field.tec")
-    want, info = _python_run(cs, steps, 0 if precision == "fp64" else 1)
+    want, info = _python_run(cs, steps, 0 if precision == "fp64" else 1, irs)
     assert info["iter"] == steps
     for g, w, B in zip(got, want, cs.blocks):
         assert np.array_equal(g.nodes, np.asarray(B.nodes))
