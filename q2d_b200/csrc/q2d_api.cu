@@ -892,10 +892,14 @@ int check_recs(q2d_ctx* ctx, const HCase& cs, const std::vector<q2d_bc_rec>& v) 
             case 0: case 300: case 401: case 405: case 406:
                 if (r.f <= 2 && B.ni < 2) return fail(ctx, Q2D_ERR_BADARG, "set_bcs: block too thin");
                 break;
-            case 101:
+            case 101: {
                 if (r.bs < 1 || r.bs > (int)cs.blocks.size() || r.fs < 1 || r.fs > 4)
                     return fail(ctx, Q2D_ERR_BADARG, "set_bcs: bad connection donor");
+                const HBlock& D = ctx->blocks[cs.blocks[r.bs - 1]];
+                if (r.is < 1 || r.is > D.ni || r.js < 1 || r.js > D.nj)
+                    return fail(ctx, Q2D_ERR_BADARG, "set_bcs: connection donor cell out of range");
                 break;
+            }
             default:
                 return fail(ctx, Q2D_ERR_UNSUPPORTED, "set_bcs: BC type " + std::to_string(r.type) +
                                                           " is not on the built path");
