@@ -281,6 +281,46 @@ def area_nozzle(ni: int, nj: int, k: float, xt: float, p0: float, T0: float) -> 
                     {"k": k, "xt": xt, "p0": p0, "T0": T0})
 
 
+def planar_nozzle_area(x):
+    """Cross-section of the reference's planar-nozzle case (test/2D/euler/planar-nozzle/
+    gen_case.py:30-35): throat A_t = 1 at x_t = 0.4 on x in [0, 1], inlet A = 2, exit A = 2.5,
+    half-cosine blends on each side, so that dA/dx = 0 at the throat."""
+    x = np.asarray(x, dtype=np.float64)
+    up = 1.0 + (2.0 - 1.0) * 0.5 * (1.0 + np.cos(np.pi * x / 0.4))
+    down = 1.0 + (2.5 - 1.0) * 0.5 * (1.0 - np.cos(np.pi * (x - 0.4) / 0.6))
+    return np.where(x <= 0.4, up, down)
+
+
+def planar_nozzle(ni: int = 200, nj: int = 4) -> CaseSpec:
+    """The reference's planar-nozzle steady case (test/2D/euler/planar-nozzle/gen_case.py:19-94,
+    input.ini): x in [0, 1], y in [0, 0.1], the cross-section above as nodal Cross_Section,
+    constant-cp air (c_p = 1004.5, W = 28.970418, Runiv = 8314.462618), stagnation inflow
+    p0 = 1e6 Pa, T0 = 300 K (BC 401, 'normal'), extrapolation outflow (400), symmetry sides (300),
+    the quasi-1D isentropic state as initial condition (subsonic before the throat, supersonic
+    after); van Leer MUSCL + HLLC, SSP-RK3, CFL 0.5 with a 50-iteration ramp, IRS beta 0.5, local
+    time steps, area-variation sources, 40000 iterations at most."""
+    R = 8314.462618 / 28.970418
+    g = 1004.5 / (1004.5 - R)
+    p0, T0 = 1.0e6, 300.0
+    xn = np.linspace(0.0, 1.0, ni + 1)
+    yn = np.linspace(0.0, 0.1, nj + 1)
+    nodes = np.stack(np.meshgrid(xn, yn), axis=-1)
+    area = np.broadcast_to(planar_nozzle_area(xn)[None, :], (nj + 1, ni + 1)).copy()
+    xc = 0.5 * (xn[:-1] + xn[1:])
+    M = mach_of_area(planar_nozzle_area(xc), xc > 0.4, g)
+    rho, u, p = isentropic_state(M, p0, T0, R, g)
+    prim = np.zeros((nj, ni, 4))
+    prim[..., 0] = rho[None, :]
+    prim[..., 1] = u[None, :]
+    prim[..., 3] = p[None, :]
+    blk = BlockSpec(ni, nj, nodes, prim, area)
+    bcs = edge_records(1, ni, nj, {1: (401, stagnation_props(T0, p0)), 2: (400, {}),
+                                   3: (300, {}), 4: (300, {})})
+    opts = dict(limiter="vanleer", riemann="HLLC", n_rk=3, cfl=0.5, rampa_iter=50, time_accurate=0,
+                irs_beta=0.5, source="area_variation", itermax=40000, gas_R=R, gas_gamma=g)
+    return CaseSpec("planar_nozzle", [blk], bcs, opts, {"xc": xc, "p0": p0, "T0": T0})
+
+
 def area_nozzle_batch(n: int = 4096, seed: int = BASE_SEED + 3, nx_range=(64, 1024),
                       ny_range=(8, 64)) -> list:
     """The batched workload: n independent area-variation nozzles with

@@ -11,6 +11,10 @@ Fixtures written (all small text/npz files):
   riemann_exact.npz   exact Riemann solutions sampled at cell centres for the seeded 1-D
                       Riemann workloads, from the reference's own exact solver
                       (test/common/pycheck/q2d_exact1d.py:riemann_exact, imported, not copied)
+  planar_nozzle_residuals.txt   iteration and density residual of every line the reference
+                      binary printed while solving its planar-nozzle case (IRS beta 0.5,
+                      stagnation inflow, area-variation source; test/2D/euler/planar-nozzle/
+                      solve.log), the last line being the iteration that met res-threshold
 """
 import importlib.util
 import shutil
@@ -49,6 +53,14 @@ def main(ref_root: str) -> None:
     sol = ex.riemann_exact(np.array([0.5]), 0.2, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1, 1.4)
     out["toro1_pstar_ustar"] = np.array([sol["pstar"], sol["ustar"]])
     np.savez(HERE / "riemann_exact.npz", **out)
+    rows = []
+    for line in (ref / "test/2D/euler/planar-nozzle/solve.log").read_text().splitlines():
+        if "| Iter =" in line and "Density residual" in line:
+            it = int(line.split("Iter =")[1].split("|")[0])
+            res = float(line.split("Density residual =")[1].replace("D", "E"))
+            rows.append((it, res))
+    np.savetxt(HERE / "planar_nozzle_residuals.txt", np.array(rows), fmt=["%d", "%.6E"],
+               header="iteration density_residual (reference binary, test/2D/euler/planar-nozzle/solve.log)")
     print("written:", sorted(p.name for p in HERE.iterdir() if p.suffix in (".txt", ".npz")))
 
 

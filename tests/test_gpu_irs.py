@@ -81,3 +81,45 @@ def test_irs_fp32flux_vs_fp64(schedule):
     for ca, cb in zip(*out):
         for xa, xb in zip(ca, cb):
             assert rel_l1(xa, xb).max() <= 1e-6
+
+
+def test_planar_nozzle_reference_case_through_host(tmp_path):
+    """The reference's planar-nozzle case written in its own formats and run by q2d_host on the
+    GPU (FP64 form, IRS beta 0.5): the density residual follows the reference binary's printed
+    history within 5 %, res-threshold 1e-10 is met within 5 iterations of the binary (3172),
+    and the field it writes passes the case's area-law acceptance gates."""
+    from pathlib import Path
+    from q2d_b200 import refio
+    from tests.helpers import planar_nozzle_gates
+    from tests.test_host_harness import host
+    hist = np.loadtxt(Path(__file__).resolve().parent / "golden" / "planar_nozzle_residuals.txt")
+    cs = cases.planar_nozzle()
+    refio.write_case(cs, tmp_path)
+    gamma = make_options(cs).gas_gamma
+    host(tmp_path, "--gamma", repr(gamma), "--steps-per-call", 500, "--quiet")
+    res = np.loadtxt(tmp_path / "OUTPUT" / "residuals.dat")
+    by_iter = {int(r[0]): r[3] for r in res}
+    for it, ref in hist[:-1]:
+        assert abs(by_iter[int(it)] / ref - 1.0) < 0.05, (it, by_iter[int(it)], ref)
+    assert abs(res[-1, 0] - hist[-1, 0]) <= 5 and res[-1, 3] <= 1e-10
+    prim = refio.read_field(tmp_path / "OUTPUT" / "field.tec")[0].prim
+    planar_nozzle_gates(prim, cs.meta["xc"], gamma)
+
+
+def test_planar_nozzle_fp32flux_passes_the_area_law():
+    """The same case in the FP32-flux form: its residual stalls at the FP32 level of the fluxes
+    (far above the FP64 threshold), so it runs 4000 iterations; the state then passes the same
+    acceptance gates and differs from the FP64 form's by less than the form's bound."""
+    from tests.helpers import planar_nozzle_gates
+    cs = cases.planar_nozzle()
+    out = []
+    for prec in (1, 0):
+        s = Q2DSolver(make_options(cs, precision=prec, itermax=4000, res_threshold=0.0), [cs])
+        try:
+            infos = s.step(4000, check=False)
+            assert infos[0]["err"] == 0 and infos[0]["iter"] == 4000
+            out.append(s.prim(0, 0))
+        finally:
+            s.close()
+    planar_nozzle_gates(out[0], cs.meta["xc"], make_options(cs).gas_gamma)
+    assert rel_l1(out[0], out[1]).max() <= 1e-6
