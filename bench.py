@@ -364,6 +364,19 @@ def main():
                 "schedule": tuned64["schedule"] + " (autotuned)",
                 "ratio_fp32flux_over_fp64": value / v64}
         s64.close()
+    # ---- the same batch with implicit residual smoothing (irs-beta 0.5), FP32-flux form ----------
+    irs = None
+    if not args.no_fp64:
+        sir = Q2DSolver(make_options(batch[0], precision=prec, irs_beta=0.5), batch)
+        sir.set_schedule(tuned["schedule"].replace(" (autotuned)", "").replace(" (pinned)", ""))
+        sir.step(W)
+        Ki = max(5, K // 4)
+        msi, li = time_device(lib, sir, Ki)
+        msi = max_over_ranks(msi)
+        irs = {"value": cells_all * Ki / (msi / 1e3), "unit": UNIT, "steps": Ki, "ms_per_step": msi / Ki,
+               "irs_beta": 0.5, "gpu_launches": li, "schedule": sir.schedule,
+               "note": "each stage: scaled-residual pass, smoothing along i and j, update pass"}
+        sir.close()
     served = None
     if not args.no_serve:
         served = serving_leg(args, lib)
@@ -389,7 +402,7 @@ def main():
                      "bytes_per_cell_update": B_ALG, "launch_ms": t_launch * 1e3},
         "gpu_launches": launches, "errors": errs,
         "clocks": clk.summary(),
-        "e2e": e2e, "plain_fp64": fp64, "served": served, "accuracy_fp32flux": accuracy,
+        "e2e": e2e, "plain_fp64": fp64, "irs": irs, "served": served, "accuracy_fp32flux": accuracy,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
