@@ -275,9 +275,58 @@ inline Flux4 riemann_llf(const Gas& g, double dl, double ul, double vl, double p
     return F;
 }
 
+// riemann_SLAU_base + riemann_SLAU / riemann_SLAU2 (Lib_Riemann_SLAU.f90:10-124): mass flux
+// from the density-weighted normal speed with the low-Mach pressure term, the pressure flux by
+// Mach-split weights (SLAU: (1 - chi) blend; SLAU2: |V| a_F scaling), upwinded momentum and
+// total enthalpy.
+inline Flux4 riemann_slau(const Gas& g, bool slau2, double dltot, double ul, double vl, double pl, double al,
+                          double drtot, double ur, double vr, double pr, double ar, double nx, double ny) {
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    const double sq_veli = ul * ul + vl * vl;
+    const double sq_velj = ur * ur + vr * vr;
+    const double aF = 0.5 * (al + ar);
+    const double mL = unl / aF;
+    const double mR = unr / aF;
+    const double Mach_tilde = fmin_(1.0, std::sqrt(0.5 * (sq_veli + sq_velj)) / aF);
+    const double Chi = (1.0 - Mach_tilde) * (1.0 - Mach_tilde);
+    const double Vn_mag = (dltot * std::fabs(unl) + drtot * std::fabs(unr)) / (dltot + drtot);
+    const double f_rho = -fmax_(fmin_(mL, 0.0), -1.0) * fmin_(fmax_(mR, 0.0), 1.0);
+    const double Vn_magL = (1.0 - f_rho) * Vn_mag + f_rho * std::fabs(unl);
+    const double Vn_magR = (1.0 - f_rho) * Vn_mag + f_rho * std::fabs(unr);
+    Flux4 F;
+    F.r = 0.5 * (dltot * (unl + Vn_magL) + drtot * (unr - Vn_magR) - (Chi / aF) * (pr - pl));
+    double BetaL, BetaR;
+    if (std::fabs(mL) < 1.0) BetaL = 0.25 * (2.0 - mL) * ((mL + 1.0) * (mL + 1.0));
+    else BetaL = mL >= 0.0 ? 1.0 : 0.0;
+    if (std::fabs(mR) < 1.0) BetaR = 0.25 * (2.0 + mR) * ((mR - 1.0) * (mR - 1.0));
+    else BetaR = mR >= 0.0 ? 0.0 : 1.0;
+    const double p_half = slau2
+        ? 0.5 * (pl + pr) + 0.5 * (BetaL - BetaR) * (pl - pr) +
+              std::sqrt(0.5 * (sq_veli + sq_velj)) * (BetaL + BetaR - 1.0) * aF * 0.5 * (dltot + drtot)
+        : 0.5 * (pl + pr) + 0.5 * (BetaL - BetaR) * (pl - pr) +
+              (1.0 - Chi) * (BetaL + BetaR - 1.0) * 0.5 * (pl + pr);
+    const double H_L = H0(g, pl, dltot, std::sqrt(sq_veli));
+    const double H_R = H0(g, pr, drtot, std::sqrt(sq_velj));
+    if (F.r >= 0.0) {
+        F.u = F.r * ul + nx * p_half;
+        F.v = F.r * vl + ny * p_half;
+        F.e = F.r * H_L;
+    } else {
+        F.u = F.r * ur + nx * p_half;
+        F.v = F.r * vr + ny * p_half;
+        F.e = F.r * H_R;
+    }
+    return F;
+}
+
 inline Flux4 riemann(int kind, const Gas& g, const double* L, double aL, const double* R,
                      double aR, double nx, double ny) {
     switch (kind) {
+        case Q2D_RIEMANN_SLAU:
+        case Q2D_RIEMANN_SLAU2:
+            return riemann_slau(g, kind == Q2D_RIEMANN_SLAU2, L[0], L[1], L[2], L[3], aL, R[0], R[1], R[2],
+                                R[3], aR, nx, ny);
         case Q2D_RIEMANN_HLLE:
             return riemann_hlle(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR,
                                 R[0], nx, ny);

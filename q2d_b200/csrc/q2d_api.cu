@@ -809,7 +809,8 @@ const Schedule kSchedules[] = {{0, 0, 16}, {0, 1, 16}, {0, 2, 16}, {1, 0, 8}, {1
 constexpr int kNumSchedules = (int)(sizeof(kSchedules) / sizeof(kSchedules[0]));
 
 bool schedule_allowed(const q2d_ctx* ctx, int k) {
-    if (kSchedules[k].kernel == 1 && ctx->opt.irs_beta > 0.0) return false;   // no IRS passes
+    if (kSchedules[k].kernel == 1 && (ctx->opt.irs_beta > 0.0 || ctx->opt.riemann > 2))
+        return false;   // the warp-marching kernel has no IRS passes and no SLAU instantiation
     return kSchedules[k].kernel != 2 || ctx->opt.precision == Q2D_PREC_FP32_FLUX;
 }
 
@@ -869,7 +870,7 @@ int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
 
 int check_options(const q2d_options* opt) {
     if (opt->n_rk < 1 || opt->n_rk > 3 || opt->limiter < 0 || opt->limiter > 6 || opt->riemann < 0 ||
-        opt->riemann > 2 || opt->source < 0 || opt->source > 2 || opt->precision < 0 ||
+        opt->riemann > 4 || opt->source < 0 || opt->source > 2 || opt->precision < 0 ||
         opt->precision > 1 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) || opt->res_diter < 1 ||
         opt->sol_diter < 1 || !(opt->cfl > 0.0) || !(opt->irs_beta >= 0.0) || !(opt->irs_beta < 1e300))
         return Q2D_ERR_BADARG;

@@ -398,11 +398,61 @@ __device__ __forceinline__ F4 riemann_llf(const Gas& g, const double* L, double 
     return F;
 }
 
+// riemann_SLAU_base + riemann_SLAU / riemann_SLAU2 (Lib_Riemann_SLAU.f90:10-124), FP64, the
+// reference's operation order: mass flux from the density-weighted normal speed with the
+// low-Mach pressure term, pressure flux by Mach-split weights (SLAU: (1 - chi) blend; SLAU2:
+// |V| a_F scaling), momentum and total enthalpy upwinded on the mass flux.
+template <bool SLAU2>
+__device__ __forceinline__ F4 riemann_slau(const Gas& g, const double* L, double al, const double* R, double ar,
+                                           double nx, double ny) {
+    const double dltot = L[0], ul = L[1], vl = L[2], pl = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], pr = R[3];
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    const double sq_veli = ul * ul + vl * vl;
+    const double sq_velj = ur * ur + vr * vr;
+    const double aF = 0.5 * (al + ar);
+    const double mL = unl / aF;
+    const double mR = unr / aF;
+    const double Mach_tilde = dmin(1.0, sqrt(0.5 * (sq_veli + sq_velj)) / aF);
+    const double Chi = (1.0 - Mach_tilde) * (1.0 - Mach_tilde);
+    const double Vn_mag = (dltot * fabs(unl) + drtot * fabs(unr)) / (dltot + drtot);
+    const double f_rho = -dmax(dmin(mL, 0.0), -1.0) * dmin(dmax(mR, 0.0), 1.0);
+    const double Vn_magL = (1.0 - f_rho) * Vn_mag + f_rho * fabs(unl);
+    const double Vn_magR = (1.0 - f_rho) * Vn_mag + f_rho * fabs(unr);
+    F4 F;
+    F.r = 0.5 * (dltot * (unl + Vn_magL) + drtot * (unr - Vn_magR) - (Chi / aF) * (pr - pl));
+    double BetaL, BetaR;
+    if (fabs(mL) < 1.0) BetaL = 0.25 * (2.0 - mL) * ((mL + 1.0) * (mL + 1.0));
+    else BetaL = mL >= 0.0 ? 1.0 : 0.0;
+    if (fabs(mR) < 1.0) BetaR = 0.25 * (2.0 + mR) * ((mR - 1.0) * (mR - 1.0));
+    else BetaR = mR >= 0.0 ? 0.0 : 1.0;
+    const double p_half = SLAU2
+        ? 0.5 * (pl + pr) + 0.5 * (BetaL - BetaR) * (pl - pr) +
+              sqrt(0.5 * (sq_veli + sq_velj)) * (BetaL + BetaR - 1.0) * aF * 0.5 * (dltot + drtot)
+        : 0.5 * (pl + pr) + 0.5 * (BetaL - BetaR) * (pl - pr) +
+              (1.0 - Chi) * (BetaL + BetaR - 1.0) * 0.5 * (pl + pr);
+    const double H_L = H0(g, pl, dltot, sqrt(sq_veli));
+    const double H_R = H0(g, pr, drtot, sqrt(sq_velj));
+    if (F.r >= 0.0) {
+        F.u = F.r * ul + nx * p_half;
+        F.v = F.r * vl + ny * p_half;
+        F.e = F.r * H_L;
+    } else {
+        F.u = F.r * ur + nx * p_half;
+        F.v = F.r * vr + ny * p_half;
+        F.e = F.r * H_R;
+    }
+    return F;
+}
+
 template <int RIEM>
 __device__ __forceinline__ F4 riemann64(const Gas& g, const double* L, double al, const double* R,
                                         double ar, double nx, double ny) {
     if (RIEM == 1) return riemann_hlle(g, L, al, R, ar, nx, ny);
     if (RIEM == 2) return riemann_llf(g, L, al, R, ar, nx, ny);
+    if (RIEM == 3) return riemann_slau<false>(g, L, al, R, ar, nx, ny);
+    if (RIEM == 4) return riemann_slau<true>(g, L, al, R, ar, nx, ny);
     return riemann_hllc(g, L, al, R, ar, nx, ny);
 }
 

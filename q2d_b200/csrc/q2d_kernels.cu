@@ -641,10 +641,14 @@ cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int g
     if (prec == 0) {                                                                           \
         if (riem == 1) e = launch_stage_t<0, 1, TX, TY, NT>(a, grid, s);                      \
         else if (riem == 2) e = launch_stage_t<0, 2, TX, TY, NT>(a, grid, s);                 \
+        else if (riem == 3) e = launch_stage_t<0, 3, TX, TY, NT>(a, grid, s);                 \
+        else if (riem == 4) e = launch_stage_t<0, 4, TX, TY, NT>(a, grid, s);                 \
         else e = launch_stage_t<0, 0, TX, TY, NT>(a, grid, s);                                \
     } else {                                                                                   \
         if (riem == 1) e = launch_stage_t<1, 1, TX, TY, NT>(a, grid, s);                      \
         else if (riem == 2) e = launch_stage_t<1, 2, TX, TY, NT>(a, grid, s);                 \
+        else if (riem == 3) e = launch_stage_t<1, 3, TX, TY, NT>(a, grid, s);                 \
+        else if (riem == 4) e = launch_stage_t<1, 4, TX, TY, NT>(a, grid, s);                 \
         else e = launch_stage_t<1, 0, TX, TY, NT>(a, grid, s);                                \
     }
     Q2D_TILE_SWITCH(tile, Q2D_CALL)
@@ -657,11 +661,15 @@ int stage_occupancy(int prec, int riem, int tile) {
 #define Q2D_CALL(TX, TY, NT)                                                                   \
     if (prec == 0) {                                                                           \
         if (riem == 1) n = occupancy_t<0, 1, TX, TY, NT>();                                   \
-        else if (riem == 2) n = occupancy_t<0, 2, TX, TY, NT>();                              \
+        else if (riem == 2) n = occupancy_t<0, 2, TX, TY, NT>();                 \
+        else if (riem == 3) n = occupancy_t<0, 3, TX, TY, NT>();                 \
+        else if (riem == 4) n = occupancy_t<0, 4, TX, TY, NT>();                              \
         else n = occupancy_t<0, 0, TX, TY, NT>();                                             \
     } else {                                                                                   \
         if (riem == 1) n = occupancy_t<1, 1, TX, TY, NT>();                                   \
-        else if (riem == 2) n = occupancy_t<1, 2, TX, TY, NT>();                              \
+        else if (riem == 2) n = occupancy_t<1, 2, TX, TY, NT>();                 \
+        else if (riem == 3) n = occupancy_t<1, 3, TX, TY, NT>();                 \
+        else if (riem == 4) n = occupancy_t<1, 4, TX, TY, NT>();                              \
         else n = occupancy_t<1, 0, TX, TY, NT>();                                             \
     }
     Q2D_TILE_SWITCH(tile, Q2D_CALL)
@@ -779,19 +787,27 @@ cudaError_t launch_resume(CaseState* cs, int n, int* flag, cudaStream_t s) {
 cudaError_t launch_stage32_r0(const StageArgs& a, int tile, int grid, cudaStream_t s);
 cudaError_t launch_stage32_r1(const StageArgs& a, int tile, int grid, cudaStream_t s);
 cudaError_t launch_stage32_r2(const StageArgs& a, int tile, int grid, cudaStream_t s);
+cudaError_t launch_stage32_r3(const StageArgs& a, int tile, int grid, cudaStream_t s);
+cudaError_t launch_stage32_r4(const StageArgs& a, int tile, int grid, cudaStream_t s);
 int stage32_occupancy_r0(int tile);
 int stage32_occupancy_r1(int tile);
 int stage32_occupancy_r2(int tile);
+int stage32_occupancy_r3(int tile);
+int stage32_occupancy_r4(int tile);
 
 cudaError_t launch_stage32(const StageArgs& a, int riem, int tile, int grid, cudaStream_t s) {
     if (riem == 1) return launch_stage32_r1(a, tile, grid, s);
     if (riem == 2) return launch_stage32_r2(a, tile, grid, s);
+    if (riem == 3) return launch_stage32_r3(a, tile, grid, s);
+    if (riem == 4) return launch_stage32_r4(a, tile, grid, s);
     return launch_stage32_r0(a, tile, grid, s);
 }
 
 int stage32_occupancy(int riem, int tile) {
     if (riem == 1) return stage32_occupancy_r1(tile);
     if (riem == 2) return stage32_occupancy_r2(tile);
+    if (riem == 3) return stage32_occupancy_r3(tile);
+    if (riem == 4) return stage32_occupancy_r4(tile);
     return stage32_occupancy_r0(tile);
 }
 
@@ -803,6 +819,7 @@ Q2D_MARCH_DECL(1, 0) Q2D_MARCH_DECL(1, 1) Q2D_MARCH_DECL(1, 2)
 #undef Q2D_MARCH_DECL
 
 cudaError_t launch_march(const StageArgs& a, int prec, int riem, int lim, int grid, cudaStream_t s) {
+    if (riem > 2) return cudaErrorInvalidValue;   // the warp-marching schedule has no SLAU instantiation
     if (prec == 0) {
         if (riem == 1) return launch_march_p0_r1(a, lim, grid, s);
         if (riem == 2) return launch_march_p0_r2(a, lim, grid, s);
@@ -814,6 +831,7 @@ cudaError_t launch_march(const StageArgs& a, int prec, int riem, int lim, int gr
 }
 
 int march_occupancy(int prec, int riem, int lim) {
+    if (riem > 2) return 0;
     if (prec == 0) {
         if (riem == 1) return march_occupancy_p0_r1(lim);
         if (riem == 2) return march_occupancy_p0_r2(lim);

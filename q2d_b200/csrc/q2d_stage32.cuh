@@ -93,6 +93,31 @@ __device__ __forceinline__ void riemann_f32(const FS32& L, const FS32& R, float 
                                             float gm1, float gf, float* F) {
     const float irl = rcp_approx(L.r), irr = rcp_approx(R.r);
     const float al = sqrtf(gam * L.p * irl), ar = sqrtf(gam * R.p * irr);
+    if (RIEM == 3 || RIEM == 4) {   // SLAU / SLAU2 (Lib_Riemann_SLAU.f90:10-124)
+        const float sqi = L.u * L.u + L.v * L.v, sqj = R.u * R.u + R.v * R.v;
+        const float aF = 0.5f * (al + ar), iaF = rcp_approx(aF);
+        const float mL = L.un * iaF, mR = R.un * iaF;
+        const float vbar = sqrtf(0.5f * (sqi + sqj));
+        const float Mt = fminf(1.0f, vbar * iaF);
+        const float Chi = (1.0f - Mt) * (1.0f - Mt);
+        const float Vn = (L.r * fabsf(L.un) + R.r * fabsf(R.un)) * rcp_approx(L.r + R.r);
+        const float frho = -fmaxf(fminf(mL, 0.0f), -1.0f) * fminf(fmaxf(mR, 0.0f), 1.0f);
+        const float VnL = (1.0f - frho) * Vn + frho * fabsf(L.un);
+        const float VnR = (1.0f - frho) * Vn + frho * fabsf(R.un);
+        const float m = 0.5f * (L.r * (L.un + VnL) + R.r * (R.un - VnR) - Chi * iaF * (R.p - L.p));
+        const float BL = fabsf(mL) < 1.0f ? 0.25f * (2.0f - mL) * (mL + 1.0f) * (mL + 1.0f) : (mL >= 0.0f ? 1.0f : 0.0f);
+        const float BR = fabsf(mR) < 1.0f ? 0.25f * (2.0f + mR) * (mR - 1.0f) * (mR - 1.0f) : (mR >= 0.0f ? 0.0f : 1.0f);
+        const float pm = 0.5f * (L.p + R.p);
+        const float ph = RIEM == 4 ? pm + 0.5f * (BL - BR) * (L.p - R.p) + vbar * (BL + BR - 1.0f) * aF * 0.5f * (L.r + R.r)
+                                   : pm + 0.5f * (BL - BR) * (L.p - R.p) + (1.0f - Chi) * (BL + BR - 1.0f) * pm;
+        const bool up = m >= 0.0f;
+        const float h0 = up ? gf * L.p * irl + 0.5f * sqi : gf * R.p * irr + 0.5f * sqj;
+        F[0] = m;
+        F[1] = m * (up ? L.u : R.u) + nx * ph;
+        F[2] = m * (up ? L.v : R.v) + ny * ph;
+        F[3] = m * h0;
+        return;
+    }
     if (RIEM == 2) {
         const float A = fmaxf(fmaxf(fabsf(L.un - al), fabsf(R.un - ar)), fmaxf(fabsf(L.un + al), fabsf(R.un + ar)));
         const float igm1 = 1.0f / gm1;

@@ -94,10 +94,10 @@ def test_inputs_outside_the_path_fail_loudly(tmp_path):
     refio.write_case(cs, tmp_path)
     ini = (tmp_path / "input.ini").read_text()
     (tmp_path / "input.ini").write_text(ini.replace("space-reconstruction = MUSCL", "space-reconstruction = MUSCL-SD")
-                                        .replace("riemann-solver = HLLC", "riemann-solver = SLAU"))
+                                        .replace("riemann-solver = HLLC", "riemann-solver = AUSM+"))
     d = json.loads(host(tmp_path, "--check").stdout)
     assert "[Q2D-Numerics] space-reconstruction = MUSCL-SD" in d["unsupported"]
-    assert "[Q2D-Numerics] riemann-solver = SLAU" in d["unsupported"]
+    assert "[Q2D-Numerics] riemann-solver = AUSM+" in d["unsupported"]
     r = host(tmp_path, check=False)   # refused before any device call
     assert r.returncode == 2 and "not on the built path" in r.stderr
     (tmp_path / "input.ini").write_text(ini)

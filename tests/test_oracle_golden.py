@@ -53,6 +53,34 @@ def test_shuosher_negative_control():
     assert rel_l1 > 1e-7
 
 
+def sod79(riemann):
+    cs = cases.riemann_1d(ni=400, nj=1, states=(1.0, 1.0, 0.125, 0.1), limiter="mc", t_end=0.2)
+    for r in cs.bcs:   # the Sod79 case has BC 300 on every face (closed tube)
+        r["type"] = 300
+    return cs
+
+
+def sod79_l1(P):
+    ex = np.loadtxt(GOLD / "sod79_exact.txt")
+    xc = 0.5 * (np.linspace(0, 1, 401)[:-1] + np.linspace(0, 1, 401)[1:])
+    rho, p = P[0, :, 0], P[0, :, 3]
+    re = np.interp(xc, ex[:, 0], ex[:, 1])
+    pe = np.interp(xc, ex[:, 0], ex[:, 3])
+    return np.abs(rho - re).sum() / np.abs(re).sum(), np.abs(p - pe).sum() / np.abs(pe).sum()
+
+
+def test_sod79_slau_matches_reference_calibration():
+    """The reference's own Sod79 configuration (400 cells, MC + SLAU, RK3, CFL 0.9, t = 0.2,
+    closed tube; test/1D/Sod79/input.ini): the relative L1 errors of rho and p against the
+    exact solution equal the values the reference binary measured when the case's gates were
+    calibrated (test/1D/Sod79/check.py:14-15: 2.94e-3 and 2.08e-3) to the three digits
+    printed there."""
+    P, info = run_oracle(sod79("SLAU"), cfl=0.9, riemann="SLAU")
+    l1r, l1p = sod79_l1(P)
+    assert round(l1r, 5) == 0.00294 and round(l1p, 5) == 0.00208, (l1r, l1p)
+    assert info["todo"] == 3 and info["time"] >= 0.2
+
+
 def test_sod79_exact_gates():
     """Sod (rho 1/0.125, p 1/0.1) at 400 cells to t=0.2 with MC + HLLC, RK3, CFL 0.9:
     relative L1 of rho and p against the reference's exact.txt within the check.py gates
