@@ -55,17 +55,17 @@ def test_sod79_slau_on_gpu_matches_reference_calibration():
 
 
 @pytest.mark.parametrize("riemann", ["SLAU", "SLAU2"])
-def test_slau_fp32flux_vs_fp64(riemann):
-    batch = [cases.ramp(64, 24, seed=8), cases.nozzle_axi(ni=40, nj=12, nblocks=2, seed=5)]
+@pytest.mark.parametrize("which", ["ramp", "nozzle_axi"])
+def test_slau_fp32flux_vs_fp64(riemann, which):
+    cs = cases.ramp(64, 24, seed=8) if which == "ramp" else cases.nozzle_axi(ni=40, nj=12, nblocks=2, seed=5)
     out = []
     for prec in (1, 0):
-        s = Q2DSolver(make_options(batch[0], precision=prec, riemann=riemann), batch)
+        s = Q2DSolver(make_options(cs, precision=prec, riemann=riemann), [cs])
         try:
             infos = s.step(20, check=False)
-            assert all(i["err"] == 0 for i in infos)
-            out.append([[s.prim(c, b) for b in range(len(cs.blocks))] for c, cs in enumerate(batch)])
+            assert infos[0]["err"] == 0, (prec, infos[0])
+            out.append([s.prim(0, b) for b in range(len(cs.blocks))])
         finally:
             s.close()
-    for ca, cb in zip(*out):
-        for xa, xb in zip(ca, cb):
-            assert rel_l1(xa, xb).max() <= 1e-6
+    for xa, xb in zip(*out):
+        assert rel_l1(xa, xb).max() <= 1e-6
