@@ -11,6 +11,11 @@ Fixtures written (all small text/npz files):
   riemann_exact.npz   exact Riemann solutions sampled at cell centres for the seeded 1-D
                       Riemann workloads, from the reference's own exact solver
                       (test/common/pycheck/q2d_exact1d.py:riemann_exact, imported, not copied)
+  chang_nozzle.npz    the reference's chang-nozzle case (test/2D/euler/chang-nozzle): its grid
+                      nodes and initial state read from INPUT/ic.tec, the stagnation values of
+                      its BC 401 records (INPUT/bc.txt), and Chang's (1996) Mach number along the
+                      axis and the wall that its check.py compares against (reference/ref1.dat,
+                      ref2.dat)
   planar_nozzle_residuals.txt   iteration and density residual of every line the reference
                       binary printed while solving its planar-nozzle case (IRS beta 0.5,
                       stagnation inflow, area-variation source; test/2D/euler/planar-nozzle/
@@ -53,6 +58,21 @@ def main(ref_root: str) -> None:
     sol = ex.riemann_exact(np.array([0.5]), 0.2, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1, 1.4)
     out["toro1_pstar_ustar"] = np.array([sol["pstar"], sol["ustar"]])
     np.savez(HERE / "riemann_exact.npz", **out)
+    from q2d_b200 import refio
+    cdir = ref / "test/2D/euler/chang-nozzle"
+    blk = refio.read_field(cdir / "INPUT" / "ic.tec")[0]
+    props = None
+    lines = (cdir / "INPUT" / "bc.txt").read_text().splitlines()
+    for k, line in enumerate(lines):
+        t = line.split()
+        if len(t) == 5 and t[4] == "401":
+            vals = lines[k + 1].replace(",", " ").split()
+            cur = (float(vals[0]), float(vals[1]))
+            assert props is None or props == cur
+            props = cur
+    np.savez_compressed(HERE / "chang_nozzle.npz", nodes=blk.nodes, prim=blk.prim, T0_p0=np.array(props),
+                        axis_mach=np.loadtxt(cdir / "reference" / "ref1.dat"),
+                        wall_mach=np.loadtxt(cdir / "reference" / "ref2.dat"))
     rows = []
     for line in (ref / "test/2D/euler/planar-nozzle/solve.log").read_text().splitlines():
         if "| Iter =" in line and "Density residual" in line:

@@ -123,3 +123,31 @@ def test_planar_nozzle_fp32flux_passes_the_area_law():
             s.close()
     planar_nozzle_gates(out[0], cs.meta["xc"], make_options(cs).gas_gamma)
     assert rel_l1(out[0], out[1]).max() <= 1e-6
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_chang_nozzle_reference_case(precision):
+    """The reference's chang-nozzle case (axisymmetric source, IRS beta 0.5, MC + HLLC, CFL 0.8)
+    on the GPU: the FP64 form converges to the oracle's iteration count and state, the FP32-flux
+    form runs the case's 5000 iterations; both pass the case's gates against Chang's data along
+    the wall and the axis."""
+    from tests.helpers import chang_nozzle_case, chang_nozzle_gates
+    cs = chang_nozzle_case()
+    s = Q2DSolver(make_options(cs, precision=precision), [cs])
+    try:
+        info = s.solve(steps_per_call=500)
+        assert info["err"] == 0
+        prim = s.prim(0, 0)
+    finally:
+        s.close()
+    chang_nozzle_gates(cs, prim)
+    if precision == 0:
+        from oracle import oracle
+        o = oracle.solver(make_options(cs), [cs])
+        try:
+            oi = o.solve(steps_per_call=500)
+            ref = o.prim()
+        finally:
+            o.close()
+        assert info["iter"] == oi["iter"] and info["residual"][0] <= 1e-10
+        assert rel_linf(prim, ref).max() <= 1e-8

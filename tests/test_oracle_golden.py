@@ -232,3 +232,19 @@ def test_planar_nozzle_irs_matches_reference_binary():
         planar_nozzle_gates(s.prim(), cs.meta["xc"], opts.gas_gamma)
     finally:
         s.close()
+
+
+def test_chang_nozzle_axisymmetric_matches_reference_data():
+    """The reference's chang-nozzle case (axisymmetric source, IRS, stagnation inflow) through
+    the oracle: it converges (density residual below the case's 1e-6 sentinel within its 5000
+    iterations) and the Mach number along the wall and the axis passes the case's gates against
+    Chang's data (mean relative error < 5e-2, maximum < 1e-1)."""
+    from tests.helpers import chang_nozzle_case, chang_nozzle_gates
+    cs = chang_nozzle_case()
+    s = oracle.solver(make_options(cs), [cs])
+    try:
+        info = s.solve(steps_per_call=500)
+        assert info["err"] == 0 and info["residual"][0] < 1e-6, info
+        chang_nozzle_gates(cs, s.prim())
+    finally:
+        s.close()
