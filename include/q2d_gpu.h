@@ -114,6 +114,10 @@ typedef struct q2d_options {
     double gas_gamma;       /* ratio of specific heats of the calorically perfect closure */
     double irs_beta;        /* irs-beta: implicit residual smoothing when > 0 (Lib_IRS.f90:17-177,
                                Assign_Setup.f90:61); 0 by default */
+    int    shock_detector;  /* 1: space-reconstruction = MUSCL-SD, the limited slopes of a face
+                               scaled by the Tramel pressure sensor of its left / lower cell
+                               (Mod_Space.f90:25-27, Mod_Fluxes.f90:132-204,
+                               Lib_Shock_Detector.f90:14-38); 0 by default */
 } q2d_options;
 
 /* One boundary-cell record: the 5-integer header line of bc.txt plus its property line

@@ -354,6 +354,7 @@ struct Block {
     std::vector<double> f2;       // j-faces (1:ni,0:nj): nx ny len
     std::vector<double> dtlocal;  // (1:ni,1:nj)
     std::vector<double> inv_r, Gx, Gy;   // (1:ni,1:nj)
+    std::vector<double> beta;     // (1:ni,1:nj) shock sensor of the stage (MUSCL-SD only)
 
     int c(int i, int j) const { return (i + 1) + (ni + 4) * (j + 1); }
     double nx_(int i, int j) const { return node[2 * (i + (ni + 1) * j)]; }
@@ -365,6 +366,7 @@ struct Block {
     const double* face2(int i, int j) const { return &f2[3 * ((i - 1) + ni * j)]; }
     const double* face(int dir, int i, int j) const { return dir == 1 ? face1(i, j) : face2(i, j); }
     double dlc(int i, int j, int d) const { return dl[2 * c(i, j) + (d - 1)]; }
+    double sd(int i, int j) const { return beta[(i - 1) + ni * (j - 1)]; }
 };
 
 struct Case {
@@ -704,22 +706,48 @@ inline bool face_flux_from_states(const q2d_oracle* o, const double* P1, const d
     return true;
 }
 
-// Convective_Flux (Lib_Convective.f90:15-82): dl[-1..2], Prim[-1..2] along the direction.
+// Convective_Flux (Lib_Convective.f90:15-82): dl[-1..2], Prim[-1..2] along the direction; beta
+// scales both limited slopes (the SD_limiter branch, :40-47; 1 without MUSCL-SD).
 inline bool convective_flux(const q2d_oracle* o, const double* dlm1, const double* const* pr,
-                            double nx, double ny, double int_l, double* flux) {
+                            double nx, double ny, double int_l, double beta, double* flux) {
     const double l0 = 0.5 * (dlm1[0] + dlm1[1]);
     const double l1 = 0.5 * (dlm1[1] + dlm1[2]);
     const double l2 = 0.5 * (dlm1[2] + dlm1[3]);
     const double lm = 0.5 * dlm1[1];
     const double lp = 0.5 * dlm1[2];
     double P1[4], P4[4];
-    reconstruct(o->opt.limiter, pr[0], pr[1], pr[2], pr[3], l0, l1, l2, lm, lp, 1.0, P1, P4);
+    reconstruct(o->opt.limiter, pr[0], pr[1], pr[2], pr[3], l0, l1, l2, lm, lp, beta, P1, P4);
     return face_flux_from_states(o, P1, P4, nx, ny, int_l, flux);
+}
+
+// SD_Tramel (Lib_Shock_Detector.f90:14-38): Jameson-type pressure sensor on the cross stencil
+// p(i+-1, j), p(i, j+-1); 0 in shock cells, 1 - tanh(10 phi^3) (within 1.6e-7 of 1) elsewhere.
+inline double sd_tramel(double p, double p1, double p2, double p3, double p4) {
+    const double kp1 = std::fabs((p2 - 2.0 * p + p1) / (p2 + 2.0 * p + p1));
+    const double kp2 = std::fabs((p4 - 2.0 * p + p3) / (p4 + 2.0 * p + p3));
+    const double sw = std::max(kp1, kp2);
+    if (sw < 1.0 / 20.0) {
+        const double phi = std::max(sw / 20.0, 0.0);
+        return 1.0 - std::tanh(10.0 * phi * phi * phi);
+    }
+    return 0.0;
+}
+
+// beta(i,j) of every interior cell from the ghost-filled stage state (Mod_Fluxes.f90:132-138).
+void shock_sensor(Block& B) {
+    B.beta.resize((size_t)B.ni * B.nj);
+#pragma omp parallel for schedule(static)
+    for (int j = 1; j <= B.nj; ++j)
+        for (int i = 1; i <= B.ni; ++i)
+            B.beta[(i - 1) + B.ni * (j - 1)] = sd_tramel(B.pc(i, j)[3], B.pc(i - 1, j)[3], B.pc(i + 1, j)[3],
+                                                         B.pc(i, j - 1)[3], B.pc(i, j + 1)[3]);
 }
 
 // Fluxes_blk_omp_do (Mod_Fluxes.f90:97-234), Euler part. Returns false on a bad state.
 bool block_fluxes(const q2d_oracle* o, Block& B, int& eb_i, int& eb_j) {
     const int n1 = B.ni, n2 = B.nj;
+    const bool sd = o->opt.shock_detector != 0;
+    if (sd) shock_sensor(B);
     bool ok = true;
 #pragma omp parallel for schedule(static)
     for (int j = 1; j <= n2; ++j)
@@ -736,7 +764,7 @@ bool block_fluxes(const q2d_oracle* o, Block& B, int& eb_i, int& eb_j) {
             const double* pr[4] = {B.pc(i - 1, j), B.pc(i, j), B.pc(i + 1, j), B.pc(i + 2, j)};
             const double* f = B.face1(i, j);
             double fl[4];
-            if (!convective_flux(o, dl4, pr, f[0], f[1], f[2], fl)) {
+            if (!convective_flux(o, dl4, pr, f[0], f[1], f[2], sd ? B.sd(i, j) : 1.0, fl)) {
 #pragma omp critical
                 { if (ok) { ok = false; bi = i; bj = j; } }
                 continue;
@@ -754,7 +782,7 @@ bool block_fluxes(const q2d_oracle* o, Block& B, int& eb_i, int& eb_j) {
             const double* pr[4] = {B.pc(i, j - 1), B.pc(i, j), B.pc(i, j + 1), B.pc(i, j + 2)};
             const double* f = B.face2(i, j);
             double fl[4];
-            if (!convective_flux(o, dl4, pr, f[0], f[1], f[2], fl)) {
+            if (!convective_flux(o, dl4, pr, f[0], f[1], f[2], sd ? B.sd(i, j) : 1.0, fl)) {
 #pragma omp critical
                 { if (ok) { ok = false; bi = i; bj = j; } }
                 continue;
@@ -1051,8 +1079,10 @@ bool bc_connection(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm) {
     const double Dl4 = B.dlc(I4, J4, dir) * 0.5;
     const double Dist23 = Dl2 + Dl3, Dist12 = Dl1 + Dl2, Dist34 = Dl3 + Dl4;
     double PL[4], PR[4];
+    // SD_limiter: beta of the boundary cell (Lib_BC_Fluxes_Connection.f90, beta_ = blk%beta(Im,Jm))
+    const double beta = o->opt.shock_detector ? B.sd(Im, Jm) : 1.0;
     reconstruct(o->opt.limiter, B.pc(I1, J1), B.pc(I2, J2), B.pc(I3, J3), B.pc(I4, J4), Dist12,
-                Dist23, Dist34, Dl2, Dl3, 1.0, PL, PR);
+                Dist23, Dist34, Dl2, Dl3, beta, PL, PR);
     double F[4];
     if (!face_flux_from_states(o, PL, PR, fc[0], fc[1], fc[2], F)) return false;
     double* r = B.r(Im, Jm);
@@ -1422,7 +1452,7 @@ int q2d_oracle_set_threads(int n) {
 int q2d_oracle_create(q2d_oracle** out, const q2d_options* opt) {
     if (!out || !opt) return Q2D_ERR_BADARG;
     if (opt->n_rk < 1 || opt->n_rk > 3 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) || !(opt->irs_beta >= 0.0) ||
-        opt->res_diter < 1 || opt->sol_diter < 1)
+        opt->res_diter < 1 || opt->sol_diter < 1 || opt->shock_detector < 0 || opt->shock_detector > 1)
         return Q2D_ERR_BADARG;
     q2d_oracle* o = new (std::nothrow) q2d_oracle();
     if (!o) return Q2D_ERR_OOM;
@@ -1558,6 +1588,21 @@ int q2d_oracle_get_geometry(q2d_oracle* o, int block_id, double* dl, double* sur
 void q2d_oracle_destroy(q2d_oracle* o) { delete o; }
 
 double q2d_oracle_limiter(int limiter, double x, double y) { return rlimiter(limiter, x, y); }
+
+double q2d_oracle_sd_tramel(double p, double p1, double p2, double p3, double p4) {
+    return sd_tramel(p, p1, p2, p3, p4);
+}
+
+int q2d_oracle_shock_sensor(q2d_oracle* o, int block_id, double* beta) {
+    if (!o || block_id < 0 || block_id >= (int)o->blk.size() || !beta) return Q2D_ERR_BADARG;
+    int e = commit(o);
+    if (e) return e;
+    ghost_fill(o, o->cases[o->blk[block_id].case_id]);
+    Block& B = o->blk[block_id];
+    shock_sensor(B);
+    std::memcpy(beta, B.beta.data(), sizeof(double) * B.beta.size());
+    return Q2D_OK;
+}
 
 void q2d_oracle_riemann(int kind, const q2d_options* opt, const double* L, const double* R,
                         double nx, double ny, double* flux4) {

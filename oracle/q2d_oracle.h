@@ -45,8 +45,14 @@ int  q2d_oracle_set_threads(int n);   /* OpenMP threads used by the cell loops; 
 int  q2d_oracle_get_geometry(q2d_oracle* o, int block_id, double* dl, double* sur,
                              double* fi, double* fj);
 
+/* Shock sensor (SD_Tramel, Lib_Shock_Detector.f90:14-38) of every interior cell of a block,
+ * i fastest, from its current state with freshly filled ghosts: the 'beta' field the reference
+ * writes to its diagnostic output. */
+int  q2d_oracle_shock_sensor(q2d_oracle* o, int block_id, double* beta);
+
 /* Scalar kernels for known-answer tests. */
 double q2d_oracle_limiter(int limiter, double x, double y);
+double q2d_oracle_sd_tramel(double p, double p1, double p2, double p3, double p4);
 void   q2d_oracle_riemann(int riemann, const q2d_options* opt, const double* primL,
                           const double* primR, double nx, double ny, double* flux4);
 

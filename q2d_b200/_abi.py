@@ -40,7 +40,7 @@ class Options(C.Structure):
         ("itermax", C.c_longlong),
         ("cfl", C.c_double), ("res_threshold", C.c_double), ("time_threshold", C.c_double),
         ("sol_dtime", C.c_double), ("gas_R", C.c_double), ("gas_gamma", C.c_double),
-        ("irs_beta", C.c_double),
+        ("irs_beta", C.c_double), ("shock_detector", C.c_int),
     ]
 
 
@@ -91,6 +91,7 @@ def default_options(**kw) -> Options:
     o.gas_R = 287.0
     o.gas_gamma = 1.4
     o.irs_beta = 0.0
+    o.shock_detector = 0
     for k, v in kw.items():
         if isinstance(v, str):
             v = {"limiter": LIM, "riemann": RIEMANN, "source": SRC}[k][v]

@@ -216,6 +216,7 @@ StageArgs base_args(q2d_ctx* ctx) {
     a.cfl = ctx->opt.cfl;
     a.n_rk = ctx->opt.n_rk;
     a.limiter = ctx->opt.limiter;
+    a.sd = ctx->opt.shock_detector;
     a.source = ctx->opt.source;
     a.time_accurate = ctx->opt.time_accurate;
     a.rampa = ctx->opt.rampa_iter;
@@ -718,7 +719,8 @@ int rebuild_device_lists(q2d_ctx* ctx) {
         ctx->grid = (int)std::min<long long>(((long long)items.size() + 3) / 4, (long long)occ * ctx->num_sms);
     } else {
         const int occ = std::max(1, ctx->kernel == 2 ? stage32_occupancy(ctx->opt.riemann, ctx->tile)
-                                                     : stage_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->tile));
+                                                     : stage_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->tile,
+                                                                       ctx->opt.shock_detector));
         ctx->grid = (int)std::min<long long>((long long)items.size(), (long long)occ * ctx->num_sms);
     }
     if (ctx->grid < 1) ctx->grid = 1;
@@ -809,8 +811,11 @@ const Schedule kSchedules[] = {{0, 0, 16}, {0, 1, 16}, {0, 2, 16}, {1, 0, 8}, {1
 constexpr int kNumSchedules = (int)(sizeof(kSchedules) / sizeof(kSchedules[0]));
 
 bool schedule_allowed(const q2d_ctx* ctx, int k) {
-    if (kSchedules[k].kernel == 1 && (ctx->opt.irs_beta > 0.0 || ctx->opt.riemann > 2))
-        return false;   // the warp-marching kernel has no IRS passes and no SLAU instantiation
+    if (kSchedules[k].kernel == 1 &&
+        (ctx->opt.irs_beta > 0.0 || ctx->opt.riemann > 2 || ctx->opt.shock_detector))
+        return false;   // the warp-marching kernel has no IRS passes, SLAU or shock sensor
+    if (kSchedules[k].kernel == 0 && ctx->opt.shock_detector && ctx->opt.precision != Q2D_PREC_FP64)
+        return false;   // MUSCL-SD tile kernel: FP64 form only (FP32-flux: the FP32-flux kernel)
     return kSchedules[k].kernel != 2 || ctx->opt.precision == Q2D_PREC_FP32_FLUX;
 }
 
@@ -872,7 +877,8 @@ int check_options(const q2d_options* opt) {
     if (opt->n_rk < 1 || opt->n_rk > 3 || opt->limiter < 0 || opt->limiter > 6 || opt->riemann < 0 ||
         opt->riemann > 4 || opt->source < 0 || opt->source > 2 || opt->precision < 0 ||
         opt->precision > 1 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) || opt->res_diter < 1 ||
-        opt->sol_diter < 1 || !(opt->cfl > 0.0) || !(opt->irs_beta >= 0.0) || !(opt->irs_beta < 1e300))
+        opt->sol_diter < 1 || !(opt->cfl > 0.0) || !(opt->irs_beta >= 0.0) || !(opt->irs_beta < 1e300) ||
+        opt->shock_detector < 0 || opt->shock_detector > 1)
         return Q2D_ERR_BADARG;
     return Q2D_OK;
 }

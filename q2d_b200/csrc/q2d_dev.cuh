@@ -122,6 +122,7 @@ struct StageArgs {
     int dt_first;          // local time steps computed in the first stage from the step's
                            // starting state (else in the last stage of the previous step)
     int limiter, source, time_accurate, rampa;
+    int sd;                // MUSCL-SD: face slopes scaled by the Tramel sensor of the face's cell
     int res_diter, sol_diter, res_relative;
     long long itermax;
     double res_threshold, time_threshold, sol_dtime;
@@ -146,6 +147,30 @@ __device__ __forceinline__ bool gas_state_bad(double rho, double p) {
 }
 
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+
+// SD_Tramel (Lib_Shock_Detector.f90:14-38): pressure sensor on the cross stencil p1 = p(i-1,j),
+// p2 = p(i+1,j), p3 = p(i,j-1), p4 = p(i,j+1). 0 where max(kp1, kp2) >= 1/20 (a shock), else
+// 1 - tanh(10 phi^3), phi = sw/20 (within 1.6e-7 of 1).
+__device__ __forceinline__ double sd_tramel(double p, double p1, double p2, double p3, double p4) {
+    const double kp1 = fabs((p2 - 2.0 * p + p1) / (p2 + 2.0 * p + p1));
+    const double kp2 = fabs((p4 - 2.0 * p + p3) / (p4 + 2.0 * p + p3));
+    const double sw = kp1 > kp2 ? kp1 : kp2;
+    if (sw < 1.0 / 20.0) {
+        const double phi = sw / 20.0 > 0.0 ? sw / 20.0 : 0.0;
+        return 1.0 - tanh(10.0 * phi * phi * phi);
+    }
+    return 0.0;
+}
+__device__ __forceinline__ float sd_tramel32(float p, float p1, float p2, float p3, float p4) {
+    const float kp1 = fabsf((p2 - 2.0f * p + p1) / (p2 + 2.0f * p + p1));
+    const float kp2 = fabsf((p4 - 2.0f * p + p3) / (p4 + 2.0f * p + p3));
+    const float sw = kp1 > kp2 ? kp1 : kp2;
+    if (sw < 1.0f / 20.0f) {
+        const float phi = sw / 20.0f > 0.0f ? sw / 20.0f : 0.0f;
+        return 1.0f - tanhf(10.0f * phi * phi * phi);
+    }
+    return 0.0f;
+}
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
 
 // Limiters, FP64, operation order of Lib_Limiters.f90:26-110.

@@ -1,5 +1,5 @@
-// q2d_kernels.cuh — launch interface of the device code (q2d_kernels.cu) for the host
-// runtime (q2d_api.cu).
+// q2d_kernels.cuh — launch interface of the device code (q2d_kernels.cu and the stage kernels)
+// for the host runtime (q2d_api.cu).
 #pragma once
 #include "q2d_dev.cuh"
 
@@ -10,8 +10,11 @@ namespace q2d {
 constexpr int kNumTiles = 5;
 void tile_dims(int tile, int* tx, int* ty, int* nt);
 
+// FP64 stage kernel (q2d_stage64.cuh); a.sd selects the MUSCL-SD instantiation (FP64 form only).
 cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int grid, cudaStream_t s);
-int stage_occupancy(int prec, int riem, int tile);
+int stage_occupancy(int prec, int riem, int tile, int sd);
+cudaError_t launch_stage_sd(const StageArgs& a, int prec, int riem, int tile, int grid, cudaStream_t s);
+int stage_occupancy_sd(int prec, int riem, int tile);
 // FP32-flux stage kernel (q2d_stage32.cuh) on the same tiles and work items.
 cudaError_t launch_stage32(const StageArgs& a, int riem, int tile, int grid, cudaStream_t s);
 int stage32_occupancy(int riem, int tile);

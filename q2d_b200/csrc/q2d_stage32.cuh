@@ -182,9 +182,11 @@ __device__ __forceinline__ void riemann_f32(const FS32& L, const FS32& R, float 
 
 // One interior face: stencil cells m (= L-1), L, R, p (= R+1) at shared positions base + k*step;
 // dlp is the cell-length pair array viewed as floats, offset to the face's direction.
+// beta: the shock sensor scaling both limited slopes (1 without MUSCL-SD; Lib_Convective.f90:40-47)
 template <int RIEM, int LIM>
 __device__ __forceinline__ bool face32(const float4* sP, const float* dlp, int base, int step, float nx,
-                                      float ny, float len, float gam, float gm1, float gf, float* out) {
+                                      float ny, float len, float gam, float gm1, float gf, float beta,
+                                      float* out) {
     const float dm = dlp[2 * base], d0 = dlp[2 * (base + step)], d1 = dlp[2 * (base + 2 * step)],
                 d2 = dlp[2 * (base + 3 * step)];
     const float il0 = rcp_approx(0.5f * (dm + d0));
@@ -197,8 +199,8 @@ __device__ __forceinline__ bool face32(const float4* sP, const float* dlp, int b
     for (int v = 0; v < 4; ++v) {
         const float qm = comp(Cm, v), q0 = comp(C0, v), q1 = comp(C1, v), q2 = comp(C2, v);
         const float s0 = (q0 - qm) * il0, s1 = (q1 - q0) * il1, s2 = (q2 - q1) * il2;
-        QL[v] = q0 + lim32<LIM>(s1, s0) * lm;
-        QR[v] = q1 - lim32<LIM>(s2, s1) * lp;
+        QL[v] = q0 + beta * lim32<LIM>(s1, s0) * lm;
+        QR[v] = q1 - beta * lim32<LIM>(s2, s1) * lp;
     }
     const bool ok = QL[0] > 0.0f && QL[3] > 0.0f && QR[0] > 0.0f && QR[3] > 0.0f;
     const FS32 L = phys32(QL[0], QL[1], QL[2], QL[3], nx, ny, gf);
@@ -210,9 +212,17 @@ __device__ __forceinline__ bool face32(const float4* sP, const float* dlp, int b
     return ok;
 }
 
+// SD_Tramel (Lib_Shock_Detector.f90:14-38) of the tile cell at slot c, from the FP32 pressures of
+// its cross stencil.
+template <int W>
+__device__ __forceinline__ float sd_cell32(const float4* sP, int c) {
+    return sd_tramel32(sP[c].w, sP[c - 1].w, sP[c + 1].w, sP[c - W].w, sP[c + W].w);
+}
+
 // Interior faces of a tile (i faces, then j faces); boundary positions are left to the
-// boundary-face loop.
-template <int RIEM, int LIM, int NT, int TX, int TY>
+// boundary-face loop. With MUSCL-SD a face takes the sensor of its left / lower cell
+// (Mod_Fluxes.f90:140-204).
+template <int RIEM, int LIM, int NT, int TX, int TY, bool SD>
 __device__ __forceinline__ void interior_faces32(const StageArgs& a, const DBlock& B, CaseState* cs, int i0,
                                                  int j0, const float4* sP, const float* sD, const float4* sG,
                                                  float4* sF, float gam, float gm1, float gf) {
@@ -237,7 +247,8 @@ __device__ __forceinline__ void interior_faces32(const StageArgs& a, const DBloc
         if (k >= kmax || pos <= 0 || pos >= lenn) continue;
         float out[4];
         const float4 gq = sG[f];
-        const bool ok = face32<RIEM, LIM>(sP, dlp, base, step, gq.x, gq.y, gq.z, gam, gm1, gf, out);
+        const float beta = SD ? sd_cell32<W>(sP, base + step) : 1.0f;
+        const bool ok = face32<RIEM, LIM>(sP, dlp, base, step, gq.x, gq.y, gq.z, gam, gm1, gf, beta, out);
         if (!ok) record_error(cs, 4, B.local_b, ii, jj, a.irk);
         sF[f] = make_float4(out[0], out[1], out[2], out[3]);
     }
@@ -246,15 +257,15 @@ __device__ __forceinline__ void interior_faces32(const StageArgs& a, const DBloc
 template <int RIEM>
 __device__ __forceinline__ bool face32_lim(int lim, const float4* sP, const float* dlp, int base, int step,
                                           float nx, float ny, float len, float gam, float gm1, float gf,
-                                          float* out) {
+                                          float beta, float* out) {
     switch (lim) {
-        case 0: return face32<RIEM, 0>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        case 1: return face32<RIEM, 1>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        case 2: return face32<RIEM, 2>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        case 3: return face32<RIEM, 3>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        case 4: return face32<RIEM, 4>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        case 5: return face32<RIEM, 5>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
-        default: return face32<RIEM, 6>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, out);
+        case 0: return face32<RIEM, 0>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
+        case 1: return face32<RIEM, 1>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
+        case 2: return face32<RIEM, 2>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
+        case 3: return face32<RIEM, 3>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
+        case 4: return face32<RIEM, 4>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
+        case 5: return face32<RIEM, 5>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
+        default: return face32<RIEM, 6>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
     }
 }
 
@@ -407,7 +418,7 @@ __device__ __forceinline__ void boundary_face_slot(int t, int nl, int nr, int nb
     }
 }
 
-template <int RIEM, int TX, int TY, int NT, int MB>
+template <int RIEM, int TX, int TY, int NT, int MB, bool SD>
 __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
     using L = Tile32<TX, TY>;
     constexpr int W = L::W, AREA = L::AREA, NFI = L::NFI, NF = L::NF, NC = L::NC;
@@ -584,6 +595,26 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                     ghosts = true;
                 }
             }
+            if (SD && tid < 3) {
+                // pressures the sensor of the halo column / row on the tile's left / lower faces
+                // reads outside the cross the loads above fill: the corner (i0-1, j0-1), and
+                // (i0-1, min(j0+TY, nj)) / (min(i0+TX, ni), j0-1), a corner or, on a ragged tile, a
+                // ghost beside the cross
+                const int ii = tid == 1 ? min(i0 + TX, ni) : i0 - 1;
+                const int jj = tid == 2 ? min(j0 + TY, nj) : j0 - 1;
+                const bool need = tid == 0 ? (i0 > 0 || j0 > 0) : (tid == 1 ? j0 > 0 : i0 > 0);
+                if (need) {
+                    float p;
+                    if (ii >= 0 && ii < ni && jj >= 0 && jj < nj) {
+                        p = (float)__ldg(Pin + 3 * pc + (long long)jj * ni + ii);
+                    } else {
+                        double qd[4] = {0.0, 0.0, 0.0, 0.0};
+                        ghost_value(a, B, ii, jj, qd);
+                        p = (float)qd[3];
+                    }
+                    sP[(jj - j0 + 2) * W + (ii - i0 + 2)] = make_float4(0.0f, 0.0f, 0.0f, p);
+                }
+            }
             if (__syncthreads_or(ghosts)) {
                 // ghost cells (Fill_Ghost_Cell, Lib_Ghost.f90:16-299) from the tile's FP32 state:
                 // symmetry mirrors the boundary cell's velocity about the face normal (:163-196),
@@ -647,13 +678,13 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
         if (irs != 2) {
             // ---- 2. face fluxes ------------------------------------------------------------------
             switch (a.limiter) {
-                case 0: interior_faces32<RIEM, 0, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-                case 1: interior_faces32<RIEM, 1, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-                case 2: interior_faces32<RIEM, 2, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-                case 3: interior_faces32<RIEM, 3, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-                case 4: interior_faces32<RIEM, 4, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-                case 5: interior_faces32<RIEM, 5, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
-                default: interior_faces32<RIEM, 6, NT, TX, TY>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 0: interior_faces32<RIEM, 0, NT, TX, TY, SD>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 1: interior_faces32<RIEM, 1, NT, TX, TY, SD>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 2: interior_faces32<RIEM, 2, NT, TX, TY, SD>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 3: interior_faces32<RIEM, 3, NT, TX, TY, SD>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 4: interior_faces32<RIEM, 4, NT, TX, TY, SD>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                case 5: interior_faces32<RIEM, 5, NT, TX, TY, SD>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
+                default: interior_faces32<RIEM, 6, NT, TX, TY, SD>(a, B, cs, i0, j0, sP, sD, sG, sF, gam, gm1, gf); break;
             }
             {   // boundary faces (BC_Fluxes, Mod_BC_Fluxes.f90:79-269), on the threads with the fewest
                 // interior faces (the highest thread indices)
@@ -678,7 +709,10 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                     if (e.type == 101) {   // BC_Connection_Eul: the interior scheme on the ghost stencil
                         const int step = Fm <= 2 ? 1 : W;
                         const int base = (Fm == 1 || Fm == 3) ? cb - 2 * step : cb - step;
-                        const bool ok = face32_lim<RIEM>(a.limiter, sP, dlp, base, step, nx, ny, ln, gam, gm1, gf, X);
+                        // the sensor of the boundary cell (beta_ = blk%beta(Im,Jm))
+                        const float beta = SD ? sd_cell32<W>(sP, cb) : 1.0f;
+                        const bool ok = face32_lim<RIEM>(a.limiter, sP, dlp, base, step, nx, ny, ln, gam, gm1, gf,
+                                                         beta, X);
                         if (!ok) record_error(cs, 4, B.local_b, bi + 1, bj + 1, a.irk);
                     } else if (e.type == 300 || e.type == 400) {
                         const float4 Bc = sP[cb], Ic = sP[ci];
@@ -878,10 +912,12 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
     }
 }
 
-template <int RIEM, int TX, int TY, int NT, int MB>
-cudaError_t launch_stage32_t(const StageArgs& a, int grid, cudaStream_t s) {
+// SD: the MUSCL-SD instantiation (the shock sensor in the face phase), a separate kernel so that
+// the plain form keeps its register allocation.
+template <int RIEM, int TX, int TY, int NT, int MB, bool SD>
+cudaError_t launch_stage32_sd(const StageArgs& a, int grid, cudaStream_t s) {
     constexpr size_t smem = Tile32<TX, TY>::bytes;
-    auto k = stage32_kernel<RIEM, TX, TY, NT, MB>;
+    auto k = stage32_kernel<RIEM, TX, TY, NT, MB, SD>;
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -893,9 +929,15 @@ cudaError_t launch_stage32_t(const StageArgs& a, int grid, cudaStream_t s) {
 }
 
 template <int RIEM, int TX, int TY, int NT, int MB>
+cudaError_t launch_stage32_t(const StageArgs& a, int grid, cudaStream_t s) {
+    return a.sd ? launch_stage32_sd<RIEM, TX, TY, NT, MB, true>(a, grid, s)
+                : launch_stage32_sd<RIEM, TX, TY, NT, MB, false>(a, grid, s);
+}
+
+template <int RIEM, int TX, int TY, int NT, int MB>
 int stage32_occupancy_t() {
     constexpr size_t smem = Tile32<TX, TY>::bytes;
-    auto k = stage32_kernel<RIEM, TX, TY, NT, MB>;
+    auto k = stage32_kernel<RIEM, TX, TY, NT, MB, false>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, NT, smem);

@@ -1,0 +1,48 @@
+// MUSCL-SD instantiations of the FP64 stage kernel (q2d_stage64.cuh): the shock sensor of
+// Lib_Shock_Detector.f90:14-38 scales the face slopes. FP64 form only; the FP32-flux form of
+// MUSCL-SD runs on the FP32-flux kernel.
+#include "q2d_stage64.cuh"
+
+namespace q2d {
+
+cudaError_t launch_stage_sd(const StageArgs& a, int prec, int riem, int tile, int grid, cudaStream_t s) {
+    if (prec != 0) return cudaErrorInvalidValue;
+    cudaError_t e = cudaErrorInvalidValue;
+#define Q2D_CALL(TX, TY, NT)                                                  \
+    switch (riem) {                                                           \
+        case 1: e = launch_stage_t<0, 1, TX, TY, NT, true>(a, grid, s); break; \
+        case 2: e = launch_stage_t<0, 2, TX, TY, NT, true>(a, grid, s); break; \
+        case 3: e = launch_stage_t<0, 3, TX, TY, NT, true>(a, grid, s); break; \
+        case 4: e = launch_stage_t<0, 4, TX, TY, NT, true>(a, grid, s); break; \
+        default: e = launch_stage_t<0, 0, TX, TY, NT, true>(a, grid, s); break; \
+    }
+    switch (tile) {
+        case 1: Q2D_CALL(32, 8, 256); break;
+        case 2: Q2D_CALL(64, 4, 256); break;
+        default: Q2D_CALL(32, 10, 256); break;
+    }
+#undef Q2D_CALL
+    return e;
+}
+
+int stage_occupancy_sd(int prec, int riem, int tile) {
+    if (prec != 0) return 0;
+    int n = 0;
+#define Q2D_CALL(TX, TY, NT)                                        \
+    switch (riem) {                                                 \
+        case 1: n = occupancy_t<0, 1, TX, TY, NT, true>(); break;   \
+        case 2: n = occupancy_t<0, 2, TX, TY, NT, true>(); break;   \
+        case 3: n = occupancy_t<0, 3, TX, TY, NT, true>(); break;   \
+        case 4: n = occupancy_t<0, 4, TX, TY, NT, true>(); break;   \
+        default: n = occupancy_t<0, 0, TX, TY, NT, true>(); break;  \
+    }
+    switch (tile) {
+        case 1: Q2D_CALL(32, 8, 256); break;
+        case 2: Q2D_CALL(64, 4, 256); break;
+        default: Q2D_CALL(32, 10, 256); break;
+    }
+#undef Q2D_CALL
+    return n;
+}
+
+}  // namespace q2d

@@ -159,8 +159,7 @@ Setup read_options(const Ini& ini) {
     if (const std::string* v = ini_get(ini, "Numerics", "flux-limiter")) lim = *v;
     if (recon.find("MUSCL") != std::string::npos) {
         if (lim == "none") lim = "vanleer";
-        if (recon.find("SD") != std::string::npos)
-            s.unsupported.push_back("[Q2D-Numerics] space-reconstruction = " + recon);
+        o.shock_detector = recon.find("SD") != std::string::npos ? 1 : 0;   // MUSCL-SD (:25-27)
     }
     static const std::map<std::string, int> kLim = {{"minmod", Q2D_LIM_MINMOD},     {"vanleer", Q2D_LIM_VANLEER},
                                                     {"vanalbada", Q2D_LIM_VANALBADA}, {"mc", Q2D_LIM_MC},
@@ -562,10 +561,10 @@ int run(int argc, char** argv) {
                         "\"precision\": %d, \"rampa_iter\": %d, \"res_diter\": %d, \"sol_diter\": %d, "
                         "\"itermax\": %lld, \"cfl\": %.17g, \"res_threshold\": %.17g, \"time_threshold\": %.17g, "
                         "\"sol_dtime\": %.17g, \"gas_R\": %.17g, \"gas_gamma\": %.17g, \"shell_diter\": %d, "
-                        "\"irs_beta\": %.17g,\n",
+                        "\"irs_beta\": %.17g, \"shock_detector\": %d,\n",
                      o.limiter, o.riemann, o.n_rk, o.time_accurate, o.source, o.precision, o.rampa_iter, o.res_diter,
                      o.sol_diter, o.itermax, o.cfl, o.res_threshold, o.time_threshold, o.sol_dtime, o.gas_R,
-                     o.gas_gamma, S.shell_diter, o.irs_beta);
+                     o.gas_gamma, S.shell_diter, o.irs_beta, o.shock_detector);
         std::fprintf(f, " \"blocks\": [");
         for (size_t b = 0; b < blocks.size(); ++b) {
             double s = 0.0, sa = 0.0;

@@ -54,7 +54,8 @@ def _ini(o: _abi.Options) -> str:
     if o.limiter == 0:
         lines.append("space-reconstruction = first-order")
     else:
-        lines += ["space-reconstruction = MUSCL", f"flux-limiter = {_LIM_NAMES[o.limiter]}"]
+        recon = "MUSCL-SD" if o.shock_detector else "MUSCL"
+        lines += [f"space-reconstruction = {recon}", f"flux-limiter = {_LIM_NAMES[o.limiter]}"]
     lines += [f"riemann-solver = {_RIEMANN_NAMES[o.riemann]}",
               "", "[Q2D-IO]",
               f"res-diter = {o.res_diter}",

@@ -16,6 +16,9 @@ Fixtures written (all small text/npz files):
                       its BC 401 records (INPUT/bc.txt), and Chang's (1996) Mach number along the
                       axis and the wall that its check.py compares against (reference/ref1.dat,
                       ref2.dat)
+  ramp_channel.npz    the reference's ramp-channel case (test/2D/euler/ramp-channel): its grid
+                      nodes and initial state read from INPUT/ic.tec and the Mach number,
+                      temperature and pressure of its BC 405 records (INPUT/bc.txt)
   planar_nozzle_residuals.txt   iteration and density residual of every line the reference
                       binary printed while solving its planar-nozzle case (IRS beta 0.5,
                       stagnation inflow, area-variation source; test/2D/euler/planar-nozzle/
@@ -73,6 +76,18 @@ def main(ref_root: str) -> None:
     np.savez_compressed(HERE / "chang_nozzle.npz", nodes=blk.nodes, prim=blk.prim, T0_p0=np.array(props),
                         axis_mach=np.loadtxt(cdir / "reference" / "ref1.dat"),
                         wall_mach=np.loadtxt(cdir / "reference" / "ref2.dat"))
+    rdir = ref / "test/2D/euler/ramp-channel"
+    blk = refio.read_field(rdir / "INPUT" / "ic.tec")[0]
+    props = None
+    lines = (rdir / "INPUT" / "bc.txt").read_text().splitlines()
+    for k, line in enumerate(lines):
+        t = line.split()
+        if len(t) == 5 and t[4] == "405":
+            vals = lines[k + 1].replace(",", " ").split()
+            cur = (float(vals[0]), float(vals[1]), float(vals[2]))
+            assert props is None or props == cur
+            props = cur
+    np.savez_compressed(HERE / "ramp_channel.npz", nodes=blk.nodes, prim=blk.prim, mach_T_p=np.array(props))
     rows = []
     for line in (ref / "test/2D/euler/planar-nozzle/solve.log").read_text().splitlines():
         if "| Iter =" in line and "Density residual" in line:

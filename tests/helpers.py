@@ -8,13 +8,15 @@ from q2d_b200 import make_options
 from q2d_b200.solver import Q2DSolver
 
 
-def run_pair(cases, steps: int, chunks: int = 1, **opt_overrides):
-    """Advances the cases `steps` steps on both implementations (in `chunks` calls) and returns
-    (gpu_states, oracle_states, gpu_infos, oracle_infos); states are lists over cases of lists
-    over blocks of (nj, ni, 4) arrays."""
+def run_pair(cases, steps: int, chunks: int = 1, schedule=None, **opt_overrides):
+    """Advances the cases `steps` steps on both implementations (in `chunks` calls; the CUDA
+    library on `schedule` when given) and returns (gpu_states, oracle_states, gpu_infos,
+    oracle_infos); states are lists over cases of lists over blocks of (nj, ni, 4) arrays."""
     from oracle import oracle
     opts = make_options(cases[0], **opt_overrides)
     g = Q2DSolver(opts, cases)
+    if schedule is not None:
+        g.set_schedule(schedule)
     o = oracle.solver(opts, cases)
     try:
         per = max(1, steps // chunks)
@@ -90,3 +92,149 @@ def chang_nozzle_gates(cs, prim):
         out += [float(eps.mean()), float(eps.max())]
     assert out[0] < 5e-2 and out[2] < 5e-2 and out[1] < 1e-1 and out[3] < 1e-1, out
     return out
+
+
+def ramp_channel_case():
+    """The reference's ramp-channel case (test/2D/euler/ramp-channel: input.ini, INPUT/) from the
+    committed fixture: Mach 3 flow over a 30-degree ramp in a channel, 95 x 100 cells, supersonic
+    inflow (BC 405: M 3, T 1, p 1), extrapolation outflow (400), symmetry walls (300), MUSCL-SD
+    with minmod + HLLE, SSP-RK3, CFL 0.9 reached over 100 iterations, IRS beta 0.5, local time
+    steps, 10000 iterations; the air of its phase.txt (W = 28.970418) with gamma 1.4."""
+    from pathlib import Path
+    from q2d_b200.cases import BlockSpec, CaseSpec, edge_records, supersonic_props
+    f = np.load(Path(__file__).resolve().parent / "golden" / "ramp_channel.npz")
+    nodes, prim = f["nodes"], f["prim"]
+    nj, ni = prim.shape[:2]
+    mach, T, p = (float(v) for v in f["mach_T_p"])
+    blk = BlockSpec(ni, nj, nodes, prim)
+    bcs = edge_records(1, ni, nj, {1: (405, supersonic_props(mach, T, p)), 2: (400, {}), 3: (300, {}),
+                                   4: (300, {})})
+    opts = dict(limiter="minmod", riemann="HLLE", n_rk=3, cfl=0.9, rampa_iter=100, time_accurate=0,
+                irs_beta=0.5, shock_detector=1, itermax=10000, gas_R=8314.46 / 28.970418, gas_gamma=1.4)
+    return CaseSpec("ramp_channel", [blk], bcs, opts, {"mach": mach})
+
+
+def oblique_shock(M1: float, delta: float, g: float):
+    """Weak oblique-shock solution for a wedge of angle delta (radians): the theta-beta-Mach
+    relation tan(delta) = 2 cot(b) (M1^2 sin^2 b - 1) / (M1^2 (g + cos 2b) + 2) solved for the
+    smallest b above the Mach angle, then the normal-shock relations on M1 sin(b). Returns
+    (M2, b, p2/p1, T2/T1, rho2/rho1)."""
+    def tan_delta(b):
+        return 2.0 / np.tan(b) * (M1 ** 2 * np.sin(b) ** 2 - 1.0) / (M1 ** 2 * (g + np.cos(2.0 * b)) + 2.0)
+    mu = np.arcsin(1.0 / M1)
+    bs = np.linspace(mu, 0.5 * np.pi, 20001)
+    k = int(np.argmax(tan_delta(bs) >= np.tan(delta)))
+    assert k > 0, "detached shock"
+    lo, hi = bs[k - 1], bs[k]
+    for _ in range(100):
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if tan_delta(mid) < np.tan(delta) else (lo, mid)
+    b = 0.5 * (lo + hi)
+    mn1 = M1 * np.sin(b)
+    p21 = 1.0 + 2.0 * g / (g + 1.0) * (mn1 ** 2 - 1.0)
+    r21 = (g + 1.0) * mn1 ** 2 / ((g - 1.0) * mn1 ** 2 + 2.0)
+    mn2 = np.sqrt((mn1 ** 2 + 2.0 / (g - 1.0)) / (2.0 * g / (g - 1.0) * mn1 ** 2 - 1.0))
+    return mn2 / np.sin(b - delta), b, p21, p21 / r21, r21
+
+
+def ramp_channel_gates(cs, prim, beta=None):
+    """The ramp-channel acceptance gates (test/2D/euler/ramp-channel/check.py), with the grid
+    indices of its probes: (1) post / pre-shock ratios against the weak oblique-shock theory for
+    the ramp angle measured from wall nodes 20..50 (pre-shock probe cells i 5:15, j 70:90; post-
+    shock plateau cells i 36:48, j 0:12): p2/p1 within 1 %, T2/T1, rho2/rho1 and M2 within 2 %;
+    (2) with the sensor field beta: it differentiates, >= 1 % of the cells below 0.99, >= 90 % of
+    the cells below 0.5 downstream of the ramp tip, mean > 0.99 over cells i 2:12, j 40:60 and
+    <= 2 % of the cells upstream of the tip below 0.5; (4) positive density and pressure. Returns
+    the four signed relative errors of (1)."""
+    assert np.all(np.isfinite(prim)) and np.all(prim[..., 0] > 0) and np.all(prim[..., 3] > 0)
+    g, R = cs.options["gas_gamma"], cs.options["gas_R"]
+    nodes = cs.blocks[0].nodes                       # (nj + 1, ni + 1, 2)
+    delta = np.arctan2(nodes[0, 50, 1] - nodes[0, 20, 1], nodes[0, 50, 0] - nodes[0, 20, 0])
+    m2_th, _, p21_th, t21_th, r21_th = oblique_shock(cs.meta["mach"], delta, g)
+    pre, post = prim[70:90, 5:15], prim[0:12, 36:48]
+    rho1, p1 = pre[..., 0].mean(), pre[..., 3].mean()
+    T1 = (pre[..., 3] / (pre[..., 0] * R)).mean()
+    rho2, p2 = post[..., 0].mean(), post[..., 3].mean()
+    T2 = (post[..., 3] / (post[..., 0] * R)).mean()
+    u2, v2 = post[..., 1].mean(), post[..., 2].mean()
+    m2 = np.hypot(u2, v2) / np.sqrt(g * R * T2)
+    errs = [p2 / p1 / p21_th - 1.0, T2 / T1 / t21_th - 1.0, rho2 / rho1 / r21_th - 1.0, m2 / m2_th - 1.0]
+    assert abs(errs[0]) < 0.01 and max(map(abs, errs[1:])) < 0.02, errs
+    if beta is not None:
+        assert np.all(np.isfinite(beta)) and beta.max() > beta.min()
+        assert (beta < 0.99).sum() >= beta.size // 100
+        xc = 0.25 * (nodes[:-1, :-1, 0] + nodes[:-1, 1:, 0] + nodes[1:, :-1, 0] + nodes[1:, 1:, 0])
+        x_tip = nodes[0, 20, 0]
+        shock = beta < 0.5
+        assert shock.any() and (xc[shock] > x_tip).mean() >= 0.90
+        assert beta[40:60, 2:12].mean() > 0.99
+        up = xc < x_tip
+        assert (shock & up).sum() / max(up.sum(), 1) <= 0.02
+    return errs
+
+
+def sensor_field(cs, prims) -> list:
+    """The shock sensor beta (SD_Tramel) of every block of a case for the given interior states
+    ([block] -> (nj, ni, 4)), from the oracle's ghost fill: the field the reference writes as
+    'beta' to its diagnostic output. Returns [block] -> (nj, ni)."""
+    import ctypes as C
+    import dataclasses
+    from oracle import oracle
+    blocks = [dataclasses.replace(b, prim=np.ascontiguousarray(p)) for b, p in zip(cs.blocks, prims)]
+    cs2 = dataclasses.replace(cs, blocks=blocks)
+    o = oracle.solver(make_options(cs2), [cs2])
+    try:
+        out = []
+        for k, b in enumerate(blocks):
+            beta = np.empty((b.nj, b.ni))
+            st = o.lib.q2d_oracle_shock_sensor(o.ctx, o.block_ids[0][k], beta.ctypes.data_as(C.POINTER(C.c_double)))
+            assert st == 0, st
+            out.append(beta)
+        return out
+    finally:
+        o.close()
+
+
+def split_case(cs, icuts=(), jcuts=()):
+    """A single-block case cut into a grid of blocks stitched by block-interface records (BC 101,
+    identity orientation) at the interior node lines icuts (i) and jcuts (j); the original edge
+    records go to the blocks that own their cells."""
+    import dataclasses
+    from q2d_b200.cases import BlockSpec
+    (b0,) = cs.blocks
+    ib = [0, *icuts, b0.ni]
+    jb = [0, *jcuts, b0.nj]
+    nI, nJ = len(ib) - 1, len(jb) - 1
+    bid = lambda I, J: J * nI + I + 1   # noqa: E731
+    blocks, bcs = [], []
+    for J in range(nJ):
+        for I in range(nI):
+            i0, i1, j0, j1 = ib[I], ib[I + 1], jb[J], jb[J + 1]
+            blocks.append(BlockSpec(i1 - i0, j1 - j0, b0.nodes[j0:j1 + 1, i0:i1 + 1].copy(),
+                                    b0.prim[j0:j1, i0:i1].copy()))
+    for r in cs.bcs:   # edge records of the original block, in face order
+        i, j = r["i"] - 1, r["j"] - 1
+        I = max(k for k in range(nI) if ib[k] <= i)
+        J = max(k for k in range(nJ) if jb[k] <= j)
+        rr = dict(r, b=bid(I, J), i=i - ib[I] + 1, j=j - jb[J] + 1)
+        bcs.append(rr)
+    conn = dict(d11=1, d12=0, d21=0, d22=1)
+    for J in range(nJ):
+        for I in range(nI):
+            ni, nj = ib[I + 1] - ib[I], jb[J + 1] - jb[J]
+            if I > 0:
+                nl = ib[I] - ib[I - 1]
+                bcs += [dict(b=bid(I, J), i=1, j=k, f=1, type=101, bs=bid(I - 1, J), is_=nl, js=k, fs=2, **conn)
+                        for k in range(1, nj + 1)]
+            if I < nI - 1:
+                bcs += [dict(b=bid(I, J), i=ni, j=k, f=2, type=101, bs=bid(I + 1, J), is_=1, js=k, fs=1, **conn)
+                        for k in range(1, nj + 1)]
+            if J > 0:
+                nl = jb[J] - jb[J - 1]
+                bcs += [dict(b=bid(I, J), i=k, j=1, f=3, type=101, bs=bid(I, J - 1), is_=k, js=nl, fs=4, **conn)
+                        for k in range(1, ni + 1)]
+            if J < nJ - 1:
+                bcs += [dict(b=bid(I, J), i=k, j=nj, f=4, type=101, bs=bid(I, J + 1), is_=k, js=1, fs=3, **conn)
+                        for k in range(1, ni + 1)]
+    bcs.sort(key=lambda r: (r["b"], r["f"], r["j"] if r["f"] <= 2 else r["i"]))
+    return dataclasses.replace(cs, name=cs.name + "_split", blocks=blocks, bcs=bcs)

@@ -1,0 +1,124 @@
+"""MUSCL-SD (space-reconstruction = MUSCL-SD): the face slopes scaled by the Tramel pressure
+sensor of the face's left / lower cell (Mod_Fluxes.f90:132-204, Lib_Shock_Detector.f90:14-38),
+of the boundary cell on a block-interface face (Lib_BC_Fluxes_Connection.f90).
+
+* FP64 form against the CPU oracle: <= 1e-12 relative L-infinity after one step, <= 1e-10 after
+  several, on every FP64 tile (ragged tiles included: the reference's ramp-channel grid is
+  95 x 100 cells), on a developed flow whose shocks cross the tile edges, and on the same flow
+  cut into 2 x 2 blocks whose interfaces the shocks cross (the sensor of halo cells across a tile
+  or block edge, the corner ghosts), with each Riemann solver and limiter family.
+* FP32-flux form against the FP64 form: <= 1e-6 relative L1 on every FP32-flux tile.
+* The reference's ramp-channel case run to its 10000 iterations on the GPU passes its check.py
+  gates (oblique-shock theory, sensor localisation, residual below 1e-3) with the errors the
+  reference binary records.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from q2d_b200 import make_options
+from q2d_b200.solver import Q2DSolver
+from tests.conftest import rel_l1, rel_linf
+from tests.helpers import (ramp_channel_case, ramp_channel_gates, run_pair, sensor_field,
+                           split_case)
+
+pytestmark = pytest.mark.gpu
+
+
+def check(gs, os_, tol, what):
+    for c, (gb, ob) in enumerate(zip(gs, os_)):
+        for b, (g, o) in enumerate(zip(gb, ob)):
+            assert np.all(np.isfinite(g)), f"{what}: non-finite state case {c} block {b}"
+            err = rel_linf(g, o)
+            assert err.max() <= tol, f"{what}: case {c} block {b} rel Linf {err} > {tol}"
+
+
+@pytest.fixture(scope="module")
+def developed():
+    """The ramp-channel flow after 150 oracle iterations (the oblique shock and its reflection
+    formed), as a single-block case and cut into 2 x 2 blocks at i = 40, j = 50."""
+    from oracle import oracle
+    cs = ramp_channel_case()
+    o = oracle.solver(make_options(cs), [cs])
+    try:
+        o.step(150)
+        prim = o.prim()
+    finally:
+        o.close()
+    one = dataclasses.replace(cs, blocks=[dataclasses.replace(cs.blocks[0], prim=prim)])
+    beta = sensor_field(one, [prim])[0]
+    assert (beta[:, 36:44] < 0.5).any() and (beta[46:54, :] < 0.5).any()   # shocks at the cuts
+    return one, split_case(one, icuts=(40,), jcuts=(50,))
+
+
+@pytest.mark.parametrize("schedule", [0, 1, 2])
+def test_sd_ramp_channel_start_vs_oracle(schedule):
+    cs = ramp_channel_case()
+    gs, os_, _, _ = run_pair([cs], 1, schedule=schedule)
+    check(gs, os_, 1e-12, f"ramp-channel sd schedule {schedule} 1 step")
+
+
+@pytest.mark.parametrize("schedule", [0, 1, 2])
+def test_sd_developed_vs_oracle(developed, schedule):
+    for cs in developed:
+        gs, os_, _, _ = run_pair([cs], 1, schedule=schedule)
+        check(gs, os_, 1e-12, f"{cs.name} sd schedule {schedule} 1 step")
+        gs, os_, gi, oi = run_pair([cs], 8, chunks=2, schedule=schedule)
+        check(gs, os_, 1e-10, f"{cs.name} sd schedule {schedule} 8 steps")
+        assert gi[0]["residual"][0] == pytest.approx(oi[0]["residual"][0], rel=1e-9)
+
+
+@pytest.mark.parametrize("riemann,limiter", [("HLLC", "mc"), ("LLF", "vanleer"), ("SLAU", "vanalbada"),
+                                             ("SLAU2", "superbee"), ("HLLE", "LIMO3")])
+def test_sd_solvers_limiters_vs_oracle(developed, riemann, limiter):
+    one, split = developed
+    gs, os_, _, _ = run_pair([split], 4, chunks=2, riemann=riemann, limiter=limiter, irs_beta=0.0, cfl=0.5)
+    check(gs, os_, 1e-10, f"split sd {riemann} {limiter}")
+    gs, os_, _, _ = run_pair([one], 1, riemann=riemann, limiter=limiter, irs_beta=0.0, n_rk=2, cfl=0.5)
+    check(gs, os_, 1e-12, f"one block sd {riemann} {limiter} rk2")
+
+
+@pytest.mark.parametrize("schedule", [5, 6, 7, 8, 9])
+def test_sd_fp32flux_vs_fp64(developed, schedule):
+    for cs in developed:
+        out = []
+        for prec, sch in ((0, 0), (1, schedule)):
+            s = Q2DSolver(make_options(cs, precision=prec), [cs])
+            try:
+                s.set_schedule(sch)
+                info = s.step(10)[0]
+                assert info["err"] == 0, info
+                out.append(s.prims()[0])
+            finally:
+                s.close()
+        for b, (g32, g64) in enumerate(zip(*out)):
+            err = rel_l1(g32, g64)
+            assert err.max() <= 1e-6, f"{cs.name} block {b} schedule {schedule}: rel L1 {err}"
+
+
+def test_sd_changes_the_trajectory(developed):
+    one, _ = developed
+    a, _, _, _ = run_pair([one], 3)
+    b, _, _, _ = run_pair([one], 3, shock_detector=0)
+    assert rel_linf(a[0][0], b[0][0]).max() > 1e-6
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_ramp_channel_reference_gates(precision):
+    """The reference's ramp-channel case on the GPU, its 10000 iterations: density residual below
+    1e-3, the oblique-shock and sensor gates of its check.py, and the post / pre-shock errors the
+    reference binary records (p2/p1 -0.002 %, T2/T1 +0.95 %, rho2/rho1 -0.94 %, M2 -0.94 %) to
+    the digits given."""
+    cs = ramp_channel_case()
+    s = Q2DSolver(make_options(cs, precision=precision), [cs])
+    try:
+        info = s.step(10000)[0]
+        prim = s.prims()[0][0]
+    finally:
+        s.close()
+    assert info["err"] == 0 and info["iter"] == 10000 and info["residual"][0] < 1e-3, info
+    beta = sensor_field(cs, [prim])[0]
+    errs = 100.0 * np.array(ramp_channel_gates(cs, prim, beta))
+    assert abs(errs[0] - (-0.002)) < 0.005, errs
+    assert np.all(np.abs(errs[1:] - np.array([0.95, -0.94, -0.94])) < 0.01), errs

@@ -17,7 +17,8 @@ from q2d_b200.solver import Q2DSolver
 
 GOLD = Path(__file__).resolve().parent / "golden"
 OPT_FIELDS = ["limiter", "riemann", "n_rk", "time_accurate", "source", "rampa_iter", "res_diter",
-              "sol_diter", "itermax", "cfl", "res_threshold", "time_threshold", "sol_dtime", "gas_R", "irs_beta"]
+              "sol_diter", "itermax", "cfl", "res_threshold", "time_threshold", "sol_dtime", "gas_R", "irs_beta",
+              "shock_detector"]
 
 
 def host(*args, check=True):
@@ -87,17 +88,21 @@ def test_check_mode_limiter_keywords(tmp_path):
         extra = f"space-reconstruction = {recon}\n" + (f"flux-limiter = {lim}\n" if lim else "")
         (tmp_path / "input.ini").write_text(base.replace("[Q2D-Numerics]\n", "[Q2D-Numerics]\n" + extra))
         assert json.loads(host(tmp_path, "--check").stdout)["limiter"] == want, (recon, lim)
+    # MUSCL-SD turns the shock sensor on (Mod_Space.f90:25-27); without MUSCL it stays off
+    for recon, want in [("MUSCL-SD", 1), ("MUSCL", 0), ("first-order", 0), ("SD", 0)]:
+        extra = f"space-reconstruction = {recon}\nflux-limiter = minmod\n"
+        (tmp_path / "input.ini").write_text(base.replace("[Q2D-Numerics]\n", "[Q2D-Numerics]\n" + extra))
+        d = json.loads(host(tmp_path, "--check").stdout)
+        assert d["shock_detector"] == want and not d["unsupported"], (recon, d["unsupported"])
 
 
 def test_inputs_outside_the_path_fail_loudly(tmp_path):
     cs = cases.ramp(20, 8)
     refio.write_case(cs, tmp_path)
     ini = (tmp_path / "input.ini").read_text()
-    (tmp_path / "input.ini").write_text(ini.replace("space-reconstruction = MUSCL", "space-reconstruction = MUSCL-SD")
-                                        .replace("riemann-solver = HLLC", "riemann-solver = AUSM+"))
+    (tmp_path / "input.ini").write_text(ini.replace("riemann-solver = HLLC", "riemann-solver = AUSM+"))
     d = json.loads(host(tmp_path, "--check").stdout)
-    assert "[Q2D-Numerics] space-reconstruction = MUSCL-SD" in d["unsupported"]
-    assert "[Q2D-Numerics] riemann-solver = AUSM+" in d["unsupported"]
+    assert d["unsupported"] == ["[Q2D-Numerics] riemann-solver = AUSM+"]
     r = host(tmp_path, check=False)   # refused before any device call
     assert r.returncode == 2 and "not on the built path" in r.stderr
     (tmp_path / "input.ini").write_text(ini)

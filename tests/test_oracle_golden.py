@@ -248,3 +248,45 @@ def test_chang_nozzle_axisymmetric_matches_reference_data():
         chang_nozzle_gates(cs, s.prim())
     finally:
         s.close()
+
+
+def test_sd_tramel_known_answers():
+    """SD_Tramel (Lib_Shock_Detector.f90:14-38): 1 on a uniform or linear pressure stencil, 0 at
+    and above the switch max(kp1, kp2) = 1/20, 1 - tanh(10 (sw/20)^3) below it, symmetric in the
+    two directions."""
+    lib = oracle.load()
+    sd = lib.q2d_oracle_sd_tramel
+    assert sd(1.0, 1.0, 1.0, 1.0, 1.0) == 1.0
+    assert sd(2.0, 1.0, 3.0, 2.0, 2.0) == 1.0          # linear in i: no second difference
+    assert sd(1.0, 1.0, 2.0, 1.0, 1.0) == 0.0          # kp1 = 1/5
+    assert sd(1.0, 1.0, 1.0, 1.0, 2.0) == 0.0          # kp2 = 1/5
+    for p2 in (1.01, 1.1, 1.2):
+        sw = (p2 - 1.0) / (p2 + 3.0)
+        want = 1.0 - np.tanh(10.0 * (sw / 20.0) ** 3) if sw < 0.05 else 0.0
+        assert sd(1.0, 1.0, p2, 1.0, 1.0) == pytest.approx(want, rel=0, abs=1e-16)
+        assert sd(1.0, 1.0, 1.0, 1.0, p2) == sd(1.0, 1.0, p2, 1.0, 1.0)
+    # the switch: sw = 1/20 exactly (p2 = 23/19 gives (p2 - 1) / (p2 + 3) = 4/80) is a shock
+    assert sd(1.0, 1.0, 1.0 + 4.0 / 19.0 - 1e-12, 1.0, 1.0) > 0.999999
+    assert sd(1.0, 1.0, 1.0 + 4.0 / 19.0 + 1e-12, 1.0, 1.0) == 0.0
+
+
+def test_ramp_channel_matches_reference_calibration():
+    """The reference's ramp-channel case (Mach 3 over a 30-degree ramp: MUSCL-SD with minmod,
+    HLLE, IRS beta 0.5, CFL 0.9 after a 100-iteration ramp) through the oracle: after 1500 of its
+    10000 iterations the density residual is below the case's 1e-3 gate, the oblique-shock gates
+    of its check.py pass, the sensor field passes its localisation gates, and the post / pre-shock
+    errors against the theory equal those check.py records for the reference binary (p2/p1
+    -0.002 %, T2/T1 +0.95 %, rho2/rho1 -0.94 %, M2 -0.94 %) to the digits it gives."""
+    from tests.helpers import ramp_channel_case, ramp_channel_gates, sensor_field
+    cs = ramp_channel_case()
+    s = oracle.solver(make_options(cs), [cs])
+    try:
+        info = s.step(1500)[0]
+        prim = s.prim()
+    finally:
+        s.close()
+    assert info["err"] == 0 and info["iter"] == 1500 and info["residual"][0] < 1e-3, info
+    beta = sensor_field(cs, [prim])[0]
+    errs = 100.0 * np.array(ramp_channel_gates(cs, prim, beta))
+    assert abs(errs[0] - (-0.002)) < 0.005, errs
+    assert np.all(np.abs(errs[1:] - np.array([0.95, -0.94, -0.94])) < 0.01), errs
