@@ -10,7 +10,7 @@ of the boundary cell on a block-interface face (Lib_BC_Fluxes_Connection.f90).
 * FP32-flux form against the FP64 form: <= 1e-6 relative L1 on every FP32-flux tile.
 * The reference's ramp-channel case run to its 10000 iterations on the GPU passes its check.py
   gates (oblique-shock theory, sensor localisation, residual below 1e-3) with the errors the
-  reference binary records.
+  reference binary records, through the API and through q2d_host from the reference's formats.
 """
 import dataclasses
 
@@ -122,3 +122,19 @@ def test_ramp_channel_reference_gates(precision):
     errs = 100.0 * np.array(ramp_channel_gates(cs, prim, beta))
     assert abs(errs[0] - (-0.002)) < 0.005, errs
     assert np.all(np.abs(errs[1:] - np.array([0.95, -0.94, -0.94])) < 0.01), errs
+
+
+def test_ramp_channel_reference_case_through_host(tmp_path):
+    """The ramp-channel case written in the reference's formats (space-reconstruction = MUSCL-SD)
+    and run by q2d_host to its iteration limit: the residual history it writes stays finite and
+    ends below 1e-3, and the field it writes passes the case's gates."""
+    from q2d_b200 import refio
+    from tests.test_host_harness import host
+    cs = ramp_channel_case()
+    refio.write_case(cs, tmp_path)
+    assert "space-reconstruction = MUSCL-SD" in (tmp_path / "input.ini").read_text()
+    host(tmp_path, "--gamma", repr(cs.options["gas_gamma"]), "--steps-per-call", 1000, "--quiet")
+    res = np.loadtxt(tmp_path / "OUTPUT" / "residuals.dat")
+    assert np.all(np.isfinite(res[:, 3])) and res[-1, 0] == 10000 and res[-1, 3] < 1e-3
+    prim = refio.read_field(tmp_path / "OUTPUT" / "field.tec")[0].prim
+    ramp_channel_gates(cs, prim, sensor_field(cs, [prim])[0])
