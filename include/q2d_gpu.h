@@ -65,6 +65,10 @@ extern "C" {
 #define Q2D_RIEMANN_LLF    2   /* 'LLF' / 'Rusanov'   Lib_Riemann_LF.f90:11-40 */
 #define Q2D_RIEMANN_SLAU   3   /* 'SLAU'              Lib_Riemann_SLAU.f90:10-91 */
 #define Q2D_RIEMANN_SLAU2  4   /* 'SLAU2'             Lib_Riemann_SLAU.f90:10-53, 94-124 */
+#define Q2D_RIEMANN_HLLCP  5   /* 'HLLC+'  HLLC / HLLE blend by the shock sensor,
+                                            Lib_Riemann_HLL.f90:572-605 (computes the sensor) */
+#define Q2D_RIEMANN_HLLEPP 6   /* 'HLLE++' Roe / HLLE eigenvalue blend by the shock sensor,
+                                            Lib_Riemann_HLL.f90:437-533 (computes the sensor) */
 
 #define Q2D_SRC_NONE       0
 #define Q2D_SRC_AXI        1   /* [Q2D-Sources] active = axisymmetric   Lib_Source_Axisymmetry.f90:40-78 */

@@ -39,6 +39,10 @@ def load():
         lib.q2d_oracle_riemann.argtypes = [C.c_int, C.POINTER(_abi.Options),
                                            C.POINTER(C.c_double), C.POINTER(C.c_double),
                                            C.c_double, C.c_double, C.POINTER(C.c_double)]
+        lib.q2d_oracle_riemann_sd.restype = None
+        lib.q2d_oracle_riemann_sd.argtypes = [C.c_int, C.POINTER(_abi.Options),
+                                              C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                              C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
         lib.q2d_oracle_sd_tramel.restype = C.c_double
         lib.q2d_oracle_sd_tramel.argtypes = [C.c_double] * 5
         lib.q2d_oracle_shock_sensor.restype = C.c_int

@@ -320,9 +320,85 @@ inline Flux4 riemann_slau(const Gas& g, bool slau2, double dltot, double ul, dou
     return F;
 }
 
+// the solvers that run the shock sensor (obj_riemann%SD, Mod_Riemann.f90:70-80)
+inline bool riemann_sd(int kind) { return kind == Q2D_RIEMANN_HLLCP || kind == Q2D_RIEMANN_HLLEPP; }
+
+// hartenHyman (Lib_Riemann_HLL.f90:320-331): entropy fix of an acoustic eigenvalue
+inline double harten_hyman(double v, double e) {
+    const double al = std::fabs(v);
+    return al <= e ? (v * v + e * e) / (2.0 * e) : al;
+}
+
+// riemann_HLLEpp (Lib_Riemann_HLL.f90:437-533): centred flux minus the wave sum of a Roe
+// linearisation whose eigenvalues blend Roe's (Harten-Hyman fix on the acoustic waves, |un| on
+// the contact and the shear) and HLLE's by the shock sensor beta.
+inline Flux4 riemann_hllepp(const Gas& g, double dl, double ul, double vl, double pl, double al,
+                            double dltot, double dr, double ur, double vr, double pr, double ar,
+                            double drtot, double beta, double nx, double ny) {
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    double h0l, h0r, rho_roe, u_roe, v_roe, a_roe, h0_roe;
+    roe_averages(g, dl, dr, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, rho_roe, u_roe,
+                 v_roe, a_roe, h0_roe);
+    const double un_roe = u_roe * nx + v_roe * ny;
+    const double Sm = fmin_(fmin_(0.0, unl - al), un_roe - a_roe);
+    const double Sp = fmax_(fmax_(0.0, unr + ar), un_roe + a_roe);
+    const double inv_denom = 1.0 / (Sp - Sm);
+    const double lam1_hlle = std::fabs((Sp + Sm) * un_roe * inv_denom - 2.0 * Sp * Sm * inv_denom);
+    const double lam2_hlle = std::fabs((Sp + Sm) * (un_roe - a_roe) * inv_denom - 2.0 * Sp * Sm * inv_denom);
+    const double lam3_hlle = std::fabs((Sp + Sm) * (un_roe + a_roe) * inv_denom - 2.0 * Sp * Sm * inv_denom);
+    const double eps = 0.3 * (std::fabs(un_roe) + a_roe);
+    const double lam1_roe = std::fabs(un_roe);
+    const double lam2_roe = harten_hyman(un_roe - a_roe, eps);
+    const double lam3_roe = harten_hyman(un_roe + a_roe, eps);
+    const double lam1 = beta * lam1_roe + (1.0 - beta) * lam1_hlle;
+    const double lam2 = beta * lam2_roe + (1.0 - beta) * lam2_hlle;
+    const double lam3 = beta * lam3_roe + (1.0 - beta) * lam3_hlle;
+    const Flux4 FL = physical_flux(g, pl, dl, ul, vl, nx, ny);   // fluxes_helper (:334-352)
+    const Flux4 FR = physical_flux(g, pr, dr, ur, vr, nx, ny);
+    Flux4 F;
+    F.r = 0.5 * (FL.r + FR.r);
+    F.u = 0.5 * (FL.u + FR.u);
+    F.v = 0.5 * (FL.v + FR.v);
+    F.e = 0.5 * (FL.e + FR.e);
+    const double drho = drtot - dltot, dp = pr - pl, du = ur - ul, dv = vr - vl, dun = unr - unl;
+    const double tx = -ny, ty = nx;
+    const double alpha_m = (dp - rho_roe * a_roe * dun) / (2.0 * a_roe * a_roe);
+    const double alpha_c = drho - dp / (a_roe * a_roe);
+    const double alpha_s = rho_roe * (du * tx + dv * ty);
+    const double alpha_p = (dp + rho_roe * a_roe * dun) / (2.0 * a_roe * a_roe);
+    F.r = F.r - 0.5 * (alpha_c * lam1 + alpha_m * lam2 + alpha_p * lam3);
+    F.u = F.u - 0.5 * (alpha_c * lam1 * u_roe + alpha_s * lam1 * tx + alpha_m * lam2 * (u_roe - a_roe * nx) +
+                       alpha_p * lam3 * (u_roe + a_roe * nx));
+    F.v = F.v - 0.5 * (alpha_c * lam1 * v_roe + alpha_s * lam1 * ty + alpha_m * lam2 * (v_roe - a_roe * ny) +
+                       alpha_p * lam3 * (v_roe + a_roe * ny));
+    F.e = F.e - 0.5 * (alpha_c * lam1 * 0.5 * (u_roe * u_roe + v_roe * v_roe) +
+                       alpha_s * lam1 * (u_roe * tx + v_roe * ty) + alpha_m * lam2 * (h0_roe - a_roe * un_roe) +
+                       alpha_p * lam3 * (h0_roe + a_roe * un_roe));
+    return F;
+}
+
+// beta: the shock sensor of the face's cell for the sensor-driven solvers (HLLC+, HLLE++;
+// Convective_Flux passes it, Lib_Convective.f90:62-64), 1 from the wall and inflow boundaries.
 inline Flux4 riemann(int kind, const Gas& g, const double* L, double aL, const double* R,
-                     double aR, double nx, double ny) {
+                     double aR, double nx, double ny, double beta = 1.0) {
     switch (kind) {
+        case Q2D_RIEMANN_HLLCP: {   // riemann_HLLCSD (Lib_Riemann_HLL.f90:572-605)
+            if (beta == 0.0)
+                return riemann_hlle(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], nx, ny);
+            if (beta >= 1.0)
+                return riemann_hllc(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], nx, ny);
+            const Flux4 E = riemann_hlle(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], nx, ny);
+            const Flux4 C = riemann_hllc(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], nx, ny);
+            Flux4 F;
+            F.r = beta * C.r + (1.0 - beta) * E.r;
+            F.u = beta * C.u + (1.0 - beta) * E.u;
+            F.v = beta * C.v + (1.0 - beta) * E.v;
+            F.e = beta * C.e + (1.0 - beta) * E.e;
+            return F;
+        }
+        case Q2D_RIEMANN_HLLEPP:
+            return riemann_hllepp(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], beta, nx, ny);
         case Q2D_RIEMANN_SLAU:
         case Q2D_RIEMANN_SLAU2:
             return riemann_slau(g, kind == Q2D_RIEMANN_SLAU2, L[0], L[1], L[2], L[3], aL, R[0], R[1], R[2],
@@ -690,13 +766,13 @@ inline void reconstruct(int lim, const double* prev, const double* loc, const do
 // Flux from two reconstructed states: Lib_Convective.f90:56-80 (also used by the connection
 // BC, Lib_BC_Fluxes_Connection.f90:97-130, which has the same body).
 inline bool face_flux_from_states(const q2d_oracle* o, const double* P1, const double* P4,
-                                  double nx, double ny, double int_l, double* flux) {
+                                  double nx, double ny, double int_l, double beta, double* flux) {
     if (gas_state_bad(P1[0], P1[3]) || gas_state_bad(P4[0], P4[3])) return false;
     const Gas& g = o->gas;
     const double rotot1 = P1[0], rotot4 = P4[0];
     const double a1 = f_ss(g, P1[3], rotot1);
     const double a4 = f_ss(g, P4[3], rotot4);
-    const Flux4 F = riemann(o->opt.riemann, g, P1, a1, P4, a4, nx, ny);
+    const Flux4 F = riemann(o->opt.riemann, g, P1, a1, P4, a4, nx, ny, beta);
     const double su = std::copysign(0.5, F.r);
     const double sp = 0.5 + su, sm = su - 0.5;
     flux[0] = F.r * int_l * (sp * (P1[0] / rotot1) - sm * (P4[0] / rotot4));
@@ -706,18 +782,20 @@ inline bool face_flux_from_states(const q2d_oracle* o, const double* P1, const d
     return true;
 }
 
-// Convective_Flux (Lib_Convective.f90:15-82): dl[-1..2], Prim[-1..2] along the direction; beta
-// scales both limited slopes (the SD_limiter branch, :40-47; 1 without MUSCL-SD).
+// Convective_Flux (Lib_Convective.f90:15-82): dl[-1..2], Prim[-1..2] along the direction; beta_l
+// scales both limited slopes (the SD_limiter branch, :40-47; 1 without MUSCL-SD), beta_r goes to
+// the Riemann solver (the cell's sensor whenever the sensor runs, :62-64).
 inline bool convective_flux(const q2d_oracle* o, const double* dlm1, const double* const* pr,
-                            double nx, double ny, double int_l, double beta, double* flux) {
+                            double nx, double ny, double int_l, double beta_l, double beta_r,
+                            double* flux) {
     const double l0 = 0.5 * (dlm1[0] + dlm1[1]);
     const double l1 = 0.5 * (dlm1[1] + dlm1[2]);
     const double l2 = 0.5 * (dlm1[2] + dlm1[3]);
     const double lm = 0.5 * dlm1[1];
     const double lp = 0.5 * dlm1[2];
     double P1[4], P4[4];
-    reconstruct(o->opt.limiter, pr[0], pr[1], pr[2], pr[3], l0, l1, l2, lm, lp, beta, P1, P4);
-    return face_flux_from_states(o, P1, P4, nx, ny, int_l, flux);
+    reconstruct(o->opt.limiter, pr[0], pr[1], pr[2], pr[3], l0, l1, l2, lm, lp, beta_l, P1, P4);
+    return face_flux_from_states(o, P1, P4, nx, ny, int_l, beta_r, flux);
 }
 
 // SD_Tramel (Lib_Shock_Detector.f90:14-38): Jameson-type pressure sensor on the cross stencil
@@ -746,7 +824,9 @@ void shock_sensor(Block& B) {
 // Fluxes_blk_omp_do (Mod_Fluxes.f90:97-234), Euler part. Returns false on a bad state.
 bool block_fluxes(const q2d_oracle* o, Block& B, int& eb_i, int& eb_j) {
     const int n1 = B.ni, n2 = B.nj;
-    const bool sd = o->opt.shock_detector != 0;
+    // obj_shock_detector%SD: MUSCL-SD or a sensor-driven Riemann solver (Assign_Setup.f90:49-53)
+    const bool sdl = o->opt.shock_detector != 0;
+    const bool sd = sdl || riemann_sd(o->opt.riemann);
     if (sd) shock_sensor(B);
     bool ok = true;
 #pragma omp parallel for schedule(static)
@@ -764,7 +844,8 @@ bool block_fluxes(const q2d_oracle* o, Block& B, int& eb_i, int& eb_j) {
             const double* pr[4] = {B.pc(i - 1, j), B.pc(i, j), B.pc(i + 1, j), B.pc(i + 2, j)};
             const double* f = B.face1(i, j);
             double fl[4];
-            if (!convective_flux(o, dl4, pr, f[0], f[1], f[2], sd ? B.sd(i, j) : 1.0, fl)) {
+            if (!convective_flux(o, dl4, pr, f[0], f[1], f[2], sdl ? B.sd(i, j) : 1.0, sd ? B.sd(i, j) : 1.0,
+                                 fl)) {
 #pragma omp critical
                 { if (ok) { ok = false; bi = i; bj = j; } }
                 continue;
@@ -782,7 +863,8 @@ bool block_fluxes(const q2d_oracle* o, Block& B, int& eb_i, int& eb_j) {
             const double* pr[4] = {B.pc(i, j - 1), B.pc(i, j), B.pc(i, j + 1), B.pc(i, j + 2)};
             const double* f = B.face2(i, j);
             double fl[4];
-            if (!convective_flux(o, dl4, pr, f[0], f[1], f[2], sd ? B.sd(i, j) : 1.0, fl)) {
+            if (!convective_flux(o, dl4, pr, f[0], f[1], f[2], sdl ? B.sd(i, j) : 1.0, sd ? B.sd(i, j) : 1.0,
+                                 fl)) {
 #pragma omp critical
                 { if (ok) { ok = false; bi = i; bj = j; } }
                 continue;
@@ -1079,12 +1161,14 @@ bool bc_connection(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm) {
     const double Dl4 = B.dlc(I4, J4, dir) * 0.5;
     const double Dist23 = Dl2 + Dl3, Dist12 = Dl1 + Dl2, Dist34 = Dl3 + Dl4;
     double PL[4], PR[4];
-    // SD_limiter: beta of the boundary cell (Lib_BC_Fluxes_Connection.f90, beta_ = blk%beta(Im,Jm))
-    const double beta = o->opt.shock_detector ? B.sd(Im, Jm) : 1.0;
+    // SD_limiter / SD_riemann: beta of the boundary cell (Lib_BC_Fluxes_Connection.f90,
+    // beta_ = blk%beta(Im,Jm)) for the reconstruction / the Riemann solver
+    const double beta_l = o->opt.shock_detector ? B.sd(Im, Jm) : 1.0;
+    const double beta_r = riemann_sd(o->opt.riemann) ? B.sd(Im, Jm) : 1.0;
     reconstruct(o->opt.limiter, B.pc(I1, J1), B.pc(I2, J2), B.pc(I3, J3), B.pc(I4, J4), Dist12,
-                Dist23, Dist34, Dl2, Dl3, beta, PL, PR);
+                Dist23, Dist34, Dl2, Dl3, beta_l, PL, PR);
     double F[4];
-    if (!face_flux_from_states(o, PL, PR, fc[0], fc[1], fc[2], F)) return false;
+    if (!face_flux_from_states(o, PL, PR, fc[0], fc[1], fc[2], beta_r, F)) return false;
     double* r = B.r(Im, Jm);
     for (int v = 0; v < 4; ++v) r[v] = r[v] + F[v] * modfm2;
     return true;
@@ -1611,6 +1695,16 @@ void q2d_oracle_riemann(int kind, const q2d_options* opt, const double* L, const
     g.cp = g.gamma * g.R / g.gm1; g.cv = g.R / g.gm1;
     const double aL = f_ss(g, L[3], L[0]), aR = f_ss(g, R[3], R[0]);
     const Flux4 F = riemann(kind, g, L, aL, R, aR, nx, ny);
+    flux4[0] = F.r; flux4[1] = F.u; flux4[2] = F.v; flux4[3] = F.e;
+}
+
+void q2d_oracle_riemann_sd(int kind, const q2d_options* opt, const double* L, const double* R,
+                           double beta, double nx, double ny, double* flux4) {
+    Gas g;
+    g.R = opt->gas_R; g.gamma = opt->gas_gamma; g.gm1 = g.gamma - 1.0;
+    g.cp = g.gamma * g.R / g.gm1; g.cv = g.R / g.gm1;
+    const double aL = f_ss(g, L[3], L[0]), aR = f_ss(g, R[3], R[0]);
+    const Flux4 F = riemann(kind, g, L, aL, R, aR, nx, ny, beta);
     flux4[0] = F.r; flux4[1] = F.u; flux4[2] = F.v; flux4[3] = F.e;
 }
 

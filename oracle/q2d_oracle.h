@@ -53,6 +53,9 @@ int  q2d_oracle_shock_sensor(q2d_oracle* o, int block_id, double* beta);
 /* Scalar kernels for known-answer tests. */
 double q2d_oracle_limiter(int limiter, double x, double y);
 double q2d_oracle_sd_tramel(double p, double p1, double p2, double p3, double p4);
+/* the Riemann solver with the shock sensor beta the sensor-driven solvers blend by */
+void   q2d_oracle_riemann_sd(int riemann, const q2d_options* opt, const double* primL,
+                             const double* primR, double beta, double nx, double ny, double* flux4);
 void   q2d_oracle_riemann(int riemann, const q2d_options* opt, const double* primL,
                           const double* primR, double nx, double ny, double* flux4);
 

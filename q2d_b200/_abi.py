@@ -24,7 +24,7 @@ OK, ERR_BADARG, ERR_OOM, ERR_CUDA, ERR_NONPHYSICAL, ERR_NAN, ERR_TIMEOUT, ERR_UN
 
 LIM = {"iord": 0, "none": 0, "first-order": 0, "minmod": 1, "vanleer": 2, "vanalbada": 3,
        "mc": 4, "superbee": 5, "LIMO3": 6}
-RIEMANN = {"HLLC": 0, "HLLE": 1, "LLF": 2, "Rusanov": 2, "SLAU": 3, "SLAU2": 4}
+RIEMANN = {"HLLC": 0, "HLLE": 1, "LLF": 2, "Rusanov": 2, "SLAU": 3, "SLAU2": 4, "HLLC+": 5, "HLLE++": 6}
 SRC = {"none": 0, "axisymmetric": 1, "area_variation": 2}
 PREC_FP64, PREC_FP32_FLUX = 0, 1
 TODO_CONTINUE, TODO_IO, TODO_END = 1, 2, 3

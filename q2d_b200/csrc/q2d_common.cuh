@@ -302,8 +302,8 @@ __device__ __noinline__ Q4 bc_face(const Gas g, int lim, int etype, int Fm, cons
 // ------------------------------------------------------------------------------------------
 template <int PREC, int RIEM>
 __device__ __forceinline__ bool face_flux(const Gas& g, const double* PL, const double* PR, double nx,
-                                          double ny, double int_l, double* X) {
-    if (PREC == 0) return flux_from_states64<RIEM>(g, PL, PR, nx, ny, int_l, X);
+                                          double ny, double int_l, double* X, double beta = 1.0) {
+    if (PREC == 0) return flux_from_states64<RIEM>(g, PL, PR, nx, ny, int_l, X, beta);
     const bool bad = gas_state_bad(PL[0], PL[3]) || gas_state_bad(PR[0], PR[3]);
     FluxState L, R;
     phys64(g, PL, nx, ny, L);

@@ -280,7 +280,8 @@ struct F4 { double r, u, v, e; };
 __device__ __forceinline__ void roe_averages(const Gas& g, double dltot, double drtot, double ul,
                                              double vl, double ur, double vr, double pl,
                                              double pr, double& h0l, double& h0r,
-                                             double& u_roe, double& v_roe, double& a_roe) {
+                                             double& u_roe, double& v_roe, double& a_roe,
+                                             double& rho_roe, double& h0_roe) {
     const double inv_dltot = 1.0 / dltot;
     const double inv_drtot = 1.0 / drtot;
     const double Tl = pl * inv_dltot / g.R;
@@ -288,6 +289,7 @@ __device__ __forceinline__ void roe_averages(const Gas& g, double dltot, double 
     const double srL = sqrt(dltot);
     const double srR = sqrt(drtot);
     const double inv_sr = 1.0 / (srL + srR);
+    rho_roe = srL * srR;
     u_roe = (srR * ur + srL * ul) * inv_sr;
     v_roe = (srR * vr + srL * vl) * inv_sr;
     const double R_roe = (srR * g.R + srL * g.R) * inv_sr;
@@ -303,7 +305,7 @@ __device__ __forceinline__ void roe_averages(const Gas& g, double dltot, double 
     const double sum_ei = 0.0 + d_roe * (srR * er + srL * el) * inv_sr;
     h0l = h0l + 0.5 * (ul * ul + vl * vl);
     h0r = h0r + 0.5 * (ur * ur + vr * vr);
-    const double h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+    h0_roe = (srR * h0r + srL * h0l) * inv_sr;
     const double gam_roe = 1.0 + R_roe / cv_roe;
     const double vel2 = u_roe * u_roe + v_roe * v_roe;
     a_roe = sqrt((gam_roe - 1.0) * (h0_roe - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
@@ -317,8 +319,8 @@ __device__ __forceinline__ F4 riemann_hllc(const Gas& g, const double* L, double
     F4 F;
     const double unl = ul * nx + vl * ny;
     const double unr = ur * nx + vr * ny;
-    double h0l, h0r, u_roe, v_roe, a_roe;
-    roe_averages(g, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, u_roe, v_roe, a_roe);
+    double h0l, h0r, u_roe, v_roe, a_roe, rho_roe, h0_roe;
+    roe_averages(g, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, u_roe, v_roe, a_roe, rho_roe, h0_roe);
     const double un_roe = u_roe * nx + v_roe * ny;
     const double e0l = h0l - pl / dltot;
     const double e0r = h0r - pr / drtot;
@@ -377,8 +379,8 @@ __device__ __forceinline__ F4 riemann_hlle(const Gas& g, const double* L, double
     F4 F;
     const double unl = ul * nx + vl * ny;
     const double unr = ur * nx + vr * ny;
-    double h0l, h0r, u_roe, v_roe, a_roe;
-    roe_averages(g, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, u_roe, v_roe, a_roe);
+    double h0l, h0r, u_roe, v_roe, a_roe, rho_roe, h0_roe;
+    roe_averages(g, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, u_roe, v_roe, a_roe, rho_roe, h0_roe);
     const double un_roe = u_roe * nx + v_roe * ny;
     const double S1 = dmin(dmin(0.0, unl - al), un_roe - a_roe);
     const double S4 = dmax(dmax(0.0, unr + ar), un_roe + a_roe);
@@ -471,9 +473,74 @@ __device__ __forceinline__ F4 riemann_slau(const Gas& g, const double* L, double
     return F;
 }
 
+// riemann_HLLEpp (Lib_Riemann_HLL.f90:437-533), FP64: centred flux minus the wave sum of a
+// Roe linearisation whose eigenvalues blend Roe's (Harten-Hyman fix on the acoustic waves,
+// hartenHyman :320-331) and HLLE's by the shock sensor beta.
+__device__ __forceinline__ double harten_hyman(double v, double e) {
+    const double al = fabs(v);
+    return al <= e ? (v * v + e * e) / (2.0 * e) : al;
+}
+__device__ __forceinline__ F4 riemann_hllepp(const Gas& g, const double* L, double al, const double* R,
+                                             double ar, double beta, double nx, double ny) {
+    const double dltot = L[0], ul = L[1], vl = L[2], pl = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], pr = R[3];
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    double h0l, h0r, u_roe, v_roe, a_roe, rho_roe, h0_roe;
+    roe_averages(g, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, u_roe, v_roe, a_roe, rho_roe, h0_roe);
+    const double un_roe = u_roe * nx + v_roe * ny;
+    const double Sm = dmin(dmin(0.0, unl - al), un_roe - a_roe);
+    const double Sp = dmax(dmax(0.0, unr + ar), un_roe + a_roe);
+    const double inv_denom = 1.0 / (Sp - Sm);
+    const double lam1_hlle = fabs((Sp + Sm) * un_roe * inv_denom - 2.0 * Sp * Sm * inv_denom);
+    const double lam2_hlle = fabs((Sp + Sm) * (un_roe - a_roe) * inv_denom - 2.0 * Sp * Sm * inv_denom);
+    const double lam3_hlle = fabs((Sp + Sm) * (un_roe + a_roe) * inv_denom - 2.0 * Sp * Sm * inv_denom);
+    const double eps = 0.3 * (fabs(un_roe) + a_roe);
+    const double lam1 = beta * fabs(un_roe) + (1.0 - beta) * lam1_hlle;
+    const double lam2 = beta * harten_hyman(un_roe - a_roe, eps) + (1.0 - beta) * lam2_hlle;
+    const double lam3 = beta * harten_hyman(un_roe + a_roe, eps) + (1.0 - beta) * lam3_hlle;
+    const F4 FL = phys_flux(g, pl, dltot, ul, vl, nx, ny);   // fluxes_helper (:334-352)
+    const F4 FR = phys_flux(g, pr, drtot, ur, vr, nx, ny);
+    F4 F;
+    F.r = 0.5 * (FL.r + FR.r);
+    F.u = 0.5 * (FL.u + FR.u);
+    F.v = 0.5 * (FL.v + FR.v);
+    F.e = 0.5 * (FL.e + FR.e);
+    const double drho = drtot - dltot, dp = pr - pl, du = ur - ul, dv = vr - vl, dun = unr - unl;
+    const double tx = -ny, ty = nx;
+    const double alpha_m = (dp - rho_roe * a_roe * dun) / (2.0 * a_roe * a_roe);
+    const double alpha_c = drho - dp / (a_roe * a_roe);
+    const double alpha_s = rho_roe * (du * tx + dv * ty);
+    const double alpha_p = (dp + rho_roe * a_roe * dun) / (2.0 * a_roe * a_roe);
+    F.r = F.r - 0.5 * (alpha_c * lam1 + alpha_m * lam2 + alpha_p * lam3);
+    F.u = F.u - 0.5 * (alpha_c * lam1 * u_roe + alpha_s * lam1 * tx + alpha_m * lam2 * (u_roe - a_roe * nx) +
+                       alpha_p * lam3 * (u_roe + a_roe * nx));
+    F.v = F.v - 0.5 * (alpha_c * lam1 * v_roe + alpha_s * lam1 * ty + alpha_m * lam2 * (v_roe - a_roe * ny) +
+                       alpha_p * lam3 * (v_roe + a_roe * ny));
+    F.e = F.e - 0.5 * (alpha_c * lam1 * 0.5 * (u_roe * u_roe + v_roe * v_roe) +
+                       alpha_s * lam1 * (u_roe * tx + v_roe * ty) + alpha_m * lam2 * (h0_roe - a_roe * un_roe) +
+                       alpha_p * lam3 * (h0_roe + a_roe * un_roe));
+    return F;
+}
+
+// beta: the shock sensor of the face's cell for the sensor-driven solvers (HLLC+ blends HLLC and
+// HLLE by it, riemann_HLLCSD, Lib_Riemann_HLL.f90:572-605; HLLE++); 1 from walls and inflows.
 template <int RIEM>
 __device__ __forceinline__ F4 riemann64(const Gas& g, const double* L, double al, const double* R,
-                                        double ar, double nx, double ny) {
+                                        double ar, double nx, double ny, double beta = 1.0) {
+    if (RIEM == 5) {
+        if (beta == 0.0) return riemann_hlle(g, L, al, R, ar, nx, ny);
+        if (beta >= 1.0) return riemann_hllc(g, L, al, R, ar, nx, ny);
+        const F4 E = riemann_hlle(g, L, al, R, ar, nx, ny);
+        const F4 C = riemann_hllc(g, L, al, R, ar, nx, ny);
+        F4 F;
+        F.r = beta * C.r + (1.0 - beta) * E.r;
+        F.u = beta * C.u + (1.0 - beta) * E.u;
+        F.v = beta * C.v + (1.0 - beta) * E.v;
+        F.e = beta * C.e + (1.0 - beta) * E.e;
+        return F;
+    }
+    if (RIEM == 6) return riemann_hllepp(g, L, al, R, ar, beta, nx, ny);
     if (RIEM == 1) return riemann_hlle(g, L, al, R, ar, nx, ny);
     if (RIEM == 2) return riemann_llf(g, L, al, R, ar, nx, ny);
     if (RIEM == 3) return riemann_slau<false>(g, L, al, R, ar, nx, ny);
@@ -485,11 +552,12 @@ __device__ __forceinline__ F4 riemann64(const Gas& g, const double* L, double al
 // a non-physical state (check_gas_state).
 template <int RIEM>
 __device__ __forceinline__ bool flux_from_states64(const Gas& g, const double* P1, const double* P4,
-                                                   double nx, double ny, double int_l, double* fl) {
+                                                   double nx, double ny, double int_l, double* fl,
+                                                   double beta = 1.0) {
     const bool bad = gas_state_bad(P1[0], P1[3]) || gas_state_bad(P4[0], P4[3]);
     const double a1 = f_ss(g, P1[3], P1[0]);
     const double a4 = f_ss(g, P4[3], P4[0]);
-    const F4 F = riemann64<RIEM>(g, P1, a1, P4, a4, nx, ny);
+    const F4 F = riemann64<RIEM>(g, P1, a1, P4, a4, nx, ny, beta);
     // single species: sp*(rho1/rho1) - sm*(rho4/rho4) == 1 exactly
     fl[0] = F.r * int_l;
     fl[1] = F.u * int_l;

@@ -199,7 +199,7 @@ cudaError_t launch_finalize(const StageArgs& a, cudaStream_t s) {
     }
 
 cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int grid, cudaStream_t s) {
-    if (a.sd) return launch_stage_sd(a, prec, riem, tile, grid, s);
+    if (a.sd || riem >= 5) return launch_stage_sd(a, prec, riem, tile, grid, s);   // the sensor runs
     cudaError_t e = cudaErrorInvalidValue;
 #define Q2D_CALL(TX, TY, NT)                                                                   \
     if (prec == 0) {                                                                           \
@@ -221,7 +221,7 @@ cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int g
 }
 
 int stage_occupancy(int prec, int riem, int tile, int sd) {
-    if (sd) return stage_occupancy_sd(prec, riem, tile);
+    if (sd || riem >= 5) return stage_occupancy_sd(prec, riem, tile);
     int n = 0;
 #define Q2D_CALL(TX, TY, NT)                                                                   \
     if (prec == 0) {                                                                           \
@@ -354,17 +354,23 @@ cudaError_t launch_stage32_r1(const StageArgs& a, int tile, int grid, cudaStream
 cudaError_t launch_stage32_r2(const StageArgs& a, int tile, int grid, cudaStream_t s);
 cudaError_t launch_stage32_r3(const StageArgs& a, int tile, int grid, cudaStream_t s);
 cudaError_t launch_stage32_r4(const StageArgs& a, int tile, int grid, cudaStream_t s);
+cudaError_t launch_stage32_r5(const StageArgs& a, int tile, int grid, cudaStream_t s);
+cudaError_t launch_stage32_r6(const StageArgs& a, int tile, int grid, cudaStream_t s);
 int stage32_occupancy_r0(int tile);
 int stage32_occupancy_r1(int tile);
 int stage32_occupancy_r2(int tile);
 int stage32_occupancy_r3(int tile);
 int stage32_occupancy_r4(int tile);
+int stage32_occupancy_r5(int tile);
+int stage32_occupancy_r6(int tile);
 
 cudaError_t launch_stage32(const StageArgs& a, int riem, int tile, int grid, cudaStream_t s) {
     if (riem == 1) return launch_stage32_r1(a, tile, grid, s);
     if (riem == 2) return launch_stage32_r2(a, tile, grid, s);
     if (riem == 3) return launch_stage32_r3(a, tile, grid, s);
     if (riem == 4) return launch_stage32_r4(a, tile, grid, s);
+    if (riem == 5) return launch_stage32_r5(a, tile, grid, s);
+    if (riem == 6) return launch_stage32_r6(a, tile, grid, s);
     return launch_stage32_r0(a, tile, grid, s);
 }
 
@@ -373,6 +379,8 @@ int stage32_occupancy(int riem, int tile) {
     if (riem == 2) return stage32_occupancy_r2(tile);
     if (riem == 3) return stage32_occupancy_r3(tile);
     if (riem == 4) return stage32_occupancy_r4(tile);
+    if (riem == 5) return stage32_occupancy_r5(tile);
+    if (riem == 6) return stage32_occupancy_r6(tile);
     return stage32_occupancy_r0(tile);
 }
 

@@ -88,9 +88,20 @@ __device__ __forceinline__ FS32 phys32(float r, float u, float v, float p, float
 // Riemann solvers in FP32 (riemann_HLLC / riemann_HLLE, Lib_Riemann_HLL.f90:34-169; riemann_LLF,
 // Lib_Riemann_LF.f90:11-40): clamped Einfeldt speeds from constant-cp Roe averages, HLLC star
 // states written through the jumps (S* - un_K, p* - p_K). Returns the flux per unit length.
+// beta: the shock sensor the sensor-driven solvers blend by (HLLC+, HLLE++).
 template <int RIEM>
 __device__ __forceinline__ void riemann_f32(const FS32& L, const FS32& R, float nx, float ny, float gam,
-                                            float gm1, float gf, float* F) {
+                                            float gm1, float gf, float* F, float beta = 1.0f) {
+    if (RIEM == 5) {   // HLLC+ (riemann_HLLCSD, Lib_Riemann_HLL.f90:572-605)
+        if (beta == 0.0f) { riemann_f32<1>(L, R, nx, ny, gam, gm1, gf, F); return; }
+        if (beta >= 1.0f) { riemann_f32<0>(L, R, nx, ny, gam, gm1, gf, F); return; }
+        float E[4], Cf[4];
+        riemann_f32<1>(L, R, nx, ny, gam, gm1, gf, E);
+        riemann_f32<0>(L, R, nx, ny, gam, gm1, gf, Cf);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) F[v] = beta * Cf[v] + (1.0f - beta) * E[v];
+        return;
+    }
     const float irl = rcp_approx(L.r), irr = rcp_approx(R.r);
     const float al = sqrtf(gam * L.p * irl), ar = sqrtf(gam * R.p * irr);
     if (RIEM == 3 || RIEM == 4) {   // SLAU / SLAU2 (Lib_Riemann_SLAU.f90:10-124)
@@ -140,6 +151,31 @@ __device__ __forceinline__ void riemann_f32(const FS32& L, const FS32& R, float 
     const float un_roe = u_roe * nx + v_roe * ny;
     const float S1 = fminf(fminf(0.0f, L.un - al), un_roe - a_roe);
     const float S4 = fmaxf(fmaxf(0.0f, R.un + ar), un_roe + a_roe);
+    if (RIEM == 6) {   // HLLE++ (riemann_HLLEpp, Lib_Riemann_HLL.f90:437-533)
+        const float inv = rcp_approx(S4 - S1);
+        const float ps = (S4 + S1) * inv, pp = 2.0f * S4 * S1 * inv;
+        const float eps = 0.3f * (fabsf(un_roe) + a_roe);
+        const float v2 = un_roe - a_roe, v3 = un_roe + a_roe;
+        const float l2r = fabsf(v2) <= eps ? (v2 * v2 + eps * eps) * rcp_approx(2.0f * eps) : fabsf(v2);
+        const float l3r = fabsf(v3) <= eps ? (v3 * v3 + eps * eps) * rcp_approx(2.0f * eps) : fabsf(v3);
+        const float l1 = beta * fabsf(un_roe) + (1.0f - beta) * fabsf(ps * un_roe - pp);
+        const float l2 = beta * l2r + (1.0f - beta) * fabsf(ps * v2 - pp);
+        const float l3 = beta * l3r + (1.0f - beta) * fabsf(ps * v3 - pp);
+        const float rho_roe = srL * srR;
+        const float dp = R.p - L.p, dun = R.un - L.un, tx = -ny, ty = nx;
+        const float ia2 = rcp_approx(a_roe * a_roe);
+        const float am = 0.5f * (dp - rho_roe * a_roe * dun) * ia2;
+        const float ac = (R.r - L.r) - dp * ia2;
+        const float as = rho_roe * ((R.u - L.u) * tx + (R.v - L.v) * ty);
+        const float ap = 0.5f * (dp + rho_roe * a_roe * dun) * ia2;
+        const float w1 = ac * l1, ws = as * l1, w2 = am * l2, w3 = ap * l3;
+        F[0] = 0.5f * (L.Fr + R.Fr - (w1 + w2 + w3));
+        F[1] = 0.5f * (L.Fu + R.Fu - (w1 * u_roe + ws * tx + w2 * (u_roe - a_roe * nx) + w3 * (u_roe + a_roe * nx)));
+        F[2] = 0.5f * (L.Fv + R.Fv - (w1 * v_roe + ws * ty + w2 * (v_roe - a_roe * ny) + w3 * (v_roe + a_roe * ny)));
+        F[3] = 0.5f * (L.Fe + R.Fe - (w1 * 0.5f * (u_roe * u_roe + v_roe * v_roe) + ws * (u_roe * tx + v_roe * ty) +
+                                      w2 * (h0_roe - a_roe * un_roe) + w3 * (h0_roe + a_roe * un_roe)));
+        return;
+    }
     if (RIEM == 1) {
         const float inv = rcp_approx(S4 - S1);
         const float c = S1 * S4;
@@ -182,11 +218,12 @@ __device__ __forceinline__ void riemann_f32(const FS32& L, const FS32& R, float 
 
 // One interior face: stencil cells m (= L-1), L, R, p (= R+1) at shared positions base + k*step;
 // dlp is the cell-length pair array viewed as floats, offset to the face's direction.
-// beta: the shock sensor scaling both limited slopes (1 without MUSCL-SD; Lib_Convective.f90:40-47)
+// beta_l: the shock sensor scaling both limited slopes (1 without MUSCL-SD; Lib_Convective.f90:
+// 40-47); beta_r: the sensor the Riemann solver receives (:62-64)
 template <int RIEM, int LIM>
 __device__ __forceinline__ bool face32(const float4* sP, const float* dlp, int base, int step, float nx,
-                                      float ny, float len, float gam, float gm1, float gf, float beta,
-                                      float* out) {
+                                      float ny, float len, float gam, float gm1, float gf, float beta_l,
+                                      float beta_r, float* out) {
     const float dm = dlp[2 * base], d0 = dlp[2 * (base + step)], d1 = dlp[2 * (base + 2 * step)],
                 d2 = dlp[2 * (base + 3 * step)];
     const float il0 = rcp_approx(0.5f * (dm + d0));
@@ -199,14 +236,14 @@ __device__ __forceinline__ bool face32(const float4* sP, const float* dlp, int b
     for (int v = 0; v < 4; ++v) {
         const float qm = comp(Cm, v), q0 = comp(C0, v), q1 = comp(C1, v), q2 = comp(C2, v);
         const float s0 = (q0 - qm) * il0, s1 = (q1 - q0) * il1, s2 = (q2 - q1) * il2;
-        QL[v] = q0 + beta * lim32<LIM>(s1, s0) * lm;
-        QR[v] = q1 - beta * lim32<LIM>(s2, s1) * lp;
+        QL[v] = q0 + beta_l * lim32<LIM>(s1, s0) * lm;
+        QR[v] = q1 - beta_l * lim32<LIM>(s2, s1) * lp;
     }
     const bool ok = QL[0] > 0.0f && QL[3] > 0.0f && QR[0] > 0.0f && QR[3] > 0.0f;
     const FS32 L = phys32(QL[0], QL[1], QL[2], QL[3], nx, ny, gf);
     const FS32 R = phys32(QR[0], QR[1], QR[2], QR[3], nx, ny, gf);
     float F[4];
-    riemann_f32<RIEM>(L, R, nx, ny, gam, gm1, gf, F);
+    riemann_f32<RIEM>(L, R, nx, ny, gam, gm1, gf, F, beta_r);
 #pragma unroll
     for (int v = 0; v < 4; ++v) out[v] = F[v] * len;
     return ok;
@@ -248,7 +285,8 @@ __device__ __forceinline__ void interior_faces32(const StageArgs& a, const DBloc
         float out[4];
         const float4 gq = sG[f];
         const float beta = SD ? sd_cell32<W>(sP, base + step) : 1.0f;
-        const bool ok = face32<RIEM, LIM>(sP, dlp, base, step, gq.x, gq.y, gq.z, gam, gm1, gf, beta, out);
+        const bool ok = face32<RIEM, LIM>(sP, dlp, base, step, gq.x, gq.y, gq.z, gam, gm1, gf, a.sd ? beta : 1.0f,
+                                          beta, out);
         if (!ok) record_error(cs, 4, B.local_b, ii, jj, a.irk);
         sF[f] = make_float4(out[0], out[1], out[2], out[3]);
     }
@@ -257,15 +295,15 @@ __device__ __forceinline__ void interior_faces32(const StageArgs& a, const DBloc
 template <int RIEM>
 __device__ __forceinline__ bool face32_lim(int lim, const float4* sP, const float* dlp, int base, int step,
                                           float nx, float ny, float len, float gam, float gm1, float gf,
-                                          float beta, float* out) {
+                                          float beta_l, float beta_r, float* out) {
     switch (lim) {
-        case 0: return face32<RIEM, 0>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
-        case 1: return face32<RIEM, 1>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
-        case 2: return face32<RIEM, 2>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
-        case 3: return face32<RIEM, 3>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
-        case 4: return face32<RIEM, 4>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
-        case 5: return face32<RIEM, 5>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
-        default: return face32<RIEM, 6>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta, out);
+        case 0: return face32<RIEM, 0>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
+        case 1: return face32<RIEM, 1>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
+        case 2: return face32<RIEM, 2>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
+        case 3: return face32<RIEM, 3>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
+        case 4: return face32<RIEM, 4>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
+        case 5: return face32<RIEM, 5>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
+        default: return face32<RIEM, 6>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
     }
 }
 
@@ -712,7 +750,7 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                         // the sensor of the boundary cell (beta_ = blk%beta(Im,Jm))
                         const float beta = SD ? sd_cell32<W>(sP, cb) : 1.0f;
                         const bool ok = face32_lim<RIEM>(a.limiter, sP, dlp, base, step, nx, ny, ln, gam, gm1, gf,
-                                                         beta, X);
+                                                         a.sd ? beta : 1.0f, beta, X);
                         if (!ok) record_error(cs, 4, B.local_b, bi + 1, bj + 1, a.irk);
                     } else if (e.type == 300 || e.type == 400) {
                         const float4 Bc = sP[cb], Ic = sP[ci];
@@ -928,16 +966,21 @@ cudaError_t launch_stage32_sd(const StageArgs& a, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// The sensor-driven Riemann solvers (HLLC+, HLLE++) run the sensor whatever the reconstruction.
 template <int RIEM, int TX, int TY, int NT, int MB>
 cudaError_t launch_stage32_t(const StageArgs& a, int grid, cudaStream_t s) {
-    return a.sd ? launch_stage32_sd<RIEM, TX, TY, NT, MB, true>(a, grid, s)
-                : launch_stage32_sd<RIEM, TX, TY, NT, MB, false>(a, grid, s);
+    if constexpr (RIEM >= 5) {
+        return launch_stage32_sd<RIEM, TX, TY, NT, MB, true>(a, grid, s);
+    } else {
+        return a.sd ? launch_stage32_sd<RIEM, TX, TY, NT, MB, true>(a, grid, s)
+                    : launch_stage32_sd<RIEM, TX, TY, NT, MB, false>(a, grid, s);
+    }
 }
 
 template <int RIEM, int TX, int TY, int NT, int MB>
 int stage32_occupancy_t() {
     constexpr size_t smem = Tile32<TX, TY>::bytes;
-    auto k = stage32_kernel<RIEM, TX, TY, NT, MB, false>;
+    auto k = stage32_kernel<RIEM, TX, TY, NT, MB, (RIEM >= 5)>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, NT, smem);

@@ -82,9 +82,10 @@ __device__ __forceinline__ void sigma_phase(const ST* sSi, const ST* sSj, ST* sG
 
 // Face fluxes of one direction of a tile (step 5 of the stage kernel). IDIR: i-faces
 // (F = i0..i0+TX on TY rows) or j-faces (G = j0..j0+TY on TX columns).
-// SD (MUSCL-SD): both limited slopes scaled by the shock sensor sB of the face's left / lower
-// cell for an interior face (Mod_Fluxes.f90:140-204), of its boundary cell for a block-interface
-// face (Lib_BC_Fluxes_Connection.f90, beta_ = blk%beta(Im,Jm)).
+// SD: the shock sensor sB runs (MUSCL-SD or a sensor-driven Riemann solver); an interior face
+// takes it from its left / lower cell (Mod_Fluxes.f90:140-204), a block-interface face from its
+// boundary cell (Lib_BC_Fluxes_Connection.f90, beta_ = blk%beta(Im,Jm)). It scales both limited
+// slopes under MUSCL-SD (a.sd) and goes to the Riemann solver.
 template <int PREC, int RIEM, bool IDIR, int NT, int TX, int TY, bool SD, typename ST>
 __device__ __forceinline__ void face_phase(const StageArgs& a, const DBlock& B, CaseState* cs, int i0,
                                            int j0, const double* sP, const double* sD,
@@ -113,18 +114,19 @@ __device__ __forceinline__ void face_phase(const StageArgs& a, const DBlock& B, 
             const int gL = IDIR ? row * (TX + 2) + col : row * TX + col;
             const int gR = gL + (IDIR ? 1 : TX);
             const double lm = 0.5 * dlp[pL], lp = 0.5 * dlp[pL + DSTEP];
-            double beta = 1.0;
+            double beta = 1.0, beta_l = 1.0;   // the sensor; its value for the slopes (MUSCL-SD)
             if (SD) {   // cell (col - 1, row) for i-faces, (col, row - 1) for j-faces
                 const int bL = IDIR ? (row + 1) * (TX + 1) + col : row * (TX + 1) + col + 1;
                 beta = sB[Fm == 1 || Fm == 3 ? bL + (IDIR ? 1 : TX + 1) : bL];
+                if (a.sd) beta_l = beta;
             }
             double QL[4], QR[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
-                QL[v] = sP[v * AREA + pL] + (double)(beta * sg[v * NG + gL] * lm);
-                QR[v] = sP[v * AREA + pL + DSTEP] - (double)(beta * sg[v * NG + gR] * lp);
+                QL[v] = sP[v * AREA + pL] + (double)(beta_l * sg[v * NG + gL] * lm);
+                QR[v] = sP[v * AREA + pL + DSTEP] - (double)(beta_l * sg[v * NG + gR] * lp);
             }
-            if (!face_flux<PREC, RIEM>(a.gas, QL, QR, nx, ny, ln, X))
+            if (!face_flux<PREC, RIEM>(a.gas, QL, QR, nx, ny, ln, X, beta))
                 record_error(cs, 4, B.local_b, IDIR ? pos : k + 1, IDIR ? k + 1 : pos, a.irk);
         } else if (etype >= 0) {
             const bool minside = (Fm == 1 || Fm == 3);

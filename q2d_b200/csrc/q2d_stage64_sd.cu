@@ -1,6 +1,7 @@
-// MUSCL-SD instantiations of the FP64 stage kernel (q2d_stage64.cuh): the shock sensor of
-// Lib_Shock_Detector.f90:14-38 scales the face slopes. FP64 form only; the FP32-flux form of
-// MUSCL-SD runs on the FP32-flux kernel.
+// Shock-sensor instantiations of the FP64 stage kernel (q2d_stage64.cuh): the sensor of
+// Lib_Shock_Detector.f90:14-38 runs, for MUSCL-SD (it scales the face slopes) and for the
+// sensor-driven Riemann solvers HLLC+ / HLLE++ (they blend by it). FP64 form only; the FP32-flux
+// form runs on the FP32-flux kernel.
 #include "q2d_stage64.cuh"
 
 namespace q2d {
@@ -14,6 +15,8 @@ cudaError_t launch_stage_sd(const StageArgs& a, int prec, int riem, int tile, in
         case 2: e = launch_stage_t<0, 2, TX, TY, NT, true>(a, grid, s); break; \
         case 3: e = launch_stage_t<0, 3, TX, TY, NT, true>(a, grid, s); break; \
         case 4: e = launch_stage_t<0, 4, TX, TY, NT, true>(a, grid, s); break; \
+        case 5: e = launch_stage_t<0, 5, TX, TY, NT, true>(a, grid, s); break; \
+        case 6: e = launch_stage_t<0, 6, TX, TY, NT, true>(a, grid, s); break; \
         default: e = launch_stage_t<0, 0, TX, TY, NT, true>(a, grid, s); break; \
     }
     switch (tile) {
@@ -34,6 +37,8 @@ int stage_occupancy_sd(int prec, int riem, int tile) {
         case 2: n = occupancy_t<0, 2, TX, TY, NT, true>(); break;   \
         case 3: n = occupancy_t<0, 3, TX, TY, NT, true>(); break;   \
         case 4: n = occupancy_t<0, 4, TX, TY, NT, true>(); break;   \
+        case 5: n = occupancy_t<0, 5, TX, TY, NT, true>(); break;   \
+        case 6: n = occupancy_t<0, 6, TX, TY, NT, true>(); break;   \
         default: n = occupancy_t<0, 0, TX, TY, NT, true>(); break;  \
     }
     switch (tile) {

@@ -175,6 +175,8 @@ Setup read_options(const Ini& ini) {
     else if (s.riemann_name == "LLF" || s.riemann_name == "Rusanov") o.riemann = Q2D_RIEMANN_LLF;
     else if (s.riemann_name == "SLAU") o.riemann = Q2D_RIEMANN_SLAU;
     else if (s.riemann_name == "SLAU2") o.riemann = Q2D_RIEMANN_SLAU2;
+    else if (s.riemann_name == "HLLC+") o.riemann = Q2D_RIEMANN_HLLCP;
+    else if (s.riemann_name == "HLLE++") o.riemann = Q2D_RIEMANN_HLLEPP;
     else s.unsupported.push_back("[Q2D-Numerics] riemann-solver = " + s.riemann_name);
     if (const std::string* v = ini_get(ini, "Parameters", "res-threshold")) o.res_threshold = to_double(*v, "res-threshold");
     if (const std::string* v = ini_get(ini, "Parameters", "time-threshold")) o.time_threshold = to_double(*v, "time-threshold");

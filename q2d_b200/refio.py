@@ -29,7 +29,7 @@ from .cases import BlockSpec, CaseSpec
 RUNIV = 8314.46   # docs/theory/thermo.md:56
 
 _LIM_NAMES = {1: "minmod", 2: "vanleer", 3: "vanalbada", 4: "mc", 5: "superbee", 6: "LIMO3"}
-_RIEMANN_NAMES = {0: "HLLC", 1: "HLLE", 2: "LLF", 3: "SLAU", 4: "SLAU2"}
+_RIEMANN_NAMES = {0: "HLLC", 1: "HLLE", 2: "LLF", 3: "SLAU", 4: "SLAU2", 5: "HLLC+", 6: "HLLE++"}
 _SCHEME_NAMES = {1: "euler", 2: "RK2", 3: "RK3"}
 _SOURCE_NAMES = {0: "none", 1: "axisymmetric", 2: "area_variation"}
 

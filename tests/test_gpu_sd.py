@@ -11,6 +11,9 @@ of the boundary cell on a block-interface face (Lib_BC_Fluxes_Connection.f90).
 * The reference's ramp-channel case run to its 10000 iterations on the GPU passes its check.py
   gates (oblique-shock theory, sensor localisation, residual below 1e-3) with the errors the
   reference binary records, through the API and through q2d_host from the reference's formats.
+* The sensor-driven Riemann solvers HLLC+ and HLLE++ (Lib_Riemann_HLL.f90:437-533, 572-605),
+  which run the sensor with either reconstruction, to the same bars, and the ramp-channel case
+  with each of them to the case's gates.
 """
 import dataclasses
 
@@ -137,4 +140,52 @@ def test_ramp_channel_reference_case_through_host(tmp_path):
     res = np.loadtxt(tmp_path / "OUTPUT" / "residuals.dat")
     assert np.all(np.isfinite(res[:, 3])) and res[-1, 0] == 10000 and res[-1, 3] < 1e-3
     prim = refio.read_field(tmp_path / "OUTPUT" / "field.tec")[0].prim
+    ramp_channel_gates(cs, prim, sensor_field(cs, [prim])[0])
+
+
+@pytest.mark.parametrize("riemann", ["HLLC+", "HLLE++"])
+@pytest.mark.parametrize("sd", [1, 0])
+def test_sensor_driven_solvers_vs_oracle(developed, riemann, sd):
+    """HLLC+ / HLLE++ (the sensor runs whatever the reconstruction; the Riemann solver blends by
+    it) with MUSCL-SD and with plain MUSCL, on the three FP64 tiles."""
+    for cs in developed:
+        for schedule in (0, 1, 2):
+            gs, os_, _, _ = run_pair([cs], 1, schedule=schedule, riemann=riemann, shock_detector=sd)
+            check(gs, os_, 1e-12, f"{cs.name} {riemann} sd {sd} schedule {schedule} 1 step")
+        gs, os_, gi, oi = run_pair([cs], 6, chunks=2, riemann=riemann, shock_detector=sd)
+        check(gs, os_, 1e-10, f"{cs.name} {riemann} sd {sd} 6 steps")
+
+
+@pytest.mark.parametrize("riemann", ["HLLC+", "HLLE++"])
+def test_sensor_driven_solvers_fp32flux_vs_fp64(developed, riemann):
+    for cs in developed:
+        for schedule in (5, 6, 7, 8, 9):
+            out = []
+            for prec, sch in ((0, 0), (1, schedule)):
+                s = Q2DSolver(make_options(cs, precision=prec, riemann=riemann), [cs])
+                try:
+                    s.set_schedule(sch)
+                    info = s.step(10)[0]
+                    assert info["err"] == 0, info
+                    out.append(s.prims()[0])
+                finally:
+                    s.close()
+            for b, (g32, g64) in enumerate(zip(*out)):
+                err = rel_l1(g32, g64)
+                assert err.max() <= 1e-6, f"{cs.name} {riemann} block {b} schedule {schedule}: rel L1 {err}"
+
+
+@pytest.mark.parametrize("riemann", ["HLLC+", "HLLE++"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_ramp_channel_sensor_driven_solvers(riemann, precision):
+    """The ramp-channel case with HLLC+ / HLLE++ (the reference's solver sweep) to its 10000
+    iterations: residual below 1e-3 and the oblique-shock and sensor gates of its check.py."""
+    cs = ramp_channel_case()
+    s = Q2DSolver(make_options(cs, precision=precision, riemann=riemann), [cs])
+    try:
+        info = s.step(10000)[0]
+        prim = s.prims()[0][0]
+    finally:
+        s.close()
+    assert info["err"] == 0 and info["residual"][0] < 1e-3, info
     ramp_channel_gates(cs, prim, sensor_field(cs, [prim])[0])

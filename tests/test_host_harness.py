@@ -105,6 +105,12 @@ def test_inputs_outside_the_path_fail_loudly(tmp_path):
     assert d["unsupported"] == ["[Q2D-Numerics] riemann-solver = AUSM+"]
     r = host(tmp_path, check=False)   # refused before any device call
     assert r.returncode == 2 and "not on the built path" in r.stderr
+    # Assign_Riemann_Solver keywords (Mod_Riemann.f90:25-109) of the built solvers
+    for name, want in [("HLLC", 0), ("HLLE", 1), ("LLF", 2), ("Rusanov", 2), ("SLAU", 3), ("SLAU2", 4),
+                       ("HLLC+", 5), ("HLLE++", 6)]:
+        (tmp_path / "input.ini").write_text(ini.replace("riemann-solver = HLLC", f"riemann-solver = {name}"))
+        d = json.loads(host(tmp_path, "--check").stdout)
+        assert d["riemann"] == want and not d["unsupported"], (name, d["unsupported"])
     (tmp_path / "input.ini").write_text(ini)
     bc = (tmp_path / "INPUT" / "bc.txt").read_text().splitlines()
     bc[0] = bc[0][:-8] + f"{410:8d}"

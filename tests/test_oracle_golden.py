@@ -290,3 +290,58 @@ def test_ramp_channel_matches_reference_calibration():
     errs = 100.0 * np.array(ramp_channel_gates(cs, prim, beta))
     assert abs(errs[0] - (-0.002)) < 0.005, errs
     assert np.all(np.abs(errs[1:] - np.array([0.95, -0.94, -0.94])) < 0.01), errs
+
+
+def riemann_sd(kind, L, R, beta, nx=1.0, ny=0.0):
+    import ctypes as C
+    lib = oracle.load()
+    opt = make_options({})
+    a = (C.c_double * 4)(*L)
+    b = (C.c_double * 4)(*R)
+    out = (C.c_double * 4)()
+    lib.q2d_oracle_riemann_sd(kind, C.byref(opt), a, b, beta, nx, ny, out)
+    return np.array(out[:])
+
+
+def test_sensor_driven_riemann_known_answers():
+    """HLLC+ (riemann_HLLCSD, Lib_Riemann_HLL.f90:572-605) is HLLE where the sensor is 0, HLLC
+    where it is 1 and their beta-weighted blend between. HLLE++ (riemann_HLLEpp, :437-533) is
+    consistent (F(U, U) the physical flux) for every beta; with beta = 0 its eigenvalues are the
+    HLLE ones written in Roe waves, so it equals HLLE; with beta = 1 it is Roe's flux, which keeps
+    a stationary contact exactly (no mass flux), where HLLE diffuses it."""
+    rng = np.random.default_rng(17)
+    for _ in range(20):
+        L = [rng.uniform(0.2, 3), rng.uniform(-2, 2), rng.uniform(-2, 2), rng.uniform(0.2, 5)]
+        R = [rng.uniform(0.2, 3), rng.uniform(-2, 2), rng.uniform(-2, 2), rng.uniform(0.2, 5)]
+        th = rng.uniform(0, 2 * np.pi)
+        n = (np.cos(th), np.sin(th))
+        hllc, hlle = riemann(0, L, R, *n), riemann(1, L, R, *n)
+        assert np.array_equal(riemann_sd(5, L, R, 1.0, *n), hllc)
+        assert np.array_equal(riemann_sd(5, L, R, 0.0, *n), hlle)
+        b = rng.uniform(0.01, 0.99)
+        assert np.allclose(riemann_sd(5, L, R, b, *n), b * hllc + (1 - b) * hlle, rtol=1e-13, atol=1e-13)
+        scale = np.abs(hlle).max()
+        assert np.allclose(riemann_sd(6, L, R, 0.0, *n), hlle, rtol=1e-11, atol=1e-11 * scale)
+        for beta in (0.0, 0.3, 1.0):
+            assert np.allclose(riemann_sd(6, L, L, beta, *n), phys_flux(L, *n), rtol=1e-12, atol=1e-12)
+    L, R = [1.0, 0.0, 0.3, 1.0], [0.25, 0.0, 0.3, 1.0]      # stationary contact, tangential flow
+    assert abs(riemann_sd(6, L, R, 1.0)[0]) < 1e-15
+    assert abs(riemann_sd(5, L, R, 1.0)[0]) < 1e-15          # HLLC resolves it too
+    assert riemann_sd(6, L, R, 0.0)[0] > 1e-3               # HLLE does not
+
+
+@pytest.mark.parametrize("riem", ["HLLC+", "HLLE++"])
+def test_ramp_channel_sensor_driven_solvers(riem):
+    """The ramp-channel case with the sensor-driven solvers of the reference's solver sweep
+    (ramp-channel/Q2D.sh: HLLE, HLLC, HLLC+, SLAU) in place of HLLE: after 1500 iterations the
+    residual is below 1e-3 and the oblique-shock and sensor gates of its check.py pass."""
+    from tests.helpers import ramp_channel_case, ramp_channel_gates, sensor_field
+    cs = ramp_channel_case()
+    s = oracle.solver(make_options(cs, riemann=riem), [cs])
+    try:
+        info = s.step(1500)[0]
+        prim = s.prim()
+    finally:
+        s.close()
+    assert info["err"] == 0 and info["residual"][0] < 1e-3, info
+    ramp_channel_gates(cs, prim, sensor_field(cs, [prim])[0])
