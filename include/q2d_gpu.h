@@ -69,6 +69,15 @@ extern "C" {
                                             Lib_Riemann_HLL.f90:572-605 (computes the sensor) */
 #define Q2D_RIEMANN_HLLEPP 6   /* 'HLLE++' Roe / HLLE eigenvalue blend by the shock sensor,
                                             Lib_Riemann_HLL.f90:437-533 (computes the sensor) */
+#define Q2D_RIEMANN_HLLEM  7   /* 'HLLEM'             Lib_Riemann_HLL.f90:355-434 */
+#define Q2D_RIEMANN_HLLC_ROTATED 8 /* 'HLLC Rotated' HLLE / HLLC on rotated normals,
+                                            Lib_Riemann_HLL.f90:172-226 */
+#define Q2D_RIEMANN_PLLF   9   /* 'PLLF'              Lib_Riemann_LF.f90:44-98 */
+#define Q2D_RIEMANN_EXACT  10  /* 'exact' / 'Exact'   Lib_Riemann_Godunov.f90:14-248 */
+#define Q2D_RIEMANN_HANEL  11  /* 'Hanel'             Lib_Riemann_AUSM.f90:18-70 */
+#define Q2D_RIEMANN_AUSMP  12  /* 'AUSM+'             Lib_Riemann_AUSM.f90:73-128 */
+#define Q2D_RIEMANN_AUSMP_UP  13 /* 'AUSM+-up'        Lib_Riemann_AUSM.f90:131-225 (riemann_minf > 0) */
+#define Q2D_RIEMANN_AUSMP_UP2 14 /* 'AUSM+-up2'       Lib_Riemann_AUSM.f90:228-321 (riemann_minf > 0) */
 
 #define Q2D_SRC_NONE       0
 #define Q2D_SRC_AXI        1   /* [Q2D-Sources] active = axisymmetric   Lib_Source_Axisymmetry.f90:40-78 */
@@ -122,6 +131,9 @@ typedef struct q2d_options {
                                scaled by the Tramel pressure sensor of its left / lower cell
                                (Mod_Space.f90:25-27, Mod_Fluxes.f90:132-204,
                                Lib_Shock_Detector.f90:14-38); 0 by default */
+    double riemann_minf;    /* riemann-options-Minf: the reference Mach number of AUSM+-up /
+                               AUSM+-up2, required > 0 by them (Register_Numerics.f90:76,
+                               Assign_Setup.f90:108-112); 0 by default */
 } q2d_options;
 
 /* One boundary-cell record: the 5-integer header line of bc.txt plus its property line

@@ -38,6 +38,7 @@ constexpr int GUIDE[5][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}};
 // ---------------------------------------------------------------------------------------
 struct Gas {
     double R, gamma, gm1, cp, cv;
+    double minf = 0.0;   // riemann-options-Minf (AUSM+-up, AUSM+-up2)
 };
 
 inline double f_ss(const Gas& g, double p, double rho) { return std::sqrt(g.gamma * p / rho); }
@@ -378,6 +379,331 @@ inline Flux4 riemann_hllepp(const Gas& g, double dl, double ul, double vl, doubl
     return F;
 }
 
+// riemann_HLLEM (Lib_Riemann_HLL.f90:355-434): HLL flux plus Einfeldt's antidiffusion on the
+// contact and the shear wave when S1 < 0 < S4.
+inline Flux4 riemann_hllem(const Gas& g, double dl, double ul, double vl, double pl, double al,
+                           double dltot, double dr, double ur, double vr, double pr, double ar,
+                           double drtot, double nx, double ny) {
+    double h0l, h0r, rho_roe, u_roe, v_roe, a_roe, h0_roe;
+    roe_averages(g, dl, dr, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, rho_roe, u_roe,
+                 v_roe, a_roe, h0_roe);
+    const double un_roe = u_roe * nx + v_roe * ny;
+    const double S1 = fmin_(fmin_(0.0, (ul * nx + vl * ny) - al), un_roe - a_roe);
+    const double S4 = fmax_(fmax_(0.0, (ur * nx + vr * ny) + ar), un_roe + a_roe);
+    const Flux4 FL = physical_flux(g, pl, dl, ul, vl, nx, ny);
+    const Flux4 FR = physical_flux(g, pr, dr, ur, vr, nx, ny);
+    const double e0l = h0l - pl / dltot, e0r = h0r - pr / drtot;
+    const double inv_denom = 1.0 / (S4 - S1);
+    Flux4 F;
+    F.r = (S4 * FL.r - S1 * FR.r + S1 * S4 * (drtot - dltot)) * inv_denom;
+    F.u = (S4 * FL.u - S1 * FR.u + S1 * S4 * (drtot * ur - dltot * ul)) * inv_denom;
+    F.v = (S4 * FL.v - S1 * FR.v + S1 * S4 * (drtot * vr - dltot * vl)) * inv_denom;
+    F.e = (S4 * FL.e - S1 * FR.e + S1 * S4 * (drtot * e0r - dltot * e0l)) * inv_denom;
+    if (S1 < 0.0 && S4 > 0.0) {
+        const double drho = drtot - dltot, dp = pr - pl, du = ur - ul, dv = vr - vl;
+        const double tx = -ny, ty = nx;
+        const double alpha_c = drho - dp / (a_roe * a_roe);
+        const double alpha_s = rho_roe * (du * tx + dv * ty);
+        const double delta = a_roe / (a_roe + std::fabs(0.5 * (S1 + S4)));
+        const double C = (S1 * S4) * inv_denom;
+        F.r = F.r - C * delta * alpha_c;
+        F.u = F.u - C * delta * (alpha_c * u_roe + alpha_s * tx);
+        F.v = F.v - C * delta * (alpha_c * v_roe + alpha_s * ty);
+        F.e = F.e - C * delta * (alpha_c * 0.5 * (u_roe * u_roe + v_roe * v_roe) + alpha_s * (u_roe * tx + v_roe * ty));
+    }
+    return F;
+}
+
+// riemann_HLLCHLLE (Lib_Riemann_HLL.f90:172-226): HLLE along the velocity-jump direction and
+// HLLC across it, weighted by their projections on the face normal; HLLC when the jump vanishes.
+inline Flux4 riemann_hllc_rotated(const Gas& g, double dl, double ul, double vl, double pl, double al,
+                                  double dltot, double dr, double ur, double vr, double pr, double ar,
+                                  double drtot, double nx, double ny) {
+    const double abs_dv = std::sqrt((ur - ul) * (ur - ul) + (vr - vl) * (vr - vl));
+    const double dum = 0.5 * (std::sqrt(ul * ul + vl * vl) + std::sqrt(ur * ur + vr * vr));
+    if (abs_dv / (dum + 1.0e-10) > 1.0e-12) {
+        double nx1 = (ur - ul) / abs_dv, ny1 = (vr - vl) / abs_dv;
+        double alfa1 = nx * nx1 + ny * ny1;
+        const double s1 = std::copysign(1.0, alfa1);
+        nx1 = s1 * nx1; ny1 = s1 * ny1; alfa1 = s1 * alfa1;
+        double nx2 = -ny1, ny2 = nx1;
+        double alfa2 = nx * nx2 + ny * ny2;
+        const double s2 = std::copysign(1.0, alfa2);
+        nx2 = s2 * nx2; ny2 = s2 * ny2; alfa2 = s2 * alfa2;
+        const Flux4 E = riemann_hlle(g, dl, ul, vl, pl, al, dltot, dr, ur, vr, pr, ar, drtot, nx1, ny1);
+        const Flux4 C = riemann_hllc(g, dl, ul, vl, pl, al, dltot, dr, ur, vr, pr, ar, drtot, nx2, ny2);
+        Flux4 F;
+        F.r = E.r * alfa1 + C.r * alfa2;
+        F.u = E.u * alfa1 + C.u * alfa2;
+        F.v = E.v * alfa1 + C.v * alfa2;
+        F.e = E.e * alfa1 + C.e * alfa2;
+        return F;
+    }
+    return riemann_hllc(g, dl, ul, vl, pl, al, dltot, dr, ur, vr, pr, ar, drtot, nx, ny);
+}
+
+// Riemann_PLLF (Lib_Riemann_LF.f90:44-98): Rusanov flux with the dissipation speed of the
+// low-Mach preconditioned system (reference speed clipped to [1e-5 a, a]).
+inline Flux4 riemann_pllf(const Gas& g, double dl, double ul, double vl, double pl, double al,
+                          double dltot, double dr, double ur, double vr, double pr, double ar,
+                          double drtot, double nx, double ny) {
+    const double uln = ul * nx + vl * ny;
+    const double urn = ur * nx + vr * ny;
+    const double U_rl = fmax_(1e-5 * al, fmin_(std::fabs(uln), al));
+    const double U_rr = fmax_(1e-5 * ar, fmin_(std::fabs(urn), ar));
+    const double betal = 1.0 / (al * al), betar = 1.0 / (ar * ar);
+    const double alphal = 0.5 * (1.0 - betal * (U_rl * U_rl));
+    const double alphar = 0.5 * (1.0 - betar * (U_rr * U_rr));
+    const double ul_mod = std::fabs(uln * (1.0 - alphal));
+    const double ur_mod = std::fabs(urn * (1.0 - alphar));
+    const double al_mod = std::sqrt((alphal * alphal) * (uln * uln) + U_rl * U_rl);
+    const double ar_mod = std::sqrt((alphar * alphar) * (urn * urn) + U_rr * U_rr);
+    const double A = fmax_(ul_mod + al_mod, ur_mod + ar_mod);
+    const Flux4 Fr = physical_flux(g, pr, dr, ur, vr, nx, ny);
+    const Flux4 Fl = physical_flux(g, pl, dl, ul, vl, nx, ny);
+    Flux4 F;
+    F.r = 0.5 * (Fl.r + Fr.r - A * (drtot - dltot));
+    F.u = 0.5 * (Fr.u + Fl.u - A * (drtot * ur - dltot * ul));
+    F.v = 0.5 * (Fr.v + Fl.v - A * (drtot * vr - dltot * vl));
+    F.e = 0.5 * (Fl.e + Fr.e - A * (drtot * E0(g, pr, dr, std::sqrt(ur * ur + vr * vr)) -
+                                    dltot * E0(g, pl, dl, std::sqrt(ul * ul + vl * vl))));
+    return F;
+}
+
+// riemann_exact (Lib_Riemann_Godunov.f90:14-152) with its wave routines (:177-248): Newton
+// iteration on the contact velocity (|1 - p2/p3| < 1e-5, at most 1001 passes) from the
+// two-rarefaction guess, then the sampled state at x/t = 0 and its physical flux. Integer
+// powers are products; the wave-family flags keep the values of their last evaluation (0
+// before any).
+inline void ex_rareleft(double ps, double as, double us, double ud, double& pd, double& ad,
+                        double& dpr, double& v1, double& v2, double gamma) {
+    const double delta = 0.5 * (gamma - 1.0);
+    const double dum1 = 2.0 * gamma / (gamma - 1.0);
+    ad = as - delta * (ud - us);
+    pd = ps * std::pow(ad / as, dum1);
+    dpr = -gamma * pd / ad;
+    v1 = us - as;
+    v2 = ud - ad;
+}
+inline void ex_rareright(double pd, double ad, double ud, double us, double& ps, double& as,
+                         double& dpl, double& v3, double& v4, double gamma) {
+    const double delta = 0.5 * (gamma - 1.0);
+    const double dum1 = 2.0 * gamma / (gamma - 1.0);
+    as = ad + delta * (us - ud);
+    ps = pd * std::pow(as / ad, dum1);
+    dpl = gamma * ps / as;
+    v3 = us + as;
+    v4 = ud + ad;
+}
+inline void ex_shockleft(double us, double as, double ps, double ud, double& ad, double& pd,
+                         double& dpr, double& ws, double gamma) {
+    const double x1 = (gamma + 1.0) * (ud - us) / (4.0 * as);
+    const double M = x1 - std::sqrt(1.0 + x1 * x1);
+    const double C1 = gamma * ps / as;
+    pd = ps + C1 * (ud - us) * M;
+    dpr = 2.0 * C1 * (M * M * M) / (1.0 + M * M);
+    const double rpd = pd / ps;
+    ws = us + as * M;
+    ad = as * std::sqrt((gamma + 1.0 + (gamma - 1.0) * rpd) / (gamma + 1.0 + (gamma - 1.0) / rpd));
+}
+inline void ex_shockright(double ud, double ad, double pd, double us, double& as, double& ps,
+                          double& dpl, double& ws, double gamma) {
+    const double x4 = (gamma + 1.0) * (us - ud) / (4.0 * ad);
+    const double M = x4 + std::sqrt(1.0 + x4 * x4);
+    const double C4 = gamma * pd / ad;
+    ps = pd + C4 * (us - ud) * M;
+    dpl = 2.0 * C4 * (M * M * M) / (1.0 + M * M);
+    const double rps = ps / pd;
+    ws = ud + ad * M;
+    as = ad * std::sqrt((gamma + 1.0 + (gamma - 1.0) * rps) / (gamma + 1.0 + (gamma - 1.0) / rps));
+}
+inline Flux4 riemann_exact(const Gas& g, double dl, double ul, double vl, double p1, double a1,
+                           double dltot, double dr, double ur, double vr, double p4, double a4,
+                           double drtot, double nx, double ny) {
+    const double gam1 = g.gamma, gam4 = g.gamma;   // f_gamma
+    const double gm1_1 = gam1 - 1.0, gm1_4 = gam4 - 1.0;
+    const double delta1 = 0.5 * gm1_1, delta4 = 0.5 * gm1_4;
+    const double eta1 = gam1 / delta1, eta4 = gam4 / delta4;
+    const double un1 = ul * nx + vl * ny;
+    const double ut1 = ul - un1 * nx, vt1 = vl - un1 * ny;
+    const double un4 = ur * nx + vr * ny;
+    const double ut4 = ur - un4 * nx, vt4 = vr - un4 * ny;
+    const double R2I = un1 + (2.0 / gm1_1) * a1;
+    const double R1IV = un4 - (2.0 / gm1_4) * a4;
+    const double dum = p1 < p4 ? gm1_4 / (2.0 * gam4) : gm1_1 / (2.0 * gam1);
+    const double z = (gm1_1 / gm1_4) * (a4 / a1) * std::pow(p1 / p4, dum);
+    double vel = (z * R2I + R1IV) / (1.0 + z);
+    double p3 = 1.0, p2 = 2.0 * p3, a2 = 0.0, a3 = 0.0, dpr = 0.0, dpl = 0.0;
+    double sw_l = 0.0, sw_r = 0.0, vw1 = 0.0, vw2 = 0.0, vw3 = 0.0, vw4 = 0.0;
+    int iter = 0;
+    while (std::fabs(1.0 - (p2 / p3)) >= 1e-5 && iter <= 1000) {
+        if (vel < un1) ex_shockleft(un1, a1, p1, vel, a2, p2, dpr, sw_l, gam1);
+        else ex_rareleft(p1, a1, un1, vel, p2, a2, dpr, vw1, vw2, gam1);
+        if (vel > un4) ex_shockright(un4, a4, p4, vel, a3, p3, dpl, sw_r, gam4);
+        else ex_rareright(p4, a4, un4, vel, p3, a3, dpl, vw3, vw4, gam4);
+        vel = vel - ((p2 - p3) / (dpr - dpl));
+        ++iter;
+    }
+    double af, pf, rhof, uf, vf;
+    if (vel > 0.0) {
+        af = a2; pf = p2;
+        if (vel <= un1) {
+            if (sw_l > 0.0) { af = a1; vel = un1; pf = p1; }
+        } else if (vw1 > 0.0) {
+            vel = un1; af = a1; pf = p1;
+        } else if (vw2 > 0.0) {
+            af = (un1 + a1 / delta1) / (1.0 + 1.0 / delta1);
+            vel = af;
+            pf = p1 * std::pow(af / a1, eta1);
+        }
+        rhof = gam1 * pf / (af * af);
+        rhof = dl / dltot * rhof;
+        uf = vel * nx + ut1;
+        vf = vel * ny + vt1;
+    } else {
+        af = a3; pf = p3;
+        if (vel >= un4) {
+            if (sw_r < 0.0) { af = a4; vel = un4; pf = p4; }
+        } else if (vw4 < 0.0) {
+            af = a4; vel = un4; pf = p4;
+        } else if (vw3 < 0.0) {
+            af = -(un4 - a4 / delta4) / (1.0 + 1.0 / delta4);
+            vel = -af;
+            pf = p4 * std::pow(af / a4, eta4);
+        }
+        rhof = gam4 * pf / (af * af);
+        rhof = dr / drtot * rhof;
+        uf = vel * nx + ut4;
+        vf = vel * ny + vt4;
+    }
+    return physical_flux(g, pf, rhof, uf, vf, nx, ny);   // fluxes (:155-174)
+}
+
+// riemann_Hanel (Lib_Riemann_AUSM.f90:18-70): van Leer splitting of the normal velocity and
+// the pressure, total enthalpy convected.
+inline Flux4 riemann_hanel(const Gas& g, double dl, double ul, double vl, double pl, double al,
+                           double dltot, double dr, double ur, double vr, double pr, double ar,
+                           double drtot, double nx, double ny) {
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    const double H_L = H0(g, pl, dl, std::sqrt(ul * ul + vl * vl));
+    const double H_R = H0(g, pr, dr, std::sqrt(ur * ur + vr * vr));
+    const double uLp = std::fabs(unl) <= al ? (unl + al) * (unl + al) / (4.0 * al) : 0.5 * (unl + std::fabs(unl));
+    const double uRm = std::fabs(unr) <= ar ? (-((unr - ar) * (unr - ar))) / (4.0 * ar) : 0.5 * (unr - std::fabs(unr));
+    const double pLp = std::fabs(unl) <= al ? pl * uLp * (2.0 - unl / al) / al : pl * uLp / unl;
+    const double pRm = std::fabs(unr) <= ar ? pr * uRm * (-2.0 - unr / ar) / ar : pr * uRm / unr;
+    const double phalf = pLp + pRm;
+    Flux4 F;
+    F.r = uLp * dltot + uRm * drtot;
+    F.u = uLp * (dltot * ul) + uRm * (drtot * ur) + phalf * nx;
+    F.v = uLp * (dltot * vl) + uRm * (drtot * vr) + phalf * ny;
+    F.e = uLp * (dltot * H_L) + uRm * (drtot * H_R);
+    return F;
+}
+
+// riemann_AUSMp (Lib_Riemann_AUSM.f90:73-128): AUSM+ with the geometric-mean interface sound
+// speed, quartic Mach and quintic pressure polynomials (beta 1/8, alpha 3/16).
+inline Flux4 riemann_ausmp(const Gas& g, double dl, double ul, double vl, double pl, double al,
+                           double dltot, double dr, double ur, double vr, double pr, double ar,
+                           double drtot, double nx, double ny) {
+    const double betap = 0.125, alpha = 0.1875;
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    const double H_L = H0(g, pl, dl, std::sqrt(ul * ul + vl * vl));
+    const double H_R = H0(g, pr, dr, std::sqrt(ur * ur + vr * vr));
+    const double a_half = std::sqrt(al * ar);
+    const double ML = unl / a_half, MR = unr / a_half;
+    double MplusL, pplusL, MminusR, pminusR;
+    if (std::fabs(ML) < 1.0) {
+        const double q = (ML + 1.0) * (ML + 1.0), w = (ML * ML - 1.0) * (ML * ML - 1.0);
+        MplusL = 0.25 * q + betap * w;
+        pplusL = 0.25 * q * (2.0 - ML) + alpha * ML * w;
+    } else {
+        MplusL = 0.5 * (ML + std::fabs(ML));
+        pplusL = 0.5 * (1.0 + std::copysign(1.0, ML));
+    }
+    if (std::fabs(MR) < 1.0) {
+        const double q = (MR - 1.0) * (MR - 1.0), w = (MR * MR - 1.0) * (MR * MR - 1.0);
+        MminusR = -0.25 * q - betap * w;
+        pminusR = 0.25 * q * (2.0 + MR) - alpha * MR * w;
+    } else {
+        MminusR = 0.5 * (MR - std::fabs(MR));
+        pminusR = 0.5 * (1.0 - std::copysign(1.0, MR));
+    }
+    const double Mhalf = MplusL + MminusR;
+    const double phalf = pplusL * pl + pminusR * pr;
+    const double mdotp = dltot * a_half * 0.5 * (Mhalf + std::fabs(Mhalf));
+    const double mdotm = drtot * a_half * 0.5 * (Mhalf - std::fabs(Mhalf));
+    Flux4 F;
+    F.r = mdotp + mdotm;
+    F.u = mdotp * ul + mdotm * ur + nx * phalf;
+    F.v = mdotp * vl + mdotm * vr + ny * phalf;
+    F.e = mdotp * H_L + mdotm * H_R;
+    return F;
+}
+
+// riemann_AUSMp_up / riemann_AUSMp_up2 (Lib_Riemann_AUSM.f90:131-321): AUSM+-up with the
+// critical-speed interface sound speed, the reference Mach number from max(M_F^2, Minf^2),
+// pressure diffusion in the mass flux (Kp 1/4, sigma 1) and, for AUSM+-up, velocity diffusion
+// in the pressure flux (Ku 3/4); AUSM+-up2 takes its pressure flux in Kitamura-Shima form.
+inline Flux4 riemann_ausmp_up(const Gas& g, bool up2, double minf, double dl, double ul, double vl,
+                              double pl, double dltot, double dr, double ur, double vr, double pr,
+                              double drtot, double nx, double ny) {
+    const double Kp = 0.25, Ku = 0.75, sigma = 1.0, betap = 0.125;
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    const double H_L = H0(g, pl, dl, std::sqrt(ul * ul + vl * vl));
+    const double H_R = H0(g, pr, dr, std::sqrt(ur * ur + vr * vr));
+    const double gamma_L = g.gamma, gamma_R = g.gamma;   // f_gamma
+    const double astarL2 = 2.0 * (gamma_L - 1.0) / (gamma_L + 1.0) * H_L;
+    const double astarR2 = 2.0 * (gamma_R - 1.0) / (gamma_R + 1.0) * H_R;
+    const double astarL = std::sqrt(astarL2), astarR = std::sqrt(astarR2);
+    const double atildeL = astarL2 / fmax_(astarL, unl);
+    const double atildeR = astarR2 / fmax_(astarR, -unr);
+    const double aF = fmin_(atildeL, atildeR);
+    const double mL = unl / aF, mR = unr / aF;
+    const double MFsq = 0.5 * (mL * mL + mR * mR);
+    const double Mrefsq = fmin_(1.0, fmax_(MFsq, minf * minf));
+    const double fa = 2.0 * std::sqrt(Mrefsq) - Mrefsq;
+    const double alpha = 0.1875 * (-4.0 + 5.0 * fa * fa);
+    double mLP, bLP, mRM, bRM;
+    if (std::fabs(mL) <= 1.0) {
+        const double p1 = 0.25 * ((mL + 1.0) * (mL + 1.0)), p2 = (mL * mL - 1.0) * (mL * mL - 1.0);
+        mLP = p1 + betap * p2;
+        bLP = p1 * (2.0 - mL) + alpha * mL * p2;
+    } else {
+        mLP = 0.5 * (mL + std::fabs(mL));
+        bLP = mLP / mL;
+    }
+    if (std::fabs(mR) <= 1.0) {
+        const double p1 = 0.25 * ((mR - 1.0) * (mR - 1.0)), p2 = (mR * mR - 1.0) * (mR * mR - 1.0);
+        mRM = -p1 - betap * p2;
+        bRM = p1 * (2.0 + mR) - alpha * mR * p2;
+    } else {
+        mRM = 0.5 * (mR - std::fabs(mR));
+        bRM = mRM / mR;
+    }
+    const double rhoF = 0.5 * (dltot + drtot);
+    const double Mp = -(Kp / fa) * fmax_(0.0, 1.0 - sigma * MFsq) * (pr - pl) / (rhoF * aF * aF);
+    const double mF = mLP + mRM + Mp;
+    const double mdot = aF * (fmax_(mF, 0.0) * dltot + fmin_(mF, 0.0) * drtot);
+    double phalf;
+    if (up2) {
+        const double sq_vel = 0.5 * ((ul * ul + vl * vl) + (ur * ur + vr * vr));
+        phalf = 0.5 * (pr + pl) + 0.5 * (bLP - bRM) * (pl - pr) + std::sqrt(sq_vel) * (bLP + bRM - 1.0) * rhoF * aF;
+    } else {
+        const double Pu = -Ku * fa * bLP * bRM * 2.0 * rhoF * aF * (unr - unl);
+        phalf = bLP * pl + bRM * pr + Pu;
+    }
+    const bool upw = mF >= 0.0;
+    Flux4 F;
+    F.r = mdot;
+    F.u = mdot * (upw ? ul : ur) + nx * phalf;
+    F.v = mdot * (upw ? vl : vr) + ny * phalf;
+    F.e = mdot * (upw ? H_L : H_R);
+    return F;
+}
+
 // beta: the shock sensor of the face's cell for the sensor-driven solvers (HLLC+, HLLE++;
 // Convective_Flux passes it, Lib_Convective.f90:62-64), 1 from the wall and inflow boundaries.
 inline Flux4 riemann(int kind, const Gas& g, const double* L, double aL, const double* R,
@@ -399,6 +725,22 @@ inline Flux4 riemann(int kind, const Gas& g, const double* L, double aL, const d
         }
         case Q2D_RIEMANN_HLLEPP:
             return riemann_hllepp(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], beta, nx, ny);
+        case Q2D_RIEMANN_HLLEM:
+            return riemann_hllem(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], nx, ny);
+        case Q2D_RIEMANN_HLLC_ROTATED:
+            return riemann_hllc_rotated(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], nx, ny);
+        case Q2D_RIEMANN_PLLF:
+            return riemann_pllf(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], nx, ny);
+        case Q2D_RIEMANN_EXACT:
+            return riemann_exact(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], nx, ny);
+        case Q2D_RIEMANN_HANEL:
+            return riemann_hanel(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], nx, ny);
+        case Q2D_RIEMANN_AUSMP:
+            return riemann_ausmp(g, L[0], L[1], L[2], L[3], aL, L[0], R[0], R[1], R[2], R[3], aR, R[0], nx, ny);
+        case Q2D_RIEMANN_AUSMP_UP:
+        case Q2D_RIEMANN_AUSMP_UP2:
+            return riemann_ausmp_up(g, kind == Q2D_RIEMANN_AUSMP_UP2, g.minf, L[0], L[1], L[2], L[3], L[0], R[0], R[1],
+                                    R[2], R[3], R[0], nx, ny);
         case Q2D_RIEMANN_SLAU:
         case Q2D_RIEMANN_SLAU2:
             return riemann_slau(g, kind == Q2D_RIEMANN_SLAU2, L[0], L[1], L[2], L[3], aL, R[0], R[1], R[2],
@@ -1536,7 +1878,9 @@ int q2d_oracle_set_threads(int n) {
 int q2d_oracle_create(q2d_oracle** out, const q2d_options* opt) {
     if (!out || !opt) return Q2D_ERR_BADARG;
     if (opt->n_rk < 1 || opt->n_rk > 3 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) || !(opt->irs_beta >= 0.0) ||
-        opt->res_diter < 1 || opt->sol_diter < 1 || opt->shock_detector < 0 || opt->shock_detector > 1)
+        opt->res_diter < 1 || opt->sol_diter < 1 || opt->shock_detector < 0 || opt->shock_detector > 1 ||
+        opt->riemann < 0 || opt->riemann > Q2D_RIEMANN_AUSMP_UP2 || !(opt->riemann_minf >= 0.0) ||
+        ((opt->riemann == Q2D_RIEMANN_AUSMP_UP || opt->riemann == Q2D_RIEMANN_AUSMP_UP2) && !(opt->riemann_minf > 0.0)))
         return Q2D_ERR_BADARG;
     q2d_oracle* o = new (std::nothrow) q2d_oracle();
     if (!o) return Q2D_ERR_OOM;
@@ -1546,6 +1890,7 @@ int q2d_oracle_create(q2d_oracle** out, const q2d_options* opt) {
     o->gas.gm1 = opt->gas_gamma - 1.0;
     o->gas.cp = opt->gas_gamma * opt->gas_R / (opt->gas_gamma - 1.0);
     o->gas.cv = opt->gas_R / (opt->gas_gamma - 1.0);
+    o->gas.minf = opt->riemann_minf;
     *out = o;
     return Q2D_OK;
 }
@@ -1693,6 +2038,7 @@ void q2d_oracle_riemann(int kind, const q2d_options* opt, const double* L, const
     Gas g;
     g.R = opt->gas_R; g.gamma = opt->gas_gamma; g.gm1 = g.gamma - 1.0;
     g.cp = g.gamma * g.R / g.gm1; g.cv = g.R / g.gm1;
+    g.minf = opt->riemann_minf;
     const double aL = f_ss(g, L[3], L[0]), aR = f_ss(g, R[3], R[0]);
     const Flux4 F = riemann(kind, g, L, aL, R, aR, nx, ny);
     flux4[0] = F.r; flux4[1] = F.u; flux4[2] = F.v; flux4[3] = F.e;
@@ -1703,6 +2049,7 @@ void q2d_oracle_riemann_sd(int kind, const q2d_options* opt, const double* L, co
     Gas g;
     g.R = opt->gas_R; g.gamma = opt->gas_gamma; g.gm1 = g.gamma - 1.0;
     g.cp = g.gamma * g.R / g.gm1; g.cv = g.R / g.gm1;
+    g.minf = opt->riemann_minf;
     const double aL = f_ss(g, L[3], L[0]), aR = f_ss(g, R[3], R[0]);
     const Flux4 F = riemann(kind, g, L, aL, R, aR, nx, ny, beta);
     flux4[0] = F.r; flux4[1] = F.u; flux4[2] = F.v; flux4[3] = F.e;

@@ -24,7 +24,9 @@ OK, ERR_BADARG, ERR_OOM, ERR_CUDA, ERR_NONPHYSICAL, ERR_NAN, ERR_TIMEOUT, ERR_UN
 
 LIM = {"iord": 0, "none": 0, "first-order": 0, "minmod": 1, "vanleer": 2, "vanalbada": 3,
        "mc": 4, "superbee": 5, "LIMO3": 6}
-RIEMANN = {"HLLC": 0, "HLLE": 1, "LLF": 2, "Rusanov": 2, "SLAU": 3, "SLAU2": 4, "HLLC+": 5, "HLLE++": 6}
+RIEMANN = {"HLLC": 0, "HLLE": 1, "LLF": 2, "Rusanov": 2, "SLAU": 3, "SLAU2": 4, "HLLC+": 5, "HLLE++": 6,
+           "HLLEM": 7, "HLLC Rotated": 8, "PLLF": 9, "exact": 10, "Exact": 10, "Hanel": 11, "AUSM+": 12,
+           "AUSM+-up": 13, "AUSM+-up2": 14}
 SRC = {"none": 0, "axisymmetric": 1, "area_variation": 2}
 PREC_FP64, PREC_FP32_FLUX = 0, 1
 TODO_CONTINUE, TODO_IO, TODO_END = 1, 2, 3
@@ -40,7 +42,7 @@ class Options(C.Structure):
         ("itermax", C.c_longlong),
         ("cfl", C.c_double), ("res_threshold", C.c_double), ("time_threshold", C.c_double),
         ("sol_dtime", C.c_double), ("gas_R", C.c_double), ("gas_gamma", C.c_double),
-        ("irs_beta", C.c_double), ("shock_detector", C.c_int),
+        ("irs_beta", C.c_double), ("shock_detector", C.c_int), ("riemann_minf", C.c_double),
     ]
 
 
@@ -92,6 +94,7 @@ def default_options(**kw) -> Options:
     o.gas_gamma = 1.4
     o.irs_beta = 0.0
     o.shock_detector = 0
+    o.riemann_minf = 0.0
     for k, v in kw.items():
         if isinstance(v, str):
             v = {"limiter": LIM, "riemann": RIEMANN, "source": SRC}[k][v]

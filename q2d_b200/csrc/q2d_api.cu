@@ -814,7 +814,9 @@ bool schedule_allowed(const q2d_ctx* ctx, int k) {
     if (kSchedules[k].kernel == 1 &&
         (ctx->opt.irs_beta > 0.0 || ctx->opt.riemann > 2 || ctx->opt.shock_detector))
         return false;   // the warp-marching kernel has no IRS passes, SLAU or shock sensor
-    if (kSchedules[k].kernel == 0 && (ctx->opt.shock_detector || ctx->opt.riemann >= Q2D_RIEMANN_HLLCP) &&
+    const bool sensor = ctx->opt.shock_detector || ctx->opt.riemann == Q2D_RIEMANN_HLLCP ||
+                        ctx->opt.riemann == Q2D_RIEMANN_HLLEPP;
+    if (kSchedules[k].kernel == 0 && sensor &&
         ctx->opt.precision != Q2D_PREC_FP64)
         return false;   // the shock sensor on the tile kernel: FP64 form only (FP32-flux: the FP32-flux kernel)
     return kSchedules[k].kernel != 2 || ctx->opt.precision == Q2D_PREC_FP32_FLUX;
@@ -876,11 +878,12 @@ int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
 
 int check_options(const q2d_options* opt) {
     if (opt->n_rk < 1 || opt->n_rk > 3 || opt->limiter < 0 || opt->limiter > 6 || opt->riemann < 0 ||
-        opt->riemann > 6 || opt->source < 0 || opt->source > 2 || opt->precision < 0 ||
+        opt->riemann > Q2D_RIEMANN_AUSMP_UP2 || opt->source < 0 || opt->source > 2 || opt->precision < 0 ||
         opt->precision > 1 || !(opt->gas_gamma > 1.0) || !(opt->gas_R > 0.0) || opt->res_diter < 1 ||
         opt->sol_diter < 1 || !(opt->cfl > 0.0) || !(opt->irs_beta >= 0.0) || !(opt->irs_beta < 1e300) ||
-        opt->shock_detector < 0 || opt->shock_detector > 1)
-        return Q2D_ERR_BADARG;
+        opt->shock_detector < 0 || opt->shock_detector > 1 || !(opt->riemann_minf >= 0.0) ||
+        ((opt->riemann == Q2D_RIEMANN_AUSMP_UP || opt->riemann == Q2D_RIEMANN_AUSMP_UP2) && !(opt->riemann_minf > 0.0)))
+        return Q2D_ERR_BADARG;   // AUSM+-up needs Minf (Assign_Setup.f90:108-112)
     return Q2D_OK;
 }
 
@@ -941,6 +944,8 @@ q2d_ctx* new_ctx(const q2d_options* opt) {
     ctx->gas.cv = opt->gas_R / (opt->gas_gamma - 1.0);
     ctx->gas.gfac = opt->gas_gamma / (opt->gas_gamma - 1.0);
     ctx->gas.igm1 = 1.0 / (opt->gas_gamma - 1.0);
+    ctx->gas.rkind = opt->riemann;
+    ctx->gas.minf = opt->riemann_minf;
     cudaGetDevice(&ctx->device);
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {

@@ -84,6 +84,8 @@ struct Gas {
     double R, gamma, gm1, cp, cv;
     double gfac;   // gamma / (gamma - 1)
     double igm1;   // 1 / (gamma - 1)
+    int rkind;     // the Riemann solver (Q2D_RIEMANN_*): selects among the ones of the generic form
+    double minf;   // riemann-options-Minf (AUSM+-up, AUSM+-up2)
 };
 
 struct StageArgs {
@@ -523,6 +525,323 @@ __device__ __forceinline__ F4 riemann_hllepp(const Gas& g, const double* L, doub
     return F;
 }
 
+// The Riemann solvers the reference offers beside the ones above, FP64, in the oracle's operation
+// order; riemann64<kRiemGeneric> selects among them at run time (Gas::rkind).
+// riemann_HLLEM (Lib_Riemann_HLL.f90:355-434): HLL plus antidiffusion on contact and shear.
+static __device__ __noinline__ F4 riemann_hllem(const Gas& g, const double* L, double al, const double* R, double ar,
+                                         double nx, double ny) {
+    const double dltot = L[0], ul = L[1], vl = L[2], pl = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], pr = R[3];
+    double h0l, h0r, u_roe, v_roe, a_roe, rho_roe, h0_roe;
+    roe_averages(g, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, u_roe, v_roe, a_roe, rho_roe, h0_roe);
+    const double un_roe = u_roe * nx + v_roe * ny;
+    const double S1 = dmin(dmin(0.0, (ul * nx + vl * ny) - al), un_roe - a_roe);
+    const double S4 = dmax(dmax(0.0, (ur * nx + vr * ny) + ar), un_roe + a_roe);
+    const F4 FL = phys_flux(g, pl, dltot, ul, vl, nx, ny);
+    const F4 FR = phys_flux(g, pr, drtot, ur, vr, nx, ny);
+    const double e0l = h0l - pl / dltot, e0r = h0r - pr / drtot;
+    const double inv_denom = 1.0 / (S4 - S1);
+    F4 F;
+    F.r = (S4 * FL.r - S1 * FR.r + S1 * S4 * (drtot - dltot)) * inv_denom;
+    F.u = (S4 * FL.u - S1 * FR.u + S1 * S4 * (drtot * ur - dltot * ul)) * inv_denom;
+    F.v = (S4 * FL.v - S1 * FR.v + S1 * S4 * (drtot * vr - dltot * vl)) * inv_denom;
+    F.e = (S4 * FL.e - S1 * FR.e + S1 * S4 * (drtot * e0r - dltot * e0l)) * inv_denom;
+    if (S1 < 0.0 && S4 > 0.0) {
+        const double drho = drtot - dltot, dp = pr - pl, du = ur - ul, dv = vr - vl;
+        const double tx = -ny, ty = nx;
+        const double alpha_c = drho - dp / (a_roe * a_roe);
+        const double alpha_s = rho_roe * (du * tx + dv * ty);
+        const double delta = a_roe / (a_roe + fabs(0.5 * (S1 + S4)));
+        const double C = (S1 * S4) * inv_denom;
+        F.r = F.r - C * delta * alpha_c;
+        F.u = F.u - C * delta * (alpha_c * u_roe + alpha_s * tx);
+        F.v = F.v - C * delta * (alpha_c * v_roe + alpha_s * ty);
+        F.e = F.e - C * delta * (alpha_c * 0.5 * (u_roe * u_roe + v_roe * v_roe) + alpha_s * (u_roe * tx + v_roe * ty));
+    }
+    return F;
+}
+
+// riemann_HLLCHLLE (Lib_Riemann_HLL.f90:172-226): HLLE along the velocity jump, HLLC across it.
+static __device__ __noinline__ F4 riemann_hllc_rotated(const Gas& g, const double* L, double al, const double* R,
+                                                double ar, double nx, double ny) {
+    const double ul = L[1], vl = L[2], ur = R[1], vr = R[2];
+    const double abs_dv = sqrt((ur - ul) * (ur - ul) + (vr - vl) * (vr - vl));
+    const double dum = 0.5 * (sqrt(ul * ul + vl * vl) + sqrt(ur * ur + vr * vr));
+    if (abs_dv / (dum + 1.0e-10) > 1.0e-12) {
+        double nx1 = (ur - ul) / abs_dv, ny1 = (vr - vl) / abs_dv;
+        double alfa1 = nx * nx1 + ny * ny1;
+        const double s1 = copysign(1.0, alfa1);
+        nx1 = s1 * nx1; ny1 = s1 * ny1; alfa1 = s1 * alfa1;
+        double nx2 = -ny1, ny2 = nx1;
+        double alfa2 = nx * nx2 + ny * ny2;
+        const double s2 = copysign(1.0, alfa2);
+        nx2 = s2 * nx2; ny2 = s2 * ny2; alfa2 = s2 * alfa2;
+        const F4 E = riemann_hlle(g, L, al, R, ar, nx1, ny1);
+        const F4 C = riemann_hllc(g, L, al, R, ar, nx2, ny2);
+        F4 F;
+        F.r = E.r * alfa1 + C.r * alfa2;
+        F.u = E.u * alfa1 + C.u * alfa2;
+        F.v = E.v * alfa1 + C.v * alfa2;
+        F.e = E.e * alfa1 + C.e * alfa2;
+        return F;
+    }
+    return riemann_hllc(g, L, al, R, ar, nx, ny);
+}
+
+// Riemann_PLLF (Lib_Riemann_LF.f90:44-98): Rusanov with the preconditioned dissipation speed.
+static __device__ __noinline__ F4 riemann_pllf(const Gas& g, const double* L, double al, const double* R, double ar,
+                                        double nx, double ny) {
+    const double dltot = L[0], ul = L[1], vl = L[2], pl = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], pr = R[3];
+    const double uln = ul * nx + vl * ny;
+    const double urn = ur * nx + vr * ny;
+    const double U_rl = dmax(1e-5 * al, dmin(fabs(uln), al));
+    const double U_rr = dmax(1e-5 * ar, dmin(fabs(urn), ar));
+    const double betal = 1.0 / (al * al), betar = 1.0 / (ar * ar);
+    const double alphal = 0.5 * (1.0 - betal * (U_rl * U_rl));
+    const double alphar = 0.5 * (1.0 - betar * (U_rr * U_rr));
+    const double ul_mod = fabs(uln * (1.0 - alphal));
+    const double ur_mod = fabs(urn * (1.0 - alphar));
+    const double al_mod = sqrt((alphal * alphal) * (uln * uln) + U_rl * U_rl);
+    const double ar_mod = sqrt((alphar * alphar) * (urn * urn) + U_rr * U_rr);
+    const double A = dmax(ul_mod + al_mod, ur_mod + ar_mod);
+    const F4 Fr = phys_flux(g, pr, drtot, ur, vr, nx, ny);
+    const F4 Fl = phys_flux(g, pl, dltot, ul, vl, nx, ny);
+    F4 F;
+    F.r = 0.5 * (Fl.r + Fr.r - A * (drtot - dltot));
+    F.u = 0.5 * (Fr.u + Fl.u - A * (drtot * ur - dltot * ul));
+    F.v = 0.5 * (Fr.v + Fl.v - A * (drtot * vr - dltot * vl));
+    F.e = 0.5 * (Fl.e + Fr.e - A * (drtot * E0(g, pr, drtot, sqrt(ur * ur + vr * vr)) -
+                                    dltot * E0(g, pl, dltot, sqrt(ul * ul + vl * vl))));
+    return F;
+}
+
+// riemann_exact (Lib_Riemann_Godunov.f90:14-248): Newton iteration on the contact velocity
+// (|1 - p2/p3| < 1e-5, at most 1001 passes; bounded), the sampled state at x/t = 0, its flux.
+__device__ __forceinline__ void ex_rare(double ps, double as, double us, double ud, double sgn, double gamma,
+                                        double& pd, double& ad, double& dp, double& v1, double& v2) {
+    // rareleft (sgn = +1): ad = as - delta (ud - us), v1 = us - as, v2 = ud - ad; rareright
+    // (sgn = -1, with the roles of the two states exchanged): ad = as + delta (ud - us),
+    // v1 = ud + ad, v2 = us + as
+    const double delta = 0.5 * (gamma - 1.0);
+    const double dum1 = 2.0 * gamma / (gamma - 1.0);
+    ad = sgn > 0.0 ? as - delta * (ud - us) : as + delta * (ud - us);
+    pd = ps * pow(ad / as, dum1);
+    dp = sgn > 0.0 ? -gamma * pd / ad : gamma * pd / ad;
+    v1 = sgn > 0.0 ? us - as : ud + ad;
+    v2 = sgn > 0.0 ? ud - ad : us + as;
+}
+__device__ __forceinline__ void ex_shock(double us, double as, double ps, double ud, double sgn, double gamma,
+                                         double& ad, double& pd, double& dp, double& ws) {
+    // shockleft (sgn = +1): M = x - sqrt(1 + x^2); shockright (sgn = -1): M = x + sqrt(1 + x^2)
+    const double x = (gamma + 1.0) * (ud - us) / (4.0 * as);
+    const double M = sgn > 0.0 ? x - sqrt(1.0 + x * x) : x + sqrt(1.0 + x * x);
+    const double C = gamma * ps / as;
+    pd = ps + C * (ud - us) * M;
+    dp = 2.0 * C * (M * M * M) / (1.0 + M * M);
+    const double rp = pd / ps;
+    ws = us + as * M;
+    ad = as * sqrt((gamma + 1.0 + (gamma - 1.0) * rp) / (gamma + 1.0 + (gamma - 1.0) / rp));
+}
+static __device__ __noinline__ F4 riemann_exact(const Gas& g, const double* L, double a1, const double* R, double a4,
+                                         double nx, double ny) {
+    const double dltot = L[0], ul = L[1], vl = L[2], p1 = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], p4 = R[3];
+    const double gam1 = g.gamma, gam4 = g.gamma;
+    const double gm1_1 = gam1 - 1.0, gm1_4 = gam4 - 1.0;
+    const double delta1 = 0.5 * gm1_1, delta4 = 0.5 * gm1_4;
+    const double eta1 = gam1 / delta1, eta4 = gam4 / delta4;
+    const double un1 = ul * nx + vl * ny;
+    const double ut1 = ul - un1 * nx, vt1 = vl - un1 * ny;
+    const double un4 = ur * nx + vr * ny;
+    const double ut4 = ur - un4 * nx, vt4 = vr - un4 * ny;
+    const double R2I = un1 + (2.0 / gm1_1) * a1;
+    const double R1IV = un4 - (2.0 / gm1_4) * a4;
+    const double dum = p1 < p4 ? gm1_4 / (2.0 * gam4) : gm1_1 / (2.0 * gam1);
+    const double z = (gm1_1 / gm1_4) * (a4 / a1) * pow(p1 / p4, dum);
+    double vel = (z * R2I + R1IV) / (1.0 + z);
+    double p3 = 1.0, p2 = 2.0 * p3, a2 = 0.0, a3 = 0.0, dpr = 0.0, dpl = 0.0;
+    double sw_l = 0.0, sw_r = 0.0, vw1 = 0.0, vw2 = 0.0, vw3 = 0.0, vw4 = 0.0;
+    for (int iter = 0; fabs(1.0 - (p2 / p3)) >= 1e-5 && iter <= 1000; ++iter) {
+        if (vel < un1) ex_shock(un1, a1, p1, vel, 1.0, gam1, a2, p2, dpr, sw_l);
+        else ex_rare(p1, a1, un1, vel, 1.0, gam1, p2, a2, dpr, vw1, vw2);
+        if (vel > un4) ex_shock(un4, a4, p4, vel, -1.0, gam4, a3, p3, dpl, sw_r);
+        else ex_rare(p4, a4, un4, vel, -1.0, gam4, p3, a3, dpl, vw3, vw4);
+        vel = vel - ((p2 - p3) / (dpr - dpl));
+    }
+    double af, pf, rhof, uf, vf;
+    if (vel > 0.0) {
+        af = a2; pf = p2;
+        if (vel <= un1) {
+            if (sw_l > 0.0) { af = a1; vel = un1; pf = p1; }
+        } else if (vw1 > 0.0) {
+            vel = un1; af = a1; pf = p1;
+        } else if (vw2 > 0.0) {
+            af = (un1 + a1 / delta1) / (1.0 + 1.0 / delta1);
+            vel = af;
+            pf = p1 * pow(af / a1, eta1);
+        }
+        rhof = gam1 * pf / (af * af);
+        rhof = dltot / dltot * rhof;
+        uf = vel * nx + ut1;
+        vf = vel * ny + vt1;
+    } else {
+        af = a3; pf = p3;
+        if (vel >= un4) {
+            if (sw_r < 0.0) { af = a4; vel = un4; pf = p4; }
+        } else if (vw4 < 0.0) {
+            af = a4; vel = un4; pf = p4;
+        } else if (vw3 < 0.0) {
+            af = -(un4 - a4 / delta4) / (1.0 + 1.0 / delta4);
+            vel = -af;
+            pf = p4 * pow(af / a4, eta4);
+        }
+        rhof = gam4 * pf / (af * af);
+        rhof = drtot / drtot * rhof;
+        uf = vel * nx + ut4;
+        vf = vel * ny + vt4;
+    }
+    return phys_flux(g, pf, rhof, uf, vf, nx, ny);
+}
+
+// riemann_Hanel (Lib_Riemann_AUSM.f90:18-70): van Leer splitting of velocity and pressure.
+static __device__ __noinline__ F4 riemann_hanel(const Gas& g, const double* L, double al, const double* R, double ar,
+                                         double nx, double ny) {
+    const double dltot = L[0], ul = L[1], vl = L[2], pl = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], pr = R[3];
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    const double H_L = H0(g, pl, dltot, sqrt(ul * ul + vl * vl));
+    const double H_R = H0(g, pr, drtot, sqrt(ur * ur + vr * vr));
+    const double uLp = fabs(unl) <= al ? (unl + al) * (unl + al) / (4.0 * al) : 0.5 * (unl + fabs(unl));
+    const double uRm = fabs(unr) <= ar ? (-((unr - ar) * (unr - ar))) / (4.0 * ar) : 0.5 * (unr - fabs(unr));
+    const double pLp = fabs(unl) <= al ? pl * uLp * (2.0 - unl / al) / al : pl * uLp / unl;
+    const double pRm = fabs(unr) <= ar ? pr * uRm * (-2.0 - unr / ar) / ar : pr * uRm / unr;
+    const double phalf = pLp + pRm;
+    F4 F;
+    F.r = uLp * dltot + uRm * drtot;
+    F.u = uLp * (dltot * ul) + uRm * (drtot * ur) + phalf * nx;
+    F.v = uLp * (dltot * vl) + uRm * (drtot * vr) + phalf * ny;
+    F.e = uLp * (dltot * H_L) + uRm * (drtot * H_R);
+    return F;
+}
+
+// riemann_AUSMp (Lib_Riemann_AUSM.f90:73-128).
+static __device__ __noinline__ F4 riemann_ausmp(const Gas& g, const double* L, double al, const double* R, double ar,
+                                         double nx, double ny) {
+    const double betap = 0.125, alpha = 0.1875;
+    const double dltot = L[0], ul = L[1], vl = L[2], pl = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], pr = R[3];
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    const double H_L = H0(g, pl, dltot, sqrt(ul * ul + vl * vl));
+    const double H_R = H0(g, pr, drtot, sqrt(ur * ur + vr * vr));
+    const double a_half = sqrt(al * ar);
+    const double ML = unl / a_half, MR = unr / a_half;
+    double MplusL, pplusL, MminusR, pminusR;
+    if (fabs(ML) < 1.0) {
+        const double q = (ML + 1.0) * (ML + 1.0), w = (ML * ML - 1.0) * (ML * ML - 1.0);
+        MplusL = 0.25 * q + betap * w;
+        pplusL = 0.25 * q * (2.0 - ML) + alpha * ML * w;
+    } else {
+        MplusL = 0.5 * (ML + fabs(ML));
+        pplusL = 0.5 * (1.0 + copysign(1.0, ML));
+    }
+    if (fabs(MR) < 1.0) {
+        const double q = (MR - 1.0) * (MR - 1.0), w = (MR * MR - 1.0) * (MR * MR - 1.0);
+        MminusR = -0.25 * q - betap * w;
+        pminusR = 0.25 * q * (2.0 + MR) - alpha * MR * w;
+    } else {
+        MminusR = 0.5 * (MR - fabs(MR));
+        pminusR = 0.5 * (1.0 - copysign(1.0, MR));
+    }
+    const double Mhalf = MplusL + MminusR;
+    const double phalf = pplusL * pl + pminusR * pr;
+    const double mdotp = dltot * a_half * 0.5 * (Mhalf + fabs(Mhalf));
+    const double mdotm = drtot * a_half * 0.5 * (Mhalf - fabs(Mhalf));
+    F4 F;
+    F.r = mdotp + mdotm;
+    F.u = mdotp * ul + mdotm * ur + nx * phalf;
+    F.v = mdotp * vl + mdotm * vr + ny * phalf;
+    F.e = mdotp * H_L + mdotm * H_R;
+    return F;
+}
+
+// riemann_AUSMp_up / riemann_AUSMp_up2 (Lib_Riemann_AUSM.f90:131-321).
+static __device__ __noinline__ F4 riemann_ausmp_up(const Gas& g, bool up2, const double* L, const double* R, double nx,
+                                            double ny) {
+    const double Kp = 0.25, Ku = 0.75, sigma = 1.0, betap = 0.125;
+    const double dltot = L[0], ul = L[1], vl = L[2], pl = L[3];
+    const double drtot = R[0], ur = R[1], vr = R[2], pr = R[3];
+    const double unl = ul * nx + vl * ny;
+    const double unr = ur * nx + vr * ny;
+    const double H_L = H0(g, pl, dltot, sqrt(ul * ul + vl * vl));
+    const double H_R = H0(g, pr, drtot, sqrt(ur * ur + vr * vr));
+    const double gamma_L = g.gamma, gamma_R = g.gamma;
+    const double astarL2 = 2.0 * (gamma_L - 1.0) / (gamma_L + 1.0) * H_L;
+    const double astarR2 = 2.0 * (gamma_R - 1.0) / (gamma_R + 1.0) * H_R;
+    const double astarL = sqrt(astarL2), astarR = sqrt(astarR2);
+    const double atildeL = astarL2 / dmax(astarL, unl);
+    const double atildeR = astarR2 / dmax(astarR, -unr);
+    const double aF = dmin(atildeL, atildeR);
+    const double mL = unl / aF, mR = unr / aF;
+    const double MFsq = 0.5 * (mL * mL + mR * mR);
+    const double Mrefsq = dmin(1.0, dmax(MFsq, g.minf * g.minf));
+    const double fa = 2.0 * sqrt(Mrefsq) - Mrefsq;
+    const double alpha = 0.1875 * (-4.0 + 5.0 * fa * fa);
+    double mLP, bLP, mRM, bRM;
+    if (fabs(mL) <= 1.0) {
+        const double p1 = 0.25 * ((mL + 1.0) * (mL + 1.0)), p2 = (mL * mL - 1.0) * (mL * mL - 1.0);
+        mLP = p1 + betap * p2;
+        bLP = p1 * (2.0 - mL) + alpha * mL * p2;
+    } else {
+        mLP = 0.5 * (mL + fabs(mL));
+        bLP = mLP / mL;
+    }
+    if (fabs(mR) <= 1.0) {
+        const double p1 = 0.25 * ((mR - 1.0) * (mR - 1.0)), p2 = (mR * mR - 1.0) * (mR * mR - 1.0);
+        mRM = -p1 - betap * p2;
+        bRM = p1 * (2.0 + mR) - alpha * mR * p2;
+    } else {
+        mRM = 0.5 * (mR - fabs(mR));
+        bRM = mRM / mR;
+    }
+    const double rhoF = 0.5 * (dltot + drtot);
+    const double Mp = -(Kp / fa) * dmax(0.0, 1.0 - sigma * MFsq) * (pr - pl) / (rhoF * aF * aF);
+    const double mF = mLP + mRM + Mp;
+    const double mdot = aF * (dmax(mF, 0.0) * dltot + dmin(mF, 0.0) * drtot);
+    double phalf;
+    if (up2) {
+        const double sq_vel = 0.5 * ((ul * ul + vl * vl) + (ur * ur + vr * vr));
+        phalf = 0.5 * (pr + pl) + 0.5 * (bLP - bRM) * (pl - pr) + sqrt(sq_vel) * (bLP + bRM - 1.0) * rhoF * aF;
+    } else {
+        const double Pu = -Ku * fa * bLP * bRM * 2.0 * rhoF * aF * (unr - unl);
+        phalf = bLP * pl + bRM * pr + Pu;
+    }
+    const bool upw = mF >= 0.0;
+    F4 F;
+    F.r = mdot;
+    F.u = mdot * (upw ? ul : ur) + nx * phalf;
+    F.v = mdot * (upw ? vl : vr) + ny * phalf;
+    F.e = mdot * (upw ? H_L : H_R);
+    return F;
+}
+
+constexpr int kRiemGeneric = 7;   // instantiation id of the run-time selected solvers (ids 7-14)
+static __device__ __noinline__ F4 riemann_generic(const Gas& g, const double* L, double al, const double* R, double ar,
+                                           double nx, double ny) {
+    switch (g.rkind) {
+        case 8: return riemann_hllc_rotated(g, L, al, R, ar, nx, ny);
+        case 9: return riemann_pllf(g, L, al, R, ar, nx, ny);
+        case 10: return riemann_exact(g, L, al, R, ar, nx, ny);
+        case 11: return riemann_hanel(g, L, al, R, ar, nx, ny);
+        case 12: return riemann_ausmp(g, L, al, R, ar, nx, ny);
+        case 13: return riemann_ausmp_up(g, false, L, R, nx, ny);
+        case 14: return riemann_ausmp_up(g, true, L, R, nx, ny);
+        default: return riemann_hllem(g, L, al, R, ar, nx, ny);
+    }
+}
+
 // beta: the shock sensor of the face's cell for the sensor-driven solvers (HLLC+ blends HLLC and
 // HLLE by it, riemann_HLLCSD, Lib_Riemann_HLL.f90:572-605; HLLE++); 1 from walls and inflows.
 template <int RIEM>
@@ -541,6 +860,7 @@ __device__ __forceinline__ F4 riemann64(const Gas& g, const double* L, double al
         return F;
     }
     if (RIEM == 6) return riemann_hllepp(g, L, al, R, ar, beta, nx, ny);
+    if (RIEM == kRiemGeneric) return riemann_generic(g, L, al, R, ar, nx, ny);
     if (RIEM == 1) return riemann_hlle(g, L, al, R, ar, nx, ny);
     if (RIEM == 2) return riemann_llf(g, L, al, R, ar, nx, ny);
     if (RIEM == 3) return riemann_slau<false>(g, L, al, R, ar, nx, ny);
@@ -594,6 +914,10 @@ __device__ __forceinline__ float frcp(float x) { return __fdividef(1.0f, x); }
 template <int RIEM>
 __device__ __forceinline__ F4 riemann32(const Gas& g, const FluxState& L, const FluxState& R,
                                         float nx, float ny) {
+    if (RIEM >= 3) {   // no FP32 wave structure of their own here: the FP64 solver on the face states
+        const double ql[4] = {L.r, L.u, L.v, L.p}, qr[4] = {R.r, R.u, R.v, R.p};
+        return riemann64<RIEM>(g, ql, f_ss(g, L.p, L.r), qr, f_ss(g, R.p, R.r), (double)nx, (double)ny);
+    }
     // FP32 wave structure
     const float rl = (float)L.r, rr = (float)R.r;
     const float ul = (float)L.u, vl = (float)L.v, ur = (float)R.u, vr = (float)R.v;

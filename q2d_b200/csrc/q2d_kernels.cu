@@ -199,7 +199,7 @@ cudaError_t launch_finalize(const StageArgs& a, cudaStream_t s) {
     }
 
 cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int grid, cudaStream_t s) {
-    if (a.sd || riem >= 5) return launch_stage_sd(a, prec, riem, tile, grid, s);   // the sensor runs
+    if (a.sd || riem == 5 || riem == 6) return launch_stage_sd(a, prec, riem, tile, grid, s);   // the sensor runs
     cudaError_t e = cudaErrorInvalidValue;
 #define Q2D_CALL(TX, TY, NT)                                                                   \
     if (prec == 0) {                                                                           \
@@ -207,12 +207,14 @@ cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int g
         else if (riem == 2) e = launch_stage_t<0, 2, TX, TY, NT, false>(a, grid, s);                 \
         else if (riem == 3) e = launch_stage_t<0, 3, TX, TY, NT, false>(a, grid, s);                 \
         else if (riem == 4) e = launch_stage_t<0, 4, TX, TY, NT, false>(a, grid, s);                 \
+        else if (riem >= 7) e = launch_stage_t<0, 7, TX, TY, NT, false>(a, grid, s);                 \
         else e = launch_stage_t<0, 0, TX, TY, NT, false>(a, grid, s);                                \
     } else {                                                                                   \
         if (riem == 1) e = launch_stage_t<1, 1, TX, TY, NT, false>(a, grid, s);                      \
         else if (riem == 2) e = launch_stage_t<1, 2, TX, TY, NT, false>(a, grid, s);                 \
         else if (riem == 3) e = launch_stage_t<1, 3, TX, TY, NT, false>(a, grid, s);                 \
         else if (riem == 4) e = launch_stage_t<1, 4, TX, TY, NT, false>(a, grid, s);                 \
+        else if (riem >= 7) e = launch_stage_t<1, 7, TX, TY, NT, false>(a, grid, s);                 \
         else e = launch_stage_t<1, 0, TX, TY, NT, false>(a, grid, s);                                \
     }
     Q2D_TILE_SWITCH(tile, Q2D_CALL)
@@ -221,7 +223,7 @@ cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int g
 }
 
 int stage_occupancy(int prec, int riem, int tile, int sd) {
-    if (sd || riem >= 5) return stage_occupancy_sd(prec, riem, tile);
+    if (sd || riem == 5 || riem == 6) return stage_occupancy_sd(prec, riem, tile);
     int n = 0;
 #define Q2D_CALL(TX, TY, NT)                                                                   \
     if (prec == 0) {                                                                           \
@@ -229,12 +231,14 @@ int stage_occupancy(int prec, int riem, int tile, int sd) {
         else if (riem == 2) n = occupancy_t<0, 2, TX, TY, NT, false>();                 \
         else if (riem == 3) n = occupancy_t<0, 3, TX, TY, NT, false>();                 \
         else if (riem == 4) n = occupancy_t<0, 4, TX, TY, NT, false>();                              \
+        else if (riem >= 7) n = occupancy_t<0, 7, TX, TY, NT, false>();                              \
         else n = occupancy_t<0, 0, TX, TY, NT, false>();                                             \
     } else {                                                                                   \
         if (riem == 1) n = occupancy_t<1, 1, TX, TY, NT, false>();                                   \
         else if (riem == 2) n = occupancy_t<1, 2, TX, TY, NT, false>();                 \
         else if (riem == 3) n = occupancy_t<1, 3, TX, TY, NT, false>();                 \
         else if (riem == 4) n = occupancy_t<1, 4, TX, TY, NT, false>();                              \
+        else if (riem >= 7) n = occupancy_t<1, 7, TX, TY, NT, false>();                              \
         else n = occupancy_t<1, 0, TX, TY, NT, false>();                                             \
     }
     Q2D_TILE_SWITCH(tile, Q2D_CALL)
@@ -356,6 +360,7 @@ cudaError_t launch_stage32_r3(const StageArgs& a, int tile, int grid, cudaStream
 cudaError_t launch_stage32_r4(const StageArgs& a, int tile, int grid, cudaStream_t s);
 cudaError_t launch_stage32_r5(const StageArgs& a, int tile, int grid, cudaStream_t s);
 cudaError_t launch_stage32_r6(const StageArgs& a, int tile, int grid, cudaStream_t s);
+cudaError_t launch_stage32_r7(const StageArgs& a, int tile, int grid, cudaStream_t s);
 int stage32_occupancy_r0(int tile);
 int stage32_occupancy_r1(int tile);
 int stage32_occupancy_r2(int tile);
@@ -363,6 +368,7 @@ int stage32_occupancy_r3(int tile);
 int stage32_occupancy_r4(int tile);
 int stage32_occupancy_r5(int tile);
 int stage32_occupancy_r6(int tile);
+int stage32_occupancy_r7(int tile);
 
 cudaError_t launch_stage32(const StageArgs& a, int riem, int tile, int grid, cudaStream_t s) {
     if (riem == 1) return launch_stage32_r1(a, tile, grid, s);
@@ -371,6 +377,7 @@ cudaError_t launch_stage32(const StageArgs& a, int riem, int tile, int grid, cud
     if (riem == 4) return launch_stage32_r4(a, tile, grid, s);
     if (riem == 5) return launch_stage32_r5(a, tile, grid, s);
     if (riem == 6) return launch_stage32_r6(a, tile, grid, s);
+    if (riem >= 7) return launch_stage32_r7(a, tile, grid, s);   // the run-time selected solvers
     return launch_stage32_r0(a, tile, grid, s);
 }
 
@@ -381,6 +388,7 @@ int stage32_occupancy(int riem, int tile) {
     if (riem == 4) return stage32_occupancy_r4(tile);
     if (riem == 5) return stage32_occupancy_r5(tile);
     if (riem == 6) return stage32_occupancy_r6(tile);
+    if (riem >= 7) return stage32_occupancy_r7(tile);
     return stage32_occupancy_r0(tile);
 }
 

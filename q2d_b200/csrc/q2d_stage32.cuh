@@ -91,7 +91,14 @@ __device__ __forceinline__ FS32 phys32(float r, float u, float v, float p, float
 // beta: the shock sensor the sensor-driven solvers blend by (HLLC+, HLLE++).
 template <int RIEM>
 __device__ __forceinline__ void riemann_f32(const FS32& L, const FS32& R, float nx, float ny, float gam,
-                                            float gm1, float gf, float* F, float beta = 1.0f) {
+                                            float gm1, float gf, float* F, float beta = 1.0f,
+                                            const Gas* gp = nullptr) {
+    if (RIEM == kRiemGeneric) {   // the run-time selected solvers: FP64 on the FP32 face states
+        const double ql[4] = {L.r, L.u, L.v, L.p}, qr[4] = {R.r, R.u, R.v, R.p};
+        const F4 X = riemann_generic(*gp, ql, f_ss(*gp, ql[3], ql[0]), qr, f_ss(*gp, qr[3], qr[0]), nx, ny);
+        F[0] = (float)X.r; F[1] = (float)X.u; F[2] = (float)X.v; F[3] = (float)X.e;
+        return;
+    }
     if (RIEM == 5) {   // HLLC+ (riemann_HLLCSD, Lib_Riemann_HLL.f90:572-605)
         if (beta == 0.0f) { riemann_f32<1>(L, R, nx, ny, gam, gm1, gf, F); return; }
         if (beta >= 1.0f) { riemann_f32<0>(L, R, nx, ny, gam, gm1, gf, F); return; }
@@ -223,7 +230,7 @@ __device__ __forceinline__ void riemann_f32(const FS32& L, const FS32& R, float 
 template <int RIEM, int LIM>
 __device__ __forceinline__ bool face32(const float4* sP, const float* dlp, int base, int step, float nx,
                                       float ny, float len, float gam, float gm1, float gf, float beta_l,
-                                      float beta_r, float* out) {
+                                      float beta_r, float* out, const Gas& g) {
     const float dm = dlp[2 * base], d0 = dlp[2 * (base + step)], d1 = dlp[2 * (base + 2 * step)],
                 d2 = dlp[2 * (base + 3 * step)];
     const float il0 = rcp_approx(0.5f * (dm + d0));
@@ -243,7 +250,7 @@ __device__ __forceinline__ bool face32(const float4* sP, const float* dlp, int b
     const FS32 L = phys32(QL[0], QL[1], QL[2], QL[3], nx, ny, gf);
     const FS32 R = phys32(QR[0], QR[1], QR[2], QR[3], nx, ny, gf);
     float F[4];
-    riemann_f32<RIEM>(L, R, nx, ny, gam, gm1, gf, F, beta_r);
+    riemann_f32<RIEM>(L, R, nx, ny, gam, gm1, gf, F, beta_r, &g);
 #pragma unroll
     for (int v = 0; v < 4; ++v) out[v] = F[v] * len;
     return ok;
@@ -286,7 +293,7 @@ __device__ __forceinline__ void interior_faces32(const StageArgs& a, const DBloc
         const float4 gq = sG[f];
         const float beta = SD ? sd_cell32<W>(sP, base + step) : 1.0f;
         const bool ok = face32<RIEM, LIM>(sP, dlp, base, step, gq.x, gq.y, gq.z, gam, gm1, gf, a.sd ? beta : 1.0f,
-                                          beta, out);
+                                          beta, out, a.gas);
         if (!ok) record_error(cs, 4, B.local_b, ii, jj, a.irk);
         sF[f] = make_float4(out[0], out[1], out[2], out[3]);
     }
@@ -295,15 +302,15 @@ __device__ __forceinline__ void interior_faces32(const StageArgs& a, const DBloc
 template <int RIEM>
 __device__ __forceinline__ bool face32_lim(int lim, const float4* sP, const float* dlp, int base, int step,
                                           float nx, float ny, float len, float gam, float gm1, float gf,
-                                          float beta_l, float beta_r, float* out) {
+                                          float beta_l, float beta_r, float* out, const Gas& g) {
     switch (lim) {
-        case 0: return face32<RIEM, 0>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
-        case 1: return face32<RIEM, 1>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
-        case 2: return face32<RIEM, 2>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
-        case 3: return face32<RIEM, 3>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
-        case 4: return face32<RIEM, 4>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
-        case 5: return face32<RIEM, 5>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
-        default: return face32<RIEM, 6>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out);
+        case 0: return face32<RIEM, 0>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out, g);
+        case 1: return face32<RIEM, 1>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out, g);
+        case 2: return face32<RIEM, 2>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out, g);
+        case 3: return face32<RIEM, 3>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out, g);
+        case 4: return face32<RIEM, 4>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out, g);
+        case 5: return face32<RIEM, 5>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out, g);
+        default: return face32<RIEM, 6>(sP, dlp, base, step, nx, ny, len, gam, gm1, gf, beta_l, beta_r, out, g);
     }
 }
 
@@ -313,7 +320,7 @@ __device__ __forceinline__ bool face32_lim(int lim, const float4* sP, const floa
 template <int RIEM, int LIM>
 __device__ __forceinline__ void bc_symmetry32(int Fm, const float* B, const float* I, float dlb, float dli,
                                               float nx, float ny, float len, float gam, float gm1, float gf,
-                                              float* out) {
+                                              float* out, const Gas& g) {
     const bool minside = (Fm & 1) != 0;   // faces 1 and 3
     const float bd = 0.5f * dlb, id = 0.5f * dli;
     const float un = B[1] * nx + B[2] * ny;
@@ -333,7 +340,7 @@ __device__ __forceinline__ void bc_symmetry32(int Fm, const float* B, const floa
     const FS32 L = phys32(Fc[0], Un1 * nx + vtx, Un1 * ny + vty, Fc[3], nx, ny, gf);
     const FS32 R = phys32(Fc[0], -Un1 * nx + vtx, -Un1 * ny + vty, Fc[3], nx, ny, gf);
     float F[4];
-    riemann_f32<RIEM>(L, R, nx, ny, gam, gm1, gf, F);
+    riemann_f32<RIEM>(L, R, nx, ny, gam, gm1, gf, F, 1.0f, &g);
     out[0] = 0.0f;
     out[1] = F[1] * len;
     out[2] = F[2] * len;
@@ -400,15 +407,15 @@ __device__ __forceinline__ int bc_stagnation32(int Fm, const float* B, float n0,
 template <int RIEM>
 __device__ __forceinline__ void bc_symmetry32_lim(int lim, int Fm, const float* B, const float* I, float dlb,
                                                   float dli, float nx, float ny, float len, float gam,
-                                                  float gm1, float gf, float* out) {
+                                                  float gm1, float gf, float* out, const Gas& g) {
     switch (lim) {
-        case 0: bc_symmetry32<RIEM, 0>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
-        case 1: bc_symmetry32<RIEM, 1>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
-        case 2: bc_symmetry32<RIEM, 2>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
-        case 3: bc_symmetry32<RIEM, 3>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
-        case 4: bc_symmetry32<RIEM, 4>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
-        case 5: bc_symmetry32<RIEM, 5>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
-        default: bc_symmetry32<RIEM, 6>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out); break;
+        case 0: bc_symmetry32<RIEM, 0>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out, g); break;
+        case 1: bc_symmetry32<RIEM, 1>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out, g); break;
+        case 2: bc_symmetry32<RIEM, 2>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out, g); break;
+        case 3: bc_symmetry32<RIEM, 3>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out, g); break;
+        case 4: bc_symmetry32<RIEM, 4>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out, g); break;
+        case 5: bc_symmetry32<RIEM, 5>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out, g); break;
+        default: bc_symmetry32<RIEM, 6>(Fm, B, I, dlb, dli, nx, ny, len, gam, gm1, gf, out, g); break;
     }
 }
 
@@ -750,14 +757,14 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                         // the sensor of the boundary cell (beta_ = blk%beta(Im,Jm))
                         const float beta = SD ? sd_cell32<W>(sP, cb) : 1.0f;
                         const bool ok = face32_lim<RIEM>(a.limiter, sP, dlp, base, step, nx, ny, ln, gam, gm1, gf,
-                                                         a.sd ? beta : 1.0f, beta, X);
+                                                         a.sd ? beta : 1.0f, beta, X, g);
                         if (!ok) record_error(cs, 4, B.local_b, bi + 1, bj + 1, a.irk);
                     } else if (e.type == 300 || e.type == 400) {
                         const float4 Bc = sP[cb], Ic = sP[ci];
                         const float Bq[4] = {Bc.x, Bc.y, Bc.z, Bc.w}, Iq[4] = {Ic.x, Ic.y, Ic.z, Ic.w};
                         if (e.type == 300)
                             bc_symmetry32_lim<RIEM>(a.limiter, Fm, Bq, Iq, dlp[2 * cb], dlp[2 * ci], nx, ny, ln, gam, gm1,
-                                                    gf, X);
+                                                    gf, X, g);
                         else
                             bc_extrapolation32(Bq, nx, ny, ln, gf, X);
                     } else if (e.type > 0) {   // inflow / outflow records
@@ -768,7 +775,7 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                             path = bc_stagnation32(Fm, Bq, nx, ny, ln, gam, (float)g.R, a.bcp[e.param], X);
                             if (path == 1) {
                                 bc_symmetry32_lim<RIEM>(a.limiter, Fm, Bq, Iq, dlp[2 * cb], dlp[2 * ci], nx, ny, ln, gam,
-                                                        gm1, gf, X);
+                                                        gm1, gf, X, g);
                                 path = 0;
                             }
                         }
@@ -969,7 +976,7 @@ cudaError_t launch_stage32_sd(const StageArgs& a, int grid, cudaStream_t s) {
 // The sensor-driven Riemann solvers (HLLC+, HLLE++) run the sensor whatever the reconstruction.
 template <int RIEM, int TX, int TY, int NT, int MB>
 cudaError_t launch_stage32_t(const StageArgs& a, int grid, cudaStream_t s) {
-    if constexpr (RIEM >= 5) {
+    if constexpr (RIEM == 5 || RIEM == 6) {
         return launch_stage32_sd<RIEM, TX, TY, NT, MB, true>(a, grid, s);
     } else {
         return a.sd ? launch_stage32_sd<RIEM, TX, TY, NT, MB, true>(a, grid, s)
@@ -980,7 +987,7 @@ cudaError_t launch_stage32_t(const StageArgs& a, int grid, cudaStream_t s) {
 template <int RIEM, int TX, int TY, int NT, int MB>
 int stage32_occupancy_t() {
     constexpr size_t smem = Tile32<TX, TY>::bytes;
-    auto k = stage32_kernel<RIEM, TX, TY, NT, MB, (RIEM >= 5)>;
+    auto k = stage32_kernel<RIEM, TX, TY, NT, MB, (RIEM == 5 || RIEM == 6)>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, NT, smem);

@@ -17,7 +17,8 @@ cudaError_t launch_stage_sd(const StageArgs& a, int prec, int riem, int tile, in
         case 4: e = launch_stage_t<0, 4, TX, TY, NT, true>(a, grid, s); break; \
         case 5: e = launch_stage_t<0, 5, TX, TY, NT, true>(a, grid, s); break; \
         case 6: e = launch_stage_t<0, 6, TX, TY, NT, true>(a, grid, s); break; \
-        default: e = launch_stage_t<0, 0, TX, TY, NT, true>(a, grid, s); break; \
+        case 0: e = launch_stage_t<0, 0, TX, TY, NT, true>(a, grid, s); break; \
+        default: e = launch_stage_t<0, 7, TX, TY, NT, true>(a, grid, s); break; \
     }
     switch (tile) {
         case 1: Q2D_CALL(32, 8, 256); break;
@@ -39,7 +40,8 @@ int stage_occupancy_sd(int prec, int riem, int tile) {
         case 4: n = occupancy_t<0, 4, TX, TY, NT, true>(); break;   \
         case 5: n = occupancy_t<0, 5, TX, TY, NT, true>(); break;   \
         case 6: n = occupancy_t<0, 6, TX, TY, NT, true>(); break;   \
-        default: n = occupancy_t<0, 0, TX, TY, NT, true>(); break;  \
+        case 0: n = occupancy_t<0, 0, TX, TY, NT, true>(); break;   \
+        default: n = occupancy_t<0, 7, TX, TY, NT, true>(); break;  \
     }
     switch (tile) {
         case 1: Q2D_CALL(32, 8, 256); break;

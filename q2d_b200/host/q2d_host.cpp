@@ -177,7 +177,21 @@ Setup read_options(const Ini& ini) {
     else if (s.riemann_name == "SLAU2") o.riemann = Q2D_RIEMANN_SLAU2;
     else if (s.riemann_name == "HLLC+") o.riemann = Q2D_RIEMANN_HLLCP;
     else if (s.riemann_name == "HLLE++") o.riemann = Q2D_RIEMANN_HLLEPP;
-    else s.unsupported.push_back("[Q2D-Numerics] riemann-solver = " + s.riemann_name);
+    else if (s.riemann_name == "HLLEM") o.riemann = Q2D_RIEMANN_HLLEM;
+    else if (s.riemann_name == "HLLC Rotated") o.riemann = Q2D_RIEMANN_HLLC_ROTATED;
+    else if (s.riemann_name == "PLLF") o.riemann = Q2D_RIEMANN_PLLF;
+    else if (s.riemann_name == "exact" || s.riemann_name == "Exact") o.riemann = Q2D_RIEMANN_EXACT;
+    else if (s.riemann_name == "Hanel") o.riemann = Q2D_RIEMANN_HANEL;
+    else if (s.riemann_name == "AUSM+") o.riemann = Q2D_RIEMANN_AUSMP;
+    else if (s.riemann_name == "AUSM+-up") o.riemann = Q2D_RIEMANN_AUSMP_UP;
+    else if (s.riemann_name == "AUSM+-up2") o.riemann = Q2D_RIEMANN_AUSMP_UP2;
+    else o.riemann = Q2D_RIEMANN_HLLC;   // case default (:101-104)
+    if (const std::string* v = ini_get(ini, "Numerics", "riemann-options-Minf")) {
+        o.riemann_minf = to_double(*v, "riemann-options-Minf");
+        if (o.riemann_minf < 0.0) die("riemann-options-Minf must be >= 0");
+    }
+    if ((o.riemann == Q2D_RIEMANN_AUSMP_UP || o.riemann == Q2D_RIEMANN_AUSMP_UP2) && !(o.riemann_minf > 0.0))
+        die("AUSM+-up solver selected. Minf must be defined in input (riemann-options-Minf)");
     if (const std::string* v = ini_get(ini, "Parameters", "res-threshold")) o.res_threshold = to_double(*v, "res-threshold");
     if (const std::string* v = ini_get(ini, "Parameters", "time-threshold")) o.time_threshold = to_double(*v, "time-threshold");
     if (const std::string* v = ini_get(ini, "Parameters", "iter-threshold")) o.itermax = to_int(*v, "iter-threshold");
@@ -563,10 +577,10 @@ int run(int argc, char** argv) {
                         "\"precision\": %d, \"rampa_iter\": %d, \"res_diter\": %d, \"sol_diter\": %d, "
                         "\"itermax\": %lld, \"cfl\": %.17g, \"res_threshold\": %.17g, \"time_threshold\": %.17g, "
                         "\"sol_dtime\": %.17g, \"gas_R\": %.17g, \"gas_gamma\": %.17g, \"shell_diter\": %d, "
-                        "\"irs_beta\": %.17g, \"shock_detector\": %d,\n",
+                        "\"irs_beta\": %.17g, \"shock_detector\": %d, \"riemann_minf\": %.17g,\n",
                      o.limiter, o.riemann, o.n_rk, o.time_accurate, o.source, o.precision, o.rampa_iter, o.res_diter,
                      o.sol_diter, o.itermax, o.cfl, o.res_threshold, o.time_threshold, o.sol_dtime, o.gas_R,
-                     o.gas_gamma, S.shell_diter, o.irs_beta, o.shock_detector);
+                     o.gas_gamma, S.shell_diter, o.irs_beta, o.shock_detector, o.riemann_minf);
         std::fprintf(f, " \"blocks\": [");
         for (size_t b = 0; b < blocks.size(); ++b) {
             double s = 0.0, sa = 0.0;

@@ -29,7 +29,9 @@ from .cases import BlockSpec, CaseSpec
 RUNIV = 8314.46   # docs/theory/thermo.md:56
 
 _LIM_NAMES = {1: "minmod", 2: "vanleer", 3: "vanalbada", 4: "mc", 5: "superbee", 6: "LIMO3"}
-_RIEMANN_NAMES = {0: "HLLC", 1: "HLLE", 2: "LLF", 3: "SLAU", 4: "SLAU2", 5: "HLLC+", 6: "HLLE++"}
+_RIEMANN_NAMES = {0: "HLLC", 1: "HLLE", 2: "LLF", 3: "SLAU", 4: "SLAU2", 5: "HLLC+", 6: "HLLE++", 7: "HLLEM",
+                  8: "HLLC Rotated", 9: "PLLF", 10: "exact", 11: "Hanel", 12: "AUSM+", 13: "AUSM+-up",
+                  14: "AUSM+-up2"}
 _SCHEME_NAMES = {1: "euler", 2: "RK2", 3: "RK3"}
 _SOURCE_NAMES = {0: "none", 1: "axisymmetric", 2: "area_variation"}
 
@@ -56,6 +58,8 @@ def _ini(o: _abi.Options) -> str:
     else:
         recon = "MUSCL-SD" if o.shock_detector else "MUSCL"
         lines += [f"space-reconstruction = {recon}", f"flux-limiter = {_LIM_NAMES[o.limiter]}"]
+    if o.riemann_minf > 0.0:
+        lines.append(f"riemann-options-Minf = {o.riemann_minf!r}")
     lines += [f"riemann-solver = {_RIEMANN_NAMES[o.riemann]}",
               "", "[Q2D-IO]",
               f"res-diter = {o.res_diter}",

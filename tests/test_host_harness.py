@@ -18,7 +18,7 @@ from q2d_b200.solver import Q2DSolver
 GOLD = Path(__file__).resolve().parent / "golden"
 OPT_FIELDS = ["limiter", "riemann", "n_rk", "time_accurate", "source", "rampa_iter", "res_diter",
               "sol_diter", "itermax", "cfl", "res_threshold", "time_threshold", "sol_dtime", "gas_R", "irs_beta",
-              "shock_detector"]
+              "shock_detector", "riemann_minf"]
 
 
 def host(*args, check=True):
@@ -100,17 +100,26 @@ def test_inputs_outside_the_path_fail_loudly(tmp_path):
     cs = cases.ramp(20, 8)
     refio.write_case(cs, tmp_path)
     ini = (tmp_path / "input.ini").read_text()
-    (tmp_path / "input.ini").write_text(ini.replace("riemann-solver = HLLC", "riemann-solver = AUSM+"))
+    (tmp_path / "input.ini").write_text(ini.replace("integration-variables = cons", "integration-variables = prim"))
     d = json.loads(host(tmp_path, "--check").stdout)
-    assert d["unsupported"] == ["[Q2D-Numerics] riemann-solver = AUSM+"]
+    assert d["unsupported"] == ["[Q2D-Numerics] integration-variables = prim"]
     r = host(tmp_path, check=False)   # refused before any device call
     assert r.returncode == 2 and "not on the built path" in r.stderr
     # Assign_Riemann_Solver keywords (Mod_Riemann.f90:25-109) of the built solvers
     for name, want in [("HLLC", 0), ("HLLE", 1), ("LLF", 2), ("Rusanov", 2), ("SLAU", 3), ("SLAU2", 4),
-                       ("HLLC+", 5), ("HLLE++", 6)]:
+                       ("HLLC+", 5), ("HLLE++", 6), ("HLLEM", 7), ("HLLC Rotated", 8), ("PLLF", 9), ("exact", 10),
+                       ("Exact", 10), ("Hanel", 11), ("AUSM+", 12), ("Roe", 0), ("hllc", 0)]:   # default: HLLC
         (tmp_path / "input.ini").write_text(ini.replace("riemann-solver = HLLC", f"riemann-solver = {name}"))
         d = json.loads(host(tmp_path, "--check").stdout)
         assert d["riemann"] == want and not d["unsupported"], (name, d["unsupported"])
+    for name, want in [("AUSM+-up", 13), ("AUSM+-up2", 14)]:   # Minf required (Assign_Setup.f90:108-112)
+        text = ini.replace("riemann-solver = HLLC", f"riemann-solver = {name}")
+        (tmp_path / "input.ini").write_text(text)
+        r = host(tmp_path, "--check", check=False)
+        assert r.returncode != 0 and "Minf" in r.stderr
+        (tmp_path / "input.ini").write_text(text.replace("[Q2D-Numerics]\n", "[Q2D-Numerics]\nriemann-options-Minf = 0.3\n"))
+        d = json.loads(host(tmp_path, "--check").stdout)
+        assert d["riemann"] == want and d["riemann_minf"] == 0.3 and not d["unsupported"]
     (tmp_path / "input.ini").write_text(ini)
     bc = (tmp_path / "INPUT" / "bc.txt").read_text().splitlines()
     bc[0] = bc[0][:-8] + f"{410:8d}"

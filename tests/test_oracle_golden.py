@@ -345,3 +345,63 @@ def test_ramp_channel_sensor_driven_solvers(riem):
         s.close()
     assert info["err"] == 0 and info["residual"][0] < 1e-3, info
     ramp_channel_gates(cs, prim, sensor_field(cs, [prim])[0])
+
+
+REMAINING = ["HLLEM", "HLLC Rotated", "PLLF", "exact", "Hanel", "AUSM+", "AUSM+-up", "AUSM+-up2"]
+
+
+def riemann_kw(kind, L, R, nx=1.0, ny=0.0, minf=0.1):
+    import ctypes as C
+    lib = oracle.load()
+    opt = make_options({}, riemann_minf=minf)
+    a = (C.c_double * 4)(*L)
+    b = (C.c_double * 4)(*R)
+    out = (C.c_double * 4)()
+    lib.q2d_oracle_riemann_sd(kind, C.byref(opt), a, b, 1.0, nx, ny, out)
+    return np.array(out[:])
+
+
+def test_remaining_riemann_known_answers():
+    """The rest of Assign_Riemann_Solver's solvers (HLLEM, rotated HLLC, PLLF, exact, Hanel,
+    AUSM+, AUSM+-up, AUSM+-up2): consistent (F(U, U) is the physical flux) in any direction;
+    the exact solver keeps a stationary contact (no mass flux), and HLLEM's antidiffusion removes
+    most of the mass flux HLLE puts across it (its weight a / (a + |S1 + S4| / 2) stays below 1
+    when the wave speeds are not symmetric); the exact solver's Godunov flux for Sod (rho
+    1/0.125, p 1/0.1, at rest; the left fan's tail u* - a*_L < 0, so x/t = 0 is in the left star
+    region) is the flux of the left star state, p* and u* from the reference's own exact solver
+    (test/common/pycheck/q2d_exact1d.py, riemann_exact.npz), rho*_L = rho_L (p* / p_L)^(1 /
+    gamma)."""
+    rng = np.random.default_rng(23)
+    for kind in range(7, 15):
+        for _ in range(20):
+            P = [rng.uniform(0.2, 3), rng.uniform(-2, 2), rng.uniform(-2, 2), rng.uniform(0.2, 5)]
+            th = rng.uniform(0, 2 * np.pi)
+            n = (np.cos(th), np.sin(th))
+            F = riemann_kw(kind, P, P, *n)
+            assert np.allclose(F, phys_flux(P, *n), rtol=1e-10, atol=1e-10), (kind, F, phys_flux(P, *n))
+    L, R = [1.0, 0.0, 0.3, 1.0], [0.25, 0.0, 0.3, 1.0]
+    assert abs(riemann_kw(10, L, R)[0]) < 1e-15
+    hlle, hllem = riemann(1, L, R)[0], riemann_kw(7, L, R)[0]
+    assert 0.0 < hllem < 0.5 * hlle, (hllem, hlle)   # antidiffusion weight a / (a + |S1 + S4| / 2) < 1
+    ps, us = np.load(GOLD / "riemann_exact.npz")["toro1_pstar_ustar"]
+    F = riemann_kw(10, [1.0, 0.0, 0.0, 1.0], [0.125, 0.0, 0.0, 0.1])
+    assert np.allclose(F, phys_flux([ps ** (1.0 / 1.4), us, 0.0, ps], 1.0, 0.0), rtol=1e-6, atol=0), F
+
+
+@pytest.mark.parametrize("riem", REMAINING)
+def test_sod79_remaining_solvers(riem):
+    """Sod at 400 cells with MC and each remaining solver (CFL 0.5; 0.2 for AUSM+-up and
+    AUSM+-up2, Minf 0.1) meets the Sod79 check.py error gates (relative L1 of rho < 5e-3, of
+    p < 3.5e-3) against the reference's exact.txt."""
+    kw = dict(cfl=0.2, riemann_minf=0.1) if "up" in riem else dict(cfl=0.5)
+    P, info = run_oracle(sod79(riem), riemann=riem, **kw)
+    l1r, l1p = sod79_l1(P)
+    assert info["todo"] == 3 and l1r < 5e-3 and l1p < 3.5e-3, (l1r, l1p)
+
+
+def test_ausm_up_needs_minf():
+    """AUSM+-up / AUSM+-up2 without riemann-options-Minf are refused (Assign_Setup.f90:108-112)."""
+    cs = sod79("AUSM+-up")
+    for riem in ("AUSM+-up", "AUSM+-up2"):
+        with pytest.raises(Exception):
+            oracle.solver(make_options(cs, riemann=riem), [cs])
