@@ -184,6 +184,10 @@ int  q2d_gpu_set_bcs(q2d_ctx* ctx, int case_id, const q2d_bc_rec* recs, int n);
 
 /* Copies the interior of a block's primitive state host->device (Read_IC result). */
 int  q2d_gpu_upload_prim(q2d_ctx* ctx, int block_id, const double* P);
+/* Restart (newrun = false; Wrap_Setup.f90:132-149, Read_IC IO_Solution.f90:38-126): the physical
+ * time a time-accurate case resumes from (SOLUTIONTIME of the restart field); the step and
+ * iteration counters restart at 0 as in the reference. Before q2d_gpu_commit. */
+int  q2d_gpu_set_case_time(q2d_ctx* ctx, int case_id, double time);
 
 /* Builds metrics (Setup_Metrics, Mod_Metrics.f90:11-148) and the device work lists.
  * Called implicitly by the first q2d_gpu_step(). */

@@ -1955,6 +1955,13 @@ int q2d_oracle_upload_prim(q2d_oracle* o, int block_id, const double* P) {
     return Q2D_OK;
 }
 
+int q2d_oracle_set_case_time(q2d_oracle* o, int case_id, double time) {
+    if (!o || o->committed || case_id < 0 || case_id >= (int)o->cases.size() || !std::isfinite(time))
+        return Q2D_ERR_BADARG;
+    o->cases[case_id].time = time;   // Wrap_Setup.f90:141-144: time = solutiontime, counters at 0
+    return Q2D_OK;
+}
+
 int q2d_oracle_download_prim(q2d_oracle* o, int block_id, double* P) {
     if (!o || block_id < 0 || block_id >= (int)o->blk.size() || !P) return Q2D_ERR_BADARG;
     Block& B = o->blk[block_id];

@@ -1009,6 +1009,14 @@ int q2d_gpu_add_case(q2d_ctx* ctx, int* case_id) {
     return Q2D_OK;
 }
 
+int q2d_gpu_set_case_time(q2d_ctx* ctx, int case_id, double time) {
+    if (!ctx || ctx->committed || ctx->serving || case_id < 0 || case_id >= (int)ctx->cases.size() ||
+        !std::isfinite(time))
+        return fail(ctx, Q2D_ERR_BADARG, "set_case_time: bad argument or after commit");
+    ctx->cases[case_id].time0 = time;
+    return Q2D_OK;
+}
+
 int q2d_gpu_add_block(q2d_ctx* ctx, int case_id, int ni, int nj, const double* nodes_xy,
                       const double* cross_section, int* block_id) {
     if (!ctx || ctx->committed || ctx->serving || case_id < 0 || case_id >= (int)ctx->cases.size() ||

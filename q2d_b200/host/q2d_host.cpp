@@ -115,6 +115,7 @@ struct Setup {
     std::vector<std::string> unsupported;   // keys or values outside the built path
     int shell_diter = 1;
     bool area = false;
+    bool newrun = true;   // newrun = false: restart from OUTPUT/field.tec (Register_Sim_Param.f90:26)
     std::string limiter_name, riemann_name, scheme_name, source_name;
 };
 
@@ -195,8 +196,7 @@ Setup read_options(const Ini& ini) {
     if (const std::string* v = ini_get(ini, "Parameters", "res-threshold")) o.res_threshold = to_double(*v, "res-threshold");
     if (const std::string* v = ini_get(ini, "Parameters", "time-threshold")) o.time_threshold = to_double(*v, "time-threshold");
     if (const std::string* v = ini_get(ini, "Parameters", "iter-threshold")) o.itermax = to_int(*v, "iter-threshold");
-    if (const std::string* v = ini_get(ini, "Parameters", "newrun"))
-        if (!to_bool(*v, "newrun")) s.unsupported.push_back("[Q2D-Parameters] newrun = " + *v);
+    if (const std::string* v = ini_get(ini, "Parameters", "newrun")) s.newrun = to_bool(*v, "newrun");
     if (const std::string* v = ini_get(ini, "IO", "res-diter")) o.res_diter = (int)to_int(*v, "res-diter");
     if (const std::string* v = ini_get(ini, "IO", "sol-diter")) o.sol_diter = (int)std::min<long long>(to_int(*v, "sol-diter"), 1000000000);
     if (const std::string* v = ini_get(ini, "IO", "sol-dtime")) o.sol_dtime = to_double(*v, "sol-dtime");
@@ -491,6 +491,42 @@ std::vector<double> ghosted(const Block& B) {
     return P;
 }
 
+// The restart field of newrun = false (Read_IC, IO_Solution.f90:78-96): OUTPUT/field.tec, else
+// the last of OUTPUT/field1.tec, field2.tec, ... that exists.
+std::string restart_field(const std::string& dir) {
+    const std::string base = dir + "/OUTPUT/field";
+    if (std::ifstream(base + ".tec")) return base + ".tec";
+    std::string found;
+    for (int i = 1;; ++i) {
+        const std::string t = base + std::to_string(i) + ".tec";
+        if (!std::ifstream(t)) break;
+        found = t;
+    }
+    if (found.empty()) die("[ERROR] reading input file " + base + ".tec");
+    return found;
+}
+
+// Fortran Ew.d edit descriptor (w = 20, d = 10): 0.dddddddddd E+xx, right-justified.
+std::string fortran_e20_10(double v) {
+    char buf[64];
+    if (v == 0.0) {
+        std::snprintf(buf, sizeof buf, "%20s", "0.0000000000E+00");
+        return buf;
+    }
+    char m[32];
+    std::snprintf(m, sizeof m, "%.9E", v);   // [-]d.dddddddddE[+-]xx: the 10 significant digits
+    const bool neg = m[0] == '-';
+    const char* p = m + (neg ? 1 : 0);
+    std::string digits;
+    digits += p[0];
+    digits.append(p + 2, 9);
+    const int e = std::atoi(std::strchr(p, 'E') + 1) + 1;
+    char out[40];
+    std::snprintf(out, sizeof out, "%s0.%sE%c%02d", neg ? "-" : "", digits.c_str(), e < 0 ? '-' : '+', e < 0 ? -e : e);
+    std::snprintf(buf, sizeof buf, "%20s", out);
+    return buf;
+}
+
 void write_tec(const std::string& path, const std::vector<Block>& blocks, const std::vector<std::vector<double>>& P,
                double time) {
     FILE* f = std::fopen(path.c_str(), "w");
@@ -499,7 +535,7 @@ void write_tec(const std::string& path, const std::vector<Block>& blocks, const 
     for (size_t b = 0; b < blocks.size(); ++b) {
         const Block& B = blocks[b];
         std::fprintf(f, " ZONE  T = B%zu, I=%d, J=%d, K=1, DATAPACKING=BLOCK, "
-                        "VARLOCATION=([1-2]=NODAL,[3-6]=CELLCENTERED), SOLUTIONTIME=%.15E\n",
+                        "VARLOCATION=([1-2]=NODAL,[3-6]=CELLCENTERED), SOLUTIONTIME=%.17E\n",
                      b + 1, B.ni + 1, B.nj + 1, time);
         const size_t nn = (size_t)(B.ni + 1) * (B.nj + 1);
         for (int c = 0; c < 2; ++c)
@@ -562,13 +598,18 @@ int run(int argc, char** argv) {
     S.opt.precision = A.precision == "fp64" ? Q2D_PREC_FP64 : Q2D_PREC_FP32_FLUX;
     std::string gas_note;
     read_gas(A.dir, A.gamma, S.opt, gas_note);
+    // newrun: INPUT/ic.tec, its SOLUTIONTIME ignored; restart: the last field written, time-accurate
+    // cases resume at its SOLUTIONTIME, steady ones count iterations from int(SOLUTIONTIME)
+    // (Wrap_Setup.f90:132-149; the writer stores -iterations there, Wrap_Postprocess.f90:41-47)
+    const std::string icpath = S.newrun ? A.dir + "/INPUT/ic.tec" : restart_field(A.dir);
     double time0 = 0.0;
-    std::vector<Block> blocks = read_tec(A.dir + "/INPUT/ic.tec", &time0);
+    std::vector<Block> blocks = read_tec(icpath, &time0);
+    const double case_time = (!S.newrun && S.opt.time_accurate) ? time0 : 0.0;
+    const long long iter_base = (!S.newrun && !S.opt.time_accurate) ? (long long)time0 : 0;
     if (S.area)
         for (size_t b = 0; b < blocks.size(); ++b)
             blocks[b].area = read_area(A.dir + "/INPUT/block" + std::to_string(b + 1) + "_area.dat", blocks[b]);
     std::vector<q2d_bc_rec> recs = read_bc(A.dir + "/INPUT/bc.txt", S.unsupported);
-    if (time0 != 0.0) S.unsupported.push_back("ic.tec: SOLUTIONTIME != 0 (restart time)");
     const q2d_options& o = S.opt;
 
     if (A.check) {   // parse summary, no GPU
@@ -577,10 +618,15 @@ int run(int argc, char** argv) {
                         "\"precision\": %d, \"rampa_iter\": %d, \"res_diter\": %d, \"sol_diter\": %d, "
                         "\"itermax\": %lld, \"cfl\": %.17g, \"res_threshold\": %.17g, \"time_threshold\": %.17g, "
                         "\"sol_dtime\": %.17g, \"gas_R\": %.17g, \"gas_gamma\": %.17g, \"shell_diter\": %d, "
-                        "\"irs_beta\": %.17g, \"shock_detector\": %d, \"riemann_minf\": %.17g,\n",
+                        "\"irs_beta\": %.17g, \"shock_detector\": %d, \"riemann_minf\": %.17g, \"newrun\": %d, "
+                        "\"case_time\": %.17g, \"iter_base\": %lld,\n",
                      o.limiter, o.riemann, o.n_rk, o.time_accurate, o.source, o.precision, o.rampa_iter, o.res_diter,
                      o.sol_diter, o.itermax, o.cfl, o.res_threshold, o.time_threshold, o.sol_dtime, o.gas_R,
-                     o.gas_gamma, S.shell_diter, o.irs_beta, o.shock_detector, o.riemann_minf);
+                     o.gas_gamma, S.shell_diter, o.irs_beta, o.shock_detector, o.riemann_minf, S.newrun ? 1 : 0,
+                     case_time, iter_base);
+        std::fprintf(f, " \"initial_field\": ");
+        json_str(f, icpath);
+        std::fprintf(f, ",\n");
         std::fprintf(f, " \"blocks\": [");
         for (size_t b = 0; b < blocks.size(); ++b) {
             double s = 0.0, sa = 0.0;
@@ -632,6 +678,7 @@ int run(int argc, char** argv) {
             check(q2d_gpu_upload_prim(ctx, bid[b], P[b].data()), "q2d_gpu_upload_prim");
         }
         check(q2d_gpu_set_bcs(ctx, cid, recs.data(), (int)recs.size()), "q2d_gpu_set_bcs");
+        if (case_time != 0.0) check(q2d_gpu_set_case_time(ctx, cid, case_time), "q2d_gpu_set_case_time");
         check(q2d_gpu_commit(ctx), "q2d_gpu_commit");
         if (!A.quiet)
             std::printf("q2d_host: %zu blocks, %lld cells, %zu boundary records, %s, limiter %s, %s, RK%d, cfl %g, %s\n",
@@ -646,17 +693,37 @@ int run(int argc, char** argv) {
         FILE* hist = std::fopen((A.out.empty() ? outdir + "/residuals.dat" : A.out + ".residuals").c_str(), "w");
         if (!hist) die("cannot write the residual history");
         std::fprintf(hist, "# iter time dtglobal res_rho res_u res_v res_p\n");
+        // the reference's residual history (Wrap_Setup.f90:114-127, Wrap_Postprocess.f90:128-133,
+        // 248-253): iter_general, time (-1 for steady runs), the 4 residuals, (I8,E20.10,4E20.10),
+        // every res-diter iterations; appended to on a restart
+        FILE* rh = A.out.empty() ? std::fopen((outdir + "/residual-history.dat").c_str(), S.newrun ? "w" : "a")
+                                 : nullptr;
+        if (A.out.empty() && !rh) die("cannot write OUTPUT/residual-history.dat");
+        // SOLUTIONTIME of a written field: the time, or -iter_general for steady runs
+        auto sol_time = [&](const q2d_step_info& in) {
+            return o.time_accurate ? in.time : -(double)(iter_base + in.iter);
+        };
         q2d_step_info info{};
         long long done = 0, last_shell = 0;
         int rc = 0;
         for (;;) {
             int n = A.per_call;
+            n = (int)std::min<long long>(n, o.res_diter - done % o.res_diter);   // land on res-diter multiples
             if (A.max_steps >= 0) n = (int)std::min<long long>(n, A.max_steps - done);
             if (n <= 0) break;
             const int st = q2d_gpu_step(ctx, n, &info);
             done = info.iter;
             std::fprintf(hist, "%lld %.17g %.17g %.17g %.17g %.17g %.17g\n", info.iter, info.time, info.dtglobal,
                          info.residual[0], info.residual[1], info.residual[2], info.residual[3]);
+            if (rh && st == Q2D_OK && info.iter % o.res_diter == 0) {
+                std::string line;
+                char ib[32];
+                std::snprintf(ib, sizeof ib, "%8lld", iter_base + info.iter);
+                line += ib;
+                line += fortran_e20_10(o.time_accurate ? info.time : -1.0);
+                for (int k = 0; k < 4; ++k) line += fortran_e20_10(info.residual[k]);
+                std::fprintf(rh, "%s\n", line.c_str());
+            }
             if (!A.quiet && (info.iter - last_shell >= S.shell_diter || info.todo != Q2D_TODO_CONTINUE || st)) {
                 std::printf("iter %lld  time %.6e  dt %.6e  res %.6e %.6e %.6e %.6e\n", info.iter, info.time,
                             info.dtglobal, info.residual[0], info.residual[1], info.residual[2], info.residual[3]);
@@ -671,16 +738,17 @@ int run(int argc, char** argv) {
             if (info.todo == Q2D_TODO_IO || info.todo == Q2D_TODO_END) {   // Write_Solution
                 for (size_t b = 0; b < blocks.size(); ++b)
                     check(q2d_gpu_download_prim(ctx, bid[b], P[b].data()), "q2d_gpu_download_prim");
-                write_tec(out, blocks, P, info.time);
+                write_tec(out, blocks, P, sol_time(info));
             }
             if (info.todo == Q2D_TODO_END) break;
         }
         if (rc == 0 && info.todo != Q2D_TODO_END) {   // stopped by --max-steps
             for (size_t b = 0; b < blocks.size(); ++b)
                 check(q2d_gpu_download_prim(ctx, bid[b], P[b].data()), "q2d_gpu_download_prim");
-            write_tec(out, blocks, P, info.time);
+            write_tec(out, blocks, P, sol_time(info));
         }
         std::fclose(hist);
+        if (rh) std::fclose(rh);
         if (!A.quiet)
             std::printf("q2d_host: %s after %lld steps, wrote %s\n",
                         rc ? "stopped on error" : (info.todo == Q2D_TODO_END ? "converged/ended" : "stopped"), done,

@@ -58,6 +58,8 @@ class Q2DSolver:
                     self._call("upload_prim", self.ctx, bid.value, _abi.dptr(P))
                     ids.append(bid.value)
                 self.block_ids.append(ids)
+                if cs.meta.get("restart_time") is not None:   # resume a time-accurate case
+                    self._call("set_case_time", self.ctx, cid.value, float(cs.meta["restart_time"]))
                 recs = _abi.bc_array(cs.bcs)
                 self._call("set_bcs", self.ctx, cid.value, recs, len(cs.bcs))
             self._call("commit", self.ctx)

@@ -189,3 +189,35 @@ def test_host_shuosher_matches_reference_binary(tmp_path):
     rho = refio.read_field(tmp_path / "OUTPUT" / "field.tec")[0].prim[0, :, 0]
     rel_l1 = np.abs(rho - ref[:, 1]).sum() / np.abs(ref[:, 1]).sum()
     assert rel_l1 <= 1e-8, rel_l1
+
+
+def test_restart_input_selection(tmp_path):
+    """newrun = false (Read_IC, IO_Solution.f90:78-96; Wrap_Setup.f90:132-149): the initial field
+    is OUTPUT/field.tec, else the last of OUTPUT/field1.tec, field2.tec, ...; a time-accurate
+    case resumes at its SOLUTIONTIME, a steady one counts iterations from int(SOLUTIONTIME); a
+    new run ignores SOLUTIONTIME; no restart field is an error."""
+    cs = cases.riemann_1d(ni=40, nj=2, seed=4)
+    refio.write_case(cs, tmp_path)
+    ini = (tmp_path / "input.ini").read_text()
+    ic = (tmp_path / "INPUT" / "ic.tec").read_text()
+    out = tmp_path / "OUTPUT"
+    out.mkdir()
+    stamped = ic.replace("SOLUTIONTIME=0.000000000000000E+000", "SOLUTIONTIME=1.25E-002")
+    assert stamped != ic
+    (tmp_path / "INPUT" / "ic.tec").write_text(stamped)
+    d = json.loads(host(tmp_path, "--check").stdout)
+    assert d["newrun"] == 1 and d["case_time"] == 0.0 and d["initial_field"].endswith("INPUT/ic.tec")
+    restart = ini.replace("[Q2D-Parameters]\n", "[Q2D-Parameters]\nnewrun = false\n")
+    (tmp_path / "input.ini").write_text(restart)
+    r = host(tmp_path, "--check", check=False)
+    assert r.returncode != 0 and "OUTPUT/field.tec" in r.stderr
+    (out / "field1.tec").write_text(stamped)
+    (out / "field2.tec").write_text(stamped.replace("1.25E-002", "2.5E-002"))
+    d = json.loads(host(tmp_path, "--check").stdout)
+    assert d["initial_field"].endswith("OUTPUT/field2.tec") and d["case_time"] == 0.025 and d["iter_base"] == 0
+    (out / "field.tec").write_text(stamped.replace("1.25E-002", "-3.0E+002"))
+    d = json.loads(host(tmp_path, "--check").stdout)
+    assert d["initial_field"].endswith("OUTPUT/field.tec") and d["case_time"] == -300.0
+    (tmp_path / "input.ini").write_text(restart.replace("time-accurate = true", "time-accurate = false"))
+    d = json.loads(host(tmp_path, "--check").stdout)
+    assert d["time_accurate"] == 0 and d["case_time"] == 0.0 and d["iter_base"] == -300
