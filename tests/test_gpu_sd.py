@@ -189,3 +189,41 @@ def test_ramp_channel_sensor_driven_solvers(riemann, precision):
         s.close()
     assert info["err"] == 0 and info["residual"][0] < 1e-3, info
     ramp_channel_gates(cs, prim, sensor_field(cs, [prim])[0])
+
+
+@pytest.mark.parametrize("riemann", ["HLLC", "HLLC+", "AUSM+"])
+def test_sd_one_dimensional_time_accurate(riemann):
+    """MUSCL-SD on a 1-D time-accurate case (nj = 1: the sensor's j-neighbours are the ghost
+    rows of both walls), FP64 against the oracle and the FP32-flux form against FP64."""
+    from q2d_b200 import cases
+    cs = cases.riemann_1d(ni=160, nj=1, states=(1.0, 1.0, 0.125, 0.1), limiter="minmod", t_end=0.2)
+    gs, os_, _, _ = run_pair([cs], 1, shock_detector=1, riemann=riemann)
+    check(gs, os_, 1e-12, f"1-D sd {riemann} 1 step")
+    gs, os_, _, _ = run_pair([cs], 30, chunks=3, shock_detector=1, riemann=riemann)
+    check(gs, os_, 1e-10, f"1-D sd {riemann} 30 steps")
+    out = []
+    for prec in (0, 1):
+        s = Q2DSolver(make_options(cs, precision=prec, shock_detector=1, riemann=riemann), [cs])
+        try:
+            assert s.step(30)[0]["err"] == 0
+            out.append(s.prim())
+        finally:
+            s.close()
+    assert rel_l1(out[1], out[0]).max() <= 1e-6
+
+
+@pytest.mark.parametrize("riemann", ["HLLEM", "exact", "AUSM+-up"])
+def test_sd_with_run_time_solvers_fp32flux(developed, riemann):
+    """MUSCL-SD with the run-time selected solvers in the FP32-flux form (its shock-sensor
+    instantiation of the generic solver group) against the FP64 form."""
+    one, _ = developed
+    out = []
+    for prec, sch in ((0, 0), (1, 6)):
+        s = Q2DSolver(make_options(one, precision=prec, riemann=riemann, riemann_minf=3.0), [one])
+        try:
+            s.set_schedule(sch)
+            assert s.step(10)[0]["err"] == 0
+            out.append(s.prims()[0][0])
+        finally:
+            s.close()
+    assert rel_l1(out[1], out[0]).max() <= 1e-6
