@@ -466,15 +466,24 @@ void read_gas(const std::string& dir, const std::string& gamma_arg, q2d_options&
     if (gamma_arg == "table") {
         std::ifstream th(dir + "/INPUT/thermo.dat");
         if (!th) die("--gamma table needs INPUT/thermo.dat");
+        // the calorically perfect closure is exact only for a constant cp (the reference's Air
+        // table: 1004.5 J/(kg K) on every row, 1-10000 K); a temperature-dependent cp needs the
+        // table lerp (Lib_Riemann_HLL.f90:258-303), which this path does not build
         std::string line;
+        double cp0 = 0.0;
+        long long rows = 0;
         while (std::getline(th, line)) {
             auto t = split_list(line);
             if (t.size() >= 2 && (std::isdigit((unsigned char)t[0][0]) || t[0][0] == '.')) {
                 const double cp = to_double(t[1], "thermo.dat");
-                o.gas_gamma = cp / (cp - o.gas_R);
-                break;
+                if (rows++ == 0) cp0 = cp;
+                else if (std::fabs(cp - cp0) > 1e-12 * std::fabs(cp0))
+                    die("INPUT/thermo.dat: cp varies with temperature (" + t[0] +
+                        "): table thermodynamics is not on this path");
             }
         }
+        if (rows == 0) die("INPUT/thermo.dat: no table rows");
+        o.gas_gamma = cp0 / (cp0 - o.gas_R);
     } else {
         o.gas_gamma = to_double(gamma_arg, "--gamma");
     }

@@ -221,3 +221,24 @@ def test_restart_input_selection(tmp_path):
     (tmp_path / "input.ini").write_text(restart.replace("time-accurate = true", "time-accurate = false"))
     d = json.loads(host(tmp_path, "--check").stdout)
     assert d["time_accurate"] == 0 and d["case_time"] == 0.0 and d["iter_base"] == -300
+
+
+def test_gamma_from_the_constant_cp_table(tmp_path):
+    """--gamma table: gamma = cp / (cp - R) from INPUT/thermo.dat when cp is the same on every row
+    (the reference's Air table); a temperature-dependent cp is refused (table thermodynamics is
+    not on this path)."""
+    cs = cases.ramp(20, 8)
+    refio.write_case(cs, tmp_path)
+    d = json.loads(host(tmp_path, "--check", "--gamma", "table").stdout)
+    R = d["gas_R"]
+    lines = (tmp_path / "INPUT" / "thermo.dat").read_text().splitlines()
+    rows = [ln for ln in lines if ln.strip() and (ln.strip()[0].isdigit() or ln.strip()[0] == ".")]
+    cp = float(rows[0].split()[1])
+    assert d["gas_gamma"] == pytest.approx(cp / (cp - R), rel=1e-15)
+    k = lines.index(rows[-1])
+    t = rows[-1].split()
+    t[1] = repr(cp * 1.01)
+    lines[k] = " ".join(t)
+    (tmp_path / "INPUT" / "thermo.dat").write_text("\n".join(lines) + "\n")
+    r = host(tmp_path, "--check", "--gamma", "table", check=False)
+    assert r.returncode != 0 and "cp varies with temperature" in r.stderr
