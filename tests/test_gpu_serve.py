@@ -136,3 +136,27 @@ def test_request_loop_small_stream():
     for r in reqs:
         assert r.iters <= 300 and (r.iters == 300 or r.residual_drop <= 1e-3)
     assert st["cell_updates"] > 0 and st["p99_latency_s"] >= st["p50_latency_s"] > 0
+
+
+@pytest.mark.parametrize("precision", [_abi.PREC_FP64, _abi.PREC_FP32_FLUX])
+@pytest.mark.parametrize("kw", [dict(shock_detector=1, riemann="HLLE", irs_beta=0.5), dict(riemann="HLLC+"),
+                                dict(riemann="AUSM+")])
+def test_serving_with_sensor_and_other_solvers(precision, kw):
+    """The serving context on the shock-sensor instantiations, HLLC+ and a run-time selected
+    solver (with IRS for the first): every case in the mix, admitted while others run, ends
+    with the state it reaches alone."""
+    reqs = small_requests()
+    steps = 12
+    opts = serve_options(precision=precision, itermax=steps, drop=1e-30, **kw)
+    alone = [run_alone(c, opts, steps + 4) for c in reqs]
+    with ServeContext(opts, BUDGET, 8) as sc:
+        ids = [sc.admit(reqs[0]), sc.admit(reqs[1])]
+        sc.step_async(4); sc.wait()
+        ids += [sc.admit(reqs[2]), sc.admit(reqs[3])]
+        for _ in range(4):
+            sc.step_async(4)
+            infos = sc.wait()
+        for k, (cid, c) in enumerate(zip(ids, reqs)):
+            assert infos[cid].iter == steps and infos[cid].err == 0
+            for b in range(len(c.blocks)):
+                assert np.array_equal(sc.prim(cid, b), alone[k][0][b]), (kw, k, b)
