@@ -151,3 +151,20 @@ def test_chang_nozzle_reference_case(precision):
             o.close()
         assert info["iter"] == oi["iter"] and info["residual"][0] <= 1e-10
         assert rel_linf(prim, ref).max() <= 1e-8
+
+
+def test_chang_nozzle_reference_case_through_host(tmp_path):
+    """The chang-nozzle case written in the reference's formats (axisymmetric source, IRS) and
+    run by q2d_host: it stops at the case's res-threshold within its 5000 iterations, the
+    residual history is the reference's format, and the field passes the case's Mach gates."""
+    from q2d_b200 import refio
+    from tests.helpers import chang_nozzle_case, chang_nozzle_gates
+    from tests.test_host_harness import host
+    cs = chang_nozzle_case()
+    refio.write_case(cs, tmp_path, res_threshold=1e-10, res_diter=100)
+    host(tmp_path, "--gamma", repr(cs.options["gas_gamma"]), "--steps-per-call", 500, "--quiet")
+    lines = (tmp_path / "OUTPUT" / "residual-history.dat").read_text().splitlines()
+    assert lines and all(len(ln) == 108 for ln in lines)
+    res = np.loadtxt(tmp_path / "OUTPUT" / "residuals.dat")
+    assert res[-1, 0] < 5000 and res[-1, 3] <= 1e-10
+    chang_nozzle_gates(cs, refio.read_field(tmp_path / "OUTPUT" / "field.tec")[0].prim)
