@@ -201,8 +201,9 @@ Setup read_options(const Ini& ini) {
     if (const std::string* v = ini_get(ini, "IO", "sol-diter")) o.sol_diter = (int)std::min<long long>(to_int(*v, "sol-diter"), 1000000000);
     if (const std::string* v = ini_get(ini, "IO", "sol-dtime")) o.sol_dtime = to_double(*v, "sol-dtime");
     if (const std::string* v = ini_get(ini, "IO", "shell-diter")) s.shell_diter = (int)to_int(*v, "shell-diter");
-    if (const std::string* v = ini_get(ini, "IO", "ini-format"))
-        if (lower(*v) != "tecplot ascii") s.unsupported.push_back("[Q2D-IO] ini-format = " + *v);
+    for (const char* k : {"ini-format", "sol-format"})   // Register_IO.f90:23-24: ASCII Tecplot only here
+        if (const std::string* v = ini_get(ini, "IO", k))
+            if (lower(*v) != "tecplot ascii") s.unsupported.push_back(std::string("[Q2D-IO] ") + k + " = " + *v);
     s.source_name = "none";
     if (const std::string* v = ini_get(ini, "Sources", "active")) {
         s.source_name = *v;
