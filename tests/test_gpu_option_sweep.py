@@ -2,7 +2,8 @@
 combinations of limiter, Riemann solver, MUSCL-SD, implicit residual smoothing, RK scheme and
 schedule, on the developed ramp-channel flow cut into 2 x 2 blocks (shocks across the block and
 tile edges) or on a multi-block axisymmetric nozzle, two steps agree with the oracle to 1e-10
-relative L-infinity. A draw whose flow leaves the physical states (both implementations report
+relative L-infinity; 16 more draws in the FP32-flux form on its five tiles against the FP64 form
+to 1e-6 relative L1. A draw whose flow leaves the physical states (both implementations report
 it) is skipped in favour of the next."""
 import numpy as np
 import pytest
@@ -39,3 +40,34 @@ def test_option_sweep_vs_oracle(developed, k, d):   # noqa: F811
         assert gi[0]["err"] == oi[0]["err"], (d, gi[0]["err"], oi[0]["err"])
         pytest.skip(f"non-physical state in both implementations: {d}")
     check(gs, os_, 1e-9 if d["riemann"] == "HLLC Rotated" else 1e-10, f"draw {k} {d}")
+
+
+@pytest.mark.parametrize("k,d", list(enumerate(draws(16, seed=4821))))
+def test_option_sweep_fp32flux_vs_fp64(developed, k, d):   # noqa: F811
+    """The same kind of draws in the FP32-flux form on the FP32-flux kernel's five tiles against
+    the FP64 form: <= 1e-6 relative L1 after 4 steps (2e-6 for the rotated HLLC)."""
+    from q2d_b200 import make_options
+    from q2d_b200.solver import Q2DSolver
+    from tests.conftest import rel_l1
+    d = dict(d)
+    case, sch = d.pop("case"), 5 + k % 5
+    d.pop("schedule")
+    cs = developed[1] if case == 0 else cases.nozzle_axi(ni=36, nj=10, nblocks=2, seed=60 + k)
+    if "up" in d["riemann"]:
+        d["riemann_minf"] = 3.0 if case == 0 else 0.3
+    out = []
+    for prec, s_ in ((0, 0), (1, sch)):
+        s = Q2DSolver(make_options(cs, precision=prec, **d), [cs])
+        try:
+            s.set_schedule(s_)
+            info = s.step(4, check=False)[0]
+            out.append((info["err"], s.prims()[0]))
+        finally:
+            s.close()
+    if out[0][0] or out[1][0]:
+        assert out[0][0] == out[1][0], (d, out[0][0], out[1][0])
+        pytest.skip(f"non-physical state in both forms: {d}")
+    tol = 2e-6 if d["riemann"] == "HLLC Rotated" else 1e-6
+    for b, (x32, x64) in enumerate(zip(out[1][1], out[0][1])):
+        err = rel_l1(x32, x64)
+        assert err.max() <= tol, f"draw {k} {d} schedule {sch} block {b}: rel L1 {err}"
