@@ -10,6 +10,9 @@
 // until the process exits.
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "../../include/q2d_gpu.h"
 
 namespace {
@@ -22,8 +25,29 @@ constexpr int kMaxDevices = 64;
 // 4 partial sums of squares (rho, u, v, p) per chunk: 8192 * 4 * 8 B = 256 KiB per device.
 static __device__ __align__(256) double g_noalloc_scratch[4 * kMaxPartials];
 
-// Device address of g_noalloc_scratch per device, resolved once per device.
-double* g_scratch_ptr[kMaxDevices] = {nullptr};
+// Device address of g_noalloc_scratch per device, resolved once per device under g_scratch_mu
+// and published with release / acquire ordering, so that host threads making their first calls
+// at the same time resolve it once and never see a half-written slot. The cache is not rebuilt
+// after cudaDeviceReset: a process that resets a device must not call this entry point on it
+// afterwards.
+std::atomic<double*> g_scratch_ptr[kMaxDevices];
+std::mutex g_scratch_mu;
+
+// The device address of the scratch array on the current device `dev`, or nullptr when the
+// runtime cannot resolve it.
+double* scratch_on(int dev) {
+    double* p = g_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (p) return p;
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    p = g_scratch_ptr[dev].load(std::memory_order_relaxed);
+    if (!p) {
+        // First call on this device (its device is current): the host-side name of the array
+        // is only a stand-in, so fetch its device address once.
+        if (cudaGetSymbolAddress((void**)&p, g_noalloc_scratch) != cudaSuccess || !p) return nullptr;
+        g_scratch_ptr[dev].store(p, std::memory_order_release);
+    }
+    return p;
+}
 
 // Sum over cells of |new - old|^2 per variable, one chunk of kCellsPerPartial cells per CTA,
 // in a fixed order (thread-strided sums, then a fixed shuffle/warp tree), as in
@@ -84,16 +108,14 @@ extern "C" int q2d_gpu_residual_norm_noalloc(const double* p_new, const double* 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return Q2D_ERR_CUDA;
     if (dev < 0 || dev >= kMaxDevices) return Q2D_ERR_CAPACITY;
-    if (!g_scratch_ptr[dev]) {
-        // First call on this device (its device must be current): the host-side name of the
-        // array is only a stand-in, so fetch its device address once.
-        double* p = nullptr;
-        if (cudaGetSymbolAddress((void**)&p, g_noalloc_scratch) != cudaSuccess || !p) return Q2D_ERR_CUDA;
-        g_scratch_ptr[dev] = p;
-    }
+    // An error the caller left pending is theirs: report it without launching and without
+    // clearing it, so that the launch check below sees only this call's own launches.
+    if (cudaPeekAtLastError() != cudaSuccess) return Q2D_ERR_CUDA;
+    double* scratch = scratch_on(dev);
+    if (!scratch) return Q2D_ERR_CUDA;
     const int nparts = (int)((ncells + kCellsPerPartial - 1) / kCellsPerPartial);
     cudaStream_t s = (cudaStream_t)stream;
-    residual_partials<<<nparts, kThreads, 0, s>>>(p_new, p_old, ncells, plane_stride, g_scratch_ptr[dev]);
-    residual_final<<<1, kThreads, 0, s>>>(g_scratch_ptr[dev], nparts, norms_out);
+    residual_partials<<<nparts, kThreads, 0, s>>>(p_new, p_old, ncells, plane_stride, scratch);
+    residual_final<<<1, kThreads, 0, s>>>(scratch, nparts, norms_out);
     return cudaGetLastError() == cudaSuccess ? Q2D_OK : Q2D_ERR_CUDA;
 }

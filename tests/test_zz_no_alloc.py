@@ -60,3 +60,38 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     assert lib.q2d_gpu_residual_norm_noalloc(x.data_ptr(), x.data_ptr(), limit + 1, limit + 1,
                                              x.data_ptr(), None) == _abi.ERR_CAPACITY
     assert lib.q2d_gpu_residual_norm_noalloc(x.data_ptr(), x.data_ptr(), 0, 1, x.data_ptr(), None) == _abi.ERR_BADARG
+
+
+def _numpy_norms(new, old, n):
+    d = new[:, :n] - old[:, :n]
+    return np.sqrt((d * d).sum(axis=1))
+
+
+@pytest.mark.parametrize("ncells,stride", [
+    (3 * 2048, 3 * 2048 + 37),        # padded planes: the padding holds garbage
+    (5 * 2048, 5 * 2048),             # last chunk exactly full
+    (5 * 2048 + 1, 5 * 2048 + 64),    # one cell in the last chunk, padded
+    (8192 * 2048, 8192 * 2048),       # the largest accepted size
+])
+def test_noalloc_sizes_and_strides_against_numpy(ncells, stride):
+    import torch
+    from q2d_b200 import _abi
+
+    lib = _abi.load_library()
+    rng = np.random.default_rng(ncells)
+    old = rng.standard_normal((4, stride))
+    new = old + rng.standard_normal((4, stride)) * np.array([[1e-3], [1.0], [0.5], [1e3]])
+    old[:, ncells:] = np.nan   # padding beyond ncells is never read
+    new[:, ncells:] = 1e300
+    pn = torch.tensor(new, dtype=torch.float64, device="cuda")
+    po = torch.tensor(old, dtype=torch.float64, device="cuda")
+    ref = _numpy_norms(new, old, ncells)
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):   # two calls in a row share the scratch array
+        out = torch.full((4,), -1.0, dtype=torch.float64, device="cuda")
+        st = lib.q2d_gpu_residual_norm_noalloc(pn.data_ptr(), po.data_ptr(), ncells, stride,
+                                               out.data_ptr(), C.c_void_p(stream))
+        assert st == 0
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert np.allclose(got, ref, rtol=RTOL, atol=0.0), (got, ref)
