@@ -990,9 +990,11 @@ void symmetry_metrics(Block& B, int Im, int Jm, int Fm) {
     }
 }
 
-// BC_Connect_Metrics (Lib_Metrics.f90:444-553)
+// BC_Connect_Metrics (Lib_Metrics.f90:444-553); with periodic, BC_Connect_Metrics_Periodic
+// (:556-700): every donor node read is moved by the rigid translation T that maps the donor's
+// seam nodes of step g = 0 onto this block's seam nodes (T from both seam nodes must agree).
 int connect_metrics(Block& Bm, int Im, int Jm, int Fm, const Block& Bs, int Is, int Js, int Fs,
-                    int d11s, int d21s) {
+                    int d11s, int d21s, bool periodic = false) {
     static const int guides[5][2] = {{0, 0}, {0, 0}, {-1, 0}, {0, 0}, {0, -1}};
     static const int guides2[5][2] = {{0, 0}, {1, 0}, {-2, 0}, {0, 1}, {0, -2}};
     V2 N1[GC + 1], N2[GC + 1], N3[GC + 1], N4[GC + 1];
@@ -1003,6 +1005,27 @@ int connect_metrics(Block& Bm, int Im, int Jm, int Fm, const Block& Bs, int Is, 
         case 4: N2[0] = nodev(Bm, Im - 1, Jm); N4[0] = nodev(Bm, Im, Jm); break;
     }
     int e = Q2D_OK;
+    V2 T{0.0, 0.0};
+    if (periodic) {
+        const int Is1 = Is + GC * guides[Fs][0] - guides2[Fs][0];
+        const int Js1 = Js + GC * guides[Fs][1] - guides2[Fs][1];
+        int II0, JJ0, III0, JJJ0;
+        if (Fs <= 2) { II0 = Is1; JJ0 = (2 * Js1 + d11s + d21s) / 2; III0 = II0; JJJ0 = JJ0 - d11s; }
+        else { II0 = (2 * Is1 + d11s + d21s) / 2; JJ0 = Js1; III0 = II0 - d11s; JJJ0 = JJ0; }
+        if (II0 < 0 || II0 > Bs.ni || JJ0 < 0 || JJ0 > Bs.nj || III0 < 0 || III0 > Bs.ni || JJJ0 < 0 ||
+            JJJ0 > Bs.nj)
+            return Q2D_ERR_BADARG;
+        const V2 a0 = nodev(Bs, II0, JJ0), b0 = nodev(Bs, III0, JJJ0);
+        V2 T2;
+        switch (Fm) {
+            case 1: T = {N2[0].x - a0.x, N2[0].y - a0.y}; T2 = {N1[0].x - b0.x, N1[0].y - b0.y}; break;
+            case 2: T = {N4[0].x - a0.x, N4[0].y - a0.y}; T2 = {N3[0].x - b0.x, N3[0].y - b0.y}; break;
+            case 3: T = {N3[0].x - a0.x, N3[0].y - a0.y}; T2 = {N1[0].x - b0.x, N1[0].y - b0.y}; break;
+            default: T = {N4[0].x - a0.x, N4[0].y - a0.y}; T2 = {N2[0].x - b0.x, N2[0].y - b0.y}; break;
+        }
+        const double big = 1.0 + std::max(std::fabs(T.x), std::fabs(T.y));
+        if (std::max(std::fabs(T.x - T2.x), std::fabs(T.y - T2.y)) > 1e-10 * big) return Q2D_ERR_BADARG;
+    }
     for (int g = 1; g <= GC; ++g) {
         const int Is1 = Is + (GC - g) * guides[Fs][0] + (g - 1) * guides2[Fs][0];
         const int Js1 = Js + (GC - g) * guides[Fs][1] + (g - 1) * guides2[Fs][1];
@@ -1010,12 +1033,14 @@ int connect_metrics(Block& Bm, int Im, int Jm, int Fm, const Block& Bs, int Is, 
         if (Fs <= 2) { II = Is1; JJ = (2 * Js1 + d11s + d21s) / 2; }
         else { II = (2 * Is1 + d11s + d21s) / 2; JJ = Js1; }
         if (II < 0 || II > Bs.ni || JJ < 0 || JJ > Bs.nj) return Q2D_ERR_BADARG;
-        const V2 a = nodev(Bs, II, JJ);
+        V2 a = nodev(Bs, II, JJ);
+        a = {a.x + T.x, a.y + T.y};
         switch (Fm) { case 1: N2[g] = a; break; case 2: N4[g] = a; break;
                       case 3: N3[g] = a; break; case 4: N4[g] = a; break; }
         if (Fs <= 2) { III = II; JJJ = JJ - d11s; } else { III = II - d11s; JJJ = JJ; }
         if (III < 0 || III > Bs.ni || JJJ < 0 || JJJ > Bs.nj) return Q2D_ERR_BADARG;
-        const V2 b = nodev(Bs, III, JJJ);
+        V2 b = nodev(Bs, III, JJJ);
+        b = {b.x + T.x, b.y + T.y};
         switch (Fm) { case 1: N1[g] = b; break; case 2: N3[g] = b; break;
                       case 3: N1[g] = b; break; case 4: N2[g] = b; break; }
         switch (Fm) {
@@ -1036,7 +1061,7 @@ void ghost_fill(q2d_oracle* o, Case& cs) {
         Block& B = o->blk[cs.blocks[rec.b - 1]];
         const int Im = rec.i, Jm = rec.j, Fm = rec.f;
         switch (rec.type) {
-            case 101: {   // Ghost_Connection :143-160
+            case 101: case 201: {   // Ghost_Connection :143-160 (201: Lib_Ghost.f90:63)
                 const Block& S = o->blk[cs.blocks[rec.bs - 1]];
                 for (int g = 1; g <= GC; ++g) {
                     const int Ig = Im - GUIDE[Fm][0] * g, Jg = Jm - GUIDE[Fm][1] * g;
@@ -1522,7 +1547,7 @@ bool bc_fluxes(q2d_oracle* o, Case& cs, int& eb, int& ei, int& ej) {
         Block& B = o->blk[cs.blocks[rec.b - 1]];
         const int Im = rec.i, Jm = rec.j, Fm = rec.f;
         switch (rec.type) {
-            case 101:
+            case 101: case 201:   // connection and periodic seam (Mod_BC_Fluxes.f90:99-102)
                 if (!bc_connection(o, B, Im, Jm, Fm)) { eb = rec.b; ei = Im; ej = Jm; return false; }
                 break;
             case 300: bc_symmetry(o, B, Im, Jm, Fm); break;
@@ -1622,7 +1647,7 @@ void residual_smoothing(q2d_oracle* o, Case& cs, double beta) {
             Block& B = o->blk[cs.blocks[r.b - 1]];
             const int gi = r.i - (r.f == 1 ? 1 : r.f == 2 ? -1 : 0);
             const int gj = r.j - (r.f == 3 ? 1 : r.f == 4 ? -1 : 0);
-            const double* src = r.type == 101 ? o->blk[cs.blocks[r.bs - 1]].r(r.is, r.js) : B.r(r.i, r.j);
+            const double* src = (r.type == 101 || r.type == 201) ? o->blk[cs.blocks[r.bs - 1]].r(r.is, r.js) : B.r(r.i, r.j);
             double* g = B.r(gi, gj);
             for (int v = 0; v < 4; ++v) g[v] = src[v];
         }
@@ -1840,9 +1865,10 @@ int commit(q2d_oracle* o) {
         for (const q2d_bc_rec& rec : cs.bc) {
             Block& B = o->blk[cs.blocks[rec.b - 1]];
             int e = Q2D_OK;
-            if (rec.type == 101) {
+            if (rec.type == 101 || rec.type == 201) {
                 const Block& S = o->blk[cs.blocks[rec.bs - 1]];
-                e = connect_metrics(B, rec.i, rec.j, rec.f, S, rec.is, rec.js, rec.fs, rec.d11, rec.d21);
+                e = connect_metrics(B, rec.i, rec.j, rec.f, S, rec.is, rec.js, rec.fs, rec.d11, rec.d21,
+                                    rec.type == 201);
             } else if (rec.type == 300) {
                 symmetry_metrics(B, rec.i, rec.j, rec.f);
             } else {
@@ -1935,7 +1961,7 @@ int q2d_oracle_set_bcs(q2d_oracle* o, int case_id, const q2d_bc_rec* recs, int n
             case 0: case 300: case 401: case 405: case 406:
                 if (r.f <= 2 && B.ni < 2) return Q2D_ERR_BADARG;
                 break;
-            case 101:
+            case 101: case 201:
                 if (r.bs < 1 || r.bs > (int)cs.blocks.size() || r.fs < 1 || r.fs > 4) return Q2D_ERR_BADARG;
                 break;
             default: return Q2D_ERR_UNSUPPORTED;

@@ -428,8 +428,11 @@ int build_case_edges(q2d_ctx* ctx, int c) {
         const int k = (r.f <= 2) ? r.j - 1 : r.i - 1;
         EdgeRec& er = B.edge[r.f - 1][k];
         if (er.type != -1) return fail(ctx, Q2D_ERR_BADARG, "duplicate boundary record");
-        er.type = r.type;
-        if (r.type == 101) {
+        // A periodic seam (201) is a connection on the device: Ghost_Connection and
+        // BC_Connection_Eul serve both (Lib_Ghost.f90:63, Mod_BC_Fluxes.f90:99-102); only its
+        // ghost metrics differ (ghost_metrics)
+        er.type = r.type == 201 ? 101 : r.type;
+        if (r.type == 101 || r.type == 201) {
             const HBlock& D = ctx->blocks[cs.blocks[r.bs - 1]];
             const int gi = r.fs == 1 ? 1 : (r.fs == 2 ? -1 : 0);
             const int gj = r.fs == 3 ? 1 : (r.fs == 4 ? -1 : 0);
@@ -543,7 +546,7 @@ int prepare_case(q2d_ctx* ctx, int c) {
     }
     for (const q2d_bc_rec& r : cs.bc) {
         HBlock& B = ctx->blocks[cs.blocks[r.b - 1]];
-        const HBlock* D = r.type == 101 ? &ctx->blocks[cs.blocks[r.bs - 1]] : nullptr;
+        const HBlock* D = (r.type == 101 || r.type == 201) ? &ctx->blocks[cs.blocks[r.bs - 1]] : nullptr;
         int e = ghost_metrics(r, B.ni, B.nj, B.nodes.data(), geo[r.b - 1], D ? D->ni : 0, D ? D->nj : 0,
                               D ? D->nodes.data() : nullptr);
         if (e) return fail(ctx, e, "ghost metrics failed for a boundary record");
@@ -903,7 +906,7 @@ int check_recs(q2d_ctx* ctx, const HCase& cs, const std::vector<q2d_bc_rec>& v) 
             case 0: case 300: case 401: case 405: case 406:
                 if (r.f <= 2 && B.ni < 2) return fail(ctx, Q2D_ERR_BADARG, "set_bcs: block too thin");
                 break;
-            case 101: {
+            case 101: case 201: {   // connection / translational periodic seam (Mod_BC_Fluxes.f90:99-102)
                 if (r.bs < 1 || r.bs > (int)cs.blocks.size() || r.fs < 1 || r.fs > 4)
                     return fail(ctx, Q2D_ERR_BADARG, "set_bcs: bad connection donor");
                 const HBlock& D = ctx->blocks[cs.blocks[r.bs - 1]];

@@ -2,6 +2,7 @@
 // Lib_Metrics.f90). Built with -ffp-contract=off: setup arithmetic is plain IEEE double.
 #include "q2d_setup.h"
 
+#include <algorithm>
 #include <cmath>
 
 namespace q2d {
@@ -227,7 +228,11 @@ int ghost_metrics(const q2d_bc_rec& r, int ni, int nj, const double* nodes, Host
         }
         return Q2D_OK;
     }
-    if (r.type == 101) {   // BC_Connect_Metrics (Lib_Metrics.f90:444-553)
+    if (r.type == 101 || r.type == 201) {
+        // BC_Connect_Metrics (Lib_Metrics.f90:444-553); for a translational periodic seam (201)
+        // BC_Connect_Metrics_Periodic (:556-700): the donor nodes moved by the rigid offset T
+        // that brings the donor's seam onto this block's, so that the ghost cells are the
+        // donor's cells, not a quadrilateral folded across the domain
         static const int gd[5][2] = {{0, 0}, {0, 0}, {-1, 0}, {0, 0}, {0, -1}};
         static const int gd2[5][2] = {{0, 0}, {1, 0}, {-2, 0}, {0, 1}, {0, -2}};
         auto D = [&](int i, int j) { return node(donor, dni, i, j); };
@@ -238,16 +243,33 @@ int ghost_metrics(const q2d_bc_rec& r, int ni, int nj, const double* nodes, Host
             case 3: A0 = X(Im - 1, Jm - 1); B0 = X(Im, Jm - 1); break;
             default: A0 = X(Im - 1, Jm); B0 = X(Im, Jm); break;
         }
-        P2 Ap = A0, Bp = B0;
-        for (int g = 1; g <= 2; ++g) {
+        // donor nodes of step g of the recurrence: a pairs with B0's role, b with A0's
+        auto donor_nodes = [&](int g, int& II, int& JJ, int& III, int& JJJ) {
             const int Is1 = r.is + (2 - g) * gd[r.fs][0] + (g - 1) * gd2[r.fs][0];
             const int Js1 = r.js + (2 - g) * gd[r.fs][1] + (g - 1) * gd2[r.fs][1];
-            int II, JJ, III, JJJ;
             if (r.fs <= 2) { II = Is1; JJ = (2 * Js1 + r.d11 + r.d21) / 2; III = II; JJJ = JJ - r.d11; }
             else { II = (2 * Is1 + r.d11 + r.d21) / 2; JJ = Js1; III = II - r.d11; JJJ = JJ; }
-            if (II < 0 || II > dni || JJ < 0 || JJ > dnj || III < 0 || III > dni || JJJ < 0 || JJJ > dnj)
-                return Q2D_ERR_BADARG;
+            return !(II < 0 || II > dni || JJ < 0 || JJ > dnj || III < 0 || III > dni || JJJ < 0 || JJJ > dnj);
+        };
+        P2 T{0.0, 0.0};
+        if (r.type == 201) {   // T from the seam (step g = 0); it must be one rigid translation
+            int II, JJ, III, JJJ;
+            if (!donor_nodes(0, II, JJ, III, JJJ)) return Q2D_ERR_BADARG;
             const P2 a = D(II, JJ), b = D(III, JJJ);
+            T = P2{B0.x - a.x, B0.y - a.y};
+            const P2 T2{A0.x - b.x, A0.y - b.y};
+            const double big = 1.0 + std::max(std::fabs(T.x), std::fabs(T.y));
+            if (std::max(std::fabs(T.x - T2.x), std::fabs(T.y - T2.y)) > 1e-10 * big) return Q2D_ERR_BADARG;
+        }
+        P2 Ap = A0, Bp = B0;
+        for (int g = 1; g <= 2; ++g) {
+            int II, JJ, III, JJJ;
+            if (!donor_nodes(g, II, JJ, III, JJJ)) return Q2D_ERR_BADARG;
+            P2 a = D(II, JJ), b = D(III, JJJ);
+            if (r.type == 201) {
+                a = P2{a.x + T.x, a.y + T.y};
+                b = P2{b.x + T.x, b.y + T.y};
+            }
             // a replaces the node paired with B0, b the node paired with A0 (N2/N1, N4/N3, ...)
             switch (Fm) {
                 case 1: e |= metric_at(G, Im - g, Jm, b, a, Ap, Bp); break;   // (N1g,N2g,N1g-1,N2g-1)

@@ -313,7 +313,7 @@ std::vector<q2d_bc_rec> read_bc(const std::string& path, std::vector<std::string
             default: break;   // no property line (IO_BC.f90:427-431)
         }
         switch (b.type) {
-            case 0: case 101: case 300: case 400: case 401: case 405: case 406: break;
+            case 0: case 101: case 201: case 300: case 400: case 401: case 405: case 406: break;
             default: odd[b.type] += 1;
         }
         recs.push_back(b);

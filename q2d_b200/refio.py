@@ -78,7 +78,7 @@ def _bc_lines(r: dict) -> list:
     get = lambda k, d=0.0: r.get(k, d)
     t = r["type"]
     out = [f"{r['b']:8d}{r['i']:8d}{r['j']:8d}{r['f']:8d}{t:8d}"]
-    if t == 101:
+    if t in (101, 201):
         vals = [r.get("bs", 0), r.get("is_", r.get("is", 0))] + [r.get(k, 0) for k in ("js", "fs", "d11", "d12", "d21", "d22")]
         out.append("".join(f"{int(v):8d}" for v in vals))
     elif t == 401:
