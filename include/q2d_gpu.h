@@ -159,7 +159,8 @@ typedef struct q2d_step_info {
     double    residual[4];   /* sqrt(sum over cells of |d rho|^2, |du|^2, |dv|^2, |dp|^2) */
     double    residual0;     /* residual[0] of the first step of the case */
     int       todo;          /* Q2D_TODO_* */
-    int       err;           /* Q2D_OK or Q2D_ERR_NONPHYSICAL / Q2D_ERR_NAN */
+    int       err;           /* Q2D_OK, Q2D_ERR_NONPHYSICAL / Q2D_ERR_NAN, or Q2D_ERR_BADARG when a
+                                stage kernel was launched with a layout it was not built for */
     int       err_b, err_i, err_j, err_stage;   /* where err was first raised (1-based) */
 } q2d_step_info;
 
@@ -234,8 +235,12 @@ int  q2d_gpu_get_schedule(const q2d_ctx* ctx);
  * until the process exits; ncells above Q2D_NOALLOC_MAX_PARTIALS *
  * Q2D_NOALLOC_CELLS_PER_PARTIAL (16,777,216) returns Q2D_ERR_CAPACITY. The first call on a
  * device looks up that array's device address on the current device, so make it before any
- * stream capture. All calls on one device share the array and each call overwrites the part
- * it uses: calls that overlap on the GPU (concurrent streams) race. */
+ * stream capture; host threads may make their first calls at the same time. The looked-up
+ * address is kept for the life of the process: do not call this entry point on a device after
+ * cudaDeviceReset. A CUDA error already pending when the call starts is returned as
+ * Q2D_ERR_CUDA without launching anything and is left pending for the caller. All calls on one
+ * device share the array and each call overwrites the part it uses: calls that overlap on the
+ * GPU (concurrent streams) race. */
 #define Q2D_NOALLOC_MAX_PARTIALS      8192
 #define Q2D_NOALLOC_CELLS_PER_PARTIAL 2048
 int  q2d_gpu_residual_norm_noalloc(const double* p_new, const double* p_old, long long ncells,
