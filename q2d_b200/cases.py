@@ -357,6 +357,32 @@ def closed_box(ni: int = 24, nj: int = 24, seed: int = 3, **options) -> CaseSpec
     return CaseSpec("box", [blk], bcs, opts)
 
 
+def periodic_box(ni: int = 32, nj: int = 24, seed: int = 5, **options) -> CaseSpec:
+    """A doubly periodic curvilinear unit square: each edge is a translational periodic seam
+    (BC 201) onto the opposite edge, the grid x = X + 0.03 sin(2 pi Y), y = Y + 0.03 sin(2 pi X)
+    repeats under the offsets (1, 0) and (0, 1), and the state is random. Nothing enters or
+    leaves, so mass, both momenta and energy change only by round-off. Options default to
+    van Leer, RK3, CFL 0.4, time-accurate."""
+    rng = np.random.default_rng(seed)
+    X, Y = np.meshgrid(np.linspace(0, 1, ni + 1), np.linspace(0, 1, nj + 1))
+    nodes = np.stack([X + 0.03 * np.sin(2 * np.pi * Y), Y + 0.03 * np.sin(2 * np.pi * X)], axis=-1)
+    prim = np.zeros((nj, ni, 4))
+    prim[..., 0] = 1 + 0.1 * rng.random((nj, ni))
+    prim[..., 1] = 0.2 + 0.1 * rng.standard_normal((nj, ni))
+    prim[..., 2] = -0.1 + 0.1 * rng.standard_normal((nj, ni))
+    prim[..., 3] = 1 + 0.1 * rng.random((nj, ni))
+    blk = BlockSpec(ni, nj, nodes, prim)
+    conn = dict(d11=1, d12=0, d21=0, d22=1)
+    bcs = edge_records(1, ni, nj, {
+        1: lambda k: (201, dict(bs=1, is_=ni, js=k, fs=2, **conn)),
+        2: lambda k: (201, dict(bs=1, is_=1, js=k, fs=1, **conn)),
+        3: lambda k: (201, dict(bs=1, is_=k, js=nj, fs=4, **conn)),
+        4: lambda k: (201, dict(bs=1, is_=k, js=1, fs=3, **conn))})
+    opts = dict(limiter="vanleer", n_rk=3, cfl=0.4, time_accurate=1)
+    opts.update(options)
+    return CaseSpec("periodic_box", [blk], bcs, opts)
+
+
 def cell_areas(block: BlockSpec) -> np.ndarray:
     """Quadrilateral cell areas from the nodes (half the cross product of the diagonals)."""
     X, Y = block.nodes[..., 0], block.nodes[..., 1]

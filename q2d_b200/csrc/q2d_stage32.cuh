@@ -23,6 +23,7 @@
 #pragma once
 #include "q2d_common.cuh"
 #include "q2d_kernels.cuh"
+#include "../../include/q2d_gpu.h"
 
 namespace q2d {
 
@@ -480,7 +481,14 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
     __shared__ double red[(NT / 32) * 5];
     __shared__ int s_flag;
     const int tid = threadIdx.x;
-    if (a.part_stride != NT / 32) return;   // partials are laid out one set per warp
+    if (a.part_stride != NT / 32) {
+        // the partials are laid out one set per warp: a host / kernel mismatch of that layout
+        // fails every case of the launch with Q2D_ERR_BADARG instead of skipping the stage
+        if (tid == 0)
+            for (int it = blockIdx.x; it < a.n_items; it += gridDim.x)
+                record_error(&a.cstate[__ldg(&a.items[it].case_id)], Q2D_ERR_BADARG, -1, -1, -1, a.irk);
+        return;
+    }
     const Gas& g = a.gas;
     const float gam = (float)g.gamma, gm1 = (float)g.gm1, gf = (float)g.gfac;
 

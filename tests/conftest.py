@@ -54,6 +54,19 @@ def rel_l1(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     return np.abs(a - b).sum(axis=0) / (a.shape[0] * s)
 
 
+def rel_l1_cons(a: np.ndarray, b: np.ndarray, gamma: float = 1.4) -> np.ndarray:
+    """The conventional relative L1 error per conserved variable (rho, rho u, rho v, rho E):
+    sum |U(a) - U(b)| / sum |U(b)| over the cells. Both momentum components are measured
+    against the momentum magnitude sum |rho V| of b, so that a component that is identically
+    zero (v in a 1-D problem) has a finite denominator."""
+    Ua = cons(a, gamma).reshape(-1, 4)
+    Ub = cons(b, gamma).reshape(-1, 4)
+    den = np.abs(Ub).sum(axis=0)
+    mom = np.hypot(Ub[:, 1], Ub[:, 2]).sum()
+    den[1] = den[2] = max(mom, 1e-300)
+    return np.abs(Ua - Ub).sum(axis=0) / den
+
+
 def cons(prim: np.ndarray, gamma: float = 1.4) -> np.ndarray:
     r, u, v, p = (prim[..., k] for k in range(4))
     return np.stack([r, r * u, r * v, p / (gamma - 1) + 0.5 * r * (u * u + v * v)], axis=-1)
