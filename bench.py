@@ -57,9 +57,14 @@ def parse():
     ap.add_argument("--form", default="fp32-flux", choices=["fp32-flux", "fp64"],
                     help="precision form of the headline leg (profiling of the plain FP64 kernel)")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrivals per second")
-    ap.add_argument("--serve-seconds", type=float, default=1.0, help="length of the arrival window")
-    ap.add_argument("--serve-iters", type=int, default=200, help="iteration cap (fixed end) per request")
-    ap.add_argument("--serve-gb", type=float, default=6.0, help="device-memory budget of the pools")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="length of the arrival window")
+    ap.add_argument("--serve-end", type=float, default=1.0e7,
+                    help="fixed end of a request: its cells x iterations budget (cell-updates)")
+    ap.add_argument("--serve-gb", type=float, default=24.0, help="device-memory budget of the pools")
+    ap.add_argument("--serve-seq", type=int, default=64, help="requests solved one after another in FP64")
+    ap.add_argument("--serve-distinct", type=int, default=512, help="distinct seeded payloads of the stream")
+    ap.add_argument("--serve-readback-gb", type=float, default=2.0,
+                    help="page-locked host buffer the results of each step call are read back into")
     return ap.parse_args()
 
 
@@ -176,32 +181,55 @@ def cpu_baseline(batch, budget_s=12.0):
                       f"{dt:.1f} s, C++ oracle -O3 OpenMP"}
 
 
-def serving_leg(args, lib):
-    """The served request stream: Poisson arrivals of planar ramps and quasi-2D nozzles with
-    log-normal sizes in [4e3, 2e6] cells, admitted by memory budget into one serving context
-    (FP32-flux / FP64-state), retired on a 1e-8 relative residual drop or at the iteration cap.
-    Beside it, a sample of the same requests solved one after another through the plain FP64
-    path (one context per request, wall clock including setup and read-back, as for serving).
-    The payloads of both are generated before the timed region; admission (validation, metrics,
-    upload) is timed."""
-    from q2d_b200 import _abi, make_options
+def serving_leg(args, lib, fp64_batched=None):
+    """The served request stream: Poisson arrivals (args.serve_rate per second over
+    args.serve_seconds) of planar ramps and quasi-2D nozzles with log-normal sizes in [4e3, 2e6]
+    cells, admitted by memory budget into one serving context (FP32-flux / FP64-state). A request
+    retires on a 1e-8 relative residual drop or at its fixed end, the iteration at which its
+    cells x iterations reach args.serve_end cell-updates; its state is read back to the host
+    before it is retired, inside its latency. Beside it, the first args.serve_seq requests of the
+    same stream solved one after another through the plain FP64 path with the same retirement
+    rule and read-back (one context per request, wall clock including setup). The payloads of
+    both come from the clients and are built before the timed region; admission (validation,
+    metrics, upload) is timed."""
+    from q2d_b200 import _abi
     from q2d_b200.serve import request_stream, serve, serve_options
     from q2d_b200.solver import Q2DSolver
-    reqs = request_stream(args.serve_rate, args.serve_seconds)
-    for r in reqs:   # the request payloads (grid, initial state, boundary records) come from clients
+    reqs = request_stream(args.serve_rate, args.serve_seconds, distinct=args.serve_distinct)
+    # the request payloads (grid, initial state, boundary records) come from clients: built before
+    # the timed region, one per distinct seeded case
+    for r in reqs[:args.serve_distinct]:
         r.build()
-    opts = serve_options(itermax=args.serve_iters, drop=1e-8)
-    st = serve(reqs, opts, device_bytes=int(args.serve_gb * (1 << 30)), max_cases=4096, steps_per_call=10)
-    # sequential plain FP64 on the first requests of the same stream
-    seq = request_stream(args.serve_rate, args.serve_seconds)[:8]
-    opts64 = serve_options(precision=_abi.PREC_FP64, itermax=args.serve_iters, drop=1e-8)
+    for r in reqs[args.serve_distinct:]:
+        r.case = reqs[r.rid % args.serve_distinct].case
+    bad = []
+
+    def sink(r, states):   # the client takes the result away (a spot check of each block)
+        if not all(np.isfinite(x[2:-2:7, 2:-2:7]).all() for x in states):
+            bad.append(r.rid)
+    import torch
+    rb = torch.empty(int(args.serve_readback_gb * (1 << 30)) // 8, dtype=torch.float64, pin_memory=True).numpy()
+    opts = serve_options(itermax=10 ** 9, drop=1e-8)
+    st = serve(reqs, opts, device_bytes=int(args.serve_gb * (1 << 30)), max_cases=4096, steps_per_call=10,
+               keep_results=True, end_cell_updates=args.serve_end, result_sink=sink, readback_buffer=rb)
+    del rb
+    st["nonfinite_results"] = len(bad)
+    st["distinct_payloads"] = args.serve_distinct
+    for r in reqs:
+        r.case = None
+    # sequential plain FP64 on the first requests of the same stream, same rule and read-back
+    seq = request_stream(args.serve_rate, args.serve_seconds, distinct=args.serve_distinct)[:args.serve_seq]
+    for r in seq:
+        r.build()
+    opts64 = serve_options(precision=_abi.PREC_FP64, itermax=10 ** 9, drop=1e-8)
     t0 = time.perf_counter()
     cu = 0
     for r in seq:
-        case = r.build()
+        case = r.case
         s = Q2DSolver(opts64, [case])
         try:
-            info = s.solve(steps_per_call=args.serve_iters)
+            end_iter = max(1, -(-int(args.serve_end) // case.cells))
+            info = s.step(end_iter)[0]
             _ = [s.prim(0, b) for b in range(len(case.blocks))]
             cu += case.cells * info["iter"]
         finally:
@@ -209,40 +237,105 @@ def serving_leg(args, lib):
     tseq = time.perf_counter() - t0
     seq_v = cu / tseq
     st.update({"arrival_rate_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,
-               "iteration_cap": args.serve_iters, "residual_drop": 1e-8, "budget_gb": args.serve_gb,
-               "dtype": "fp32-flux/fp64-state",
+               "end_cell_updates_per_request": args.serve_end, "residual_drop": 1e-8,
+               "budget_gb": args.serve_gb, "dtype": "fp32-flux/fp64-state", "readback": True,
                "sequential_plain_fp64": {"value": seq_v, "unit": UNIT, "requests": len(seq),
-                                         "cell_updates": cu, "seconds": tseq},
+                                         "cell_updates": cu, "seconds": tseq, "readback": True},
                "ratio_served_over_sequential_fp64": st["cell_updates_per_s"] / seq_v})
+    if fp64_batched:
+        st["ratio_served_over_batched_fp64"] = st["cell_updates_per_s"] / fp64_batched
     return st
 
 
-def accuracy_leg(batch):
-    """FP32-flux vs plain FP64 on the same cases after the same steps: relative L1 and L-inf
-    of the primitive variables (each variable over its own scale), worst case of the sample."""
+def _rel_l1(a, b, gamma=1.4):
+    """Relative L1 error per conserved variable, sum |U(a) - U(b)| / sum |U(b)| (both momenta
+    against sum |rho V|), and the same per primitive variable over its scale (max |b|)."""
+    def cons(p):
+        r, u, v, q = (p[..., k] for k in range(4))
+        return np.stack([r, r * u, r * v, q / (gamma - 1) + 0.5 * r * (u * u + v * v)], axis=-1).reshape(-1, 4)
+    Ua, Ub = cons(a), cons(b)
+    den = np.abs(Ub).sum(axis=0)
+    den[1] = den[2] = max(np.hypot(Ub[:, 1], Ub[:, 2]).sum(), 1e-300)
+    std = np.abs(Ua - Ub).sum(axis=0) / den
+    bb = b.reshape(-1, 4)
+    snd = np.sqrt(gamma * np.abs(bb[:, 3]) / np.abs(bb[:, 0]))
+    vs = max(np.abs(bb[:, 1]).max(), np.abs(bb[:, 2]).max(), snd.max())
+    sc = np.array([np.abs(bb[:, 0]).max(), vs, vs, np.abs(bb[:, 3]).max()])
+    d = np.abs(a.reshape(-1, 4) - bb) / sc
+    return float(std.max()), float(d.mean(axis=0).max()), float(d.max())
+
+
+def accuracy_leg(batch, n=512, steps=2000):
+    """The batched workload's FP32-flux error against the plain FP64 GPU path after the
+    configuration's 2000 steps, on the first n cases: relative L1 per conserved variable (the
+    north star's metric), the max-scaled relative L1 and L-inf of the primitive variables,
+    worst case of the sample."""
     from q2d_b200 import make_options
     from q2d_b200.solver import Q2DSolver
-    sample = batch[:64]
-    steps = 200
+    sample = batch[:n]
     out = []
     for prec in (1, 0):
         s = Q2DSolver(make_options(sample[0], precision=prec), sample)
         try:
-            s.step(steps)
-            out.append([s.prim(c, 0) for c in range(len(sample))])
+            for _ in range(steps // 500):
+                s.step(500)
+            if steps % 500:
+                s.step(steps % 500)
+            out.append([p[0] for p in s.prims()])
         finally:
             s.close()
-    l1 = linf = 0.0
-    for a, b in zip(out[0], out[1]):
-        bb = b.reshape(-1, 4)
-        snd = np.sqrt(1.4 * np.abs(bb[:, 3]) / np.abs(bb[:, 0]))
-        vs = max(np.abs(bb[:, 1]).max(), np.abs(bb[:, 2]).max(), snd.max())
-        sc = np.array([np.abs(bb[:, 0]).max(), vs, vs, np.abs(bb[:, 3]).max()])
-        d = np.abs(a.reshape(-1, 4) - bb) / sc
-        l1 = max(l1, float(d.mean(axis=0).max()))
-        linf = max(linf, float(d.max()))
+    errs = [_rel_l1(a, b) for a, b in zip(out[0], out[1])]
     return {"vs": "plain FP64 GPU path", "cases": len(sample), "steps": steps,
-            "rel_l1_max": l1, "rel_linf_max": linf}
+            "rel_l1_cons_max": max(e[0] for e in errs), "rel_l1_max": max(e[1] for e in errs),
+            "rel_linf_max": max(e[2] for e in errs)}
+
+
+def configs_leg(lib):
+    """Configurations 1-3 at their stated sizes: each solved in the plain FP64 form and in the
+    FP32-flux form, device time per step (CUDA events), cell-updates/s and the FP32-flux error
+    against FP64 at the end."""
+    from q2d_b200 import cases, make_options
+    from q2d_b200.solver import Q2DSolver
+
+    def solve(cs, prec, steps, chunk, **ov):
+        s = Q2DSolver(make_options(cs, precision=prec, **ov), [cs])
+        try:
+            s.step(1)
+            ms, _ = time_device(lib, s, 1)
+            info = s.info(0)
+            t0 = time.perf_counter()
+            done = 2
+            while done < steps and info["todo"] != 3:
+                info = s.step(min(chunk, steps - done))[0]
+                done = info["iter"]
+            wall = time.perf_counter() - t0
+            return [s.prim(0, b) for b in range(len(cs.blocks))], info, ms, wall
+        finally:
+            s.close()
+
+    out = {}
+    specs = [("1", cases.riemann_1d(), 10 ** 6, 1000, {},
+              "1-D Riemann 1024x4, minmod + HLLC, SSP-RK3, CFL 0.5, time accurate to t = 0.15"),
+             ("2", cases.ramp(), 4000, 500, {},
+              "compression ramp 1536x512, van Leer + HLLC, SSP-RK3, local dt, 4000 steps"),
+             ("3", cases.nozzle_axi(), 20000, 2000, {"cfl": 0.2, "res_relative": 1},
+              "axisymmetric nozzle 4 x 512x128, minmod + HLLC, SSP-RK3, local dt at CFL 0.2, 20000 "
+              "iterations (the residual stalls near 1e-3 of its peak: no 1e-10 drop)")]
+    for key, cs, steps, chunk, ov, what in specs:
+        res = {"workload": what, "cells": cs.cells}
+        states = {}
+        for name, prec in (("fp64", 0), ("fp32_flux", 1)):
+            P, info, ms, wall = solve(cs, prec, steps, chunk, **ov)
+            states[name] = P
+            res[name] = {"iterations": int(info["iter"]), "time": info["time"], "err": info["err"],
+                         "ms_per_step": ms, "cell_updates_per_s": cs.cells / (ms / 1e3),
+                         "residual_drop": info["residual"][0] / info["residual0"] if info["residual0"] > 0 else None,
+                         "wall_s": wall}
+        e = [_rel_l1(a, b) for a, b in zip(states["fp32_flux"], states["fp64"])]
+        res["fp32_flux_vs_fp64"] = {"rel_l1_cons_max": max(x[0] for x in e), "rel_l1_max": max(x[1] for x in e),
+                                    "rel_linf_max": max(x[2] for x in e)}
+        out[key] = res
+    return out
 
 
 WORKLOAD = ("batched area-variation nozzles (4096 independent cases per GPU, Nx~lognormal[64,1024], "
@@ -379,8 +472,9 @@ def main():
         sir.close()
     served = None
     if not args.no_serve:
-        served = serving_leg(args, lib)
+        served = serving_leg(args, lib, fp64["value"] if fp64 else None)
     accuracy = accuracy_leg(batch) if not args.no_fp64 else None
+    configs = configs_leg(lib) if not args.no_fp64 else None
     cpu = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline(batch)
@@ -403,6 +497,7 @@ def main():
         "gpu_launches": launches, "errors": errs,
         "clocks": clk.summary(),
         "e2e": e2e, "plain_fp64": fp64, "irs": irs, "served": served, "accuracy_fp32flux": accuracy,
+        "configs": configs,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)

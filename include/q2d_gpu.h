@@ -209,15 +209,17 @@ int  q2d_gpu_wait(q2d_ctx* ctx, q2d_step_info* out);
 int  q2d_gpu_prepare(q2d_ctx* ctx, int nsteps);
 
 /* Autotuner (no reference counterpart): times each candidate schedule of the stage kernels
- * (tile shape of the CTA-tile kernel, rows per item of the warp-marching kernel) for `steps`
- * steps on this context's workload, keeps the fastest and restores the state. *schedule gets
- * the chosen candidate index, *ms_per_step its time (either may be NULL). */
+ * (stage kernel and tile shape) for `steps` steps on this context's workload, keeps the fastest
+ * and restores the state. *schedule gets the chosen candidate index, *ms_per_step its time
+ * (either may be NULL). */
 int  q2d_gpu_autotune(q2d_ctx* ctx, int steps, int* schedule, float* ms_per_step);
 
 /* Pins the schedule of the stage kernels (the index the autotuner reports) without tuning:
- * 0-2 CTA-tile kernel on 32x10, 32x8, 64x4 tiles; 3-4 warp-marching kernel with 8 / 16 rows
- * per item; 5-9 FP32-flux tile kernel on 32x10, 32x8, 64x4 (256 threads) and 32x16, 64x8 (512
- * threads) tiles (FP32-flux form only; 5 is its default). q2d_gpu_get_schedule returns the current one. */
+ * 0-2 FP64 tile kernel on 32x10, 32x8, 64x4 tiles; 3-7 FP32-flux tile kernel on 32x10, 32x8,
+ * 64x4 (256 threads) and 32x16, 64x8 (512 threads) tiles (FP32-flux form only); 8 FP32-flux tile
+ * kernel in difference form on 32x8 tiles (FP32-flux form with HLLC, HLLE or LLF, without
+ * MUSCL-SD or residual smoothing; the default of those options). q2d_gpu_get_schedule returns
+ * the current one. */
 int  q2d_gpu_set_schedule(q2d_ctx* ctx, int schedule);
 int  q2d_gpu_get_schedule(const q2d_ctx* ctx);
 

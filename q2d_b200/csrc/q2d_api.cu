@@ -148,8 +148,8 @@ struct q2d_ctx {
     bool dirty = false;           // uploads, slot resets or list rebuild pending
     std::vector<int> reset_slots; // retired slots whose device run state still has to be reset
     int tile = 0;
-    int kernel = 0;       // 0: CTA-tile stage kernel, 1: warp-marching, 2: FP32-flux tile kernel
-    int march_h = 16;     // rows per warp-marching item
+    int kernel = 0;       // 0: FP64 tile stage kernel, 2: FP32-flux tile kernel, 3: FP32-flux
+                          // tile kernel in difference form
     int grid = 0;
     // device pools and their allocators
     DevBuf<double> PA, PB, PC, SC, DL, FI, FJ, PART;
@@ -236,12 +236,13 @@ StageArgs base_args(q2d_ctx* ctx) {
 // Mod_Explicit.f90:44-53); the other kernels, and global time stepping (which needs the minimum
 // over the case before any cell updates), compute it in the last stage of the previous step and
 // in the time-step passes of ensure_dt.
-bool dt_in_first_stage(const q2d_ctx* ctx) { return ctx->kernel == 2 && !ctx->opt.time_accurate; }
+bool dt_in_first_stage(const q2d_ctx* ctx) { return ctx->kernel >= 2 && !ctx->opt.time_accurate; }
 
-// Item partials per work item: one set per warp for the FP32-flux kernel (256 threads on tiles
-// 0-2, 512 on tiles 3-4, as launch_stage32 instantiates them), which ends its items without a
-// CTA-wide reduction and leaves the case finalisation to finalize_kernel; one otherwise.
-int part_stride(const q2d_ctx* ctx) { return ctx->kernel == 2 ? (ctx->tile >= 3 ? 16 : 8) : 1; }
+// Item partials per work item: one set per warp for the FP32-flux kernels (256 threads on tiles
+// 0-2, 512 on tiles 3-4, as launch_stage32 / launch_stage32d instantiate them), which end their
+// items without a CTA-wide reduction and leave the case finalisation to finalize_kernel; one
+// otherwise.
+int part_stride(const q2d_ctx* ctx) { return ctx->kernel >= 2 ? (ctx->tile >= 3 ? 16 : 8) : 1; }
 
 // RKcoeff (Lib_RK.f90:8-11)
 double rk_coeff(int n_rk, int irk) {
@@ -262,7 +263,7 @@ int enqueue_step(q2d_ctx* ctx, cudaStream_t s, int* nk) {
         a.last = irk == n_rk;
         a.dt_first = dt_in_first_stage(ctx) ? 1 : 0;
         a.part_stride = part_stride(ctx);
-        a.fin_sep = ctx->kernel == 2 ? 1 : 0;
+        a.fin_sep = ctx->kernel >= 2 ? 1 : 0;
         a.rk_c = rk_coeff(n_rk, irk);
         a.PO = ctx->PA.p;
         if (n_rk == 1) { a.Pin = ctx->PA.p; a.Pout = ctx->PB.p; }
@@ -275,8 +276,8 @@ int enqueue_step(q2d_ctx* ctx, cudaStream_t s, int* nk) {
             else { a.Pin = ctx->PC.p; a.Pout = ctx->PA.p; }
         }
         auto stage = [&](const StageArgs& x) -> int {
-            if (ctx->kernel == 1)
-                CK(launch_march(x, ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter, ctx->grid, s));
+            if (ctx->kernel == 3)
+                CK(launch_stage32d(x, ctx->opt.riemann, ctx->grid, s));
             else if (ctx->kernel == 2)
                 CK(launch_stage32(x, ctx->opt.riemann, ctx->tile, ctx->grid, s));
             else
@@ -326,8 +327,7 @@ int ensure_dt(q2d_ctx* ctx, bool force = false) {
         StageArgs a = base_args(ctx);
         a.Pin = ctx->PA.p;
         a.first = ctx->dt_valid ? 1 : 0;   // pending-only pass
-        if (ctx->kernel == 1) CK(launch_dt_march(a, ctx->grid, ctx->stream));
-        else CK(launch_dt(a, ctx->tile, ctx->grid, ctx->stream));
+        CK(launch_dt(a, ctx->tile, ctx->grid, ctx->stream));
         ctx->launches += 1;
     }
     ctx->dt_valid = true;
@@ -571,7 +571,7 @@ int prepare_case(q2d_ctx* ctx, int c) {
         for (int q = 0; q < 3; ++q) parallel_zero(S.fi, q * (size_t)pfi + nfi, (q + 1) * (size_t)pfi);
         for (int q = 0; q < 3; ++q) parallel_zero(S.fj, q * (size_t)pfj + nfj, (q + 1) * (size_t)pfj);
         if (fp32) {
-            for (int v = 0; v < 2; ++v) parallel_zero(S.dl32, v * (size_t)pg + ngh, (v + 1) * (size_t)pg);
+            parallel_zero(S.dl32, 2 * (size_t)ngh, 2 * (size_t)pg);
             parallel_zero(S.fi4, 4 * (size_t)nfi, 4 * (size_t)pfi);
             parallel_zero(S.fj4, 4 * (size_t)nfj, 4 * (size_t)pfj);
         }
@@ -596,8 +596,8 @@ int prepare_case(q2d_ctx* ctx, int c) {
                 S.dl[k] = G.dl[2 * k];
                 S.dl[pg + k] = G.dl[2 * k + 1];
                 if (fp32) {
-                    S.dl32[k] = (float)G.dl[2 * k];
-                    S.dl32[pg + k] = (float)G.dl[2 * k + 1];
+                    S.dl32[2 * k] = (float)G.dl[2 * k];   // interleaved: (dl(1), dl(2)) per frame cell
+                    S.dl32[2 * k + 1] = (float)G.dl[2 * k + 1];
                 }
             }
         });
@@ -685,14 +685,8 @@ int rebuild_device_lists(q2d_ctx* ctx) {
                         edges.push_back(e);
                     }
                 }
-                if (ctx->kernel == 1) {
-                    for (int i0 = 0; i0 < B.ni; i0 += kMarchCols)
-                        for (int j0 = 0; j0 < B.nj; j0 += ctx->march_h)
-                            items.push_back(WorkItem{gb, i0, j0, (int)c, std::min(B.nj, j0 + ctx->march_h), 0});
-                } else {
-                    for (int j0 = 0; j0 < B.nj; j0 += TY)
-                        for (int i0 = 0; i0 < B.ni; i0 += TX) items.push_back(WorkItem{gb, i0, j0, (int)c, 0, 0});
-                }
+                for (int j0 = 0; j0 < B.nj; j0 += TY)
+                    for (int i0 = 0; i0 < B.ni; i0 += TX) items.push_back(WorkItem{gb, i0, j0, (int)c, 0, 0});
             }
             dcases[c].ndir = ctx->blocks[cs.blocks[0]].nj == 1 ? 1 : 2;
         }
@@ -717,13 +711,11 @@ int rebuild_device_lists(q2d_ctx* ctx) {
         CK(cudaMemcpy(ctx->items.p, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->dcases.p, dcases.data(), sizeof(DCase) * dcases.size(), cudaMemcpyHostToDevice));
     ctx->n_items = (int)items.size();
-    if (ctx->kernel == 1) {
-        const int occ = std::max(1, march_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->opt.limiter));
-        ctx->grid = (int)std::min<long long>(((long long)items.size() + 3) / 4, (long long)occ * ctx->num_sms);
-    } else {
-        const int occ = std::max(1, ctx->kernel == 2 ? stage32_occupancy(ctx->opt.riemann, ctx->tile)
-                                                     : stage_occupancy(ctx->opt.precision, ctx->opt.riemann, ctx->tile,
-                                                                       ctx->opt.shock_detector));
+    {
+        const int occ = std::max(1, ctx->kernel == 3   ? stage32d_occupancy(ctx->opt.riemann)
+                                    : ctx->kernel == 2 ? stage32_occupancy(ctx->opt.riemann, ctx->tile)
+                                                       : stage_occupancy(ctx->opt.precision, ctx->opt.riemann,
+                                                                         ctx->tile, ctx->opt.shock_detector));
         ctx->grid = (int)std::min<long long>((long long)items.size(), (long long)occ * ctx->num_sms);
     }
     if (ctx->grid < 1) ctx->grid = 1;
@@ -801,27 +793,26 @@ int ready(q2d_ctx* ctx) {
 }
 
 // ---- autotuner ------------------------------------------------------------------------------
-// Times every schedule (stage-kernel tile shape or warp-marching rows per item) for `steps`
+// Times every schedule (stage kernel and tile shape) for `steps`
 // explicit steps on the context's own workload and keeps the fastest. The state, the scalar
 // planes (time steps) and the case states are saved before and restored after each candidate,
 // so tuning leaves the results unchanged.
-struct Schedule { int kernel, tile, march_h; };
-// Candidate schedules, indexed like the autotuner's result: CTA-tile stage kernel on tiles
-// 32x10, 32x8, 64x4; warp-marching kernel with 8 or 16 rows per item; FP32-flux tile kernel
-// on tiles 32x10, 32x8, 64x4 (256 threads) and 32x16, 64x8 (512 threads) (FP32-flux form only).
-const Schedule kSchedules[] = {{0, 0, 16}, {0, 1, 16}, {0, 2, 16}, {1, 0, 8}, {1, 0, 16},
-                               {2, 0, 16}, {2, 1, 16}, {2, 2, 16}, {2, 3, 16}, {2, 4, 16}};
+struct Schedule { int kernel, tile; };
+// Candidate schedules, indexed like the autotuner's result: FP64 tile stage kernel on tiles
+// 32x10, 32x8, 64x4; FP32-flux tile kernel on tiles 32x10, 32x8, 64x4 (256 threads) and 32x16,
+// 64x8 (512 threads); FP32-flux tile kernel in difference form on 32x8 (FP32-flux form only).
+const Schedule kSchedules[] = {{0, 0}, {0, 1}, {0, 2}, {2, 0}, {2, 1}, {2, 2}, {2, 3}, {2, 4}, {3, 1}};
 constexpr int kNumSchedules = (int)(sizeof(kSchedules) / sizeof(kSchedules[0]));
 
 bool schedule_allowed(const q2d_ctx* ctx, int k) {
-    if (kSchedules[k].kernel == 1 &&
-        (ctx->opt.irs_beta > 0.0 || ctx->opt.riemann > 2 || ctx->opt.shock_detector))
-        return false;   // the warp-marching kernel has no IRS passes, SLAU or shock sensor
     const bool sensor = ctx->opt.shock_detector || ctx->opt.riemann == Q2D_RIEMANN_HLLCP ||
                         ctx->opt.riemann == Q2D_RIEMANN_HLLEPP;
     if (kSchedules[k].kernel == 0 && sensor &&
         ctx->opt.precision != Q2D_PREC_FP64)
         return false;   // the shock sensor on the tile kernel: FP64 form only (FP32-flux: the FP32-flux kernel)
+    if (kSchedules[k].kernel == 3)   // difference form: HLLC / HLLE / LLF, no sensor, no smoothing
+        return ctx->opt.precision == Q2D_PREC_FP32_FLUX && ctx->opt.riemann <= 2 && !sensor &&
+               !(ctx->opt.irs_beta > 0.0);
     return kSchedules[k].kernel != 2 || ctx->opt.precision == Q2D_PREC_FP32_FLUX;
 }
 
@@ -849,7 +840,6 @@ int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
         CK(cudaStreamSynchronize(ctx->stream));
         ctx->kernel = cands[k].kernel;
         ctx->tile = cands[k].tile;
-        ctx->march_h = cands[k].march_h;
         if (int e = rebuild_device_lists(ctx)) return e;
         int nk = 0;
         if (int e = enqueue_step(ctx, ctx->stream, &nk)) return e;   // warm-up step
@@ -869,7 +859,6 @@ int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->kernel = cands[besti].kernel;
     ctx->tile = cands[besti].tile;
-    ctx->march_h = cands[besti].march_h;
     if (int e = rebuild_device_lists(ctx)) return e;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -955,7 +944,11 @@ q2d_ctx* new_ctx(const q2d_options* opt) {
         delete ctx;
         return nullptr;
     }
-    if (opt->precision == Q2D_PREC_FP32_FLUX) ctx->kernel = 2;   // default schedules 0 / 5
+    if (opt->precision == Q2D_PREC_FP32_FLUX) {   // default schedules 0 / 8 (difference form) / 3
+        const bool df = opt->riemann <= 2 && !opt->shock_detector && !(opt->irs_beta > 0.0);
+        ctx->kernel = df ? 3 : 2;
+        ctx->tile = df ? 1 : 0;
+    }
     return ctx;
 }
 
@@ -1247,16 +1240,13 @@ int q2d_gpu_set_schedule(q2d_ctx* ctx, int schedule) {
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->kernel = kSchedules[schedule].kernel;
     ctx->tile = kSchedules[schedule].tile;
-    ctx->march_h = kSchedules[schedule].march_h;
     return rebuild_device_lists(ctx);
 }
 
 int q2d_gpu_get_schedule(const q2d_ctx* ctx) {
     if (!ctx) return -1;
     for (int k = 0; k < kNumSchedules; ++k)
-        if (kSchedules[k].kernel == ctx->kernel && kSchedules[k].tile == ctx->tile &&
-            (ctx->kernel != 1 || kSchedules[k].march_h == ctx->march_h))
-            return k;
+        if (kSchedules[k].kernel == ctx->kernel && kSchedules[k].tile == ctx->tile) return k;
     return -1;
 }
 

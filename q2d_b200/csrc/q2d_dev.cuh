@@ -5,7 +5,8 @@
 //   state pools A, B, C    4 cell planes per block (rho, u, v, p), cell (i,j) at j*ni + i
 //   scalar pool            8 cell planes per block: sur, dtlocal, versor1 (x,y), versor2 (x,y),
 //                          source 0/1 (1/r for axisymmetric; Gx, Gy for area variation)
-//   dl pool                2 ghost-frame planes per block ((ni+4) x (nj+4), gc = 2)
+//   dl pool                2 ghost-frame planes per block ((ni+4) x (nj+4), gc = 2); its FP32
+//                          copy holds the same region with the two lengths interleaved per cell
 //   i-face / j-face pools  3 planes (nx, ny, int_l) on (ni+1) x nj and ni x (nj+1) faces
 //   node pool              2 planes (x, y) on (ni+1) x (nj+1) nodes
 // Index conventions follow the reference: face F of a row (0..ni) separates 1-based cells F
@@ -100,7 +101,8 @@ struct StageArgs {
     double* Pout;
     double* sc;            // scalar pool
     const double* dl;
-    const float* dl32;     // FP32 copy of the dl pool (FP32-flux form)
+    const float* dl32;     // FP32 copy of the dl pool (FP32-flux form), the two lengths of a
+                           // ghost-frame cell k interleaved at og + 2k (float2)
     const double* fi;
     const double* fj;
     const float4* fi4;     // FP32 copies of the face pools as (nx, ny, len, 0); a block's faces

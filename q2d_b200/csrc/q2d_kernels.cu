@@ -4,7 +4,6 @@
 // resumption, implicit residual smoothing, the end-of-step finalisation and the state transfers.
 // No spin-waits: cross-CTA ordering uses only atomic counters observed by the last CTA.
 #include "q2d_stage64.cuh"
-#include "q2d_march.cuh"
 
 #include <cfloat>
 #include <type_traits>
@@ -47,43 +46,6 @@ __global__ void __launch_bounds__(NT) dt_kernel(const StageArgs a) {
             for (int k = 0; k < 5; ++k) a.part[5 * (size_t)it + k] = tile_part[k];
         item_done<NT>(a, w.case_id, false, true, false, red, &s_flag);
     }
-}
-
-// Initial time step for warp-marching items (a warp per item: strip columns x rows).
-__global__ void __launch_bounds__(128) dt_march_kernel(const StageArgs a) {
-    const int lane = threadIdx.x & 31;
-    const int gw = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
-    const int nw = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
-    for (int it = gw; it < a.n_items; it += nw) {
-        const WorkItem w = a.items[it];
-        const DBlock B = a.blocks[w.block];
-        CaseState* cs = &a.cstate[w.case_id];
-        // a.first != 0: only cases admitted since the last pass (others keep their time step)
-        if (__ldcg(&cs->status) != kStatus_Running || (a.first && !__ldcg(&cs->dt_pending))) continue;
-        const long long iter_next = __ldcg(&cs->iter) + 1;
-        const int ndir = a.cases[w.case_id].ndir;
-        double acc[5] = {0.0, 0.0, 0.0, 0.0, 1e300};
-        const int ii = w.i0 + lane;
-        if (lane < kMarchCols && ii < B.ni) {
-            for (int jj = w.j0; jj < w.j1; ++jj) {
-                const long long cg = (long long)jj * B.ni + ii;
-                double P[4];
-                for (int v = 0; v < 4; ++v) P[v] = a.Pin[B.oc + v * B.pc + cg];
-                const long long gidx = B.og + (long long)(jj + 2) * (B.ni + 4) + (ii + 2);
-                const double* scb = a.sc + 2 * B.oc;
-                const double dtn = cell_dt(a, P, scb, cg, B.pc, a.dl[gidx], a.dl[gidx + B.pg], ndir, iter_next);
-                if (!a.time_accurate) a.sc[2 * B.oc + B.pc + cg] = dtn;
-                acc[4] = fmin(acc[4], dtn);
-            }
-        }
-        for (int o = 16; o > 0; o >>= 1) acc[4] = fmin(acc[4], __shfl_down_sync(kFull, acc[4], o));
-        warp_item_done(a, w.case_id, acc, it, false, true, false);
-    }
-}
-
-cudaError_t launch_dt_march(const StageArgs& a, int grid, cudaStream_t s) {
-    dt_march_kernel<<<grid, 128, 0, s>>>(a);
-    return cudaGetLastError();
 }
 
 // Copies the interior state B -> A for the single-stage (euler) scheme.
@@ -390,37 +352,6 @@ int stage32_occupancy(int riem, int tile) {
     if (riem == 6) return stage32_occupancy_r6(tile);
     if (riem >= 7) return stage32_occupancy_r7(tile);
     return stage32_occupancy_r0(tile);
-}
-
-#define Q2D_MARCH_DECL(P, R)                                                                  \
-    cudaError_t launch_march_p##P##_r##R(const StageArgs& a, int lim, int grid, cudaStream_t s); \
-    int march_occupancy_p##P##_r##R(int lim);
-Q2D_MARCH_DECL(0, 0) Q2D_MARCH_DECL(0, 1) Q2D_MARCH_DECL(0, 2)
-Q2D_MARCH_DECL(1, 0) Q2D_MARCH_DECL(1, 1) Q2D_MARCH_DECL(1, 2)
-#undef Q2D_MARCH_DECL
-
-cudaError_t launch_march(const StageArgs& a, int prec, int riem, int lim, int grid, cudaStream_t s) {
-    if (riem > 2) return cudaErrorInvalidValue;   // the warp-marching schedule has no SLAU instantiation
-    if (prec == 0) {
-        if (riem == 1) return launch_march_p0_r1(a, lim, grid, s);
-        if (riem == 2) return launch_march_p0_r2(a, lim, grid, s);
-        return launch_march_p0_r0(a, lim, grid, s);
-    }
-    if (riem == 1) return launch_march_p1_r1(a, lim, grid, s);
-    if (riem == 2) return launch_march_p1_r2(a, lim, grid, s);
-    return launch_march_p1_r0(a, lim, grid, s);
-}
-
-int march_occupancy(int prec, int riem, int lim) {
-    if (riem > 2) return 0;
-    if (prec == 0) {
-        if (riem == 1) return march_occupancy_p0_r1(lim);
-        if (riem == 2) return march_occupancy_p0_r2(lim);
-        return march_occupancy_p0_r0(lim);
-    }
-    if (riem == 1) return march_occupancy_p1_r1(lim);
-    if (riem == 2) return march_occupancy_p1_r2(lim);
-    return march_occupancy_p1_r0(lim);
 }
 
 }  // namespace q2d

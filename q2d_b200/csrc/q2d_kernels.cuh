@@ -18,11 +18,10 @@ int stage_occupancy_sd(int prec, int riem, int tile);
 // FP32-flux stage kernel (q2d_stage32.cuh) on the same tiles and work items.
 cudaError_t launch_stage32(const StageArgs& a, int riem, int tile, int grid, cudaStream_t s);
 int stage32_occupancy(int riem, int tile);
-// Warp-marching stage kernel (q2d_march.cuh): strips of 28 columns, item rows [j0, j1).
-constexpr int kMarchCols = 28;
-cudaError_t launch_march(const StageArgs& a, int prec, int riem, int lim, int grid, cudaStream_t s);
-int march_occupancy(int prec, int riem, int lim);
-cudaError_t launch_dt_march(const StageArgs& a, int grid, cudaStream_t s);
+// FP32-flux stage kernel in difference form (q2d_stage32d.cuh): HLLC / HLLE / LLF on 32 x 8 tiles
+// (tile id 1) of 256 threads, without MUSCL-SD or implicit residual smoothing.
+cudaError_t launch_stage32d(const StageArgs& a, int riem, int grid, cudaStream_t s);
+int stage32d_occupancy(int riem);
 cudaError_t launch_dt(const StageArgs& a, int tile, int grid, cudaStream_t s);
 cudaError_t launch_copy(const double* src, double* dst, long long n, int* flag, cudaStream_t s);
 // cell-interleaved (rho, u, v, p) <-> 4 planes of stride pc, n cells (state upload / download)

@@ -551,8 +551,9 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                     cp_async8(sC + (4 + v) * NC + k, a.Rin + B.oc + v * pc + cg);
                 }
                 if (a.last && !a.dt_first) {   // cell lengths of the next step's time step
-                    const float* dsrc = a.dl32 + B.og + (long long)(jj + 2) * (ni + 4) + (ii + 2);
-                    sD2[(row + 2) * W + (col + 2)] = make_float2(__ldg(dsrc), __ldg(dsrc + B.pg));
+                    const float2* dsrc = reinterpret_cast<const float2*>(a.dl32 + B.og) +
+                                         (long long)(jj + 2) * (ni + 4) + (ii + 2);
+                    sD2[(row + 2) * W + (col + 2)] = __ldg(dsrc);
                 }
             }
         } else {
@@ -622,10 +623,11 @@ __global__ void __launch_bounds__(NT, MB) stage32_kernel(const StageArgs a) {
                 const bool inner = cross && inI && inJ;
                 const bool indl = cross && ii >= -2 && ii <= ni + 1 && jj >= -2 && jj <= nj + 1;
                 const double* src = Pin + (inner ? (long long)jj * ni + ii : 0);
-                const float* dsrc = a.dl32 + B.og + (indl ? (long long)(jj + 2) * (ni + 4) + (ii + 2) : 0);
+                const float2* dsrc = reinterpret_cast<const float2*>(a.dl32 + B.og) +
+                                     (indl ? (long long)(jj + 2) * (ni + 4) + (ii + 2) : 0);
                 const double q0 = __ldg(src), q1 = __ldg(src + pc), q2 = __ldg(src + 2 * pc), q3 = __ldg(src + 3 * pc);
-                const float d0 = __ldg(dsrc), d1 = __ldg(dsrc + B.pg);
-                if (indl) sD2[idx] = make_float2(d0, d1);
+                const float2 d01 = __ldg(dsrc);
+                if (indl) sD2[idx] = d01;
                 if (inner) sP[idx] = make_float4((float)q0, (float)q1, (float)q2, (float)q3);
                 if (inner && r >= 2 && r < TY + 2 && c >= 2 && c < TX + 2) {   // the tile's own cells, FP64
                     const int kk = (r - 2) * TX + (c - 2);

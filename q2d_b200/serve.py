@@ -5,8 +5,9 @@ The reference solves one domain per process, from input files to TODO = END
 resident in one serving context (q2d_serve_* in include/q2d_gpu.h): requests that arrive
 while others run are admitted as case slots and device memory free up (FIFO, memory-budget
 admission), every resident case advances in the same captured step graphs, and a case is
-retired when its residual has dropped by the requested factor or it reaches its iteration
-cap (the fixed end), after its state has been read back.
+retired when its residual has dropped by the requested factor or it reaches its fixed end (the
+context's iteration cap, or a per-request budget of cell-updates), after its state has been read
+back when the caller keeps results.
 
 Admission does its host work (validation, metrics) while the GPU runs the previous steps; its
 device writes are applied at the next step call.
@@ -106,6 +107,38 @@ class ServeContext:
         self._check(self.lib.q2d_gpu_download_prim(self.ctx, bid.value, _abi.dptr(P)), "q2d_gpu_download_prim")
         return P[2:b.nj + 2, 2:b.ni + 2, :].copy()
 
+    def prims_many(self, cids: list, buffer: Optional[np.ndarray] = None) -> list:
+        """Interior states of several resident cases, [case][block] -> (nj, ni, 4), read back by
+        one many-block transfer (q2d_gpu_download_prim_many). With `buffer` (a float64 array,
+        best in page-locked memory) the ghosted arrays of the transfer are carved out of it while
+        it has room, so that the returned views stay valid until the buffer is reused."""
+        arrs, ids = [], []
+        used = 0
+        for cid in cids:
+            for k, b in enumerate(self.cases[cid].blocks):
+                bid = C.c_int()
+                self._check(self.lib.q2d_serve_block_id(self.ctx, cid, k + 1, C.byref(bid)), "q2d_serve_block_id")
+                n = (b.nj + 4) * (b.ni + 4) * 4
+                if buffer is not None and used + n <= buffer.size:
+                    arrs.append(buffer[used:used + n].reshape(b.nj + 4, b.ni + 4, 4))
+                    used += n
+                else:
+                    arrs.append(np.empty((b.nj + 4, b.ni + 4, 4)))
+                ids.append(bid.value)
+        if ids:
+            ptrs = (C.POINTER(C.c_double) * len(arrs))(*[_abi.dptr(a) for a in arrs])
+            idv = (C.c_int * len(ids))(*ids)
+            self._check(self.lib.q2d_gpu_download_prim_many(self.ctx, len(ids), idv, ptrs),
+                        "q2d_gpu_download_prim_many")
+        out, k = [], 0
+        for cid in cids:
+            row = []
+            for b in self.cases[cid].blocks:
+                row.append(arrs[k][2:b.nj + 2, 2:b.ni + 2, :])
+                k += 1
+            out.append(row)
+        return out
+
     def free_cells(self) -> int:
         return int(self.lib.q2d_serve_free_cells(self.ctx))
 
@@ -140,6 +173,7 @@ class Request:
     iters: int = 0
     residual_drop: float = math.nan
     err: int = 0
+    rule: str = ""               # why it retired: "drop", "end" or "error"
     rejected: bool = False
     result: Optional[list] = None
     meta: dict = field(default_factory=dict)
@@ -155,12 +189,23 @@ class Request:
     def latency(self) -> float:
         return self.done - self.arrival
 
+    @property
+    def queueing(self) -> float:
+        return self.admitted - self.arrival
+
+    @property
+    def service(self) -> float:
+        return self.done - self.admitted
+
 
 def request_stream(rate: float, duration: float, seed: int = BASE_SEED + 5, cells_lo: float = 4e3,
-                   cells_hi: float = 2e6, max_requests: Optional[int] = None) -> list:
+                   cells_hi: float = 2e6, max_requests: Optional[int] = None,
+                   distinct: Optional[int] = None) -> list:
     """Poisson arrivals at `rate` per second over `duration` seconds. Each request is a planar
     ramp or a quasi-2D nozzle (equal odds) with a log-normal cell count whose +-3 sigma range
-    is [cells_lo, cells_hi], clipped to it."""
+    is [cells_lo, cells_hi], clipped to it. With `distinct`, request k carries the payload
+    (kind, cells, seed) of request k mod distinct: a long stream replays that many distinct
+    seeded cases, so that their payloads can be held in host memory."""
     rng = np.random.default_rng(seed)
     mu = 0.5 * (math.log(cells_lo) + math.log(cells_hi))
     sigma = (math.log(cells_hi) - math.log(cells_lo)) / 6.0
@@ -172,6 +217,10 @@ def request_stream(rate: float, duration: float, seed: int = BASE_SEED + 5, cell
         cells = int(np.clip(rng.lognormal(mu, sigma), cells_lo, cells_hi))
         kind = "ramp" if rng.random() < 0.5 else "nozzle"
         out.append(Request(len(out), t, kind, cells, int(rng.integers(1 << 31))))
+    if distinct:
+        for r in out[distinct:]:
+            src = out[r.rid % distinct]
+            r.kind, r.cells, r.seed = src.kind, src.cells, src.seed
     return out
 
 
@@ -189,16 +238,27 @@ def serve_options(precision: int = _abi.PREC_FP32_FLUX, itermax: int = 2000, dro
 
 def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: int = 1024,
           steps_per_call: int = 10, keep_results: bool = False, lib=None, clock=time.perf_counter,
-          realtime: bool = True) -> dict:
+          realtime: bool = True, end_cell_updates: Optional[float] = None,
+          result_sink=None, readback_buffer: Optional[np.ndarray] = None) -> dict:
     """Runs the request loop until every request is retired (or rejected as larger than the
     whole budget). With realtime=False arrivals are taken as already due (a replay of a
-    backlog), which makes the admission order independent of host timing."""
+    backlog), which makes the admission order independent of host timing.
+
+    A request retires on the residual drop of the options, on an error, or at its fixed end:
+    the options' iteration cap or, with end_cell_updates, the iteration at which its cells
+    times its iterations first reach that budget (checked after each step call). With
+    keep_results the states of the cases retiring after a step call are read back in one
+    many-block transfer before they are retired; that read-back is inside their latency. The
+    states are kept in Request.result, or handed to result_sink(request, states) when given
+    (a client that takes the result away); with readback_buffer the states handed to the sink
+    are views into it, valid until the sink returns."""
     reqs = sorted(requests, key=lambda r: r.arrival)
     pending = deque(reqs)
     queue: deque = deque()
     active: dict = {}
     cell_updates = 0
     steps_calls = 0
+    readback_bytes = 0
     with ServeContext(options, device_bytes, max_cases, lib=lib) as sc:
         budget_cells = sc.free_cells()
         t0 = clock()
@@ -222,6 +282,8 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
                 if cid is None:
                     break
                 r.admitted = clock() - t0
+                if end_cell_updates is not None:
+                    r.meta["end_iter"] = max(1, math.ceil(end_cell_updates / case.cells))
                 active[cid] = r
                 queue.popleft()
 
@@ -239,29 +301,60 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
             admit_due()              # host work overlaps the steps in flight
             infos = sc.wait()
             busy += clock() - tb
+            leaving = []
             for cid in sorted(on_device):
                 inf = infos[cid]
-                if inf.todo == _abi.TODO_END or inf.err:
+                r = active[cid]
+                end_iter = r.meta.get("end_iter")
+                if inf.err:
+                    r.rule = "error"
+                elif inf.todo == _abi.TODO_END:
+                    r.rule = "end" if inf.iter >= options.itermax else "drop"
+                elif end_iter is not None and inf.iter >= end_iter:
+                    r.rule = "end"
+                else:
+                    continue
+                r.iters = int(inf.iter)
+                r.err = int(inf.err)
+                r.residual_drop = inf.residual[0] / inf.residual0 if inf.residual0 > 0 else math.nan
+                leaving.append(cid)
+            if leaving:
+                if keep_results:
+                    buf = readback_buffer if result_sink is not None else None
+                    for cid, res in zip(leaving, sc.prims_many(leaving, buf)):
+                        readback_bytes += sum(x.nbytes for x in res)
+                        if result_sink is not None:
+                            result_sink(active[cid], res)
+                        else:
+                            active[cid].result = res
+                for cid in leaving:
                     r = active.pop(cid)
-                    r.iters = int(inf.iter)
-                    r.err = int(inf.err)
-                    r.residual_drop = inf.residual[0] / inf.residual0 if inf.residual0 > 0 else math.nan
-                    if keep_results:
-                        r.result = [sc.prim(cid, b) for b in range(len(r.case.blocks))]
                     sc.retire(cid)
                     r.done = clock() - t0
                     cell_updates += r.case.cells * r.iters
-                    r.case = None if not keep_results else r.case
+                    r.case = None if not keep_results or result_sink is not None else r.case
         makespan = clock() - t0
         launches = sc.launches()
     done = [r for r in reqs if not r.rejected]
-    lat = np.array([r.latency for r in done]) if done else np.array([math.nan])
+
+    def pct(xs, q):
+        return float(np.percentile(np.array(xs), q)) if xs else math.nan
+    lat = [r.latency for r in done]
+    que = [r.queueing for r in done]
+    ser = [r.service for r in done]
+    rules = {k: sum(1 for r in done if r.rule == k) / max(1, len(done)) for k in ("drop", "end", "error")}
+    drops = [r.residual_drop for r in done if math.isfinite(r.residual_drop)]
     return {
         "requests": len(reqs), "served": len(done), "rejected": sum(r.rejected for r in reqs),
         "errors": sum(1 for r in done if r.err),
         "cell_updates": int(cell_updates), "makespan_s": makespan, "busy_s": busy,
         "cell_updates_per_s": cell_updates / makespan if makespan > 0 else math.nan,
-        "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
-        "mean_latency_s": float(lat.mean()), "step_calls": steps_calls, "gpu_launches": launches,
+        "p50_latency_s": pct(lat, 50), "p99_latency_s": pct(lat, 99),
+        "mean_latency_s": float(np.mean(lat)) if lat else math.nan,
+        "p50_queueing_s": pct(que, 50), "p99_queueing_s": pct(que, 99),
+        "p50_service_s": pct(ser, 50), "p99_service_s": pct(ser, 99),
+        "retired_by": rules, "median_residual_drop": pct(drops, 50),
+        "readback_bytes": int(readback_bytes),
+        "step_calls": steps_calls, "gpu_launches": launches,
         "budget_cells": int(budget_cells),
     }

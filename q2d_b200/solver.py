@@ -90,9 +90,9 @@ class Q2DSolver:
             raise Q2DError(st, f"{self.prefix}_step", str([o["err_at"] for o in out if o["err"]]))
         return out
 
-    SCHEDULES = ["tile 32x10", "tile 32x8", "tile 64x4", "march 28 cols x 8 rows", "march 28 cols x 16 rows",
+    SCHEDULES = ["tile 32x10", "tile 32x8", "tile 64x4",
                  "fp32-flux tile 32x10", "fp32-flux tile 32x8", "fp32-flux tile 64x4",
-                 "fp32-flux tile 32x16", "fp32-flux tile 64x8"]
+                 "fp32-flux tile 32x16", "fp32-flux tile 64x8", "fp32-flux difference tile 32x8"]
 
     def set_schedule(self, schedule) -> None:
         """Pins a schedule (index or name from SCHEDULES) without tuning (q2d_gpu_set_schedule)."""

@@ -25,7 +25,8 @@ from tests.helpers import run_pair
 pytestmark = pytest.mark.gpu
 
 FP64_SCHEDULES = ["tile 32x10", "tile 32x8", "tile 64x4"]
-FP32_SCHEDULES = ["fp32-flux tile 32x10", "fp32-flux tile 32x8", "fp32-flux tile 64x4"]
+FP32_SCHEDULES = ["fp32-flux tile 32x10", "fp32-flux tile 32x8", "fp32-flux tile 64x4",
+                  "fp32-flux difference tile 32x8"]
 
 
 def outflow_case(kind: str):

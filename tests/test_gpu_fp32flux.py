@@ -19,7 +19,8 @@ pytestmark = pytest.mark.gpu
 
 L1_TOL = 1e-6
 LINF_TOL = 1e-4
-SCHED = ["fp32-flux tile 32x10", "fp32-flux tile 32x8", "fp32-flux tile 64x4", "tile 32x10"]
+SCHED = ["fp32-flux tile 32x10", "fp32-flux tile 32x8", "fp32-flux tile 64x4", "tile 32x10",
+         "fp32-flux difference tile 32x8"]
 
 
 def run(cs_list, steps, schedule=None, **ov):
@@ -115,7 +116,7 @@ def test_fp32flux_state_independent_of_tile():
     for ca, cb in zip(again, ref):
         for xa, xb in zip(ca, cb):
             assert np.array_equal(xa, xb)
-    for sch in (SCHED[1], SCHED[2], "fp32-flux tile 32x16", "fp32-flux tile 64x8"):
+    for sch in (SCHED[1], SCHED[2], "fp32-flux tile 32x16", "fp32-flux tile 64x8", SCHED[4]):
         got, _ = run(batch, 30, schedule=sch, precision=1)
         compare(got, ref, sch)
 

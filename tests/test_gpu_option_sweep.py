@@ -50,7 +50,7 @@ def test_option_sweep_fp32flux_vs_fp64(developed, k, d):   # noqa: F811
     from q2d_b200.solver import Q2DSolver
     from tests.conftest import rel_l1
     d = dict(d)
-    case, sch = d.pop("case"), 5 + k % 5
+    case, sch = d.pop("case"), 3 + k % 5
     d.pop("schedule")
     cs = developed[1] if case == 0 else cases.nozzle_axi(ni=36, nj=10, nblocks=2, seed=60 + k)
     if "up" in d["riemann"]:
