@@ -299,13 +299,13 @@ __device__ __forceinline__ void bc_symmetry_df(int Fm, const double* Bp, const d
 
 }  // namespace dform
 
-template <int RIEM, int TX, int TY, int NT, int MB>
+template <int RIEM, int LIM, int TX, int TY, int NT, int MB>
 __global__ void __launch_bounds__(NT, MB) stage32d_kernel(const StageArgs a) {
     using namespace dform;
     using L = TileD<TX, TY>;
     constexpr int HR = L::HR, RW = L::RW, RGI = L::RGI, RGJ = L::RGJ, RO = L::RO, PS = L::PS;
     constexpr int NFI = L::NFI, NF = L::NF, NC = L::NC;
-    static_assert(TX == 32 && NT % 32 == 0 && NT >= NC && 5 * HR + 3 * TY + 3 * (TY + 1) <= NT && L::NOWN * TY <= NT,
+    static_assert(TX == 32 && NT % 32 == 0 && NT >= NC && 5 * HR + 3 * TY + 3 * (TY + 1) <= NT && L::NOWN * TY < NT,
                   "one cell and at most one copy of each group per thread");
     static_assert(NT / 32 >= TY && NT / 32 >= 4, "a warp per tile row, and warps for the third face pass");
     static_assert(4 * TY + 4 * TX <= NT, "one ghost slot per thread");
@@ -321,6 +321,10 @@ __global__ void __launch_bounds__(NT, MB) stage32d_kernel(const StageArgs a) {
     // after the previous tile's end, so both usually land before they are needed
     __shared__ unsigned long long barS, barO;
     __shared__ int shS[2][HR], shD[2][HR], shGI[2][TY], shGJ[2][TY + 1], shO[2][TY];   // row shifts by slot
+    // the first 80 bytes of the item's CaseState (dt_step at 0, iter at 72), copied with the own rows
+    __shared__ __align__(16) double sCase[2][10];
+    static_assert(sizeof(CaseState) % 16 == 0 && offsetof(CaseState, dt_step) == 0 && offsetof(CaseState, iter) == 72,
+                  "CaseState head copied in one 80-byte bulk copy");
     __shared__ WorkItem sW[2];
     __shared__ DBlock sBk[2];
     __shared__ int sSt[2];
@@ -414,6 +418,10 @@ __global__ void __launch_bounds__(NT, MB) stage32d_kernel(const StageArgs a) {
                 rc = row_copy(reinterpret_cast<const char*>(plane), (long long)(j0 + r) * ni + i0, ncol, 8);
             dst = sO + k * L::PO + r * RO;
             if (k == 4) shO[sl][r] = rc.bytes ? rc.shift : 0;
+        } else if (t == L::NOWN * TY) {   // the case's time step and iteration
+            rc.src = &a.cstate[w.case_id];
+            rc.bytes = 80u;
+            dst = sCase[sl];
         }
         if (rc.bytes) {
             mbar_arrive_expect_tx(&barO, rc.bytes);
@@ -467,9 +475,6 @@ __global__ void __launch_bounds__(NT, MB) stage32d_kernel(const StageArgs a) {
         // ---- 1. loads: one bulk copy per staged row (unless the last iteration issued them) ----
         if (!s_pre) issue_stencil(w, B, cur);
         if (!o_pre) issue_own(w, B, cur);
-        // the case's time step and iteration (read by the cell phase), in flight with the copies
-        const double dt_case = __ldcg(&cs->dt_step);
-        const long long iter_now = __ldcg(&cs->iter);
         // The thread's ghost slot (one ghost cell the tile's stencils read beyond a block edge:
         // two layers of i-ghosts beside the tile rows, two of j-ghosts beside its columns), its
         // boundary record and boundary-face normal, and a connection ghost's donor value, while
@@ -626,15 +631,7 @@ __global__ void __launch_bounds__(NT, MB) stage32d_kernel(const StageArgs a) {
             const float* dlf = reinterpret_cast<const float*>(sD) + (idir ? 0 : 1);
             double X[4];
             bool ok;
-            switch (a.limiter) {
-                case 0: ok = face_df<RIEM, 0, PS>(sS, o0, o1, o2, o3, dlf, e0, e1, e2, e3, nx, ny, ln, g, gam, gm1, gf, X); break;
-                case 1: ok = face_df<RIEM, 1, PS>(sS, o0, o1, o2, o3, dlf, e0, e1, e2, e3, nx, ny, ln, g, gam, gm1, gf, X); break;
-                case 2: ok = face_df<RIEM, 2, PS>(sS, o0, o1, o2, o3, dlf, e0, e1, e2, e3, nx, ny, ln, g, gam, gm1, gf, X); break;
-                case 3: ok = face_df<RIEM, 3, PS>(sS, o0, o1, o2, o3, dlf, e0, e1, e2, e3, nx, ny, ln, g, gam, gm1, gf, X); break;
-                case 4: ok = face_df<RIEM, 4, PS>(sS, o0, o1, o2, o3, dlf, e0, e1, e2, e3, nx, ny, ln, g, gam, gm1, gf, X); break;
-                case 5: ok = face_df<RIEM, 5, PS>(sS, o0, o1, o2, o3, dlf, e0, e1, e2, e3, nx, ny, ln, g, gam, gm1, gf, X); break;
-                default: ok = face_df<RIEM, 6, PS>(sS, o0, o1, o2, o3, dlf, e0, e1, e2, e3, nx, ny, ln, g, gam, gm1, gf, X); break;
-            }
+            ok = face_df<RIEM, LIM, PS>(sS, o0, o1, o2, o3, dlf, e0, e1, e2, e3, nx, ny, ln, g, gam, gm1, gf, X);
             if (!ok) record_error(cs, 4, B.local_b, ei, ej, a.irk);
 #pragma unroll
             for (int v = 0; v < 4; ++v) sF[v * NF + slot] = X[v];
@@ -669,15 +666,7 @@ __global__ void __launch_bounds__(NT, MB) stage32d_kernel(const StageArgs a) {
                 if (sgn * un >= 0.0) sym = true;
             }
             if (sym) {
-                switch (a.limiter) {
-                    case 0: bc_symmetry_df<RIEM, 0>(Fm, Bq, Iq, dlb, dli, nx, ny, ln, g, gam, gm1, gf, X); break;
-                    case 1: bc_symmetry_df<RIEM, 1>(Fm, Bq, Iq, dlb, dli, nx, ny, ln, g, gam, gm1, gf, X); break;
-                    case 2: bc_symmetry_df<RIEM, 2>(Fm, Bq, Iq, dlb, dli, nx, ny, ln, g, gam, gm1, gf, X); break;
-                    case 3: bc_symmetry_df<RIEM, 3>(Fm, Bq, Iq, dlb, dli, nx, ny, ln, g, gam, gm1, gf, X); break;
-                    case 4: bc_symmetry_df<RIEM, 4>(Fm, Bq, Iq, dlb, dli, nx, ny, ln, g, gam, gm1, gf, X); break;
-                    case 5: bc_symmetry_df<RIEM, 5>(Fm, Bq, Iq, dlb, dli, nx, ny, ln, g, gam, gm1, gf, X); break;
-                    default: bc_symmetry_df<RIEM, 6>(Fm, Bq, Iq, dlb, dli, nx, ny, ln, g, gam, gm1, gf, X); break;
-                }
+                bc_symmetry_df<RIEM, LIM>(Fm, Bq, Iq, dlb, dli, nx, ny, ln, g, gam, gm1, gf, X);
             } else if (btype != 400 && btype > 0) {
                 // inflow / outflow records in FP64 from the FP64 state (the reference's routines);
                 // the flux through an inlet is the large term of a nozzle's balance
@@ -722,7 +711,9 @@ __global__ void __launch_bounds__(NT, MB) stage32d_kernel(const StageArgs a) {
 
         // ---- 4. residual, sources, RK update (+ time step and residual norm) --------------------
         double acc[5] = {0.0, 0.0, 0.0, 0.0, 1e300};
-        const long long iter_dt = iter_now + (dt_here || a.first ? 1 : 0) + (dt_here ? 0 : 1);
+        const double dt_case = sCase[cur][0];   // CaseState.dt_step
+        const long long iter_dt = *reinterpret_cast<const long long*>(&sCase[cur][9]) + (dt_here || a.first ? 1 : 0) +
+                                  (dt_here ? 0 : 1);   // CaseState.iter
         if (mine) {
             const int ii = i0 + col, jj = j0 + row;
             const long long cg = (long long)jj * ni + ii;
@@ -856,10 +847,10 @@ __global__ void __launch_bounds__(NT, MB) stage32d_kernel(const StageArgs a) {
     }
 }
 
-template <int RIEM, int TX, int TY, int NT, int MB>
-cudaError_t launch_stage32d_t(const StageArgs& a, int grid, cudaStream_t s) {
+template <int RIEM, int LIM, int TX, int TY, int NT, int MB>
+cudaError_t launch_stage32d_l(const StageArgs& a, int grid, cudaStream_t s) {
     constexpr size_t smem = dform::TileD<TX, TY>::bytes;
-    auto k = stage32d_kernel<RIEM, TX, TY, NT, MB>;
+    auto k = stage32d_kernel<RIEM, LIM, TX, TY, NT, MB>;
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -870,10 +861,24 @@ cudaError_t launch_stage32d_t(const StageArgs& a, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// One instantiation per limiter (a.limiter), so that each kernel holds one copy of the face code.
+template <int RIEM, int TX, int TY, int NT, int MB>
+cudaError_t launch_stage32d_t(const StageArgs& a, int grid, cudaStream_t s) {
+    switch (a.limiter) {
+        case 0: return launch_stage32d_l<RIEM, 0, TX, TY, NT, MB>(a, grid, s);
+        case 1: return launch_stage32d_l<RIEM, 1, TX, TY, NT, MB>(a, grid, s);
+        case 2: return launch_stage32d_l<RIEM, 2, TX, TY, NT, MB>(a, grid, s);
+        case 3: return launch_stage32d_l<RIEM, 3, TX, TY, NT, MB>(a, grid, s);
+        case 4: return launch_stage32d_l<RIEM, 4, TX, TY, NT, MB>(a, grid, s);
+        case 5: return launch_stage32d_l<RIEM, 5, TX, TY, NT, MB>(a, grid, s);
+        default: return launch_stage32d_l<RIEM, 6, TX, TY, NT, MB>(a, grid, s);
+    }
+}
+
 template <int RIEM, int TX, int TY, int NT, int MB>
 int stage32d_occupancy_t() {
     constexpr size_t smem = dform::TileD<TX, TY>::bytes;
-    auto k = stage32d_kernel<RIEM, TX, TY, NT, MB>;
+    auto k = stage32d_kernel<RIEM, 2, TX, TY, NT, MB>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, NT, smem);

@@ -110,12 +110,29 @@ bool to_bool(const std::string& v, const std::string& what) {
     die(what + ": not a logical: '" + v + "'");
 }
 
+// A point probe (IO_Probes.f90, registered by Register_IO.f90:44-82): its output file
+// OUTPUT/<file>.txt, the variables written, the iteration and time frequencies, and its cell
+// (block, i, j, 1-based), given or placed at the grid node nearest to `position`.
+struct Probe {
+    std::string file;
+    std::vector<std::string> vars;
+    double dtime = 1e30;
+    long long diter = 1000000000;
+    int b = 0, i = 0, j = 0;
+    double x = 0.0, y = 0.0;
+    long long ntime = 1;
+    FILE* f = nullptr;
+};
+
 struct Setup {
     q2d_options opt;
     std::vector<std::string> unsupported;   // keys or values outside the built path
     int shell_diter = 1;
     bool area = false;
     bool newrun = true;   // newrun = false: restart from OUTPUT/field.tec (Register_Sim_Param.f90:26)
+    bool sol_overwrite = true;   // sol-overwrite (Register_IO.f90:28)
+    std::string sol_format = "tecplot ascii";   // sol-format (Register_IO.f90:24)
+    std::vector<Probe> probes;
     std::string limiter_name, riemann_name, scheme_name, source_name;
 };
 
@@ -201,9 +218,55 @@ Setup read_options(const Ini& ini) {
     if (const std::string* v = ini_get(ini, "IO", "sol-diter")) o.sol_diter = (int)std::min<long long>(to_int(*v, "sol-diter"), 1000000000);
     if (const std::string* v = ini_get(ini, "IO", "sol-dtime")) o.sol_dtime = to_double(*v, "sol-dtime");
     if (const std::string* v = ini_get(ini, "IO", "shell-diter")) s.shell_diter = (int)to_int(*v, "shell-diter");
-    for (const char* k : {"ini-format", "sol-format"})   // Register_IO.f90:23-24: ASCII Tecplot only here
-        if (const std::string* v = ini_get(ini, "IO", k))
-            if (lower(*v) != "tecplot ascii") s.unsupported.push_back(std::string("[Q2D-IO] ") + k + " = " + *v);
+    // Register_IO.f90:23-28: initial conditions in ASCII Tecplot; solutions in ASCII Tecplot or
+    // VTK (ascii, raw)
+    if (const std::string* v = ini_get(ini, "IO", "ini-format"))
+        if (lower(*v) != "tecplot ascii") s.unsupported.push_back("[Q2D-IO] ini-format = " + *v);
+    if (const std::string* v = ini_get(ini, "IO", "sol-format")) {
+        const std::string t = lower(*v);
+        if (t == "tecplot ascii" || t == "vtk ascii" || t == "vtk raw") s.sol_format = t;
+        else s.unsupported.push_back("[Q2D-IO] sol-format = " + *v);
+    }
+    if (const std::string* v = ini_get(ini, "IO", "sol-overwrite")) s.sol_overwrite = to_bool(*v, "sol-overwrite");
+    // [Q2D-Probes] probe1, probe2, ... name sections of their own (Backend_INI.f90:65-75,
+    // Register_IO.f90:44-82)
+    if (ini.count("Q2D-Probes")) {
+        for (int n = 1;; ++n) {
+            const std::string* name = ini_get(ini, "Probes", "probe" + std::to_string(n));
+            if (!name) break;
+            Probe pr;
+            pr.file = *name;
+            auto sec = ini.find(*name);
+            auto get = [&](const char* k) -> const std::string* {
+                if (sec == ini.end()) return nullptr;
+                auto it = sec->second.find(k);
+                return it == sec->second.end() ? nullptr : &it->second;
+            };
+            if (const std::string* v = get("variables")) {
+                std::istringstream is(*v);
+                std::string w;
+                while (is >> w) pr.vars.push_back(w);
+            }
+            for (const std::string& w : pr.vars)
+                if (w != "rho(1)" && w != "u" && w != "v" && w != "p" && w != "T" && w != "M")
+                    die("probe " + *name + ": unknown variable '" + w + "'");
+            if (const std::string* v = get("dtime")) pr.dtime = to_double(*v, "dtime");
+            if (const std::string* v = get("diter")) pr.diter = to_int(*v, "diter");
+            if (pr.diter < 1 || !(pr.dtime > 0.0)) die("probe " + *name + ": dtime and diter must be > 0");
+            if (const std::string* v = get("index-position")) {
+                std::istringstream is(*v);
+                if (!(is >> pr.b >> pr.i >> pr.j)) die("probe " + *name + ": index-position needs b i j");
+            }
+            if (const std::string* v = get("position")) {
+                std::istringstream is(*v);
+                std::string a, b;
+                if (!(is >> a >> b)) die("probe " + *name + ": position needs x y");
+                pr.x = to_double(a, "position");
+                pr.y = to_double(b, "position");
+            }
+            s.probes.push_back(pr);
+        }
+    }
     s.source_name = "none";
     if (const std::string* v = ini_get(ini, "Sources", "active")) {
         s.source_name = *v;
@@ -558,6 +621,115 @@ void write_tec(const std::string& path, const std::vector<Block>& blocks, const 
     std::fclose(f);
 }
 
+// Cell (i, j) (1-based) of a ghosted reference-layout array P(4, -1:ni+2, -1:nj+2).
+inline const double* cell_at(const std::vector<double>& P, int ni, int i, int j) {
+    return &P[4 * ((size_t)(i + 1) + (size_t)(ni + 4) * (j + 1))];
+}
+
+// VTK XML structured grids (Write_vtk_tec, IO_Solution.f90:234-326, sol-format 'vtk ascii' or
+// 'vtk raw'): one OUTPUT/vtk/<stem>_Block<b>.vts per block with the node coordinates and the cell
+// variables rho(1), u, v, p, T (the reference's Ovarnames, T = p / (rho R)), and the multiblock
+// index OUTPUT/<stem>.vtm; the time as field data.
+void write_vtk(const std::string& outdir, const std::string& stem, const std::vector<Block>& blocks,
+               const std::vector<std::vector<double>>& P, double time, double R, bool raw) {
+    const std::string vdir = outdir + "/vtk";
+    if (std::system(("mkdir -p '" + vdir + "'").c_str()) != 0) die("cannot create " + vdir);
+    static const char* names[5] = {"rho(1)", "u", "v", "p", "T"};
+    for (size_t b = 0; b < blocks.size(); ++b) {
+        const Block& B = blocks[b];
+        const std::string path = vdir + "/" + stem + "_Block" + std::to_string(b + 1) + ".vts";
+        FILE* f = std::fopen(path.c_str(), "wb");
+        if (!f) die("cannot write " + path);
+        const size_t nn = (size_t)(B.ni + 1) * (B.nj + 1), nc = (size_t)B.ni * B.nj;
+        std::vector<std::vector<double>> arrays;   // points (3 per node), then the cell variables
+        arrays.emplace_back(3 * nn);
+        for (size_t k = 0; k < nn; ++k) {
+            arrays[0][3 * k] = B.nodes[2 * k];
+            arrays[0][3 * k + 1] = B.nodes[2 * k + 1];
+            arrays[0][3 * k + 2] = 0.0;
+        }
+        for (int v = 0; v < 5; ++v) {
+            std::vector<double> a(nc);
+            for (int j = 0; j < B.nj; ++j)
+                for (int i = 0; i < B.ni; ++i) {
+                    const double* q = cell_at(P[b], B.ni, i + 1, j + 1);
+                    a[(size_t)j * B.ni + i] = v < 4 ? q[v] : q[3] / (q[0] * R);
+                }
+            arrays.push_back(std::move(a));
+        }
+        std::fprintf(f, "<?xml version=\"1.0\"?>\n<VTKFile type=\"StructuredGrid\" version=\"1.0\" "
+                        "byte_order=\"LittleEndian\" header_type=\"UInt64\">\n");
+        std::fprintf(f, "  <StructuredGrid WholeExtent=\"0 %d 0 %d 0 0\">\n", B.ni, B.nj);
+        std::fprintf(f, "    <FieldData>\n      <DataArray type=\"Float64\" Name=\"TIME\" NumberOfTuples=\"1\" "
+                        "format=\"ascii\">%.17E</DataArray>\n    </FieldData>\n", time);
+        std::fprintf(f, "    <Piece Extent=\"0 %d 0 %d 0 0\">\n", B.ni, B.nj);
+        unsigned long long offset = 0;
+        auto array = [&](size_t k, const char* name, int ncomp) {
+            std::fprintf(f, "        <DataArray type=\"Float64\"");
+            if (name) std::fprintf(f, " Name=\"%s\"", name);
+            if (ncomp > 1) std::fprintf(f, " NumberOfComponents=\"%d\"", ncomp);
+            if (raw) {
+                std::fprintf(f, " format=\"appended\" offset=\"%llu\"/>\n", offset);
+                offset += 8 + 8 * arrays[k].size();
+                return;
+            }
+            std::fprintf(f, " format=\"ascii\">\n");
+            for (size_t q = 0; q < arrays[k].size(); ++q) std::fprintf(f, " %.17E\n", arrays[k][q]);
+            std::fprintf(f, "        </DataArray>\n");
+        };
+        std::fprintf(f, "      <Points>\n");
+        array(0, nullptr, 3);
+        std::fprintf(f, "      </Points>\n      <CellData>\n");
+        for (int v = 0; v < 5; ++v) array(1 + v, names[v], 1);
+        std::fprintf(f, "      </CellData>\n    </Piece>\n  </StructuredGrid>\n");
+        if (raw) {
+            std::fprintf(f, "  <AppendedData encoding=\"raw\">\n_");
+            for (const std::vector<double>& a : arrays) {
+                const unsigned long long nb = 8ull * a.size();
+                std::fwrite(&nb, sizeof nb, 1, f);
+                std::fwrite(a.data(), sizeof(double), a.size(), f);
+            }
+            std::fprintf(f, "\n  </AppendedData>\n");
+        }
+        std::fprintf(f, "</VTKFile>\n");
+        std::fclose(f);
+    }
+    const std::string vtm = outdir + "/" + stem + ".vtm";
+    FILE* f = std::fopen(vtm.c_str(), "w");
+    if (!f) die("cannot write " + vtm);
+    std::fprintf(f, "<?xml version=\"1.0\"?>\n<VTKFile type=\"vtkMultiBlockDataSet\" version=\"1.0\" "
+                    "byte_order=\"LittleEndian\" header_type=\"UInt64\">\n  <vtkMultiBlockDataSet>\n");
+    for (size_t b = 0; b < blocks.size(); ++b)
+        std::fprintf(f, "    <DataSet index=\"%zu\" name=\"Block%zu\" file=\"vtk/%s_Block%zu.vts\"/>\n", b, b + 1,
+                     stem.c_str(), b + 1);
+    std::fprintf(f, "  </vtkMultiBlockDataSet>\n</VTKFile>\n");
+    std::fclose(f);
+}
+
+// gfortran list-directed output (write(unit, *)) of an integer and of a REAL(8): I12, and 17
+// significant digits in F form for 0.1 <= |x| < 1e16, E form with a 3-digit exponent otherwise.
+std::string ld_int(long long v) {
+    char b[32];
+    std::snprintf(b, sizeof b, "%12lld", v);
+    return b;
+}
+std::string ld_real(double v) {
+    char b[64];
+    const double a = std::fabs(v);
+    if (v == 0.0 || (a >= 0.1 && a < 1e16)) {
+        const int e = v == 0.0 ? 0 : (int)std::floor(std::log10(a));
+        std::snprintf(b, sizeof b, "%*.*f     ", 21, std::max(0, 16 - e), v);
+    } else {
+        char m[40];
+        std::snprintf(m, sizeof m, "%.16E", v);
+        char* ep = std::strchr(m, 'E');
+        const int ex = std::atoi(ep + 1);
+        *ep = 0;
+        std::snprintf(b, sizeof b, "%24sE%c%03d", m, ex < 0 ? '-' : '+', ex < 0 ? -ex : ex);
+    }
+    return std::string(" ") + b;
+}
+
 void json_str(FILE* f, const std::string& s) {
     std::fputc('"', f);
     for (char c : s) {
@@ -601,6 +773,31 @@ Args parse_args(int argc, char** argv) {
     return a;
 }
 
+// Setup_Probes (IO_Probes.f90:43-114): a probe without an index position sits at the grid node
+// nearest to its position (Place, :118-136: nodes i = 1..ni, j = 0..nj of every block, the first
+// nearest in block, j, i order); its cell is (b, i, j) of that node. A row-0 node reads the
+// boundary cell (j = 1): the ghost row the reference would read is not kept.
+void place_probes(std::vector<Probe>& probes, const std::vector<Block>& blocks) {
+    for (Probe& pr : probes) {
+        if (pr.b == 0 && pr.i == 0 && pr.j == 0) {
+            double d0 = HUGE_VAL;
+            for (size_t b = 0; b < blocks.size(); ++b) {
+                const Block& B = blocks[b];
+                for (int j = 0; j <= B.nj; ++j)
+                    for (int i = 1; i <= B.ni; ++i) {
+                        const double* xy = &B.nodes[2 * ((size_t)j * (B.ni + 1) + i)];
+                        const double d = std::hypot(pr.x - xy[0], pr.y - xy[1]);
+                        if (d < d0) { d0 = d; pr.b = (int)b + 1; pr.i = i; pr.j = j; }
+                    }
+            }
+        }
+        if (pr.b < 1 || pr.b > (int)blocks.size() || pr.i < 1 || pr.i > blocks[pr.b - 1].ni || pr.j < 0 ||
+            pr.j > blocks[pr.b - 1].nj)
+            die("probe " + pr.file + ": cell outside the grid");
+        if (pr.j == 0) pr.j = 1;
+    }
+}
+
 int run(int argc, char** argv) {
     const Args A = parse_args(argc, argv);
     const Ini ini = read_ini(A.dir + "/input.ini");
@@ -621,6 +818,7 @@ int run(int argc, char** argv) {
             blocks[b].area = read_area(A.dir + "/INPUT/block" + std::to_string(b + 1) + "_area.dat", blocks[b]);
     std::vector<q2d_bc_rec> recs = read_bc(A.dir + "/INPUT/bc.txt", S.unsupported);
     const q2d_options& o = S.opt;
+    place_probes(S.probes, blocks);
 
     if (A.check) {   // parse summary, no GPU
         FILE* f = stdout;
@@ -651,6 +849,21 @@ int run(int argc, char** argv) {
             std::fprintf(f, "%s[%d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %.17g, %.17g, %.17g, %.17g, %.17g, %.17g]",
                          k ? ", " : "", r.b, r.i, r.j, r.f, r.type, r.bs, r.is, r.js, r.fs, r.d11, r.d12, r.d21, r.d22,
                          r.T0, r.p0, r.pamb, r.mach, r.alpha >= 0.5 * DBL_MAX ? -1.0 : r.alpha, r.rel_fac);
+        }
+        std::fprintf(f, "],\n \"sol_format\": ");
+        json_str(f, S.sol_format);
+        std::fprintf(f, ", \"sol_overwrite\": %d, \"probes\": [", S.sol_overwrite ? 1 : 0);
+        for (size_t k = 0; k < S.probes.size(); ++k) {
+            const Probe& pr = S.probes[k];
+            std::fprintf(f, "%s{\"file\": ", k ? ", " : "");
+            json_str(f, pr.file);
+            std::fprintf(f, ", \"variables\": [");
+            for (size_t q = 0; q < pr.vars.size(); ++q) {
+                if (q) std::fprintf(f, ", ");
+                json_str(f, pr.vars[q]);
+            }
+            std::fprintf(f, "], \"diter\": %lld, \"dtime\": %.17g, \"cell\": [%d, %d, %d]}", pr.diter, pr.dtime,
+                         pr.b, pr.i, pr.j);
         }
         std::fprintf(f, "],\n \"unsupported\": [");
         for (size_t k = 0; k < S.unsupported.size(); ++k) {
@@ -700,6 +913,63 @@ int run(int argc, char** argv) {
             std::string cmd = "mkdir -p '" + outdir + "'";
             if (std::system(cmd.c_str()) != 0) die("cannot create " + outdir);
         }
+        // Write_Solution (Wrap_Postprocess.f90:104-106, 120-125): OUTPUT/field at the end and, with
+        // sol-overwrite = false, OUTPUT/field<k> for the k-th intermediate solution; Tecplot or VTK
+        int id_stampa = 0;
+        auto write_solution = [&](bool intermediate, double t) {
+            std::string stem = "field";
+            if (intermediate) {
+                ++id_stampa;
+                if (!S.sol_overwrite) stem += std::to_string(id_stampa);
+            }
+            if (!A.out.empty()) {
+                write_tec(out, blocks, P, t);
+            } else if (S.sol_format == "tecplot ascii") {
+                write_tec(outdir + "/" + stem + ".tec", blocks, P, t);
+            } else {
+                write_vtk(outdir, stem, blocks, P, t, o.gas_R, S.sol_format == "vtk raw");
+            }
+            return stem;
+        };
+        for (Probe& pr : S.probes) {
+            const std::string path = outdir + "/" + pr.file + ".txt";
+            if (!S.newrun && !std::ifstream(path))
+                die("[ERROR] You restarted from an old solution but the probes files were not found.");
+            pr.f = std::fopen(path.c_str(), S.newrun ? "w" : "a");
+            if (!pr.f) die("cannot write " + path);
+        }
+        bool probe_dtime = false;
+        for (const Probe& pr : S.probes) probe_dtime = probe_dtime || pr.dtime < 1e30;
+        // Write_Probes_Data (IO_Probes.f90:187-207) after an iteration that needs no solution output
+        // (TODO = 1, Wrap_Postprocess.f90:246-257): every diter iterations the iteration and the
+        // variables, else once the time passes the next multiple of dtime, the time and the variables
+        auto write_probes = [&](long long iter_general, double t) {
+            std::vector<char> have(blocks.size(), 0);
+            for (Probe& pr : S.probes) {
+                const bool by_iter = iter_general % pr.diter == 0;
+                const bool by_time = !by_iter && t >= pr.dtime * (double)pr.ntime;
+                if (!by_iter && !by_time) continue;
+                const int b = pr.b - 1;
+                if (!have[b]) {
+                    check(q2d_gpu_download_prim(ctx, bid[b], P[b].data()), "q2d_gpu_download_prim");
+                    have[b] = 1;
+                }
+                const double* q = cell_at(P[b], blocks[b].ni, pr.i, pr.j);
+                std::string line = by_iter ? ld_int(iter_general) : ld_real(t);
+                for (const std::string& w : pr.vars) {
+                    double x;
+                    if (w == "rho(1)") x = q[0];
+                    else if (w == "u") x = q[1];
+                    else if (w == "v") x = q[2];
+                    else if (w == "p") x = q[3];
+                    else if (w == "T") x = q[3] / (q[0] * o.gas_R);
+                    else x = std::hypot(q[1], q[2]) / std::sqrt(o.gas_gamma * q[3] / q[0]);
+                    line += ld_real(x);
+                }
+                std::fprintf(pr.f, "%s\n", line.c_str());
+                if (by_time) pr.ntime += 1;
+            }
+        };
         FILE* hist = std::fopen((A.out.empty() ? outdir + "/residuals.dat" : A.out + ".residuals").c_str(), "w");
         if (!hist) die("cannot write the residual history");
         std::fprintf(hist, "# iter time dtglobal res_rho res_u res_v res_p\n");
@@ -719,6 +989,9 @@ int run(int argc, char** argv) {
         for (;;) {
             int n = A.per_call;
             n = (int)std::min<long long>(n, o.res_diter - done % o.res_diter);   // land on res-diter multiples
+            for (const Probe& pr : S.probes)   // and on the probes' iterations
+                n = (int)std::min<long long>(n, pr.diter - (iter_base + done) % pr.diter);
+            if (probe_dtime) n = 1;            // time-based probes: every step is checked
             if (A.max_steps >= 0) n = (int)std::min<long long>(n, A.max_steps - done);
             if (n <= 0) break;
             const int st = q2d_gpu_step(ctx, n, &info);
@@ -748,15 +1021,18 @@ int run(int argc, char** argv) {
             if (info.todo == Q2D_TODO_IO || info.todo == Q2D_TODO_END) {   // Write_Solution
                 for (size_t b = 0; b < blocks.size(); ++b)
                     check(q2d_gpu_download_prim(ctx, bid[b], P[b].data()), "q2d_gpu_download_prim");
-                write_tec(out, blocks, P, sol_time(info));
+                write_solution(info.todo == Q2D_TODO_IO, sol_time(info));
+            } else if (!S.probes.empty()) {
+                write_probes(iter_base + info.iter, info.time);
             }
             if (info.todo == Q2D_TODO_END) break;
         }
         if (rc == 0 && info.todo != Q2D_TODO_END) {   // stopped by --max-steps
             for (size_t b = 0; b < blocks.size(); ++b)
                 check(q2d_gpu_download_prim(ctx, bid[b], P[b].data()), "q2d_gpu_download_prim");
-            write_tec(out, blocks, P, sol_time(info));
+            write_solution(false, sol_time(info));
         }
+        for (Probe& pr : S.probes) std::fclose(pr.f);
         std::fclose(hist);
         if (rh) std::fclose(rh);
         if (!A.quiet)

@@ -92,13 +92,14 @@ def _bc_lines(r: dict) -> list:
     return out
 
 
-def write_case(cs: CaseSpec, directory, **option_overrides) -> Path:
-    """Writes the case directory; options are the case's (make_options) with the overrides."""
+def write_case(cs: CaseSpec, directory, extra_ini: str = "", **option_overrides) -> Path:
+    """Writes the case directory; options are the case's (make_options) with the overrides.
+    extra_ini is appended to input.ini (more [Q2D-IO] keys, probe sections)."""
     from .solver import make_options
     o = make_options(cs, **option_overrides)
     d = Path(directory)
     (d / "INPUT").mkdir(parents=True, exist_ok=True)
-    (d / "input.ini").write_text(_ini(o))
+    (d / "input.ini").write_text(_ini(o) + ("\n" + extra_ini if extra_ini else ""))
     with open(d / "INPUT" / "bc.txt", "w") as f:
         for r in cs.bcs:
             f.write("\n".join(_bc_lines(r)) + "\n")

@@ -16,6 +16,8 @@ Fixtures written (all small text/npz files):
                       its BC 401 records (INPUT/bc.txt), and Chang's (1996) Mach number along the
                       axis and the wall that its check.py compares against (reference/ref1.dat,
                       ref2.dat)
+  prandtl_meyer.npz   the reference's prandtl-meyer case (test/2D/euler/prandtl-meyer): its grid,
+                      initial state and bc.txt records (type; M, T, p of the supersonic inflow)
   ramp_channel.npz    the reference's ramp-channel case (test/2D/euler/ramp-channel): its grid
                       nodes and initial state read from INPUT/ic.tec and the Mach number,
                       temperature and pressure of its BC 405 records (INPUT/bc.txt)
@@ -88,6 +90,20 @@ def main(ref_root: str) -> None:
             assert props is None or props == cur
             props = cur
     np.savez_compressed(HERE / "ramp_channel.npz", nodes=blk.nodes, prim=blk.prim, mach_T_p=np.array(props))
+    pdir = ref / "test/2D/euler/prandtl-meyer"
+    blk = refio.read_field(pdir / "INPUT" / "ic.tec")[0]
+    recs = []
+    lines = (pdir / "INPUT" / "bc.txt").read_text().splitlines()
+    for k, line in enumerate(lines):
+        t = line.split()
+        if len(t) == 5:
+            b, i, j, f, typ = (int(x) for x in t)
+            props = (0.0, 0.0, 0.0)
+            if typ == 405:
+                vals = lines[k + 1].replace(",", " ").split()
+                props = (float(vals[0]), float(vals[1]), float(vals[2]))
+            recs.append((b, i, j, f, typ) + props)
+    np.savez_compressed(HERE / "prandtl_meyer.npz", nodes=blk.nodes, prim=blk.prim, bcs=np.array(recs))
     rows = []
     for line in (ref / "test/2D/euler/planar-nozzle/solve.log").read_text().splitlines():
         if "| Iter =" in line and "Density residual" in line:

@@ -114,6 +114,48 @@ def ramp_channel_case():
     return CaseSpec("ramp_channel", [blk], bcs, opts, {"mach": mach})
 
 
+def prandtl_meyer_case():
+    """The reference's prandtl-meyer case (test/2D/euler/prandtl-meyer: input.ini, INPUT/) from the
+    committed fixture: Mach 2 flow turning round a convex corner, 50 x 50 cells, supersonic inflow
+    (BC 405: M 2, T 1, p 1) on face 1, extrapolation (400) on faces 2 and 3, symmetry (300) on
+    face 4; MUSCL van Leer + HLLE, SSP-RK3, CFL 1.0, IRS beta 0.5, local time steps, 2500
+    iterations; the air of its phase.txt (W = 28.970418) with gamma 1.4."""
+    from pathlib import Path
+    from q2d_b200.cases import BlockSpec, CaseSpec, supersonic_props
+    f = np.load(Path(__file__).resolve().parent / "golden" / "prandtl_meyer.npz")
+    nodes, prim = f["nodes"], f["prim"]
+    nj, ni = prim.shape[:2]
+    bcs = []
+    for row in f["bcs"]:
+        b, i, j, fc, typ = (int(x) for x in row[:5])
+        r = {"b": b, "i": i, "j": j, "f": fc, "type": typ}
+        if typ == 405:
+            r.update(supersonic_props(float(row[5]), float(row[6]), float(row[7])))
+        bcs.append(r)
+    opts = dict(limiter="vanleer", riemann="HLLE", n_rk=3, cfl=1.0, time_accurate=0, irs_beta=0.5,
+                itermax=2500, gas_R=8314.46 / 28.970418, gas_gamma=1.4)
+    return CaseSpec("prandtl_meyer", [BlockSpec(ni, nj, nodes, prim)], bcs, opts, {"mach": 2.0})
+
+
+def prandtl_meyer_exit_mach(M1: float = 2.0, theta_deg: float = 34.971, g: float = 1.4) -> float:
+    """The exit Mach number of the case's check.py: the Prandtl-Meyer expansion of M1 by
+    theta (nu(M2) = nu(M1) + theta), by bisection."""
+    import math
+
+    def nu(M):
+        return math.sqrt((g + 1) / (g - 1)) * math.atan(math.sqrt((g - 1) / (g + 1) * (M * M - 1))) - \
+            math.atan(math.sqrt(M * M - 1))
+    target = nu(M1) + math.radians(theta_deg)
+    lo, hi = 1.01, 30.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if nu(mid) < target:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
 def oblique_shock(M1: float, delta: float, g: float):
     """Weak oblique-shock solution for a wedge of angle delta (radians): the theta-beta-Mach
     relation tan(delta) = 2 cot(b) (M1^2 sin^2 b - 1) / (M1^2 (g + cos 2b) + 2) solved for the
