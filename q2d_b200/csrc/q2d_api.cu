@@ -242,7 +242,11 @@ bool dt_in_first_stage(const q2d_ctx* ctx) { return ctx->kernel >= 2 && !ctx->op
 // 0-2, 512 on tiles 3-4, as launch_stage32 / launch_stage32d instantiate them), which end their
 // items without a CTA-wide reduction and leave the case finalisation to finalize_kernel; one
 // otherwise.
-int part_stride(const q2d_ctx* ctx) { return ctx->kernel >= 2 ? (ctx->tile >= 3 ? 16 : 8) : 1; }
+int part_stride(const q2d_ctx* ctx) {
+    int TX, TY, NT;
+    tile_dims(ctx->tile, &TX, &TY, &NT);
+    return ctx->kernel >= 2 ? NT / 32 : 1;
+}
 
 // RKcoeff (Lib_RK.f90:8-11)
 double rk_coeff(int n_rk, int irk) {
@@ -816,6 +820,16 @@ bool schedule_allowed(const q2d_ctx* ctx, int k) {
     return kSchedules[k].kernel != 2 || ctx->opt.precision == Q2D_PREC_FP32_FLUX;
 }
 
+// The FP32-flux form of HLLC / HLLE / LLF without MUSCL-SD or smoothing is the difference-form
+// kernel: its error against FP64 stays at ~1e-9 relative L1 over thousands of steps where the
+// tile kernels that round whole fluxes to FP32 reach ~1e-6. The autotuner does not trade that
+// form for another one; q2d_gpu_set_schedule can still pin the others.
+bool difference_form(const q2d_ctx* ctx) {
+    for (int k = 0; k < kNumSchedules; ++k)
+        if (kSchedules[k].kernel == 3 && schedule_allowed(ctx, k)) return true;
+    return false;
+}
+
 int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
     const Schedule* cands = kSchedules;
     const int ncand = kNumSchedules;
@@ -835,8 +849,9 @@ int autotune(q2d_ctx* ctx, int steps, int* best_out, float* ms_out) {
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
     int besti = 0;
+    const bool df = difference_form(ctx);
     for (int k = 0; k < ncand; ++k) {
-        if (!schedule_allowed(ctx, k)) continue;
+        if (!schedule_allowed(ctx, k) || (df && cands[k].kernel != 3)) continue;
         CK(cudaStreamSynchronize(ctx->stream));
         ctx->kernel = cands[k].kernel;
         ctx->tile = cands[k].tile;

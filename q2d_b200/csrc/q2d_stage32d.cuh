@@ -350,7 +350,9 @@ __global__ void __launch_bounds__(NT, MB) stage32d_kernel(const StageArgs a) {
         const int nrow = min(TY, nj - j0), ncol = min(TX, ni - i0);
         RowCopy rc{nullptr, 0u, 0};
         void* dst = nullptr;
-        const int t = tid;
+        // copy index of the thread: consecutive copies go to different warps, so that the lanes
+        // each warp issues one after another are spread over all of them
+        const int t = lane * (NT / 32) + warp;
         if (t < 4 * HR) {                                   // state rows j0-2 .. j0+TY+1
             const int v = t / HR, r = t - v * HR, jj = j0 - 2 + r;
             const int cs0 = max(i0 - 2, 0), ce = min(i0 + TX + 2, ni);
@@ -400,7 +402,7 @@ __global__ void __launch_bounds__(NT, MB) stage32d_kernel(const StageArgs a) {
         const double* scb = a.sc + 2 * B.oc;
         RowCopy rc{nullptr, 0u, 0};
         void* dst = nullptr;
-        const int t = tid;
+        const int t = lane * (NT / 32) + warp;   // spread over the warps like the stencil copies
         if (t < L::NOWN * TY) {
             const int k = t / TY, r = t - k * TY;
             const double* plane = nullptr;

@@ -101,9 +101,9 @@ def test_inputs_outside_the_path_fail_loudly(tmp_path):
     refio.write_case(cs, tmp_path)
     ini = (tmp_path / "input.ini").read_text()
     (tmp_path / "input.ini").write_text(ini.replace("integration-variables = cons", "integration-variables = prim")
-                                        .replace("[Q2D-IO]\n", "[Q2D-IO]\nsol-format = vtk ascii\n"))
+                                        .replace("[Q2D-IO]\n", "[Q2D-IO]\nsol-format = tecplot binary\n"))
     d = json.loads(host(tmp_path, "--check").stdout)
-    assert d["unsupported"] == ["[Q2D-Numerics] integration-variables = prim", "[Q2D-IO] sol-format = vtk ascii"]
+    assert d["unsupported"] == ["[Q2D-Numerics] integration-variables = prim", "[Q2D-IO] sol-format = tecplot binary"]
     r = host(tmp_path, check=False)   # refused before any device call
     assert r.returncode == 2 and "not on the built path" in r.stderr
     # Assign_Riemann_Solver keywords (Mod_Riemann.f90:25-109) of the built solvers
