@@ -119,8 +119,9 @@ def read_traffic(schedule):
     the stage kernel under profiles/ (a smaller batch captured and scaled by cells), when that
     summary holds a capture taken with the same schedule (lines "- schedule: S" followed by
     "- dram_bytes_per_launch_full_batch: B"); otherwise None."""
-    name = "stage32_kernel_batched_nozzles.md" if schedule.startswith("fp32-flux") else \
-        "stage_kernel_fp64_batched_nozzles.md"
+    name = ("stage32d_kernel_batched_nozzles.md" if "difference" in schedule else
+            "stage32_kernel_batched_nozzles.md" if schedule.startswith("fp32-flux") else
+            "stage_kernel_fp64_batched_nozzles.md")
     f = REPO / "profiles" / name
     try:
         cur = None

@@ -190,6 +190,12 @@ int  q2d_gpu_upload_prim(q2d_ctx* ctx, int block_id, const double* P);
  * iteration counters restart at 0 as in the reference. Before q2d_gpu_commit. */
 int  q2d_gpu_set_case_time(q2d_ctx* ctx, int case_id, double time);
 
+/* A case's own fixed end (no counterpart in the reference, whose domain has one iteration limit):
+ * the case reports TODO = END once its iteration count reaches iter_end (0: none), besides the
+ * context's limits. Usable before or after commit and on admitted serving cases; a served
+ * request's end is set this way right after q2d_serve_admit. */
+int  q2d_gpu_set_case_end(q2d_ctx* ctx, int case_id, long long iter_end);
+
 /* Builds metrics (Setup_Metrics, Mod_Metrics.f90:11-148) and the device work lists.
  * Called implicitly by the first q2d_gpu_step(). */
 int  q2d_gpu_commit(q2d_ctx* ctx);

@@ -797,6 +797,7 @@ struct Case {
     int todo = Q2D_TODO_CONTINUE;
     int err = Q2D_OK, err_b = 0, err_i = 0, err_j = 0, err_stage = 0;
     bool done = false;
+    long long iter_end = 0;       // the case's own fixed end, 0 for none
 };
 
 }  // namespace
@@ -1797,7 +1798,7 @@ void explicit_step(q2d_oracle* o, Case& cs) {
     }
     const double thr = op.res_relative ? op.res_threshold * cs.res0 : op.res_threshold;
     const bool endsim = (cs.iter_from_call >= op.itermax) || (cs.res[0] <= thr) ||
-                        (cs.time >= op.time_threshold);
+                        (cs.time >= op.time_threshold) || (cs.iter_end > 0 && cs.iter >= cs.iter_end);
     const bool iosim = ((cs.iter % op.sol_diter) == 0) || (cs.time >= cs.time_from_call + op.sol_dtime);
     if (endsim) { cs.todo = Q2D_TODO_END; cs.done = true; }
     else if (iosim) cs.todo = Q2D_TODO_IO;
@@ -1985,6 +1986,12 @@ int q2d_oracle_set_case_time(q2d_oracle* o, int case_id, double time) {
     if (!o || o->committed || case_id < 0 || case_id >= (int)o->cases.size() || !std::isfinite(time))
         return Q2D_ERR_BADARG;
     o->cases[case_id].time = time;   // Wrap_Setup.f90:141-144: time = solutiontime, counters at 0
+    return Q2D_OK;
+}
+
+int q2d_oracle_set_case_end(q2d_oracle* o, int case_id, long long iter_end) {
+    if (!o || case_id < 0 || case_id >= (int)o->cases.size() || iter_end < 0) return Q2D_ERR_BADARG;
+    o->cases[case_id].iter_end = iter_end;
     return Q2D_OK;
 }
 

@@ -34,6 +34,7 @@ int  q2d_oracle_add_block(q2d_oracle* o, int case_id, int ni, int nj, const doub
 int  q2d_oracle_set_bcs(q2d_oracle* o, int case_id, const q2d_bc_rec* recs, int n);
 int  q2d_oracle_upload_prim(q2d_oracle* o, int block_id, const double* P);
 int  q2d_oracle_set_case_time(q2d_oracle* o, int case_id, double time);
+int  q2d_oracle_set_case_end(q2d_oracle* o, int case_id, long long iter_end);
 int  q2d_oracle_commit(q2d_oracle* o);
 int  q2d_oracle_step(q2d_oracle* o, int nsteps, q2d_step_info* out);
 int  q2d_oracle_case_info(q2d_oracle* o, int case_id, q2d_step_info* out);

@@ -128,6 +128,7 @@ def _declare(lib: C.CDLL, prefix: str, ctx_t) -> None:
         "set_bcs": (C.c_int, [ctx_t, C.c_int, P(BCRec), C.c_int]),
         "upload_prim": (C.c_int, [ctx_t, C.c_int, P(C.c_double)]),
         "set_case_time": (C.c_int, [ctx_t, C.c_int, C.c_double]),
+        "set_case_end": (C.c_int, [ctx_t, C.c_int, C.c_longlong]),
         "commit": (C.c_int, [ctx_t]),
         "step": (C.c_int, [ctx_t, C.c_int, P(StepInfo)]),
         "case_info": (C.c_int, [ctx_t, C.c_int, P(StepInfo)]),

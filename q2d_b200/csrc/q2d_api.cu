@@ -56,6 +56,7 @@ struct HCase {
     std::vector<q2d_bc_rec> bc;
     std::vector<BCParam> params;
     double time0 = 0.0;
+    int iter_end = 0;              // the case's own fixed end (q2d_gpu_set_case_end), 0 for none
     bool used = false;             // slot holds a case
     bool prepared = false;         // regions reserved, device images staged
     bool resident = false;         // device images and run state uploaded
@@ -385,9 +386,10 @@ bool rec_less(const q2d_bc_rec& a, const q2d_bc_rec& b) {
     return a.b != b.b ? a.b < b.b : a.f < b.f;
 }
 
-CaseState fresh_state(double time0) {
+CaseState fresh_state(double time0, int iter_end) {
     CaseState s;
     std::memset(&s, 0, sizeof(s));
+    s.iter_end = iter_end;
     s.res0 = -1.0;
     s.todo = Q2D_TODO_CONTINUE;
     s.status = kStatus_Running;
@@ -655,7 +657,7 @@ int upload_case(q2d_ctx* ctx, int c) {
         if (S.heap) CK(cudaStreamSynchronize(s));   // a heap image is freed right away
         S = Staged{};
     }
-    const CaseState st = fresh_state(cs.time0);
+    const CaseState st = fresh_state(cs.time0, cs.iter_end);
     CK(cudaMemcpyAsync(ctx->cstate.p + c, &st, sizeof(CaseState), h2d, s));
     CK(cudaStreamSynchronize(s));   // st is on this stack frame
     cs.resident = true;
@@ -1025,6 +1027,20 @@ int q2d_gpu_set_case_time(q2d_ctx* ctx, int case_id, double time) {
         !std::isfinite(time))
         return fail(ctx, Q2D_ERR_BADARG, "set_case_time: bad argument or after commit");
     ctx->cases[case_id].time0 = time;
+    return Q2D_OK;
+}
+
+int q2d_gpu_set_case_end(q2d_ctx* ctx, int case_id, long long iter_end) {
+    if (!ctx || case_id < 0 || case_id >= (int)ctx->cases.size() ||
+        (ctx->serving && !ctx->cases[case_id].used) || iter_end < 0 || iter_end > 2000000000LL)
+        return fail(ctx, Q2D_ERR_BADARG, "set_case_end: bad argument");
+    HCase& cs = ctx->cases[case_id];
+    cs.iter_end = (int)iter_end;
+    if (cs.resident) {   // stream-ordered after the steps in flight
+        const int v = cs.iter_end;
+        CK(cudaMemcpyAsync(&ctx->cstate.p[case_id].iter_end, &v, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     return Q2D_OK;
 }
 

@@ -389,7 +389,7 @@ __device__ void finalize_case(const StageArgs& a, int case_id, bool with_res, bo
             }
             const double thr = a.res_relative ? a.res_threshold * cs->res0 : a.res_threshold;
             const bool endsim = (cs->iter_from_call >= a.itermax) || (cs->res[0] <= thr) ||
-                                (cs->time >= a.time_threshold);
+                                (cs->time >= a.time_threshold) || (cs->iter_end > 0 && cs->iter >= cs->iter_end);
             const bool iosim = ((cs->iter % a.sol_diter) == 0) ||
                                (cs->time >= cs->time_from_call + a.sol_dtime);
             cs->todo = endsim ? 3 : (iosim ? 2 : 1);

@@ -71,7 +71,9 @@ struct CaseState {
     int err, err_b, err_i, err_j, err_stage;
     unsigned int counter;  // items of the current stage finished (reset by the last CTA)
     int dt_pending;        // the case has no time step yet (admitted after the last dt pass)
+    int iter_end;          // the case's own fixed end (iteration count), 0 for none
 };
+static_assert(sizeof(CaseState) == 128, "case state: 128 bytes");
 
 struct WorkItem {
     int block;   // global block id

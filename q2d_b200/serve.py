@@ -85,6 +85,11 @@ class ServeContext:
         self.cases[cid.value] = case
         return cid.value
 
+    def set_end(self, cid: int, iter_end: int) -> None:
+        """The case's own fixed end: it reports TODO = END at iteration iter_end, inside a
+        multi-step call (q2d_gpu_set_case_end)."""
+        self._check(self.lib.q2d_gpu_set_case_end(self.ctx, cid, int(iter_end)), "q2d_gpu_set_case_end")
+
     def retire(self, cid: int) -> None:
         self._check(self.lib.q2d_serve_retire(self.ctx, cid), "q2d_serve_retire")
         self.cases.pop(cid, None)
@@ -246,7 +251,8 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
 
     A request retires on the residual drop of the options, on an error, or at its fixed end:
     the options' iteration cap or, with end_cell_updates, the iteration at which its cells
-    times its iterations first reach that budget (checked after each step call). With
+    times its iterations first reach that budget (set on the device at admission, so that the
+    case stops there inside a multi-step call). With
     keep_results the states of the cases retiring after a step call are read back in one
     many-block transfer before they are retired; that read-back is inside their latency. The
     states are kept in Request.result, or handed to result_sink(request, states) when given
@@ -263,6 +269,7 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
         budget_cells = sc.free_cells()
         t0 = clock()
         busy = 0.0
+        t_admit = t_readback = t_retire = 0.0
 
         def now():
             return clock() - t0 if realtime else math.inf
@@ -284,6 +291,7 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
                 r.admitted = clock() - t0
                 if end_cell_updates is not None:
                     r.meta["end_iter"] = max(1, math.ceil(end_cell_updates / case.cells))
+                    sc.set_end(cid, r.meta["end_iter"])
                 active[cid] = r
                 queue.popleft()
 
@@ -298,7 +306,9 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
             sc.step_async(steps_per_call)
             on_device = set(active.keys())   # cases admitted from here on join the next call
             steps_calls += 1
+            ta = clock()
             admit_due()              # host work overlaps the steps in flight
+            t_admit += clock() - ta
             infos = sc.wait()
             busy += clock() - tb
             leaving = []
@@ -309,9 +319,8 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
                 if inf.err:
                     r.rule = "error"
                 elif inf.todo == _abi.TODO_END:
-                    r.rule = "end" if inf.iter >= options.itermax else "drop"
-                elif end_iter is not None and inf.iter >= end_iter:
-                    r.rule = "end"
+                    fixed = inf.iter >= options.itermax or (end_iter is not None and inf.iter >= end_iter)
+                    r.rule = "end" if fixed else "drop"
                 else:
                     continue
                 r.iters = int(inf.iter)
@@ -319,6 +328,7 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
                 r.residual_drop = inf.residual[0] / inf.residual0 if inf.residual0 > 0 else math.nan
                 leaving.append(cid)
             if leaving:
+                tr = clock()
                 if keep_results:
                     buf = readback_buffer if result_sink is not None else None
                     for cid, res in zip(leaving, sc.prims_many(leaving, buf)):
@@ -327,12 +337,15 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
                             result_sink(active[cid], res)
                         else:
                             active[cid].result = res
+                t_readback += clock() - tr
+                tr = clock()
                 for cid in leaving:
                     r = active.pop(cid)
                     sc.retire(cid)
                     r.done = clock() - t0
                     cell_updates += r.case.cells * r.iters
                     r.case = None if not keep_results or result_sink is not None else r.case
+                t_retire += clock() - tr
         makespan = clock() - t0
         launches = sc.launches()
     done = [r for r in reqs if not r.rejected]
@@ -355,6 +368,7 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
         "p50_service_s": pct(ser, 50), "p99_service_s": pct(ser, 99),
         "retired_by": rules, "median_residual_drop": pct(drops, 50),
         "readback_bytes": int(readback_bytes),
+        "host_s": {"admission_during_steps": t_admit, "readback": t_readback, "retire": t_retire},
         "step_calls": steps_calls, "gpu_launches": launches,
         "budget_cells": int(budget_cells),
     }

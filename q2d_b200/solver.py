@@ -60,6 +60,8 @@ class Q2DSolver:
                 self.block_ids.append(ids)
                 if cs.meta.get("restart_time") is not None:   # resume a time-accurate case
                     self._call("set_case_time", self.ctx, cid.value, float(cs.meta["restart_time"]))
+                if cs.meta.get("iter_end"):   # the case's own fixed end
+                    self._call("set_case_end", self.ctx, cid.value, int(cs.meta["iter_end"]))
                 recs = _abi.bc_array(cs.bcs)
                 self._call("set_bcs", self.ctx, cid.value, recs, len(cs.bcs))
             self._call("commit", self.ctx)
@@ -111,6 +113,11 @@ class Q2DSolver:
         ms = C.c_float()
         self._call("autotune", self.ctx, steps, C.byref(idx), C.byref(ms))
         return {"schedule": self.SCHEDULES[idx.value], "ms_per_step": ms.value}
+
+    def set_case_end(self, case: int, iter_end: int) -> None:
+        """Gives a case its own fixed end: TODO = END once its iteration count reaches iter_end
+        (0 clears it), besides the options' limits (q2d_gpu_set_case_end)."""
+        self._call("set_case_end", self.ctx, case, int(iter_end))
 
     def info(self, case: int = 0) -> dict:
         s = _abi.StepInfo()

@@ -43,6 +43,23 @@ def test_oracle_mirrors_the_boundary():
     lib = oracle.load()
     for n in declared_functions():
         if n.startswith("q2d_gpu_") and n[8:] in ("create", "add_case", "add_block", "set_bcs",
-                                                   "upload_prim", "commit", "step", "case_info",
+                                                   "upload_prim", "set_case_time", "set_case_end",
+                                                   "commit", "step", "case_info",
                                                    "download_prim", "destroy"):
             assert hasattr(lib, "q2d_oracle_" + n[8:])
+
+
+def test_oracle_case_end():
+    """A case's own fixed end (set_case_end): the case stops at that iteration, inside a
+    multi-step call, while the case next to it runs on; a finished case stays finished."""
+    from oracle import oracle
+    from q2d_b200 import cases, make_options
+    batch = [cases.ramp(16, 6, seed=2), cases.ramp(12, 6, seed=4)]
+    s = oracle.solver(make_options(batch[0], itermax=100), batch)
+    try:
+        s.set_case_end(0, 4)
+        assert [i["iter"] for i in s.step(6)] == [4, 6]
+        assert [i["todo"] for i in s.step(3)] == [_abi.TODO_END, _abi.TODO_CONTINUE]
+        assert s.info(0)["iter"] == 4
+    finally:
+        s.close()

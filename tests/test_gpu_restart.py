@@ -109,3 +109,29 @@ def test_steady_solution_time_and_restart_count(tmp_path):
     assert np.all(h[:, 1] == -1.0)
     text = (tmp_path / "OUTPUT" / "field.tec").read_text()
     assert float(text.split("SOLUTIONTIME=")[1].split()[0]) == 20.0
+
+
+def test_case_end_batch_vs_oracle():
+    """A per-case end in a batch context (q2d_gpu_set_case_end before commit and between
+    calls): the GPU and the oracle stop each case at the same iteration with the same state."""
+    from oracle import oracle
+    batch = [cases.ramp(60, 20, seed=2), cases.ramp(48, 16, seed=4)]
+    opts = make_options(batch[0], itermax=100)
+    batch[0].meta["iter_end"] = 9
+    try:
+        g, o = Q2DSolver(opts, batch), oracle.solver(opts, batch)
+    finally:
+        batch[0].meta.pop("iter_end")
+    try:
+        gi, oi = g.step(15), o.step(15)
+        assert [x["iter"] for x in gi] == [x["iter"] for x in oi] == [9, 15]
+        assert gi[0]["todo"] == oi[0]["todo"] == 3
+        g.set_case_end(1, 18)
+        o.set_case_end(1, 18)
+        gi, oi = g.step(15), o.step(15)
+        assert gi[1]["iter"] == oi[1]["iter"] == 18 and gi[1]["todo"] == 3
+        for c in range(2):
+            assert rel_linf(g.prim(c, 0), o.prim(c, 0)).max() <= 1e-12
+    finally:
+        g.close()
+        o.close()

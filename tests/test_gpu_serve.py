@@ -160,3 +160,30 @@ def test_serving_with_sensor_and_other_solvers(precision, kw):
             assert infos[cid].iter == steps and infos[cid].err == 0
             for b in range(len(c.blocks)):
                 assert np.array_equal(sc.prim(cid, b), alone[k][0][b]), (kw, k, b)
+
+
+def test_case_end_inside_a_multi_step_call():
+    """q2d_gpu_set_case_end: a served case with its own end stops at exactly that iteration
+    inside a 20-step call, its state equal to the same case served alone for that many steps,
+    while the case next to it runs the whole call; the request loop's end budget lands on the
+    first iteration at which cells x iterations reach it."""
+    rng = np.random.default_rng(31)
+    a, b = cases.request_case("ramp", 900, rng), cases.request_case("nozzle", 1200, rng)
+    opts = serve_options(itermax=1000, drop=1e-12)
+    ref, _ = run_alone(a, opts, 7)
+    with ServeContext(opts, BUDGET, 4) as sc:
+        ca, cb = sc.admit(a), sc.admit(b)
+        sc.set_end(ca, 7)
+        sc.step_async(20)
+        infos = sc.wait()
+        assert infos[ca].iter == 7 and infos[ca].todo == _abi.TODO_END and infos[ca].err == 0
+        assert infos[cb].iter == 20 and infos[cb].todo != _abi.TODO_END
+        assert np.array_equal(sc.prim(ca, 0), ref[0])
+    reqs = [Request(k, 0.0, kind, cells, int(rng.integers(1 << 31)))
+            for k, (kind, cells) in enumerate([("ramp", 900), ("nozzle", 1300), ("ramp", 2100)])]
+    st = serve(reqs, opts, device_bytes=int(3 * 2100 * 306 + (1 << 20)), max_cases=3, steps_per_call=50,
+               realtime=False, end_cell_updates=40000)
+    for r in reqs:
+        end = -(-40000 // r.cells)
+        assert r.rule == "end" and r.iters == end, (r.cells, r.iters, end)
+    assert st["retired_by"]["end"] == 1.0
