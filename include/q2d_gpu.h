@@ -190,6 +190,17 @@ int  q2d_gpu_upload_prim(q2d_ctx* ctx, int block_id, const double* P);
  * iteration counters restart at 0 as in the reference. Before q2d_gpu_commit. */
 int  q2d_gpu_set_case_time(q2d_ctx* ctx, int case_id, double time);
 
+/* Thermally perfect single-species gas (replaces the constant-cp table of
+ * FLINT_Lib_Thermodynamic for the path's routines: f_tabT_expr lerps at int(T) in roe_averages,
+ * Lib_Riemann_HLL.f90:229-317, and in Compute_Prim_Residual, Lib_Newstate.f90:245-294; f_ss /
+ * f_gamma / E0 / H0 / prim2cons / cons2prim of Lib_Newstate.f90:131-159 and the BC and source
+ * routines): h(T) [J/kg] and cp(T) [J/(kg K)] at T = 0, 1, .., ntab-1 K, interpolated linearly
+ * at int(T); gas constant options.gas_R, gamma(T) = cp/(cp - R). The state from the conserved
+ * variables solves e(T) = h(T) - R T on the table, starting from the temperature before the
+ * update. Plain FP64 form, HLLC / HLLE / LLF, no shock sensor, batch contexts only; before
+ * q2d_gpu_commit. Q2D_ERR_BADARG otherwise, or when cp <= R or e(T) does not increase. */
+int  q2d_gpu_set_thermo_table(q2d_ctx* ctx, int ntab, const double* h_tab, const double* cp_tab);
+
 /* A case's own fixed end (no counterpart in the reference, whose domain has one iteration limit):
  * the case reports TODO = END once its iteration count reaches iter_end (0: none), besides the
  * context's limits. Usable before or after commit and on admitted serving cases; a served

@@ -94,6 +94,10 @@ module q2d_gpu_m
       import; type(c_ptr), value :: ctx; integer(c_int), value :: case_id
       real(c_double), value :: time
     end function
+    integer(c_int) function q2d_gpu_set_thermo_table(ctx, ntab, h_tab, cp_tab) bind(c)
+      import; type(c_ptr), value :: ctx; integer(c_int), value :: ntab
+      real(c_double), intent(in) :: h_tab(*), cp_tab(*)
+    end function
     integer(c_int) function q2d_gpu_set_case_end(ctx, case_id, iter_end) bind(c)
       import; type(c_ptr), value :: ctx; integer(c_int), value :: case_id
       integer(c_long_long), value :: iter_end

@@ -39,6 +39,9 @@ def load():
         lib.q2d_oracle_riemann.argtypes = [C.c_int, C.POINTER(_abi.Options),
                                            C.POINTER(C.c_double), C.POINTER(C.c_double),
                                            C.c_double, C.c_double, C.POINTER(C.c_double)]
+        lib.q2d_oracle_thermo_tab.restype = C.c_int
+        lib.q2d_oracle_thermo_tab.argtypes = [C.c_int, C.POINTER(_abi.Options), C.c_int] + \
+            [C.POINTER(C.c_double)] * 4 + [C.c_double, C.c_double, C.POINTER(C.c_double)]
         lib.q2d_oracle_riemann_sd.restype = None
         lib.q2d_oracle_riemann_sd.argtypes = [C.c_int, C.POINTER(_abi.Options),
                                               C.POINTER(C.c_double), C.POINTER(C.c_double),
@@ -53,10 +56,10 @@ def load():
     return _LIB
 
 
-def solver(options, cases):
-    """A Q2DSolver over the oracle library."""
+def solver(options, cases, **kw):
+    """A Q2DSolver over the oracle library (keywords as Q2DSolver's, e.g. thermo_table)."""
     from q2d_b200.solver import Q2DSolver
-    return Q2DSolver(options, cases, lib=load(), prefix="q2d_oracle")
+    return Q2DSolver(options, cases, lib=load(), prefix="q2d_oracle", **kw)
 
 
 def set_threads(n: int) -> int:

@@ -29,39 +29,95 @@ constexpr int NPRIM = 4;   // rho, u, v, p (nsc = 1)
 constexpr int GUIDE[5][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}};
 
 // ---------------------------------------------------------------------------------------
-// THERMO: calorically perfect closure standing in for FLINT_Lib_Thermodynamic.
+// THERMO: single-species closures standing in for FLINT_Lib_Thermodynamic (an un-vendored
+// submodule of the reference; its documented formulas are in docs/theory/thermo.md:39-99).
+// Calorically perfect (the default, what the reference's constant-cp gas tables give):
 //   co_rotot_Rtot -> rho = rho_1, R = gas_R ; f_ss -> sqrt(gamma p / rho) ; f_gamma -> gamma
 //   E0(p,rho,|V|) = p/((gamma-1) rho) + |V|^2/2 ; H0 = gamma p/((gamma-1) rho) + |V|^2/2
 //   h_tab/cp_tab lerp -> h = cp T, cp = gamma R/(gamma-1)
 //   prim2cons -> (rho, rho u, rho v, p/(gamma-1) + rho |V|^2/2)
 //   cons2prim -> p = (gamma-1)(rho E - rho |V|^2/2)
+// Thermally perfect (a table set by q2d_oracle_set_thermo_table): h(T) and cp(T) on 1-K knots,
+// interpolated linearly at int(T) (f_tabT_expr, as called at Lib_Riemann_HLL.f90:258-291 and
+// Lib_Newstate.f90:281-282), T = p / (rho R):
+//   gamma(T) = cp / (cp - R) ; f_ss -> sqrt(gamma(T) p / rho) ; e(T) = h(T) - R T
+//   E0 = h(T) - p/rho + |V|^2/2 ; H0 = h(T) + |V|^2/2 ; prim2cons -> rho E = rho h(T) - p + ..
+//   cons2prim -> T solving e(T) = E - |V|^2/2 on the interpolated table (e is linear between
+//   knots: the knot interval is found from the temperature guess, then solved exactly),
+//   p = rho R T.
 // ---------------------------------------------------------------------------------------
 struct Gas {
     double R, gamma, gm1, cp, cv;
     double minf = 0.0;   // riemann-options-Minf (AUSM+-up, AUSM+-up2)
+    const double* htab = nullptr;    // thermally perfect: h(T) [J/kg] at T = 0, 1, .. ntab-1 K
+    const double* cptab = nullptr;   //   cp(T) [J/(kg K)] on the same knots
+    int ntab = 0;
 };
 
-inline double f_ss(const Gas& g, double p, double rho) { return std::sqrt(g.gamma * p / rho); }
+// Knot interval of T: int(T) (truncation, T >= 0), kept inside the table; a T past either end
+// extrapolates its end interval.
+inline int tab_knot(const Gas& g, double T) {
+    if (!(T >= 0.0)) return 0;
+    if (T >= (double)(g.ntab - 2)) return g.ntab - 2;
+    return (int)T;
+}
+inline double tab_at(const Gas& g, const double* t, double T) {
+    const int Ti = tab_knot(g, T);
+    const double dT = T - Ti;
+    return t[Ti] + (t[Ti + 1] - t[Ti]) * dT;
+}
+inline double h_of_T(const Gas& g, double T) { return g.htab ? tab_at(g, g.htab, T) : g.cp * T; }
+inline double cp_of_T(const Gas& g, double T) { return g.htab ? tab_at(g, g.cptab, T) : g.cp; }
+inline double f_gamma(const Gas& g, double p, double rho) {
+    if (!g.htab) return g.gamma;
+    const double cp = tab_at(g, g.cptab, p / (rho * g.R));
+    return cp / (cp - g.R);
+}
+inline double f_ss(const Gas& g, double p, double rho) {
+    if (!g.htab) return std::sqrt(g.gamma * p / rho);
+    return std::sqrt(f_gamma(g, p, rho) * p / rho);
+}
 inline double E0(const Gas& g, double p, double rho, double modv) {
+    if (g.htab) return tab_at(g, g.htab, p / (rho * g.R)) - p / rho + 0.5 * modv * modv;
     return p / (g.gm1 * rho) + 0.5 * modv * modv;
 }
 inline double H0(const Gas& g, double p, double rho, double modv) {
+    if (g.htab) return tab_at(g, g.htab, p / (rho * g.R)) + 0.5 * modv * modv;
     return g.gamma * p / (g.gm1 * rho) + 0.5 * modv * modv;
 }
 inline void prim2cons(const Gas& g, const double* P, double* U) {
     U[0] = P[0];
     U[1] = P[0] * P[1];
     U[2] = P[0] * P[2];
-    U[3] = P[3] / g.gm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
+    if (g.htab)
+        U[3] = P[0] * tab_at(g, g.htab, P[3] / (P[0] * g.R)) - P[3] + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
+    else
+        U[3] = P[3] / g.gm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
 }
-inline void cons2prim(const Gas& g, const double* U, double* P) {
+// Temperature of the specific internal energy e on the interpolated table, from the knot
+// interval of the guess T0 (walked to the interval holding e; e(T) = h(T) - R T increases
+// with T for cp > R).
+inline double T_of_e(const Gas& g, double e, double T0) {
+    int k = tab_knot(g, T0);
+    auto ek = [&](int n) { return g.htab[n] - g.R * (double)n; };
+    for (int w = 0; w < g.ntab && k > 0 && e < ek(k); ++w) --k;
+    for (int w = 0; w < g.ntab && k < g.ntab - 2 && e >= ek(k + 1); ++w) ++k;
+    return (double)k + (e - ek(k)) / (ek(k + 1) - ek(k));
+}
+// cons2prim(cons, temperature): the guess is the temperature of the state before the update.
+inline void cons2prim(const Gas& g, const double* U, double* P, double Tguess = 0.0) {
     const double rho = U[0];
     const double u = U[1] / rho;
     const double v = U[2] / rho;
     P[0] = rho;
     P[1] = u;
     P[2] = v;
-    P[3] = g.gm1 * (U[3] - 0.5 * rho * (u * u + v * v));
+    if (g.htab) {
+        const double T = T_of_e(g, U[3] / rho - 0.5 * (u * u + v * v), Tguess);
+        P[3] = rho * g.R * T;
+    } else {
+        P[3] = g.gm1 * (U[3] - 0.5 * rho * (u * u + v * v));
+    }
 }
 // check_gas_state (Lib_Convective.f90:49-54): non-physical when rho<=0, p<=0 or NaN.
 inline bool gas_state_bad(double rho, double p) { return !(rho > 0.0) || !(p > 0.0); }
@@ -124,7 +180,8 @@ inline double rlimiter(int lim, double x, double y) {
 // ---------------------------------------------------------------------------------------
 struct Flux4 { double r, u, v, e; };
 
-// roe_averages (Lib_Riemann_HLL.f90:229-317), constant-cp identities for the table lerps.
+// roe_averages (Lib_Riemann_HLL.f90:229-317); the table lerps at int(Tl), int(Tr) (constant cp:
+// h = cp T, cp).
 inline void roe_averages(const Gas& g, double dl, double dr, double dltot, double drtot,
                          double ul, double vl, double ur, double vr, double pl, double pr,
                          double& h0l, double& h0r, double& rho_roe, double& u_roe,
@@ -143,14 +200,14 @@ inline void roe_averages(const Gas& g, double dl, double dr, double dltot, doubl
     const double R_roe = (srR * Rr + srL * Rl) * inv_sr;
     const double T_roe = (srR * Tr + srL * Tl) * inv_sr;
     const double invW = g.R;                                // Runiv / Wm_tab
-    const double hl = g.cp * Tl;                            // h_tab lerp at Tl
-    const double hr = g.cp * Tr;
+    const double hl = h_of_T(g, Tl);                        // h_tab lerp at Tl
+    const double hr = h_of_T(g, Tr);
     const double el = hl - invW * Tl;
     const double er = hr - invW * Tr;
     h0l = 0.0 + hl * dl * inv_dltot;
     h0r = 0.0 + hr * dr * inv_drtot;
     const double d_roe = (srR * dr * inv_drtot + srL * dl * inv_dltot) * inv_sr;
-    const double cv_roe = 0.0 + d_roe * (0.5 * (g.cp + g.cp) - invW);
+    const double cv_roe = 0.0 + d_roe * (0.5 * (cp_of_T(g, Tl) + cp_of_T(g, Tr)) - invW);
     const double sum_ei = 0.0 + d_roe * (srR * er + srL * el) * inv_sr;
     h0l = h0l + 0.5 * (ul * ul + vl * vl);
     h0r = h0r + 0.5 * (ur * ur + vr * vr);
@@ -805,6 +862,7 @@ struct Case {
 struct q2d_oracle {
     q2d_options opt;
     Gas gas;
+    std::vector<double> htab, cptab;   // thermally perfect table (empty: constant cp)
     std::vector<Block> blk;
     std::vector<Case> cases;
     bool committed = false;
@@ -1345,7 +1403,7 @@ InflowGeom inflow_geometry(const q2d_oracle* o, const Block& B, int Im, int Jm, 
     G.Un = G.Bp[1] * G.n0 + G.Bp[2] * G.n1;
     G.rho = G.Bp[0];
     G.Sound = f_ss(o->gas, G.Bp[3], G.rho);
-    G.Gamma = o->gas.gamma;
+    G.Gamma = f_gamma(o->gas, G.Bp[3], G.rho);
     G.Riem = G.Sound + G.BC_Sign * 0.5 * (G.Gamma - 1.0) * G.Un;
     return G;
 }
@@ -1396,7 +1454,7 @@ bool bc_stagnation(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm, const 
     const double fu = Un3 * G.n0 + Ut3 * G.t0;
     const double fv = Un3 * G.n1 + Ut3 * G.t1;
     const double Face_T = p3 / (Rg * Face_rho);
-    const double Face_H = 0.0 + Face_r1 / Face_rho * (o->gas.cp * Face_T);
+    const double Face_H = 0.0 + Face_r1 / Face_rho * h_of_T(o->gas, Face_T);
     double F[4];
     F[0] = Face_r1 * Un3 * G.int_l;
     const double Fmass = Face_rho * Un3 * G.int_l;
@@ -1471,7 +1529,7 @@ bool bc_outflow(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm, const q2d
     const Gas& g = o->gas;
     const double rho = Bp[0];
     const double Sound = f_ss(g, Bp[3], rho);
-    const double Gamma = g.gamma;
+    const double Gamma = f_gamma(g, Bp[3], rho);
     const double Riem = Sound + BC_Sign * 0.5 * (Gamma - 1.0) * Un;
     const double vtx = Bp[1] - Un * n0, vty = Bp[2] - Un * n1;
     const double Mach_N = std::fabs(Un / Sound);
@@ -1496,7 +1554,7 @@ bool bc_outflow(const q2d_oracle* o, Block& B, int Im, int Jm, int Fm, const q2d
         Face_rho = rho;
     }
     const double Face_T = Face[3] / (g.R * Face_rho);
-    const double Face_H = 0.0 + Face[0] / Face_rho * (g.cp * Face_T);
+    const double Face_H = 0.0 + Face[0] / Face_rho * h_of_T(g, Face_T);
     double F[4];
     F[0] = Face[0] * int_l * Face_Un;
     const double mdot = Face_rho * int_l * Face_Un;
@@ -1624,7 +1682,7 @@ bool newstate(const q2d_oracle* o, Block& B, int irk, int& ei, int& ej, bool sca
             prim2cons(g, primold, consold);
             prim2cons(g, prim, cons);
             for (int v = 0; v < 4; ++v) cons[v] = consold[v] + (cons[v] - consold[v] + res[v]) * c;
-            cons2prim(g, cons, prim);
+            cons2prim(g, cons, prim, prim[3] / (prim[0] * g.R));   // guess: the state before
             bool bad = false;
             for (int v = 0; v < 4; ++v) bad = bad || std::isnan(prim[v]);
             if (bad || prim[3] < 0.0) {
@@ -1989,6 +2047,22 @@ int q2d_oracle_set_case_time(q2d_oracle* o, int case_id, double time) {
     return Q2D_OK;
 }
 
+int q2d_oracle_set_thermo_table(q2d_oracle* o, int ntab, const double* h_tab, const double* cp_tab) {
+    if (!o || o->committed || ntab < 2 || !h_tab || !cp_tab) return Q2D_ERR_BADARG;
+    if (o->opt.precision != Q2D_PREC_FP64 || o->opt.riemann > Q2D_RIEMANN_LLF || o->opt.shock_detector)
+        return Q2D_ERR_BADARG;   // HLLC, HLLE and LLF in the FP64 form
+    for (int k = 0; k < ntab; ++k)
+        if (!std::isfinite(h_tab[k]) || !(cp_tab[k] > o->gas.R)) return Q2D_ERR_BADARG;
+    for (int k = 0; k + 1 < ntab; ++k)   // e(T) = h - R T increasing: an invertible energy
+        if (!(h_tab[k + 1] - h_tab[k] > o->gas.R)) return Q2D_ERR_BADARG;
+    o->htab.assign(h_tab, h_tab + ntab);
+    o->cptab.assign(cp_tab, cp_tab + ntab);
+    o->gas.htab = o->htab.data();
+    o->gas.cptab = o->cptab.data();
+    o->gas.ntab = ntab;
+    return Q2D_OK;
+}
+
 int q2d_oracle_set_case_end(q2d_oracle* o, int case_id, long long iter_end) {
     if (!o || case_id < 0 || case_id >= (int)o->cases.size() || iter_end < 0) return Q2D_ERR_BADARG;
     o->cases[case_id].iter_end = iter_end;
@@ -2082,6 +2156,28 @@ void q2d_oracle_riemann(int kind, const q2d_options* opt, const double* L, const
     const double aL = f_ss(g, L[3], L[0]), aR = f_ss(g, R[3], R[0]);
     const Flux4 F = riemann(kind, g, L, aL, R, aR, nx, ny);
     flux4[0] = F.r; flux4[1] = F.u; flux4[2] = F.v; flux4[3] = F.e;
+}
+
+int q2d_oracle_thermo_tab(int kind, const q2d_options* opt, int ntab, const double* h_tab, const double* cp_tab,
+                          const double* L, const double* R, double nx, double ny, double* out) {
+    if (!opt || ntab < 2 || !h_tab || !cp_tab || !L || !R || !out || kind < 0 || kind > Q2D_RIEMANN_LLF)
+        return Q2D_ERR_BADARG;
+    Gas g;
+    g.R = opt->gas_R; g.gamma = opt->gas_gamma; g.gm1 = g.gamma - 1.0;
+    g.cp = g.gamma * g.R / g.gm1; g.cv = g.R / g.gm1;
+    g.htab = h_tab; g.cptab = cp_tab; g.ntab = ntab;
+    const double aL = f_ss(g, L[3], L[0]), aR = f_ss(g, R[3], R[0]);
+    const Flux4 F = riemann(kind, g, L, aL, R, aR, nx, ny);
+    out[0] = F.r; out[1] = F.u; out[2] = F.v; out[3] = F.e;
+    double h0l, h0r, rho_roe, u_roe, v_roe, a_roe, h0_roe;
+    roe_averages(g, L[0], R[0], L[0], R[0], L[1], L[2], R[1], R[2], L[3], R[3], h0l, h0r, rho_roe, u_roe,
+                 v_roe, a_roe, h0_roe);
+    out[4] = aL; out[5] = aR; out[6] = a_roe; out[7] = h0_roe;
+    double U[4], P[4];
+    prim2cons(g, L, U);
+    cons2prim(g, U, P, 0.5 * L[3] / (L[0] * g.R));   // a guess far from the answer
+    out[8] = U[3]; out[9] = P[3];
+    return Q2D_OK;
 }
 
 void q2d_oracle_riemann_sd(int kind, const q2d_options* opt, const double* L, const double* R,

@@ -12,7 +12,10 @@
  * reference's committed outputs (tests/golden/: ShuOsher limiter baselines written by the
  * reference binary, exact Riemann solutions) — see tests/test_oracle_golden.py.
  * Thermodynamics uses the calorically perfect single-species closure that the reference's
- * constant-cp gas tables imply (h = cp T, e = cv T, a = sqrt(gamma p / rho)).
+ * constant-cp gas tables imply (h = cp T, e = cv T, a = sqrt(gamma p / rho)), or a thermally
+ * perfect single-species table (q2d_oracle_set_thermo_table). The table form is unpinned:
+ * FLINT, which holds the reference's table routines, is absent, and no reference case uses a
+ * variable-cp table; it is checked against closed forms of its own.
  *
  * The exported API mirrors include/q2d_gpu.h one to one (q2d_oracle_* <-> q2d_gpu_*), so a
  * test drives both through the same sequence of calls.
@@ -35,6 +38,7 @@ int  q2d_oracle_set_bcs(q2d_oracle* o, int case_id, const q2d_bc_rec* recs, int 
 int  q2d_oracle_upload_prim(q2d_oracle* o, int block_id, const double* P);
 int  q2d_oracle_set_case_time(q2d_oracle* o, int case_id, double time);
 int  q2d_oracle_set_case_end(q2d_oracle* o, int case_id, long long iter_end);
+int  q2d_oracle_set_thermo_table(q2d_oracle* o, int ntab, const double* h_tab, const double* cp_tab);
 int  q2d_oracle_commit(q2d_oracle* o);
 int  q2d_oracle_step(q2d_oracle* o, int nsteps, q2d_step_info* out);
 int  q2d_oracle_case_info(q2d_oracle* o, int case_id, q2d_step_info* out);
@@ -56,6 +60,13 @@ int  q2d_oracle_shock_sensor(q2d_oracle* o, int block_id, double* beta);
 double q2d_oracle_limiter(int limiter, double x, double y);
 double q2d_oracle_sd_tramel(double p, double p1, double p2, double p3, double p4);
 /* the Riemann solver with the shock sensor beta the sensor-driven solvers blend by */
+/* Thermally perfect gas on a table (h, cp at T = 0 .. ntab-1 K), for known-answer tests: out[0..3]
+ * the flux of solver `riemann` (HLLC, HLLE, LLF), out[4], out[5] the sound speeds of the two
+ * states, out[6] the Roe-averaged sound speed, out[7] the Roe-averaged total enthalpy, out[8]
+ * rho E of primL, out[9] the pressure recovered from it (cons2prim from a guess of half its T). */
+int    q2d_oracle_thermo_tab(int riemann, const q2d_options* opt, int ntab, const double* h_tab,
+                             const double* cp_tab, const double* primL, const double* primR,
+                             double nx, double ny, double* out);
 void   q2d_oracle_riemann_sd(int riemann, const q2d_options* opt, const double* primL,
                              const double* primR, double beta, double nx, double ny, double* flux4);
 void   q2d_oracle_riemann(int riemann, const q2d_options* opt, const double* primL,

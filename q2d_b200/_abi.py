@@ -129,6 +129,7 @@ def _declare(lib: C.CDLL, prefix: str, ctx_t) -> None:
         "upload_prim": (C.c_int, [ctx_t, C.c_int, P(C.c_double)]),
         "set_case_time": (C.c_int, [ctx_t, C.c_int, C.c_double]),
         "set_case_end": (C.c_int, [ctx_t, C.c_int, C.c_longlong]),
+        "set_thermo_table": (C.c_int, [ctx_t, C.c_int, P(C.c_double), P(C.c_double)]),
         "commit": (C.c_int, [ctx_t]),
         "step": (C.c_int, [ctx_t, C.c_int, P(StepInfo)]),
         "case_info": (C.c_int, [ctx_t, C.c_int, P(StepInfo)]),

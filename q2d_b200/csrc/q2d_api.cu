@@ -166,7 +166,9 @@ struct q2d_ctx {
     DevBuf<EdgeRec> edges;
     DevBuf<BCParam> bcp;
     DevBuf<int> flag;
+    DevBuf<double> TAB;             // thermally perfect gas table: h(T) then cp(T), ntab knots each
     CaseState* h_state = nullptr;   // pinned mirror
+    CaseState* h_fresh = nullptr;   // pinned starting run states of the cases being uploaded
     char* pin = nullptr;            // pinned staging area of admissions (serving contexts)
     size_t pin_cap = 0, pin_used = 0;
     int n_items = 0;
@@ -635,7 +637,8 @@ int prepare_case(q2d_ctx* ctx, int c) {
 
 // Device half: copies the staged images into the case's regions and starts its run state.
 // Called only while no work is in flight on the context's stream. The copies are queued on the
-// stream; images in the pinned staging area stay allocated until finish_uploads().
+// stream (heap images wait for theirs); the caller synchronises the stream before the pinned
+// staging area or the pinned run states are reused.
 int upload_case(q2d_ctx* ctx, int c) {
     HCase& cs = ctx->cases[c];
     const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
@@ -657,9 +660,8 @@ int upload_case(q2d_ctx* ctx, int c) {
         if (S.heap) CK(cudaStreamSynchronize(s));   // a heap image is freed right away
         S = Staged{};
     }
-    const CaseState st = fresh_state(cs.time0, cs.iter_end);
-    CK(cudaMemcpyAsync(ctx->cstate.p + c, &st, sizeof(CaseState), h2d, s));
-    CK(cudaStreamSynchronize(s));   // st is on this stack frame
+    ctx->h_fresh[c] = fresh_state(cs.time0, cs.iter_end);   // one pinned entry per slot
+    CK(cudaMemcpyAsync(ctx->cstate.p + c, ctx->h_fresh + c, sizeof(CaseState), h2d, s));
     cs.resident = true;
     ctx->dt_new = true;
     return Q2D_OK;
@@ -744,7 +746,8 @@ int apply_pending(q2d_ctx* ctx) {
         if (cs.used && cs.prepared && !cs.resident)
             if (int e = upload_case(ctx, (int)c)) return e;
     }
-    ctx->pin_used = 0;   // every staged image has been uploaded (upload_case waits for its copies)
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->pin_used = 0;   // every staged image has been uploaded
     if (int e = rebuild_device_lists(ctx)) return e;
     ctx->dirty = false;
     return Q2D_OK;
@@ -764,6 +767,7 @@ int allocate_pools(q2d_ctx* ctx, long long ec, long long eg, long long efi, long
     CK(ctx->cstate.alloc(ncases));
     CK(ctx->flag.alloc(1));
     CK(cudaMallocHost(&ctx->h_state, sizeof(CaseState) * ncases));
+    CK(cudaMallocHost(&ctx->h_fresh, sizeof(CaseState) * ncases));
     std::vector<CaseState> st(ncases, empty_state());   // empty slots read as finished
     CK(cudaMemcpy(ctx->cstate.p, st.data(), sizeof(CaseState) * ncases, cudaMemcpyHostToDevice));
     return Q2D_OK;
@@ -786,6 +790,7 @@ int commit(q2d_ctx* ctx) {
         if (int e = prepare_case(ctx, (int)c)) return e;
         if (int e = upload_case(ctx, (int)c)) return e;
     }
+    CK(cudaStreamSynchronize(ctx->stream));
     if (int e = rebuild_device_lists(ctx)) return e;
     ctx->committed = true;
     ctx->dt_valid = false;
@@ -1030,6 +1035,28 @@ int q2d_gpu_set_case_time(q2d_ctx* ctx, int case_id, double time) {
     return Q2D_OK;
 }
 
+int q2d_gpu_set_thermo_table(q2d_ctx* ctx, int ntab, const double* h_tab, const double* cp_tab) {
+    if (!ctx || ctx->committed || ctx->serving || ntab < 2 || ntab > (1 << 20) || !h_tab || !cp_tab)
+        return fail(ctx, Q2D_ERR_BADARG, "set_thermo_table: bad argument or after commit");
+    if (ctx->opt.precision != Q2D_PREC_FP64 || ctx->opt.riemann > Q2D_RIEMANN_LLF || ctx->opt.shock_detector)
+        return fail(ctx, Q2D_ERR_BADARG, "set_thermo_table: plain FP64 form with HLLC, HLLE or LLF only");
+    const double R = ctx->gas.R;
+    for (int k = 0; k < ntab; ++k)
+        if (!std::isfinite(h_tab[k]) || !(cp_tab[k] > R))
+            return fail(ctx, Q2D_ERR_BADARG, "set_thermo_table: h not finite or cp <= R");
+    for (int k = 0; k + 1 < ntab; ++k)
+        if (!(h_tab[k + 1] - h_tab[k] > R))
+            return fail(ctx, Q2D_ERR_BADARG, "set_thermo_table: internal energy not increasing");
+    ctx->TAB.release();
+    CK(ctx->TAB.alloc(2 * (size_t)ntab));
+    CK(cudaMemcpy(ctx->TAB.p, h_tab, sizeof(double) * ntab, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->TAB.p + ntab, cp_tab, sizeof(double) * ntab, cudaMemcpyHostToDevice));
+    ctx->gas.htab = ctx->TAB.p;
+    ctx->gas.cptab = ctx->TAB.p + ntab;
+    ctx->gas.ntab = ntab;
+    return Q2D_OK;
+}
+
 int q2d_gpu_set_case_end(q2d_ctx* ctx, int case_id, long long iter_end) {
     if (!ctx || case_id < 0 || case_id >= (int)ctx->cases.size() ||
         (ctx->serving && !ctx->cases[case_id].used) || iter_end < 0 || iter_end > 2000000000LL)
@@ -1138,8 +1165,14 @@ static int transfer_many(q2d_ctx* ctx, int n, const int* ids, double* const* P, 
         if (ids[k] < 0 || ids[k] >= (int)ctx->blocks.size() || !P[k] || ctx->blocks[ids[k]].case_id < 0)
             return fail(ctx, Q2D_ERR_BADARG, "transfer: bad block id or array");
     }
-    if (!up) {
-        if (int e = ready(ctx)) return e;
+    if (!up) {   // a serving context reads resident cases without applying admissions first
+        bool all_resident = ctx->serving;
+        for (int k = 0; k < n && all_resident; ++k) {
+            const HBlock& b = ctx->blocks[ids[k]];
+            all_resident = b.alive && ctx->cases[b.case_id].resident;
+        }
+        if (!all_resident)
+            if (int e = ready(ctx)) return e;
     }
     long long need_max = 0, total = 0;
     for (int k = 0; k < n; ++k) {
@@ -1452,8 +1485,9 @@ void q2d_gpu_destroy(q2d_ctx* ctx) {
     ctx->RA.release(); ctx->RB.release();
     ctx->DL32.release(); ctx->FI4.release(); ctx->FJ4.release();
     ctx->dcases.release(); ctx->cstate.release(); ctx->items.release(); ctx->edges.release();
-    ctx->bcp.release(); ctx->flag.release();
+    ctx->bcp.release(); ctx->flag.release(); ctx->TAB.release();
     if (ctx->h_state) cudaFreeHost(ctx->h_state);
+    if (ctx->h_fresh) cudaFreeHost(ctx->h_fresh);
     if (ctx->pin) cudaFreeHost(ctx->pin);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;

@@ -144,7 +144,7 @@ static __device__ bool bc_stagnation(const Gas& g, int Fm, const double* Bp, dou
     const double BC_Sign = modfm2;
     const double Un = Bp[1] * n0 + Bp[2] * n1;
     if (BC_Sign * Un >= 0.0) return false;
-    const double Gamma = g.gamma;
+    const double Gamma = f_gamma(g, Bp[3], Bp[0]);
     const double Sound = f_ss(g, Bp[3], Bp[0]);
     const double Riem = Sound + BC_Sign * 0.5 * (Gamma - 1.0) * Un;
     const double alpha = inflow_direction(n0, n1, bp.alpha);
@@ -180,7 +180,7 @@ static __device__ bool bc_stagnation(const Gas& g, int Fm, const double* Bp, dou
     const double fu = Un3 * n0 + Ut3 * bp.t0;
     const double fv = Un3 * n1 + Ut3 * bp.t1;
     const double Face_T = p3 / (g.R * Face_rho);
-    const double Face_H = 0.0 + Face_r1 / Face_rho * (g.cp * Face_T);
+    const double Face_H = 0.0 + Face_r1 / Face_rho * h_of_T(g, Face_T);
     X[0] = Face_r1 * Un3 * int_l;
     const double Fmass = Face_rho * Un3 * int_l;
     X[1] = Fmass * fu + p3 * int_l * n0;
@@ -242,7 +242,7 @@ static __device__ bool bc_outflow(const Gas& g, int Fm, const double* Bp, double
     if (BC_Sign * Un < 0.0) return false;
     const double rho = Bp[0];
     const double Sound = f_ss(g, Bp[3], rho);
-    const double Gamma = g.gamma;
+    const double Gamma = f_gamma(g, Bp[3], rho);
     const double Riem = Sound + BC_Sign * 0.5 * (Gamma - 1.0) * Un;
     const double vtx = Bp[1] - Un * n0, vty = Bp[2] - Un * n1;
     const double Mach_N = fabs(Un / Sound);
@@ -267,7 +267,7 @@ static __device__ bool bc_outflow(const Gas& g, int Fm, const double* Bp, double
         Face_rho = rho;
     }
     const double Face_T = Face[3] / (g.R * Face_rho);
-    const double Face_H = 0.0 + Face[0] / Face_rho * (g.cp * Face_T);
+    const double Face_H = 0.0 + Face[0] / Face_rho * h_of_T(g, Face_T);
     X[0] = Face[0] * int_l * Face_Un;
     const double mdot = Face_rho * int_l * Face_Un;
     X[1] = Face[1] * mdot + Face[3] * int_l * n0;
@@ -471,10 +471,10 @@ __device__ void block_reduce_store(double* acc, double* red, double* out) {
 }
 
 // Compute_dt body for one cell (Mod_dt.f90:59-104), model == 0, plus the CFL ramp (:43).
-__device__ __forceinline__ double cell_dt(const StageArgs& a, const double* P, const double* sc,
+__device__ __forceinline__ double cell_dt(const StageArgs& a, const Gas& g, const double* P, const double* sc,
                                           long long cidx, long long pc, double dl_i, double dl_j,
                                           int ndir, long long iter_next) {
-    const double Sound = f_ss(a.gas, P[3], P[0]);
+    const double Sound = f_ss(g, P[3], P[0]);
     double dtmin = 1e8;
     {
         const double v0 = sc[2 * pc + cidx], v1 = sc[3 * pc + cidx];

@@ -89,6 +89,9 @@ struct Gas {
     double igm1;   // 1 / (gamma - 1)
     int rkind;     // the Riemann solver (Q2D_RIEMANN_*): selects among the ones of the generic form
     double minf;   // riemann-options-Minf (AUSM+-up, AUSM+-up2)
+    const double* htab;    // thermally perfect gas: h(T) [J/kg] at T = 0, 1, .. ntab-1 K (null:
+    const double* cptab;   //   calorically perfect); cp(T) [J/(kg K)] on the same knots
+    int ntab;
 };
 
 struct StageArgs {
@@ -136,17 +139,68 @@ struct StageArgs {
 };
 
 // ---------------------------------------------------------------------------------------
-// Calorically perfect closure (the oracle's THERMO section): a = sqrt(gamma p / rho),
+// Single-species closures (FLINT_Lib_Thermodynamic's roles; formulas of docs/theory/thermo.md:
+// 39-99 of the reference). Calorically perfect: a = sqrt(gamma p / rho),
 // E0 = p/((gamma-1) rho) + |V|^2/2, H0 = gamma p/((gamma-1) rho) + |V|^2/2, h = cp T.
+// Thermally perfect (g.htab set): h(T), cp(T) interpolated linearly at int(T) on 1-K knots,
+// T = p / (rho R), gamma(T) = cp / (cp - R), E0 = h(T) - p/rho + |V|^2/2, H0 = h(T) + |V|^2/2,
+// and the state from the conserved variables by solving e(T) = h(T) - R T on the table.
 // ---------------------------------------------------------------------------------------
+__device__ __forceinline__ int tab_knot(const Gas& g, double T) {   // int(T), kept in the table
+    if (!(T >= 0.0)) return 0;
+    if (T >= (double)(g.ntab - 2)) return g.ntab - 2;
+    return (int)T;
+}
+__device__ __forceinline__ double tab_at(const Gas& g, const double* t, double T) {
+    const int Ti = tab_knot(g, T);
+    const double dT = T - Ti;
+    const double a = __ldg(t + Ti), b = __ldg(t + Ti + 1);
+    return a + (b - a) * dT;
+}
+__device__ __forceinline__ double h_of_T(const Gas& g, double T) {
+    return g.htab ? tab_at(g, g.htab, T) : g.cp * T;
+}
+__device__ __forceinline__ double cp_of_T(const Gas& g, double T) {
+    return g.htab ? tab_at(g, g.cptab, T) : g.cp;
+}
+__device__ __forceinline__ double f_gamma(const Gas& g, double p, double rho) {
+    if (!g.htab) return g.gamma;
+    const double cp = tab_at(g, g.cptab, p / (rho * g.R));
+    return cp / (cp - g.R);
+}
 __device__ __forceinline__ double f_ss(const Gas& g, double p, double rho) {
+    if (g.htab) return sqrt(f_gamma(g, p, rho) * p / rho);
     return sqrt(g.gamma * p / rho);
 }
 __device__ __forceinline__ double E0(const Gas& g, double p, double rho, double modv) {
+    if (g.htab) return tab_at(g, g.htab, p / (rho * g.R)) - p / rho + 0.5 * modv * modv;
     return p / (g.gm1 * rho) + 0.5 * modv * modv;
 }
 __device__ __forceinline__ double H0(const Gas& g, double p, double rho, double modv) {
+    if (g.htab) return tab_at(g, g.htab, p / (rho * g.R)) + 0.5 * modv * modv;
     return g.gamma * p / (g.gm1 * rho) + 0.5 * modv * modv;
+}
+// rho E of a primitive state on the table: rho h(T) - p + rho |V|^2 / 2.
+__device__ __forceinline__ double rhoE_tab(const Gas& g, const double* P) {
+    return P[0] * tab_at(g, g.htab, P[3] / (P[0] * g.R)) - P[3] + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
+}
+// Temperature of the specific internal energy e on the table, from the knot interval of the
+// guess T0 walked to the interval holding e (e(T) increases with T where cp > R), then solved
+// exactly on that interval (e is linear between knots).
+__device__ __forceinline__ double T_of_e(const Gas& g, double e, double T0) {
+    int k = tab_knot(g, T0);
+    double ek = __ldg(g.htab + k) - g.R * (double)k;
+    for (int w = 0; w < g.ntab && k > 0 && e < ek; ++w) {
+        --k;
+        ek = __ldg(g.htab + k) - g.R * (double)k;
+    }
+    double ek1 = __ldg(g.htab + k + 1) - g.R * (double)(k + 1);
+    for (int w = 0; w < g.ntab && k < g.ntab - 2 && e >= ek1; ++w) {
+        ++k;
+        ek = ek1;
+        ek1 = __ldg(g.htab + k + 1) - g.R * (double)(k + 1);
+    }
+    return (double)k + (e - ek) / (ek1 - ek);
 }
 __device__ __forceinline__ bool gas_state_bad(double rho, double p) {
     return !(rho > 0.0) || !(p > 0.0);
@@ -300,14 +354,14 @@ __device__ __forceinline__ void roe_averages(const Gas& g, double dltot, double 
     v_roe = (srR * vr + srL * vl) * inv_sr;
     const double R_roe = (srR * g.R + srL * g.R) * inv_sr;
     const double T_roe = (srR * Tr + srL * Tl) * inv_sr;
-    const double hl = g.cp * Tl;
-    const double hr = g.cp * Tr;
+    const double hl = h_of_T(g, Tl);
+    const double hr = h_of_T(g, Tr);
     const double el = hl - g.R * Tl;
     const double er = hr - g.R * Tr;
     h0l = 0.0 + hl * dltot * inv_dltot;
     h0r = 0.0 + hr * drtot * inv_drtot;
     const double d_roe = (srR * drtot * inv_drtot + srL * dltot * inv_dltot) * inv_sr;
-    const double cv_roe = 0.0 + d_roe * (0.5 * (g.cp + g.cp) - g.R);
+    const double cv_roe = 0.0 + d_roe * (0.5 * (cp_of_T(g, Tl) + cp_of_T(g, Tr)) - g.R);
     const double sum_ei = 0.0 + d_roe * (srR * er + srL * el) * inv_sr;
     h0l = h0l + 0.5 * (ul * ul + vl * vl);
     h0r = h0r + 0.5 * (ur * ur + vr * vr);

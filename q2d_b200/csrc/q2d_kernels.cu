@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(NT) dt_kernel(const StageArgs a) {
             for (int v = 0; v < 4; ++v) P[v] = a.Pin[B.oc + v * B.pc + cg];
             const long long gidx = B.og + (long long)(jj + 2) * (B.ni + 4) + (ii + 2);
             const double* scb = a.sc + 2 * B.oc;
-            const double dtn = cell_dt(a, P, scb, cg, B.pc, a.dl[gidx], a.dl[gidx + B.pg], ndir, iter_next);
+            const double dtn = cell_dt(a, a.gas, P, scb, cg, B.pc, a.dl[gidx], a.dl[gidx + B.pg], ndir, iter_next);
             if (!a.time_accurate) a.sc[2 * B.oc + B.pc + cg] = dtn;
             acc[4] = fmin(acc[4], dtn);
         }
@@ -164,7 +164,11 @@ cudaError_t launch_stage(const StageArgs& a, int prec, int riem, int tile, int g
     if (a.sd || riem == 5 || riem == 6) return launch_stage_sd(a, prec, riem, tile, grid, s);   // the sensor runs
     cudaError_t e = cudaErrorInvalidValue;
 #define Q2D_CALL(TX, TY, NT)                                                                   \
-    if (prec == 0) {                                                                           \
+    if (prec == 0 && a.gas.htab) {   /* thermally perfect gas: HLLC, HLLE, LLF */              \
+        if (riem == 1) e = launch_stage_t<0, 1, TX, TY, NT, false, true>(a, grid, s);                \
+        else if (riem == 2) e = launch_stage_t<0, 2, TX, TY, NT, false, true>(a, grid, s);           \
+        else if (riem == 0) e = launch_stage_t<0, 0, TX, TY, NT, false, true>(a, grid, s);           \
+    } else if (prec == 0) {                                                                    \
         if (riem == 1) e = launch_stage_t<0, 1, TX, TY, NT, false>(a, grid, s);                      \
         else if (riem == 2) e = launch_stage_t<0, 2, TX, TY, NT, false>(a, grid, s);                 \
         else if (riem == 3) e = launch_stage_t<0, 3, TX, TY, NT, false>(a, grid, s);                 \

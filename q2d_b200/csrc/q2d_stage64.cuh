@@ -87,7 +87,7 @@ __device__ __forceinline__ void sigma_phase(const ST* sSi, const ST* sSj, ST* sG
 // boundary cell (Lib_BC_Fluxes_Connection.f90, beta_ = blk%beta(Im,Jm)). It scales both limited
 // slopes under MUSCL-SD (a.sd) and goes to the Riemann solver.
 template <int PREC, int RIEM, bool IDIR, int NT, int TX, int TY, bool SD, typename ST>
-__device__ __forceinline__ void face_phase(const StageArgs& a, const DBlock& B, CaseState* cs, int i0,
+__device__ __forceinline__ void face_phase(const StageArgs& a, const Gas& g, const DBlock& B, CaseState* cs, int i0,
                                            int j0, const double* sP, const double* sD,
                                            const double* sG, const ST* sg, const double* sB, double* sF) {
     constexpr int W = TX + 4, AREA = W * (TY + 4);
@@ -126,7 +126,7 @@ __device__ __forceinline__ void face_phase(const StageArgs& a, const DBlock& B, 
                 QL[v] = sP[v * AREA + pL] + (double)(beta_l * sg[v * NG + gL] * lm);
                 QR[v] = sP[v * AREA + pL + DSTEP] - (double)(beta_l * sg[v * NG + gR] * lp);
             }
-            if (!face_flux<PREC, RIEM>(a.gas, QL, QR, nx, ny, ln, X, beta))
+            if (!face_flux<PREC, RIEM>(g, QL, QR, nx, ny, ln, X, beta))
                 record_error(cs, 4, B.local_b, IDIR ? pos : k + 1, IDIR ? k + 1 : pos, a.irk);
         } else if (etype >= 0) {
             const bool minside = (Fm == 1 || Fm == 3);
@@ -136,7 +136,7 @@ __device__ __forceinline__ void face_phase(const StageArgs& a, const DBlock& B, 
 #pragma unroll
             for (int v = 0; v < 4; ++v) { Bp.v[v] = sP[v * AREA + cb]; Ip.v[v] = sP[v * AREA + ci]; }
             const int prm = a.edges[B.eo[Fm - 1] + k].param;
-            const Q4 q = bc_face<RIEM>(a.gas, a.limiter, etype, Fm, Bp, Ip, dlp[cb], dlp[ci], nx, ny, ln,
+            const Q4 q = bc_face<RIEM>(g, a.limiter, etype, Fm, Bp, Ip, dlp[cb], dlp[ci], nx, ny, ln,
                                        prm >= 0 ? a.bcp + prm : nullptr);
 #pragma unroll
             for (int v = 0; v < 4; ++v) X[v] = q.v[v];
@@ -149,7 +149,9 @@ __device__ __forceinline__ void face_phase(const StageArgs& a, const DBlock& B, 
     }
 }
 
-template <int PREC, int RIEM, int TX, int TY, int NT, bool SD>
+// TAB: the thermally perfect gas (a.gas.htab set); without it the calorically perfect closure
+// is fixed at compile time.
+template <int PREC, int RIEM, int TX, int TY, int NT, bool SD, bool TAB = false>
 __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
     using L = Tile<PREC, TX, TY, SD>;
     using ST = typename L::ST;
@@ -172,7 +174,8 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
     __shared__ double tile_part[5];
     __shared__ int s_flag;
     const int tid = threadIdx.x;
-    const Gas& g = a.gas;
+    Gas g = a.gas;
+    if (!TAB) g.htab = nullptr;
     const int lim = a.limiter;
 
     for (int it = blockIdx.x; it < a.n_items; it += gridDim.x) {
@@ -323,8 +326,8 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
             __syncthreads();
 
             // ---- 5. face fluxes (interior: Riemann on MUSCL states; boundary: BC_Fluxes) -----
-            face_phase<PREC, RIEM, true, NT, TX, TY, SD>(a, B, cs, i0, j0, sP, sD, sGi, sGI, sB, sFi);
-            face_phase<PREC, RIEM, false, NT, TX, TY, SD>(a, B, cs, i0, j0, sP, sD, sGj, sGJ, sB, sFj);
+            face_phase<PREC, RIEM, true, NT, TX, TY, SD>(a, g, B, cs, i0, j0, sP, sD, sGi, sGI, sB, sFi);
+            face_phase<PREC, RIEM, false, NT, TX, TY, SD>(a, g, B, cs, i0, j0, sP, sD, sGj, sGJ, sB, sFj);
         }
         __syncthreads();
 
@@ -410,7 +413,10 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
             for (int v = 0; v < 4; ++v) PO[v] = a.first ? P[v] : sC[v * NC + k];
             double U0[4], U[4];
             U0[0] = PO[0]; U0[1] = PO[0] * PO[1]; U0[2] = PO[0] * PO[2];
-            if (PREC == 0) {
+            if (PREC == 0 && g.htab) {   // thermally perfect gas
+                U0[3] = rhoE_tab(g, PO);
+                U[3] = rhoE_tab(g, P);
+            } else if (PREC == 0) {
                 U0[3] = PO[3] / g.gm1 + 0.5 * PO[0] * (PO[1] * PO[1] + PO[2] * PO[2]);
                 U[3] = P[3] / g.gm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
             } else {
@@ -430,7 +436,11 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
                 N[1] = U[1] * ir;
                 N[2] = U[2] * ir;
             }
-            N[3] = g.gm1 * (U[3] - 0.5 * U[0] * (N[1] * N[1] + N[2] * N[2]));
+            if (PREC == 0 && g.htab)   // cons2prim on the table, guess: the state before the update
+                N[3] = N[0] * g.R *
+                       T_of_e(g, U[3] / U[0] - 0.5 * (N[1] * N[1] + N[2] * N[2]), P[3] / (P[0] * g.R));
+            else
+                N[3] = g.gm1 * (U[3] - 0.5 * U[0] * (N[1] * N[1] + N[2] * N[2]));
             // Check_And_Fix_State (Lib_Newstate.f90:316-350)
             if (isnan(N[0]) || isnan(N[1]) || isnan(N[2]) || isnan(N[3]) || N[3] < 0.0)
                 record_error(cs, 5, B.local_b, i1, j1, a.irk);
@@ -444,7 +454,7 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
                     const double d = fabs(N[v] - PO[v]);
                     acc[v] += d * d;
                 }
-                const double dtn = cell_dt(a, N, scb, cg, pc, sD[sidx], sD[AREA + sidx], ndir, iter_next);
+                const double dtn = cell_dt(a, g, N, scb, cg, pc, sD[sidx], sD[AREA + sidx], ndir, iter_next);
                 if (!a.time_accurate) a.sc[2 * B.oc + pc + cg] = dtn;
                 acc[4] = fmin(acc[4], dtn);
             }
@@ -461,10 +471,10 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
 // ------------------------------------------------------------------------------------------
 // launch helpers (instantiated by q2d_kernels.cu, and by q2d_stage64_sd.cu for MUSCL-SD)
 // ------------------------------------------------------------------------------------------
-template <int PREC, int RIEM, int TX, int TY, int NT, bool SD>
+template <int PREC, int RIEM, int TX, int TY, int NT, bool SD, bool TAB = false>
 cudaError_t launch_stage_t(const StageArgs& a, int grid, cudaStream_t s) {
     constexpr size_t smem = Tile<PREC, TX, TY, SD>::bytes;
-    auto k = stage_kernel<PREC, RIEM, TX, TY, NT, SD>;
+    auto k = stage_kernel<PREC, RIEM, TX, TY, NT, SD, TAB>;
     static bool attr_set = false;
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

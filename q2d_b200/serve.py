@@ -269,7 +269,7 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
         budget_cells = sc.free_cells()
         t0 = clock()
         busy = 0.0
-        t_admit = t_readback = t_retire = 0.0
+        t_admit = t_readback = t_retire = t_launch = 0.0
 
         def now():
             return clock() - t0 if realtime else math.inf
@@ -303,7 +303,8 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
                 admit_due()
                 continue
             tb = clock()
-            sc.step_async(steps_per_call)
+            sc.step_async(steps_per_call)   # applies admissions and retirements, then launches
+            t_launch += clock() - tb
             on_device = set(active.keys())   # cases admitted from here on join the next call
             steps_calls += 1
             ta = clock()
@@ -368,7 +369,8 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
         "p50_service_s": pct(ser, 50), "p99_service_s": pct(ser, 99),
         "retired_by": rules, "median_residual_drop": pct(drops, 50),
         "readback_bytes": int(readback_bytes),
-        "host_s": {"admission_during_steps": t_admit, "readback": t_readback, "retire": t_retire},
+        "host_s": {"apply_and_launch": t_launch, "admission_during_steps": t_admit, "readback": t_readback,
+                   "retire": t_retire},
         "step_calls": steps_calls, "gpu_launches": launches,
         "budget_cells": int(budget_cells),
     }

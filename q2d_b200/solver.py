@@ -32,10 +32,12 @@ class Q2DSolver:
     """A set of cases advanced together through one library context.
 
     lib/prefix select the implementation behind the C ABI: the CUDA library
-    (`q2d_gpu`, default) or another library exporting the same entry points."""
+    (`q2d_gpu`, default) or another library exporting the same entry points. thermo_table =
+    (h, cp), arrays on 1-K knots from 0 K, selects the thermally perfect gas
+    (q2d_gpu_set_thermo_table)."""
 
     def __init__(self, options: _abi.Options, cases: Iterable[CaseSpec], lib=None,
-                 prefix: str = "q2d_gpu"):
+                 prefix: str = "q2d_gpu", thermo_table=None):
         self.lib = lib if lib is not None else _abi.load_library()
         self.prefix = prefix
         self.options = options
@@ -44,6 +46,11 @@ class Q2DSolver:
         self._call("create", C.byref(self.ctx), C.byref(options))
         self.block_ids = []
         try:
+            if thermo_table is not None:
+                h, cp = (np.ascontiguousarray(t, dtype=np.float64) for t in thermo_table)
+                if h.shape != cp.shape or h.ndim != 1:
+                    raise ValueError("thermo_table: h and cp must be 1-D arrays of one length")
+                self._call("set_thermo_table", self.ctx, len(h), _abi.dptr(h), _abi.dptr(cp))
             for cs in self.cases:
                 cid = C.c_int()
                 self._call("add_case", self.ctx, C.byref(cid))

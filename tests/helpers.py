@@ -8,16 +8,17 @@ from q2d_b200 import make_options
 from q2d_b200.solver import Q2DSolver
 
 
-def run_pair(cases, steps: int, chunks: int = 1, schedule=None, **opt_overrides):
+def run_pair(cases, steps: int, chunks: int = 1, schedule=None, thermo_table=None, **opt_overrides):
     """Advances the cases `steps` steps on both implementations (in `chunks` calls; the CUDA
-    library on `schedule` when given) and returns (gpu_states, oracle_states, gpu_infos,
-    oracle_infos); states are lists over cases of lists over blocks of (nj, ni, 4) arrays."""
+    library on `schedule` when given; both on the thermally perfect gas of thermo_table when
+    given) and returns (gpu_states, oracle_states, gpu_infos, oracle_infos); states are lists over
+    cases of lists over blocks of (nj, ni, 4) arrays."""
     from oracle import oracle
     opts = make_options(cases[0], **opt_overrides)
-    g = Q2DSolver(opts, cases)
+    g = Q2DSolver(opts, cases, thermo_table=thermo_table)
     if schedule is not None:
         g.set_schedule(schedule)
-    o = oracle.solver(opts, cases)
+    o = oracle.solver(opts, cases, thermo_table=thermo_table)
     try:
         per = max(1, steps // chunks)
         done = 0
@@ -280,3 +281,17 @@ def split_case(cs, icuts=(), jcuts=()):
                         for k in range(1, ni + 1)]
     bcs.sort(key=lambda r: (r["b"], r["f"], r["j"] if r["f"] <= 2 else r["i"]))
     return dataclasses.replace(cs, name=cs.name + "_split", blocks=blocks, bcs=bcs)
+
+
+def linear_cp_table(a: float = 1000.0, b: float = 0.2, ntab: int = 5000):
+    """A thermally perfect gas with cp(T) = a + b T [J/(kg K)]: the table of cp and of
+    h(T) = a T + b T^2 / 2 on the knots T = 0, 1, .. ntab-1 K (h exact at the knots)."""
+    T = np.arange(ntab, dtype=np.float64)
+    return a * T + 0.5 * b * T * T, a + b * T
+
+
+def constant_cp_table(gamma: float = 1.4, R: float = 287.0, ntab: int = 5000):
+    """The calorically perfect gas written as a table: cp = gamma R / (gamma - 1), h = cp T."""
+    cp = gamma * R / (gamma - 1.0)
+    T = np.arange(ntab, dtype=np.float64)
+    return cp * T, np.full(ntab, cp)
