@@ -69,7 +69,10 @@ __device__ __forceinline__ void sigma_phase(const ST* sSi, const ST* sSj, ST* sG
             else sGI[v * NGI + k] = lim32<LIM>(sSi[v * NSI + sfw], sSi[v * NSI + sfw - 1]);
         }
     }
-    for (int k = threadIdx.x; k < NGJ; k += NT) {
+    // the j slopes start on the warp after the one that took the last i slopes (no barrier in
+    // between): no warp gets two partial rounds
+    constexpr int NW = NT / 32, ROT = ((NGI + 31) / 32) % NW;
+    for (int k = (((int)(threadIdx.x >> 5) - ROT + NW) % NW) * 32 + (int)(threadIdx.x & 31); k < NGJ; k += NT) {
         const int r = k / TX, c = k - r * TX;               // cell at smem row r+1
         const int sfw = (r + 1) * TX + c, sbw = r * TX + c;
 #pragma unroll
@@ -97,7 +100,10 @@ __device__ __forceinline__ void face_phase(const StageArgs& a, const Gas& g, con
     constexpr int DSTEP = IDIR ? 1 : W;
     const int ni = B.ni, nj = B.nj;
     const double* dlp = sD + (IDIR ? 0 : AREA);
-    for (int f = threadIdx.x; f < NF; f += NT) {
+    // j-faces start on the warp after the one that took the last i-faces (the two directions
+    // run back to back with no barrier): every warp has at most ceil((NFI + NFJ) / NT) rounds
+    constexpr int NW = NT / 32, ROT = IDIR ? 0 : (((TX + 1) * TY + 31) / 32) % NW;
+    for (int f = (((int)(threadIdx.x >> 5) - ROT + NW) % NW) * 32 + (int)(threadIdx.x & 31); f < NF; f += NT) {
         const int row = f / ROWLEN, col = f - row * ROWLEN;
         int pos, lenn, k;        // face index along the direction, its limit, edge position
         if (IDIR) { pos = i0 + col; lenn = ni; k = j0 + row; if (k >= nj || pos > ni) continue; }

@@ -508,9 +508,12 @@ std::vector<double> read_area(const std::string& path, const Block& B) {
     return a;
 }
 
-// Gas of the constant-cp single-species tables: R = Runiv / W from phase.txt; gamma from the
-// first thermo.dat row when asked ("table"), else the given value.
-void read_gas(const std::string& dir, const std::string& gamma_arg, q2d_options& o, std::string& note) {
+// Gas of the single-species tables: R = Runiv / W from phase.txt; with "table" gamma from the
+// first thermo.dat row, and when cp varies with temperature the whole table (Temperature, Cp,
+// Enthalpy rows at 1, 2, .. K; knot 0 extrapolated from knots 1 and 2) for the thermally
+// perfect gas (q2d_gpu_set_thermo_table); else gamma is the given value.
+void read_gas(const std::string& dir, const std::string& gamma_arg, q2d_options& o, std::string& note,
+              std::vector<double>& h_tab, std::vector<double>& cp_tab) {
     const double runiv = 8314.46;   // docs/theory/thermo.md:56
     std::ifstream ph(dir + "/INPUT/phase.txt");
     if (!ph) {
@@ -530,24 +533,35 @@ void read_gas(const std::string& dir, const std::string& gamma_arg, q2d_options&
     if (gamma_arg == "table") {
         std::ifstream th(dir + "/INPUT/thermo.dat");
         if (!th) die("--gamma table needs INPUT/thermo.dat");
-        // the calorically perfect closure is exact only for a constant cp (the reference's Air
-        // table: 1004.5 J/(kg K) on every row, 1-10000 K); a temperature-dependent cp needs the
-        // table lerp (Lib_Riemann_HLL.f90:258-303), which this path does not build
+        // a constant cp (the reference's Air table: 1004.5 J/(kg K) on every row, 1-10000 K) is
+        // the calorically perfect closure exactly; a temperature-dependent cp takes the table
+        // lerp (Lib_Riemann_HLL.f90:258-303) of the plain FP64 form
         std::string line;
         double cp0 = 0.0;
         long long rows = 0;
+        bool varies = false;
+        std::vector<double> hs(1, 0.0), cps(1, 0.0);
         while (std::getline(th, line)) {
             auto t = split_list(line);
-            if (t.size() >= 2 && (std::isdigit((unsigned char)t[0][0]) || t[0][0] == '.')) {
-                const double cp = to_double(t[1], "thermo.dat");
+            if (t.size() >= 3 && (std::isdigit((unsigned char)t[0][0]) || t[0][0] == '.')) {
+                const double T = to_double(t[0], "thermo.dat"), cp = to_double(t[1], "thermo.dat");
+                if (T != (double)(rows + 1)) die("INPUT/thermo.dat: rows must be at T = 1, 2, .. K");
                 if (rows++ == 0) cp0 = cp;
-                else if (std::fabs(cp - cp0) > 1e-12 * std::fabs(cp0))
-                    die("INPUT/thermo.dat: cp varies with temperature (" + t[0] +
-                        "): table thermodynamics is not on this path");
+                else if (std::fabs(cp - cp0) > 1e-12 * std::fabs(cp0)) varies = true;
+                cps.push_back(cp);
+                hs.push_back(to_double(t[2], "thermo.dat"));
             }
         }
         if (rows == 0) die("INPUT/thermo.dat: no table rows");
         o.gas_gamma = cp0 / (cp0 - o.gas_R);
+        if (varies) {
+            if (rows < 2) die("INPUT/thermo.dat: a variable-cp table needs two rows or more");
+            hs[0] = 2.0 * hs[1] - hs[2];
+            cps[0] = 2.0 * cps[1] - cps[2];
+            h_tab = std::move(hs);
+            cp_tab = std::move(cps);
+            note += ", thermally perfect table of " + std::to_string(rows) + " K";
+        }
     } else {
         o.gas_gamma = to_double(gamma_arg, "--gamma");
     }
@@ -804,7 +818,8 @@ int run(int argc, char** argv) {
     Setup S = read_options(ini);
     S.opt.precision = A.precision == "fp64" ? Q2D_PREC_FP64 : Q2D_PREC_FP32_FLUX;
     std::string gas_note;
-    read_gas(A.dir, A.gamma, S.opt, gas_note);
+    std::vector<double> h_tab, cp_tab;
+    read_gas(A.dir, A.gamma, S.opt, gas_note, h_tab, cp_tab);
     // newrun: INPUT/ic.tec, its SOLUTIONTIME ignored; restart: the last field written, time-accurate
     // cases resume at its SOLUTIONTIME, steady ones count iterations from int(SOLUTIONTIME)
     // (Wrap_Setup.f90:132-149; the writer stores -iterations there, Wrap_Postprocess.f90:41-47)
@@ -850,7 +865,7 @@ int run(int argc, char** argv) {
                          k ? ", " : "", r.b, r.i, r.j, r.f, r.type, r.bs, r.is, r.js, r.fs, r.d11, r.d12, r.d21, r.d22,
                          r.T0, r.p0, r.pamb, r.mach, r.alpha >= 0.5 * DBL_MAX ? -1.0 : r.alpha, r.rel_fac);
         }
-        std::fprintf(f, "],\n \"sol_format\": ");
+        std::fprintf(f, "],\n \"thermo_knots\": %zu, \"sol_format\": ", h_tab.size());
         json_str(f, S.sol_format);
         std::fprintf(f, ", \"sol_overwrite\": %d, \"probes\": [", S.sol_overwrite ? 1 : 0);
         for (size_t k = 0; k < S.probes.size(); ++k) {
@@ -887,6 +902,9 @@ int run(int argc, char** argv) {
         }
     };
     check(q2d_gpu_create(&ctx, &o), "q2d_gpu_create");
+    if (!h_tab.empty())
+        check(q2d_gpu_set_thermo_table(ctx, (int)h_tab.size(), h_tab.data(), cp_tab.data()),
+              "q2d_gpu_set_thermo_table");
     int cid = -1;
     std::vector<int> bid(blocks.size());
     std::vector<std::vector<double>> P(blocks.size());

@@ -92,9 +92,11 @@ def _bc_lines(r: dict) -> list:
     return out
 
 
-def write_case(cs: CaseSpec, directory, extra_ini: str = "", **option_overrides) -> Path:
+def write_case(cs: CaseSpec, directory, extra_ini: str = "", thermo_table=None, **option_overrides) -> Path:
     """Writes the case directory; options are the case's (make_options) with the overrides.
-    extra_ini is appended to input.ini (more [Q2D-IO] keys, probe sections)."""
+    extra_ini is appended to input.ini (more [Q2D-IO] keys, probe sections). thermo_table =
+    (h, cp) on the knots T = 0, 1, .. K writes INPUT/thermo.dat from knot 1 on (the file's rows
+    start at 1 K); without it the table holds the constant cp of gas_gamma."""
     from .solver import make_options
     o = make_options(cs, **option_overrides)
     d = Path(directory)
@@ -118,12 +120,17 @@ def write_case(cs: CaseSpec, directory, extra_ini: str = "", **option_overrides)
     W = RUNIV / o.gas_R
     (d / "INPUT" / "phase.txt").write_text(f"ideal-gas phase\nair {W!r}\n")
     cp = o.gas_gamma * o.gas_R / (o.gas_gamma - 1.0)
+    if thermo_table is None:
+        rows = [(T, cp, cp * T) for T in (1.0, 2.0)]
+    else:
+        h, c = (np.asarray(t, dtype=np.float64) for t in thermo_table)
+        rows = [(float(T), c[T], h[T]) for T in range(1, len(h))]
     with open(d / "INPUT" / "thermo.dat", "w") as f:
         f.write('TITLE = "Mass Thermodynamic Properties"\n'
                 'VARIABLES = "Temperature", "Cp", "Enthalpy", "Entropy", "dCp"\n'
-                'ZONE T="air"\nI=2, F=POINT\n')
-        for T in (1.0, 2.0):
-            f.write(f"{T:.1f} {cp:.6f} {cp * T:.6f} 0.000000 0.000000\n")
+                f'ZONE T="air"\nI={len(rows)}, F=POINT\n')
+        for T, c_, h_ in rows:
+            f.write(f"{T:.1f} {c_!r} {h_!r} 0.000000 0.000000\n")
     return d
 
 

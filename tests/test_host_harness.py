@@ -226,8 +226,8 @@ def test_restart_input_selection(tmp_path):
 
 def test_gamma_from_the_constant_cp_table(tmp_path):
     """--gamma table: gamma = cp / (cp - R) from INPUT/thermo.dat when cp is the same on every row
-    (the reference's Air table); a temperature-dependent cp is refused (table thermodynamics is
-    not on this path)."""
+    (the reference's Air table); a temperature-dependent cp selects the thermally perfect table
+    (every row, knot 0 extrapolated); rows off the 1-K grid are refused."""
     cs = cases.ramp(20, 8)
     refio.write_case(cs, tmp_path)
     d = json.loads(host(tmp_path, "--check", "--gamma", "table").stdout)
@@ -241,5 +241,10 @@ def test_gamma_from_the_constant_cp_table(tmp_path):
     t[1] = repr(cp * 1.01)
     lines[k] = " ".join(t)
     (tmp_path / "INPUT" / "thermo.dat").write_text("\n".join(lines) + "\n")
+    d = json.loads(host(tmp_path, "--check", "--gamma", "table").stdout)
+    assert d["thermo_knots"] == len(rows) + 1 and d["gas_gamma"] == pytest.approx(cp / (cp - R), rel=1e-15)
+    t[0] = "7.5"
+    lines[k] = " ".join(t)
+    (tmp_path / "INPUT" / "thermo.dat").write_text("\n".join(lines) + "\n")
     r = host(tmp_path, "--check", "--gamma", "table", check=False)
-    assert r.returncode != 0 and "cp varies with temperature" in r.stderr
+    assert r.returncode != 0 and "rows must be at T = 1, 2" in r.stderr

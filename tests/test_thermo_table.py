@@ -236,3 +236,23 @@ def test_gpu_table_refused_outside_the_fp64_hll_forms():
         with pytest.raises(Q2DError) as e:
             Q2DSolver(make_options(cs, **bad), [cs], thermo_table=tab)
         assert e.value.status == _abi.ERR_BADARG
+
+
+@pytest.mark.gpu
+def test_host_runs_a_variable_cp_thermo_dat(tmp_path):
+    """q2d_host --gamma table with a temperature-dependent INPUT/thermo.dat runs the thermally
+    perfect gas: its field equals the library's with the same table (to the 17 digits written)."""
+    from q2d_b200 import refio
+    from tests.test_host_harness import host
+    cs = cases.ramp(40, 14, seed=3)
+    tab = linear_cp_table(A_CP, B_CP, 3000)
+    refio.write_case(cs, tmp_path, itermax=25, thermo_table=tab)
+    host(tmp_path, "--gamma", "table", "--steps-per-call", 10, "--quiet")
+    got = refio.read_field(tmp_path / "OUTPUT" / "field.tec")[0].prim
+    s = Q2DSolver(make_options(cs, itermax=25), [cs], thermo_table=tab)
+    try:
+        s.step(25)
+        want = s.prim(0, 0)
+    finally:
+        s.close()
+    assert rel_linf(got, want).max() <= 1e-15
