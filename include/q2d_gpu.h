@@ -301,12 +301,14 @@ long long q2d_gpu_num_cells(const q2d_ctx* ctx);
  * q2d_serve_admit adds a case between steps: nblocks blocks with the arguments of
  * q2d_gpu_add_block and q2d_gpu_upload_prim (P[b] in the ghosted Fortran layout) and the
  * boundary records of q2d_gpu_set_bcs. It validates the input, computes the metrics and
- * reserves device memory on the host at once, and its device writes are applied by the next
- * step call after the work in flight, so it may overlap a running step. It returns
+ * reserves device memory on the host at once, and queues the copies of its device images on a
+ * copy stream of the context right away (they overlap the steps in flight, into memory that no
+ * listed case uses); its run state is started by the next step call. It returns
  * Q2D_ERR_CAPACITY when no slot is free or the pools cannot hold the case (nothing is kept).
  * The case starts at iteration 0 with a fresh residual reference; the other cases' results do
  * not depend on when it arrives.
- * q2d_serve_retire frees a case's slot and memory (its results are no longer readable).
+ * q2d_serve_retire frees a case's slot and memory (its results are no longer readable); called
+ * while steps are in flight it waits for them first.
  * q2d_serve_block_id maps (case, 1-based block) to the block id of download_prim / upload_prim.
  * q2d_serve_free_cells estimates how many more interior cells the pools can take. */
 int  q2d_serve_create(q2d_ctx** out, const q2d_options* opt, unsigned long long device_bytes, int max_cases);

@@ -60,6 +60,7 @@ struct HCase {
     bool used = false;             // slot holds a case
     bool prepared = false;         // regions reserved, device images staged
     bool resident = false;         // device images and run state uploaded
+    bool images_sent = false;      // device images queued on the copy stream at admission
 };
 
 template <typename T>
@@ -140,6 +141,8 @@ struct q2d_ctx {
     int device = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;   // serving: admissions' image uploads during the steps
+    bool copies_pending = false;
     std::vector<HBlock> blocks;
     std::vector<HCase> cases;     // slots
     bool serving = false;
@@ -170,6 +173,8 @@ struct q2d_ctx {
     CaseState* h_state = nullptr;   // pinned mirror
     CaseState* h_fresh = nullptr;   // pinned starting run states of the cases being uploaded
     char* pin = nullptr;            // pinned staging area of admissions (serving contexts)
+    char* h_lists = nullptr;        // pinned staging of the device work lists
+    size_t h_lists_cap = 0;
     size_t pin_cap = 0, pin_used = 0;
     int n_items = 0;
     std::map<int, cudaGraphExec_t> graphs;
@@ -635,14 +640,14 @@ int prepare_case(q2d_ctx* ctx, int c) {
     return Q2D_OK;
 }
 
-// Device half: copies the staged images into the case's regions and starts its run state.
-// Called only while no work is in flight on the context's stream. The copies are queued on the
-// stream (heap images wait for theirs); the caller synchronises the stream before the pinned
-// staging area or the pinned run states are reused.
-int upload_case(q2d_ctx* ctx, int c) {
+// Device half: copies the staged images into the case's regions (send_images; a serving
+// admission queues them on the copy stream right away, while the steps in flight run: the
+// regions belong to no listed case) and starts its run state (upload_case, called only while
+// no work is in flight on the context's stream). Heap images wait for their copies; the caller
+// synchronises both streams before the pinned staging area or the pinned run states are reused.
+int send_images(q2d_ctx* ctx, int c, cudaStream_t s) {
     HCase& cs = ctx->cases[c];
     const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
-    cudaStream_t s = ctx->stream;
     for (int gb : cs.blocks) {
         HBlock& b = ctx->blocks[gb];
         const DBlock& d = b.d;
@@ -660,8 +665,17 @@ int upload_case(q2d_ctx* ctx, int c) {
         if (S.heap) CK(cudaStreamSynchronize(s));   // a heap image is freed right away
         S = Staged{};
     }
+    cs.images_sent = true;
+    return Q2D_OK;
+}
+
+int upload_case(q2d_ctx* ctx, int c) {
+    HCase& cs = ctx->cases[c];
+    cudaStream_t s = ctx->stream;
+    if (!cs.images_sent)
+        if (int e = send_images(ctx, c, s)) return e;
     ctx->h_fresh[c] = fresh_state(cs.time0, cs.iter_end);   // one pinned entry per slot
-    CK(cudaMemcpyAsync(ctx->cstate.p + c, ctx->h_fresh + c, sizeof(CaseState), h2d, s));
+    CK(cudaMemcpyAsync(ctx->cstate.p + c, ctx->h_fresh + c, sizeof(CaseState), cudaMemcpyHostToDevice, s));
     cs.resident = true;
     ctx->dt_new = true;
     return Q2D_OK;
@@ -708,16 +722,33 @@ int rebuild_device_lists(q2d_ctx* ctx) {
     const size_t npart = 5 * (size_t)part_stride(ctx) * items.size();
     if (!ctx->PART.p || ctx->PART.n < npart) {
         CK(ensure_cap(ctx->PART, npart));
-        CK(cudaMemset(ctx->PART.p, 0, sizeof(double) * ctx->PART.n));
+        CK(cudaMemsetAsync(ctx->PART.p, 0, sizeof(double) * ctx->PART.n, ctx->stream));
     }
-    if (!db.empty()) CK(cudaMemcpy(ctx->dblocks.p, db.data(), sizeof(DBlock) * db.size(), cudaMemcpyHostToDevice));
-    if (!edges.empty())
-        CK(cudaMemcpy(ctx->edges.p, edges.data(), sizeof(EdgeRec) * edges.size(), cudaMemcpyHostToDevice));
-    if (!params.empty())
-        CK(cudaMemcpy(ctx->bcp.p, params.data(), sizeof(BCParam) * params.size(), cudaMemcpyHostToDevice));
-    if (!items.empty())
-        CK(cudaMemcpy(ctx->items.p, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->dcases.p, dcases.data(), sizeof(DCase) * dcases.size(), cudaMemcpyHostToDevice));
+    {   // one pinned staging buffer, copies queued on the context's stream (no work is in flight,
+        // and the next rebuild comes after a synchronisation of the stream)
+        auto al = [](size_t n) { return (n + 255) & ~size_t(255); };
+        const size_t nb[5] = {sizeof(DBlock) * db.size(), sizeof(EdgeRec) * edges.size(),
+                              sizeof(BCParam) * params.size(), sizeof(WorkItem) * items.size(),
+                              sizeof(DCase) * dcases.size()};
+        size_t need = 0;
+        for (size_t n : nb) need += al(n);
+        if (need > ctx->h_lists_cap) {
+            if (ctx->h_lists) CK(cudaFreeHost(ctx->h_lists));
+            ctx->h_lists = nullptr;
+            ctx->h_lists_cap = 0;
+            CK(cudaMallocHost(&ctx->h_lists, need + need / 2));
+            ctx->h_lists_cap = need + need / 2;
+        }
+        const void* src[5] = {db.data(), edges.data(), params.data(), items.data(), dcases.data()};
+        void* dst[5] = {ctx->dblocks.p, ctx->edges.p, ctx->bcp.p, ctx->items.p, ctx->dcases.p};
+        size_t off = 0;
+        for (int k = 0; k < 5; ++k) {
+            if (nb[k] == 0) continue;
+            std::memcpy(ctx->h_lists + off, src[k], nb[k]);
+            CK(cudaMemcpyAsync(dst[k], ctx->h_lists + off, nb[k], cudaMemcpyHostToDevice, ctx->stream));
+            off += al(nb[k]);
+        }
+    }
     ctx->n_items = (int)items.size();
     {
         const int occ = std::max(1, ctx->kernel == 3   ? stage32d_occupancy(ctx->opt.riemann)
@@ -735,6 +766,10 @@ int rebuild_device_lists(q2d_ctx* ctx) {
 int apply_pending(q2d_ctx* ctx) {
     if (!ctx->dirty) return Q2D_OK;
     CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->copies_pending) {   // the admissions' image copies (done during the steps, as a rule)
+        CK(cudaStreamSynchronize(ctx->copy_stream));
+        ctx->copies_pending = false;
+    }
     for (int c : ctx->reset_slots) {
         if (ctx->cases[c].used) continue;   // slot taken again: the upload below starts it
         const CaseState s = empty_state();
@@ -1362,6 +1397,11 @@ int q2d_serve_create(q2d_ctx** out, const q2d_options* opt, unsigned long long d
     q2d_ctx* ctx = new_ctx(opt);
     if (!ctx) return Q2D_ERR_OOM;
     ctx->serving = true;
+    if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        ctx->copy_stream = nullptr;
+        q2d_gpu_destroy(ctx);
+        return Q2D_ERR_CUDA;
+    }
     ctx->cases.resize(max_cases);
     // Bytes per interior cell: states 3 x 4 planes + scalars 8 planes (160 B), ghost frame
     // 2 planes with up to 50 % halo (24 B), i- and j-faces 3 planes each with up to 15 %
@@ -1425,6 +1465,10 @@ int q2d_serve_admit(q2d_ctx* ctx, int nblocks, const int* ni, const int* nj, con
         cs.bc = std::move(v);
         e = prepare_case(ctx, slot);
     }
+    if (!e && ctx->copy_stream) {
+        e = send_images(ctx, slot, ctx->copy_stream);
+        ctx->copies_pending = true;
+    }
     if (e) {
         free_case_blocks(ctx, cs);
         return e;
@@ -1437,6 +1481,9 @@ int q2d_serve_admit(q2d_ctx* ctx, int nblocks, const int* ni, const int* nj, con
 int q2d_serve_retire(q2d_ctx* ctx, int case_id) {
     if (!ctx || !ctx->serving || case_id < 0 || case_id >= (int)ctx->cases.size() || !ctx->cases[case_id].used)
         return fail(ctx, Q2D_ERR_BADARG, "serve_retire: bad argument");
+    // the freed regions may go to the next admission, whose images are copied at once: steps in
+    // flight (which may still read this case) finish first
+    if (cudaStreamQuery(ctx->stream) == cudaErrorNotReady) CK(cudaStreamSynchronize(ctx->stream));
     free_case_blocks(ctx, ctx->cases[case_id]);
     ctx->reset_slots.push_back(case_id);
     ctx->dirty = true;
@@ -1488,7 +1535,12 @@ void q2d_gpu_destroy(q2d_ctx* ctx) {
     ctx->bcp.release(); ctx->flag.release(); ctx->TAB.release();
     if (ctx->h_state) cudaFreeHost(ctx->h_state);
     if (ctx->h_fresh) cudaFreeHost(ctx->h_fresh);
+    if (ctx->h_lists) cudaFreeHost(ctx->h_lists);
     if (ctx->pin) cudaFreeHost(ctx->pin);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

@@ -184,6 +184,35 @@ def test_case_end_inside_a_multi_step_call():
     st = serve(reqs, opts, device_bytes=int(3 * 2100 * 306 + (1 << 20)), max_cases=3, steps_per_call=50,
                realtime=False, end_cell_updates=40000)
     for r in reqs:
-        end = -(-40000 // r.cells)
-        assert r.rule == "end" and r.iters == end, (r.cells, r.iters, end)
+        cells = r.build().cells   # the built grid's cells (near the requested number)
+        end = -(-40000 // cells)
+        assert r.rule == "end" and r.iters == end == r.meta["end_iter"], (cells, r.iters, end)
     assert st["retired_by"]["end"] == 1.0
+
+
+def test_admission_and_retirement_while_steps_run():
+    """Admissions during a step call copy their images on the context's copy stream while the
+    steps run, retirements during a call wait for it; cases admitted while others run, and after
+    a retirement that frees a slot, end bitwise where they end alone."""
+    a, b, c, d = small_requests()
+    opts = serve_options(itermax=1000, drop=1e-30)
+    ref_c, _ = run_alone(c, opts, 20)
+    ref_d, _ = run_alone(d, opts, 12)
+    ref_a, _ = run_alone(a, opts, 32)
+    budget = int((a.cells + b.cells + max(c.cells, d.cells)) * 306 * 1.3 + (1 << 20))
+    with ServeContext(opts, budget, 3) as sc:
+        ca, cb = sc.admit(a), sc.admit(b)
+        sc.step_async(12)
+        cc = sc.admit(c)                     # images copied while the 12 steps run
+        assert cc is not None
+        sc.wait()
+        sc.step_async(8)
+        sc.retire(cb)                        # waits for the 8 steps
+        cd = sc.admit(d)                     # into the slot b left
+        assert cd is not None
+        sc.step_async(12)
+        infos = sc.wait()
+        assert infos[ca].iter == 32 and infos[cc].iter == 20 and infos[cd].iter == 12
+        assert np.array_equal(sc.prim(ca, 0), ref_a[0])
+        assert np.array_equal(sc.prim(cc, 0), ref_c[0])
+        assert np.array_equal(sc.prim(cd, 0), ref_d[0])
