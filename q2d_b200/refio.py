@@ -124,7 +124,7 @@ def write_case(cs: CaseSpec, directory, extra_ini: str = "", thermo_table=None, 
         rows = [(T, cp, cp * T) for T in (1.0, 2.0)]
     else:
         h, c = (np.asarray(t, dtype=np.float64) for t in thermo_table)
-        rows = [(float(T), c[T], h[T]) for T in range(1, len(h))]
+        rows = [(float(T), float(c[T]), float(h[T])) for T in range(1, len(h))]
     with open(d / "INPUT" / "thermo.dat", "w") as f:
         f.write('TITLE = "Mass Thermodynamic Properties"\n'
                 'VARIABLES = "Temperature", "Cp", "Enthalpy", "Entropy", "dCp"\n'
