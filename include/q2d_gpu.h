@@ -235,8 +235,7 @@ int  q2d_gpu_autotune(q2d_ctx* ctx, int steps, int* schedule, float* ms_per_step
  * 0-2 FP64 tile kernel on 32x10, 32x8, 64x4 tiles; 3-7 FP32-flux tile kernel on 32x10, 32x8,
  * 64x4 (256 threads) and 32x16, 64x8 (512 threads) tiles (FP32-flux form only); 8 FP32-flux tile
  * kernel in difference form on 32x8 tiles (FP32-flux form with HLLC, HLLE or LLF, without
- * MUSCL-SD or residual smoothing; the default of those options); 9 FP64 tile kernel on 32x4
- * tiles of 128 threads (plain FP64 form without the shock sensor). q2d_gpu_get_schedule returns
+ * MUSCL-SD or residual smoothing; the default of those options). q2d_gpu_get_schedule returns
  * the current one. */
 int  q2d_gpu_set_schedule(q2d_ctx* ctx, int schedule);
 int  q2d_gpu_get_schedule(const q2d_ctx* ctx);

@@ -847,7 +847,7 @@ struct Schedule { int kernel, tile; };
 // Candidate schedules, indexed like the autotuner's result: FP64 tile stage kernel on tiles
 // 32x10, 32x8, 64x4; FP32-flux tile kernel on tiles 32x10, 32x8, 64x4 (256 threads) and 32x16,
 // 64x8 (512 threads); FP32-flux tile kernel in difference form on 32x8 (FP32-flux form only).
-const Schedule kSchedules[] = {{0, 0}, {0, 1}, {0, 2}, {2, 0}, {2, 1}, {2, 2}, {2, 3}, {2, 4}, {3, 1}, {0, 5}};
+const Schedule kSchedules[] = {{0, 0}, {0, 1}, {0, 2}, {2, 0}, {2, 1}, {2, 2}, {2, 3}, {2, 4}, {3, 1}};
 constexpr int kNumSchedules = (int)(sizeof(kSchedules) / sizeof(kSchedules[0]));
 
 bool schedule_allowed(const q2d_ctx* ctx, int k) {
@@ -856,8 +856,6 @@ bool schedule_allowed(const q2d_ctx* ctx, int k) {
     if (kSchedules[k].kernel == 0 && sensor &&
         ctx->opt.precision != Q2D_PREC_FP64)
         return false;   // the shock sensor on the tile kernel: FP64 form only (FP32-flux: the FP32-flux kernel)
-    if (kSchedules[k].kernel == 0 && kSchedules[k].tile == 5)   // 32x4 tiles: plain FP64, no sensor
-        return ctx->opt.precision == Q2D_PREC_FP64 && !sensor;
     if (kSchedules[k].kernel == 3)   // difference form: HLLC / HLLE / LLF, no sensor, no smoothing
         return ctx->opt.precision == Q2D_PREC_FP32_FLUX && ctx->opt.riemann <= 2 && !sensor &&
                !(ctx->opt.irs_beta > 0.0);

@@ -124,7 +124,6 @@ cudaError_t launch_irs(const StageArgs& a, int tile, int grid, int dir, double b
         case 2: irs_kernel<64, 4, 256><<<grid, 256, 0, s>>>(a, dir, beta, Rin, Rout); break;
         case 3: irs_kernel<32, 16, 512><<<grid, 512, 0, s>>>(a, dir, beta, Rin, Rout); break;
         case 4: irs_kernel<64, 8, 512><<<grid, 512, 0, s>>>(a, dir, beta, Rin, Rout); break;
-        case 5: irs_kernel<32, 4, 128><<<grid, 128, 0, s>>>(a, dir, beta, Rin, Rout); break;
         default: irs_kernel<32, 10, 256><<<grid, 256, 0, s>>>(a, dir, beta, Rin, Rout); break;
     }
     return cudaGetLastError();
@@ -158,7 +157,6 @@ cudaError_t launch_finalize(const StageArgs& a, cudaStream_t s) {
     switch (TILE) {                                                          \
         case 1: CALL(32, 8, 256); break;                                     \
         case 2: CALL(64, 4, 256); break;                                     \
-        case 5: CALL(32, 4, 128); break;                                     \
         default: CALL(32, 10, 256); break;                                   \
     }
 
@@ -220,7 +218,6 @@ void tile_dims(int tile, int* tx, int* ty, int* nt) {
         case 2: *tx = 64; *ty = 4; *nt = 256; break;
         case 3: *tx = 32; *ty = 16; *nt = 512; break;
         case 4: *tx = 64; *ty = 8; *nt = 512; break;
-        case 5: *tx = 32; *ty = 4; *nt = 128; break;
         default: *tx = 32; *ty = 10; *nt = 256; break;
     }
 }
@@ -231,7 +228,6 @@ cudaError_t launch_dt(const StageArgs& a, int tile, int grid, cudaStream_t s) {
         case 2: dt_kernel<64, 4, 256><<<grid, 256, 0, s>>>(a); break;
         case 3: dt_kernel<32, 16, 512><<<grid, 512, 0, s>>>(a); break;
         case 4: dt_kernel<64, 8, 512><<<grid, 512, 0, s>>>(a); break;
-        case 5: dt_kernel<32, 4, 128><<<grid, 128, 0, s>>>(a); break;
         default: dt_kernel<32, 10, 256><<<grid, 256, 0, s>>>(a); break;
     }
     return cudaGetLastError();

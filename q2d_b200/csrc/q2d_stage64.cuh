@@ -158,7 +158,7 @@ __device__ __forceinline__ void face_phase(const StageArgs& a, const Gas& g, con
 // TAB: the thermally perfect gas (a.gas.htab set); without it the calorically perfect closure
 // is fixed at compile time.
 template <int PREC, int RIEM, int TX, int TY, int NT, bool SD, bool TAB = false>
-__global__ void __launch_bounds__(NT, 512 / NT) stage_kernel(const StageArgs a) {   // 128 registers
+__global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
     using L = Tile<PREC, TX, TY, SD>;
     using ST = typename L::ST;
     constexpr int W = L::W, AREA = L::AREA, NFI = L::NFI, NFJ = L::NFJ, NSI = L::NSI, NSJ = L::NSJ,

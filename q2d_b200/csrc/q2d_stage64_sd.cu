@@ -20,7 +20,6 @@ cudaError_t launch_stage_sd(const StageArgs& a, int prec, int riem, int tile, in
         case 0: e = launch_stage_t<0, 0, TX, TY, NT, true>(a, grid, s); break; \
         default: e = launch_stage_t<0, 7, TX, TY, NT, true>(a, grid, s); break; \
     }
-    if (tile > 2) return cudaErrorInvalidValue;   // MUSCL-SD / sensor instantiations: tiles 0-2
     switch (tile) {
         case 1: Q2D_CALL(32, 8, 256); break;
         case 2: Q2D_CALL(64, 4, 256); break;

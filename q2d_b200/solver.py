@@ -101,8 +101,7 @@ class Q2DSolver:
 
     SCHEDULES = ["tile 32x10", "tile 32x8", "tile 64x4",
                  "fp32-flux tile 32x10", "fp32-flux tile 32x8", "fp32-flux tile 64x4",
-                 "fp32-flux tile 32x16", "fp32-flux tile 64x8", "fp32-flux difference tile 32x8",
-                 "tile 32x4"]
+                 "fp32-flux tile 32x16", "fp32-flux tile 64x8", "fp32-flux difference tile 32x8"]
 
     def set_schedule(self, schedule) -> None:
         """Pins a schedule (index or name from SCHEDULES) without tuning (q2d_gpu_set_schedule)."""

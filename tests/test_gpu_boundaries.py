@@ -24,7 +24,7 @@ from tests.helpers import run_pair
 
 pytestmark = pytest.mark.gpu
 
-FP64_SCHEDULES = ["tile 32x10", "tile 32x8", "tile 64x4", "tile 32x4"]
+FP64_SCHEDULES = ["tile 32x10", "tile 32x8", "tile 64x4"]
 FP32_SCHEDULES = ["fp32-flux tile 32x10", "fp32-flux tile 32x8", "fp32-flux tile 64x4",
                   "fp32-flux difference tile 32x8"]
 
