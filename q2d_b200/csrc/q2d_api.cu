@@ -995,6 +995,7 @@ q2d_ctx* new_ctx(const q2d_options* opt) {
     ctx->gas.igm1 = 1.0 / (opt->gas_gamma - 1.0);
     ctx->gas.rkind = opt->riemann;
     ctx->gas.minf = opt->riemann_minf;
+    ctx->gas.iR = 1.0 / opt->gas_R;
     cudaGetDevice(&ctx->device);
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {

@@ -89,6 +89,7 @@ struct Gas {
     double igm1;   // 1 / (gamma - 1)
     int rkind;     // the Riemann solver (Q2D_RIEMANN_*): selects among the ones of the generic form
     double minf;   // riemann-options-Minf (AUSM+-up, AUSM+-up2)
+    double iR;     // 1 / R
     const double* htab;    // thermally perfect gas: h(T) [J/kg] at T = 0, 1, .. ntab-1 K (null:
     const double* cptab;   //   calorically perfect); cp(T) [J/(kg K)] on the same knots
     int ntab;
@@ -170,7 +171,7 @@ __device__ __forceinline__ double f_gamma(const Gas& g, double p, double rho) {
 }
 __device__ __forceinline__ double f_ss(const Gas& g, double p, double rho) {
     if (g.htab) return sqrt(f_gamma(g, p, rho) * p / rho);
-    return sqrt(g.gamma * p / rho);
+    return sqrt(g.gamma * p * (1.0 / rho));   // 1 / rho shared with the Roe averages' reciprocal
 }
 __device__ __forceinline__ double E0(const Gas& g, double p, double rho, double modv) {
     if (g.htab) return tab_at(g, g.htab, p / (rho * g.R)) - p / rho + 0.5 * modv * modv;
@@ -316,6 +317,10 @@ __device__ __forceinline__ double lim64(double x, double y) {
         return r;
     }
     if (LIM == 0) return 0.0;
+    if (LIM == 2) {   // van Leer with one division: phi(ru) x = 2 x y / ((x + 1e-30) + y) for ru > 0
+        const double xe = x + 1e-30;
+        return y * xe > 0.0 ? (2.0 * x * y) / (xe + y) : 0.0;
+    }
     const double ru = y / (x + 1e-30);
     double phi;
     if (LIM == 2) phi = (ru + fabs(ru)) / (1.0 + fabs(ru));
@@ -344,8 +349,8 @@ __device__ __forceinline__ void roe_averages(const Gas& g, double dltot, double 
                                              double& rho_roe, double& h0_roe) {
     const double inv_dltot = 1.0 / dltot;
     const double inv_drtot = 1.0 / drtot;
-    const double Tl = pl * inv_dltot / g.R;
-    const double Tr = pr * inv_drtot / g.R;
+    const double Tl = pl * inv_dltot * g.iR;
+    const double Tr = pr * inv_drtot * g.iR;
     const double srL = sqrt(dltot);
     const double srR = sqrt(drtot);
     const double inv_sr = 1.0 / (srL + srR);
@@ -382,8 +387,8 @@ __device__ __forceinline__ F4 riemann_hllc(const Gas& g, const double* L, double
     double h0l, h0r, u_roe, v_roe, a_roe, rho_roe, h0_roe;
     roe_averages(g, dltot, drtot, ul, vl, ur, vr, pl, pr, h0l, h0r, u_roe, v_roe, a_roe, rho_roe, h0_roe);
     const double un_roe = u_roe * nx + v_roe * ny;
-    const double e0l = h0l - pl / dltot;
-    const double e0r = h0r - pr / drtot;
+    const double e0l = h0l - pl * (1.0 / dltot);   // the Roe averages' reciprocals
+    const double e0r = h0r - pr * (1.0 / drtot);
     const double S1 = dmin(dmin(0.0, unl - al), un_roe - a_roe);
     const double S4 = dmax(dmax(0.0, unr + ar), un_roe + a_roe);
     double inv_denom = 1.0 / (dltot * (S1 - unl) - drtot * (S4 - unr));
@@ -453,7 +458,7 @@ __device__ __forceinline__ F4 riemann_hlle(const Gas& g, const double* L, double
     F.v = (S4 * (FrL * vl + pl * ny) - S1 * (FrR * vr + pr * ny) +
            S1 * S4 * (drtot * vr - dltot * vl)) * inv_denom;
     F.e = (S4 * (FrL * h0l) - S1 * (FrR * h0r) +
-           S1 * S4 * (drtot * (h0r - pr / drtot) - dltot * (h0l - pl / dltot))) * inv_denom;
+           S1 * S4 * (drtot * (h0r - pr * (1.0 / drtot)) - dltot * (h0l - pl * (1.0 / dltot)))) * inv_denom;
     return F;
 }
 

@@ -295,17 +295,29 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
                     const int r = k / (TX + 3), c = k - r * (TX + 3);
                     const int p0 = (r + 2) * W + c;
                     const double da = sD[p0], db = sD[p0 + 1];
+                    if constexpr (sizeof(ST) == 8) {   // one reciprocal of the interface distance
+                        const double inv = 1.0 / (0.5 * (da + db));
 #pragma unroll
-                    for (int v = 0; v < 4; ++v)
-                        sSi[v * NSI + k] = iface_slope<ST>(sP[v * AREA + p0], sP[v * AREA + p0 + 1], da, db);
+                        for (int v = 0; v < 4; ++v) sSi[v * NSI + k] = (sP[v * AREA + p0 + 1] - sP[v * AREA + p0]) * inv;
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < 4; ++v)
+                            sSi[v * NSI + k] = iface_slope<ST>(sP[v * AREA + p0], sP[v * AREA + p0 + 1], da, db);
+                    }
                 } else {
                     const int kk = k - NSI;
                     const int r = kk / TX, c = kk - r * TX;
                     const int p0 = r * W + c + 2;
                     const double da = sD[AREA + p0], db = sD[AREA + p0 + W];
+                    if constexpr (sizeof(ST) == 8) {
+                        const double inv = 1.0 / (0.5 * (da + db));
 #pragma unroll
-                    for (int v = 0; v < 4; ++v)
-                        sSj[v * NSJ + kk] = iface_slope<ST>(sP[v * AREA + p0], sP[v * AREA + p0 + W], da, db);
+                        for (int v = 0; v < 4; ++v) sSj[v * NSJ + kk] = (sP[v * AREA + p0 + W] - sP[v * AREA + p0]) * inv;
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < 4; ++v)
+                            sSj[v * NSJ + kk] = iface_slope<ST>(sP[v * AREA + p0], sP[v * AREA + p0 + W], da, db);
+                    }
                 }
             }
             if (SD) {   // SD_Tramel of the cells whose faces the tile computes (Mod_Fluxes.f90:132-138)
@@ -399,10 +411,7 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
             }
             // Compute_Cons_NoIRS (Lib_Newstate.f90:131-159)
             const double dt = a.time_accurate ? dt_case : sC[5 * NC + k];
-            if (PREC == 0) {
-#pragma unroll
-                for (int v = 0; v < 4; ++v) res[v] = -r[v] / sur * dt * 1.0;
-            } else {
+            {   // -R / sur * dt with one division
                 const double f = -dt / sur;
 #pragma unroll
                 for (int v = 0; v < 4; ++v) res[v] = r[v] * f;
@@ -422,9 +431,6 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
             if (PREC == 0 && g.htab) {   // thermally perfect gas
                 U0[3] = rhoE_tab(g, PO);
                 U[3] = rhoE_tab(g, P);
-            } else if (PREC == 0) {
-                U0[3] = PO[3] / g.gm1 + 0.5 * PO[0] * (PO[1] * PO[1] + PO[2] * PO[2]);
-                U[3] = P[3] / g.gm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
             } else {
                 U0[3] = PO[3] * g.igm1 + 0.5 * PO[0] * (PO[1] * PO[1] + PO[2] * PO[2]);
                 U[3] = P[3] * g.igm1 + 0.5 * P[0] * (P[1] * P[1] + P[2] * P[2]);
@@ -434,10 +440,7 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
             for (int v = 0; v < 4; ++v) U[v] = U0[v] + (U[v] - U0[v] + res[v]) * a.rk_c;
             double N[4];
             N[0] = U[0];
-            if (PREC == 0) {
-                N[1] = U[1] / U[0];
-                N[2] = U[2] / U[0];
-            } else {
+            {
                 const double ir = 1.0 / U[0];
                 N[1] = U[1] * ir;
                 N[2] = U[2] * ir;
