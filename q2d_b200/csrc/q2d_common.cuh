@@ -319,14 +319,11 @@ __device__ __forceinline__ bool face_flux(const Gas& g, const double* PL, const 
 // MUSCL pieces shared between faces (Lib_Reconstruction.f90:21-27): the slope of an
 // interface between cells a and b, (q_b - q_a) / (0.5 (dl_a + dl_b)), and the limited slope
 // of a cell, rlimiter(forward slope, backward slope). Every face of the reference recomputes
-// both for its two cells; here each is computed once per interface / cell, with the same
-// operations, so the face states are bitwise those of Convective_Flux.
+// both for its two cells; here each is computed once per interface / cell (the FP64 kernel
+// takes the interface distance's reciprocal once for the four variables: within an ulp of the
+// reference's quotient). The FP32 form of the interface slope:
 template <typename ST>
 __device__ __forceinline__ ST iface_slope(double qa, double qb, double dla, double dlb);
-template <>
-__device__ __forceinline__ double iface_slope<double>(double qa, double qb, double dla, double dlb) {
-    return (qb - qa) / (0.5 * (dla + dlb));
-}
 template <>
 __device__ __forceinline__ float iface_slope<float>(double qa, double qb, double dla, double dlb) {
     return (float)(qb - qa) * __frcp_rn(0.5f * (float)(dla + dlb));

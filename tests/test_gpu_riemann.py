@@ -33,7 +33,10 @@ def opts(riem, **kw):
 def test_remaining_solvers_ramp_vs_oracle(developed, riem):   # noqa: F811
     one, split = developed
     gs, os_, _, _ = run_pair([one], 1, **opts(riem))
-    check(gs, os_, 1e-12, f"one block {riem} 1 step")
+    # the rotated HLLC splits each face along the direction of the velocity jump, which turns
+    # ulp-level differences of the face states (the FP64 kernel's shared reciprocals) into
+    # differences of a few 1e-12 where that jump is small
+    check(gs, os_, 5e-12 if riem == "HLLC Rotated" else 1e-12, f"one block {riem} 1 step")
     gs, os_, _, _ = run_pair([split], 4, chunks=2, **opts(riem, shock_detector=0))
     check(gs, os_, 1e-10, f"split {riem} 4 steps")
 
