@@ -161,6 +161,8 @@ struct q2d_ctx {
     DevBuf<double> XFER;            // staging rows of one block's state for upload / download
     DevBuf<XferDesc> XDESC;         // block descriptors of a many-block transfer segment
     DevBuf<float> DL32, FI4, FJ4;   // FP32 geometry (FP32-flux form only): same regions as DL/FI/FJ
+    bool f4 = true;                 // FP32 face records kept (off in serving contexts that run only
+                                    // the difference-form kernel, which reads the FP64 faces)
     Arena ac, ag, afi, afj;
     DevBuf<DBlock> dblocks;
     DevBuf<DCase> dcases;
@@ -522,7 +524,7 @@ void stage_alloc(q2d_ctx* ctx, Staged& S, const DBlock& d, bool fp32) {
     auto al = [](size_t bytes) { return (bytes + 255) & ~size_t(255); };
     S.n_pa = 4 * (size_t)d.pc; S.n_sc = 8 * (size_t)d.pc; S.n_dl = 2 * (size_t)d.pg;
     S.n_fi = 3 * (size_t)d.pfi; S.n_fj = 3 * (size_t)d.pfj;
-    S.n_dl32 = fp32 ? 2 * (size_t)d.pg : 0; S.n_fi4 = fp32 ? 4 * (size_t)d.pfi : 0;
+    S.n_dl32 = fp32 ? 2 * (size_t)d.pg : 0; S.n_fi4 = fp32 && ctx->f4 ? 4 * (size_t)d.pfi : 0;
     S.n_fj4 = fp32 ? 4 * (size_t)d.pfj : 0;
     const size_t sizes[8] = {al(8 * S.n_pa), al(8 * S.n_sc), al(8 * S.n_dl), al(8 * S.n_fi), al(8 * S.n_fj),
                              al(4 * S.n_dl32), al(4 * S.n_fi4), al(4 * S.n_fj4)};
@@ -543,8 +545,8 @@ void stage_alloc(q2d_ctx* ctx, Staged& S, const DBlock& d, bool fp32) {
     S.fi = reinterpret_cast<double*>(p); p += sizes[3];
     S.fj = reinterpret_cast<double*>(p); p += sizes[4];
     S.dl32 = fp32 ? reinterpret_cast<float*>(p) : nullptr; p += sizes[5];
-    S.fi4 = fp32 ? reinterpret_cast<float*>(p) : nullptr; p += sizes[6];
-    S.fj4 = fp32 ? reinterpret_cast<float*>(p) : nullptr;
+    S.fi4 = S.n_fi4 ? reinterpret_cast<float*>(p) : nullptr; p += sizes[6];
+    S.fj4 = S.n_fj4 ? reinterpret_cast<float*>(p) : nullptr;
 }
 
 int prepare_case(q2d_ctx* ctx, int c) {
@@ -585,8 +587,10 @@ int prepare_case(q2d_ctx* ctx, int c) {
         for (int q = 0; q < 3; ++q) parallel_zero(S.fj, q * (size_t)pfj + nfj, (q + 1) * (size_t)pfj);
         if (fp32) {
             parallel_zero(S.dl32, 2 * (size_t)ngh, 2 * (size_t)pg);
-            parallel_zero(S.fi4, 4 * (size_t)nfi, 4 * (size_t)pfi);
-            parallel_zero(S.fj4, 4 * (size_t)nfj, 4 * (size_t)pfj);
+            if (S.fi4) {
+                parallel_zero(S.fi4, 4 * (size_t)nfi, 4 * (size_t)pfi);
+                parallel_zero(S.fj4, 4 * (size_t)nfj, 4 * (size_t)pfj);
+            }
         }
         parallel_rows(b.nj, 160L * b.ni, [&](long long r0, long long r1) {
             for (int j = (int)r0; j < (int)r1; ++j)
@@ -618,18 +622,18 @@ int prepare_case(q2d_ctx* ctx, int c) {
             for (long long k = k0; k < k1; ++k)
                 for (int q = 0; q < 3; ++q) {
                     S.fi[q * pfi + k] = G.fi[3 * k + q];
-                    if (fp32) S.fi4[4 * k + q] = (float)G.fi[3 * k + q];
+                    if (S.fi4) S.fi4[4 * k + q] = (float)G.fi[3 * k + q];
                 }
-            if (fp32)
+            if (S.fi4)
                 for (long long k = k0; k < k1; ++k) S.fi4[4 * k + 3] = 0.0f;
         });
         parallel_rows(nfj, 48, [&](long long k0, long long k1) {
             for (long long k = k0; k < k1; ++k)
                 for (int q = 0; q < 3; ++q) {
                     S.fj[q * pfj + k] = G.fj[3 * k + q];
-                    if (fp32) S.fj4[4 * k + q] = (float)G.fj[3 * k + q];
+                    if (S.fj4) S.fj4[4 * k + q] = (float)G.fj[3 * k + q];
                 }
-            if (fp32)
+            if (S.fj4)
                 for (long long k = k0; k < k1; ++k) S.fj4[4 * k + 3] = 0.0f;
         });
         b.prim.clear();
@@ -659,8 +663,10 @@ int send_images(q2d_ctx* ctx, int c, cudaStream_t s) {
         CK(cudaMemcpyAsync(ctx->FJ.p + d.ofj, S.fj, sizeof(double) * S.n_fj, h2d, s));
         if (ctx->DL32.p) {   // face offsets are multiples of 32, so float index 2*off is 16-byte aligned
             CK(cudaMemcpyAsync(ctx->DL32.p + d.og, S.dl32, sizeof(float) * S.n_dl32, h2d, s));
-            CK(cudaMemcpyAsync(ctx->FI4.p + 2 * d.ofi, S.fi4, sizeof(float) * S.n_fi4, h2d, s));
-            CK(cudaMemcpyAsync(ctx->FJ4.p + 2 * d.ofj, S.fj4, sizeof(float) * S.n_fj4, h2d, s));
+            if (ctx->FI4.p && S.fi4) {
+                CK(cudaMemcpyAsync(ctx->FI4.p + 2 * d.ofi, S.fi4, sizeof(float) * S.n_fi4, h2d, s));
+                CK(cudaMemcpyAsync(ctx->FJ4.p + 2 * d.ofj, S.fj4, sizeof(float) * S.n_fj4, h2d, s));
+            }
         }
         if (S.heap) CK(cudaStreamSynchronize(s));   // a heap image is freed right away
         S = Staged{};
@@ -793,7 +799,8 @@ int allocate_pools(q2d_ctx* ctx, long long ec, long long eg, long long efi, long
     if (ctx->opt.irs_beta > 0.0) { CK(ctx->RA.alloc(ec)); CK(ctx->RB.alloc(ec)); }
     CK(ctx->SC.alloc(2 * ec)); CK(ctx->DL.alloc(eg)); CK(ctx->FI.alloc(efi)); CK(ctx->FJ.alloc(efj));
     if (ctx->opt.precision == Q2D_PREC_FP32_FLUX) {
-        CK(ctx->DL32.alloc(eg)); CK(ctx->FI4.alloc(2 * efi)); CK(ctx->FJ4.alloc(2 * efj));
+        CK(ctx->DL32.alloc(eg));
+        if (ctx->f4) { CK(ctx->FI4.alloc(2 * efi)); CK(ctx->FJ4.alloc(2 * efj)); }
     }
     CK(cudaMemset(ctx->PB.p, 0, sizeof(double) * (ec ? ec : 1)));
     CK(cudaMemset(ctx->PC.p, 0, sizeof(double) * (ec ? ec : 1)));
@@ -856,6 +863,7 @@ bool schedule_allowed(const q2d_ctx* ctx, int k) {
     if (kSchedules[k].kernel == 0 && sensor &&
         ctx->opt.precision != Q2D_PREC_FP64)
         return false;   // the shock sensor on the tile kernel: FP64 form only (FP32-flux: the FP32-flux kernel)
+    if (kSchedules[k].kernel == 2 && !ctx->f4) return false;   // no FP32 face records
     if (kSchedules[k].kernel == 3)   // difference form: HLLC / HLLE / LLF, no sensor, no smoothing
         return ctx->opt.precision == Q2D_PREC_FP32_FLUX && ctx->opt.riemann <= 2 && !sensor &&
                !(ctx->opt.irs_beta > 0.0);
@@ -1404,11 +1412,13 @@ int q2d_serve_create(q2d_ctx** out, const q2d_options* opt, unsigned long long d
         return Q2D_ERR_CUDA;
     }
     ctx->cases.resize(max_cases);
+    ctx->f4 = !(opt->precision == Q2D_PREC_FP32_FLUX && difference_form(ctx));
     // Bytes per interior cell: states 3 x 4 planes + scalars 8 planes (160 B), ghost frame
     // 2 planes with up to 50 % halo (24 B), i- and j-faces 3 planes each with up to 15 %
     // extra faces (55 B); the FP32-flux form adds FP32 copies of the ghost-frame and face
-    // geometry (12 B + 55 B).
-    const double per_cell = (opt->precision == Q2D_PREC_FP32_FLUX ? 306.4 : 239.2) +
+    // geometry (12 B + 55 B), the face part only where a kernel other than the difference form
+    // can run.
+    const double per_cell = (opt->precision == Q2D_PREC_FP32_FLUX ? (ctx->f4 ? 306.4 : 251.2) : 239.2) +
                             (opt->irs_beta > 0.0 ? 64.0 : 0.0);   // two residual pools with IRS
     const long long cells = (long long)((double)device_bytes / per_cell);
     const long long ec = 4 * cells, eg = 3 * cells + 4096, efi = (long long)(3.45 * (double)cells) + 4096,
