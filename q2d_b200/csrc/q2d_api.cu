@@ -177,6 +177,9 @@ struct q2d_ctx {
     char* pin = nullptr;            // pinned staging area of admissions (serving contexts)
     char* h_lists = nullptr;        // pinned staging of the device work lists
     size_t h_lists_cap = 0;
+    // host geometry of the case being prepared, kept between cases: its pages stay mapped, so
+    // the next admission's metrics do not fault them in again
+    std::vector<HostGeom> geo_cache;
     size_t pin_cap = 0, pin_used = 0;
     int n_items = 0;
     std::map<int, cudaGraphExec_t> graphs;
@@ -552,7 +555,8 @@ void stage_alloc(q2d_ctx* ctx, Staged& S, const DBlock& d, bool fp32) {
 int prepare_case(q2d_ctx* ctx, int c) {
     HCase& cs = ctx->cases[c];
     if (int e = build_case_edges(ctx, c)) return e;
-    std::vector<HostGeom> geo(cs.blocks.size());
+    std::vector<HostGeom>& geo = ctx->geo_cache;   // every array is rewritten by setup_block
+    if (geo.size() < cs.blocks.size()) geo.resize(cs.blocks.size());
     for (size_t lb = 0; lb < cs.blocks.size(); ++lb) {
         HBlock& b = ctx->blocks[cs.blocks[lb]];
         int e = setup_block(b.ni, b.nj, b.nodes.data(), b.area.empty() ? nullptr : b.area.data(),
@@ -638,7 +642,6 @@ int prepare_case(q2d_ctx* ctx, int c) {
         });
         b.prim.clear();
         b.prim.shrink_to_fit();
-        geo[lb] = HostGeom{};
     }
     cs.prepared = true;
     return Q2D_OK;
