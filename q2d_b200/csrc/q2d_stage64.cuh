@@ -287,7 +287,6 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
                     for (int q = 0; q < 3; ++q) cp_async8(sGj + q * NFJ + ff, src + q * B.pfj);
                 }
             }
-            cp_async_commit();   // the second group
         }
         if (irs == 2) cp_async_wait_all();
         else cp_async_wait_group<1>();   // the own-cell data and face geometry may still be in flight
