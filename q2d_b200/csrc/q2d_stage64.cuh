@@ -253,9 +253,6 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
                     }
                 }
             }
-            // the state and cell lengths (needed first) and, in a second group, the own-cell data
-            // and face geometry, which land while the slopes are computed
-            cp_async_commit();
             for (int k = tid; k < NC; k += NT) {
                 const int row = k / TX, col = k - row * TX;
                 const int ii = i0 + col, jj = j0 + row;
@@ -288,8 +285,7 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
                 }
             }
         }
-        if (irs == 2) cp_async_wait_all();
-        else cp_async_wait_group<1>();   // the own-cell data and face geometry may still be in flight
+        cp_async_wait_all();
         __syncthreads();
 
         if (irs != 2) {
@@ -345,7 +341,6 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
                 case 5: sigma_phase<5, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
                 default: sigma_phase<6, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
             }
-            cp_async_wait_all();   // own-cell data and face geometry
             __syncthreads();
 
             // ---- 5. face fluxes (interior: Riemann on MUSCL states; boundary: BC_Fluxes) -----
