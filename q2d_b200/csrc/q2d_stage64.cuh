@@ -83,40 +83,6 @@ __device__ __forceinline__ void sigma_phase(const ST* sSi, const ST* sSj, ST* sG
     }
 }
 
-// Limited cell slopes of a tile in FP64 straight from the state (steps 3 and 4 in one pass):
-// each limited slope takes its two interface slopes, (q_b - q_a) times the reciprocal of
-// 0.5 (dl_a + dl_b) shared by the four variables, with the same operations as the interface
-// pass, so the values are those of the two-pass form; one CTA barrier less per tile.
-template <int LIM, int NT, int TX, int TY>
-__device__ __forceinline__ void sigma_fused64(const double* sP, const double* sD, double* sGI, double* sGJ) {
-    constexpr int W = TX + 4, AREA = W * (TY + 4);
-    constexpr int NGI = (TX + 2) * TY, NGJ = TX * (TY + 2);
-    for (int k = threadIdx.x; k < NGI; k += NT) {
-        const int r = k / (TX + 2), c = k - r * (TX + 2);
-        const int p = (r + 2) * W + c + 1;                  // the cell: smem row r+2, column c+1
-        const double ibw = 1.0 / (0.5 * (sD[p - 1] + sD[p]));
-        const double ifw = 1.0 / (0.5 * (sD[p] + sD[p + 1]));
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const double* q = sP + v * AREA;
-            sGI[v * NGI + k] = lim64<LIM>((q[p + 1] - q[p]) * ifw, (q[p] - q[p - 1]) * ibw);
-        }
-    }
-    constexpr int NW = NT / 32, ROT = ((NGI + 31) / 32) % NW;
-    const double* dj = sD + AREA;
-    for (int k = (((int)(threadIdx.x >> 5) - ROT + NW) % NW) * 32 + (int)(threadIdx.x & 31); k < NGJ; k += NT) {
-        const int r = k / TX, c = k - r * TX;
-        const int p = (r + 1) * W + c + 2;                  // the cell: smem row r+1, column c+2
-        const double ibw = 1.0 / (0.5 * (dj[p - W] + dj[p]));
-        const double ifw = 1.0 / (0.5 * (dj[p] + dj[p + W]));
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const double* q = sP + v * AREA;
-            sGJ[v * NGJ + k] = lim64<LIM>((q[p + W] - q[p]) * ifw, (q[p] - q[p - W]) * ibw);
-        }
-    }
-}
-
 // Face fluxes of one direction of a tile (step 5 of the stage kernel). IDIR: i-faces
 // (F = i0..i0+TX on TY rows) or j-faces (G = j0..j0+TY on TX columns).
 // SD: the shock sensor sB runs (MUSCL-SD or a sensor-driven Riemann solver); an interior face
@@ -323,8 +289,8 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
         __syncthreads();
 
         if (irs != 2) {
-            // ---- 3. interface slopes (FP32-slope form; the FP64 form fuses them into step 4) ---
-            for (int k = (sizeof(ST) == 8 ? NSI + NSJ : tid); k < NSI + NSJ; k += NT) {
+            // ---- 3. interface slopes ---------------------------------------------------------
+            for (int k = tid; k < NSI + NSJ; k += NT) {
                 if (k < NSI) {
                     const int r = k / (TX + 3), c = k - r * (TX + 3);
                     const int p0 = (r + 2) * W + c;
@@ -363,31 +329,17 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
                     sB[k] = sd_tramel(pp[0], pp[-1], pp[1], pp[-W], pp[W]);
                 }
             }
-            if (sizeof(ST) != 8 || SD) __syncthreads();   // the slopes or the sensor before step 4
+            __syncthreads();
 
             // ---- 4. limited slope of every cell next to a face of the tile -------------------
-            if constexpr (sizeof(ST) == 8) {
-                double* gI = reinterpret_cast<double*>(sGI);
-                double* gJ = reinterpret_cast<double*>(sGJ);
-                switch (lim) {
-                    case 0: sigma_fused64<0, NT, TX, TY>(sP, sD, gI, gJ); break;
-                    case 1: sigma_fused64<1, NT, TX, TY>(sP, sD, gI, gJ); break;
-                    case 2: sigma_fused64<2, NT, TX, TY>(sP, sD, gI, gJ); break;
-                    case 3: sigma_fused64<3, NT, TX, TY>(sP, sD, gI, gJ); break;
-                    case 4: sigma_fused64<4, NT, TX, TY>(sP, sD, gI, gJ); break;
-                    case 5: sigma_fused64<5, NT, TX, TY>(sP, sD, gI, gJ); break;
-                    default: sigma_fused64<6, NT, TX, TY>(sP, sD, gI, gJ); break;
-                }
-            } else {
-                switch (lim) {
-                    case 0: sigma_phase<0, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-                    case 1: sigma_phase<1, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-                    case 2: sigma_phase<2, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-                    case 3: sigma_phase<3, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-                    case 4: sigma_phase<4, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-                    case 5: sigma_phase<5, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-                    default: sigma_phase<6, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
-                }
+            switch (lim) {
+                case 0: sigma_phase<0, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                case 1: sigma_phase<1, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                case 2: sigma_phase<2, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                case 3: sigma_phase<3, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                case 4: sigma_phase<4, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                case 5: sigma_phase<5, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
+                default: sigma_phase<6, NT, TX, TY>(sSi, sSj, sGI, sGJ); break;
             }
             __syncthreads();
 
