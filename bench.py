@@ -212,8 +212,7 @@ def serving_leg(args, lib, fp64_batched=None):
     rb = torch.empty(int(args.serve_readback_gb * (1 << 30)) // 8, dtype=torch.float64, pin_memory=True).numpy()
     opts = serve_options(itermax=10 ** 9, drop=1e-8)
     st = serve(reqs, opts, device_bytes=int(args.serve_gb * (1 << 30)), max_cases=4096, steps_per_call=10,
-               keep_results=True, end_cell_updates=args.serve_end, result_sink=sink, readback_buffer=rb,
-               max_steps_per_call=40)
+               keep_results=True, end_cell_updates=args.serve_end, result_sink=sink, readback_buffer=rb)
     del rb
     st["nonfinite_results"] = len(bad)
     st["distinct_payloads"] = args.serve_distinct

@@ -244,7 +244,7 @@ def serve_options(precision: int = _abi.PREC_FP32_FLUX, itermax: int = 2000, dro
 def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: int = 1024,
           steps_per_call: int = 10, keep_results: bool = False, lib=None, clock=time.perf_counter,
           realtime: bool = True, end_cell_updates: Optional[float] = None,
-          result_sink=None, readback_buffer: Optional[np.ndarray] = None, max_steps_per_call: int = 0) -> dict:
+          result_sink=None, readback_buffer: Optional[np.ndarray] = None) -> dict:
     """Runs the request loop until every request is retired (or rejected as larger than the
     whole budget). With realtime=False arrivals are taken as already due (a replay of a
     backlog), which makes the admission order independent of host timing.
@@ -257,10 +257,7 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
     many-block transfer before they are retired; that read-back is inside their latency. The
     states are kept in Request.result, or handed to result_sink(request, states) when given
     (a client that takes the result away); with readback_buffer the states handed to the sink
-    are views into it, valid until the sink returns. With max_steps_per_call above
-    steps_per_call the call length adapts: when the GPU finished a call before the admissions made
-    during it (the host is the bottleneck) the next call runs twice the steps, up to that maximum;
-    when the GPU ran well past the admissions it halves back toward steps_per_call."""
+    are views into it, valid until the sink returns."""
     reqs = sorted(requests, key=lambda r: r.arrival)
     pending = deque(reqs)
     queue: deque = deque()
@@ -273,8 +270,6 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
         t0 = clock()
         busy = 0.0
         t_admit = t_readback = t_retire = t_launch = 0.0
-        spc = steps_per_call
-        steps_total = 0
 
         def now():
             return clock() - t0 if realtime else math.inf
@@ -308,24 +303,15 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
                 admit_due()
                 continue
             tb = clock()
-            sc.step_async(spc)   # applies admissions and retirements, then launches
-            steps_total += spc
+            sc.step_async(steps_per_call)   # applies admissions and retirements, then launches
             t_launch += clock() - tb
             on_device = set(active.keys())   # cases admitted from here on join the next call
             steps_calls += 1
             ta = clock()
             admit_due()              # host work overlaps the steps in flight
-            t_ad = clock() - ta
-            t_admit += t_ad
-            tw = clock()
+            t_admit += clock() - ta
             infos = sc.wait()
-            t_wait = clock() - tw
             busy += clock() - tb
-            if max_steps_per_call > steps_per_call:
-                if t_wait < 0.1 * t_ad:
-                    spc = min(max_steps_per_call, 2 * spc)
-                elif t_wait > 0.5 * t_ad:
-                    spc = max(steps_per_call, spc // 2)
             leaving = []
             for cid in sorted(on_device):
                 inf = infos[cid]
@@ -385,7 +371,6 @@ def serve(requests: list, options: _abi.Options, device_bytes: int, max_cases: i
         "readback_bytes": int(readback_bytes),
         "host_s": {"apply_and_launch": t_launch, "admission_during_steps": t_admit, "readback": t_readback,
                    "retire": t_retire},
-        "step_calls": steps_calls, "mean_steps_per_call": steps_total / max(1, steps_calls),
-        "gpu_launches": launches,
+        "step_calls": steps_calls, "gpu_launches": launches,
         "budget_cells": int(budget_cells),
     }
