@@ -45,10 +45,17 @@ struct HBlock {
     int ni = 0, nj = 0, case_id = -1, local_b = 0;
     std::vector<double> nodes, area;
     std::vector<double> prim;      // 4 planes, interior (until the case is prepared)
+    // a serving admission's caller arrays, read in place while the admission prepares the case
+    // (the nodes, the cross-section and the ghosted state P): no host copies
+    const double* nodes_ext = nullptr;
+    const double* area_ext = nullptr;
+    const double* P_ext = nullptr;
     std::vector<EdgeRec> edge[4];  // records of faces 1..4 (param: index into the case's params)
     Staged staged;
     DBlock d{};
     bool alive = false;            // holds device regions
+    const double* nd() const { return nodes_ext ? nodes_ext : nodes.data(); }
+    const double* ar() const { return area_ext ? area_ext : (area.empty() ? nullptr : area.data()); }
 };
 
 struct HCase {
@@ -466,7 +473,7 @@ int build_case_edges(q2d_ctx* ctx, int c) {
             BCParam p{};
             p.T0 = r.T0; p.p0 = r.p0; p.pamb = r.pamb; p.mach = r.mach;
             p.alpha = r.alpha; p.rel_fac = r.rel_fac;
-            face_tangent(r, B.ni, B.nodes.data(), &p.t0, &p.t1);
+            face_tangent(r, B.ni, B.nd(), &p.t0, &p.t1);
             er.param = (int)cs.params.size();
             cs.params.push_back(p);
         }
@@ -559,15 +566,15 @@ int prepare_case(q2d_ctx* ctx, int c) {
     if (geo.size() < cs.blocks.size()) geo.resize(cs.blocks.size());
     for (size_t lb = 0; lb < cs.blocks.size(); ++lb) {
         HBlock& b = ctx->blocks[cs.blocks[lb]];
-        int e = setup_block(b.ni, b.nj, b.nodes.data(), b.area.empty() ? nullptr : b.area.data(),
+        int e = setup_block(b.ni, b.nj, b.nd(), b.ar(),
                             ctx->opt.source, geo[lb]);
         if (e) return fail(ctx, e, "degenerate cell in block " + std::to_string(b.local_b));
     }
     for (const q2d_bc_rec& r : cs.bc) {
         HBlock& B = ctx->blocks[cs.blocks[r.b - 1]];
         const HBlock* D = (r.type == 101 || r.type == 201) ? &ctx->blocks[cs.blocks[r.bs - 1]] : nullptr;
-        int e = ghost_metrics(r, B.ni, B.nj, B.nodes.data(), geo[r.b - 1], D ? D->ni : 0, D ? D->nj : 0,
-                              D ? D->nodes.data() : nullptr);
+        int e = ghost_metrics(r, B.ni, B.nj, B.nd(), geo[r.b - 1], D ? D->ni : 0, D ? D->nj : 0,
+                              D ? D->nd() : nullptr);
         if (e) return fail(ctx, e, "ghost metrics failed for a boundary record");
     }
     if (!reserve_regions(ctx, c)) return fail(ctx, Q2D_ERR_CAPACITY, "device memory budget exhausted");
@@ -609,7 +616,12 @@ int prepare_case(q2d_ctx* ctx, int c) {
                     S.sc[5 * pc + k] = v[3];
                     S.sc[6 * pc + k] = G.src0[k];
                     S.sc[7 * pc + k] = G.src1[k];
-                    for (int q = 0; q < 4; ++q) S.pa[q * pc + k] = b.prim[(size_t)q * n + k];
+                    if (b.P_ext) {   // the caller's P(4, -1:ni+2, -1:nj+2)
+                        const double* src = &b.P_ext[4 * ((size_t)(i + 2) + (size_t)(b.ni + 4) * (j + 2))];
+                        for (int q = 0; q < 4; ++q) S.pa[q * pc + k] = src[q];
+                    } else {
+                        for (int q = 0; q < 4; ++q) S.pa[q * pc + k] = b.prim[(size_t)q * n + k];
+                    }
                 }
         });
         parallel_rows(ngh, 32, [&](long long k0, long long k1) {
@@ -1151,9 +1163,13 @@ int q2d_gpu_upload_prim(q2d_ctx* ctx, int block_id, const double* P) {
     if (!ctx || block_id < 0 || block_id >= (int)ctx->blocks.size() || !P || ctx->blocks[block_id].case_id < 0)
         return fail(ctx, Q2D_ERR_BADARG, "upload_prim: bad argument");
     HBlock& b = ctx->blocks[block_id];
-    if (ctx->cases[b.case_id].resident) {
+    const HCase& hc = ctx->cases[b.case_id];
+    if (hc.images_sent && !hc.resident && ctx->copy_stream)   // the admission's image copies first
+        CK(cudaStreamSynchronize(ctx->copy_stream));
+    if (hc.resident || hc.images_sent) {
         // the interior rows of P (4*ni doubles each, pitch 4*(ni+4)) by one strided copy into a
-        // staging buffer, then into the state planes on the device
+        // staging buffer, then into the state planes on the device (a serving admission's
+        // region, whose images were copied at admission, takes the same path)
         const long long n = (long long)b.ni * b.nj;
         CK(ensure_cap(ctx->XFER, 4 * (size_t)n));
         const double* row0 = P + 4 * (2 + (size_t)(b.ni + 4) * 2);
@@ -1466,10 +1482,9 @@ int q2d_serve_admit(q2d_ctx* ctx, int nblocks, const int* ni, const int* nj, con
         HBlock& hb = ctx->blocks[gid];
         hb = HBlock{};
         hb.ni = ni[b]; hb.nj = nj[b]; hb.case_id = slot; hb.local_b = b + 1;
-        hb.nodes.assign(nodes_xy[b], nodes_xy[b] + 2 * (size_t)(ni[b] + 1) * (nj[b] + 1));
-        if (cross_sections && cross_sections[b])
-            hb.area.assign(cross_sections[b], cross_sections[b] + (size_t)(ni[b] + 1) * (nj[b] + 1));
-        fortran_to_planes(ni[b], nj[b], P[b], hb.prim);
+        hb.nodes_ext = nodes_xy[b];   // read in place until this call returns
+        if (cross_sections && cross_sections[b]) hb.area_ext = cross_sections[b];
+        hb.P_ext = P[b];
         cs.blocks.push_back(gid);
     }
     std::vector<q2d_bc_rec> v(recs, recs + nrecs);
@@ -1482,6 +1497,10 @@ int q2d_serve_admit(q2d_ctx* ctx, int nblocks, const int* ni, const int* nj, con
     if (!e && ctx->copy_stream) {
         e = send_images(ctx, slot, ctx->copy_stream);
         ctx->copies_pending = true;
+    }
+    for (int gb : cs.blocks) {   // the caller's arrays are not kept past this call
+        HBlock& hb = ctx->blocks[gb];
+        hb.nodes_ext = hb.area_ext = hb.P_ext = nullptr;
     }
     if (e) {
         free_case_blocks(ctx, cs);

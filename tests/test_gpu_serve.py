@@ -216,3 +216,27 @@ def test_admission_and_retirement_while_steps_run():
         assert np.array_equal(sc.prim(ca, 0), ref_a[0])
         assert np.array_equal(sc.prim(cc, 0), ref_c[0])
         assert np.array_equal(sc.prim(cd, 0), ref_d[0])
+
+
+def test_upload_after_admission_before_the_first_step():
+    """q2d_gpu_upload_prim on an admitted case before its first step (its images are already
+    on the copy stream) replaces the admitted state: the case then runs as if admitted with
+    the uploaded state."""
+    import copy
+    from q2d_b200 import _abi as abi
+    a = small_requests()[0]
+    b = copy.deepcopy(a)
+    b.blocks[0].prim[..., 3] *= 1.02
+    b.blocks[0].prim[..., 1] *= 0.97
+    opts = serve_options(itermax=1000, drop=1e-30)
+    ref, _ = run_alone(b, opts, 6)
+    with ServeContext(opts, BUDGET, 4) as sc:
+        cid = sc.admit(a)
+        import ctypes as C
+        bid = C.c_int()
+        assert sc.lib.q2d_serve_block_id(sc.ctx, cid, 1, C.byref(bid)) == abi.OK
+        P = b.blocks[0].prim_ghost(ghosts=None)
+        assert sc.lib.q2d_gpu_upload_prim(sc.ctx, bid.value, abi.dptr(P)) == abi.OK
+        sc.step_async(6)
+        sc.wait()
+        assert np.array_equal(sc.prim(cid, 0), ref[0])
