@@ -300,7 +300,8 @@ long long q2d_gpu_num_cells(const q2d_ctx* ctx);
  *
  * q2d_serve_admit adds a case between steps: nblocks blocks with the arguments of
  * q2d_gpu_add_block and q2d_gpu_upload_prim (P[b] in the ghosted Fortran layout) and the
- * boundary records of q2d_gpu_set_bcs. It validates the input, computes the metrics and
+ * boundary records of q2d_gpu_set_bcs (the arrays are read during the call only: the caller may
+ * reuse them when it returns). It validates the input, computes the metrics and
  * reserves device memory on the host at once, and queues the copies of its device images on a
  * copy stream of the context right away (they overlap the steps in flight, into memory that no
  * listed case uses); its run state is started by the next step call. It returns
