@@ -564,10 +564,16 @@ int prepare_case(q2d_ctx* ctx, int c) {
     if (int e = build_case_edges(ctx, c)) return e;
     std::vector<HostGeom>& geo = ctx->geo_cache;   // every array is rewritten by setup_block
     if (geo.size() < cs.blocks.size()) geo.resize(cs.blocks.size());
+    // regions and staging images first: the face geometry is written straight into its images
+    if (!reserve_regions(ctx, c)) return fail(ctx, Q2D_ERR_CAPACITY, "device memory budget exhausted");
+    const bool fp32 = ctx->opt.precision == Q2D_PREC_FP32_FLUX;
     for (size_t lb = 0; lb < cs.blocks.size(); ++lb) {
         HBlock& b = ctx->blocks[cs.blocks[lb]];
-        int e = setup_block(b.ni, b.nj, b.nd(), b.ar(),
-                            ctx->opt.source, geo[lb]);
+        Staged& S = b.staged;
+        stage_alloc(ctx, S, b.d, fp32);
+        FaceOut fo;
+        fo.fi = S.fi; fo.fj = S.fj; fo.pfi = b.d.pfi; fo.pfj = b.d.pfj; fo.fi4 = S.fi4; fo.fj4 = S.fj4;
+        int e = setup_block(b.ni, b.nj, b.nd(), b.ar(), ctx->opt.source, geo[lb], &fo);
         if (e) return fail(ctx, e, "degenerate cell in block " + std::to_string(b.local_b));
     }
     for (const q2d_bc_rec& r : cs.bc) {
@@ -577,7 +583,6 @@ int prepare_case(q2d_ctx* ctx, int c) {
                               D ? D->nd() : nullptr);
         if (e) return fail(ctx, e, "ghost metrics failed for a boundary record");
     }
-    if (!reserve_regions(ctx, c)) return fail(ctx, Q2D_ERR_CAPACITY, "device memory budget exhausted");
     for (size_t lb = 0; lb < cs.blocks.size(); ++lb) {
         HBlock& b = ctx->blocks[cs.blocks[lb]];
         const DBlock& d = b.d;
@@ -586,10 +591,9 @@ int prepare_case(q2d_ctx* ctx, int c) {
         const long long ngh = (long long)(b.ni + 4) * (b.nj + 4), nfi = (long long)(b.ni + 1) * b.nj,
                         nfj = (long long)b.ni * (b.nj + 1);
         const long long pc = d.pc, pg = d.pg, pfi = d.pfi, pfj = d.pfj;
-        const bool fp32 = ctx->opt.precision == Q2D_PREC_FP32_FLUX;
         Staged& S = b.staged;
-        // images of the device planes, filled in parallel; padding and the dt plane are zero
-        stage_alloc(ctx, S, d, fp32);
+        // images of the device planes (the faces written by setup_block), filled in parallel;
+        // padding and the dt plane are zero
         parallel_zero(S.sc, (size_t)pc, 2 * (size_t)pc);   // dt
         for (int v = 0; v < 8; ++v) parallel_zero(S.sc, v * (size_t)pc + n, (v + 1) * (size_t)pc);
         for (int v = 0; v < 4; ++v) parallel_zero(S.pa, v * (size_t)pc + n, (v + 1) * (size_t)pc);
@@ -633,24 +637,6 @@ int prepare_case(q2d_ctx* ctx, int c) {
                     S.dl32[2 * k + 1] = (float)G.dl[2 * k + 1];
                 }
             }
-        });
-        parallel_rows(nfi, 48, [&](long long k0, long long k1) {
-            for (long long k = k0; k < k1; ++k)
-                for (int q = 0; q < 3; ++q) {
-                    S.fi[q * pfi + k] = G.fi[3 * k + q];
-                    if (S.fi4) S.fi4[4 * k + q] = (float)G.fi[3 * k + q];
-                }
-            if (S.fi4)
-                for (long long k = k0; k < k1; ++k) S.fi4[4 * k + 3] = 0.0f;
-        });
-        parallel_rows(nfj, 48, [&](long long k0, long long k1) {
-            for (long long k = k0; k < k1; ++k)
-                for (int q = 0; q < 3; ++q) {
-                    S.fj[q * pfj + k] = G.fj[3 * k + q];
-                    if (S.fj4) S.fj4[4 * k + q] = (float)G.fj[3 * k + q];
-                }
-            if (S.fj4)
-                for (long long k = k0; k < k1; ++k) S.fj4[4 * k + 3] = 0.0f;
         });
         b.prim.clear();
         b.prim.shrink_to_fit();

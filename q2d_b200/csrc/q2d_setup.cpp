@@ -107,7 +107,8 @@ void SetupPool::run(int T, const std::function<void(int)>& fn) {
     T_ = 0;
 }
 
-int setup_block(int ni, int nj, const double* nodes, const double* area, int source, HostGeom& G) {
+int setup_block(int ni, int nj, const double* nodes, const double* area, int source, HostGeom& G,
+                const FaceOut* out) {
     G.ni = ni;
     G.nj = nj;
     const size_t ng = (size_t)(ni + 4) * (nj + 4);
@@ -150,18 +151,41 @@ int setup_block(int ni, int nj, const double* nodes, const double* area, int sou
         const double cy = 0.5 * (X(1, 1).y + X(0, 1).y) - 0.5 * (X(1, 0).y + X(0, 0).y);
         sgn_j = std::copysign(1.0, cx * sx + cy * sy);
     }
-    G.fi.resize(3 * (size_t)(ni + 1) * nj);
-    G.fj.resize(3 * (size_t)ni * (nj + 1));
+    // a face's (nx, ny, len) into G's AoS arrays, or into the device images (planes + float4)
+    auto put = [](double* aos, double* planes, long long pstride, float* f4, long long k, double nx, double ny,
+                  double len) {
+        if (planes) {
+            planes[k] = nx;
+            planes[pstride + k] = ny;
+            planes[2 * pstride + k] = len;
+            if (f4) {
+                f4[4 * k] = (float)nx;
+                f4[4 * k + 1] = (float)ny;
+                f4[4 * k + 2] = (float)len;
+                f4[4 * k + 3] = 0.0f;
+            }
+        } else {
+            aos[3 * k] = nx;
+            aos[3 * k + 1] = ny;
+            aos[3 * k + 2] = len;
+        }
+    };
+    if (out) {
+        G.fi.clear();
+        G.fj.clear();
+    } else {
+        G.fi.resize(3 * (size_t)(ni + 1) * nj);
+        G.fj.resize(3 * (size_t)ni * (nj + 1));
+    }
     parallel_rows(nj, 24L * (ni + 1), [&](long long r0, long long r1) {
         for (int j = (int)r0 + 1; j <= (int)r1; ++j)
             for (int F = 0; F <= ni; ++F) {
                 const double dx = X(F, j).x - X(F, j - 1).x, dy = X(F, j).y - X(F, j - 1).y;
                 const double sx = dy, sy = -dx;
                 const double A = std::sqrt(sx * sx + sy * sy);
-                double* f = &G.fi[3 * ((size_t)(j - 1) * (ni + 1) + F)];
-                f[0] = A == 0.0 ? 0.0 : sx / A * sgn_i;
-                f[1] = A == 0.0 ? 0.0 : sy / A * sgn_i;
-                f[2] = A;
+                put(G.fi.data(), out ? out->fi : nullptr, out ? out->pfi : 0, out ? out->fi4 : nullptr,
+                    (long long)(j - 1) * (ni + 1) + F, A == 0.0 ? 0.0 : sx / A * sgn_i,
+                    A == 0.0 ? 0.0 : sy / A * sgn_i, A);
             }
     });
     parallel_rows(nj + 1, 24L * ni, [&](long long r0, long long r1) {
@@ -170,10 +194,9 @@ int setup_block(int ni, int nj, const double* nodes, const double* area, int sou
                 const double dx = X(i - 1, Gf).x - X(i, Gf).x, dy = X(i - 1, Gf).y - X(i, Gf).y;
                 const double sx = dy, sy = -dx;
                 const double A = std::sqrt(sx * sx + sy * sy);
-                double* f = &G.fj[3 * ((size_t)Gf * ni + (i - 1))];
-                f[0] = A == 0.0 ? 0.0 : sx / A * sgn_j;
-                f[1] = A == 0.0 ? 0.0 : sy / A * sgn_j;
-                f[2] = A;
+                put(G.fj.data(), out ? out->fj : nullptr, out ? out->pfj : 0, out ? out->fj4 : nullptr,
+                    (long long)Gf * ni + (i - 1), A == 0.0 ? 0.0 : sx / A * sgn_j, A == 0.0 ? 0.0 : sy / A * sgn_j,
+                    A);
             }
     });
     // source geometry (Precompute_Axisymmetric_Geometry / Precompute_Area_Geometry)

@@ -91,9 +91,22 @@ struct HostGeom {
     int g(int i, int j) const { return (j + 2) * (ni + 4) + (i + 2); }
 };
 
+// Where setup_block writes the face geometry instead of G.fi / G.fj: the device images of the
+// face planes (plane q of i-face k at fi[q * pfi + k], j-faces alike) and, when given, their
+// FP32 float4 records (fi4[4 k + q], the 4th component 0).
+struct FaceOut {
+    double* fi = nullptr;
+    double* fj = nullptr;
+    long long pfi = 0, pfj = 0;
+    float* fi4 = nullptr;
+    float* fj4 = nullptr;
+};
+
 // Interior metrics, face normals and source geometry of a block. nodes: (2, 0:ni, 0:nj)
-// Fortran order; area: nodal cross-section or nullptr. Returns a Q2D_* status.
-int setup_block(int ni, int nj, const double* nodes, const double* area, int source, HostGeom& G);
+// Fortran order; area: nodal cross-section or nullptr. With out, the faces go there (and
+// G.fi / G.fj stay empty). Returns a Q2D_* status.
+int setup_block(int ni, int nj, const double* nodes, const double* area, int source, HostGeom& G,
+                const FaceOut* out = nullptr);
 
 // Ghost-cell metrics of one boundary record (BC_Connect_Metrics / BC_Symmetry_Metrics /
 // BC_Extrapolate_Metrics, Lib_Metrics.f90:285-553). donor/donor_nodes only for type 101.
